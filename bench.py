@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Benchmark of the GPU global-routing hot path (InstantGR's metric: route
+wall time and nets/s at equal evaluator score).
+
+One step = one complete route of the synthetic design with the design already
+read and its trees built (inputs resident): phase 1 (colouring, per-batch
+cost refresh, tree DP, commit) and `--rrr-iters` rip-up-and-reroute passes.
+Default workload: 10 layers, 840x1140 GCells, 130,000 nets, 3 RRR passes.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (the router does not shard), one per GPU;
+`value` is the nets of all replicas over the slowest replica's time.
+`--impl reference` times the CPU restatement of the same hot path (the
+oracle: cost refresh, tree DP and commit per batch, phase 1 only) on the host
+cores, on a bounded sample of the same plan.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    0: dict(name="256x256x10, 20k nets", X=256, Y=256, nets=20000),
+    1: dict(name="840x1140x10, 130k nets, 1% 65-500-pin nets, 3 RRR passes", X=840, Y=1140, nets=130000),
+    2: dict(name="1600x1600x10, 800k nets, pin mixture, 6 hotspots", X=1600, Y=1600, nets=800000),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=1)
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--rrr-iters", type=int, default=3)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--workdir", default=os.environ.get("IGR_BENCH_DIR", "/tmp/igr_bench"))
+    ap.add_argument("--cpu-batches", type=int, default=0, help="batches in the CPU sample (0 = auto)")
+    return ap.parse_args()
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.p = None
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.rows.append([s.strip() for s in line.split(",")])
+
+    def stop(self) -> dict:
+        if not self.p:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["nvidia-smi unavailable"])
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) > 8 for i in range(4) if r[5 + i] == "Active"})
+        return dict(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=max(mx) if mx else None,
+                    reasons=reasons, samples=len(self.rows))
+
+
+def design_files(args) -> tuple[str, str]:
+    os.makedirs(args.workdir, exist_ok=True)
+    base = os.path.join(args.workdir, f"c{args.config}_s{args.seed}_x{args.scale:g}")
+    cap, net = base + ".cap", base + ".net"
+    if not (os.path.exists(cap) and os.path.exists(net)):
+        import instantgr_b200 as ig
+        tmpc, tmpn = cap + f".{os.getpid()}", net + f".{os.getpid()}"
+        ig.generate(args.config, args.seed, args.scale, tmpc, tmpn)
+        os.replace(tmpc, cap)
+        os.replace(tmpn, net)
+    return cap, net
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return dict(hbm_gbs=d.get("hbm_gbs", 6650.0), src="of measured")
+    return dict(hbm_gbs=6650.0, src="of fallback")
+
+
+def profile_traffic() -> dict:
+    """Per-launch DRAM traffic of the cost refresh from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        return json.load(open(p))
+    return {}
+
+
+def cpu_sample(router, grid, plan, max_batches: int, budget_s: float = 20.0):
+    """CPU restatement (oracle) of the phase-1 hot path on the first batches of the
+    same plan: per batch a full cost refresh, the tree DP and the commits."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle_py import Oracle
+    o = Oracle(grid)
+    N = o.N
+    dem = np.zeros(N, np.float32)
+    pre = np.zeros(N, np.int32)
+    st = np.zeros(N, np.int32)
+    w = np.zeros(N, np.float32)
+    boff = plan["batch_off"]
+    nb = len(boff) - 1
+    cap = plan["route_cap"].astype(np.int64)
+    roff = np.concatenate([[0], np.cumsum(cap)[:-1]]).astype(np.int64)
+    routes = np.zeros(int(cap.sum()) + 1, np.int32)
+    t0 = time.perf_counter()
+    nets = 0
+    b = 0
+    while b < nb and (max_batches == 0 or b < max_batches):
+        a, e = int(boff[b]), int(boff[b + 1])
+        _, vc, ps = o.cost_refresh(dem)
+        n0, n1 = int(plan["node_off"][a]), int(plan["node_off"][e])
+        o.pattern_route(vc, ps, plan["node_off"][a:e + 1] - n0, plan["nodes"][n0:n1], plan["par"][n0:n1],
+                        roff[a:e], plan["route_cap"][a:e], routes, pre, st, b + 1)
+        o.commit_wires(pre, dem, st, b + 1)
+        o.commit_vias(roff[a:e], routes, dem, st, b + 1, 1)
+        nets += e - a
+        b += 1
+        if max_batches == 0 and time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return nets / dt, dict(batches=b, of_batches=nb, nets=nets, seconds=dt)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    cfg = CONFIGS[args.config]
+    workload = dict(workload=f"global routing, {cfg['name']}", config_index=args.config, scale=args.scale,
+                    rrr_iters=args.rrr_iters, seed=args.seed, l2="per-step state exceeds L2 (inputs larger than L2)")
+    if args.impl == "reference":
+        return bench_reference(args, rank, world, workload)
+
+    import torch
+    import numpy as np
+    import instantgr_b200 as ig
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    ig.set_device(local)
+    cap, net = design_files(args) if rank == 0 or world == 1 else (None, None)
+    if dist:
+        dist.barrier()
+        cap, net = design_files(args)
+
+    r = ig.Router(cap, net, rrr_iters=args.rrr_iters, profile=1)
+    design_nets, routing_nets = r.sizes()
+    for _ in range(max(args.warmup, 0)):
+        r.run()
+
+    def sync_all():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    clk = Clocks(local)
+    sync_all()
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    launches = 0
+    ks_tot = {}
+    for _ in range(args.steps):
+        r.run()
+        launches += int(r.stats()["launches"])
+        for k, v in r.kstats().items():
+            t = ks_tot.setdefault(k, dict(launches=0, ms=0.0, bytes=0.0))
+            for f in t:
+                t[f] += v[f]
+    e1.record()
+    sync_all()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    tmax = torch.tensor([ms], device="cuda")
+    if dist:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    ms_max = float(tmax.item())
+    st = r.stats()
+
+    # e2e: the whole `-cap/-net/-out` call with host files, K steps
+    out = os.path.join(args.workdir, f"guides_r{rank}.out")
+    sync_all()
+    e0.record()
+    for _ in range(args.steps):
+        ig.route_files(cap, net, out, rrr_iters=args.rrr_iters)
+    e1.record()
+    sync_all()
+    ms_e2e = e0.elapsed_time(e1)
+    te = torch.tensor([ms_e2e], device="cuda")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    ms_e2e = float(te.item())
+
+    result = None
+    if rank == 0:
+        value = design_nets * args.steps * world / (ms_max / 1e3)
+        e2e_value = design_nets * args.steps * world / (ms_e2e / 1e3)
+        L, X, Y = 9, cfg["X"], cfg["Y"]
+        cells = L * X * Y
+        h2d = cells * 4 + (X + Y) * 4  # capacity and edge lengths each open, trees, batches (below)
+        plan = r.plan()
+        h2d += (plan["nodes"].size * 2 + plan["node_off"].size + plan["net_ids"].size) * 4
+        d2h = int(sum(plan["route_cap"])) * 4 + cells * 0
+        # dominant kernel and its roofline
+        dom = max(ks_tot, key=lambda k: ks_tot[k]["ms"])
+        cr = ks_tot["cost_refresh"]
+        pk = measured_peaks()
+        tr = profile_traffic()
+        ach = cr["bytes"] / (cr["ms"] / 1e3) / 1e9 if cr["ms"] else 0.0
+        roof = dict(kernel="cost_refresh (fused wire/via cost + f64 Sklansky prefix sums)", bound="hbm",
+                    achieved=round(ach, 1), peak=pk["hbm_gbs"], unit="GB/s",
+                    frac=round(ach / pk["hbm_gbs"], 4), peak_src=pk["src"],
+                    traffic=tr.get("cost_refresh_bytes_per_launch"),
+                    algorithmic_bytes_per_launch=cr["bytes"] / max(cr["launches"], 1),
+                    avg_launch_us=1e3 * cr["ms"] / max(cr["launches"], 1),
+                    dominant_kernel=dom, kernel_ms_per_step={k: round(v["ms"] / args.steps, 3)
+                                                             for k, v in ks_tot.items()})
+        cpu = None
+        if world == 1:
+            try:
+                g = r.grid()
+                v, info = cpu_sample(r, g, plan, args.cpu_batches)
+                cpu = dict(value=round(v, 2), unit="nets/s", cores=1, kind="port",
+                           sample=f"oracle phase-1 (cost refresh + tree DP + commit) on the first "
+                                  f"{info['batches']} of {info['of_batches']} batches ({info['nets']} nets, "
+                                  f"{info['seconds']:.1f} s)")
+            except Exception as ex:  # the CPU baseline is reported, never required
+                cpu = dict(value=None, unit="nets/s", cores=1, kind="port", sample=f"failed: {ex}")
+        result = dict(metric="route throughput (nets/s), plain RRR router", value=round(value, 2), unit="nets/s",
+                      n_gpus=world, steps=args.steps, warmup=args.warmup, ms_per_step=round(ms_max / args.steps, 3),
+                      higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32/f64 costs, i32 demand",
+                      data="synthetic (seeded generator, ISPD2024 format)", config=workload,
+                      parallelism="replicas" if world > 1 else "single GPU",
+                      e2e=dict(value=round(e2e_value, 2), unit="nets/s", h2d_bytes_per_step=int(h2d),
+                               d2h_bytes_per_step=int(d2h)),
+                      roofline=roof, cpu_baseline=cpu, clocks=clocks, gpu_launches=launches,
+                      detail=dict(design_nets=design_nets, routing_nets=routing_nets,
+                                  wirelength=st["wirelength"], via_cost=st["via_cost"],
+                                  overflow_cost=st["overflow_cost"], batches1=st["batches1"],
+                                  rerouted_last=st["rerouted"], p1_ms=st["p1_ms"], rrr_ms=st["rrr_ms"],
+                                  dag_host_ms=st["dag_host_ms"], route_s=st["route_s"]))
+        print(json.dumps(result), flush=True)
+    r.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def bench_reference(args, rank, world, workload):
+    """CPU restatement of the hot path (oracle port) on the host cores, rank 0 only."""
+    if rank != 0:
+        return None
+    import instantgr_b200 as ig
+    cap, net = design_files(args)
+    r = ig.Router(cap, net, rrr_iters=0)
+    r.run()  # plan (batches and trees) of the same design
+    g = r.grid()
+    plan = r.plan()
+    design_nets, _ = r.sizes()
+    vals, infos = [], []
+    nb = args.cpu_batches or 3
+    for i in range(args.warmup + args.steps):
+        v, info = cpu_sample(r, g, plan, nb)
+        if i >= args.warmup:
+            vals.append(v)
+            infos.append(info)
+    v = statistics.median(vals)
+    sample = (f"oracle phase-1 (cost refresh + tree DP + commit) on the first {infos[0]['batches']} of "
+              f"{infos[0]['of_batches']} batches ({infos[0]['nets']} nets) per step")
+    res = dict(impl="reference", metric="route throughput (nets/s), plain RRR router", value=round(v, 2),
+               unit="nets/s", n_gpus=world, steps=args.steps, warmup=args.warmup,
+               ms_per_step=round(1e3 * infos[0]["nets"] / v, 3), higher_is_better=True, scaling="weak",
+               vs_baseline=None, dtype="f32/f64 costs, i32 demand", data="synthetic (seeded generator)",
+               config=workload,
+               cpu_baseline=dict(value=round(v, 2), unit="nets/s", cores=1, kind="port", sample=sample),
+               e2e=dict(value=round(v, 2), unit="nets/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(res), flush=True)
+    r.close()
+    return res
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,216 @@
+/*
+ * instantgr_b200 — C ABI of a B200-native (sm_100a) GPU global router that is
+ * a drop-in for InstantGR's routing hot path.
+ *
+ * Two levels:
+ *   1. The router: the whole `-cap <f> -net <f> -out <f>` flow of InstantGR
+ *      (src/main.cpp:91-102, route() at :22-73) behind igr_route_files and
+ *      the igr_router_* calls, which a host program can drive stage by stage.
+ *   2. The device operators of the hot path, one per kernel group of
+ *      InstantGR, on an igr_ctx that owns all device state of one routing grid.
+ *
+ * Conventions
+ *   - Every call returns 0 on success or a negative IGR_ERR_* code; the
+ *     message of the last failure is returned by igr_last_error().  No call
+ *     exits the process (InstantGR calls exit() on CUDA errors,
+ *     src/Lshape_route_detour.hpp:1088-1091).
+ *   - Positions use InstantGR's encoding pos = l*X*Y + x*Y + y, with l the
+ *     routing layer (file layer - 1, src/database_cuda.hpp:2106).  Grid arrays
+ *     passed in or out are in InstantGR's layout [l][x][y] (y fastest).
+ *   - Calls on one context are ordered on its CUDA stream and must come from
+ *     one host thread at a time.  Host buffers belong to the caller.
+ *   - Route records are InstantGR's: int count c at [0] (the next free
+ *     slot, so c = 1 + 2 * pairs), then c-1 ints of position pairs.
+ */
+#ifndef INSTANTGR_B200_H
+#define INSTANTGR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IGR_OK 0
+#define IGR_ERR_INVALID (-1)  /* bad argument */
+#define IGR_ERR_IO (-2)       /* file could not be read or written */
+#define IGR_ERR_FORMAT (-3)   /* malformed .cap/.net */
+#define IGR_ERR_CUDA (-4)     /* CUDA runtime error (no device, launch failure, ...) */
+#define IGR_ERR_CAPACITY (-5) /* a fixed-size buffer or limit was exceeded */
+#define IGR_ERR_TIMEOUT (-6)  /* a bounded device wait gave up */
+#define IGR_ERR_STATE (-7)    /* inconsistent input (e.g. a tree that is not in preorder) */
+
+typedef struct igr_ctx igr_ctx;
+typedef struct igr_router igr_router;
+
+/* ------------------------------------------------------------------ router */
+
+typedef struct igr_options {
+    int rrr_iters;     /* rip-up-and-reroute iterations after phase 1 (InstantGR: 1) */
+    int threads;       /* host threads, 0 = all cores */
+    int mode;          /* DAG size mode of InstantGR (0..2); -1 = choose by net count as main.cpp:39-40 */
+    int verbose;       /* print stage times to stderr */
+    int batched;       /* 1 = size-class persistent kernels + CUDA graphs (same results as 0) */
+    int profile;       /* 1 = time every kernel launch with CUDA events (igr_router_kstats) */
+    int reserved[7];
+} igr_options;
+
+/* Fills `o` with the defaults that reproduce InstantGR (1 RRR pass). */
+void igr_default_options(igr_options *o);
+
+/* Whole flow: read .cap/.net, route, write route guides.
+ * Replaces `InstantGR -cap <cap> -net <net> -out <out>` (src/main.cpp:91-102). */
+int igr_route_files(const char *cap_path, const char *net_path, const char *out_path, const igr_options *opt);
+
+/* Stage-by-stage control of the same flow. */
+int igr_router_open(const char *cap_path, const char *net_path, const igr_options *opt, igr_router **out);
+/* Routes (or re-routes from empty demand): phase 1, then opt->rrr_iters
+ * rip-up-and-reroute passes (src/main.cpp:22-73). */
+int igr_router_run(igr_router *r);
+/* Writes the route guides (src/graph.hpp:179-235). */
+int igr_router_write(igr_router *r, const char *out_path);
+/* Statistics of the last run: [0] routing nets, [1] nets rerouted in the last
+ * pass, [2] wirelength, [3] via count, [4] overflow cost (GPU estimate,
+ * src/graph.hpp:148-169), [5] route wall seconds, [6] phase-1 batches,
+ * [7] phase-1 device ms, [8] rip-up/reroute device ms, [9] host DAG ms,
+ * [10] kernel launches, [11] design nets. */
+int igr_router_stats(igr_router *r, double *out, int n);
+/* Per-kernel-class device time of the last run (needs opt->profile): for
+ * class k in {cost refresh, tree DP, wire commit, via commit, DAG DP,
+ * colouring, rip-up/marking}, out[3k] = launches, out[3k+1] = milliseconds,
+ * out[3k+2] = algorithmic DRAM bytes (cost refresh: 20 per refreshed cell). */
+int igr_router_kstats(igr_router *r, double *out, int n);
+/* Phase-1 plan of the last run: routing order, batch offsets and trees.
+ * sizes[0..2] receive the number of nets, batches and tree nodes; the arrays
+ * (net_ids[n], batch_off[b+1], node_off[n+1], nodes[m], par[m], route_cap[n],
+ * all in routing order) are filled when non-null. */
+int igr_router_plan(igr_router *r, int64_t *sizes, int32_t *net_ids, int32_t *batch_off, int32_t *node_off,
+                    int32_t *nodes, int32_t *par, int32_t *route_cap);
+/* Grid of the design in the layout of igr_grid_desc: hdr = {L, X, Y, dir0},
+ * costs = {unit_wire, unit_via, short_cost[L]}, edge lengths, capacity. */
+int igr_router_grid(igr_router *r, int32_t *hdr, double *costs, int32_t *x_edge_len, int32_t *y_edge_len,
+                    float *capacity);
+/* Selects the CUDA device of the calling thread for subsequent calls. */
+int igr_set_device(int device);
+/* Number of design nets and routing nets. */
+int igr_router_sizes(igr_router *r, int64_t *design_nets, int64_t *routing_nets);
+/* Route record of routing net `net` (phase 1 or its latest reroute). */
+int igr_router_route(igr_router *r, int net, int32_t *out, int cap, int *len);
+/* Selected pins of design net `net` (net::init, src/database.hpp:38-243):
+ * record npins, pins (file-layer positions, ascending), nextra, extra pairs.
+ * Available right after igr_router_open (no GPU needed). */
+int igr_router_pins(igr_router *r, int net, int32_t *out, int cap, int *len);
+/* Device demand of the grid ([l][x][y], routing layers). */
+int igr_router_demand(igr_router *r, float *out);
+void igr_router_close(igr_router *r);
+
+/* Synthetic ISPD2024-style design (no counterpart in InstantGR, whose
+ * benchmarks are external).  cfg: 0..4 = the configurations of the
+ * benchmark suite of this project; scale (0,1] shrinks the net count. */
+int igr_generate(int cfg, uint64_t seed, double scale, const char *cap_path, const char *net_path);
+/* Same, with explicit sizes. */
+int igr_generate_custom(int X, int Y, int nets, uint64_t seed, int cap_mode, double block_frac, int pin_mode,
+                        double hifanout_frac, double bbox_median, double bbox_sigma, int hotspots,
+                        double hotspot_frac, const char *cap_path, const char *net_path);
+
+/* ------------------------------------------------------------------ device operators */
+
+typedef struct igr_grid_desc {
+    int32_t L, X, Y;            /* routing layers (9), grid */
+    int32_t dir0;               /* direction of routing layer 0: 0 = horizontal, 1 = vertical */
+    const int32_t *x_edge_len;  /* [X-1] */
+    const int32_t *y_edge_len;  /* [Y-1] */
+    double unit_wire, unit_via;
+    const double *short_cost;   /* [L] overflow weight per routing layer */
+    const float *capacity;      /* [L][X][Y] */
+} igr_grid_desc;
+
+/* Device state of one grid: capacity, demand, cost tables, difference array,
+ * timestamps (build_cuda_database, src/database_cuda.hpp:2096-2362). */
+int igr_create(const igr_grid_desc *g, igr_ctx **out);
+int igr_destroy(igr_ctx *c);
+const char *igr_last_error(const igr_ctx *c);
+
+/* Demand in and out ([l][x][y]).  Setting demand marks every track dirty. */
+int igr_set_demand(igr_ctx *c, const float *demand);
+int igr_get_demand(igr_ctx *c, float *demand);
+/* Timestamps and the difference array ([l][x][y]), for replay and checks. */
+int igr_get_stamp(igr_ctx *c, int32_t *stamp);
+int igr_get_pre(igr_ctx *c, int32_t *pre);
+
+/* Fused cost refresh: wire cost, via cost and per-track prefix sums
+ * (update_wcost_cuda_ispd24 + update_vcost_ispd24 + compute_presum,
+ * src/graph.hpp:40-71, :101-104, :405-430).  only_dirty != 0 recomputes only
+ * tracks whose demand changed since the previous refresh. */
+int igr_cost_refresh(igr_ctx *c, int only_dirty);
+/* Cost tables after a refresh: vcost f32 and presum f64, [l][x][y]. */
+int igr_get_costs(igr_ctx *c, float *vcost, double *presum);
+/* Loads a cost map (for replaying a reference cost map into the DP). */
+int igr_set_costs(igr_ctx *c, const float *vcost, const double *presum);
+
+/* Phase-1 tree DP (Lshape_route_cuda, src/Lshape_route.hpp:9-153) for a
+ * batch of n nets.  Trees: nodes in DFS preorder (node_off[n+1] CSR), node
+ * positions in InstantGR's encoding with layer 9 for Steiner nodes, par[i] the
+ * local index of the parent (-1 at the root).  route_cap[k] ints are
+ * available for net k; routes are written to routes_out at route_off[k].
+ * Wires go to the difference array; call igr_commit_wires afterwards. */
+int igr_pattern_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t *nodes, const int32_t *par,
+                      const int64_t *route_off, const int32_t *route_cap, int32_t *routes_out, int32_t stamp);
+/* Difference-array commit (compute_presum_general + commit_all_edge + memset,
+ * src/graph.hpp:74-137). */
+int igr_commit_wires(igr_ctx *c, int32_t stamp);
+/* Via demand of n route records (commit_via_demand, src/graph.hpp:496-543),
+ * K = +1 to add, -1 to remove. */
+int igr_commit_vias(igr_ctx *c, int n, const int64_t *route_off, const int32_t *routes, int32_t stamp, int32_t K);
+/* Wire demand of n route records by atomics (commit_wire_demand,
+ * src/graph.hpp:468-495), K = -1 for rip-up. */
+int igr_ripup_wires(igr_ctx *c, int n, const int64_t *route_off, const int32_t *routes, int32_t stamp, int32_t K);
+/* Rip-up marking (mark_overflow_edges/_nets, src/graph.hpp:432-466). */
+int igr_mark_overflow(igr_ctx *c, int n, const int64_t *route_off, const int32_t *routes, int32_t threshold,
+                      int32_t min_edges, uint8_t *is_of_out);
+/* Congestion view (extract_congestionView*, src/graph.hpp:545-584), [x][y]. */
+int igr_congestion_view(igr_ctx *c, float *xsum, float *ysum);
+/* Overflow cost and counters (report_score, src/graph.hpp:148-169). */
+int igr_score(igr_ctx *c, double *wirelength, double *vias, double *overflow);
+
+/* Batch colouring (generate_batches_rsmt_gpu, src/database_cuda.hpp:437-631),
+ * deterministic.  Nets in priority order (the last wins conflicts); CSR of
+ * 2-D conflict points and of tree segments (pairs of 2-D cells). */
+int igr_color_batches(igr_ctx *c, int n, const int32_t *pt_off, const int32_t *pts, const int32_t *h_off,
+                      const int32_t *hseg, const int32_t *v_off, const int32_t *vseg, int32_t sparsity,
+                      int32_t *batch_out, int32_t *n_batches);
+
+/* Phase-2 DAG DP (precompute_cost_edge + Lshape_route_node_layer_change_cuda
+ * + get_routing_tree_layer_change_cuda, src/Lshape_route_detour.hpp:123-195,
+ * :281-406, :520-694) for a batch of n nets.  DAG CSR per net: nodes in
+ * topological order (children before parents is NOT required; depth[] gives
+ * the level), par_off/par/child_slot per node, child_num per node. */
+int igr_dag_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t *nodes, const int32_t *depth,
+                  const int32_t *par_off, const int32_t *par, const int32_t *child_slot, const int32_t *child_num,
+                  const int64_t *route_off, const int32_t *route_cap, int32_t *routes_out, int32_t stamp);
+
+/* ------------------------------------------------------------------ host passes */
+
+/* Detour DAG of one net (net::generate_detours_reconstruct,
+ * src/database_cuda.hpp:1429-2086).  Tree of ntree nodes: positions pos[]
+ * (layer 9 marks Steiner nodes), adjacency CSR adj_off[ntree+1]/adj.
+ * Congestion view xsum/ysum as returned by igr_congestion_view.  The result
+ * record is m, nodes[m], par_num[m], child_num[m], depth[m], E, par[E],
+ * child_idx[E], npoints, points[npoints] with nodes in topological order
+ * (parents first).  *len receives its length; nothing is written when
+ * cap < *len. */
+int igr_build_dag(int X, int Y, int mode, int ntree, const int32_t *pos, const int32_t *adj_off, const int32_t *adj,
+                  const float *xsum, const float *ysum, int32_t *out, int64_t cap, int64_t *len);
+
+/* Steiner provider used in place of FLUTE (flute::flute, src/flute.hpp:1239;
+ * its POST9.dat table is absent).  Nodes: distinct input points in ascending
+ * (x, y) order, then Steiner points; edges as node index pairs. */
+int igr_steiner(int n, const int32_t *x, const int32_t *y, int32_t *node_x, int32_t *node_y, int cap_nodes,
+                int *n_nodes, int32_t *edges, int cap_edges, int *n_edges);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* INSTANTGR_B200_H */

@@ -1,0 +1,688 @@
+// extern "C" entry points of include/instantgr_b200.h.
+//
+// Every entry point catches all exceptions and returns a status code with the
+// message kept for igr_last_error(); nothing here exits the process.
+#include "../../include/instantgr_b200.h"
+
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+
+#include "router.hpp"
+
+using namespace igr;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(std::string *slot, int code, const std::string &msg) {
+    if (slot) *slot = msg;
+    g_last_error = msg;
+    return code;
+}
+
+template <typename F>
+int guard(std::string *slot, F &&f) {
+    try {
+        f();
+        return IGR_OK;
+    } catch (const Error &e) {
+        return fail(slot, e.code, e.what());
+    } catch (const std::bad_alloc &) {
+        return fail(slot, IGR_ERR_CAPACITY, "out of host memory");
+    } catch (const std::exception &e) {
+        return fail(slot, IGR_ERR_INVALID, e.what());
+    }
+}
+
+}  // namespace
+
+struct igr_router {
+    Router r;
+    std::string err;
+};
+
+struct igr_ctx {
+    GridOwner go;
+    cudaStream_t s = nullptr;
+    std::string err;
+    // staging buffers reused across calls
+    DevBuf<int> a, b, c, d, e, f, h, i, routes;
+    DevBuf<int64_t> off;
+    DevBuf<double> scr;
+    DevBuf<uint8_t> u8;
+    DevBuf<float> f1, f2;
+    DevBuf<double> d1;
+    DevBuf<unsigned> bar;
+};
+
+extern "C" {
+
+void igr_default_options(igr_options *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof *o);
+    o->rrr_iters = 1;
+    o->threads = 0;
+    o->mode = -1;
+    o->verbose = 0;
+    o->batched = 0;
+}
+
+static void apply_options(Router &r, const igr_options *o) {
+    igr_options def;
+    igr_default_options(&def);
+    if (!o) o = &def;
+    if (o->rrr_iters < 0) throw Error(ERR_INVALID, "rrr_iters must be >= 0");
+    r.rrr_iters = o->rrr_iters;
+    r.threads = o->threads;
+    r.mode = o->mode;
+    r.verbose = o->verbose;
+    r.batched = o->batched;
+    r.kt.on = o->profile != 0;
+}
+
+int igr_router_open(const char *cap, const char *net, const igr_options *opt, igr_router **out) {
+    if (!cap || !net || !out) return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    *out = nullptr;
+    auto *h = new igr_router();
+    int rc = guard(&h->err, [&] {
+        apply_options(h->r, opt);
+        h->r.open(cap, net);
+    });
+    if (rc) { delete h; return rc; }
+    *out = h;
+    return IGR_OK;
+}
+
+int igr_router_run(igr_router *h) {
+    if (!h) return fail(nullptr, IGR_ERR_INVALID, "null router");
+    return guard(&h->err, [&] { h->r.run(); });
+}
+
+int igr_router_write(igr_router *h, const char *out) {
+    if (!h || !out) return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    return guard(&h->err, [&] {
+        if (h->r.h_routes.empty() && !h->r.ns.nets.empty()) throw Error(ERR_STATE, "route before writing");
+        h->r.write(out);
+    });
+}
+
+int igr_router_stats(igr_router *h, double *o, int n) {
+    if (!h || !o) return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    const auto &r = h->r;
+    double v[12] = {(double)r.ns.nets.size(), (double)r.st.rerouted, r.score_wl, r.score_via, r.score_of,
+                    r.st.wall, (double)r.st.batches1, r.st.p1_ms, r.st.rrr_ms, r.st.dag_host_ms,
+                    (double)r.st.launches, (double)r.d.num_nets()};
+    for (int k = 0; k < n && k < 12; k++) o[k] = v[k];
+    return IGR_OK;
+}
+
+int igr_router_kstats(igr_router *h, double *o, int n) {
+    if (!h || !o) return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    const auto &r = h->r;
+    for (int k = 0; k < KC_N; k++) {
+        double v[3] = {(double)r.kt.launches[k], r.kt.ms[k], k == KC_COST ? 20.0 * (double)r.cost_cells : 0.0};
+        for (int j = 0; j < 3; j++)
+            if (3 * k + j < n) o[3 * k + j] = v[j];
+    }
+    return IGR_OK;
+}
+
+int igr_router_plan(igr_router *h, int64_t *sizes, int32_t *net_ids, int32_t *batch_off, int32_t *node_off,
+                    int32_t *nodes, int32_t *par, int32_t *route_cap) {
+    if (!h || !sizes) return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    return guard(&h->err, [&] {
+        const auto &r = h->r;
+        if (r.plan_node_off.empty()) throw Error(ERR_STATE, "route before reading the plan");
+        sizes[0] = (int64_t)r.plan_ids.size();
+        sizes[1] = (int64_t)r.plan_batch_off.size() - 1;
+        sizes[2] = (int64_t)r.plan_nodes.size();
+        auto cp = [](int32_t *o, const std::vector<int> &v) {
+            if (o && !v.empty()) std::memcpy(o, v.data(), v.size() * 4);
+        };
+        cp(net_ids, r.plan_ids);
+        cp(batch_off, r.plan_batch_off);
+        cp(node_off, r.plan_node_off);
+        cp(nodes, r.plan_nodes);
+        cp(par, r.plan_par);
+        if (route_cap)
+            for (size_t i = 0; i < r.plan_ids.size(); i++) route_cap[i] = r.plan_cap[i];
+    });
+}
+
+int igr_router_grid(igr_router *h, int32_t *hdr, double *costs, int32_t *xl, int32_t *yl, float *cap) {
+    if (!h) return fail(nullptr, IGR_ERR_INVALID, "null router");
+    return guard(&h->err, [&] {
+        const auto &d = h->r.d;
+        const int L = d.L - 1, X = d.X, Y = d.Y;
+        if (hdr) { hdr[0] = L; hdr[1] = X; hdr[2] = Y; hdr[3] = d.layer_dir[1]; }
+        if (costs) {
+            costs[0] = d.unit_wire;
+            costs[1] = d.unit_via;
+            for (int l = 0; l < L; l++) costs[2 + l] = d.short_cost[l + 1];
+        }
+        if (xl) std::memcpy(xl, d.x_edge_len.data(), 4 * (size_t)(X - 1));
+        if (yl) std::memcpy(yl, d.y_edge_len.data(), 4 * (size_t)(Y - 1));
+        if (cap) std::memcpy(cap, d.cap.data() + (size_t)X * Y, 4 * (size_t)L * X * Y);
+    });
+}
+
+int igr_set_device(int device) {
+    return guard(nullptr, [&] { cuda_check(cudaSetDevice(device), "cudaSetDevice"); });
+}
+
+int igr_router_sizes(igr_router *h, int64_t *dn, int64_t *rn) {
+    if (!h) return fail(nullptr, IGR_ERR_INVALID, "null router");
+    if (dn) *dn = h->r.d.num_nets();
+    if (rn) *rn = (int64_t)h->r.ns.nets.size();
+    return IGR_OK;
+}
+
+int igr_router_route(igr_router *h, int net, int32_t *out, int cap, int *len) {
+    if (!h || !len) return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    return guard(&h->err, [&] {
+        auto &r = h->r;
+        if (net < 0 || net >= (int)r.ns.nets.size()) throw Error(ERR_INVALID, "net id out of range");
+        if (r.h_routes.empty()) throw Error(ERR_STATE, "route before reading routes");
+        const int *rec = r.route_of(net);
+        *len = rec[0];
+        if (out) {
+            if (cap < rec[0]) throw Error(ERR_CAPACITY, "output buffer too small");
+            std::memcpy(out, rec, sizeof(int) * rec[0]);
+        }
+    });
+}
+
+int igr_router_pins(igr_router *h, int net, int32_t *out, int cap, int *len) {
+    if (!h || !len) return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    return guard(&h->err, [&] {
+        const auto &d = h->r.d;
+        if (net < 0 || net >= d.num_nets()) throw Error(ERR_INVALID, "net id out of range");
+        std::vector<int> p(d.sel.begin() + d.sel_off[net], d.sel.begin() + d.sel_off[net + 1]);
+        std::sort(p.begin(), p.end());
+        std::vector<int> v{(int)p.size()};
+        v.insert(v.end(), p.begin(), p.end());
+        v.push_back((int)(d.extra_off[net + 1] - d.extra_off[net]) / 2);
+        v.insert(v.end(), d.extra.begin() + d.extra_off[net], d.extra.begin() + d.extra_off[net + 1]);
+        *len = (int)v.size();
+        if (out) {
+            if (cap < *len) throw Error(ERR_CAPACITY, "output buffer too small");
+            std::memcpy(out, v.data(), v.size() * 4);
+        }
+    });
+}
+
+int igr_router_demand(igr_router *h, float *out) {
+    if (!h || !out) return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    return guard(&h->err, [&] {
+        auto &r = h->r;
+        DevBuf<float> t;
+        t.alloc(r.go.g.N);
+        launch_from_track_layout_f(r.go.g, r.go.demand.p, t.p, r.s);
+        cuda_check(cudaMemcpyAsync(out, t.p, r.go.g.N * sizeof(float), cudaMemcpyDeviceToHost, r.s), "D2H");
+        cuda_check(cudaStreamSynchronize(r.s), "sync");
+    });
+}
+
+void igr_router_close(igr_router *h) { delete h; }
+
+int igr_route_files(const char *cap, const char *net, const char *out, const igr_options *opt) {
+    igr_router *h = nullptr;
+    int rc = igr_router_open(cap, net, opt, &h);
+    if (rc) return rc;
+    rc = igr_router_run(h);
+    if (!rc) rc = igr_router_write(h, out);
+    if (rc) g_last_error = h->err;
+    igr_router_close(h);
+    return rc;
+}
+
+int igr_generate_custom(int X, int Y, int nets, uint64_t seed, int cap_mode, double block_frac, int pin_mode,
+                        double hifanout_frac, double bbox_median, double bbox_sigma, int hotspots,
+                        double hotspot_frac, const char *cap_path, const char *net_path) {
+    if (!cap_path || !net_path) return fail(nullptr, IGR_ERR_INVALID, "null path");
+    return guard(nullptr, [&] {
+        GenParams p;
+        p.X = X; p.Y = Y; p.nets = nets; p.seed = seed; p.cap_mode = cap_mode; p.block_frac = block_frac;
+        p.pin_mode = pin_mode; p.hifanout_frac = hifanout_frac; p.bbox_median = bbox_median;
+        p.bbox_sigma = bbox_sigma; p.hotspots = hotspots; p.hotspot_frac = hotspot_frac;
+        p.hotspot_sigma = 0.04 * std::max(X, Y);
+        generate_design(p, cap_path, net_path);
+    });
+}
+
+int igr_generate(int cfg, uint64_t seed, double scale, const char *cap_path, const char *net_path) {
+    if (scale <= 0 || scale > 1) return fail(nullptr, IGR_ERR_INVALID, "scale must be in (0, 1]");
+    auto nn = [&](int n) { return std::max(2, (int)(n * scale)); };
+    switch (cfg) {
+        case 0: return igr_generate_custom(256, 256, nn(20000), seed, 0, 0.05, 0, 0, 8, 1.0, 0, 0, cap_path, net_path);
+        case 1: return igr_generate_custom(840, 1140, nn(130000), seed, 1, 0, 0, 0.01, 8, 1.0, 0, 0, cap_path, net_path);
+        case 2: return igr_generate_custom(1600, 1600, nn(800000), seed, 1, 0, 1, 0, 10, 1.2, 6, 0.35, cap_path, net_path);
+        case 3: return igr_generate_custom(512, 512, nn(40000), seed, 1, 0, 1, 0, 10, 1.2, 6, 0.35, cap_path, net_path);
+        case 4: return igr_generate_custom(3000, 3000, nn(10000000), seed, 1, 0, 1, 0, 10, 1.2, 4, 0.40, cap_path, net_path);
+        default: return fail(nullptr, IGR_ERR_INVALID, "unknown configuration");
+    }
+}
+
+// ------------------------------------------------------------------ device operators
+int igr_create(const igr_grid_desc *g, igr_ctx **out) {
+    if (!g || !out || !g->x_edge_len || !g->y_edge_len || !g->short_cost || !g->capacity)
+        return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    *out = nullptr;
+    auto *c = new igr_ctx();
+    int rc = guard(&c->err, [&] {
+        cuda_check(cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking), "stream");
+        c->go.create(g->L, g->X, g->Y, g->dir0, g->x_edge_len, g->y_edge_len, g->unit_wire, g->unit_via,
+                     g->short_cost, g->capacity, c->s);
+    });
+    if (rc) {
+        if (c->s) cudaStreamDestroy(c->s);
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return IGR_OK;
+}
+
+int igr_destroy(igr_ctx *c) {
+    if (!c) return IGR_OK;
+    cudaStreamSynchronize(c->s);
+    cudaStream_t s = c->s;
+    delete c;
+    if (s) cudaStreamDestroy(s);
+    return IGR_OK;
+}
+
+const char *igr_last_error(const igr_ctx *c) { return c ? c->err.c_str() : g_last_error.c_str(); }
+
+#define CTX_GUARD(c, ...)                                                       \
+    do {                                                                        \
+        if (!(c)) return fail(nullptr, IGR_ERR_INVALID, "null context");        \
+        return guard(&(c)->err, [&] { __VA_ARGS__; });                          \
+    } while (0)
+
+static void sync_check(igr_ctx *c) {
+    cuda_check(cudaGetLastError(), "launch");
+    cuda_check(cudaStreamSynchronize(c->s), "sync");
+    if (int e = c->go.check_error(c->s)) throw Error(e, "device reported an error");
+}
+
+int igr_set_demand(igr_ctx *c, const float *dem) {
+    CTX_GUARD(c, {
+        if (!dem) throw Error(ERR_INVALID, "null demand");
+        c->f1.upload(dem, c->go.g.N, c->s);
+        launch_to_track_layout(c->go.g, c->f1.p, c->go.demand.p, c->s);
+        c->go.mark_all_dirty(c->s);
+        sync_check(c);
+    });
+}
+
+int igr_get_demand(igr_ctx *c, float *dem) {
+    CTX_GUARD(c, {
+        if (!dem) throw Error(ERR_INVALID, "null demand");
+        c->f1.alloc(c->go.g.N);
+        launch_from_track_layout_f(c->go.g, c->go.demand.p, c->f1.p, c->s);
+        cuda_check(cudaMemcpyAsync(dem, c->f1.p, c->go.g.N * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
+        sync_check(c);
+    });
+}
+
+int igr_get_stamp(igr_ctx *c, int32_t *o) {
+    CTX_GUARD(c, {
+        c->a.alloc(c->go.g.N);
+        launch_from_track_layout_i(c->go.g, c->go.stamp.p, c->a.p, c->s);
+        cuda_check(cudaMemcpyAsync(o, c->a.p, c->go.g.N * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
+        sync_check(c);
+    });
+}
+
+int igr_get_pre(igr_ctx *c, int32_t *o) {
+    CTX_GUARD(c, {
+        c->a.alloc(c->go.g.N);
+        launch_from_track_layout_i(c->go.g, c->go.pre.p, c->a.p, c->s);
+        cuda_check(cudaMemcpyAsync(o, c->a.p, c->go.g.N * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
+        sync_check(c);
+    });
+}
+
+int igr_cost_refresh(igr_ctx *c, int only_dirty) {
+    CTX_GUARD(c, {
+        launch_cost_refresh(c->go.g, only_dirty != 0, c->s);
+        sync_check(c);
+    });
+}
+
+int igr_get_costs(igr_ctx *c, float *vcost, double *presum) {
+    CTX_GUARD(c, {
+        if (vcost) {
+            c->f1.alloc(c->go.g.N);
+            launch_from_track_layout_f(c->go.g, c->go.vcost.p, c->f1.p, c->s);
+            cuda_check(cudaMemcpyAsync(vcost, c->f1.p, c->go.g.N * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
+        }
+        if (presum) {
+            c->d1.alloc(c->go.g.N);
+            launch_from_track_layout_d(c->go.g, c->go.presum.p, c->d1.p, c->s);
+            cuda_check(cudaMemcpyAsync(presum, c->d1.p, c->go.g.N * 8, cudaMemcpyDeviceToHost, c->s), "D2H");
+        }
+        sync_check(c);
+    });
+}
+
+int igr_set_costs(igr_ctx *c, const float *vcost, const double *presum) {
+    CTX_GUARD(c, {
+        if (!vcost || !presum) throw Error(ERR_INVALID, "null cost table");
+        c->f1.upload(vcost, c->go.g.N, c->s);
+        launch_to_track_layout(c->go.g, c->f1.p, c->go.vcost.p, c->s);
+        c->d1.upload(presum, c->go.g.N, c->s);
+        launch_to_track_layout_d(c->go.g, c->d1.p, c->go.presum.p, c->s);
+        cuda_check(cudaMemsetAsync(c->go.dirty_cost.p, 0, c->go.g.ntracks, c->s), "memset");
+        sync_check(c);
+    });
+}
+
+// length of a route-record array given offsets (records must already hold their counts)
+static int64_t records_extent(int n, const int64_t *off, const int32_t *cap_or_null, const int32_t *routes) {
+    int64_t m = 0;
+    for (int k = 0; k < n; k++) {
+        if (off[k] < 0) throw Error(ERR_INVALID, "negative route offset");
+        const int64_t len = cap_or_null ? cap_or_null[k] : (routes ? routes[off[k]] : 1);
+        if (len < 1) throw Error(ERR_INVALID, "route record without a count slot");
+        m = std::max(m, off[k] + len);
+    }
+    return m;
+}
+
+static void check_tree(int n, const int32_t *node_off, const int32_t *nodes, const int32_t *par, int L, int X, int Y) {
+    if (node_off[0] != 0) throw Error(ERR_INVALID, "node_off[0] must be 0");
+    for (int k = 0; k < n; k++) {
+        if (node_off[k + 1] < node_off[k] + 1) throw Error(ERR_INVALID, "every tree needs at least one node");
+        for (int i = node_off[k]; i < node_off[k + 1]; i++) {
+            const int loc = i - node_off[k];
+            if (nodes[i] < 0 || nodes[i] >= (L + 1) * X * Y) throw Error(ERR_INVALID, "node position out of range");
+            if (loc == 0 ? par[i] != -1 : (par[i] < 0 || par[i] >= loc))
+                throw Error(ERR_STATE, "tree nodes must be in preorder with par[i] < i");
+        }
+    }
+}
+
+int igr_pattern_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t *nodes, const int32_t *par,
+                      const int64_t *route_off, const int32_t *route_cap, int32_t *routes_out, int32_t stamp) {
+    CTX_GUARD(c, {
+        if (n < 0 || (n && (!node_off || !nodes || !par || !route_off || !route_cap || !routes_out)))
+            throw Error(ERR_INVALID, "bad arguments");
+        if (n == 0) return;
+        const auto &g = c->go.g;
+        check_tree(n, node_off, nodes, par, g.L, g.X, g.Y);
+        const int64_t ext = records_extent(n, route_off, route_cap, nullptr);
+        const int total = node_off[n];
+        std::vector<int> ids(n);
+        std::iota(ids.begin(), ids.end(), 0);
+        std::vector<int64_t> so(n, -1);
+        int64_t sn = 0;
+        for (int k = 0; k < n; k++) {
+            const int cnt = node_off[k + 1] - node_off[k];
+            if (cnt > kPatternNodeTile) { so[k] = sn; sn += cnt; }
+        }
+        c->a.upload(ids, c->s);
+        c->b.upload(node_off, n + 1, c->s);
+        c->d.upload(nodes, total, c->s);
+        c->e.upload(par, total, c->s);
+        c->f.upload(route_cap, n, c->s);
+        c->off.upload(route_off, n, c->s);
+        DevBuf<int64_t> d_so;
+        d_so.upload(so, c->s);
+        c->scr.alloc((size_t)pattern_scratch_doubles(sn));
+        c->routes.upload(routes_out, (size_t)ext, c->s);
+        TreeBatchDev tb{c->a.p, c->b.p, c->d.p, c->e.p, c->off.p, c->f.p, c->routes.p, c->scr.p, d_so.p, sn, n};
+        launch_pattern_route(g, tb, stamp, c->s);
+        cuda_check(cudaMemcpyAsync(routes_out, c->routes.p, ext * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
+        sync_check(c);
+    });
+}
+
+int igr_commit_wires(igr_ctx *c, int32_t stamp) {
+    CTX_GUARD(c, {
+        launch_wire_commit(c->go.g, stamp, true, c->s);
+        sync_check(c);
+    });
+}
+
+static void upload_records(igr_ctx *c, int n, const int64_t *off, const int32_t *routes) {
+    const int64_t ext = records_extent(n, off, nullptr, routes);
+    std::vector<int> ids(n);
+    std::iota(ids.begin(), ids.end(), 0);
+    c->a.upload(ids, c->s);
+    c->off.upload(off, n, c->s);
+    c->routes.upload(routes, (size_t)ext, c->s);
+}
+
+int igr_commit_vias(igr_ctx *c, int n, const int64_t *off, const int32_t *routes, int32_t stamp, int32_t K) {
+    CTX_GUARD(c, {
+        if (n < 0 || (n && (!off || !routes))) throw Error(ERR_INVALID, "bad arguments");
+        if (n == 0) return;
+        upload_records(c, n, off, routes);
+        launch_via_commit(c->go.g, ViaBatchDev{c->a.p, c->off.p, c->routes.p, n}, stamp, K, c->s);
+        sync_check(c);
+    });
+}
+
+int igr_ripup_wires(igr_ctx *c, int n, const int64_t *off, const int32_t *routes, int32_t stamp, int32_t K) {
+    CTX_GUARD(c, {
+        if (n < 0 || (n && (!off || !routes))) throw Error(ERR_INVALID, "bad arguments");
+        if (n == 0) return;
+        upload_records(c, n, off, routes);
+        launch_wire_ripup(c->go.g, ViaBatchDev{c->a.p, c->off.p, c->routes.p, n}, stamp, K, c->s);
+        sync_check(c);
+    });
+}
+
+int igr_mark_overflow(igr_ctx *c, int n, const int64_t *off, const int32_t *routes, int32_t threshold,
+                      int32_t min_edges, uint8_t *is_of) {
+    CTX_GUARD(c, {
+        if (n < 0 || (n && (!off || !routes || !is_of))) throw Error(ERR_INVALID, "bad arguments");
+        if (n == 0) return;
+        upload_records(c, n, off, routes);
+        c->h.alloc(c->go.g.N);
+        c->u8.alloc(n);
+        launch_mark_overflow(c->go.g, threshold, c->h.p, ViaBatchDev{c->a.p, c->off.p, c->routes.p, n}, min_edges,
+                             c->u8.p, c->s);
+        cuda_check(cudaMemcpyAsync(is_of, c->u8.p, n, cudaMemcpyDeviceToHost, c->s), "D2H");
+        sync_check(c);
+    });
+}
+
+int igr_congestion_view(igr_ctx *c, float *xsum, float *ysum) {
+    CTX_GUARD(c, {
+        if (!xsum || !ysum) throw Error(ERR_INVALID, "null output");
+        const size_t xy = (size_t)c->go.g.X * c->go.g.Y;
+        c->f1.alloc(xy);
+        c->f2.alloc(xy);
+        launch_congestion_view(c->go.g, c->f1.p, c->f2.p, c->s);
+        cuda_check(cudaMemcpyAsync(xsum, c->f1.p, xy * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
+        cuda_check(cudaMemcpyAsync(ysum, c->f2.p, xy * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
+        sync_check(c);
+    });
+}
+
+int igr_score(igr_ctx *c, double *wl, double *vias, double *of) {
+    CTX_GUARD(c, {
+        unsigned long long h[4];
+        double o = 0;
+        launch_overflow_cost(c->go.g, c->go.score.p, c->s);
+        cuda_check(cudaMemcpyAsync(h, c->go.stats.p, sizeof h, cudaMemcpyDeviceToHost, c->s), "D2H");
+        cuda_check(cudaMemcpyAsync(&o, c->go.score.p, sizeof o, cudaMemcpyDeviceToHost, c->s), "D2H");
+        sync_check(c);
+        if (wl) *wl = (double)(int64_t)h[0];
+        if (vias) *vias = (double)(int64_t)h[1];
+        if (of) *of = o;
+    });
+}
+
+int igr_color_batches(igr_ctx *c, int n, const int32_t *pt_off, const int32_t *pts, const int32_t *h_off,
+                      const int32_t *hseg, const int32_t *v_off, const int32_t *vseg, int32_t sparsity,
+                      int32_t *batch_out, int32_t *n_batches) {
+    CTX_GUARD(c, {
+        if (n < 0 || !n_batches || (n && (!pt_off || !pts || !h_off || !v_off || !batch_out)))
+            throw Error(ERR_INVALID, "bad arguments");
+        if (sparsity < 1) throw Error(ERR_INVALID, "sparsity must be >= 1");
+        *n_batches = 0;
+        if (n == 0) return;
+        const int XY = c->go.g.X * c->go.g.Y;
+        std::vector<int> pt_net;
+        for (int k = 0; k < n; k++) {
+            if (pt_off[k + 1] <= pt_off[k]) throw Error(ERR_INVALID, "every net needs a conflict point");
+            for (int i = pt_off[k]; i < pt_off[k + 1]; i++) {
+                if (pts[i] < 0 || pts[i] >= XY) throw Error(ERR_INVALID, "conflict point outside the grid");
+                pt_net.push_back(k);
+            }
+        }
+        for (int i = 0; i < 2 * h_off[n]; i++)
+            if (hseg[i] < 0 || hseg[i] >= XY) throw Error(ERR_INVALID, "segment outside the grid");
+        for (int i = 0; i < 2 * v_off[n]; i++)
+            if (vseg[i] < 0 || vseg[i] >= XY) throw Error(ERR_INVALID, "segment outside the grid");
+        DevBuf<int> po, p, pn, ho, hs, vo, vs, map, bat, sta, flags;
+        po.upload(pt_off, n + 1, c->s); p.upload(pts, pt_off[n], c->s); pn.upload(pt_net, c->s);
+        ho.upload(h_off, n + 1, c->s); hs.upload(hseg, 2 * (size_t)h_off[n], c->s);
+        vo.upload(v_off, n + 1, c->s); vs.upload(vseg, 2 * (size_t)v_off[n], c->s);
+        map.alloc(XY); bat.alloc(n); sta.alloc(n); flags.alloc(8);
+        ColorDev cd;
+        cd.n = n; cd.X = c->go.g.X; cd.Y = c->go.g.Y; cd.sparsity = sparsity;
+        cd.pt_off = po.p; cd.pts = p.p; cd.pt_net = pn.p; cd.h_off = ho.p; cd.hseg = hs.p; cd.v_off = vo.p;
+        cd.vseg = vs.p; cd.npts = pt_off[n]; cd.map = map.p; cd.batch = bat.p; cd.status = sta.p; cd.flags = flags.p;
+        const int nb = run_coloring(cd, 0, c->s);
+        if (nb == -2) throw Error(ERR_TIMEOUT, "colouring barrier timed out");
+        if (nb < 0) throw Error(ERR_CUDA, std::string("colouring launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+        cuda_check(cudaMemcpyAsync(batch_out, bat.p, n * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
+        sync_check(c);
+        *n_batches = nb;
+    });
+}
+
+int igr_dag_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t *nodes, const int32_t *depth,
+                  const int32_t *par_off, const int32_t *par, const int32_t *child_slot, const int32_t *child_num,
+                  const int64_t *route_off, const int32_t *route_cap, int32_t *routes_out, int32_t stamp) {
+    CTX_GUARD(c, {
+        if (n < 0 || (n && (!node_off || !nodes || !depth || !par_off || !par || !child_slot || !child_num ||
+                            !route_off || !route_cap || !routes_out)))
+            throw Error(ERR_INVALID, "bad arguments");
+        if (n == 0) return;
+        const auto &g = c->go.g;
+        const int N = node_off[n], E = par_off[N];
+        if (node_off[0] != 0 || par_off[0] != 0) throw Error(ERR_INVALID, "CSR offsets must start at 0");
+        int D = 0;
+        for (int v = 0; v < N; v++) {
+            if (depth[v] < 0) throw Error(ERR_INVALID, "negative depth");
+            if (child_num[v] < 0 || child_num[v] > 10) throw Error(ERR_INVALID, "at most 10 child slots per node");
+            if (nodes[v] < 0 || nodes[v] >= (g.L + 1) * g.X * g.Y) throw Error(ERR_INVALID, "node out of range");
+            D = std::max(D, depth[v] + 1);
+        }
+        for (int e = 0; e < E; e++) {
+            if (par[e] < 0 || par[e] >= N) throw Error(ERR_INVALID, "parent out of range");
+            if (child_slot[e] < 0 || child_slot[e] >= child_num[par[e]]) throw Error(ERR_INVALID, "child slot out of range");
+        }
+        std::vector<int> echild(E), child_off(N + 1, 0), ids(n);
+        for (int v = 0; v < N; v++) {
+            for (int e = par_off[v]; e < par_off[v + 1]; e++) {
+                echild[e] = v;
+                if (depth[par[e]] >= depth[v]) throw Error(ERR_STATE, "a parent must be shallower than its child");
+            }
+            child_off[v + 1] = child_off[v] + child_num[v];
+        }
+        std::iota(ids.begin(), ids.end(), 0);
+        std::vector<int> cnt(D + 1, 0), ln(N);
+        for (int v = 0; v < N; v++) cnt[depth[v] + 1]++;
+        for (int d = 0; d < D; d++) cnt[d + 1] += cnt[d];
+        std::vector<int> level_off(cnt);
+        int ml = 0;
+        for (int d = 0; d < D; d++) ml = std::max(ml, cnt[d + 1] - cnt[d]);
+        for (int v = 0; v < N; v++) ln[cnt[depth[v]]++] = v;
+        if ((int64_t)N * 100 + 99 > 0x7fffffffLL) throw Error(ERR_CAPACITY, "too many DAG nodes in one batch");
+        const int64_t ext = records_extent(n, route_off, route_cap, nullptr);
+        DevBuf<int> dn, dpo, dp, dcs, dec, dco, dlo, dln, dno, dids, dcap, dlout, dstage, dscnt, dbc;
+        DevBuf<int64_t> droff;
+        DevBuf<double> dcost, dce;
+        DevBuf<unsigned long long> dbest, dpk;
+        dn.upload(nodes, N, c->s); dpo.upload(par_off, N + 1, c->s); dp.upload(par, E, c->s);
+        dcs.upload(child_slot, E, c->s); dec.upload(echild, c->s); dco.upload(child_off, c->s);
+        dlo.upload(level_off, c->s); dln.upload(ln, c->s); dno.upload(node_off, n + 1, c->s);
+        dids.upload(ids, c->s); dcap.upload(route_cap, n, c->s); droff.upload(route_off, n, c->s);
+        dcost.alloc((size_t)N * 10); dce.alloc((size_t)std::max(E, 1) * 81); dbc.alloc((size_t)std::max(E, 1) * 81);
+        dbest.alloc((size_t)std::max(child_off[N], 1) * 10); dpk.alloc((size_t)std::max(child_off[N], 1) * 10);
+        dlout.alloc(N); dstage.alloc((size_t)N * 8); dscnt.alloc(N);
+        c->routes.upload(routes_out, (size_t)ext, c->s);
+        c->bar.alloc(2);
+        DagBatchDev db;
+        db.n_nodes = N; db.n_edges = E; db.n_slots = child_off[N]; db.depth = D; db.n_nets = n; db.max_level = ml;
+        db.nodes = dn.p; db.par_off = dpo.p; db.par = dp.p; db.child_slot = dcs.p; db.edge_child = dec.p;
+        db.child_off = dco.p; db.level_off = dlo.p; db.level_nodes = dln.p; db.h_level_off = level_off.data();
+        db.net_node_off = dno.p; db.net_ids = dids.p; db.costs = dcost.p; db.best_path = dbest.p; db.packed = dpk.p;
+        db.cost_edges = dce.p; db.best_change = dbc.p; db.layer_out = dlout.p; db.stage = dstage.p;
+        db.stage_cnt = dscnt.p; db.route_off = droff.p; db.route_cap = dcap.p; db.routes = c->routes.p;
+        int nl = launch_dag_route(g, db, stamp, c->bar.p, true, c->s);
+        if (nl < 0) {
+            cudaGetLastError();
+            launch_dag_route(g, db, stamp, c->bar.p, false, c->s);
+        }
+        cuda_check(cudaMemcpyAsync(routes_out, c->routes.p, ext * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
+        sync_check(c);
+    });
+}
+
+int igr_build_dag(int X, int Y, int mode, int ntree, const int32_t *pos, const int32_t *adj_off, const int32_t *adj,
+                  const float *xsum, const float *ysum, int32_t *out, int64_t cap, int64_t *len) {
+    if (!pos || !adj_off || !adj || !xsum || !ysum || !len || ntree < 2 || X < 2 || Y < 2)
+        return fail(nullptr, IGR_ERR_INVALID, "bad arguments");
+    return guard(nullptr, [&] {
+        NetSet ns;
+        ns.L = 9; ns.X = X; ns.Y = Y;
+        RNet r;
+        r.tnode.assign(pos, pos + ntree);
+        r.adj.assign(ntree, {});
+        for (int v = 0; v < ntree; v++) {
+            if (pos[v] < 0 || pos[v] >= 10 * X * Y) throw Error(ERR_INVALID, "node position out of range");
+            for (int q = adj_off[v]; q < adj_off[v + 1]; q++) {
+                if (adj[q] < 0 || adj[q] >= ntree) throw Error(ERR_INVALID, "adjacency out of range");
+                r.adj[v].push_back(adj[q]);
+            }
+        }
+        CongestionView cv;
+        cv.X = X; cv.Y = Y;
+        cv.xsum.assign(xsum, xsum + (size_t)X * Y);
+        cv.ysum.assign(ysum, ysum + (size_t)X * Y);
+        DagNet dn;
+        build_dag(ns, r, cv, mode, dn);
+        std::vector<int> v;
+        const int m = (int)dn.nodes.size(), E = (int)dn.par_nodes.size();
+        v.push_back(m);
+        v.insert(v.end(), dn.nodes.begin(), dn.nodes.end());
+        v.insert(v.end(), dn.par_num.begin(), dn.par_num.end());
+        v.insert(v.end(), dn.child_num.begin(), dn.child_num.end());
+        v.insert(v.end(), dn.depth.begin(), dn.depth.end());
+        v.push_back(E);
+        v.insert(v.end(), dn.par_nodes.begin(), dn.par_nodes.end());
+        v.insert(v.end(), dn.child_idx.begin(), dn.child_idx.end());
+        v.push_back((int)dn.points.size());
+        v.insert(v.end(), dn.points.begin(), dn.points.end());
+        *len = (int64_t)v.size();
+        if (out && cap >= *len) std::memcpy(out, v.data(), v.size() * 4);
+    });
+}
+
+int igr_steiner(int n, const int32_t *x, const int32_t *y, int32_t *nx, int32_t *ny, int cap_nodes, int *n_nodes,
+                int32_t *edges, int cap_edges, int *n_edges) {
+    if (n < 0 || (n && (!x || !y)) || !n_nodes || !n_edges) return fail(nullptr, IGR_ERR_INVALID, "bad arguments");
+    return guard(nullptr, [&] {
+        std::vector<int> xs(x, x + n), ys(y, y + n);
+        SteinerTree t;
+        steiner_tree(xs, ys, t);
+        *n_nodes = (int)t.x.size();
+        *n_edges = (int)t.edges.size();
+        if (*n_nodes > cap_nodes || *n_edges > cap_edges) throw Error(ERR_CAPACITY, "output buffers too small");
+        for (int i = 0; i < *n_nodes; i++) { nx[i] = t.x[i]; ny[i] = t.y[i]; }
+        for (int i = 0; i < *n_edges; i++) { edges[2 * i] = t.edges[i].first; edges[2 * i + 1] = t.edges[i].second; }
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,200 @@
+// Fused congestion-cost refresh: wire cost, via cost and the per-track prefix
+// sums of wire cost, in one pass over each track.
+//
+// Replaces three full-grid kernels of InstantGR (update_wcost_cuda_ispd24,
+// update_vcost_ispd24, compute_presum; src/graph.hpp:40-71, :101-104,
+// :405-430).  One CTA of 256 threads owns one track: it stages the track's
+// capacity and demand in shared memory with coalesced loads, evaluates the
+// cost model for every cell, writes vcost (f32), and scans the wire costs in
+// f64 into presum.  The wire cost array itself is never written: 20 bytes of
+// DRAM traffic per cell (4+4 read, 4+8 written) instead of the reference's
+// >= 44.
+//
+// The prefix sum keeps the exact association of the reference's in-place
+// Sklansky scan (at level d, element i with bit d set adds element
+// ((i >> d) << d) - 1), so presum is bit-identical to the reference's for the
+// same demand.  Element i sits at thread i % 256, row i / 256: levels 0-4 are
+// lane shuffles, levels 5-7 go through shared memory between warps, and levels
+// >= 8 combine whole rows, whose running totals every thread tracks itself.
+#include "kcommon.cuh"
+
+namespace igr {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+template <int MAXE>
+__global__ void __launch_bounds__(kThreads) cost_refresh_kernel(GridDev g, int only_dirty) {
+    const int tr = blockIdx.x;
+    if (only_dirty) {
+        if (!g.dirty_cost[tr]) return;
+    }
+    const TrackInfo ti = decode_track(g, tr);
+    const int n = ti.len;
+    const int E = (n + kThreads - 1) / kThreads;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const double sc = g.short_cost[ti.l];
+    const int *elen = ti.dir ? g.ylen : g.xlen;
+
+    __shared__ float s_cap[MAXE * kThreads], s_dem[MAXE * kThreads];
+    __shared__ double s_wt[kThreads / 32][MAXE];
+    __shared__ double s_rt[MAXE];
+
+    for (int i = tid; i < n; i += kThreads) {
+        s_cap[i] = g.cap[ti.base + i];
+        s_dem[i] = g.demand[ti.base + i];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        if (only_dirty) g.dirty_cost[tr] = 0;
+        atomicAdd(&g.stats[2], (unsigned long long)n);  // refreshed cells, for the roofline
+    }
+
+    double x[MAXE];
+#pragma unroll
+    for (int r = 0; r < MAXE; r++) {
+        x[r] = 0;
+        const int i = tid + r * kThreads;
+        if (r < E && i < n) {
+            const float c = s_cap[i], d = s_dem[i];
+            const double of0 = of_cost(c, d);
+            const double bh = fmin(1e12, (of_cost(c, (float)((double)d + 0.5)) - of0) * sc);
+            float v;
+            if (i == 0) {
+                v = (float)fmin(1e12, (of_cost(c, (float)((double)d + 1.0)) - of0) * sc);
+            } else {
+                const float cp = s_cap[i - 1], dp = s_dem[i - 1];
+                const double ofp = of_cost(cp, dp);
+                const double a1p = fmin(1e12, (of_cost(cp, (float)((double)dp + 1.0)) - ofp) * sc);
+                if (i == n - 1) {
+                    v = (float)a1p;
+                } else {
+                    const double bhp = fmin(1e12, (of_cost(cp, (float)((double)dp + 0.5)) - ofp) * sc);
+                    v = (float)(bh + bhp);
+                }
+                // scan input: wire cost of edge i-1 (graph.hpp:44-46)
+                float w = (float)a1p;
+                w = (float)fma(g.unit_wire, (double)elen[i - 1], (double)w);
+                x[r] = (double)w;
+            }
+            v = (float)((double)v + g.unit_via);
+            g.vcost[ti.base + i] = v;
+        }
+    }
+    // ---- Sklansky levels 0..4: lanes
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+        const int src = ((lane >> m) << m) - 1;
+        const bool take = (lane >> m) & 1;
+#pragma unroll
+        for (int r = 0; r < MAXE; r++) {
+            double o = __shfl_sync(0xffffffffu, x[r], src & 31);
+            if (take) x[r] += o;
+        }
+    }
+    // ---- levels 5..7: warps
+#pragma unroll
+    for (int m = 0; m < 3; m++) {
+        if (lane == 31) {
+#pragma unroll
+            for (int r = 0; r < MAXE; r++) s_wt[warp][r] = x[r];
+        }
+        __syncthreads();
+        if ((warp >> m) & 1) {
+            const int sw = ((warp >> m) << m) - 1;
+#pragma unroll
+            for (int r = 0; r < MAXE; r++) x[r] += s_wt[sw][r];
+        }
+        __syncthreads();
+    }
+    // ---- levels >= 8: rows
+    if (E > 1) {
+        if (tid == kThreads - 1) {
+#pragma unroll
+            for (int r = 0; r < MAXE; r++) s_rt[r] = x[r];
+        }
+        __syncthreads();
+        double rt[MAXE];
+#pragma unroll
+        for (int r = 0; r < MAXE; r++) rt[r] = s_rt[r];
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+            if ((1 << m) >= MAXE) break;
+#pragma unroll
+            for (int r = 0; r < MAXE; r++) {
+                if ((r >> m) & 1) {
+                    const int sr = ((r >> m) << m) - 1;
+                    x[r] += rt[sr];
+                    rt[r] += rt[sr];
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < MAXE; r++) {
+        const int i = tid + r * kThreads;
+        if (r < E && i < n) g.presum[ti.base + i] = x[r];
+    }
+}
+
+template <typename T>
+__global__ void ref_to_track_kernel(GridDev g, const T *ref, T *trk) {
+    const int64_t n = g.N;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        int l = (int)(k / ((int64_t)g.X * g.Y));
+        int rem = (int)(k - (int64_t)l * g.X * g.Y);
+        int x = rem / g.Y, y = rem % g.Y;
+        trk[cell_at(g, l, x, y)] = ref[k];
+    }
+}
+
+template <typename T>
+__global__ void track_to_ref_kernel(GridDev g, const T *trk, T *ref) {
+    const int64_t n = g.N;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        int l = (int)(k / ((int64_t)g.X * g.Y));
+        int rem = (int)(k - (int64_t)l * g.X * g.Y);
+        int x = rem / g.Y, y = rem % g.Y;
+        ref[k] = trk[cell_at(g, l, x, y)];
+    }
+}
+
+}  // namespace
+
+void launch_cost_refresh(const GridDev &g, bool only_dirty, cudaStream_t s) {
+    const int maxlen = g.X > g.Y ? g.X : g.Y;
+    const int e = (maxlen + kThreads - 1) / kThreads;
+    const int od = only_dirty ? 1 : 0;
+    if (e <= 1) cost_refresh_kernel<1><<<g.ntracks, kThreads, 0, s>>>(g, od);
+    else if (e <= 2) cost_refresh_kernel<2><<<g.ntracks, kThreads, 0, s>>>(g, od);
+    else if (e <= 4) cost_refresh_kernel<4><<<g.ntracks, kThreads, 0, s>>>(g, od);
+    else if (e <= 8) cost_refresh_kernel<8><<<g.ntracks, kThreads, 0, s>>>(g, od);
+    else cost_refresh_kernel<16><<<g.ntracks, kThreads, 0, s>>>(g, od);  // tracks of <= 4096 cells
+}
+
+static int grid_for(int64_t n) {
+    int64_t b = (n + 255) / 256;
+    if (b > 148 * 32) b = 148 * 32;
+    return (int)(b < 1 ? 1 : b);
+}
+
+void launch_to_track_layout(const GridDev &g, const float *ref, float *trk, cudaStream_t s) {
+    ref_to_track_kernel<float><<<grid_for(g.N), 256, 0, s>>>(g, ref, trk);
+}
+void launch_to_track_layout_d(const GridDev &g, const double *ref, double *trk, cudaStream_t s) {
+    ref_to_track_kernel<double><<<grid_for(g.N), 256, 0, s>>>(g, ref, trk);
+}
+void launch_from_track_layout_i(const GridDev &g, const int *trk, int *ref, cudaStream_t s) {
+    track_to_ref_kernel<int><<<grid_for(g.N), 256, 0, s>>>(g, trk, ref);
+}
+void launch_from_track_layout_f(const GridDev &g, const float *trk, float *ref, cudaStream_t s) {
+    track_to_ref_kernel<float><<<grid_for(g.N), 256, 0, s>>>(g, trk, ref);
+}
+void launch_from_track_layout_d(const GridDev &g, const double *trk, double *ref, cudaStream_t s) {
+    track_to_ref_kernel<double><<<grid_for(g.N), 256, 0, s>>>(g, trk, ref);
+}
+
+std::string cuda_error_string(cudaError_t e) { return cudaGetErrorString(e); }
+
+}  // namespace igr

@@ -1,0 +1,316 @@
+// ISPD2024 .cap/.net reader and route-guide writer.
+//
+// The reader follows the scanner of InstantGR (src/database.hpp:247-409) token
+// for token: integers are runs of digits (anything else is skipped, so signs
+// are ignored), reals are runs of digits and '.', names run up to the next
+// space or newline.  The .net file is cut at net boundaries ("\n)\n") and the
+// pieces are parsed on several threads, then concatenated in file order.
+//
+// The writer emits guides in the line format of src/graph.hpp:179-235
+// ("x0 y0 l0 x1 y1 l1", the lower 3-D position first); nets are written in
+// design order by a parallel formatter followed by one fwrite per chunk.
+#include "host.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <thread>
+
+namespace igr {
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+int hw_threads() {
+    unsigned n = std::thread::hardware_concurrency();
+    return n ? (int)n : 1;
+}
+
+void parallel_for(int n, int threads, const std::function<void(int, int)> &fn) {
+    if (n <= 0) return;
+    if (threads <= 0) threads = hw_threads();
+    threads = std::min(threads, n);
+    if (threads <= 1) { fn(0, n); return; }
+    std::vector<std::thread> ts;
+    std::vector<std::exception_ptr> errs(threads);
+    for (int t = 0; t < threads; t++) {
+        int b = (int)((int64_t)n * t / threads), e = (int)((int64_t)n * (t + 1) / threads);
+        ts.emplace_back([&, t, b, e] {
+            try { fn(b, e); } catch (...) { errs[t] = std::current_exception(); }
+        });
+    }
+    for (auto &t : ts) t.join();
+    for (auto &e : errs) if (e) std::rethrow_exception(e);
+}
+
+namespace {
+
+std::vector<char> slurp(const char *path) {
+    FILE *f = std::fopen(path, "rb");
+    if (!f) throw Error(ERR_IO, std::string("cannot open ") + path);
+    std::fseek(f, 0, SEEK_END);
+    long sz = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    std::vector<char> buf((size_t)sz + 1);
+    if (sz > 0 && std::fread(buf.data(), 1, (size_t)sz, f) != (size_t)sz) {
+        std::fclose(f);
+        throw Error(ERR_IO, std::string("short read on ") + path);
+    }
+    std::fclose(f);
+    buf[(size_t)sz] = 0;
+    buf.resize((size_t)sz + 1);
+    return buf;
+}
+
+inline bool is_dig(char c) { return c >= '0' && c <= '9'; }
+
+struct Scanner {
+    const char *b;
+    size_t n, p = 0;
+    Scanner(const char *buf, size_t len) : b(buf), n(len) {}
+    void need() {
+        if (p >= n) throw Error(ERR_FORMAT, "unexpected end of input");
+    }
+    int read_int() {
+        while (p < n && !is_dig(b[p])) p++;
+        need();
+        long long v = 0;
+        for (; p < n && is_dig(b[p]); p++) v = v * 10 + (b[p] - '0');
+        return (int)v;
+    }
+    double read_double() {
+        while (p < n && !is_dig(b[p])) p++;
+        need();
+        double ans = 0, scale = 0;
+        for (; p < n && (is_dig(b[p]) || b[p] == '.'); p++) {
+            if (b[p] == '.') scale = 1;
+            else scale *= 10, ans = ans * 10 + (b[p] - '0');
+        }
+        return scale == 0 ? ans : ans / scale;
+    }
+    void read_token(size_t &beg, size_t &end) {
+        while (p < n && (b[p] == ' ' || b[p] == '\n')) p++;
+        need();
+        beg = p;
+        while (p < n && b[p] != ' ' && b[p] != '\n') p++;
+        end = p;
+    }
+};
+
+}  // namespace
+
+void read_cap_buffer(Design &d, const char *buf, size_t n) {
+    Scanner s(buf, n);
+    d.L = s.read_int();
+    d.X = s.read_int();
+    d.Y = s.read_int();
+    if (d.L != 10) throw Error(ERR_FORMAT, "the .cap file must have 10 layers");
+    if (d.X < 2 || d.Y < 2) throw Error(ERR_FORMAT, "grid must be at least 2x2");
+    if ((int64_t)d.L * d.X * d.Y > (int64_t)2000000000) throw Error(ERR_CAPACITY, "grid too large for 32-bit positions");
+    d.unit_wire = s.read_double();
+    d.unit_via = s.read_double();
+    d.short_cost.resize(d.L);
+    for (int i = 0; i < d.L; i++) d.short_cost[i] = s.read_double();
+    d.x_edge_len.resize(d.X - 1);
+    d.y_edge_len.resize(d.Y - 1);
+    for (int i = 0; i < d.X - 1; i++) d.x_edge_len[i] = s.read_int();
+    for (int i = 0; i < d.Y - 1; i++) d.y_edge_len[i] = s.read_int();
+    d.dr_x.assign(d.X, 0);
+    d.dr_y.assign(d.Y, 0);
+    for (int i = 0; i < d.X - 1; i++) d.dr_x[i + 1] = d.dr_x[i] + d.x_edge_len[i];
+    for (int i = 0; i < d.Y - 1; i++) d.dr_y[i + 1] = d.dr_y[i] + d.y_edge_len[i];
+    d.dr2gr_x.assign(d.dr_x.back() + 1, -1);
+    d.dr2gr_y.assign(d.dr_y.back() + 1, -1);
+    for (int i = 0; i < d.X; i++) d.dr2gr_x[d.dr_x[i]] = i;
+    for (int i = 0; i < d.Y; i++) d.dr2gr_y[d.dr_y[i]] = i;
+    d.layer_dir.resize(d.L);
+    d.layer_min_len.resize(d.L);
+    d.cap.assign((size_t)d.L * d.X * d.Y, 0.f);
+    for (int l = 0; l < d.L; l++) {
+        size_t b, e;
+        s.read_token(b, e);
+        std::string name(buf + b, buf + e), want = "metal" + std::to_string(l + 1);
+        if (name != want) throw Error(ERR_FORMAT, "expected layer " + want + ", got " + name);
+        d.layer_dir[l] = s.read_int();
+        d.layer_min_len[l] = s.read_double();
+        float *c = d.cap.data() + (size_t)l * d.X * d.Y;
+        for (int y = 0; y < d.Y; y++)
+            for (int x = 0; x < d.X; x++) c[(size_t)x * d.Y + y] = (float)s.read_double();
+        if (l && d.layer_dir[l] == d.layer_dir[l - 1])
+            throw Error(ERR_FORMAT, "layer directions must alternate");
+    }
+}
+
+namespace {
+
+struct NetChunk {
+    std::vector<char> names;
+    std::vector<int64_t> name_len;
+    std::vector<int> pins_per_net;
+    std::vector<int> aps_per_pin;
+    std::vector<int> ap;
+    std::vector<int> bb;  // minx maxx miny maxy per net
+};
+
+void parse_net_chunk(const Design &d, const char *buf, size_t n, NetChunk &c) {
+    Scanner s(buf, n);
+    const int X = d.X, Y = d.Y, L = d.L;
+    while (s.p < n && (buf[s.p] == ' ' || buf[s.p] == '\n')) s.p++;
+    while (s.p < n) {
+        size_t b, e;
+        s.read_token(b, e);
+        c.names.insert(c.names.end(), buf + b, buf + e);
+        c.name_len.push_back((int64_t)(e - b));
+        int minx = X, maxx = 0, miny = Y, maxy = 0, npin = 0;
+        while (true) {  // pins
+            int nap = 0;
+            while (true) {  // access points
+                int l = s.read_int(), x = s.read_int(), y = s.read_int();
+                if (l >= L || x >= X || y >= Y) throw Error(ERR_FORMAT, "access point outside the grid");
+                minx = std::min(minx, x); maxx = std::max(maxx, x);
+                miny = std::min(miny, y); maxy = std::max(maxy, y);
+                c.ap.push_back(l * X * Y + x * Y + y);
+                if (++nap >= 20) throw Error(ERR_FORMAT, "more than 19 access points in a pin");
+                bool pin_end = false;
+                while (s.p < n && !is_dig(buf[s.p]))
+                    if (buf[s.p++] == ']') { pin_end = true; break; }
+                if (pin_end) break;
+                s.need();
+            }
+            c.aps_per_pin.push_back(nap);
+            npin++;
+            bool net_end = false;
+            while (s.p < n && !is_dig(buf[s.p]))
+                if (buf[s.p++] == ')') { net_end = true; break; }
+            if (net_end) break;
+            s.need();
+        }
+        c.pins_per_net.push_back(npin);
+        c.bb.insert(c.bb.end(), {minx, maxx, miny, maxy});
+        while (s.p < n && (buf[s.p] == ' ' || buf[s.p] == '\n')) s.p++;
+    }
+}
+
+}  // namespace
+
+void read_net_buffer(Design &d, const char *buf, size_t n) {
+    // Cut at "\n)\n" boundaries so that every piece holds whole nets.
+    int T = std::max(1, std::min(hw_threads(), (int)(n / (1 << 20)) + 1));
+    std::vector<size_t> cut{0};
+    for (int t = 1; t < T; t++) {
+        size_t g = std::max(cut.back(), n * t / T);
+        const char *hit = nullptr;
+        for (size_t p = g; p + 2 < n; p++)
+            if (buf[p] == '\n' && buf[p + 1] == ')' && buf[p + 2] == '\n') { hit = buf + p + 3; break; }
+        if (!hit) break;
+        cut.push_back((size_t)(hit - buf));
+    }
+    cut.push_back(n);
+    int parts = (int)cut.size() - 1;
+    std::vector<NetChunk> ch(parts);
+    parallel_for(parts, parts, [&](int b, int e) {
+        for (int i = b; i < e; i++) parse_net_chunk(d, buf + cut[i], cut[i + 1] - cut[i], ch[i]);
+    });
+    d.name_pool.clear(); d.name_off.assign(1, 0);
+    d.pin_off.assign(1, 0); d.ap_off.assign(1, 0); d.ap.clear();
+    d.bminx.clear(); d.bmaxx.clear(); d.bminy.clear(); d.bmaxy.clear();
+    size_t nn = 0;
+    for (auto &c : ch) nn += c.pins_per_net.size();
+    d.name_off.reserve(nn + 1); d.pin_off.reserve(nn + 1);
+    for (auto &c : ch) {
+        d.name_pool.insert(d.name_pool.end(), c.names.begin(), c.names.end());
+        for (auto len : c.name_len) d.name_off.push_back(d.name_off.back() + len);
+        for (auto np : c.pins_per_net) d.pin_off.push_back(d.pin_off.back() + np);
+        for (auto na : c.aps_per_pin) d.ap_off.push_back(d.ap_off.back() + na);
+        d.ap.insert(d.ap.end(), c.ap.begin(), c.ap.end());
+        for (size_t i = 0; i < c.pins_per_net.size(); i++) {
+            d.bminx.push_back(c.bb[4 * i]); d.bmaxx.push_back(c.bb[4 * i + 1]);
+            d.bminy.push_back(c.bb[4 * i + 2]); d.bmaxy.push_back(c.bb[4 * i + 3]);
+        }
+        c = NetChunk();
+    }
+}
+
+void read_design(Design &d, const char *cap_path, const char *net_path, int threads) {
+    {
+        auto b = slurp(cap_path);
+        read_cap_buffer(d, b.data(), b.size() - 1);
+    }
+    {
+        auto b = slurp(net_path);
+        read_net_buffer(d, b.data(), b.size() - 1);
+    }
+    select_pins(d, threads);
+}
+
+// ------------------------------------------------------------------ writer
+namespace {
+
+inline char *put_int(char *o, int v) {
+    char t[12];
+    int k = 0;
+    if (v == 0) { *o++ = '0'; return o; }
+    while (v) t[k++] = (char)('0' + v % 10), v /= 10;
+    while (k) *o++ = t[--k];
+    return o;
+}
+
+}  // namespace
+
+void write_guides(const Design &d, const NetSet &ns, const RouteSource &rs, const char *path, int threads) {
+    FILE *f = std::fopen(path, "wb");
+    if (!f) throw Error(ERR_IO, std::string("cannot open ") + path + " for writing");
+    const int X = d.X, Y = d.Y, XY = X * Y;
+    const int N = d.num_nets();
+    if (threads <= 0) threads = hw_threads();
+    // Chunks of nets are formatted in parallel into private buffers, then written in order.
+    const int CH = 4096;
+    int nch = (N + CH - 1) / CH;
+    auto fmt = [&](int c, std::vector<char> &out) {
+        out.clear();
+        auto seg = [&](int p0, int p1, std::vector<char> &o) {
+            if (p0 > p1) std::swap(p0, p1);
+            char tmp[96];
+            char *q = tmp;
+            q = put_int(q, p0 / Y % X); *q++ = ' ';
+            q = put_int(q, p0 % Y); *q++ = ' ';
+            q = put_int(q, p0 / XY); *q++ = ' ';
+            q = put_int(q, p1 / Y % X); *q++ = ' ';
+            q = put_int(q, p1 % Y); *q++ = ' ';
+            q = put_int(q, p1 / XY); *q++ = '\n';
+            o.insert(o.end(), tmp, q);
+        };
+        for (int n = c * CH; n < std::min(N, (c + 1) * CH); n++) {
+            out.insert(out.end(), d.name_pool.data() + d.name_off[n], d.name_pool.data() + d.name_off[n + 1]);
+            out.push_back('\n'); out.push_back('('); out.push_back('\n');
+            for (int64_t i = d.sel_off[n]; i < d.sel_off[n + 1]; i++)
+                if (d.sel[i] < XY) seg(d.sel[i], d.sel[i] + XY, out);
+            for (int64_t i = d.extra_off[n]; i < d.extra_off[n + 1]; i += 2) seg(d.extra[i], d.extra[i + 1], out);
+            if (n < (int)ns.subnets.size())
+                for (int s : ns.subnets[n]) {
+                    const int *r = rs.routes_of(s);
+                    if (!r) continue;
+                    for (int j = 1; j < r[0]; j += 2) seg(r[j] + XY, r[j + 1] + XY, out);
+                }
+            out.push_back(')'); out.push_back('\n');
+        }
+    };
+    std::vector<std::vector<char>> bufs(std::max(1, threads));
+    for (int c0 = 0; c0 < nch; c0 += threads) {
+        int k = std::min(threads, nch - c0);
+        parallel_for(k, k, [&](int b, int e) {
+            for (int i = b; i < e; i++) fmt(c0 + i, bufs[i]);
+        });
+        for (int i = 0; i < k; i++)
+            if (!bufs[i].empty() && std::fwrite(bufs[i].data(), 1, bufs[i].size(), f) != bufs[i].size()) {
+                std::fclose(f);
+                throw Error(ERR_IO, "write failed");
+            }
+    }
+    std::fclose(f);
+}
+
+}  // namespace igr

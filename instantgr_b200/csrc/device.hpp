@@ -1,0 +1,133 @@
+// Device state of the router and the launchers of its sm_100a kernels.
+//
+// Grid arrays are per routing layer and track-contiguous: on a vertical layer
+// (tracks run along y) cell (l, x, y) lives at l*X*Y + x*Y + y, on a
+// horizontal layer (tracks run along x) at l*X*Y + y*X + x.  Every track is
+// therefore one contiguous run, so the per-track passes (cost refresh with its
+// prefix sums, difference-array commit, overflow scans) stream it with
+// coalesced loads.  Route records keep InstantGR's position encoding
+// l*X*Y + x*Y + y so that they can be exchanged with it unchanged.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "status.hpp"
+
+namespace igr {
+
+struct GridDev {
+    int L = 0, X = 0, Y = 0, DIR = 0;  // routing layers, grid, direction of routing layer 0
+    int64_t N = 0;                      // L*X*Y cells
+    int ntracks = 0;                    // sum over layers of (X or Y)
+    double unit_wire = 0, unit_via = 0;
+    // device arrays
+    float *cap = nullptr, *demand = nullptr, *vcost = nullptr;
+    double *presum = nullptr;
+    int *pre = nullptr;        // wire difference array (zero between batches)
+    int *stamp = nullptr;      // timestamp per cell
+    int *xlen = nullptr, *ylen = nullptr;
+    double *short_cost = nullptr;  // [L]
+    uint8_t *dirty_cost = nullptr;    // [ntracks] demand changed since the last cost refresh
+    uint8_t *dirty_commit = nullptr;  // [ntracks] difference array holds entries
+    unsigned long long *stats = nullptr;  // [0] wirelength, [1] via count (signed, two's complement)
+    int *err = nullptr;                   // device error word
+};
+
+// track id of layer l, track index t (y for horizontal layers, x for vertical)
+struct TrackMap {
+    std::vector<int> first;  // [L+1] first track id of each layer
+};
+
+// ---- launchers (stream-ordered; errors are reported through cudaGetLastError)
+void launch_cost_refresh(const GridDev &g, bool only_dirty, cudaStream_t s);
+void launch_wire_commit(const GridDev &g, int stamp, bool only_dirty, cudaStream_t s);
+
+struct TreeBatchDev {
+    const int *net_ids;      // [n] routing-net id of each net of the batch
+    const int *node_off;     // [n+1] node offset of each net (into nodes/par)
+    const int *nodes;        // tree nodes, preorder, reference encoding (Steiner layer = L)
+    const int *par;          // parent (local index) per node, -1 at the root
+    const int64_t *route_off;  // [routing nets] route record offset (ints)
+    const int *route_cap;    // [routing nets] route record capacity (ints)
+    int *routes;             // route records
+    double *scratch;         // per-node DP tables of nets larger than the shared-memory tile
+    const int64_t *scratch_off;  // [n] offset (in nodes) into scratch, -1 for nets that fit on chip
+    int64_t scratch_nodes;   // nodes covered by scratch: 45 doubles each, then 46 ints each
+    int n;
+};
+// doubles of scratch needed for `nodes` oversize-net nodes
+inline int64_t pattern_scratch_doubles(int64_t nodes) { return nodes * 45 + (nodes * 46 + 1) / 2; }
+constexpr int kPatternNodeTile = 20;  // nets with more nodes use global scratch
+void launch_pattern_route(const GridDev &g, const TreeBatchDev &b, int stamp, cudaStream_t s);
+
+struct ViaBatchDev {
+    const int *net_ids;  // [n]
+    const int64_t *route_off;
+    const int *routes;
+    int n;
+};
+void launch_via_commit(const GridDev &g, const ViaBatchDev &b, int stamp, int K, cudaStream_t s);
+void launch_wire_ripup(const GridDev &g, const ViaBatchDev &b, int stamp, int K, cudaStream_t s);
+
+// Batch of detour DAGs (phase 2).  Node indices are batch-global; the parent
+// slots of node v are par_off[v]..par_off[v+1] (edge e: parent par[e], child
+// slot child_slot[e] of the parent, child node edge_child[e]); the child slots
+// of v are child_off[v]..child_off[v+1].
+struct DagBatchDev {
+    int n_nodes = 0, n_edges = 0, n_slots = 0, depth = 0, n_nets = 0, max_level = 0;
+    const int *nodes = nullptr, *par_off = nullptr, *par = nullptr, *child_slot = nullptr, *edge_child = nullptr;
+    const int *child_off = nullptr, *level_off = nullptr, *level_nodes = nullptr;
+    const int *h_level_off = nullptr;  // host copy of level_off (per-level launches)
+    const int *net_node_off = nullptr, *net_ids = nullptr;
+    double *costs = nullptr;
+    unsigned long long *best_path = nullptr, *packed = nullptr;
+    double *cost_edges = nullptr;
+    int *best_change = nullptr, *layer_out = nullptr, *stage = nullptr, *stage_cnt = nullptr;
+    const int64_t *route_off = nullptr;
+    const int *route_cap = nullptr;
+    int *routes = nullptr;
+};
+// returns the number of kernel launches, or -1 when the cooperative launch failed
+int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, unsigned *bar_words, bool cooperative,
+                     cudaStream_t s);
+
+constexpr int kRouteLayers = 9;
+
+// rip-up marking (graph.hpp:432-466): flags nets whose routes cross more than
+// `min_edges` edges with cap + threshold <= demand
+void launch_mark_overflow(const GridDev &g, int threshold, int *of_sum, const ViaBatchDev &nets,
+                          int min_edges, uint8_t *is_of, cudaStream_t s);
+// 2-D congestion view (graph.hpp:545-584): max over layers of (demand - cap)^+, then
+// exclusive prefix sums along x (xsum) and along y (ysum); layout [x][y]
+void launch_congestion_view(const GridDev &g, float *xsum, float *ysum, cudaStream_t s);
+// overflow cost of the current demand (graph.hpp:148-157), summed in fixed order
+void launch_overflow_cost(const GridDev &g, double *out, cudaStream_t s);
+
+// layout conversions between the reference layout [l][x][y] and the track layout
+void launch_to_track_layout(const GridDev &g, const float *ref, float *trk, cudaStream_t s);
+void launch_from_track_layout_f(const GridDev &g, const float *trk, float *ref, cudaStream_t s);
+void launch_from_track_layout_d(const GridDev &g, const double *trk, double *ref, cudaStream_t s);
+void launch_to_track_layout_d(const GridDev &g, const double *ref, double *trk, cudaStream_t s);
+void launch_from_track_layout_i(const GridDev &g, const int *trk, int *ref, cudaStream_t s);
+
+// ---- batch colouring (database_cuda.hpp:288-434, made deterministic)
+struct ColorDev {
+    int n = 0, X = 0, Y = 0, sparsity = 15;
+    const int *pt_off = nullptr, *pts = nullptr;   // [n+1], 2-D cells
+    const int *pt_net = nullptr;                   // [points] owner
+    const int *h_off = nullptr, *hseg = nullptr;   // [n+1], pairs
+    const int *v_off = nullptr, *vseg = nullptr;
+    int npts = 0;
+    int *map = nullptr;       // [X*Y]
+    int *batch = nullptr;     // [n]
+    int *status = nullptr;    // [n]
+    int *flags = nullptr;     // [4] device flags
+};
+int run_coloring(ColorDev &c, int max_batch, cudaStream_t s);  // returns #batches (host loop)
+
+std::string cuda_error_string(cudaError_t e);
+
+}  // namespace igr

@@ -1,0 +1,161 @@
+// Host-side data model of the global router: the parsed ISPD2024 design,
+// the routing nets derived from it, and the helpers shared by the host
+// passes (parser, pin selection, Steiner provider, net splitting, detour DAG
+// construction, route-guide writer).
+//
+// Encodings kept identical to InstantGR so that routes, pins and trees can be
+// exchanged with it verbatim:
+//   * a 3-D position is  l*X*Y + x*Y + y   (src/database.hpp:36)
+//   * a 2-D position is  x*Y + y
+//   * "file" layers are 0..L-1 (L=10, layer 0 pin-only); "routing" layers are
+//     file layer - 1 (src/database_cuda.hpp:2106, 2267), so routing layer r has
+//     direction (r & 1) ^ DIR with DIR = direction of file layer 1.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <stdexcept>
+#include <functional>
+
+#include "status.hpp"
+
+namespace igr {
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+// ---------------------------------------------------------------- design
+struct Design {
+    int L = 0, X = 0, Y = 0;               // file layers, grid size
+    double unit_wire = 0, unit_via = 0;
+    std::vector<double> short_cost;         // [L] overflow weight per layer
+    std::vector<int> x_edge_len, y_edge_len; // [X-1], [Y-1]
+    std::vector<int> dr_x, dr_y;            // cumulative coordinates [X], [Y]
+    std::vector<int> dr2gr_x, dr2gr_y;      // inverse of dr_x / dr_y (-1 = no grid line)
+    std::vector<int> layer_dir;             // [L] 0 = horizontal, 1 = vertical
+    std::vector<double> layer_min_len;      // [L]
+    std::vector<float> cap;                 // [L][X][Y] capacity (file layers)
+
+    // nets as read: CSR net -> pins -> access points
+    std::vector<char> name_pool;
+    std::vector<int64_t> name_off;          // [N+1]
+    std::vector<int64_t> pin_off;           // [N+1] into ap_off
+    std::vector<int64_t> ap_off;            // [P+1] into ap
+    std::vector<int> ap;                    // 3-D positions
+    std::vector<int> bminx, bmaxx, bminy, bmaxy; // bbox of all access points
+
+    // after pin selection (src/database.hpp:38-243)
+    std::vector<int64_t> sel_off;           // [N+1]
+    std::vector<int> sel;                   // chosen 3-D pin positions
+    std::vector<int64_t> extra_off;         // [N+1]
+    std::vector<int> extra;                 // pairs of 3-D positions (stacked pins)
+
+    int num_nets() const { return (int)name_off.size() - 1; }
+    std::string name(int n) const {
+        return std::string(name_pool.data() + name_off[n], name_pool.data() + name_off[n + 1]);
+    }
+    int dir_routing(int r) const { return layer_dir[r + 1]; }
+};
+
+// Reads the .cap and .net files with the semantics of InstantGR's scanner
+// (src/database.hpp:247-409): digits only (no signs, no exponents), '.' as the
+// only fraction mark, access points "(l, x, y)" grouped in "[...]" pins.
+void read_design(Design &d, const char *cap_path, const char *net_path, int threads);
+void read_cap_buffer(Design &d, const char *buf, size_t n);
+void read_net_buffer(Design &d, const char *buf, size_t n);
+
+// Chooses one access point per pin (src/database.hpp:38-243), fills sel/extra.
+void select_pins(Design &d, int threads);
+
+// ---------------------------------------------------------------- routing nets
+// A routing net ("subnet") is a net of >= 2 selected pins, split at
+// MAX_PIN_SIZE = 12 pins along its Steiner tree (src/database_cuda.hpp:2111-2237).
+struct RNet {
+    int orig = -1;                 // design net id
+    int hpwl = 0, minx = 0, maxx = 0, miny = 0, maxy = 0;
+    std::vector<int> pins;         // routing-layer 3-D positions
+    // Steiner tree: adjacency over nodes, node positions (3-D, Steiner -> layer L)
+    std::vector<std::vector<int>> adj;
+    std::vector<int> tnode;
+    // 2-D conflict shapes used by batch colouring (src/database_cuda.hpp:746-820)
+    std::vector<std::pair<int, int>> hseg, vseg;
+    std::vector<int> points;
+};
+
+struct NetSet {
+    int L = 0, X = 0, Y = 0, DIR = 0;   // routing layers (L = 9)
+    std::vector<RNet> nets;
+    std::vector<std::vector<int>> subnets;   // design net -> routing net ids
+    std::vector<int> unfinished;             // design net -> subnets still routing
+    std::vector<int64_t> pin_sum;            // [n+1] pin prefix sum (route slots)
+};
+
+// Builds routing nets: Steiner trees for every multi-pin net, split >12-pin nets.
+void build_netset(const Design &d, NetSet &ns, int threads);
+// Fills hseg/vseg/points/adj/tnode for one net from its tree (construct_rsmt).
+void construct_rsmt(const Design &d, const NetSet &ns, RNet &n, bool rsmt_only);
+void calc_hpwl(const NetSet &ns, RNet &n);
+
+// DFS preorder flattening of a tree (src/Lshape_route.hpp:191-208).
+void flatten_tree(const RNet &n, int *nodes, int *par);
+
+// ---------------------------------------------------------------- detour DAG
+// Per-net detour DAG (src/database_cuda.hpp:1429-2086), in topological order.
+struct DagNet {
+    std::vector<int> nodes;        // 3-D positions (routing layer; virtual = 9)
+    std::vector<int> par_num;      // parents per node
+    std::vector<int> par_sum;      // [n+1]
+    std::vector<int> par_nodes;    // parent node (local index) per parent slot
+    std::vector<int> child_idx;    // child slot of this node in the parent
+    std::vector<int> child_num;    // children per node
+    std::vector<int> depth;        // depth per node
+    std::vector<int> points;       // 2-D conflict points
+    std::vector<std::pair<int, int>> hseg, vseg;
+};
+struct CongestionView {            // host copy of the 2-D congestion prefix sums
+    int X = 0, Y = 0;
+    std::vector<float> xsum, ysum;
+};
+void build_dag(const NetSet &ns, const RNet &n, const CongestionView &cv, int mode, DagNet &out);
+
+// ---------------------------------------------------------------- Steiner provider
+// Rectilinear Steiner tree of a point set; deterministic and independent of the
+// input order.  Returns node positions (first the distinct input points in
+// ascending (x, y) order, then Steiner points) and tree edges.
+struct SteinerTree {
+    std::vector<int> x, y;
+    std::vector<std::pair<int, int>> edges;
+};
+void steiner_tree(const std::vector<int> &x, const std::vector<int> &y, SteinerTree &t);
+
+// ---------------------------------------------------------------- output
+// Writes route guides in InstantGR's order and format (src/graph.hpp:179-235).
+struct RouteSource {
+    // For routing net i: pointer to its route record (count at [0], then pairs).
+    std::function<const int *(int)> routes_of;
+};
+void write_guides(const Design &d, const NetSet &ns, const RouteSource &rs, const char *path, int threads);
+
+// ---------------------------------------------------------------- generator
+struct GenParams {
+    int X = 256, Y = 256, nets = 20000;
+    uint64_t seed = 1;
+    int cap_mode = 0;          // 0: U{4..12}; 1: mean falls 10 -> 4 over layers, +-2
+    double block_frac = 0.05;  // fraction of routing edges zeroed in blockages
+    int pin_mode = 0;          // 0: geometric(p=.5, min 2, cap 64); 1: mixture 70/20/9.5/0.5
+    double hifanout_frac = 0;  // fraction of nets with 65..500 pins (pin_mode 0)
+    int hifanout_bbox = 200;
+    double bbox_median = 8, bbox_sigma = 1.0;
+    int hotspots = 0;          // Gaussian hotspots
+    double hotspot_frac = 0;   // fraction of nets centred on a hotspot
+    double hotspot_sigma = 0;  // GCells
+};
+void generate_design(const GenParams &p, const char *cap_path, const char *net_path);
+
+int hw_threads();
+void parallel_for(int n, int threads, const std::function<void(int, int)> &fn);  // fn(begin, end)
+double now_s();
+
+}  // namespace igr

@@ -1,0 +1,133 @@
+// Host driver of the router and ownership of device memory.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "device.hpp"
+#include "host.hpp"
+
+namespace igr {
+
+void cuda_check(cudaError_t e, const char *what);
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        if (count <= n && p) return;
+        release();
+        if (count == 0) count = 1;
+        cuda_check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+        n = count;
+    }
+    void upload(const T *h, size_t count, cudaStream_t s) {
+        alloc(count);
+        if (count) cuda_check(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s), "H2D");
+    }
+    void upload(const std::vector<T> &v, cudaStream_t s) { upload(v.data(), v.size(), s); }
+};
+
+// Device arrays of one routing grid (build_cuda_database, database_cuda.hpp:2096-2362).
+struct GridOwner {
+    GridDev g;
+    DevBuf<float> cap, demand, vcost;
+    DevBuf<double> presum;
+    DevBuf<int> pre, stamp, xlen, ylen, err, of_sum;
+    DevBuf<double> short_cost, score;
+    DevBuf<uint8_t> dirty_cost, dirty_commit;
+    DevBuf<unsigned long long> stats;
+    DevBuf<float> scratch_f;
+    std::vector<int> layer_first;
+    // L, X, Y, DIR, edge lengths, unit costs, short costs [L], capacity [l][x][y] in reference layout
+    void create(int L, int X, int Y, int DIR, const int *xlen, const int *ylen, double unit_wire, double unit_via,
+                const double *short_cost, const float *cap_ref, cudaStream_t s);
+    void reset_demand(cudaStream_t s);  // zero demand/pre/stamp/stats, mark all tracks dirty
+    void mark_all_dirty(cudaStream_t s);
+    int check_error(cudaStream_t s);    // device error word -> status (and clears it)
+};
+
+struct RouterStats {
+    double wall = 0, p1_ms = 0, rrr_ms = 0, dag_host_ms = 0;
+    int batches1 = 0, rerouted = 0;
+    long long launches = 0;
+    long long h2d_bytes = 0, d2h_bytes = 0;
+};
+
+// Per-kernel-class device time, measured with CUDA events around each launch
+// when profiling is on.
+enum KernelClass { KC_COST = 0, KC_PATTERN, KC_WIRE_COMMIT, KC_VIA_COMMIT, KC_DAG, KC_COLOR, KC_RIPUP, KC_N };
+struct KernelTimer {
+    bool on = false;
+    cudaStream_t s = nullptr;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[KC_N];
+    double ms[KC_N] = {0};
+    long long launches[KC_N] = {0};
+    void begin(int k);
+    void end(int k);
+    void collect();  // after a stream synchronisation
+    void reset();
+};
+
+struct Router {
+    int rrr_iters = 1, threads = 0, mode = -1, verbose = 0, batched = 0;
+    Design d;
+    NetSet ns;
+    GridOwner go;
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // routes: one device buffer, per-net record offset/capacity (phase 1 records
+    // first, reroutes appended)
+    std::vector<int64_t> route_off;
+    std::vector<int> route_cap;
+    int64_t route_end = 0;
+    DevBuf<int> routes;
+    DevBuf<int64_t> d_route_off;
+    DevBuf<int> d_route_cap;
+    std::vector<int> h_routes;  // host copy after a run
+    RouterStats st;
+    int global_stamp = 0;
+    int mode_eff = 0;
+    std::vector<DagNet> dag;          // detour DAG of every routing net (phase 2)
+    DevBuf<int> d_all_ids, of_sum;
+    DevBuf<uint8_t> d_is_of;
+    DevBuf<float> d_xsum, d_ysum;
+    DevBuf<unsigned> d_bar;
+    bool cooperative = true;
+    KernelTimer kt;
+    // phase-1 plan of the last run (routing order, batches, trees, route capacity in order)
+    std::vector<int> plan_ids, plan_batch_off, plan_node_off, plan_nodes, plan_par, plan_cap;
+    unsigned long long cost_cells = 0;  // cells processed by cost refreshes of the last run
+    // score of the last run: wirelength, vias, overflow (GPU estimate)
+    double score_wl = 0, score_via = 0, score_of = 0;
+
+    void ensure_device();
+    void color_nets(const std::vector<int> &order, bool dag_points, int sparsity,
+                    std::vector<std::vector<int>> &batches);
+    void compute_score();
+
+    ~Router();
+    void open(const char *cap, const char *net);
+    void run();
+    void write(const char *out);
+    const int *route_of(int net) const { return h_routes.data() + route_off[net]; }
+
+   private:
+    void phase1();
+    bool rrr_pass(int iter);
+    void grow_routes(int64_t need);
+};
+
+}  // namespace igr

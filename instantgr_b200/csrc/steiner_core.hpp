@@ -1,0 +1,233 @@
+// Deterministic rectilinear Steiner tree provider.
+//
+// InstantGR builds its trees with FLUTE (src/flute.hpp), whose topology table
+// POST9.dat is not shipped with it (it is listed in .MISSING_LARGE_BLOBS), so
+// upstream FLUTE cannot run for degree >= 4.  This provider takes its place on
+// both sides of every comparison: the router of this project links it, and the
+// reference build used for baselines links it through a flute.hpp stand-in.
+//
+// Method (all in the caller's coordinate space, i.e. DR units):
+//   1. distinct points, sorted by (x, y);
+//   2. rectilinear minimum spanning tree by Kruskal over candidate edges: all
+//      pairs up to 64 points, otherwise the four-octant sweep of Zhou, Shenoy
+//      and Nicholls ("Efficient minimum spanning tree construction without
+//      Delaunay triangulation", 2002), edges ordered by (length, lo, hi);
+//   3. Steinerisation: for every node and every pair of its tree neighbours the
+//      median point of the three is tried; the best strictly positive saving
+//      is applied (edges v-a, v-b replaced by s-v, s-a, s-b), repeated for up
+//      to four passes; Steiner points of degree <= 2 are then spliced out.
+//      Degree three is FLUTE's closed form: the median point of the three.
+// The result does not depend on the order of the input points.
+#pragma once
+#include <algorithm>
+#include <cstdint>
+#include <cstdlib>
+#include <map>
+#include <numeric>
+#include <unordered_map>
+#include <utility>
+#include <vector>
+
+namespace igr_steiner {
+
+struct Tree {
+    std::vector<int> x, y;                   // node coordinates: pins first, then Steiner points
+    std::vector<std::pair<int, int>> edges;  // undirected tree edges
+    int npins = 0;
+};
+
+inline int med3(int a, int b, int c) { return std::max(std::min(a, b), std::min(std::max(a, b), c)); }
+
+inline void build(const std::vector<int> &xin, const std::vector<int> &yin, Tree &t) {
+    t = Tree();
+    const int n0 = (int)xin.size();
+    std::vector<std::pair<int, int>> pts(n0);
+    for (int i = 0; i < n0; i++) pts[i] = {xin[i], yin[i]};
+    std::sort(pts.begin(), pts.end());
+    pts.erase(std::unique(pts.begin(), pts.end()), pts.end());
+    const int P = (int)pts.size();
+    for (auto &p : pts) { t.x.push_back(p.first); t.y.push_back(p.second); }
+    t.npins = P;
+    if (P <= 1) return;
+    if (P == 2) { t.edges.push_back({0, 1}); return; }
+    auto dist = [&](int a, int b) { return std::abs(t.x[a] - t.x[b]) + std::abs(t.y[a] - t.y[b]); };
+    if (P == 3) {
+        int sx = med3(t.x[0], t.x[1], t.x[2]), sy = med3(t.y[0], t.y[1], t.y[2]);
+        int c = -1;
+        for (int i = 0; i < 3; i++) if (t.x[i] == sx && t.y[i] == sy) c = i;
+        if (c < 0) { t.x.push_back(sx); t.y.push_back(sy); c = 3; }
+        for (int i = 0; i < 3; i++) if (i != c) t.edges.push_back({std::min(i, c), std::max(i, c)});
+        return;
+    }
+    // ---- candidate edges
+    struct E { int w, a, b; };
+    std::vector<E> cand;
+    if (P <= 64) {
+        cand.reserve((size_t)P * (P - 1) / 2);
+        for (int i = 0; i < P; i++)
+            for (int j = i + 1; j < P; j++) cand.push_back({dist(i, j), i, j});
+    } else {
+        std::vector<int> px(t.x), py(t.y), id(P);
+        for (int k = 0; k < 4; k++) {
+            std::iota(id.begin(), id.end(), 0);
+            std::sort(id.begin(), id.end(), [&](int a, int b) {
+                int64_t sa = (int64_t)px[a] + py[a], sb = (int64_t)px[b] + py[b];
+                return sa != sb ? sa < sb : a < b;
+            });
+            std::map<int, int> sweep;  // key -y -> point
+            for (int i : id) {
+                for (auto it = sweep.lower_bound(-py[i]); it != sweep.end();) {
+                    int j = it->second;
+                    int dx = px[i] - px[j], dy = py[i] - py[j];
+                    if (dy > dx) break;
+                    cand.push_back({dist(i, j), std::min(i, j), std::max(i, j)});
+                    it = sweep.erase(it);
+                }
+                sweep[-py[i]] = i;
+            }
+            for (int i = 0; i < P; i++) {
+                if (k & 1) px[i] = -px[i];
+                else std::swap(px[i], py[i]);
+            }
+        }
+    }
+    std::sort(cand.begin(), cand.end(), [](const E &l, const E &r) {
+        if (l.w != r.w) return l.w < r.w;
+        if (l.a != r.a) return l.a < r.a;
+        return l.b < r.b;
+    });
+    std::vector<int> uf(P);
+    std::iota(uf.begin(), uf.end(), 0);
+    auto find = [&](int v) {
+        while (uf[v] != v) v = uf[v] = uf[uf[v]];
+        return v;
+    };
+    std::vector<std::vector<int>> adj(P);
+    int used = 0;
+    for (auto &e : cand) {
+        int ra = find(e.a), rb = find(e.b);
+        if (ra == rb) continue;
+        uf[ra] = rb;
+        adj[e.a].push_back(e.b);
+        adj[e.b].push_back(e.a);
+        if (++used == P - 1) break;
+    }
+    // ---- Steinerisation
+    std::unordered_map<int64_t, int> at;
+    auto key = [](int x, int y) { return ((int64_t)x << 32) ^ (uint32_t)y; };
+    for (int i = 0; i < P; i++) at[key(t.x[i], t.y[i])] = i;
+    auto drop = [&](int u, int v) {
+        auto &a = adj[u];
+        a.erase(std::find(a.begin(), a.end(), v));
+    };
+    for (int pass = 0; pass < 4; pass++) {
+        bool changed = false;
+        for (int v = 0; v < (int)adj.size(); v++) {
+            auto &nb = adj[v];
+            if (nb.size() < 2) continue;
+            std::vector<int> sn(nb);
+            std::sort(sn.begin(), sn.end());
+            int best_gain = 0, ba = -1, bb = -1, bx = 0, by = 0;
+            for (size_t i = 0; i < sn.size(); i++)
+                for (size_t j = i + 1; j < sn.size(); j++) {
+                    int a = sn[i], b = sn[j];
+                    int sx = med3(t.x[v], t.x[a], t.x[b]), sy = med3(t.y[v], t.y[a], t.y[b]);
+                    int g = dist(v, a) + dist(v, b) -
+                            (std::abs(sx - t.x[v]) + std::abs(sy - t.y[v]) + std::abs(sx - t.x[a]) +
+                             std::abs(sy - t.y[a]) + std::abs(sx - t.x[b]) + std::abs(sy - t.y[b]));
+                    if (g > best_gain) { best_gain = g; ba = a; bb = b; bx = sx; by = sy; }
+                }
+            if (best_gain <= 0) continue;
+            auto it = at.find(key(bx, by));
+            int s;
+            if (it != at.end()) {
+                s = it->second;
+                if (s != ba && s != bb) continue;  // would merge with an unrelated node
+                // s coincides with a neighbour: reattach the other neighbour to it
+                int o = (s == ba) ? bb : ba;
+                drop(v, o); drop(o, v);
+                adj[s].push_back(o); adj[o].push_back(s);
+            } else {
+                s = (int)t.x.size();
+                t.x.push_back(bx); t.y.push_back(by);
+                adj.emplace_back();
+                at[key(bx, by)] = s;
+                drop(v, ba); drop(ba, v); drop(v, bb); drop(bb, v);
+                for (int w : {v, ba, bb}) { adj[s].push_back(w); adj[w].push_back(s); }
+            }
+            changed = true;
+        }
+        if (!changed) break;
+    }
+    // splice out Steiner points of degree <= 2
+    bool again = true;
+    while (again) {
+        again = false;
+        for (int s = P; s < (int)adj.size(); s++) {
+            if (adj[s].size() == 1) {
+                int a = adj[s][0];
+                drop(a, s); adj[s].clear(); again = true;
+            } else if (adj[s].size() == 2) {
+                int a = adj[s][0], b = adj[s][1];
+                drop(a, s); drop(b, s); adj[s].clear();
+                adj[a].push_back(b); adj[b].push_back(a);
+                again = true;
+            }
+        }
+    }
+    // compact node ids (drop emptied Steiner points)
+    std::vector<int> nid(adj.size(), -1);
+    int k = 0;
+    for (int v = 0; v < (int)adj.size(); v++)
+        if (v < P || !adj[v].empty()) nid[v] = k++;
+    std::vector<int> nx(k), ny(k);
+    for (int v = 0; v < (int)adj.size(); v++)
+        if (nid[v] >= 0) { nx[nid[v]] = t.x[v]; ny[nid[v]] = t.y[v]; }
+    for (int v = 0; v < (int)adj.size(); v++)
+        for (int w : adj[v])
+            if (v < w) t.edges.push_back({nid[v], nid[w]});
+    std::sort(t.edges.begin(), t.edges.end());
+    t.x.swap(nx);
+    t.y.swap(ny);
+}
+
+// FLUTE-style branch list for d input points (d >= 2): 2d-2 branches, branch i
+// < d is input point i, branches d.. are Steiner points, branch.n is the
+// neighbour towards the root (node 0), the root points at itself, and unused
+// slots repeat the root.  This is the contract of flute::Tree
+// (src/flute.hpp:43-56) consumed by the reference's my_flute
+// (src/database_cuda.hpp:696-744).
+struct Branch { int x, y, n; };
+inline void to_branches(const std::vector<int> &xin, const std::vector<int> &yin, const Tree &t,
+                        std::vector<Branch> &br) {
+    const int d = (int)xin.size();
+    br.assign(std::max(0, 2 * d - 2), Branch{0, 0, 0});
+    if (d < 2) return;
+    const int V = (int)t.x.size();
+    std::vector<std::vector<int>> adj(V);
+    for (auto &e : t.edges) { adj[e.first].push_back(e.second); adj[e.second].push_back(e.first); }
+    std::vector<int> par(V, -1), order;
+    order.push_back(0);
+    par[0] = 0;
+    for (size_t i = 0; i < order.size(); i++)
+        for (int w : adj[order[i]])
+            if (par[w] < 0) { par[w] = order[i]; order.push_back(w); }
+    // branch index of each tree node: first input point at that position, or a Steiner slot
+    std::vector<int> bidx(V, -1);
+    std::map<std::pair<int, int>, int> pos2node;
+    for (int v = 0; v < t.npins; v++) pos2node[{t.x[v], t.y[v]}] = v;
+    for (int i = 0; i < d; i++) {
+        int v = pos2node.at({xin[i], yin[i]});
+        if (bidx[v] < 0) bidx[v] = i;
+    }
+    int slot = d;
+    for (int v = t.npins; v < V; v++) bidx[v] = slot++;
+    for (int v = 0; v < V; v++) br[bidx[v]] = Branch{t.x[v], t.y[v], bidx[par[v]]};
+    for (int i = 0; i < d; i++) {
+        int v = pos2node.at({xin[i], yin[i]});
+        if (bidx[v] != i) br[i] = Branch{xin[i], yin[i], bidx[v]};  // duplicate input point
+    }
+    for (int s = slot; s < 2 * d - 2; s++) br[s] = Branch{t.x[0], t.y[0], bidx[0]};
+}
+
+}  // namespace igr_steiner

@@ -1,0 +1,176 @@
+"""CUDA kernels (through the C ABI) against the CPU oracle on seeded inputs.
+
+Tolerances: cost tables within 1e-5 relative (the reference's __expf against
+the oracle's exp); every integer, route, stamp and demand result bit-exact
+(demand values are half units, exact in float).  The DP and commit kernels get
+the GPU's own cost map handed to the oracle, so their comparison is exact.
+"""
+import numpy as np
+import pytest
+
+import instantgr_b200 as ig
+import cases
+from oracle_py import Oracle, color as orc_color
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-5
+
+
+def ctx_for(g):
+    c = ig.Ctx(g["L"], g["X"], g["Y"], g["DIR"], g["xlen"], g["ylen"], g["unit_wire"], g["unit_via"], g["short"],
+               g["cap"])
+    c.set_demand(g["demand"])
+    return c
+
+
+GRIDS = [
+    dict(seed=1, X=40, Y=30, dir0=0),
+    dict(seed=2, X=300, Y=17, dir0=1, unit_wire=0.3),
+    dict(seed=3, X=23, Y=1100, dir0=0, edge_len=3, unit_via=1.5),
+    dict(seed=4, X=257, Y=513, dir0=1),
+]
+
+
+@pytest.mark.parametrize("gp", GRIDS)
+def test_cost_refresh_matches_oracle(gp):
+    gp = dict(gp)
+    g = cases.grid_case(gp.pop("seed"), **gp)
+    c = ctx_for(g)
+    c.cost_refresh()
+    v, p = c.costs()
+    _, ov, op = Oracle(g).cost_refresh(g["demand"])
+    np.testing.assert_allclose(v, ov, rtol=RTOL, atol=0)
+    np.testing.assert_allclose(p, op, rtol=RTOL, atol=1e-9)
+
+
+def test_dirty_refresh_equals_full_refresh():
+    g = cases.grid_case(5, X=120, Y=90, dir0=0)
+    c = ctx_for(g)
+    c.cost_refresh()
+    # change demand on a few cells through a via commit, then refresh only dirty tracks
+    XY = g["X"] * g["Y"]
+    routes = np.array([3, 2 * XY + 10 * g["Y"] + 20, 6 * XY + 10 * g["Y"] + 20], np.int32)
+    c.commit_vias(np.array([0], np.int64), routes, stamp=1, K=1)
+    c.cost_refresh(only_dirty=True)
+    v1, p1 = c.costs()
+    c.cost_refresh(only_dirty=False)
+    v2, p2 = c.costs()
+    assert np.array_equal(v1, v2) and np.array_equal(p1, p2)
+
+
+def _pattern_case(seed, X, Y, dir0, n, kmax=8, uw=1.0):
+    g = cases.grid_case(seed, X=X, Y=Y, dir0=dir0, unit_wire=uw)
+    tb = cases.tree_batch(g, seed + 1, n=n, kmax=kmax)
+    return g, tb
+
+
+@pytest.mark.parametrize("seed,X,Y,dir0,n,kmax", [(11, 40, 30, 0, 80, 8), (12, 64, 50, 1, 200, 8),
+                                                  (13, 120, 100, 0, 150, 24)])
+def test_pattern_route_and_commit_match_oracle(seed, X, Y, dir0, n, kmax):
+    g, tb = _pattern_case(seed, X, Y, dir0, n, kmax)
+    c = ctx_for(g)
+    c.cost_refresh()
+    vc, ps = c.costs()
+    total = int(tb["route_off"][-1] + tb["route_cap"][-1])
+    stamp = 7
+    r_gpu = np.zeros(total, np.int32)
+    c.pattern_route(tb["node_off"], tb["nodes"], tb["par"], tb["route_off"], tb["route_cap"], r_gpu, stamp)
+    pre_gpu = c.pre()
+    o = Oracle(g)
+    r_orc = np.zeros(total, np.int32)
+    pre = np.zeros(o.N, np.int32)
+    st = np.zeros(o.N, np.int32)
+    assert o.pattern_route(vc, ps, tb["node_off"], tb["nodes"], tb["par"], tb["route_off"], tb["route_cap"], r_orc,
+                           pre, st, stamp) == 0
+    for k in range(n):
+        a = int(tb["route_off"][k])
+        m = int(r_orc[a])
+        assert np.array_equal(r_gpu[a:a + m], r_orc[a:a + m]), f"net {k}"
+    assert np.array_equal(pre_gpu, pre)
+    # wire commit then via commit
+    c.commit_wires(stamp)
+    dem = g["demand"].copy()
+    wl = o.commit_wires(pre, dem, st, stamp)
+    assert np.array_equal(c.stamps(), st)
+    o.commit_vias(tb["route_off"], r_orc, dem, st, stamp, 1)
+    c.commit_vias(tb["route_off"], r_gpu, stamp, 1)
+    assert np.array_equal(c.demand(), dem)
+    assert np.array_equal(c.pre(), np.zeros_like(pre))
+    wl_gpu, vias_gpu, _ = c.score()
+    assert wl_gpu == wl
+
+
+def test_ripup_and_overflow_marking_match_oracle():
+    g, tb = _pattern_case(21, 60, 50, 0, 250, 8)
+    c = ctx_for(g)
+    c.cost_refresh()
+    vc, ps = c.costs()
+    total = int(tb["route_off"][-1] + tb["route_cap"][-1])
+    r = np.zeros(total, np.int32)
+    c.pattern_route(tb["node_off"], tb["nodes"], tb["par"], tb["route_off"], tb["route_cap"], r, 3)
+    c.commit_wires(3)
+    c.commit_vias(tb["route_off"], r, 3, 1)
+    dem = c.demand()
+    o = Oracle(g)
+    for thr, me in ((0, 10), (0, 0), (-2, 3)):
+        assert np.array_equal(c.mark_overflow(tb["route_off"], r, thr, me),
+                              o.mark_overflow(dem, tb["route_off"], r, thr, me))
+    xs, ys = c.congestion_view()
+    oxs, oys = o.congestion_view(dem)
+    assert np.array_equal(xs, oxs) and np.array_equal(ys, oys)
+    # rip-up of half of the nets: wires (K=-1) then vias with the same stamp
+    st = c.stamps()
+    d2 = dem.copy()
+    half = tb["route_off"][::2].copy()
+    o.ripup_wires(half, r, d2, st, 4, -1)
+    o.commit_vias(half, r, d2, st, 4, -1)
+    c.ripup_wires(half, r, 4, -1)
+    c.commit_vias(half, r, 4, -1)
+    assert np.array_equal(c.demand(), d2)
+    assert np.array_equal(c.stamps(), st)
+    _, _, of = c.score()
+    np.testing.assert_allclose(of, o.overflow_cost(d2), rtol=RTOL)
+
+
+@pytest.mark.parametrize("seed,n", [(31, 300), (32, 1500)])
+def test_coloring_matches_oracle(seed, n):
+    X, Y = 64, 48
+    args = cases.color_case(seed, X, Y, n)
+    g = cases.grid_case(1, X=X, Y=Y)
+    c = ctx_for(g)
+    b_gpu, nb_gpu = c.color_batches(*args, sparsity=3)
+    b_orc, nb_orc = orc_color(X, Y, *args, sparsity=3)
+    assert nb_gpu == nb_orc
+    assert np.array_equal(b_gpu, b_orc)
+    # no two nets of a batch share a conflict point
+    pt_off, pts = args[0], args[1]
+    for b in range(nb_gpu):
+        cells = [p for k in np.nonzero(b_gpu == b)[0] for p in pts[pt_off[k]:pt_off[k + 1]]]
+        assert len(cells) == len(set(cells))
+
+
+@pytest.mark.parametrize("seed,X,Y,dir0,n", [(41, 48, 40, 0, 50), (42, 70, 60, 1, 120)])
+def test_dag_route_matches_oracle(seed, X, Y, dir0, n):
+    g = cases.grid_case(seed, X=X, Y=Y, dir0=dir0)
+    d = cases.dag_batch(g, seed + 1, n=n)
+    c = ctx_for(g)
+    c.cost_refresh()
+    vc, ps = c.costs()
+    total = int(d["route_off"][-1] + d["route_cap"][-1])
+    r_gpu = np.zeros(total, np.int32)
+    stamp = 11
+    c.dag_route(d["node_off"], d["nodes"], d["depth"], d["par_off"], d["par"], d["child_slot"], d["child_num"],
+                d["route_off"], d["route_cap"], r_gpu, stamp)
+    pre_gpu = c.pre()
+    o = Oracle(g)
+    r_orc = np.zeros(total, np.int32)
+    pre = np.zeros(o.N, np.int32)
+    st = np.zeros(o.N, np.int32)
+    assert o.dag_route(vc, ps, d, d["route_off"], d["route_cap"], r_orc, pre, st, stamp) == 0
+    for k in range(n):
+        a = int(d["route_off"][k])
+        m = int(r_orc[a])
+        assert m > 1, f"net {k} produced no route"
+        assert np.array_equal(r_gpu[a:a + m], r_orc[a:a + m]), f"net {k}"
+    assert np.array_equal(pre_gpu, pre)

@@ -1,0 +1,93 @@
+"""End-to-end routing through the C ABI and the command line, scored by the
+reference's own evaluator (run/evaluator.cpp built into oracle/_ref)."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import instantgr_b200 as ig
+from conftest import GOLDEN, ROOT
+
+pytestmark = pytest.mark.gpu
+
+EVALUATOR = os.path.join(ROOT, "oracle", "_ref", "evaluator")
+
+
+def evaluate(cap, net, out):
+    p = subprocess.run([EVALUATOR, cap, net, out], capture_output=True, text=True, timeout=600)
+    stat = [l for l in p.stdout.splitlines() if l.startswith("FOR_STAT")]
+    assert p.returncode == 0 and stat, p.stdout[-2000:] + p.stderr[-2000:]
+    opens = [l for l in p.stdout.splitlines() if l.startswith("Number of open nets")]
+    assert opens and opens[0].split(":")[1].strip() == "0"
+    return [float(v) for v in stat[0].split()[1:]]
+
+
+@pytest.fixture(scope="module")
+def small_design(tmp_path_factory):
+    d = tmp_path_factory.mktemp("design")
+    cap, net = str(d / "s.cap"), str(d / "s.net")
+    ig.generate_custom(96, 96, 3000, seed=41, cap_mode=0, block_frac=0.05, pin_mode=0, bbox_median=8,
+                       bbox_sigma=1.0, cap=cap, net=net)
+    return cap, net, d
+
+
+def test_route_files_produces_connected_guides(small_design):
+    cap, net, d = small_design
+    out = str(d / "s.out")
+    ig.route_files(cap, net, out)
+    wl, via, of, tot = evaluate(cap, net, out)
+    assert tot == wl + via + of or abs(tot - (wl + via + of)) <= 2
+
+
+def test_cli_matches_library(small_design):
+    cap, net, d = small_design
+    out1, out2 = str(d / "a.out"), str(d / "b.out")
+    ig.route_files(cap, net, out1)
+    p = subprocess.run([ig.ROUTE_BIN, "-cap", cap, "-net", net, "-out", out2], capture_output=True, text=True)
+    assert p.returncode == 0, p.stderr
+    assert open(out1).read() == open(out2).read(), "routing must be deterministic"
+
+
+def test_router_stats_and_gpu_score(small_design):
+    cap, net, d = small_design
+    r = ig.Router(cap, net, rrr_iters=1)
+    r.run()
+    s = r.stats()
+    assert s["routing_nets"] > 0 and s["batches1"] > 0
+    out = str(d / "c.out")
+    r.write(out)
+    wl, via, of, tot = evaluate(cap, net, out)
+    # the in-run estimate counts wires per edge and vias per layer like the evaluator
+    assert abs(s["wirelength"] - wl) <= 1e-6 * max(1, wl)
+    r.close()
+
+
+def test_more_iterations_do_not_worsen_score(small_design):
+    cap, net, d = small_design
+    scores = []
+    for it in (1, 3):
+        out = str(d / f"it{it}.out")
+        ig.route_files(cap, net, out, rrr_iters=it)
+        scores.append(evaluate(cap, net, out)[3])
+    assert scores[1] <= scores[0] * 1.005
+
+
+def test_score_close_to_reference_router(tmp_path):
+    """Same design as the reference run recorded in tests/golden/e2e_reference.json:
+    evaluator total within 0.5%."""
+    path = os.path.join(GOLDEN, "e2e_reference.json")
+    if not os.path.exists(path):
+        pytest.fail("e2e_reference.json missing (tests/golden/make_golden.py)")
+    ref = json.load(open(path))
+    for name, rec in ref.items():
+        if "for_stat" not in rec or not rec["for_stat"]:
+            continue
+        cap, net, out = (str(tmp_path / (name + s)) for s in (".cap", ".net", ".out"))
+        ig.generate_custom(rec["X"], rec["Y"], rec["nets"], seed=rec["seed"], cap_mode=0, block_frac=0.05,
+                           pin_mode=0, bbox_median=8, bbox_sigma=1.0, cap=cap, net=net)
+        ig.route_files(cap, net, out)
+        mine = evaluate(cap, net, out)[3]
+        theirs = float(rec["for_stat"].split()[4])
+        assert mine <= theirs * 1.005, (name, mine, theirs)
