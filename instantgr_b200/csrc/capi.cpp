@@ -104,7 +104,7 @@ int igr_router_run(igr_router *h) {
 int igr_router_write(igr_router *h, const char *out) {
     if (!h || !out) return fail(nullptr, IGR_ERR_INVALID, "null argument");
     return guard(&h->err, [&] {
-        if (h->r.h_routes.empty() && !h->r.ns.nets.empty()) throw Error(ERR_STATE, "route before writing");
+        if (!h->r.ran && !h->r.ns.nets.empty()) throw Error(ERR_STATE, "route before writing");
         h->r.write(out);
     });
 }
@@ -185,7 +185,8 @@ int igr_router_route(igr_router *h, int net, int32_t *out, int cap, int *len) {
     return guard(&h->err, [&] {
         auto &r = h->r;
         if (net < 0 || net >= (int)r.ns.nets.size()) throw Error(ERR_INVALID, "net id out of range");
-        if (r.h_routes.empty()) throw Error(ERR_STATE, "route before reading routes");
+        if (!r.ran) throw Error(ERR_STATE, "route before reading routes");
+        r.fetch_routes();
         const int *rec = r.route_of(net);
         *len = rec[0];
         if (out) {
@@ -451,6 +452,20 @@ int igr_commit_wires(igr_ctx *c, int32_t stamp) {
 
 static void upload_records(igr_ctx *c, int n, const int64_t *off, const int32_t *routes) {
     const int64_t ext = records_extent(n, off, nullptr, routes);
+    const int64_t cells = c->go.g.N;
+    const int X = c->go.g.X, Y = c->go.g.Y;
+    for (int k = 0; k < n; k++) {
+        const int32_t *r = routes + off[k];
+        if (r[0] < 1 || (r[0] & 1) == 0) throw Error(ERR_INVALID, "route record count must be odd and >= 1");
+        for (int j = 1; j < r[0]; j += 2) {
+            const int a = r[j], b = r[j + 1];
+            if (a < 0 || b < 0 || a >= cells || b >= cells) throw Error(ERR_INVALID, "route position out of range");
+            const int la = a / (X * Y), lb = b / (X * Y);
+            const int xa = a / Y % X, ya = a % Y, xb = b / Y % X, yb = b % Y;
+            if (la != lb && (xa != xb || ya != yb)) throw Error(ERR_INVALID, "a via must stay on one GCell");
+            if (la == lb && xa != xb && ya != yb) throw Error(ERR_INVALID, "a wire must be straight");
+        }
+    }
     std::vector<int> ids(n);
     std::iota(ids.begin(), ids.end(), 0);
     c->a.upload(ids, c->s);

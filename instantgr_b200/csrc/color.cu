@@ -78,7 +78,8 @@ __global__ void coloring_kernel(ColorDev c, Bar bar, int *err, int max_batches) 
             for (int k = tid; k < c.n; k += nth) {
                 if (c.status[k] == 2 || c.batch[k] != -1) continue;
                 c.status[k] = 1;
-                for (int i = c.pt_off[k]; i < c.pt_off[k + 1]; i++) {
+                const int sh = c.perm ? c.perm[k] : k;
+                for (int i = c.pt_off[sh]; i < c.pt_off[sh + 1]; i++) {
                     const int p = c.pts[i], x = p / Y, y = p % Y;
                     const int dx[4] = {0, 0, -1, 1}, dy[4] = {0, -1, 0, 0};
                     for (int j = 0; j < 4; j++) {
@@ -86,12 +87,12 @@ __global__ void coloring_kernel(ColorDev c, Bar bar, int *err, int max_batches) 
                         if (nx >= 0 && nx < X && ny >= 0 && ny < Y) atomicMax(&c.map[nx * Y + ny], k);
                     }
                 }
-                for (int i = c.h_off[k]; i < c.h_off[k + 1]; i++) {
+                for (int i = c.h_off[sh]; i < c.h_off[sh + 1]; i++) {
                     const int s = c.hseg[2 * i], e = c.hseg[2 * i + 1];
                     const int y = s % Y;
                     for (int x = s / Y; x <= e / Y; x += c.sparsity) atomicMax(&c.map[x * Y + y], k);
                 }
-                for (int i = c.v_off[k]; i < c.v_off[k + 1]; i++) {
+                for (int i = c.v_off[sh]; i < c.v_off[sh + 1]; i++) {
                     const int s = c.vseg[2 * i], e = c.vseg[2 * i + 1];
                     const int x = s / Y;
                     for (int y = s % Y; y <= e % Y; y += c.sparsity) atomicMax(&c.map[x * Y + y], k);
@@ -102,7 +103,8 @@ __global__ void coloring_kernel(ColorDev c, Bar bar, int *err, int max_batches) 
             for (int k = tid; k < c.n; k += nth) {
                 if (c.status[k] == 2 || c.batch[k] != -1) continue;
                 bool ok = true;
-                for (int i = c.pt_off[k]; i < c.pt_off[k + 1] && ok; i++) ok = c.map[c.pts[i]] == k;
+                const int sh = c.perm ? c.perm[k] : k;
+                for (int i = c.pt_off[sh]; i < c.pt_off[sh + 1] && ok; i++) ok = c.map[c.pts[i]] == k;
                 if (ok) {
                     c.batch[k] = cur;
                     flags[0] = 1;
@@ -113,7 +115,8 @@ __global__ void coloring_kernel(ColorDev c, Bar bar, int *err, int max_batches) 
             if (!flags[1]) break;
             // block nets whose points belong to a member of this batch
             for (int i = tid; i < c.npts; i += nth) {
-                const int k = c.pt_net[i];
+                const int k = c.rank ? c.rank[c.pt_net[i]] : c.pt_net[i];
+                if (k < 0) continue;  // shape not in this colouring
                 if (c.status[k] != 1 || c.batch[k] != -1) continue;
                 const int pre = c.map[c.pts[i]];
                 if (pre != -1 && c.batch[pre] != -1 && c.status[k] != 2) c.status[k] = 2;

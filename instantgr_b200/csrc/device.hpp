@@ -47,14 +47,14 @@ void launch_wire_commit(const GridDev &g, int stamp, bool only_dirty, cudaStream
 
 struct TreeBatchDev {
     const int *net_ids;      // [n] routing-net id of each net of the batch
-    const int *node_off;     // [n+1] node offset of each net (into nodes/par)
+    const int *node_off;     // [routing nets+1] node offset of each net id (into nodes/par)
     const int *nodes;        // tree nodes, preorder, reference encoding (Steiner layer = L)
     const int *par;          // parent (local index) per node, -1 at the root
     const int64_t *route_off;  // [routing nets] route record offset (ints)
     const int *route_cap;    // [routing nets] route record capacity (ints)
     int *routes;             // route records
     double *scratch;         // per-node DP tables of nets larger than the shared-memory tile
-    const int64_t *scratch_off;  // [n] offset (in nodes) into scratch, -1 for nets that fit on chip
+    const int64_t *scratch_off;  // [routing nets] offset (in nodes) into scratch, -1 for nets that fit on chip
     int64_t scratch_nodes;   // nodes covered by scratch: 45 doubles each, then 46 ints each
     int n;
 };
@@ -116,9 +116,13 @@ void launch_from_track_layout_i(const GridDev &g, const int *trk, int *ref, cuda
 // ---- batch colouring (database_cuda.hpp:288-434, made deterministic)
 struct ColorDev {
     int n = 0, X = 0, Y = 0, sparsity = 15;
-    const int *pt_off = nullptr, *pts = nullptr;   // [n+1], 2-D cells
-    const int *pt_net = nullptr;                   // [points] owner
-    const int *h_off = nullptr, *hseg = nullptr;   // [n+1], pairs
+    // shapes are indexed by shape id s; the colouring ranks k = 0..n-1 (higher
+    // k wins a cell) with perm[k] = shape of rank k and rank[s] = its inverse
+    // (both null: identity)
+    const int *perm = nullptr, *rank = nullptr;
+    const int *pt_off = nullptr, *pts = nullptr;   // [shapes+1], 2-D cells
+    const int *pt_net = nullptr;                   // [points] owner shape
+    const int *h_off = nullptr, *hseg = nullptr;   // [shapes+1], pairs
     const int *v_off = nullptr, *vseg = nullptr;
     int npts = 0;
     int *map = nullptr;       // [X*Y]

@@ -150,24 +150,40 @@ void generate_design(const GenParams &p, const char *cap_path, const char *net_p
         }
         w = std::max(1, std::min(X, w));
         h = std::max(1, std::min(Y, h));
+        // room for every pin on a GCell of its own (access points of different
+        // pins never share a GCell, as in ISPD2024 designs)
+        while ((int64_t)w * h < 4LL * k && (w < X || h < Y)) {
+            if (w < X) w++;
+            if (h < Y) h++;
+        }
         int x0 = std::max(0, std::min(X - w, (int)std::lround(cx - w / 2.0)));
         int y0 = std::max(0, std::min(Y - h, (int)std::lround(cy - h / 2.0)));
         o.s("net"); o.i(n); o.s("\n(\n");
+        used.clear();
+        auto taken = [&](int x, int y) { return std::find(used.begin(), used.end(), std::make_pair(x, y)) != used.end(); };
         for (int q = 0; q < k; q++) {
-            int px = x0 + rng.range(0, w - 1), py = y0 + rng.range(0, h - 1);
+            int px = -1, py = -1;
+            for (int t = 0; t < 64; t++) {
+                int cx2 = x0 + rng.range(0, w - 1), cy2 = y0 + rng.range(0, h - 1);
+                if (!taken(cx2, cy2)) { px = cx2; py = cy2; break; }
+            }
+            if (px < 0)  // dense box: first free GCell in scan order
+                for (int x = x0; x < x0 + w && px < 0; x++)
+                    for (int y = y0; y < y0 + h; y++)
+                        if (!taken(x, y)) { px = x; py = y; break; }
+            if (px < 0) break;  // the whole box is used: fewer pins
             int nap = rng.range(1, 3);
-            used.clear();
             o.c('[');
             static const int dx[4] = {1, -1, 0, 0}, dy[4] = {0, 0, 1, -1};
             int ax = px, ay = py;
             for (int a = 0; a < nap; a++) {
-                if (a > 0) {  // a neighbouring GCell not used by this pin yet
+                if (a > 0) {  // a neighbouring GCell not used by any pin of the net yet
                     bool ok = false;
                     for (int t = 0; t < 8 && !ok; t++) {
                         int dd = rng.range(0, 3);
                         int nx = px + dx[dd], ny = py + dy[dd];
                         if (nx < 0 || ny < 0 || nx >= X || ny >= Y) continue;
-                        if (std::find(used.begin(), used.end(), std::make_pair(nx, ny)) != used.end()) continue;
+                        if (taken(nx, ny)) continue;
                         ax = nx; ay = ny; ok = true;
                     }
                     if (!ok) break;

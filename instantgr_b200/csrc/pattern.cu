@@ -69,8 +69,8 @@ __global__ void __launch_bounds__(kWarps * 32) pattern_route_kernel(GridDev g, T
 
     for (int k = gw; k < b.n; k += nw) {
         const int net = b.net_ids[k];
-        const int nb = b.node_off[k];
-        const int n = b.node_off[k + 1] - nb;
+        const int nb = b.node_off[net];
+        const int n = b.node_off[net + 1] - nb;
         const int *nodes = b.nodes + nb;
         const int *par = b.par + nb;
         double *dist;
@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kWarps * 32) pattern_route_kernel(GridDev g, T
         if (n <= kNodeTile) {
             dist = sm.dist; from = sm.from; lr = sm.lr;
         } else {
-            const int64_t so = b.scratch_off[k];
+            const int64_t so = b.scratch_off[net];
             if (so < 0) { set_error(g.err, ERR_STATE); continue; }
             if (so + n > b.scratch_nodes) { set_error(g.err, ERR_CAPACITY); continue; }
             dist = b.scratch + so * kR;

@@ -1,6 +1,8 @@
 // Rip-up-and-reroute driver (src/main.cpp:22-73, src/Lshape_route.hpp:155-257,
 // src/Lshape_route_detour.hpp:726-1112), restated for one GPU:
 //
+//   open      read, pin selection, Steiner trees, split (host threads); trees
+//             and conflict shapes uploaded once and kept resident
 //   phase 1   HPWL order -> GPU colouring -> per batch: cost refresh, tree DP,
 //             wire commit, via commit
 //   pass i    overflow marking -> congestion view -> detour DAGs of the marked
@@ -10,7 +12,8 @@
 // InstantGR runs one pass; rrr_iters > 1 repeats the pass on the nets that
 // still overflow.  All per-batch work is stream-ordered with no host
 // synchronisation between batches (the reference synchronises after every
-// phase-2 launch).
+// phase-2 launch), and no device memory is allocated per run once the
+// buffers have grown to the design's size.
 #include "router.hpp"
 
 #include <algorithm>
@@ -110,6 +113,14 @@ void KernelTimer::reset() {
     for (int k = 0; k < KC_N; k++) { ms[k] = 0; launches[k] = 0; }
 }
 
+void ShapeDev::upload(const ShapeSet &sh, cudaStream_t st) {
+    pt_off.upload(sh.pt_off, st); pts.upload(sh.pts, st); pt_net.upload(sh.pt_net, st);
+    h_off.upload(sh.h_off, st); hseg.upload(sh.hseg, st);
+    v_off.upload(sh.v_off, st); vseg.upload(sh.vseg, st);
+    npts = (int)sh.pts.size();
+    nshapes = (int)sh.pt_off.size() - 1;
+}
+
 // ------------------------------------------------------------------ router
 Router::~Router() {
     kt.collect();
@@ -122,12 +133,36 @@ void Router::open(const char *cap, const char *net) {
     const double t0 = now_s();
     read_design(d, cap, net, threads);
     build_netset(d, ns, threads);
-    if (verbose) std::fprintf(stderr, "[igr] read+trees %.2fs: %d nets, %zu routing nets\n", now_s() - t0,
-                              d.num_nets(), ns.nets.size());
+    // trees in DFS preorder, net-id order, and the phase-1 route record layout
+    const int R = (int)ns.nets.size();
+    tree_off.assign(R + 1, 0);
+    for (int i = 0; i < R; i++) tree_off[i + 1] = tree_off[i] + (int)ns.nets[i].tnode.size();
+    tree_nodes.resize(tree_off[R]);
+    tree_par.resize(tree_off[R]);
+    parallel_for(R, threads, [&](int b, int e) {
+        for (int i = b; i < e; i++) flatten_tree(ns.nets[i], tree_nodes.data() + tree_off[i], tree_par.data() + tree_off[i]);
+    });
+    route_off.assign(R, 0);
+    route_cap.assign(R, 0);
+    route_end1 = 0;
+    scratch_off.assign(R, -1);
+    scratch_nodes = 0;
+    for (int i = 0; i < R; i++) {
+        const auto &n = ns.nets[i];
+        route_cap[i] = (int)std::max<int64_t>(12 * (int64_t)n.pins.size(), 8 * (int64_t)n.tnode.size() + 1);
+        route_off[i] = route_end1;
+        route_end1 += route_cap[i];
+        const int cnt = tree_off[i + 1] - tree_off[i];
+        if (cnt > kPatternNodeTile) { scratch_off[i] = scratch_nodes; scratch_nodes += cnt; }
+    }
+    route_off1 = route_off;
+    route_cap1 = route_cap;
+    if (verbose) std::fprintf(stderr, "[igr] read+trees %.2fs: %d nets, %d routing nets\n", now_s() - t0,
+                              d.num_nets(), R);
 }
 
-// Device state is created on the first run, so that opening a design (parsing,
-// pin selection, trees) needs no GPU.
+// Device state is created and the inputs uploaded on the first run, so that
+// opening a design (parsing, pin selection, trees) needs no GPU.
 void Router::ensure_device() {
     if (s) return;
     cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
@@ -140,6 +175,28 @@ void Router::ensure_device() {
     for (int l = 0; l < L; l++) sc[l] = d.short_cost[l + 1];
     go.create(L, X, Y, d.layer_dir[1], d.x_edge_len.data(), d.y_edge_len.data(), d.unit_wire, d.unit_via, sc.data(),
               capr.data(), s);
+    // resident inputs
+    d_tree_off.upload(tree_off, s);
+    d_tree_nodes.upload(tree_nodes, s);
+    d_tree_par.upload(tree_par, s);
+    d_scratch_off.upload(scratch_off, s);
+    d_scratch.alloc((size_t)pattern_scratch_doubles(scratch_nodes));
+    ShapeSet sh;
+    const int R = (int)ns.nets.size();
+    for (int i = 0; i < R; i++) {
+        const RNet &r = ns.nets[i];
+        for (int q : r.points) { sh.pts.push_back(q); sh.pt_net.push_back(i); }
+        sh.pt_off.push_back((int)sh.pts.size());
+        for (auto &sg : r.hseg) { sh.hseg.push_back(sg.first); sh.hseg.push_back(sg.second); }
+        sh.h_off.push_back((int)(sh.hseg.size() / 2));
+        for (auto &sg : r.vseg) { sh.vseg.push_back(sg.first); sh.vseg.push_back(sg.second); }
+        sh.v_off.push_back((int)(sh.vseg.size() / 2));
+    }
+    d_shapes1.upload(sh, s);
+    std::vector<int> ids(R);
+    std::iota(ids.begin(), ids.end(), 0);
+    d_all_ids.upload(ids, s);
+    cuda_check(cudaStreamSynchronize(s), "inputs");
 }
 
 void Router::grow_routes(int64_t need) {
@@ -160,77 +217,60 @@ void Router::run() {
     kt.reset();
     go.reset_demand(s);
     global_stamp = 0;
+    h_routes_valid = false;
     const int R = (int)ns.nets.size();
-    route_off.assign(R, 0);
-    route_cap.assign(R, 0);
-    route_end = 0;
+    // phase-1 records at their fixed offsets; reroutes are appended after them
+    route_off = route_off1;
+    route_cap = route_cap1;
+    route_end = route_end1;
     int m = mode;
     if (m < 0) m = R > 20000000 ? 2 : (R > 5000000 ? 1 : 0);
     mode_eff = m;
     phase1();
     for (int it = 0; it < rrr_iters; it++)
         if (!rrr_pass(it)) break;
-    // host copy of all route records
-    h_routes.resize(route_end);
-    if (route_end)
-        cuda_check(cudaMemcpyAsync(h_routes.data(), routes.p, route_end * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
     if (int e = go.check_error(s)) throw Error(e, "device error during routing");
     st.wall = now_s() - t0;
     kt.collect();
     compute_score();
+    ran = true;
     if (verbose)
         std::fprintf(stderr, "[igr] route %.3fs  WL %.0f  via %.0f  OF %.0f  total %.0f\n", st.wall, score_wl,
                      score_via, score_of, score_wl + score_via + score_of);
 }
 
+void Router::fetch_routes() {
+    if (h_routes_valid) return;
+    h_routes.resize(route_end);
+    if (route_end)
+        cuda_check(cudaMemcpyAsync(h_routes.data(), routes.p, route_end * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    st.d2h_bytes += route_end * 4;
+    h_routes_valid = true;
+}
+
 // Phase 1 (Lshape_route.hpp:155-257)
 void Router::phase1() {
     const int R = (int)ns.nets.size();
-    const int X = ns.X, Y = ns.Y;
     std::vector<int> order(R);
     std::iota(order.begin(), order.end(), 0);
     std::sort(order.begin(), order.end(), [&](int l, int r) { return ns.nets[l].hpwl > ns.nets[r].hpwl; });
     std::vector<std::vector<int>> batches;
-    color_nets(order, false, 15, batches);
+    color_nets(order, d_shapes1, 15, batches);
     std::reverse(batches.begin(), batches.end());
     st.batches1 = (int)batches.size();
-    // routing order, tree CSR, route records
-    std::vector<int> net_ids, batch_off{0}, node_off{0};
+    std::vector<int> net_ids, batch_off{0};
     net_ids.reserve(R);
     for (auto &b : batches) {
         net_ids.insert(net_ids.end(), b.begin(), b.end());
         batch_off.push_back((int)net_ids.size());
     }
-    int64_t tot_nodes = 0;
-    for (int id : net_ids) {
-        tot_nodes += (int64_t)ns.nets[id].tnode.size();
-        node_off.push_back((int)tot_nodes);
-    }
-    std::vector<int> nodes(tot_nodes), par(tot_nodes);
-    parallel_for(R, threads, [&](int b, int e) {
-        for (int k = b; k < e; k++) flatten_tree(ns.nets[net_ids[k]], nodes.data() + node_off[k], par.data() + node_off[k]);
-    });
-    for (int id = 0; id < R; id++) {
-        const auto &n = ns.nets[id];
-        route_cap[id] = (int)std::max<int64_t>(12 * (int64_t)n.pins.size(), 8 * (int64_t)n.tnode.size() + 1);
-        route_off[id] = route_end;
-        route_end += route_cap[id];
-    }
-    std::vector<int64_t> scratch_off(R, -1);
-    int64_t scratch_nodes = 0;
-    for (int k = 0; k < R; k++) {
-        int cnt = node_off[k + 1] - node_off[k];
-        if (cnt > kPatternNodeTile) { scratch_off[k] = scratch_nodes; scratch_nodes += cnt; }
-    }
     grow_routes(route_end);
-    DevBuf<int> d_ids, d_node_off, d_nodes, d_par;
-    DevBuf<int64_t> d_scr_off;
-    DevBuf<double> d_scr;
-    d_ids.upload(net_ids, s); d_node_off.upload(node_off, s); d_nodes.upload(nodes, s); d_par.upload(par, s);
-    d_route_off.upload(route_off, s); d_route_cap.upload(route_cap, s);
-    d_scr_off.upload(scratch_off, s);
-    d_scr.alloc((size_t)pattern_scratch_doubles(scratch_nodes));
+    d_ids.upload(net_ids, s);
+    d_route_off.upload(route_off, s);
+    d_route_cap.upload(route_cap, s);
+    st.h2d_bytes += (int64_t)net_ids.size() * 4 + (int64_t)R * 12;
     cuda_check(cudaEventRecord(ev0, s), "event");
     for (size_t bi = 0; bi + 1 < batch_off.size(); bi++) {
         const int off = batch_off[bi], n = batch_off[bi + 1] - off;
@@ -238,8 +278,8 @@ void Router::phase1() {
         kt.begin(KC_COST);
         launch_cost_refresh(go.g, true, s);
         kt.end(KC_COST);
-        TreeBatchDev tb{d_ids.p + off, d_node_off.p + off, d_nodes.p, d_par.p, d_route_off.p, d_route_cap.p,
-                        routes.p, d_scr.p, d_scr_off.p + off, scratch_nodes, n};
+        TreeBatchDev tb{d_ids.p + off, d_tree_off.p, d_tree_nodes.p, d_tree_par.p, d_route_off.p, d_route_cap.p,
+                        routes.p, d_scratch.p, d_scratch_off.p, scratch_nodes, n};
         kt.begin(KC_PATTERN);
         launch_pattern_route(go.g, tb, stamp, s);
         kt.end(KC_PATTERN);
@@ -254,49 +294,52 @@ void Router::phase1() {
     }
     cuda_check(cudaEventRecord(ev1, s), "event");
     cuda_check(cudaGetLastError(), "phase-1 launch");
+    // plan of this run, in routing order (for igr_router_plan)
     plan_ids = net_ids;
     plan_batch_off = batch_off;
-    plan_node_off = node_off;
-    plan_nodes.swap(nodes);
-    plan_par.swap(par);
+    plan_node_off.assign(1, 0);
+    plan_nodes.clear();
+    plan_par.clear();
     plan_cap.resize(net_ids.size());
-    for (size_t k = 0; k < net_ids.size(); k++) plan_cap[k] = route_cap[net_ids[k]];
+    for (size_t k = 0; k < net_ids.size(); k++) {
+        const int id = net_ids[k];
+        plan_nodes.insert(plan_nodes.end(), tree_nodes.begin() + tree_off[id], tree_nodes.begin() + tree_off[id + 1]);
+        plan_par.insert(plan_par.end(), tree_par.begin() + tree_off[id], tree_par.begin() + tree_off[id + 1]);
+        plan_node_off.push_back((int)plan_nodes.size());
+        plan_cap[k] = route_cap[id];
+    }
     cuda_check(cudaEventSynchronize(ev1), "phase 1");
     float ms = 0;
     cudaEventElapsedTime(&ms, ev0, ev1);
     st.p1_ms = ms;
     if (int e = go.check_error(s)) throw Error(e, "device error in phase 1");
-    (void)X; (void)Y;
     if (verbose) std::fprintf(stderr, "[igr] phase 1: %zu batches, %.2f ms device\n", batches.size(), ms);
 }
 
 // Colours `order` (highest priority first) into batches of spatially disjoint
-// nets (database_cuda.hpp:437-631); the colouring ranks the reversed list.
-void Router::color_nets(const std::vector<int> &order, bool dag_points, int sparsity,
+// nets (database_cuda.hpp:437-631); the colouring ranks the reversed list, so
+// the first net of `order` wins every conflict.
+void Router::color_nets(const std::vector<int> &order, const ShapeDev &shapes, int sparsity,
                         std::vector<std::vector<int>> &batches) {
     const int n = (int)order.size();
     batches.clear();
     if (n == 0) return;
-    std::vector<int> list(order.rbegin(), order.rend());
-    std::vector<int> pt_off{0}, pts, pt_net, h_off{0}, hs, v_off{0}, vs;
-    for (int k = 0; k < n; k++) {
-        const RNet &r = ns.nets[list[k]];
-        const std::vector<int> &p = dag_points ? dag[list[k]].points : r.points;
-        for (int q : p) { pts.push_back(q); pt_net.push_back(k); }
-        pt_off.push_back((int)pts.size());
-        for (auto &sg : r.hseg) { hs.push_back(sg.first); hs.push_back(sg.second); }
-        h_off.push_back((int)(hs.size() / 2));
-        for (auto &sg : r.vseg) { vs.push_back(sg.first); vs.push_back(sg.second); }
-        v_off.push_back((int)(vs.size() / 2));
-    }
-    DevBuf<int> a, b, c, e, f, h, i, map, bat, sta, flags;
-    a.upload(pt_off, s); b.upload(pts, s); c.upload(pt_net, s); e.upload(h_off, s); f.upload(hs, s);
-    h.upload(v_off, s); i.upload(vs, s);
-    map.alloc((size_t)ns.X * ns.Y); bat.alloc(n); sta.alloc(n); flags.alloc(8);
+    const int nshapes = shapes.nshapes;
+    std::vector<int> perm(order.rbegin(), order.rend()), rank(nshapes, -1);
+    for (int k = 0; k < n; k++) rank[perm[k]] = k;
+    d_perm.upload(perm, s);
+    d_rank.upload(rank, s);
+    d_map.alloc((size_t)ns.X * ns.Y);
+    d_bat.alloc(n);
+    d_sta.alloc(n);
+    d_flags.alloc(8);
+    st.h2d_bytes += (int64_t)(n + nshapes) * 4;
     ColorDev cd;
     cd.n = n; cd.X = ns.X; cd.Y = ns.Y; cd.sparsity = sparsity;
-    cd.pt_off = a.p; cd.pts = b.p; cd.pt_net = c.p; cd.h_off = e.p; cd.hseg = f.p; cd.v_off = h.p; cd.vseg = i.p;
-    cd.npts = (int)pts.size(); cd.map = map.p; cd.batch = bat.p; cd.status = sta.p; cd.flags = flags.p;
+    cd.perm = d_perm.p; cd.rank = d_rank.p;
+    cd.pt_off = shapes.pt_off.p; cd.pts = shapes.pts.p; cd.pt_net = shapes.pt_net.p;
+    cd.h_off = shapes.h_off.p; cd.hseg = shapes.hseg.p; cd.v_off = shapes.v_off.p; cd.vseg = shapes.vseg.p;
+    cd.npts = shapes.npts; cd.map = d_map.p; cd.batch = d_bat.p; cd.status = d_sta.p; cd.flags = d_flags.p;
     kt.begin(KC_COLOR);
     int nb = run_coloring(cd, 0, s);
     kt.end(KC_COLOR);
@@ -304,12 +347,13 @@ void Router::color_nets(const std::vector<int> &order, bool dag_points, int spar
     if (nb == -2) throw Error(ERR_TIMEOUT, "colouring barrier timed out");
     if (nb < 0) throw Error(ERR_CUDA, std::string("colouring failed: ") + cudaGetErrorString(cudaGetLastError()));
     std::vector<int> bid(n);
-    cuda_check(cudaMemcpyAsync(bid.data(), bat.p, n * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaMemcpyAsync(bid.data(), d_bat.p, n * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
+    st.d2h_bytes += (int64_t)n * 4;
     batches.assign(nb, {});
     for (int k = 0; k < n; k++) {
         if (bid[k] < 0 || bid[k] >= nb) throw Error(ERR_STATE, "a net was left without a batch");
-        batches[bid[k]].push_back(list[k]);
+        batches[bid[k]].push_back(perm[k]);
     }
 }
 
@@ -319,18 +363,16 @@ bool Router::rrr_pass(int iter) {
     const int R = (int)ns.nets.size();
     const int X = ns.X, Y = ns.Y;
     if (R == 0) return false;
-    if (d_all_ids.n < (size_t)R) {
-        std::vector<int> ids(R);
-        std::iota(ids.begin(), ids.end(), 0);
-        d_all_ids.upload(ids, s);
-    }
     of_sum.alloc(go.g.N);
     d_is_of.alloc(R);
     d_xsum.alloc((size_t)X * Y);
     d_ysum.alloc((size_t)X * Y);
     d_bar.alloc(2);
-    d_route_off.upload(route_off, s);
-    d_route_cap.upload(route_cap, s);
+    if (iter > 0) {  // records moved in the previous pass
+        d_route_off.upload(route_off, s);
+        d_route_cap.upload(route_cap, s);
+        st.h2d_bytes += (int64_t)R * 12;
+    }
     cuda_check(cudaEventRecord(ev0, s), "event");
     // overflow marking and congestion view (graph.hpp:588-601, main.cpp:42-45)
     ViaBatchDev all{d_all_ids.p, d_route_off.p, routes.p, R};
@@ -348,6 +390,7 @@ bool Router::rrr_pass(int iter) {
     cuda_check(cudaMemcpyAsync(cv.xsum.data(), d_xsum.p, cv.xsum.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaMemcpyAsync(cv.ysum.data(), d_ysum.p, cv.ysum.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
+    st.d2h_bytes += R + (int64_t)X * Y * 8;
     std::vector<int> of_nets;
     for (int i = 0; i < R; i++)
         if (is_of[i]) of_nets.push_back(i);
@@ -358,12 +401,46 @@ bool Router::rrr_pass(int iter) {
     // detour DAGs on host threads (Lshape_route_detour.hpp:702-748)
     const double th0 = now_s();
     dag.resize(R);
+    std::vector<char> keep(of_nets.size(), 1);
     parallel_for((int)of_nets.size(), threads, [&](int b, int e) {
-        for (int k = b; k < e; k++) build_dag(ns, ns.nets[of_nets[k]], cv, mode_eff, dag[of_nets[k]]);
+        for (int k = b; k < e; k++) {
+            DagNet &dn = dag[of_nets[k]];
+            build_dag(ns, ns.nets[of_nets[k]], cv, mode_eff, dn);
+            // the DP keeps at most 10 child slots per node (the reference packs the
+            // slot as a decimal digit); nets beyond that keep their current route
+            for (int c : dn.child_num)
+                if (c > 10) keep[k] = 0;
+        }
     });
+    {
+        std::vector<int> kept;
+        for (size_t k = 0; k < of_nets.size(); k++)
+            if (keep[k]) kept.push_back(of_nets[k]);
+        of_nets.swap(kept);
+    }
     st.dag_host_ms += (now_s() - th0) * 1e3;
-    std::vector<std::vector<int>> batches;
-    color_nets(of_nets, true, mode_eff >= 1 ? 2 : 15, batches);
+    if (of_nets.empty()) return false;
+    // colouring on DAG points and tree segments (Lshape_route_detour.hpp:751)
+    ShapeSet sh;
+    for (int id : of_nets) {
+        const RNet &r = ns.nets[id];
+        for (int q : dag[id].points) { sh.pts.push_back(q); sh.pt_net.push_back((int)sh.pt_off.size() - 1); }
+        sh.pt_off.push_back((int)sh.pts.size());
+        for (auto &sg : r.hseg) { sh.hseg.push_back(sg.first); sh.hseg.push_back(sg.second); }
+        sh.h_off.push_back((int)(sh.hseg.size() / 2));
+        for (auto &sg : r.vseg) { sh.vseg.push_back(sg.first); sh.vseg.push_back(sg.second); }
+        sh.v_off.push_back((int)(sh.vseg.size() / 2));
+    }
+    ShapeDev shd;
+    shd.upload(sh, s);
+    st.h2d_bytes += (int64_t)(sh.pts.size() * 2 + sh.hseg.size() + sh.vseg.size() + 3 * of_nets.size()) * 4;
+    std::vector<int> local(of_nets.size());
+    std::iota(local.begin(), local.end(), 0);  // shape k belongs to of_nets[k]; of_nets is in priority order
+    std::vector<std::vector<int>> lb;
+    color_nets(local, shd, mode_eff >= 1 ? 2 : 15, lb);
+    std::vector<std::vector<int>> batches(lb.size());
+    for (size_t b = 0; b < lb.size(); b++)
+        for (int k : lb[b]) batches[b].push_back(of_nets[k]);
     std::reverse(batches.begin(), batches.end());
     // batch-local CSR of all batches, laid end to end
     struct BInfo { int nb, eb, pb, lb, nnb, nets, n, e, slots, depth, max_level; };
@@ -412,10 +489,10 @@ bool Router::rrr_pass(int iter) {
         // counting sort of nodes by depth (stable in node order)
         std::vector<int> cnt(depth + 1, 0);
         for (int v = 0; v < n; v++) cnt[dep[v] + 1]++;
-        for (int d = 0; d < depth; d++) cnt[d + 1] += cnt[d];
+        for (int dd = 0; dd < depth; dd++) cnt[dd + 1] += cnt[dd];
         int ml = 0;
-        for (int d = 0; d <= depth; d++) level_off.push_back(cnt[d]);
-        for (int d = 0; d < depth; d++) ml = std::max(ml, cnt[d + 1] - cnt[d]);
+        for (int dd = 0; dd <= depth; dd++) level_off.push_back(cnt[dd]);
+        for (int dd = 0; dd < depth; dd++) ml = std::max(ml, cnt[dd + 1] - cnt[dd]);
         std::vector<int> ln(n);
         for (int v = 0; v < n; v++) ln[cnt[dep[v]]++] = v;
         level_nodes.insert(level_nodes.end(), ln.begin(), ln.end());
@@ -424,26 +501,23 @@ bool Router::rrr_pass(int iter) {
         bi.push_back(f);
     }
     grow_routes(route_end);
-    DevBuf<int> d_nodes, d_paroff, d_par, d_cslot, d_echild, d_childoff, d_leveloff, d_levelnodes, d_nno, d_ids;
-    DevBuf<int64_t> d_old_off;
-    d_nodes.upload(nodes, s); d_paroff.upload(par_off, s); d_par.upload(par, s); d_cslot.upload(cslot, s);
-    d_echild.upload(echild, s); d_childoff.upload(child_off, s); d_leveloff.upload(level_off, s);
-    d_levelnodes.upload(level_nodes, s); d_nno.upload(net_node_off, s); d_ids.upload(net_ids, s);
+    dg_nodes.upload(nodes, s); dg_paroff.upload(par_off, s); dg_par.upload(par, s); dg_cslot.upload(cslot, s);
+    dg_echild.upload(echild, s); dg_childoff.upload(child_off, s); dg_leveloff.upload(level_off, s);
+    dg_levelnodes.upload(level_nodes, s); dg_nno.upload(net_node_off, s); dg_ids.upload(net_ids, s);
     d_old_off.upload(old_off, s);
     d_route_off.upload(route_off, s);
     d_route_cap.upload(route_cap, s);
+    st.h2d_bytes += (int64_t)(nodes.size() * 2 + par_off.size() * 2 + par.size() * 3 + level_off.size() +
+                              net_node_off.size() + net_ids.size()) * 4 + (int64_t)R * 20;
     int mn = 1, me = 1, ms = 1;
     for (auto &f : bi) { mn = std::max(mn, f.n); me = std::max(me, f.e); ms = std::max(ms, f.slots); }
-    DevBuf<double> costs, cedges;
-    DevBuf<unsigned long long> best, packed;
-    DevBuf<int> bchange, lout, stage, stage_cnt;
-    costs.alloc((size_t)mn * 10); cedges.alloc((size_t)me * 81);
-    best.alloc((size_t)ms * 10); packed.alloc((size_t)ms * 10);
-    bchange.alloc((size_t)me * 81); lout.alloc(mn); stage.alloc((size_t)mn * 8); stage_cnt.alloc(mn);
+    dg_costs.alloc((size_t)mn * 10); dg_cedges.alloc((size_t)me * 81);
+    dg_best.alloc((size_t)ms * 10); dg_packed.alloc((size_t)ms * 10);
+    dg_bchange.alloc((size_t)me * 81); dg_lout.alloc(mn); dg_stage.alloc((size_t)mn * 8); dg_scnt.alloc(mn);
     for (size_t b = 0; b < bi.size(); b++) {
         const BInfo &f = bi[b];
         const int nnet = (int)batches[b].size();
-        ViaBatchDev old{d_ids.p + f.nets, d_old_off.p, routes.p, nnet};
+        ViaBatchDev old{dg_ids.p + f.nets, d_old_off.p, routes.p, nnet};
         const int s1 = ++global_stamp;
         kt.begin(KC_RIPUP);
         launch_wire_ripup(go.g, old, s1, -1, s);
@@ -456,13 +530,13 @@ bool Router::rrr_pass(int iter) {
         DagBatchDev db;
         db.n_nodes = f.n; db.n_edges = f.e; db.n_slots = f.slots; db.depth = f.depth; db.n_nets = nnet;
         db.max_level = f.max_level;
-        db.nodes = d_nodes.p + f.nb; db.par_off = d_paroff.p + f.pb; db.par = d_par.p + f.eb;
-        db.child_slot = d_cslot.p + f.eb; db.edge_child = d_echild.p + f.eb; db.child_off = d_childoff.p + f.pb;
-        db.level_off = d_leveloff.p + f.lb; db.level_nodes = d_levelnodes.p + f.nb;
+        db.nodes = dg_nodes.p + f.nb; db.par_off = dg_paroff.p + f.pb; db.par = dg_par.p + f.eb;
+        db.child_slot = dg_cslot.p + f.eb; db.edge_child = dg_echild.p + f.eb; db.child_off = dg_childoff.p + f.pb;
+        db.level_off = dg_leveloff.p + f.lb; db.level_nodes = dg_levelnodes.p + f.nb;
         db.h_level_off = level_off.data() + f.lb;
-        db.net_node_off = d_nno.p + f.nnb; db.net_ids = d_ids.p + f.nets;
-        db.costs = costs.p; db.best_path = best.p; db.packed = packed.p; db.cost_edges = cedges.p;
-        db.best_change = bchange.p; db.layer_out = lout.p; db.stage = stage.p; db.stage_cnt = stage_cnt.p;
+        db.net_node_off = dg_nno.p + f.nnb; db.net_ids = dg_ids.p + f.nets;
+        db.costs = dg_costs.p; db.best_path = dg_best.p; db.packed = dg_packed.p; db.cost_edges = dg_cedges.p;
+        db.best_change = dg_bchange.p; db.layer_out = dg_lout.p; db.stage = dg_stage.p; db.stage_cnt = dg_scnt.p;
         db.route_off = d_route_off.p; db.route_cap = d_route_cap.p; db.routes = routes.p;
         kt.begin(KC_DAG);
         int nl = launch_dag_route(go.g, db, s2, d_bar.p, cooperative, s);
@@ -475,7 +549,7 @@ bool Router::rrr_pass(int iter) {
         kt.begin(KC_WIRE_COMMIT);
         launch_wire_commit(go.g, s2, true, s);
         kt.end(KC_WIRE_COMMIT);
-        ViaBatchDev nw{d_ids.p + f.nets, d_route_off.p, routes.p, nnet};
+        ViaBatchDev nw{dg_ids.p + f.nets, d_route_off.p, routes.p, nnet};
         kt.begin(KC_VIA_COMMIT);
         launch_via_commit(go.g, nw, s2, 1, s);
         kt.end(KC_VIA_COMMIT);
@@ -507,6 +581,7 @@ void Router::compute_score() {
 }
 
 void Router::write(const char *out) {
+    fetch_routes();
     RouteSource rs;
     rs.routes_of = [&](int net) -> const int * { return h_routes.empty() ? nullptr : route_of(net); };
     write_guides(d, ns, rs, out, threads);

@@ -26,6 +26,7 @@ struct DevBuf {
         p = nullptr;
         n = 0;
     }
+    // grow-only: reuses the allocation when it is large enough
     void alloc(size_t count) {
         if (count <= n && p) return;
         release();
@@ -45,11 +46,10 @@ struct GridOwner {
     GridDev g;
     DevBuf<float> cap, demand, vcost;
     DevBuf<double> presum;
-    DevBuf<int> pre, stamp, xlen, ylen, err, of_sum;
+    DevBuf<int> pre, stamp, xlen, ylen, err;
     DevBuf<double> short_cost, score;
     DevBuf<uint8_t> dirty_cost, dirty_commit;
     DevBuf<unsigned long long> stats;
-    DevBuf<float> scratch_f;
     std::vector<int> layer_first;
     // L, X, Y, DIR, edge lengths, unit costs, short costs [L], capacity [l][x][y] in reference layout
     void create(int L, int X, int Y, int DIR, const int *xlen, const int *ylen, double unit_wire, double unit_via,
@@ -81,6 +81,16 @@ struct KernelTimer {
     void reset();
 };
 
+// Conflict shapes of a set of nets for the batch colouring, in shape order.
+struct ShapeSet {
+    std::vector<int> pt_off{0}, pts, pt_net, h_off{0}, hseg, v_off{0}, vseg;
+};
+struct ShapeDev {
+    DevBuf<int> pt_off, pts, pt_net, h_off, hseg, v_off, vseg;
+    int npts = 0, nshapes = 0;
+    void upload(const ShapeSet &s, cudaStream_t st);
+};
+
 struct Router {
     int rrr_iters = 1, threads = 0, mode = -1, verbose = 0, batched = 0;
     Design d;
@@ -88,41 +98,56 @@ struct Router {
     GridOwner go;
     cudaStream_t s = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // routes: one device buffer, per-net record offset/capacity (phase 1 records
-    // first, reroutes appended)
-    std::vector<int64_t> route_off;
-    std::vector<int> route_cap;
-    int64_t route_end = 0;
-    DevBuf<int> routes;
-    DevBuf<int64_t> d_route_off;
-    DevBuf<int> d_route_cap;
-    std::vector<int> h_routes;  // host copy after a run
     RouterStats st;
+    KernelTimer kt;
     int global_stamp = 0;
     int mode_eff = 0;
-    std::vector<DagNet> dag;          // detour DAG of every routing net (phase 2)
-    DevBuf<int> d_all_ids, of_sum;
+
+    // ---- inputs resident in HBM after open(): trees and conflict shapes in net-id order
+    std::vector<int> tree_off, tree_nodes, tree_par;  // DFS preorder (Lshape_route.hpp:191-208)
+    std::vector<int64_t> scratch_off;                  // per net: DP scratch offset, -1 = on chip
+    int64_t scratch_nodes = 0;
+    DevBuf<int> d_tree_off, d_tree_nodes, d_tree_par;
+    DevBuf<int64_t> d_scratch_off;
+    DevBuf<double> d_scratch;
+    ShapeDev d_shapes1;
+    // ---- route records: phase-1 records at fixed offsets, reroutes appended per run
+    std::vector<int64_t> route_off, route_off1;
+    std::vector<int> route_cap, route_cap1;
+    int64_t route_end1 = 0, route_end = 0;
+    bool ran = false;
+    DevBuf<int> routes;
+    DevBuf<int64_t> d_route_off, d_old_off;
+    DevBuf<int> d_route_cap;
+    std::vector<int> h_routes;  // host copy, made on demand
+    bool h_routes_valid = false;
+    // ---- per-run device buffers (grow-only)
+    DevBuf<int> d_ids, d_all_ids, of_sum, d_perm, d_rank, d_map, d_bat, d_sta, d_flags;
     DevBuf<uint8_t> d_is_of;
     DevBuf<float> d_xsum, d_ysum;
     DevBuf<unsigned> d_bar;
+    DevBuf<int> dg_nodes, dg_paroff, dg_par, dg_cslot, dg_echild, dg_childoff, dg_leveloff, dg_levelnodes, dg_nno,
+        dg_ids, dg_bchange, dg_lout, dg_stage, dg_scnt;
+    DevBuf<double> dg_costs, dg_cedges;
+    DevBuf<unsigned long long> dg_best, dg_packed;
     bool cooperative = true;
-    KernelTimer kt;
+    std::vector<DagNet> dag;  // detour DAG of every rerouted net (phase 2)
+    unsigned long long cost_cells = 0;
     // phase-1 plan of the last run (routing order, batches, trees, route capacity in order)
     std::vector<int> plan_ids, plan_batch_off, plan_node_off, plan_nodes, plan_par, plan_cap;
-    unsigned long long cost_cells = 0;  // cells processed by cost refreshes of the last run
     // score of the last run: wirelength, vias, overflow (GPU estimate)
     double score_wl = 0, score_via = 0, score_of = 0;
-
-    void ensure_device();
-    void color_nets(const std::vector<int> &order, bool dag_points, int sparsity,
-                    std::vector<std::vector<int>> &batches);
-    void compute_score();
 
     ~Router();
     void open(const char *cap, const char *net);
     void run();
     void write(const char *out);
+    void fetch_routes();
     const int *route_of(int net) const { return h_routes.data() + route_off[net]; }
+    void ensure_device();
+    void color_nets(const std::vector<int> &order, const ShapeDev &shapes, int sparsity,
+                    std::vector<std::vector<int>> &batches);
+    void compute_score();
 
    private:
     void phase1();
