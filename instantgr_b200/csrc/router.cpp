@@ -199,18 +199,20 @@ void Router::ensure_device() {
     cuda_check(cudaStreamSynchronize(s), "inputs");
 }
 
+// Grows the route buffer to `need` ints, keeping the records already written.
 void Router::grow_routes(int64_t need) {
     if ((int64_t)routes.n >= need) return;
     DevBuf<int> nb;
     nb.alloc((size_t)std::max<int64_t>(need, (int64_t)(routes.n * 3 / 2)));
-    if (routes.p && route_end > 0)
-        cuda_check(cudaMemcpyAsync(nb.p, routes.p, route_end * sizeof(int), cudaMemcpyDeviceToDevice, s), "D2D");
+    if (routes.p && routes.n > 0)
+        cuda_check(cudaMemcpyAsync(nb.p, routes.p, routes.n * sizeof(int), cudaMemcpyDeviceToDevice, s), "D2D");
     std::swap(routes.p, nb.p);
     std::swap(routes.n, nb.n);
 }
 
 void Router::run() {
     ensure_device();
+    cudaGetLastError();  // start from a clean error state
     const double t0 = now_s();
     st = RouterStats();
     kt.s = s;
