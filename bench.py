@@ -48,7 +48,19 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--workdir", default=os.environ.get("IGR_BENCH_DIR", "/tmp/igr_bench"))
     ap.add_argument("--cpu-batches", type=int, default=0, help="batches in the CPU sample (0 = auto)")
+    ap.add_argument("--route-only", action="store_true",
+                    help="route --warmup + --steps times and print the router statistics (profiling runs)")
     return ap.parse_args()
+
+
+def route_only(args):
+    import instantgr_b200 as ig
+    cap, net = design_files(args)
+    r = ig.Router(cap, net, rrr_iters=args.rrr_iters, profile=1)
+    for _ in range(args.warmup + args.steps):
+        r.run()
+    print(json.dumps(dict(stats=r.stats(), kernels=r.kstats())), flush=True)
+    r.close()
 
 
 class Clocks:
@@ -167,6 +179,8 @@ def main():
     cfg = CONFIGS[args.config]
     workload = dict(workload=f"global routing, {cfg['name']}", config_index=args.config, scale=args.scale,
                     rrr_iters=args.rrr_iters, seed=args.seed, l2="per-step state exceeds L2 (inputs larger than L2)")
+    if args.route_only:
+        return route_only(args)
     if args.impl == "reference":
         return bench_reference(args, rank, world, workload)
 

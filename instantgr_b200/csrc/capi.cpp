@@ -557,15 +557,27 @@ int igr_color_batches(igr_ctx *c, int n, const int32_t *pt_off, const int32_t *p
             if (hseg[i] < 0 || hseg[i] >= XY) throw Error(ERR_INVALID, "segment outside the grid");
         for (int i = 0; i < 2 * v_off[n]; i++)
             if (vseg[i] < 0 || vseg[i] >= XY) throw Error(ERR_INVALID, "segment outside the grid");
-        DevBuf<int> po, p, pn, ho, hs, vo, vs, map, bat, sta, flags;
+        for (int k = 0; k < n; k++) {
+            for (int i = h_off[k]; i < h_off[k + 1]; i++)
+                if (hseg[2 * i] / c->go.g.Y > hseg[2 * i + 1] / c->go.g.Y || hseg[2 * i] % c->go.g.Y != hseg[2 * i + 1] % c->go.g.Y)
+                    throw Error(ERR_INVALID, "horizontal segment must run along x from low to high");
+            for (int i = v_off[k]; i < v_off[k + 1]; i++)
+                if (vseg[2 * i] / c->go.g.Y != vseg[2 * i + 1] / c->go.g.Y || vseg[2 * i] % c->go.g.Y > vseg[2 * i + 1] % c->go.g.Y)
+                    throw Error(ERR_INVALID, "vertical segment must run along y from low to high");
+        }
+        std::vector<int> co, cl;
+        build_claims(n, pt_off, pts, h_off, hseg, v_off, vseg, c->go.g.X, c->go.g.Y, sparsity, co, cl, 0);
+        DevBuf<int> po, p, pn, ho, hs, vo, vs, map, bat, sta, flags, dco, dcl, act;
         po.upload(pt_off, n + 1, c->s); p.upload(pts, pt_off[n], c->s); pn.upload(pt_net, c->s);
         ho.upload(h_off, n + 1, c->s); hs.upload(hseg, 2 * (size_t)h_off[n], c->s);
         vo.upload(v_off, n + 1, c->s); vs.upload(vseg, 2 * (size_t)v_off[n], c->s);
-        map.alloc(XY); bat.alloc(n); sta.alloc(n); flags.alloc(8);
+        dco.upload(co, c->s); dcl.upload(cl, c->s);
+        map.alloc(XY); bat.alloc(n); sta.alloc(n); flags.alloc(8); act.alloc(2 * (size_t)n);
         ColorDev cd;
         cd.n = n; cd.X = c->go.g.X; cd.Y = c->go.g.Y; cd.sparsity = sparsity;
         cd.pt_off = po.p; cd.pts = p.p; cd.pt_net = pn.p; cd.h_off = ho.p; cd.hseg = hs.p; cd.v_off = vo.p;
         cd.vseg = vs.p; cd.npts = pt_off[n]; cd.map = map.p; cd.batch = bat.p; cd.status = sta.p; cd.flags = flags.p;
+        cd.claim_off = dco.p; cd.claim = dcl.p; cd.active = act.p; cd.active2 = act.p + n;
         const int nb = run_coloring(cd, 0, c->s);
         if (nb == -2) throw Error(ERR_TIMEOUT, "colouring barrier timed out");
         if (nb < 0) throw Error(ERR_CUDA, std::string("colouring launch failed: ") + cudaGetErrorString(cudaGetLastError()));

@@ -12,10 +12,14 @@
 // The reference is nondeterministic (a claiming thread re-reads the cell right
 // after its atomicMax while others are still writing, and returns early).
 // Here claiming, committing, blocking and releasing are separate phases
-// separated by grid barriers, so the batches depend only on the input.  The
-// whole colouring is one persistent cooperative kernel: no host round trip per
-// round.  The grid barrier gives up after two seconds and reports
-// ERR_TIMEOUT instead of waiting forever.
+// separated by grid barriers, so the batches depend only on the input.
+//
+// Work layout: the cells a net claims are precomputed once (claim lists, CSR
+// per shape), one warp handles one net with its lanes over the net's claims
+// or points, and only nets still without a batch are visited: the list of
+// active nets is compacted after every batch.  The whole colouring is one
+// persistent cooperative kernel; the grid barrier gives up after two seconds
+// and reports ERR_TIMEOUT instead of waiting forever.
 #include "kcommon.cuh"
 
 namespace igr {
@@ -52,7 +56,7 @@ __device__ bool grid_barrier(Bar b, int *err) {
             while (*vgen == g) {
                 if (*(volatile int *)err) { s_ok = 0; break; }
                 if (global_ns() - t0 > 2000000000ull) { set_error(err, ERR_TIMEOUT); s_ok = 0; break; }
-                __nanosleep(64);
+                __nanosleep(32);
             }
         }
         __threadfence();
@@ -62,50 +66,45 @@ __device__ bool grid_barrier(Bar b, int *err) {
     return s_ok != 0;
 }
 
+// flags: [0] commit in batch, [1] commit in round, [2] batches, [3] active count,
+//        [4..5] barrier, [6] error, [7] next active count
 __global__ void coloring_kernel(ColorDev c, Bar bar, int *err, int max_batches) {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nth = gridDim.x * blockDim.x;
-    const int XY = c.X * c.Y, X = c.X, Y = c.Y;
-    volatile int *flags = c.flags;  // [0] commit in batch, [1] commit in round, [2] batches
+    const int lane = threadIdx.x & 31;
+    const int gw = tid >> 5, nw = nth >> 5;
+    const int XY = c.X * c.Y;
+    volatile int *flags = c.flags;
+    int *act = c.active, *act2 = c.active2;
+    for (int i = tid; i < c.n; i += nth) act[i] = i;
+    if (tid == 0) flags[3] = c.n;
+    if (!grid_barrier(bar, err)) return;
     for (int cur = 0; cur < max_batches; cur++) {
+        const int na = flags[3];
         for (int i = tid; i < XY; i += nth) c.map[i] = -1;
-        for (int i = tid; i < c.n; i += nth) c.status[i] = 0;
-        if (tid == 0) flags[0] = 0;
+        for (int i = tid; i < na; i += nth) c.status[act[i]] = 0;
+        if (tid == 0) { flags[0] = 0; flags[7] = 0; }
         if (!grid_barrier(bar, err)) return;
         for (int round = 0; round < 30; round++) {
             if (tid == 0) flags[1] = 0;
             // claim
-            for (int k = tid; k < c.n; k += nth) {
-                if (c.status[k] == 2 || c.batch[k] != -1) continue;
-                c.status[k] = 1;
+            for (int w = gw; w < na; w += nw) {
+                const int k = act[w];
+                if (c.status[k] == 2) continue;
+                if (lane == 0) c.status[k] = 1;
                 const int sh = c.perm ? c.perm[k] : k;
-                for (int i = c.pt_off[sh]; i < c.pt_off[sh + 1]; i++) {
-                    const int p = c.pts[i], x = p / Y, y = p % Y;
-                    const int dx[4] = {0, 0, -1, 1}, dy[4] = {0, -1, 0, 0};
-                    for (int j = 0; j < 4; j++) {
-                        const int nx = x + dx[j], ny = y + dy[j];
-                        if (nx >= 0 && nx < X && ny >= 0 && ny < Y) atomicMax(&c.map[nx * Y + ny], k);
-                    }
-                }
-                for (int i = c.h_off[sh]; i < c.h_off[sh + 1]; i++) {
-                    const int s = c.hseg[2 * i], e = c.hseg[2 * i + 1];
-                    const int y = s % Y;
-                    for (int x = s / Y; x <= e / Y; x += c.sparsity) atomicMax(&c.map[x * Y + y], k);
-                }
-                for (int i = c.v_off[sh]; i < c.v_off[sh + 1]; i++) {
-                    const int s = c.vseg[2 * i], e = c.vseg[2 * i + 1];
-                    const int x = s / Y;
-                    for (int y = s % Y; y <= e % Y; y += c.sparsity) atomicMax(&c.map[x * Y + y], k);
-                }
+                for (int i = c.claim_off[sh] + lane; i < c.claim_off[sh + 1]; i += 32) atomicMax(&c.map[c.claim[i]], k);
             }
             if (!grid_barrier(bar, err)) return;
             // commit: owns every point
-            for (int k = tid; k < c.n; k += nth) {
-                if (c.status[k] == 2 || c.batch[k] != -1) continue;
-                bool ok = true;
+            for (int w = gw; w < na; w += nw) {
+                const int k = act[w];
+                if (c.status[k] != 1) continue;
                 const int sh = c.perm ? c.perm[k] : k;
-                for (int i = c.pt_off[sh]; i < c.pt_off[sh + 1] && ok; i++) ok = c.map[c.pts[i]] == k;
-                if (ok) {
+                bool ok = true;
+                for (int i = c.pt_off[sh] + lane; i < c.pt_off[sh + 1]; i += 32) ok &= c.map[c.pts[i]] == k;
+                ok = __all_sync(0xffffffffu, ok);
+                if (ok && lane == 0) {
                     c.batch[k] = cur;
                     flags[0] = 1;
                     flags[1] = 1;
@@ -113,19 +112,27 @@ __global__ void coloring_kernel(ColorDev c, Bar bar, int *err, int max_batches) 
             }
             if (!grid_barrier(bar, err)) return;
             if (!flags[1]) break;
-            // block nets whose points belong to a member of this batch
-            for (int i = tid; i < c.npts; i += nth) {
-                const int k = c.rank ? c.rank[c.pt_net[i]] : c.pt_net[i];
-                if (k < 0) continue;  // shape not in this colouring
+            // block candidates whose points belong to a member of this batch
+            for (int w = gw; w < na; w += nw) {
+                const int k = act[w];
                 if (c.status[k] != 1 || c.batch[k] != -1) continue;
-                const int pre = c.map[c.pts[i]];
-                if (pre != -1 && c.batch[pre] != -1 && c.status[k] != 2) c.status[k] = 2;
+                const int sh = c.perm ? c.perm[k] : k;
+                bool hit = false;
+                for (int i = c.pt_off[sh] + lane; i < c.pt_off[sh + 1]; i += 32) {
+                    const int pre = c.map[c.pts[i]];
+                    hit |= (pre != -1 && c.batch[pre] != -1);
+                }
+                hit = __any_sync(0xffffffffu, hit);
+                if (hit && lane == 0) c.status[k] = 2;
             }
             if (!grid_barrier(bar, err)) return;
-            // release the cells of blocked nets
-            for (int i = tid; i < XY; i += nth) {
-                const int k = c.map[i];
-                if (k >= 0 && c.status[k] == 2) c.map[i] = -1;
+            // blocked nets release the cells they own
+            for (int w = gw; w < na; w += nw) {
+                const int k = act[w];
+                if (c.status[k] != 2) continue;
+                const int sh = c.perm ? c.perm[k] : k;
+                for (int i = c.claim_off[sh] + lane; i < c.claim_off[sh + 1]; i += 32)
+                    if (c.map[c.claim[i]] == k) c.map[c.claim[i]] = -1;
             }
             if (!grid_barrier(bar, err)) return;
         }
@@ -133,23 +140,60 @@ __global__ void coloring_kernel(ColorDev c, Bar bar, int *err, int max_batches) 
             if (tid == 0) flags[2] = cur;
             return;
         }
+        // nets still without a batch stay active (their order in the list does not matter)
+        for (int i = tid; i < na; i += nth) {
+            const int k = act[i];
+            if (c.batch[k] == -1) act2[atomicAdd((int *)&flags[7], 1)] = k;
+        }
         if (!grid_barrier(bar, err)) return;
+        if (tid == 0) flags[3] = flags[7];
+        int *t = act; act = act2; act2 = t;
+        if (!grid_barrier(bar, err)) return;
+        if (flags[3] == 0) {
+            if (tid == 0) flags[2] = cur + 1;
+            return;
+        }
     }
     if (tid == 0) flags[2] = max_batches;
 }
 
 }  // namespace
 
+void build_claims(int nshapes, const int *pt_off, const int *pts, const int *h_off, const int *hseg,
+                  const int *v_off, const int *vseg, int X, int Y, int sparsity, std::vector<int> &off,
+                  std::vector<int> &cells, int /*threads*/) {
+    static const int dx[4] = {0, 0, -1, 1}, dy[4] = {0, -1, 0, 0};
+    off.assign(nshapes + 1, 0);
+    cells.clear();
+    for (int k = 0; k < nshapes; k++) {
+        for (int i = pt_off[k]; i < pt_off[k + 1]; i++) {
+            const int x = pts[i] / Y, y = pts[i] % Y;
+            for (int j = 0; j < 4; j++) {
+                const int nx = x + dx[j], ny = y + dy[j];
+                if (nx >= 0 && nx < X && ny >= 0 && ny < Y) cells.push_back(nx * Y + ny);
+            }
+        }
+        for (int i = h_off[k]; i < h_off[k + 1]; i++) {
+            const int s = hseg[2 * i], e = hseg[2 * i + 1], y = s % Y;
+            for (int x = s / Y; x <= e / Y; x += sparsity) cells.push_back(x * Y + y);
+        }
+        for (int i = v_off[k]; i < v_off[k + 1]; i++) {
+            const int s = vseg[2 * i], e = vseg[2 * i + 1], x = s / Y;
+            for (int y = s % Y; y <= e % Y; y += sparsity) cells.push_back(x * Y + y);
+        }
+        off[k + 1] = (int)cells.size();
+    }
+}
+
 int run_coloring(ColorDev &c, int max_batch, cudaStream_t s) {
     (void)max_batch;
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int threads = 256;
+    const int threads = 512;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coloring_kernel, threads, 0);
-    int blocks = sms * (per < 4 ? per : 4);
+    int blocks = sms * (per < 2 ? per : 2);
     if (blocks < 1) blocks = 1;
-    // barrier words and error word live after the four flags
     Bar bar{reinterpret_cast<unsigned *>(c.flags + 4), reinterpret_cast<unsigned *>(c.flags + 5)};
     int *err = c.flags + 6;
     cudaMemsetAsync(c.flags, 0, 8 * sizeof(int), s);

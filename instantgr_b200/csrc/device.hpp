@@ -124,12 +124,20 @@ struct ColorDev {
     const int *pt_net = nullptr;                   // [points] owner shape
     const int *h_off = nullptr, *hseg = nullptr;   // [shapes+1], pairs
     const int *v_off = nullptr, *vseg = nullptr;
+    // cells claimed by each shape: 4-neighbourhood of its points, every
+    // `sparsity`-th cell of its segments (CSR over shapes)
+    const int *claim_off = nullptr, *claim = nullptr;
     int npts = 0;
     int *map = nullptr;       // [X*Y]
     int *batch = nullptr;     // [n]
     int *status = nullptr;    // [n]
-    int *flags = nullptr;     // [4] device flags
+    int *active = nullptr, *active2 = nullptr;  // [n] each
+    int *flags = nullptr;     // [8] device flags
 };
+// Claim lists of shapes (pt_off/pts/h_off/hseg/v_off/vseg as in ColorDev).
+void build_claims(int nshapes, const int *pt_off, const int *pts, const int *h_off, const int *hseg,
+                  const int *v_off, const int *vseg, int X, int Y, int sparsity, std::vector<int> &off,
+                  std::vector<int> &cells, int threads);
 int run_coloring(ColorDev &c, int max_batch, cudaStream_t s);  // returns #batches (host loop)
 
 std::string cuda_error_string(cudaError_t e);

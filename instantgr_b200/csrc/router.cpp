@@ -113,12 +113,19 @@ void KernelTimer::reset() {
     for (int k = 0; k < KC_N; k++) { ms[k] = 0; launches[k] = 0; }
 }
 
-void ShapeDev::upload(const ShapeSet &sh, cudaStream_t st) {
+void ShapeDev::upload(const ShapeSet &sh, int X, int Y, int sp, cudaStream_t st) {
     pt_off.upload(sh.pt_off, st); pts.upload(sh.pts, st); pt_net.upload(sh.pt_net, st);
     h_off.upload(sh.h_off, st); hseg.upload(sh.hseg, st);
     v_off.upload(sh.v_off, st); vseg.upload(sh.vseg, st);
     npts = (int)sh.pts.size();
     nshapes = (int)sh.pt_off.size() - 1;
+    sparsity = sp;
+    std::vector<int> co, cl;
+    build_claims(nshapes, sh.pt_off.data(), sh.pts.data(), sh.h_off.data(), sh.hseg.data(), sh.v_off.data(),
+                 sh.vseg.data(), X, Y, sp, co, cl, 0);
+    claim_off.upload(co, st);
+    claim.upload(cl, st);
+    cuda_check(cudaStreamSynchronize(st), "claims");  // host vectors go out of scope
 }
 
 // ------------------------------------------------------------------ router
@@ -192,7 +199,7 @@ void Router::ensure_device() {
         for (auto &sg : r.vseg) { sh.vseg.push_back(sg.first); sh.vseg.push_back(sg.second); }
         sh.v_off.push_back((int)(sh.vseg.size() / 2));
     }
-    d_shapes1.upload(sh, s);
+    d_shapes1.upload(sh, X, Y, 15, s);  // phase 1 samples every 15th segment cell (database_cuda.hpp:439)
     std::vector<int> ids(R);
     std::iota(ids.begin(), ids.end(), 0);
     d_all_ids.upload(ids, s);
@@ -334,13 +341,17 @@ void Router::color_nets(const std::vector<int> &order, const ShapeDev &shapes, i
     d_map.alloc((size_t)ns.X * ns.Y);
     d_bat.alloc(n);
     d_sta.alloc(n);
+    d_act.alloc(2 * (size_t)n);
     d_flags.alloc(8);
     st.h2d_bytes += (int64_t)(n + nshapes) * 4;
+    if (sparsity != shapes.sparsity) throw Error(ERR_STATE, "claim lists were built for another sparsity");
     ColorDev cd;
     cd.n = n; cd.X = ns.X; cd.Y = ns.Y; cd.sparsity = sparsity;
     cd.perm = d_perm.p; cd.rank = d_rank.p;
     cd.pt_off = shapes.pt_off.p; cd.pts = shapes.pts.p; cd.pt_net = shapes.pt_net.p;
     cd.h_off = shapes.h_off.p; cd.hseg = shapes.hseg.p; cd.v_off = shapes.v_off.p; cd.vseg = shapes.vseg.p;
+    cd.claim_off = shapes.claim_off.p; cd.claim = shapes.claim.p;
+    cd.active = d_act.p; cd.active2 = d_act.p + n;
     cd.npts = shapes.npts; cd.map = d_map.p; cd.batch = d_bat.p; cd.status = d_sta.p; cd.flags = d_flags.p;
     kt.begin(KC_COLOR);
     int nb = run_coloring(cd, 0, s);
@@ -434,7 +445,7 @@ bool Router::rrr_pass(int iter) {
         sh.v_off.push_back((int)(sh.vseg.size() / 2));
     }
     ShapeDev shd;
-    shd.upload(sh, s);
+    shd.upload(sh, X, Y, mode_eff >= 1 ? 2 : 15, s);
     st.h2d_bytes += (int64_t)(sh.pts.size() * 2 + sh.hseg.size() + sh.vseg.size() + 3 * of_nets.size()) * 4;
     std::vector<int> local(of_nets.size());
     std::iota(local.begin(), local.end(), 0);  // shape k belongs to of_nets[k]; of_nets is in priority order

@@ -86,9 +86,9 @@ struct ShapeSet {
     std::vector<int> pt_off{0}, pts, pt_net, h_off{0}, hseg, v_off{0}, vseg;
 };
 struct ShapeDev {
-    DevBuf<int> pt_off, pts, pt_net, h_off, hseg, v_off, vseg;
-    int npts = 0, nshapes = 0;
-    void upload(const ShapeSet &s, cudaStream_t st);
+    DevBuf<int> pt_off, pts, pt_net, h_off, hseg, v_off, vseg, claim_off, claim;
+    int npts = 0, nshapes = 0, sparsity = 0;
+    void upload(const ShapeSet &s, int X, int Y, int sparsity, cudaStream_t st);
 };
 
 struct Router {
@@ -122,7 +122,7 @@ struct Router {
     std::vector<int> h_routes;  // host copy, made on demand
     bool h_routes_valid = false;
     // ---- per-run device buffers (grow-only)
-    DevBuf<int> d_ids, d_all_ids, of_sum, d_perm, d_rank, d_map, d_bat, d_sta, d_flags;
+    DevBuf<int> d_ids, d_all_ids, of_sum, d_perm, d_rank, d_map, d_bat, d_sta, d_act, d_flags;
     DevBuf<uint8_t> d_is_of;
     DevBuf<float> d_xsum, d_ysum;
     DevBuf<unsigned> d_bar;
