@@ -134,8 +134,9 @@ int igr_router_plan(igr_router *h, int64_t *sizes, int32_t *net_ids, int32_t *ba
                     int32_t *nodes, int32_t *par, int32_t *route_cap) {
     if (!h || !sizes) return fail(nullptr, IGR_ERR_INVALID, "null argument");
     return guard(&h->err, [&] {
-        const auto &r = h->r;
-        if (r.plan_node_off.empty()) throw Error(ERR_STATE, "route before reading the plan");
+        auto &r = h->r;
+        if (!r.ran) throw Error(ERR_STATE, "route before reading the plan");
+        r.build_plan();
         sizes[0] = (int64_t)r.plan_ids.size();
         sizes[1] = (int64_t)r.plan_batch_off.size() - 1;
         sizes[2] = (int64_t)r.plan_nodes.size();
@@ -437,6 +438,10 @@ int igr_pattern_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t 
         c->scr.alloc((size_t)pattern_scratch_doubles(sn));
         c->routes.upload(routes_out, (size_t)ext, c->s);
         TreeBatchDev tb{c->a.p, c->b.p, c->d.p, c->e.p, c->off.p, c->f.p, c->routes.p, c->scr.p, d_so.p, sn, n};
+        c->h.alloc(1);
+        cuda_check(cudaMemsetAsync(c->h.p, 0, sizeof(int), c->s), "memset");
+        tb.queue = c->h.p;
+        tb.tile = kPatternNodeTile;
         launch_pattern_route(g, tb, stamp, c->s);
         cuda_check(cudaMemcpyAsync(routes_out, c->routes.p, ext * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
         sync_check(c);

@@ -90,7 +90,7 @@ __global__ void coloring_kernel(ColorDev c, Bar bar, int *err, int max_batches) 
             // claim
             for (int w = gw; w < na; w += nw) {
                 const int k = act[w];
-                if (c.status[k] == 2) continue;
+                if (c.status[k] == 2 || c.batch[k] != -1) continue;  // blocked, or already a member
                 if (lane == 0) c.status[k] = 1;
                 const int sh = c.perm ? c.perm[k] : k;
                 for (int i = c.claim_off[sh] + lane; i < c.claim_off[sh + 1]; i += 32) atomicMax(&c.map[c.claim[i]], k);
@@ -99,7 +99,7 @@ __global__ void coloring_kernel(ColorDev c, Bar bar, int *err, int max_batches) 
             // commit: owns every point
             for (int w = gw; w < na; w += nw) {
                 const int k = act[w];
-                if (c.status[k] != 1) continue;
+                if (c.status[k] != 1 || c.batch[k] != -1) continue;
                 const int sh = c.perm ? c.perm[k] : k;
                 bool ok = true;
                 for (int i = c.pt_off[sh] + lane; i < c.pt_off[sh + 1]; i += 32) ok &= c.map[c.pts[i]] == k;

@@ -55,12 +55,16 @@ struct TreeBatchDev {
     int *routes;             // route records
     double *scratch;         // per-node DP tables of nets larger than the shared-memory tile
     const int64_t *scratch_off;  // [routing nets] offset (in nodes) into scratch, -1 for nets that fit on chip
-    int64_t scratch_nodes;   // nodes covered by scratch: 45 doubles each, then 46 ints each
+    int64_t scratch_nodes;   // nodes covered by scratch: 81 doubles each, then 46 ints each
     int n;
+    const int *order = nullptr;  // [n] positions into net_ids in processing order (null: 0..n-1)
+    int *queue = nullptr;        // work counter of this launch (zero before the launch)
+    int lanes_per_net = 32;      // 16 or 32
+    int tile = 16;               // nodes kept on chip: 6, 16, or 1 (all in scratch)
 };
-// doubles of scratch needed for `nodes` oversize-net nodes
-inline int64_t pattern_scratch_doubles(int64_t nodes) { return nodes * 45 + (nodes * 46 + 1) / 2; }
-constexpr int kPatternNodeTile = 20;  // nets with more nodes use global scratch
+// doubles of scratch needed for `nodes` nodes of nets kept in global memory
+inline int64_t pattern_scratch_doubles(int64_t nodes) { return nodes * 81 + (nodes * 46 + 1) / 2; }
+constexpr int kPatternNodeTile = 16;  // nets with more nodes use global scratch
 void launch_pattern_route(const GridDev &g, const TreeBatchDev &b, int stamp, cudaStream_t s);
 
 struct ViaBatchDev {

@@ -4,31 +4,43 @@
 //
 // Restates Lshape_route_cuda (src/Lshape_route.hpp:9-153).  The reference runs
 // one thread per net with 81-entry f64 tables per node in global memory (928
-// bytes of stack per thread).  Here one warp owns a net: the 45 valid
-// layer-range entries of every node live in shared memory (global scratch for
-// nets with more than kNodeTile nodes), and the lanes of the warp work on the
-// nine layers, the nine layer ranges and the 4-5 bend layers of one tree edge
-// at a time.  All f64 sums are formed in the reference's order and every
-// comparison keeps its strict/non-strict tie rule, so for the same cost map
-// the chosen layers, routes and demand are bit-identical to the reference's.
+// bytes of stack per thread), and every tree edge waits on its own gathers.
+// Here a group of G lanes (G = 16 or 32) owns a net:
+//   1. every cost the net needs that depends only on geometry (via-stack
+//      columns of its nodes, the wire cost of each leg on each layer, the via
+//      columns at both corners of each bent edge) is gathered up front, all
+//      lanes in parallel, into shared memory;
+//   2. the edges are then processed bottom-up from shared memory only: the
+//      lanes work on the nine layers, the nine target layers of a bend (each
+//      looping over the 4-5 bend layers of opposite parity in the reference's
+//      order), the nine range rows (with the reference's <= rule) and the
+//      accumulation into the parent (in the reference's order of additions);
+//   3. one lane walks the nodes in preorder, emits the route record and writes
+//      the difference array.
+// Nets are taken from a per-batch queue in the order given (largest first),
+// so the long nets of a batch start early.  The 45 valid layer ranges of a
+// node live in shared memory (global scratch for nets of more than kNodeTile
+// nodes).  For the same cost map the chosen layers, routes and demand are
+// bit-identical to the reference's.
 #include "kcommon.cuh"
 
 namespace igr {
 
 namespace {
 
-constexpr int kL = kRouteL;         // 9 routing layers
-constexpr int kR = 45;              // layer ranges minl <= maxl
-constexpr int kNodeTile = kPatternNodeTile;  // nodes kept on chip per warp
-constexpr int kWarps = 4;           // warps per CTA
+constexpr int kL = kRouteL;                  // 9 routing layers
+constexpr int kR = 45;                       // layer ranges minl <= maxl
+constexpr int kPF = 36;                      // prefetched doubles per edge
 
 __host__ __device__ constexpr int tri(int a, int b) { return a * 9 - a * (a - 1) / 2 + (b - a); }
 
-struct WarpSmem {
-    double dist[kNodeTile * kR];
-    int from[kNodeTile * kR];
-    int lr[kNodeTile];
-    double costc[kL], vA[kL], vB[kL], diag[kL];
+template <int T>
+struct GroupSmem {
+    double dist[T * kR];
+    double pf[(T > 1 ? T - 1 : 1) * kPF];
+    int from[T * kR];
+    int lr[T];
+    double costc[kL], diag[kL];
     int cf[kL], pdiag[kL];
 };
 
@@ -52,9 +64,12 @@ __device__ __forceinline__ void add_wire(const GridDev &g, const int *layer_firs
     g.dirty_commit[track_of(g, l, xa, ya, layer_first)] = 1;
 }
 
-__global__ void __launch_bounds__(kWarps * 32) pattern_route_kernel(GridDev g, TreeBatchDev b, int stamp) {
+template <int G, int T>
+__global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatchDev b, int stamp) {
     extern __shared__ unsigned char smem_raw[];
-    WarpSmem &sm = reinterpret_cast<WarpSmem *>(smem_raw)[threadIdx.x >> 5];
+    constexpr int kGroups = 128 / G;
+    constexpr int kNodeTile = T;
+    GroupSmem<T> &sm = reinterpret_cast<GroupSmem<T> *>(smem_raw)[threadIdx.x / G];
     __shared__ int layer_first[kL + 1];
     if (threadIdx.x == 0) {
         int f = 0;
@@ -62,31 +77,40 @@ __global__ void __launch_bounds__(kWarps * 32) pattern_route_kernel(GridDev g, T
         layer_first[g.L] = f;
     }
     __syncthreads();
+    (void)kGroups;
     const int lane = threadIdx.x & 31;
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int gl = lane & (G - 1);                 // lane within the group
+    const int g0 = lane & ~(G - 1);                // first lane of the group
+    const unsigned gmask = G == 32 ? 0xffffffffu : (0xffffu << g0);
     const int X = g.X, Y = g.Y, XY = X * Y;
 
-    for (int k = gw; k < b.n; k += nw) {
-        const int net = b.net_ids[k];
+    while (true) {
+        int k = 0;
+        if (gl == 0) k = atomicAdd(b.queue, 1);
+        k = __shfl_sync(gmask, k, g0);
+        if (k >= b.n) break;
+        const int net = b.net_ids[b.order ? b.order[k] : k];
         const int nb = b.node_off[net];
         const int n = b.node_off[net + 1] - nb;
         const int *nodes = b.nodes + nb;
         const int *par = b.par + nb;
-        double *dist;
+        double *dist, *pf;
         int *from, *lr;
         if (n <= kNodeTile) {
-            dist = sm.dist; from = sm.from; lr = sm.lr;
+            dist = sm.dist; pf = sm.pf; from = sm.from; lr = sm.lr;
         } else {
             const int64_t so = b.scratch_off[net];
-            if (so < 0) { set_error(g.err, ERR_STATE); continue; }
-            if (so + n > b.scratch_nodes) { set_error(g.err, ERR_CAPACITY); continue; }
-            dist = b.scratch + so * kR;
-            from = reinterpret_cast<int *>(b.scratch + b.scratch_nodes * kR) + so * (kR + 1);
+            if (so < 0 || so + n > b.scratch_nodes) {
+                if (gl == 0) set_error(g.err, so < 0 ? ERR_STATE : ERR_CAPACITY);
+                continue;
+            }
+            dist = b.scratch + so * (kR + kPF);
+            pf = dist + (int64_t)n * kR;
+            from = reinterpret_cast<int *>(b.scratch + b.scratch_nodes * (kR + kPF)) + so * (kR + 1);
             lr = from + (int64_t)n * kR;
         }
-        // ---- 1. via-stack cost of every node and layer range (Lshape_route.hpp:22-32)
-        for (int p = lane; p < n * kL; p += 32) {
+        // ---- 1a. via-stack cost of every node and layer range (Lshape_route.hpp:22-32)
+        for (int p = gl; p < n * kL; p += G) {
             const int i = p / kL, mn = p % kL;
             const int v = nodes[i];
             const int l = v / XY, x = v / Y % X, y = v % Y;
@@ -97,65 +121,88 @@ __global__ void __launch_bounds__(kWarps * 32) pattern_route_kernel(GridDev g, T
                 dist[i * kR + tri(mn, mx)] = (l < kL && (mn > l || mx < l)) ? kInf : acc;
             }
         }
-        __syncwarp();
-        // ---- 2. bottom-up over tree edges (Lshape_route.hpp:33-97)
-        for (int i = n - 1; i >= 1; i--) {
+        // ---- 1b. geometry-only costs of every edge: [0,9) child leg (bent) or wire
+        //          (straight) per layer, [9,18) parent leg, [18,27) via column at (x, py),
+        //          [27,36) via column at (px, y)
+        for (int t = gl; t < (n - 1) * kPF; t += G) {
+            const int e = t / kPF, j = t % kPF, i = e + 1;
             const int pi = par[i];
-            if (pi < 0 || pi >= i) { set_error(g.err, ERR_STATE); break; }
+            if (pi < 0 || pi >= i) continue;  // reported below
             const int v = nodes[i], pv = nodes[pi];
             const int x = v / Y % X, y = v % Y, px = pv / Y % X, py = pv % Y;
             const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
+            const bool straight = (x == px || y == py);
+            double val = 0;
+            if (j < kL) {
+                const int l = j;
+                if (straight) {
+                    const int dl = layer_dir(g, l);
+                    if (!((dl == 0 && y != py) || (dl == 1 && x != px))) val = wire_cost(g, l, minx, maxx, miny, maxy);
+                } else {
+                    val = layer_dir(g, l) ? wire_cost(g, l, x, x, miny, maxy) : wire_cost(g, l, minx, maxx, y, y);
+                }
+            } else if (!straight) {
+                if (j < 2 * kL) {
+                    const int l = j - kL;
+                    val = layer_dir(g, l) ? wire_cost(g, l, px, px, miny, maxy) : wire_cost(g, l, minx, maxx, py, py);
+                } else if (j < 3 * kL) {
+                    val = (double)g.vcost[cell_at(g, j - 2 * kL, x, py)];
+                } else {
+                    val = (double)g.vcost[cell_at(g, j - 3 * kL, px, y)];
+                }
+            }
+            pf[t] = val;
+        }
+        __syncwarp(gmask);
+        // ---- 2. bottom-up over tree edges (Lshape_route.hpp:33-97)
+        bool bad = false;
+        for (int i = n - 1; i >= 1; i--) {
+            const int pi = par[i];
+            if (pi < 0 || pi >= i) { bad = true; break; }
+            const int v = nodes[i], pv = nodes[pi];
+            const int x = v / Y % X, y = v % Y, px = pv / Y % X, py = pv % Y;
             const double *nd = dist + i * kR;
             double *pd = dist + pi * kR;
             int *prev = from + i * kR;
+            const double *pe = pf + (i - 1) * kPF;
             // (a) cheapest range containing each layer
             double mcc = kInf;
             int cf = 0;
-            if (lane < kL) {
-                for (int mn = 0; mn <= lane; mn++)
-                    for (int mx = lane; mx < kL; mx++) {
+            if (gl < kL) {
+                for (int mn = 0; mn <= gl; mn++)
+                    for (int mx = gl; mx < kL; mx++) {
                         const double c = nd[tri(mn, mx)];
                         if (c < mcc) { mcc = c; cf = mn * kL + mx; }
                     }
             }
-            const bool straight = (x == px || y == py);
-            if (straight) {
-                if (lane < kL) {
+            if (x == px || y == py) {
+                if (gl < kL) {
                     double d = kInf;
                     int pp = 0;
-                    const int dl = layer_dir(g, lane);
+                    const int dl = layer_dir(g, gl);
                     if (!((dl == 0 && y != py) || (dl == 1 && x != px))) {
-                        d = mcc + wire_cost(g, lane, minx, maxx, miny, maxy);
-                        pp = cf * kL * kL + lane * kL + lane;
+                        d = mcc + pe[gl];
+                        pp = cf * kL * kL + gl * kL + gl;
                     }
-                    sm.diag[lane] = d;
-                    sm.pdiag[lane] = pp;
+                    sm.diag[gl] = d;
+                    sm.pdiag[gl] = pp;
                 }
             } else {
-                if (lane < kL) {
-                    const int c = lane;
+                if (gl < kL) {
                     double cost = mcc;
-                    if (layer_dir(g, c)) cost += wire_cost(g, c, x, x, miny, maxy);
-                    else cost += wire_cost(g, c, minx, maxx, y, y);
-                    sm.costc[c] = cost;
-                    sm.cf[c] = cf;
-                    sm.vA[lane] = (double)g.vcost[cell_at(g, lane, x, py)];
-                } else if (lane < 2 * kL) {
-                    sm.vB[lane - kL] = (double)g.vcost[cell_at(g, lane - kL, px, y)];
+                    cost += pe[gl];
+                    sm.costc[gl] = cost;
+                    sm.cf[gl] = cf;
                 }
-                double legp = 0;
-                if (lane < kL) {
-                    if (layer_dir(g, lane)) legp = wire_cost(g, lane, px, px, miny, maxy);
-                    else legp = wire_cost(g, lane, minx, maxx, py, py);
-                }
-                __syncwarp();
-                if (lane < kL) {
-                    const int p = lane;
+                __syncwarp(gmask);
+                if (gl < kL) {
+                    const int p = gl;
+                    const double legp = pe[kL + p];
                     double best = kInf;
                     int bp = 0;
                     for (int c = (p & 1) ^ 1; c < kL; c += 2) {
                         const int lo = min(c, p), hi = max(c, p);
-                        const double *vc = layer_dir(g, c) ? sm.vA : sm.vB;
+                        const double *vc = layer_dir(g, c) ? pe + 2 * kL : pe + 3 * kL;
                         double cost2 = 0;
                         for (int l = lo + 1; l < hi; l++) cost2 += vc[l];
                         cost2 += legp;
@@ -166,10 +213,10 @@ __global__ void __launch_bounds__(kWarps * 32) pattern_route_kernel(GridDev g, T
                     sm.pdiag[p] = bp;
                 }
             }
-            __syncwarp();
+            __syncwarp(gmask);
             // (b) range minimum with the reference's <= rule, then accumulate into the parent
-            if (lane < kL) {
-                const int mn = lane;
+            if (gl < kL) {
+                const int mn = gl;
                 double row = sm.diag[mn];
                 int rp = sm.pdiag[mn];
                 prev[tri(mn, mn)] = rp;
@@ -181,38 +228,44 @@ __global__ void __launch_bounds__(kWarps * 32) pattern_route_kernel(GridDev g, T
                     pd[tri(mn, mx)] += row;
                 }
             }
-            __syncwarp();
+            __syncwarp(gmask);
+        }
+        if (bad) {
+            if (gl == 0) set_error(g.err, ERR_STATE);
+            __syncwarp(gmask);
+            continue;
         }
         // ---- 3. root range: first minimum in (minl, maxl) order (Lshape_route.hpp:99-105)
         double bv = __longlong_as_double(0x7ff0000000000000LL);  // +infinity
         int bi = 1 << 30;
-        for (int t = lane; t < kR; t += 32) {
+        for (int t = gl; t < kR; t += G) {
             const double c = dist[t];
             if (c < bv || (c == bv && t < bi)) { bv = c; bi = t; }
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ov = __shfl_down_sync(0xffffffffu, bv, o);
-            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        for (int o = G / 2; o > 0; o >>= 1) {
+            const double ov = __shfl_down_sync(gmask, bv, o, G);
+            const int oi = __shfl_down_sync(gmask, bi, o, G);
             if (ov < bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
         }
         // ---- 4. backtrace, route emission and demand (Lshape_route.hpp:99-152)
-        if (lane == 0) {
+        if (gl == 0) {
             int *r = b.routes + b.route_off[net];
             const int cap = b.route_cap[net];
             int cnt = 1;
             bool ok = true;
-            auto emit = [&](int a, int c) {
-                if (cnt + 2 > cap) { ok = false; return; }
-                r[cnt++] = a;
-                r[cnt++] = c;
-            };
             // root range as (minl, maxl)
             int rmn = 0, rmx = 0;
             for (int a = 0, t = 0; a < kL; a++)
                 for (int c = a; c < kL; c++, t++)
                     if (t == bi) { rmn = a; rmx = c; }
             lr[0] = rmn * kL + rmx;
+#define EMIT(A, B)                                         \
+    do {                                                   \
+        if (!ok || cnt + 2 > cap) { ok = false; break; }   \
+        r[cnt++] = (A);                                    \
+        r[cnt++] = (B);                                    \
+    } while (0)
             for (int i = 0; i < n && ok; i++) {
                 const int v = nodes[i];
                 const int x = v / Y % X, y = v % Y;
@@ -224,49 +277,71 @@ __global__ void __launch_bounds__(kWarps * 32) pattern_route_kernel(GridDev g, T
                 }
                 const int mn = lr[i] / kL, mx = lr[i] % kL;
                 if (mn > mx || !(dist[i * kR + tri(mn, mx)] < kInf)) { set_error(g.err, ERR_STATE); ok = false; break; }
-                if (mn < mx) emit(mn * XY + x * Y + y, mx * XY + x * Y + y);
-                if (i == 0) continue;
+                if (mn < mx) EMIT(mn * XY + x * Y + y, mx * XY + x * Y + y);
+                if (!ok || i == 0) continue;
                 const int pv = nodes[par[i]];
                 const int px = pv / Y % X, py = pv % Y;
                 const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
                 const int curl = code / kL % kL, parl = code % kL;
                 if (px == x || py == y) {
-                    emit(curl * XY + minx * Y + miny, curl * XY + maxx * Y + maxy);
-                    add_wire(g, layer_first, curl, minx, maxx, miny, maxy, stamp);
+                    EMIT(curl * XY + minx * Y + miny, curl * XY + maxx * Y + maxy);
+                    if (ok) add_wire(g, layer_first, curl, minx, maxx, miny, maxy, stamp);
                 } else if (layer_dir(g, curl)) {
-                    emit(curl * XY + x * Y + y, curl * XY + x * Y + py);
-                    add_wire(g, layer_first, curl, x, x, miny, maxy, stamp);
-                    emit(curl * XY + x * Y + py, parl * XY + x * Y + py);
-                    emit(parl * XY + x * Y + py, parl * XY + px * Y + py);
-                    add_wire(g, layer_first, parl, minx, maxx, py, py, stamp);
+                    EMIT(curl * XY + x * Y + y, curl * XY + x * Y + py);
+                    if (ok) add_wire(g, layer_first, curl, x, x, miny, maxy, stamp);
+                    EMIT(curl * XY + x * Y + py, parl * XY + x * Y + py);
+                    EMIT(parl * XY + x * Y + py, parl * XY + px * Y + py);
+                    if (ok) add_wire(g, layer_first, parl, minx, maxx, py, py, stamp);
                 } else {
-                    emit(curl * XY + x * Y + y, curl * XY + px * Y + y);
-                    add_wire(g, layer_first, curl, minx, maxx, y, y, stamp);
-                    emit(curl * XY + px * Y + y, parl * XY + px * Y + y);
-                    emit(parl * XY + px * Y + y, parl * XY + px * Y + py);
-                    add_wire(g, layer_first, parl, px, px, miny, maxy, stamp);
+                    EMIT(curl * XY + x * Y + y, curl * XY + px * Y + y);
+                    if (ok) add_wire(g, layer_first, curl, minx, maxx, y, y, stamp);
+                    EMIT(curl * XY + px * Y + y, parl * XY + px * Y + y);
+                    EMIT(parl * XY + px * Y + y, parl * XY + px * Y + py);
+                    if (ok) add_wire(g, layer_first, parl, px, px, miny, maxy, stamp);
                 }
             }
+#undef EMIT
             if (!ok) set_error(g.err, ERR_CAPACITY);
             r[0] = cnt;
         }
-        __syncwarp();
+        __syncwarp(gmask);
     }
+}
+
+template <int G, int T>
+void launch_g(const GridDev &g, const TreeBatchDev &b, int stamp, cudaStream_t s) {
+    constexpr int kThreads = 128;
+    const size_t smem = sizeof(GroupSmem<T>) * (kThreads / G);
+    static bool attr = false;
+    static int sms = 0, per = 0;
+    if (!attr) {
+        cudaFuncSetAttribute(pattern_route_kernel<G, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pattern_route_kernel<G, T>, kThreads, smem);
+        attr = true;
+    }
+    if (per < 1) per = 1;
+    const int groups_per_block = kThreads / G;
+    int blocks = (b.n + groups_per_block - 1) / groups_per_block;
+    if (blocks > sms * per) blocks = sms * per;
+    if (blocks < 1) blocks = 1;
+    pattern_route_kernel<G, T><<<blocks, kThreads, smem, s>>>(g, b, stamp);
 }
 
 }  // namespace
 
+// Tile sizes (nodes kept on chip per group) compiled in: 6 (two- and three-pin
+// nets), 16, and 1 (every net in global scratch).
 void launch_pattern_route(const GridDev &g, const TreeBatchDev &b, int stamp, cudaStream_t s) {
     if (b.n <= 0) return;
-    const size_t smem = sizeof(WarpSmem) * kWarps;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(pattern_route_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
+    const bool half = b.lanes_per_net == 16;
+    switch (b.tile) {
+        case 6: half ? launch_g<16, 6>(g, b, stamp, s) : launch_g<32, 6>(g, b, stamp, s); break;
+        case 1: half ? launch_g<16, 1>(g, b, stamp, s) : launch_g<32, 1>(g, b, stamp, s); break;
+        default: half ? launch_g<16, 16>(g, b, stamp, s) : launch_g<32, 16>(g, b, stamp, s); break;
     }
-    int blocks = (b.n + kWarps - 1) / kWarps;
-    if (blocks > 148 * 8) blocks = 148 * 8;
-    pattern_route_kernel<<<blocks, kWarps * 32, smem, s>>>(g, b, stamp);
 }
 
 }  // namespace igr

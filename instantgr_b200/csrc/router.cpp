@@ -164,6 +164,11 @@ void Router::open(const char *cap, const char *net) {
     }
     route_off1 = route_off;
     route_cap1 = route_cap;
+    // phase-1 routing priority: HPWL, largest first (Lshape_route.hpp:170-172),
+    // with the reference's (unstable) std::sort and comparator
+    order1.resize(R);
+    std::iota(order1.begin(), order1.end(), 0);
+    std::sort(order1.begin(), order1.end(), [&](int l, int r) { return ns.nets[l].hpwl > ns.nets[r].hpwl; });
     if (verbose) std::fprintf(stderr, "[igr] read+trees %.2fs: %d nets, %d routing nets\n", now_s() - t0,
                               d.num_nets(), R);
 }
@@ -262,23 +267,35 @@ void Router::fetch_routes() {
 // Phase 1 (Lshape_route.hpp:155-257)
 void Router::phase1() {
     const int R = (int)ns.nets.size();
-    std::vector<int> order(R);
-    std::iota(order.begin(), order.end(), 0);
-    std::sort(order.begin(), order.end(), [&](int l, int r) { return ns.nets[l].hpwl > ns.nets[r].hpwl; });
     std::vector<std::vector<int>> batches;
-    color_nets(order, d_shapes1, 15, batches);
+    color_nets(order1, d_shapes1, 15, batches);
     std::reverse(batches.begin(), batches.end());
     st.batches1 = (int)batches.size();
-    std::vector<int> net_ids, batch_off{0};
+    // Size classes inside each batch (results do not depend on the order of nets
+    // within a batch): large nets (global scratch) first, then medium, then small,
+    // each by node count, largest first.
+    std::vector<int> net_ids, batch_off{0}, class_off;
     net_ids.reserve(R);
+    auto nodes_of = [&](int id) { return tree_off[id + 1] - tree_off[id]; };
     for (auto &b : batches) {
-        net_ids.insert(net_ids.end(), b.begin(), b.end());
+        std::vector<int> cls[3];
+        for (int id : b) {
+            const int m = nodes_of(id);
+            cls[m > kPatternNodeTile ? 0 : (m > tune.split ? 1 : 2)].push_back(id);
+        }
+        for (int c = 0; c < 3; c++) {
+            std::stable_sort(cls[c].begin(), cls[c].end(), [&](int a, int bb) { return nodes_of(a) > nodes_of(bb); });
+            class_off.push_back((int)net_ids.size());
+            net_ids.insert(net_ids.end(), cls[c].begin(), cls[c].end());
+        }
         batch_off.push_back((int)net_ids.size());
     }
     grow_routes(route_end);
     d_ids.upload(net_ids, s);
     d_route_off.upload(route_off, s);
     d_route_cap.upload(route_cap, s);
+    d_queue.alloc(3 * batches.size() + 1);
+    cuda_check(cudaMemsetAsync(d_queue.p, 0, (3 * batches.size() + 1) * sizeof(int), s), "memset");
     st.h2d_bytes += (int64_t)net_ids.size() * 4 + (int64_t)R * 12;
     cuda_check(cudaEventRecord(ev0, s), "event");
     for (size_t bi = 0; bi + 1 < batch_off.size(); bi++) {
@@ -287,10 +304,19 @@ void Router::phase1() {
         kt.begin(KC_COST);
         launch_cost_refresh(go.g, true, s);
         kt.end(KC_COST);
-        TreeBatchDev tb{d_ids.p + off, d_tree_off.p, d_tree_nodes.p, d_tree_par.p, d_route_off.p, d_route_cap.p,
-                        routes.p, d_scratch.p, d_scratch_off.p, scratch_nodes, n};
         kt.begin(KC_PATTERN);
-        launch_pattern_route(go.g, tb, stamp, s);
+        for (int c = 0; c < 3; c++) {
+            const int a = class_off[3 * bi + c];
+            const int e = c < 2 ? class_off[3 * bi + c + 1] : batch_off[bi + 1];
+            if (e <= a) continue;
+            TreeBatchDev tb{d_ids.p + a, d_tree_off.p, d_tree_nodes.p, d_tree_par.p, d_route_off.p, d_route_cap.p,
+                            routes.p, d_scratch.p, d_scratch_off.p, scratch_nodes, e - a};
+            tb.queue = d_queue.p + 3 * bi + c;
+            tb.tile = c == 0 ? 1 : (c == 1 ? kPatternNodeTile : 6);
+            tb.lanes_per_net = tune.lanes[c];
+            launch_pattern_route(go.g, tb, stamp, s);
+            st.launches += 1;
+        }
         kt.end(KC_PATTERN);
         kt.begin(KC_WIRE_COMMIT);
         launch_wire_commit(go.g, stamp, true, s);
@@ -299,30 +325,37 @@ void Router::phase1() {
         kt.begin(KC_VIA_COMMIT);
         launch_via_commit(go.g, vb, stamp, 1, s);
         kt.end(KC_VIA_COMMIT);
-        st.launches += 4;
+        st.launches += 3;
     }
     cuda_check(cudaEventRecord(ev1, s), "event");
     cuda_check(cudaGetLastError(), "phase-1 launch");
     // plan of this run, in routing order (for igr_router_plan)
-    plan_ids = net_ids;
-    plan_batch_off = batch_off;
-    plan_node_off.assign(1, 0);
-    plan_nodes.clear();
-    plan_par.clear();
-    plan_cap.resize(net_ids.size());
-    for (size_t k = 0; k < net_ids.size(); k++) {
-        const int id = net_ids[k];
-        plan_nodes.insert(plan_nodes.end(), tree_nodes.begin() + tree_off[id], tree_nodes.begin() + tree_off[id + 1]);
-        plan_par.insert(plan_par.end(), tree_par.begin() + tree_off[id], tree_par.begin() + tree_off[id + 1]);
-        plan_node_off.push_back((int)plan_nodes.size());
-        plan_cap[k] = route_cap[id];
-    }
+    plan_ids.swap(net_ids);
+    plan_batch_off.swap(batch_off);
+    plan_built = false;
     cuda_check(cudaEventSynchronize(ev1), "phase 1");
     float ms = 0;
     cudaEventElapsedTime(&ms, ev0, ev1);
     st.p1_ms = ms;
     if (int e = go.check_error(s)) throw Error(e, "device error in phase 1");
     if (verbose) std::fprintf(stderr, "[igr] phase 1: %zu batches, %.2f ms device\n", batches.size(), ms);
+}
+
+// Trees and route capacities of the last phase-1 plan, in routing order.
+void Router::build_plan() {
+    if (plan_built) return;
+    plan_node_off.assign(1, 0);
+    plan_nodes.clear();
+    plan_par.clear();
+    plan_cap.resize(plan_ids.size());
+    for (size_t k = 0; k < plan_ids.size(); k++) {
+        const int id = plan_ids[k];
+        plan_nodes.insert(plan_nodes.end(), tree_nodes.begin() + tree_off[id], tree_nodes.begin() + tree_off[id + 1]);
+        plan_par.insert(plan_par.end(), tree_par.begin() + tree_off[id], tree_par.begin() + tree_off[id + 1]);
+        plan_node_off.push_back((int)plan_nodes.size());
+        plan_cap[k] = route_cap1[id];
+    }
+    plan_built = true;
 }
 
 // Colours `order` (highest priority first) into batches of spatially disjoint
@@ -400,16 +433,19 @@ bool Router::rrr_pass(int iter) {
     cv.xsum.resize((size_t)X * Y);
     cv.ysum.resize((size_t)X * Y);
     cuda_check(cudaMemcpyAsync(is_of.data(), d_is_of.p, R, cudaMemcpyDeviceToHost, s), "D2H");
-    cuda_check(cudaMemcpyAsync(cv.xsum.data(), d_xsum.p, cv.xsum.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
-    cuda_check(cudaMemcpyAsync(cv.ysum.data(), d_ysum.p, cv.ysum.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
-    st.d2h_bytes += R + (int64_t)X * Y * 8;
+    st.d2h_bytes += R;
     std::vector<int> of_nets;
     for (int i = 0; i < R; i++)
         if (is_of[i]) of_nets.push_back(i);
     st.rerouted = (int)of_nets.size();
     if (verbose) std::fprintf(stderr, "[igr] pass %d: %zu nets to reroute\n", iter, of_nets.size());
     if (of_nets.empty()) return false;
+    // the host builds the detour DAGs from the congestion view (Lshape_route_detour.hpp:735-740)
+    cuda_check(cudaMemcpyAsync(cv.xsum.data(), d_xsum.p, cv.xsum.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaMemcpyAsync(cv.ysum.data(), d_ysum.p, cv.ysum.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    st.d2h_bytes += (int64_t)X * Y * 8;
     std::sort(of_nets.begin(), of_nets.end(), [&](int l, int r) { return ns.nets[l].hpwl > ns.nets[r].hpwl; });
     // detour DAGs on host threads (Lshape_route_detour.hpp:702-748)
     const double th0 = now_s();

@@ -106,6 +106,7 @@ struct Router {
     // ---- inputs resident in HBM after open(): trees and conflict shapes in net-id order
     std::vector<int> tree_off, tree_nodes, tree_par;  // DFS preorder (Lshape_route.hpp:191-208)
     std::vector<int64_t> scratch_off;                  // per net: DP scratch offset, -1 = on chip
+    std::vector<int> order1;                           // phase-1 priority order (HPWL descending)
     int64_t scratch_nodes = 0;
     DevBuf<int> d_tree_off, d_tree_nodes, d_tree_par;
     DevBuf<int64_t> d_scratch_off;
@@ -122,7 +123,13 @@ struct Router {
     std::vector<int> h_routes;  // host copy, made on demand
     bool h_routes_valid = false;
     // ---- per-run device buffers (grow-only)
-    DevBuf<int> d_ids, d_all_ids, of_sum, d_perm, d_rank, d_map, d_bat, d_sta, d_act, d_flags;
+    DevBuf<int> d_ids, d_all_ids, of_sum, d_perm, d_rank, d_map, d_bat, d_sta, d_act, d_flags, d_queue;
+    // launch shape of the tree DP per size class (large, medium, small) and the
+    // node count that separates small from medium nets (autotuned, see tune.cpp)
+    struct Tune {
+        int split = 6;
+        int lanes[3] = {32, 32, 16};
+    } tune;
     DevBuf<uint8_t> d_is_of;
     DevBuf<float> d_xsum, d_ysum;
     DevBuf<unsigned> d_bar;
@@ -135,6 +142,8 @@ struct Router {
     unsigned long long cost_cells = 0;
     // phase-1 plan of the last run (routing order, batches, trees, route capacity in order)
     std::vector<int> plan_ids, plan_batch_off, plan_node_off, plan_nodes, plan_par, plan_cap;
+    bool plan_built = false;
+    void build_plan();
     // score of the last run: wirelength, vias, overflow (GPU estimate)
     double score_wl = 0, score_via = 0, score_of = 0;
 

@@ -18,7 +18,9 @@ EVALUATOR = os.path.join(ROOT, "oracle", "_ref", "evaluator")
 def evaluate(cap, net, out):
     p = subprocess.run([EVALUATOR, cap, net, out], capture_output=True, text=True, timeout=600)
     stat = [l for l in p.stdout.splitlines() if l.startswith("FOR_STAT")]
-    assert p.returncode == 0 and stat, p.stdout[-2000:] + p.stderr[-2000:]
+    # the evaluator returns 1 after a complete evaluation and exits 0 after printing
+    # the name of a disconnected net (run/evaluator.cpp:267-276, :509-513)
+    assert stat, p.stdout[-2000:] + p.stderr[-2000:]
     opens = [l for l in p.stdout.splitlines() if l.startswith("Number of open nets")]
     assert opens and opens[0].split(":")[1].strip() == "0"
     return [float(v) for v in stat[0].split()[1:]]
