@@ -199,10 +199,12 @@ def main():
         dist.barrier()
         cap, net = design_files(args)
 
-    r = ig.Router(cap, net, rrr_iters=args.rrr_iters, profile=1)
-    design_nets, routing_nets = r.sizes()
+    rb = ig.Router(cap, net, rrr_iters=args.rrr_iters, profile=1, batched=1)  # batched form (headline)
+    rp = ig.Router(cap, net, rrr_iters=args.rrr_iters, profile=1, batched=0)  # plain drop-in form
+    design_nets, routing_nets = rb.sizes()
     for _ in range(max(args.warmup, 0)):
-        r.run()
+        rb.run()
+        rp.run()
 
     def sync_all():
         torch.cuda.synchronize()
@@ -210,57 +212,54 @@ def main():
             dist.barrier()
             torch.cuda.synchronize()
 
-    clk = Clocks(local)
-    sync_all()
-    clk.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    launches = 0
-    ks_tot = {}
-    for _ in range(args.steps):
-        r.run()
-        launches += int(r.stats()["launches"])
-        for k, v in r.kstats().items():
-            t = ks_tot.setdefault(k, dict(launches=0, ms=0.0, bytes=0.0))
-            for f in t:
-                t[f] += v[f]
-    e1.record()
-    sync_all()
-    clocks = clk.stop()
-    ms = e0.elapsed_time(e1)
-    tmax = torch.tensor([ms], device="cuda")
-    if dist:
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    ms_max = float(tmax.item())
-    st = r.stats()
+    def timed(router, fn):
+        """K steps bracketed by barrier + synchronize; device time (CUDA events) max over ranks."""
+        sync_all()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        launches, ks = 0, {}
+        for _ in range(args.steps):
+            fn()
+            if router is not None:
+                launches += int(router.stats()["launches"])
+                for k, v in router.kstats().items():
+                    t = ks.setdefault(k, dict(launches=0, ms=0.0, bytes=0.0))
+                    for f in t:
+                        t[f] += v[f]
+        e1.record()
+        sync_all()
+        t = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), launches, ks
 
-    # e2e: the whole `-cap/-net/-out` call with host files, K steps
+    clk = Clocks(local)
+    clk.start()
+    ms_b, launches_b, ks_b = timed(rb, rb.run)
+    ms_p, launches_p, ks_p = timed(rp, rp.run)
+    clocks = clk.stop()
+    sb, sp = rb.stats(), rp.stats()
+    same = all(sb[k] == sp[k] for k in ("wirelength", "via_cost", "overflow_cost"))
+
+    # e2e: the whole `-cap/-net/-out` call with host files (read, route, write), batched form
     out = os.path.join(args.workdir, f"guides_r{rank}.out")
-    sync_all()
-    e0.record()
-    for _ in range(args.steps):
-        ig.route_files(cap, net, out, rrr_iters=args.rrr_iters)
-    e1.record()
-    sync_all()
-    ms_e2e = e0.elapsed_time(e1)
-    te = torch.tensor([ms_e2e], device="cuda")
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    ms_e2e = float(te.item())
+    ms_e2e, _, _ = timed(None, lambda: ig.route_files(cap, net, out, rrr_iters=args.rrr_iters, batched=1))
 
     result = None
     if rank == 0:
-        value = design_nets * args.steps * world / (ms_max / 1e3)
+        value = design_nets * args.steps * world / (ms_b / 1e3)
+        value_plain = design_nets * args.steps * world / (ms_p / 1e3)
         e2e_value = design_nets * args.steps * world / (ms_e2e / 1e3)
         L, X, Y = 9, cfg["X"], cfg["Y"]
         cells = L * X * Y
-        h2d = cells * 4 + (X + Y) * 4  # capacity and edge lengths each open, trees, batches (below)
-        plan = r.plan()
-        h2d += (plan["nodes"].size * 2 + plan["node_off"].size + plan["net_ids"].size) * 4
-        d2h = int(sum(plan["route_cap"])) * 4 + cells * 0
-        # dominant kernel and its roofline
-        dom = max(ks_tot, key=lambda k: ks_tot[k]["ms"])
-        cr = ks_tot["cost_refresh"]
+        plan = rp.plan()
+        # per step: net ordering, batch offsets (route_files also uploads the grid and trees)
+        h2d = cells * 4 + (X + Y) * 4 + (plan["nodes"].size * 2 + plan["node_off"].size * 2
+                                         + plan["net_ids"].size * 3) * 4
+        d2h = int(sum(plan["route_cap"])) * 4
+        # dominant kernel of the plain form and the cost-refresh roofline
+        dom = max(ks_p, key=lambda k: ks_p[k]["ms"])
+        cr = ks_p["cost_refresh"]
         pk = measured_peaks()
         tr = profile_traffic()
         ach = cr["bytes"] / (cr["ms"] / 1e3) / 1e9 if cr["ms"] else 0.0
@@ -270,34 +269,39 @@ def main():
                     traffic=tr.get("cost_refresh_bytes_per_launch"),
                     algorithmic_bytes_per_launch=cr["bytes"] / max(cr["launches"], 1),
                     avg_launch_us=1e3 * cr["ms"] / max(cr["launches"], 1),
-                    dominant_kernel=dom, kernel_ms_per_step={k: round(v["ms"] / args.steps, 3)
-                                                             for k, v in ks_tot.items()})
+                    dominant_kernel=dom,
+                    kernel_ms_per_step_plain={k: round(v["ms"] / args.steps, 3) for k, v in ks_p.items()},
+                    kernel_ms_per_step_batched={k: round(v["ms"] / args.steps, 3) for k, v in ks_b.items()})
         cpu = None
         if world == 1:
             try:
-                g = r.grid()
-                v, info = cpu_sample(r, g, plan, args.cpu_batches)
+                g = rp.grid()
+                v, info = cpu_sample(rp, g, plan, args.cpu_batches)
                 cpu = dict(value=round(v, 2), unit="nets/s", cores=1, kind="port",
                            sample=f"oracle phase-1 (cost refresh + tree DP + commit) on the first "
                                   f"{info['batches']} of {info['of_batches']} batches ({info['nets']} nets, "
                                   f"{info['seconds']:.1f} s)")
             except Exception as ex:  # the CPU baseline is reported, never required
                 cpu = dict(value=None, unit="nets/s", cores=1, kind="port", sample=f"failed: {ex}")
-        result = dict(metric="route throughput (nets/s), plain RRR router", value=round(value, 2), unit="nets/s",
-                      n_gpus=world, steps=args.steps, warmup=args.warmup, ms_per_step=round(ms_max / args.steps, 3),
+        result = dict(metric="route throughput (nets/s), batched RRR router", value=round(value, 2), unit="nets/s",
+                      n_gpus=world, steps=args.steps, warmup=args.warmup, ms_per_step=round(ms_b / args.steps, 3),
                       higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32/f64 costs, i32 demand",
                       data="synthetic (seeded generator, ISPD2024 format)", config=workload,
                       parallelism="replicas" if world > 1 else "single GPU",
                       e2e=dict(value=round(e2e_value, 2), unit="nets/s", h2d_bytes_per_step=int(h2d),
                                d2h_bytes_per_step=int(d2h)),
-                      roofline=roof, cpu_baseline=cpu, clocks=clocks, gpu_launches=launches,
+                      roofline=roof, cpu_baseline=cpu, clocks=clocks, gpu_launches=launches_b,
+                      plain=dict(value=round(value_plain, 2), ms_per_step=round(ms_p / args.steps, 3),
+                                 gpu_launches=launches_p, same_result_as_batched=same),
                       detail=dict(design_nets=design_nets, routing_nets=routing_nets,
-                                  wirelength=st["wirelength"], via_cost=st["via_cost"],
-                                  overflow_cost=st["overflow_cost"], batches1=st["batches1"],
-                                  rerouted_last=st["rerouted"], p1_ms=st["p1_ms"], rrr_ms=st["rrr_ms"],
-                                  dag_host_ms=st["dag_host_ms"], route_s=st["route_s"]))
+                                  wirelength=sb["wirelength"], via_cost=sb["via_cost"],
+                                  overflow_cost=sb["overflow_cost"], batches1=sb["batches1"],
+                                  rerouted_last=sb["rerouted"], p1_ms=sb["p1_ms"], rrr_ms=sb["rrr_ms"],
+                                  dag_host_ms=sb["dag_host_ms"], route_s=sb["route_s"],
+                                  host_cores=os.cpu_count()))
         print(json.dumps(result), flush=True)
-    r.close()
+    rb.close()
+    rp.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

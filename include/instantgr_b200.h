@@ -74,7 +74,8 @@ int igr_router_write(igr_router *r, const char *out_path);
  * pass, [2] wirelength, [3] via count, [4] overflow cost (GPU estimate,
  * src/graph.hpp:148-169), [5] route wall seconds, [6] phase-1 batches,
  * [7] phase-1 device ms, [8] rip-up/reroute device ms, [9] host DAG ms,
- * [10] kernel launches, [11] design nets. */
+ * [10] kernel launches, [11] design nets, [12] colouring rounds,
+ * [13] host-to-device bytes, [14] device-to-host bytes. */
 int igr_router_stats(igr_router *r, double *out, int n);
 /* Per-kernel-class device time of the last run (needs opt->profile): for
  * class k in {cost refresh, tree DP, wire commit, via commit, DAG DP,

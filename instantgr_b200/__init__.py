@@ -164,10 +164,11 @@ def generate_custom(X, Y, nets, seed=1, cap_mode=0, block_frac=0.05, pin_mode=0,
                                      bbox_sigma, hotspots, hotspot_frac, cap.encode(), net.encode()))
 
 
-KERNEL_CLASSES = ["cost_refresh", "pattern_dp", "wire_commit", "via_commit", "dag_dp", "coloring", "ripup"]
+KERNEL_CLASSES = ["cost_refresh", "pattern_dp", "wire_commit", "via_commit", "dag_dp", "coloring", "ripup",
+                  "phase1_graph"]
 
 STATS = ["routing_nets", "rerouted", "wirelength", "via_cost", "overflow_cost", "route_s", "batches1", "p1_ms",
-         "rrr_ms", "dag_host_ms", "launches", "design_nets"]
+         "rrr_ms", "dag_host_ms", "launches", "design_nets", "color_rounds", "h2d_bytes", "d2h_bytes"]
 
 
 class Router:

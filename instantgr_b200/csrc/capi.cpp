@@ -112,10 +112,11 @@ int igr_router_write(igr_router *h, const char *out) {
 int igr_router_stats(igr_router *h, double *o, int n) {
     if (!h || !o) return fail(nullptr, IGR_ERR_INVALID, "null argument");
     const auto &r = h->r;
-    double v[12] = {(double)r.ns.nets.size(), (double)r.st.rerouted, r.score_wl, r.score_via, r.score_of,
+    double v[15] = {(double)r.ns.nets.size(), (double)r.st.rerouted, r.score_wl, r.score_via, r.score_of,
                     r.st.wall, (double)r.st.batches1, r.st.p1_ms, r.st.rrr_ms, r.st.dag_host_ms,
-                    (double)r.st.launches, (double)r.d.num_nets()};
-    for (int k = 0; k < n && k < 12; k++) o[k] = v[k];
+                    (double)r.st.launches, (double)r.d.num_nets(), (double)r.st.color_rounds,
+                    (double)r.st.h2d_bytes, (double)r.st.d2h_bytes};
+    for (int k = 0; k < n && k < 15; k++) o[k] = v[k];
     return IGR_OK;
 }
 
@@ -577,7 +578,7 @@ int igr_color_batches(igr_ctx *c, int n, const int32_t *pt_off, const int32_t *p
         ho.upload(h_off, n + 1, c->s); hs.upload(hseg, 2 * (size_t)h_off[n], c->s);
         vo.upload(v_off, n + 1, c->s); vs.upload(vseg, 2 * (size_t)v_off[n], c->s);
         dco.upload(co, c->s); dcl.upload(cl, c->s);
-        map.alloc(XY); bat.alloc(n); sta.alloc(n); flags.alloc(8); act.alloc(2 * (size_t)n);
+        map.alloc(XY); bat.alloc(n); sta.alloc(n); flags.alloc(16); act.alloc(2 * (size_t)n);
         ColorDev cd;
         cd.n = n; cd.X = c->go.g.X; cd.Y = c->go.g.Y; cd.sparsity = sparsity;
         cd.pt_off = po.p; cd.pts = p.p; cd.pt_net = pn.p; cd.h_off = ho.p; cd.hseg = hs.p; cd.v_off = vo.p;

@@ -86,7 +86,7 @@ __global__ void coloring_kernel(ColorDev c, Bar bar, int *err, int max_batches) 
         if (tid == 0) { flags[0] = 0; flags[7] = 0; }
         if (!grid_barrier(bar, err)) return;
         for (int round = 0; round < 30; round++) {
-            if (tid == 0) flags[1] = 0;
+            if (tid == 0) { flags[1] = 0; flags[8]++; }
             // claim
             for (int w = gw; w < na; w += nw) {
                 const int k = act[w];
@@ -196,16 +196,17 @@ int run_coloring(ColorDev &c, int max_batch, cudaStream_t s) {
     if (blocks < 1) blocks = 1;
     Bar bar{reinterpret_cast<unsigned *>(c.flags + 4), reinterpret_cast<unsigned *>(c.flags + 5)};
     int *err = c.flags + 6;
-    cudaMemsetAsync(c.flags, 0, 8 * sizeof(int), s);
+    cudaMemsetAsync(c.flags, 0, 16 * sizeof(int), s);
     cudaMemsetAsync(c.batch, 0xff, sizeof(int) * (size_t)c.n, s);
     int max_batches = c.n + 1;
     void *args[] = {&c, &bar, &err, &max_batches};
     cudaError_t e = cudaLaunchCooperativeKernel((const void *)coloring_kernel, dim3(blocks), dim3(threads), args, 0, s);
     if (e != cudaSuccess) return -1;
-    int h[8];
+    int h[16];
     if (cudaMemcpyAsync(h, c.flags, sizeof h, cudaMemcpyDeviceToHost, s) != cudaSuccess) return -1;
     if (cudaStreamSynchronize(s) != cudaSuccess) return -1;
     if (h[6] != 0) return -2;
+    c.rounds = h[8];
     return h[2];
 }
 

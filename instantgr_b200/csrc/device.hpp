@@ -136,7 +136,8 @@ struct ColorDev {
     int *batch = nullptr;     // [n]
     int *status = nullptr;    // [n]
     int *active = nullptr, *active2 = nullptr;  // [n] each
-    int *flags = nullptr;     // [8] device flags
+    int *flags = nullptr;     // [16] device flags
+    int rounds = 0;           // out: colouring rounds run
 };
 // Claim lists of shapes (pt_off/pts/h_off/hseg/v_off/vseg as in ColorDev).
 void build_claims(int nshapes, const int *pt_off, const int *pts, const int *h_off, const int *hseg,

@@ -16,8 +16,11 @@
 // buffers have grown to the design's size.
 #include "router.hpp"
 
+#include <sys/stat.h>
+
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 
@@ -131,6 +134,7 @@ void ShapeDev::upload(const ShapeSet &sh, int X, int Y, int sp, cudaStream_t st)
 // ------------------------------------------------------------------ router
 Router::~Router() {
     kt.collect();
+    if (graph1_exec) cudaGraphExecDestroy(graph1_exec);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (s) cudaStreamDestroy(s);
@@ -193,6 +197,10 @@ void Router::ensure_device() {
     d_tree_par.upload(tree_par, s);
     d_scratch_off.upload(scratch_off, s);
     d_scratch.alloc((size_t)pattern_scratch_doubles(scratch_nodes));
+    d_route_off1.upload(route_off1, s);
+    d_route_cap1.upload(route_cap1, s);
+    d_route_off.alloc(route_off1.size());
+    d_route_cap.alloc(route_cap1.size());
     ShapeSet sh;
     const int R = (int)ns.nets.size();
     for (int i = 0; i < R; i++) {
@@ -265,23 +273,31 @@ void Router::fetch_routes() {
 }
 
 // Phase 1 (Lshape_route.hpp:155-257)
-void Router::phase1() {
-    const int R = (int)ns.nets.size();
-    std::vector<std::vector<int>> batches;
-    color_nets(order1, d_shapes1, 15, batches);
-    std::reverse(batches.begin(), batches.end());
-    st.batches1 = (int)batches.size();
-    // Size classes inside each batch (results do not depend on the order of nets
-    // within a batch): large nets (global scratch) first, then medium, then small,
-    // each by node count, largest first.
-    std::vector<int> net_ids, batch_off{0}, class_off;
-    net_ids.reserve(R);
+// Routing order of phase 1 from the colouring.  Plain form: each batch in
+// colouring order, one DP launch.  Batched form: inside each batch the nets
+// are split into size classes (results do not depend on the order of nets
+// within a batch): large nets (global scratch) first, then medium, then small,
+// each by node count, largest first; one DP launch per class.
+void Router::plan_phase1(const std::vector<std::vector<int>> &batches, std::vector<int> &net_ids,
+                         std::vector<int> &batch_off, std::vector<int> &class_off) const {
+    net_ids.clear();
+    batch_off.assign(1, 0);
+    class_off.clear();
     auto nodes_of = [&](int id) { return tree_off[id + 1] - tree_off[id]; };
     for (auto &b : batches) {
+        if (!batched) {
+            class_off.push_back((int)net_ids.size());
+            class_off.push_back((int)net_ids.size());
+            class_off.push_back((int)net_ids.size());
+            net_ids.insert(net_ids.end(), b.begin(), b.end());
+            batch_off.push_back((int)net_ids.size());
+            continue;
+        }
         std::vector<int> cls[3];
         for (int id : b) {
             const int m = nodes_of(id);
-            cls[m > kPatternNodeTile ? 0 : (m > tune.split ? 1 : 2)].push_back(id);
+            // one class: every net in the medium launch (tile 16, scratch beyond it)
+            cls[tune.classes == 1 ? 1 : (m > kPatternNodeTile ? 0 : (m > tune.split ? 1 : 2))].push_back(id);
         }
         for (int c = 0; c < 3; c++) {
             std::stable_sort(cls[c].begin(), cls[c].end(), [&](int a, int bb) { return nodes_of(a) > nodes_of(bb); });
@@ -290,21 +306,19 @@ void Router::phase1() {
         }
         batch_off.push_back((int)net_ids.size());
     }
-    grow_routes(route_end);
-    d_ids.upload(net_ids, s);
-    d_route_off.upload(route_off, s);
-    d_route_cap.upload(route_cap, s);
-    d_queue.alloc(3 * batches.size() + 1);
-    cuda_check(cudaMemsetAsync(d_queue.p, 0, (3 * batches.size() + 1) * sizeof(int), s), "memset");
-    st.h2d_bytes += (int64_t)net_ids.size() * 4 + (int64_t)R * 12;
-    cuda_check(cudaEventRecord(ev0, s), "event");
-    for (size_t bi = 0; bi + 1 < batch_off.size(); bi++) {
+}
+
+// The per-batch launches of phase 1 (Lshape_route.hpp:235-242), stream-ordered.
+void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<int> &class_off, bool timed) {
+    const int nb = (int)batch_off.size() - 1;
+    cuda_check(cudaMemsetAsync(d_queue.p, 0, (3 * (size_t)nb + 1) * sizeof(int), s), "memset");
+    for (int bi = 0; bi < nb; bi++) {
         const int off = batch_off[bi], n = batch_off[bi + 1] - off;
-        const int stamp = ++global_stamp;
-        kt.begin(KC_COST);
+        const int stamp = bi + 1;
+        if (timed) kt.begin(KC_COST);
         launch_cost_refresh(go.g, true, s);
-        kt.end(KC_COST);
-        kt.begin(KC_PATTERN);
+        if (timed) kt.end(KC_COST);
+        if (timed) kt.begin(KC_PATTERN);
         for (int c = 0; c < 3; c++) {
             const int a = class_off[3 * bi + c];
             const int e = c < 2 ? class_off[3 * bi + c + 1] : batch_off[bi + 1];
@@ -312,21 +326,69 @@ void Router::phase1() {
             TreeBatchDev tb{d_ids.p + a, d_tree_off.p, d_tree_nodes.p, d_tree_par.p, d_route_off.p, d_route_cap.p,
                             routes.p, d_scratch.p, d_scratch_off.p, scratch_nodes, e - a};
             tb.queue = d_queue.p + 3 * bi + c;
-            tb.tile = c == 0 ? 1 : (c == 1 ? kPatternNodeTile : 6);
-            tb.lanes_per_net = tune.lanes[c];
+            if (batched) {
+                tb.tile = c == 0 ? 1 : (c == 1 ? kPatternNodeTile : 6);
+                tb.lanes_per_net = tune.lanes[c];
+            } else {
+                tb.tile = kPatternNodeTile;  // nets beyond the tile use global scratch in the same launch
+                tb.lanes_per_net = 32;
+            }
             launch_pattern_route(go.g, tb, stamp, s);
             st.launches += 1;
         }
-        kt.end(KC_PATTERN);
-        kt.begin(KC_WIRE_COMMIT);
+        if (timed) kt.end(KC_PATTERN);
+        if (timed) kt.begin(KC_WIRE_COMMIT);
         launch_wire_commit(go.g, stamp, true, s);
-        kt.end(KC_WIRE_COMMIT);
+        if (timed) kt.end(KC_WIRE_COMMIT);
         ViaBatchDev vb{d_ids.p + off, d_route_off.p, routes.p, n};
-        kt.begin(KC_VIA_COMMIT);
+        if (timed) kt.begin(KC_VIA_COMMIT);
         launch_via_commit(go.g, vb, stamp, 1, s);
-        kt.end(KC_VIA_COMMIT);
+        if (timed) kt.end(KC_VIA_COMMIT);
         st.launches += 3;
     }
+}
+
+void Router::phase1() {
+    const int R = (int)ns.nets.size();
+    std::vector<std::vector<int>> batches;
+    color_nets(order1, d_shapes1, 15, batches);
+    std::reverse(batches.begin(), batches.end());
+    st.batches1 = (int)batches.size();
+    if (batched && !tuned) autotune(batches);
+    std::vector<int> net_ids, batch_off, class_off;
+    plan_phase1(batches, net_ids, batch_off, class_off);
+    grow_routes(route_end);
+    d_ids.upload(net_ids, s);
+    cuda_check(cudaMemcpyAsync(d_route_off.p, d_route_off1.p, (size_t)R * 8, cudaMemcpyDeviceToDevice, s), "D2D");
+    cuda_check(cudaMemcpyAsync(d_route_cap.p, d_route_cap1.p, (size_t)R * 4, cudaMemcpyDeviceToDevice, s), "D2D");
+    d_queue.alloc(3 * batches.size() + 1);
+    st.h2d_bytes += (int64_t)net_ids.size() * 4;
+    cuda_check(cudaEventRecord(ev0, s), "event");
+    if (batched) {
+        // the whole phase-1 loop as one CUDA graph, reused while the plan is unchanged
+        if (!graph1_exec || graph1_batch_off != batch_off || graph1_class_off != class_off || graph1_routes != routes.p) {
+            if (graph1_exec) { cudaGraphExecDestroy(graph1_exec); graph1_exec = nullptr; }
+            cudaGraph_t gr = nullptr;
+            cuda_check(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed), "capture");
+            const long long l0 = st.launches;
+            emit_phase1(batch_off, class_off, false);
+            graph1_launches = st.launches - l0;
+            cuda_check(cudaStreamEndCapture(s, &gr), "capture");
+            cuda_check(cudaGraphInstantiate(&graph1_exec, gr, 0), "graph instantiate");
+            cudaGraphDestroy(gr);
+            graph1_batch_off = batch_off;
+            graph1_class_off = class_off;
+            graph1_routes = routes.p;
+        } else {
+            st.launches += graph1_launches;
+        }
+        kt.begin(KC_GRAPH1);  // whole graph: cost refreshes, DP, commits
+        cuda_check(cudaGraphLaunch(graph1_exec, s), "graph launch");
+        kt.end(KC_GRAPH1);
+    } else {
+        emit_phase1(batch_off, class_off, true);
+    }
+    global_stamp = (int)batches.size();
     cuda_check(cudaEventRecord(ev1, s), "event");
     cuda_check(cudaGetLastError(), "phase-1 launch");
     // plan of this run, in routing order (for igr_router_plan)
@@ -339,6 +401,97 @@ void Router::phase1() {
     st.p1_ms = ms;
     if (int e = go.check_error(s)) throw Error(e, "device error in phase 1");
     if (verbose) std::fprintf(stderr, "[igr] phase 1: %zu batches, %.2f ms device\n", batches.size(), ms);
+}
+
+// Autotuner of the batched form: picks the node count that separates small
+// from medium nets and the lanes per net of each size class by timing the
+// phase-1 batch loop of this design once per candidate (the routes are the
+// same for every candidate).  Results are cached per grid and net count in
+// $IGR_TUNE_CACHE (default ~/.cache/instantgr_b200/tune.txt).
+static std::string tune_cache_path() {
+    if (const char *p = std::getenv("IGR_TUNE_CACHE")) return p;
+    const char *h = std::getenv("HOME");
+    return std::string(h ? h : "/tmp") + "/.cache/instantgr_b200/tune.txt";
+}
+
+void Router::autotune(const std::vector<std::vector<int>> &batches) {
+    const int R = (int)ns.nets.size();
+    char key[96];
+    std::snprintf(key, sizeof key, "%d %d %d %d", ns.X, ns.Y, R, (int)batches.size());
+    const std::string path = tune_cache_path();
+    if (FILE *f = std::fopen(path.c_str(), "r")) {
+        char line[256];
+        while (std::fgets(line, sizeof line, f)) {
+            int x, y, r, b, cl, sp, l0, l1, l2;
+            if (std::sscanf(line, "%d %d %d %d %d %d %d %d %d", &x, &y, &r, &b, &cl, &sp, &l0, &l1, &l2) == 9) {
+                char k2[96];
+                std::snprintf(k2, sizeof k2, "%d %d %d %d", x, y, r, b);
+                auto lanes_ok = [](int l) { return l == 16 || l == 32; };
+                if (std::string(k2) == key && (cl == 1 || cl == 3) && sp >= 1 && sp <= 6 && lanes_ok(l0) &&
+                    lanes_ok(l1) && lanes_ok(l2)) {
+                    tune.classes = cl; tune.split = sp; tune.lanes[0] = l0; tune.lanes[1] = l1; tune.lanes[2] = l2;
+                    tuned = true;
+                }
+            }
+        }
+        std::fclose(f);
+        if (tuned) return;
+    }
+    std::vector<Tune> cands;
+    for (int lm : {32, 16}) {
+        Tune t;
+        t.classes = 1; t.lanes[1] = lm;
+        cands.push_back(t);
+    }
+    for (int sp : {3, 4, 6})
+        for (int lm : {16, 32})
+            for (int ls : {16, 32}) {
+                Tune t;
+                t.classes = 3; t.split = sp; t.lanes[0] = 32; t.lanes[1] = lm; t.lanes[2] = ls;
+                cands.push_back(t);
+            }
+    Tune best = tune;
+    float best_ms = 1e30f;
+    std::vector<int> net_ids, batch_off, class_off;
+    d_queue.alloc(3 * batches.size() + 1);
+    grow_routes(route_end);
+    for (const Tune &cand : cands) {
+            {
+                tune = cand;
+                plan_phase1(batches, net_ids, batch_off, class_off);
+                go.reset_demand(s);
+                d_ids.upload(net_ids, s);
+                cuda_check(cudaMemcpyAsync(d_route_off.p, d_route_off1.p, (size_t)R * 8, cudaMemcpyDeviceToDevice, s), "D2D");
+                cuda_check(cudaMemcpyAsync(d_route_cap.p, d_route_cap1.p, (size_t)R * 4, cudaMemcpyDeviceToDevice, s), "D2D");
+                cuda_check(cudaEventRecord(ev0, s), "event");
+                const long long l0 = st.launches;
+                emit_phase1(batch_off, class_off, false);
+                st.launches = l0;
+                cuda_check(cudaEventRecord(ev1, s), "event");
+                cuda_check(cudaEventSynchronize(ev1), "autotune");
+                float ms = 0;
+                cudaEventElapsedTime(&ms, ev0, ev1);
+                if (ms < best_ms) { best_ms = ms; best = tune; }
+            }
+    }
+    tune = best;
+    tuned = true;
+    go.reset_demand(s);
+    if (go.check_error(s)) throw Error(ERR_STATE, "device error while autotuning");
+    if (verbose)
+        std::fprintf(stderr, "[igr] autotune: %d classes, split %d, lanes %d/%d/%d (%.2f ms)\n", tune.classes,
+                     tune.split, tune.lanes[0], tune.lanes[1], tune.lanes[2], best_ms);
+    const size_t slash = path.rfind('/');
+    if (slash != std::string::npos) {
+        const std::string dir = path.substr(0, slash);
+        for (size_t i = 1; i <= dir.size(); i++)
+            if (i == dir.size() || dir[i] == '/') (void)mkdir(dir.substr(0, i).c_str(), 0755);
+    }
+    if (FILE *f = std::fopen(path.c_str(), "a")) {
+        std::fprintf(f, "%s %d %d %d %d %d\n", key, tune.classes, tune.split, tune.lanes[0], tune.lanes[1],
+                     tune.lanes[2]);
+        std::fclose(f);
+    }
 }
 
 // Trees and route capacities of the last phase-1 plan, in routing order.
@@ -375,7 +528,7 @@ void Router::color_nets(const std::vector<int> &order, const ShapeDev &shapes, i
     d_bat.alloc(n);
     d_sta.alloc(n);
     d_act.alloc(2 * (size_t)n);
-    d_flags.alloc(8);
+    d_flags.alloc(16);
     st.h2d_bytes += (int64_t)(n + nshapes) * 4;
     if (sparsity != shapes.sparsity) throw Error(ERR_STATE, "claim lists were built for another sparsity");
     ColorDev cd;
@@ -389,6 +542,7 @@ void Router::color_nets(const std::vector<int> &order, const ShapeDev &shapes, i
     kt.begin(KC_COLOR);
     int nb = run_coloring(cd, 0, s);
     kt.end(KC_COLOR);
+    st.color_rounds += cd.rounds;
     st.launches += 1;
     if (nb == -2) throw Error(ERR_TIMEOUT, "colouring barrier timed out");
     if (nb < 0) throw Error(ERR_CUDA, std::string("colouring failed: ") + cudaGetErrorString(cudaGetLastError()));

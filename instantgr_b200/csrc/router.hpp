@@ -64,11 +64,12 @@ struct RouterStats {
     int batches1 = 0, rerouted = 0;
     long long launches = 0;
     long long h2d_bytes = 0, d2h_bytes = 0;
+    long long color_rounds = 0;
 };
 
 // Per-kernel-class device time, measured with CUDA events around each launch
 // when profiling is on.
-enum KernelClass { KC_COST = 0, KC_PATTERN, KC_WIRE_COMMIT, KC_VIA_COMMIT, KC_DAG, KC_COLOR, KC_RIPUP, KC_N };
+enum KernelClass { KC_COST = 0, KC_PATTERN, KC_WIRE_COMMIT, KC_VIA_COMMIT, KC_DAG, KC_COLOR, KC_RIPUP, KC_GRAPH1, KC_N };
 struct KernelTimer {
     bool on = false;
     cudaStream_t s = nullptr;
@@ -127,9 +128,22 @@ struct Router {
     // launch shape of the tree DP per size class (large, medium, small) and the
     // node count that separates small from medium nets (autotuned, see tune.cpp)
     struct Tune {
+        int classes = 1;  // 1: one DP launch per batch (largest nets first); 3: large/medium/small launches
         int split = 6;
         int lanes[3] = {32, 32, 16};
     } tune;
+    bool tuned = false;
+    DevBuf<int64_t> d_route_off1;
+    DevBuf<int> d_route_cap1;
+    // phase-1 loop captured as a CUDA graph (batched form) and the plan it was captured for
+    cudaGraphExec_t graph1_exec = nullptr;
+    std::vector<int> graph1_batch_off, graph1_class_off;
+    int *graph1_routes = nullptr;
+    long long graph1_launches = 0;
+    void plan_phase1(const std::vector<std::vector<int>> &batches, std::vector<int> &net_ids,
+                     std::vector<int> &batch_off, std::vector<int> &class_off) const;
+    void emit_phase1(const std::vector<int> &batch_off, const std::vector<int> &class_off, bool timed);
+    void autotune(const std::vector<std::vector<int>> &batches);
     DevBuf<uint8_t> d_is_of;
     DevBuf<float> d_xsum, d_ysum;
     DevBuf<unsigned> d_bar;

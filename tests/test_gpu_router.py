@@ -52,6 +52,22 @@ def test_cli_matches_library(small_design):
     assert open(out1).read() == open(out2).read(), "routing must be deterministic"
 
 
+def test_batched_form_matches_plain_form(small_design):
+    """Size classes, autotuned launch shapes and the CUDA graph change no result."""
+    cap, net, d = small_design
+    outs = []
+    for batched in (0, 1, 1):  # the second batched run replays the cached graph
+        out = str(d / f"batched{batched}_{len(outs)}.out")
+        r = ig.Router(cap, net, rrr_iters=2, batched=batched)
+        r.run()
+        if batched:
+            r.run()
+        r.write(out)
+        outs.append(open(out).read())
+        r.close()
+    assert outs[0] == outs[1] == outs[2]
+
+
 def test_router_stats_and_gpu_score(small_design):
     cap, net, d = small_design
     r = ig.Router(cap, net, rrr_iters=1)
