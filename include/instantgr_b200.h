@@ -158,6 +158,35 @@ int igr_set_costs(igr_ctx *c, const float *vcost, const double *presum);
  * Wires go to the difference array; call igr_commit_wires afterwards. */
 int igr_pattern_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t *nodes, const int32_t *par,
                       const int64_t *route_off, const int32_t *route_cap, int32_t *routes_out, int32_t stamp);
+
+/* The same tree DP for callers that cannot let a library allocate device
+ * memory: hosts that give the whole GPU to their own pool allocator, loops
+ * that cannot afford the device-wide synchronisation a cudaMalloc may cause,
+ * and processes that must fix their footprint before they start.  It has no
+ * counterpart in InstantGR.
+ *
+ * Every pointer is DEVICE memory owned by the caller: node_off[n+1],
+ * nodes/par[total_nodes], route_off/route_cap[n], routes[routes_len].  Inputs
+ * must be complete on the device when the call starts; the call runs on the
+ * context's stream and returns when the routes and the difference array are
+ * written (then call igr_commit_wires as usual).  Results are identical to
+ * igr_pattern_route's.
+ *
+ * The DP's scratch (layer tables of nets with more than 16 tree nodes, 832
+ * bytes per such node, plus 12 bytes per net and a work counter) lives in one
+ * fixed array of IGR_STATIC_SCRATCH_BYTES in the library's device image, held
+ * by every GPU that loads the library until the process exits.  A call with
+ * more than IGR_STATIC_MAX_NETS nets, or whose large nets need more scratch
+ * than the array holds, returns IGR_ERR_CAPACITY and runs nothing.  The call
+ * allocates no device memory; its first call on a device looks up the
+ * array's device address, so make that first call before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU (from several
+ * threads or contexts of one device) race on it, so serialise them. */
+#define IGR_STATIC_SCRATCH_BYTES (64u << 20)
+#define IGR_STATIC_MAX_NETS (1 << 20)
+int igr_pattern_route_static(igr_ctx *c, int n, const int32_t *node_off, int64_t total_nodes, const int32_t *nodes,
+                             const int32_t *par, const int64_t *route_off, const int32_t *route_cap, int32_t *routes,
+                             int64_t routes_len, int32_t stamp);
 /* Difference-array commit (compute_presum_general + commit_all_edge + memset,
  * src/graph.hpp:74-137). */
 int igr_commit_wires(igr_ctx *c, int32_t stamp);

@@ -22,6 +22,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libigr_b200.so")
 ROUTE_BIN = os.path.join(_HERE, "bin", "igr_route")
 
 IGR_OK = 0
+IGR_ERR_INVALID, IGR_ERR_CAPACITY, IGR_ERR_STATE = -1, -5, -7
 ERRORS = {-1: "INVALID", -2: "IO", -3: "FORMAT", -4: "CUDA", -5: "CAPACITY", -6: "TIMEOUT", -7: "STATE"}
 
 _lib: Optional[C.CDLL] = None
@@ -39,7 +40,8 @@ EXPORTS = [
     "igr_router_demand", "igr_router_close", "igr_router_plan", "igr_router_grid", "igr_set_device",
     "igr_generate", "igr_generate_custom", "igr_create", "igr_destroy", "igr_last_error", "igr_set_demand",
     "igr_get_demand", "igr_get_stamp", "igr_get_pre", "igr_cost_refresh", "igr_get_costs", "igr_set_costs",
-    "igr_pattern_route", "igr_commit_wires", "igr_commit_vias", "igr_ripup_wires", "igr_mark_overflow",
+    "igr_pattern_route", "igr_pattern_route_static", "igr_commit_wires", "igr_commit_vias", "igr_ripup_wires",
+    "igr_mark_overflow",
     "igr_congestion_view", "igr_score", "igr_color_batches", "igr_dag_route", "igr_build_dag", "igr_steiner",
 ]
 
@@ -103,6 +105,7 @@ def lib() -> C.CDLL:
     L.igr_get_costs.argtypes = [vp, _f32p, _f64p]
     L.igr_set_costs.argtypes = [vp, _f32p, _f64p]
     L.igr_pattern_route.argtypes = [vp, C.c_int, _i32p, _i32p, _i32p, _i64p, _i32p, _i32p, C.c_int32]
+    L.igr_pattern_route_static.argtypes = [vp, C.c_int, vp, C.c_int64, vp, vp, vp, vp, vp, C.c_int64, C.c_int32]
     L.igr_commit_wires.argtypes = [vp, C.c_int32]
     L.igr_commit_vias.argtypes = [vp, C.c_int, _i64p, _i32p, C.c_int32, C.c_int32]
     L.igr_ripup_wires.argtypes = [vp, C.c_int, _i64p, _i32p, C.c_int32, C.c_int32]
@@ -163,6 +166,10 @@ def generate_custom(X, Y, nets, seed=1, cap_mode=0, block_frac=0.05, pin_mode=0,
     _check(lib().igr_generate_custom(X, Y, nets, seed, cap_mode, block_frac, pin_mode, hifanout_frac, bbox_median,
                                      bbox_sigma, hotspots, hotspot_frac, cap.encode(), net.encode()))
 
+
+# limits of igr_pattern_route_static (IGR_STATIC_SCRATCH_BYTES, IGR_STATIC_MAX_NETS)
+STATIC_SCRATCH_BYTES = 64 << 20
+STATIC_MAX_NETS = 1 << 20
 
 KERNEL_CLASSES = ["cost_refresh", "pattern_dp", "wire_commit", "via_commit", "dag_dp", "coloring", "ripup",
                   "phase1_graph"]
@@ -323,6 +330,14 @@ class Ctx:
         self._c(lib().igr_pattern_route(self.h, len(route_off), _i32(node_off), _i32(nodes), _i32(par),
                                         _i64(route_off), _i32(route_cap), routes, stamp))
         return routes
+
+    def pattern_route_static(self, n, node_off, total_nodes, nodes, par, route_off, route_cap, routes,
+                             routes_len, stamp):
+        """Tree DP over caller-owned DEVICE arrays (integer device addresses),
+        with its scratch in the library's fixed device array: no allocation
+        (igr_pattern_route_static)."""
+        self._c(lib().igr_pattern_route_static(self.h, n, node_off, total_nodes, nodes, par, route_off, route_cap,
+                                               routes, routes_len, stamp))
 
     def commit_wires(self, stamp):
         self._c(lib().igr_commit_wires(self.h, stamp))

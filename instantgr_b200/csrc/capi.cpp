@@ -449,6 +449,19 @@ int igr_pattern_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t 
     });
 }
 
+static_assert(IGR_STATIC_SCRATCH_BYTES == kStaticScratchBytes, "static scratch size");
+static_assert(IGR_STATIC_MAX_NETS == kStaticMaxNets, "static scratch net limit");
+
+int igr_pattern_route_static(igr_ctx *c, int n, const int32_t *node_off, int64_t total_nodes, const int32_t *nodes,
+                             const int32_t *par, const int64_t *route_off, const int32_t *route_cap, int32_t *routes,
+                             int64_t routes_len, int32_t stamp) {
+    CTX_GUARD(c, {
+        pattern_route_static(c->go.g, n, node_off, total_nodes, nodes, par, route_off, route_cap, routes, routes_len,
+                             stamp, c->s);
+        sync_check(c);
+    });
+}
+
 int igr_commit_wires(igr_ctx *c, int32_t stamp) {
     CTX_GUARD(c, {
         launch_wire_commit(c->go.g, stamp, true, c->s);

@@ -67,6 +67,15 @@ inline int64_t pattern_scratch_doubles(int64_t nodes) { return nodes * 81 + (nod
 constexpr int kPatternNodeTile = 16;  // nets with more nodes use global scratch
 void launch_pattern_route(const GridDev &g, const TreeBatchDev &b, int stamp, cudaStream_t s);
 
+// Tree DP over caller-owned device arrays with its scratch in a fixed array of
+// the library's device image (pattern_static.cu); synchronous on `s`.
+constexpr size_t kStaticScratchBytes = size_t(64) << 20;
+constexpr int kStaticMaxNets = 1 << 20;
+constexpr int kStaticMaxDevices = 64;
+void pattern_route_static(const GridDev &g, int n, const int *node_off, int64_t total_nodes, const int *nodes,
+                          const int *par, const int64_t *route_off, const int *route_cap, int *routes,
+                          int64_t routes_len, int stamp, cudaStream_t s);
+
 struct ViaBatchDev {
     const int *net_ids;  // [n]
     const int64_t *route_off;
