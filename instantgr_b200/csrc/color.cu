@@ -66,95 +66,133 @@ __device__ bool grid_barrier(Bar b, int *err) {
     return s_ok != 0;
 }
 
-// flags: [0] commit in batch, [1] commit in round, [2] batches, [3] active count,
-//        [4..5] barrier, [6] error, [7] next active count
-__global__ void coloring_kernel(ColorDev c, Bar bar, int *err, int max_batches) {
+constexpr int kG = 8;                 // lanes per net
+constexpr int kNetsPerWarp = 32 / kG;
+constexpr unsigned kGroupMask = (1u << kG) - 1;
+
+// flags (ints): [0..1] commit seen in a round (by round parity), [2] batches,
+// [4..5] barrier, [6] error, [8] rounds run, [9] lost count, [10] next
+// candidate count, [11..12] nets left after a batch (by batch parity)
+enum : int { F_ROUND = 0, F_NB = 2, F_ERR = 6, F_ROUNDS = 8, F_LOST = 9, F_CAND = 10, F_LEFT = 11 };
+
+// Appends `k` of every group leader with `want` set to list[*count++]; called
+// by all 32 lanes of the warp with the same control flow.
+__device__ __forceinline__ void warp_append(int *list, int *count, bool want, int k, int lane) {
+    const unsigned m = __ballot_sync(0xffffffffu, want);
+    if (!m) return;
+    int base = 0;
+    if (lane == 0) base = atomicAdd(count, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (want) list[base + __popc(m & ((1u << lane) - 1))] = k;
+}
+
+// Per batch: candidates claim (atomicMax of their rank on their claim cells),
+// candidates owning all their points join, the others are blocked when a
+// member owns one of their points (and release their cells at once; a blocked
+// net's cells are no member's points, so the release cannot change another
+// net's check), else they stay candidates.  Three grid barriers per round.
+// The lists are unordered: every phase is order-independent.
+__global__ void __launch_bounds__(1024, 1) coloring_kernel(ColorDev c, Bar bar, int *err, int max_batches) {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nth = gridDim.x * blockDim.x;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, grp = lane / kG, gl = lane % kG;
     const int gw = tid >> 5, nw = nth >> 5;
     const int XY = c.X * c.Y;
-    volatile int *flags = c.flags;
+    int *flags = c.flags;
+    volatile int *vflags = c.flags;
     int *act = c.active, *act2 = c.active2;
     for (int i = tid; i < c.n; i += nth) act[i] = i;
-    if (tid == 0) flags[3] = c.n;
+    for (int i = tid; i < XY; i += nth) c.map[i] = -1;
     if (!grid_barrier(bar, err)) return;
+    int na = c.n;
     for (int cur = 0; cur < max_batches; cur++) {
-        const int na = flags[3];
-        for (int i = tid; i < XY; i += nth) c.map[i] = -1;
-        for (int i = tid; i < na; i += nth) c.status[act[i]] = 0;
-        if (tid == 0) { flags[0] = 0; flags[7] = 0; }
-        if (!grid_barrier(bar, err)) return;
+        const int *cand = act;  // round 0: every net without a batch
+        int nc = na;
         for (int round = 0; round < 30; round++) {
-            if (tid == 0) { flags[1] = 0; flags[8]++; }
             // claim
-            for (int w = gw; w < na; w += nw) {
-                const int k = act[w];
-                if (c.status[k] == 2 || c.batch[k] != -1) continue;  // blocked, or already a member
-                if (lane == 0) c.status[k] = 1;
+            if (tid == 0) {
+                flags[F_ROUNDS]++;
+                flags[F_LOST] = 0;
+                flags[F_ROUND + ((round + 1) & 1)] = 0;
+            }
+            for (int base = gw * kNetsPerWarp; base < nc; base += nw * kNetsPerWarp) {
+                const int idx = base + grp;
+                if (idx >= nc) continue;
+                const int k = cand[idx];
                 const int sh = c.perm ? c.perm[k] : k;
-                for (int i = c.claim_off[sh] + lane; i < c.claim_off[sh + 1]; i += 32) atomicMax(&c.map[c.claim[i]], k);
+                const int e = c.claim_off[sh + 1];
+                for (int i = c.claim_off[sh] + gl; i < e; i += kG) atomicMax(&c.map[c.claim[i]], k);
             }
             if (!grid_barrier(bar, err)) return;
-            // commit: owns every point
-            for (int w = gw; w < na; w += nw) {
-                const int k = act[w];
-                if (c.status[k] != 1 || c.batch[k] != -1) continue;
-                const int sh = c.perm ? c.perm[k] : k;
+            // commit: members own every point; the others go to the lost list
+            if (tid == 0) {
+                flags[F_CAND] = 0;
+                if (round == 0) flags[F_LEFT + ((cur + 1) & 1)] = 0;
+            }
+            for (int base = gw * kNetsPerWarp; base < nc; base += nw * kNetsPerWarp) {
+                const int idx = base + grp;
+                const bool valid = idx < nc;
+                const int k = valid ? cand[idx] : -1;
                 bool ok = true;
-                for (int i = c.pt_off[sh] + lane; i < c.pt_off[sh + 1]; i += 32) ok &= c.map[c.pts[i]] == k;
-                ok = __all_sync(0xffffffffu, ok);
-                if (ok && lane == 0) {
+                if (valid) {
+                    const int sh = c.perm ? c.perm[k] : k;
+                    const int e = c.pt_off[sh + 1];
+                    for (int i = c.pt_off[sh] + gl; i < e; i += kG) ok &= c.map[c.pts[i]] == k;
+                }
+                const unsigned bad = (__ballot_sync(0xffffffffu, !ok) >> (grp * kG)) & kGroupMask;
+                if (valid && bad == 0 && gl == 0) {
                     c.batch[k] = cur;
-                    flags[0] = 1;
-                    flags[1] = 1;
+                    flags[F_ROUND + (round & 1)] = 1;
                 }
+                warp_append(c.lost, flags + F_LOST, valid && bad != 0 && gl == 0, k, lane);
             }
             if (!grid_barrier(bar, err)) return;
-            if (!flags[1]) break;
-            // block candidates whose points belong to a member of this batch
-            for (int w = gw; w < na; w += nw) {
-                const int k = act[w];
-                if (c.status[k] != 1 || c.batch[k] != -1) continue;
-                const int sh = c.perm ? c.perm[k] : k;
+            if (!vflags[F_ROUND + (round & 1)]) break;
+            // block (and release) or stay a candidate
+            const int nl = vflags[F_LOST];
+            for (int base = gw * kNetsPerWarp; base < nl; base += nw * kNetsPerWarp) {
+                const int idx = base + grp;
+                const bool valid = idx < nl;
+                const int k = valid ? c.lost[idx] : -1;
+                const int sh = valid ? (c.perm ? c.perm[k] : k) : 0;
                 bool hit = false;
-                for (int i = c.pt_off[sh] + lane; i < c.pt_off[sh + 1]; i += 32) {
-                    const int pre = c.map[c.pts[i]];
-                    hit |= (pre != -1 && c.batch[pre] != -1);
+                if (valid) {
+                    const int e = c.pt_off[sh + 1];
+                    for (int i = c.pt_off[sh] + gl; i < e; i += kG) {
+                        const int pre = c.map[c.pts[i]];
+                        hit |= (pre != -1 && c.batch[pre] != -1);
+                    }
                 }
-                hit = __any_sync(0xffffffffu, hit);
-                if (hit && lane == 0) c.status[k] = 2;
+                const bool blocked = ((__ballot_sync(0xffffffffu, hit) >> (grp * kG)) & kGroupMask) != 0;
+                if (valid && blocked) {
+                    const int e = c.claim_off[sh + 1];
+                    for (int i = c.claim_off[sh] + gl; i < e; i += kG)
+                        if (c.map[c.claim[i]] == k) c.map[c.claim[i]] = -1;
+                }
+                warp_append(c.cand, flags + F_CAND, valid && !blocked && gl == 0, k, lane);
             }
             if (!grid_barrier(bar, err)) return;
-            // blocked nets release the cells they own
-            for (int w = gw; w < na; w += nw) {
-                const int k = act[w];
-                if (c.status[k] != 2) continue;
-                const int sh = c.perm ? c.perm[k] : k;
-                for (int i = c.claim_off[sh] + lane; i < c.claim_off[sh + 1]; i += 32)
-                    if (c.map[c.claim[i]] == k) c.map[c.claim[i]] = -1;
-            }
-            if (!grid_barrier(bar, err)) return;
+            cand = c.cand;
+            nc = vflags[F_CAND];
+            if (nc == 0) break;
         }
-        if (!flags[0]) {
-            if (tid == 0) flags[2] = cur;
-            return;
-        }
-        // nets still without a batch stay active (their order in the list does not matter)
-        for (int i = tid; i < na; i += nth) {
-            const int k = act[i];
-            if (c.batch[k] == -1) act2[atomicAdd((int *)&flags[7], 1)] = k;
+        // nets still without a batch stay active; the map is cleared for the next batch
+        for (int i = tid; i < XY; i += nth) c.map[i] = -1;
+        if (tid == 0) flags[F_ROUND] = flags[F_ROUND + 1] = 0;
+        for (int base = gw * 32; base < na; base += nw * 32) {
+            const int i = base + lane;
+            const int k = i < na ? act[i] : -1;
+            warp_append(act2, flags + F_LEFT + (cur & 1), k >= 0 && c.batch[k] == -1, k, lane);
         }
         if (!grid_barrier(bar, err)) return;
-        if (tid == 0) flags[3] = flags[7];
+        na = vflags[F_LEFT + (cur & 1)];
         int *t = act; act = act2; act2 = t;
-        if (!grid_barrier(bar, err)) return;
-        if (flags[3] == 0) {
-            if (tid == 0) flags[2] = cur + 1;
+        if (na == 0) {
+            if (tid == 0) flags[F_NB] = cur + 1;
             return;
         }
     }
-    if (tid == 0) flags[2] = max_batches;
+    if (tid == 0) flags[F_NB] = max_batches;
 }
 
 }  // namespace
@@ -190,9 +228,9 @@ int run_coloring(ColorDev &c, int max_batch, cudaStream_t s) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int threads = 512;
+    const int threads = 1024;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coloring_kernel, threads, 0);
-    int blocks = sms * (per < 2 ? per : 2);
+    int blocks = sms * (per < 1 ? per : 1);
     if (blocks < 1) blocks = 1;
     Bar bar{reinterpret_cast<unsigned *>(c.flags + 4), reinterpret_cast<unsigned *>(c.flags + 5)};
     int *err = c.flags + 6;

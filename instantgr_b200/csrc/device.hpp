@@ -143,8 +143,9 @@ struct ColorDev {
     int npts = 0;
     int *map = nullptr;       // [X*Y]
     int *batch = nullptr;     // [n]
-    int *status = nullptr;    // [n]
-    int *active = nullptr, *active2 = nullptr;  // [n] each
+    // net lists, [n] each: nets without a batch (two buffers), candidates of a
+    // round, nets that lost a point in a round
+    int *active = nullptr, *active2 = nullptr, *cand = nullptr, *lost = nullptr;
     int *flags = nullptr;     // [16] device flags
     int rounds = 0;           // out: colouring rounds run
 };

@@ -293,16 +293,26 @@ void Router::plan_phase1(const std::vector<std::vector<int>> &batches, std::vect
             batch_off.push_back((int)net_ids.size());
             continue;
         }
-        std::vector<int> cls[3];
+        // class of a net: one class puts every net in the medium launch (tile 16,
+        // scratch beyond it); within a class, nets by node count, largest first,
+        // ties in batch order (a counting sort: node counts are small integers)
+        auto class_of = [&](int m) {
+            return tune.classes == 1 ? 1 : (m > kPatternNodeTile ? 0 : (m > tune.split ? 1 : 2));
+        };
+        int maxm = 0;
+        for (int id : b) maxm = std::max(maxm, nodes_of(id));
+        std::vector<int> cnt(3 * (size_t)(maxm + 2), 0);  // [class][maxm - m]
         for (int id : b) {
             const int m = nodes_of(id);
-            // one class: every net in the medium launch (tile 16, scratch beyond it)
-            cls[tune.classes == 1 ? 1 : (m > kPatternNodeTile ? 0 : (m > tune.split ? 1 : 2))].push_back(id);
+            cnt[(size_t)class_of(m) * (maxm + 2) + (maxm - m) + 1]++;
         }
-        for (int c = 0; c < 3; c++) {
-            std::stable_sort(cls[c].begin(), cls[c].end(), [&](int a, int bb) { return nodes_of(a) > nodes_of(bb); });
-            class_off.push_back((int)net_ids.size());
-            net_ids.insert(net_ids.end(), cls[c].begin(), cls[c].end());
+        const int base = (int)net_ids.size();
+        for (size_t i = 1; i < cnt.size(); i++) cnt[i] += cnt[i - 1];
+        for (int c = 0; c < 3; c++) class_off.push_back(base + cnt[(size_t)c * (maxm + 2)]);
+        net_ids.resize(base + b.size());
+        for (int id : b) {
+            const int m = nodes_of(id);
+            net_ids[base + cnt[(size_t)class_of(m) * (maxm + 2) + (maxm - m)]++] = id;
         }
         batch_off.push_back((int)net_ids.size());
     }
@@ -526,8 +536,7 @@ void Router::color_nets(const std::vector<int> &order, const ShapeDev &shapes, i
     d_rank.upload(rank, s);
     d_map.alloc((size_t)ns.X * ns.Y);
     d_bat.alloc(n);
-    d_sta.alloc(n);
-    d_act.alloc(2 * (size_t)n);
+    d_act.alloc(4 * (size_t)n);
     d_flags.alloc(16);
     st.h2d_bytes += (int64_t)(n + nshapes) * 4;
     if (sparsity != shapes.sparsity) throw Error(ERR_STATE, "claim lists were built for another sparsity");
@@ -537,8 +546,8 @@ void Router::color_nets(const std::vector<int> &order, const ShapeDev &shapes, i
     cd.pt_off = shapes.pt_off.p; cd.pts = shapes.pts.p; cd.pt_net = shapes.pt_net.p;
     cd.h_off = shapes.h_off.p; cd.hseg = shapes.hseg.p; cd.v_off = shapes.v_off.p; cd.vseg = shapes.vseg.p;
     cd.claim_off = shapes.claim_off.p; cd.claim = shapes.claim.p;
-    cd.active = d_act.p; cd.active2 = d_act.p + n;
-    cd.npts = shapes.npts; cd.map = d_map.p; cd.batch = d_bat.p; cd.status = d_sta.p; cd.flags = d_flags.p;
+    cd.active = d_act.p; cd.active2 = d_act.p + n; cd.cand = d_act.p + 2 * (size_t)n; cd.lost = d_act.p + 3 * (size_t)n;
+    cd.npts = shapes.npts; cd.map = d_map.p; cd.batch = d_bat.p; cd.flags = d_flags.p;
     kt.begin(KC_COLOR);
     int nb = run_coloring(cd, 0, s);
     kt.end(KC_COLOR);
