@@ -591,13 +591,15 @@ int igr_color_batches(igr_ctx *c, int n, const int32_t *pt_off, const int32_t *p
         ho.upload(h_off, n + 1, c->s); hs.upload(hseg, 2 * (size_t)h_off[n], c->s);
         vo.upload(v_off, n + 1, c->s); vs.upload(vseg, 2 * (size_t)v_off[n], c->s);
         dco.upload(co, c->s); dcl.upload(cl, c->s);
-        map.alloc(XY); bat.alloc(n); flags.alloc(16); act.alloc(4 * (size_t)n);
+        DevBuf<int4> hdr;
+        map.alloc(XY); bat.alloc(n); flags.alloc(16); act.alloc(4 * (size_t)n); hdr.alloc(n);
         ColorDev cd;
         cd.n = n; cd.X = c->go.g.X; cd.Y = c->go.g.Y; cd.sparsity = sparsity;
         cd.pt_off = po.p; cd.pts = p.p; cd.pt_net = pn.p; cd.h_off = ho.p; cd.hseg = hs.p; cd.v_off = vo.p;
         cd.vseg = vs.p; cd.npts = pt_off[n]; cd.map = map.p; cd.batch = bat.p; cd.flags = flags.p;
         cd.claim_off = dco.p; cd.claim = dcl.p;
         cd.active = act.p; cd.active2 = act.p + n; cd.cand = act.p + 2 * (size_t)n; cd.lost = act.p + 3 * (size_t)n;
+        cd.hdr = hdr.p;
         const int nb = run_coloring(cd, 0, c->s);
         if (nb == -2) throw Error(ERR_TIMEOUT, "colouring barrier timed out");
         if (nb < 0) throw Error(ERR_CUDA, std::string("colouring launch failed: ") + cudaGetErrorString(cudaGetLastError()));

@@ -11,180 +11,256 @@
 //
 // The reference is nondeterministic (a claiming thread re-reads the cell right
 // after its atomicMax while others are still writing, and returns early).
-// Here claiming, committing, blocking and releasing are separate phases
-// separated by grid barriers, so the batches depend only on the input.
+// Here claiming, committing and blocking are separate phases separated by
+// grid barriers, so the batches depend only on the input.
 //
 // Work layout: the cells a net claims are precomputed once (claim lists, CSR
-// per shape), one warp handles one net with its lanes over the net's claims
-// or points, and only nets still without a batch are visited: the list of
-// active nets is compacted after every batch.  The whole colouring is one
-// persistent cooperative kernel; the grid barrier gives up after two seconds
+// per shape) and gathered per rank into one 16-byte header; a group of 8 lanes
+// handles one net.  Each round walks only the nets it concerns: the
+// candidates (claim, commit) and the nets that lost a point (block); the lists
+// are rebuilt every phase with one global atomic per block (appends are staged
+// in shared memory).  The whole colouring is one persistent cooperative
+// kernel; the last rounds of a batch, which have few candidates, run in one
+// block with block barriers.  Every grid barrier gives up after two seconds
 // and reports ERR_TIMEOUT instead of waiting forever.
-#include "kcommon.cuh"
+#include "gridsync.cuh"
 
 namespace igr {
 
 namespace {
 
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
+constexpr int kThreads = 1024;
+constexpr int kG = 8;                          // lanes per net
+constexpr int kGroups = kThreads / kG;         // groups per block
+constexpr unsigned kGroupMask = (1u << kG) - 1;
+constexpr int kBuf = 4096;                     // staged list entries per block
+// rounds with at most this many candidates run in block 0 alone (two nets per
+// group and phase at most)
+constexpr int kBlockRounds = 2 * kGroups;
 
-struct Bar {
-    unsigned *count;
-    unsigned *gen;
+// flags (ints): [2] batches, [4] barrier counter, [6] error, [8] rounds run,
+// [9] lost count, [10] next candidate count, [11..12] nets left after a batch
+// (by batch parity)
+enum : int { F_NB = 2, F_BAR = 4, F_ERR = 6, F_ROUNDS = 8, F_LOST = 9, F_CAND = 10, F_LEFT = 11 };
+
+struct Stage {
+    int buf[kBuf];
+    int n, base;
 };
 
-// returns false when the barrier timed out or another block reported an error
-__device__ bool grid_barrier(Bar b, int *err) {
-    __syncthreads();
-    __shared__ int s_ok;
-    if (threadIdx.x == 0) {
-        s_ok = 1;
-        volatile unsigned *vgen = b.gen;
-        const unsigned g = *vgen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(b.count, 1u);
-        if (arrived == gridDim.x - 1) {
-            *b.count = 0;
-            __threadfence();
-            atomicAdd(b.gen, 1u);
-        } else {
-            const unsigned long long t0 = global_ns();
-            while (*vgen == g) {
-                if (*(volatile int *)err) { s_ok = 0; break; }
-                if (global_ns() - t0 > 2000000000ull) { set_error(err, ERR_TIMEOUT); s_ok = 0; break; }
-                __nanosleep(32);
-            }
-        }
-        __threadfence();
-        if (*(volatile int *)err) s_ok = 0;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
-
-constexpr int kG = 8;                 // lanes per net
-constexpr int kNetsPerWarp = 32 / kG;
-constexpr unsigned kGroupMask = (1u << kG) - 1;
-
-// flags (ints): [0..1] commit seen in a round (by round parity), [2] batches,
-// [4..5] barrier, [6] error, [8] rounds run, [9] lost count, [10] next
-// candidate count, [11..12] nets left after a batch (by batch parity)
-enum : int { F_ROUND = 0, F_NB = 2, F_ERR = 6, F_ROUNDS = 8, F_LOST = 9, F_CAND = 10, F_LEFT = 11 };
-
-// Appends `k` of every group leader with `want` set to list[*count++]; called
-// by all 32 lanes of the warp with the same control flow.
-__device__ __forceinline__ void warp_append(int *list, int *count, bool want, int k, int lane) {
+// Stages `k` of every lane with `want` set; called by all 32 lanes of a warp.
+__device__ __forceinline__ void stage(Stage &st, bool want, int k, int lane) {
     const unsigned m = __ballot_sync(0xffffffffu, want);
     if (!m) return;
     int base = 0;
-    if (lane == 0) base = atomicAdd(count, __popc(m));
+    if (lane == 0) base = atomicAdd(&st.n, __popc(m));
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (want) list[base + __popc(m & ((1u << lane) - 1))] = k;
+    if (want) st.buf[base + __popc(m & ((1u << lane) - 1))] = k;
+}
+
+// Appends the staged entries to list[*count ...]; every thread of the block calls it.
+__device__ __forceinline__ void flush(Stage &st, int *list, int *count) {
+    __syncthreads();
+    const int m = st.n;
+    if (threadIdx.x == 0 && m > 0) st.base = atomicAdd(count, m);
+    __syncthreads();
+    if (m > 0) {
+        const int b = st.base;
+        for (int i = threadIdx.x; i < m; i += blockDim.x) list[b + i] = st.buf[i];
+    }
+    if (threadIdx.x == 0) st.n = 0;
+    __syncthreads();
+}
+
+// map and batch change during the kernel: read them from L2
+__device__ __forceinline__ int owner(const ColorDev &c, int cell) { return __ldcg(c.map + cell); }
+
+// Candidates claim their cells, four cells in flight per lane.  Blocks blk,
+// blk+nblk, ... of the workers; group j of a block takes list entry j.
+__device__ __forceinline__ void claim_phase(const ColorDev &c, const int *list, int n, int blk, int nblk) {
+    const int gl = threadIdx.x % kG;
+    for (int idx = blk * kGroups + threadIdx.x / kG; idx < n; idx += nblk * kGroups) {
+        const int k = list[idx];
+        const int4 h = c.hdr[k];
+        for (int i = h.x + gl; i < h.y; i += 4 * kG) {
+            const int c0 = __ldg(c.claim + i);
+            const int c1 = i + kG < h.y ? __ldg(c.claim + i + kG) : -1;
+            const int c2 = i + 2 * kG < h.y ? __ldg(c.claim + i + 2 * kG) : -1;
+            const int c3 = i + 3 * kG < h.y ? __ldg(c.claim + i + 3 * kG) : -1;
+            atomicMax(c.map + c0, k);
+            if (c1 >= 0) atomicMax(c.map + c1, k);
+            if (c2 >= 0) atomicMax(c.map + c2, k);
+            if (c3 >= 0) atomicMax(c.map + c3, k);
+        }
+    }
+}
+
+// Candidates owning all their points join batch `cur`; the others go to the
+// lost list.  Block-uniform loop (staging and flushes).
+__device__ __forceinline__ void commit_phase(const ColorDev &c, Stage &st, const int *list, int n, int cur,
+                                             int *lost_cnt, int blk, int nblk) {
+    const int lane = threadIdx.x & 31, grp = lane / kG, gl = lane % kG;
+    int it = 0;
+    for (int b0 = blk * kGroups; b0 < n; b0 += nblk * kGroups, it++) {
+        const int idx = b0 + threadIdx.x / kG;
+        const bool valid = idx < n;
+        const int k = valid ? list[idx] : -1;
+        bool ok = true;
+        if (valid) {
+            const int4 h = c.hdr[k];
+            for (int i = h.z + gl; i < h.w; i += 2 * kG) {
+                const int p0 = __ldg(c.pts + i);
+                const int p1 = i + kG < h.w ? __ldg(c.pts + i + kG) : -1;
+                const int o0 = owner(c, p0);
+                const int o1 = p1 >= 0 ? owner(c, p1) : k;
+                ok &= (o0 == k) & (o1 == k);
+            }
+        }
+        const unsigned bad = (__ballot_sync(0xffffffffu, !ok) >> (grp * kG)) & kGroupMask;
+        if (valid && bad == 0 && gl == 0) c.batch[k] = cur;
+        stage(st, valid && bad != 0 && gl == 0, k, lane);
+        if ((it + 1) % (kBuf / kGroups) == 0) flush(st, c.lost, lost_cnt);
+    }
+    flush(st, c.lost, lost_cnt);
+}
+
+// Lost nets with a point owned by a member are blocked and release their
+// cells at once (a blocked net's cells are no member's points, so the release
+// cannot change another net's check); the others stay candidates.
+__device__ __forceinline__ void block_phase(const ColorDev &c, Stage &st, int n, int *cand_cnt, int blk, int nblk) {
+    const int lane = threadIdx.x & 31, grp = lane / kG, gl = lane % kG;
+    int it = 0;
+    for (int b0 = blk * kGroups; b0 < n; b0 += nblk * kGroups, it++) {
+        const int idx = b0 + threadIdx.x / kG;
+        const bool valid = idx < n;
+        const int k = valid ? c.lost[idx] : -1;
+        int4 h = make_int4(0, 0, 0, 0);
+        bool hit = false;
+        if (valid) {
+            h = c.hdr[k];
+            for (int i = h.z + gl; i < h.w; i += 2 * kG) {
+                const int p0 = __ldg(c.pts + i);
+                const int p1 = i + kG < h.w ? __ldg(c.pts + i + kG) : -1;
+                const int o0 = owner(c, p0);
+                const int o1 = p1 >= 0 ? owner(c, p1) : -1;
+                const int b0v = o0 != -1 ? __ldcg(c.batch + o0) : -1;
+                const int b1v = o1 != -1 ? __ldcg(c.batch + o1) : -1;
+                hit |= (b0v != -1) | (b1v != -1);
+            }
+        }
+        const bool blocked = ((__ballot_sync(0xffffffffu, hit) >> (grp * kG)) & kGroupMask) != 0;
+        if (valid && blocked) {
+            for (int i = h.x + gl; i < h.y; i += 4 * kG) {
+                int cl[4], ow[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) cl[u] = i + u * kG < h.y ? __ldg(c.claim + i + u * kG) : -1;
+#pragma unroll
+                for (int u = 0; u < 4; u++) ow[u] = cl[u] >= 0 ? owner(c, cl[u]) : -1;
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (ow[u] == k) c.map[cl[u]] = -1;
+            }
+        }
+        stage(st, valid && !blocked && gl == 0, k, lane);
+        if ((it + 1) % (kBuf / kGroups) == 0) flush(st, c.cand, cand_cnt);
+    }
+    flush(st, c.cand, cand_cnt);
+}
+
+// Rounds `round`.. of batch `cur` in this block alone, over the nc candidates
+// in c.cand.  Every thread of the block calls it.
+__device__ void block_rounds(const ColorDev &c, Stage &st, int round, int nc, int cur, int *rounds_ctr) {
+    __shared__ int s_lost, s_cand;
+    for (; round < 30; round++) {
+        if (threadIdx.x == 0) {
+            s_lost = 0;
+            s_cand = 0;
+            (*rounds_ctr)++;
+        }
+        __syncthreads();
+        claim_phase(c, c.cand, nc, 0, 1);
+        __syncthreads();
+        commit_phase(c, st, c.cand, nc, cur, &s_lost, 0, 1);
+        const int nl = s_lost;  // flush ends with a block barrier
+        if (nl == nc) break;    // no net joined in this round
+        block_phase(c, st, nl, &s_cand, 0, 1);
+        nc = s_cand;
+        __syncthreads();  // every thread has read the counters before they are reset
+        if (nc == 0) break;
+    }
 }
 
 // Per batch: candidates claim (atomicMax of their rank on their claim cells),
-// candidates owning all their points join, the others are blocked when a
-// member owns one of their points (and release their cells at once; a blocked
-// net's cells are no member's points, so the release cannot change another
-// net's check), else they stay candidates.  Three grid barriers per round.
-// The lists are unordered: every phase is order-independent.
-__global__ void __launch_bounds__(1024, 1) coloring_kernel(ColorDev c, Bar bar, int *err, int max_batches) {
+// candidates owning all their points join, lost nets are blocked or stay
+// candidates.  Three grid barriers per round; the last rounds of a batch,
+// with few candidates, run in block 0 alone.  The lists are unordered: every
+// phase is order-independent.
+__global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int max_batches) {
+    __shared__ Stage st;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nth = gridDim.x * blockDim.x;
-    const int lane = threadIdx.x & 31, grp = lane / kG, gl = lane % kG;
-    const int gw = tid >> 5, nw = nth >> 5;
+    const int lane = threadIdx.x & 31;
     const int XY = c.X * c.Y;
     int *flags = c.flags;
     volatile int *vflags = c.flags;
+    unsigned *bar = reinterpret_cast<unsigned *>(c.flags + F_BAR);
+    int *err = c.flags + F_ERR;
+    unsigned epoch = 0;
+    if (threadIdx.x == 0) st.n = 0;
     int *act = c.active, *act2 = c.active2;
-    for (int i = tid; i < c.n; i += nth) act[i] = i;
+    for (int k = tid; k < c.n; k += nth) {
+        const int sh = c.perm ? c.perm[k] : k;
+        c.hdr[k] = make_int4(c.claim_off[sh], c.claim_off[sh + 1], c.pt_off[sh], c.pt_off[sh + 1]);
+        act[k] = k;
+    }
     for (int i = tid; i < XY; i += nth) c.map[i] = -1;
-    if (!grid_barrier(bar, err)) return;
+    if (!grid_sync(bar, err, epoch)) return;
     int na = c.n;
     for (int cur = 0; cur < max_batches; cur++) {
         const int *cand = act;  // round 0: every net without a batch
         int nc = na;
-        for (int round = 0; round < 30; round++) {
-            // claim
+        int round = 0;
+        bool tail = false;
+        for (; round < 30; round++) {
+            if (round > 0 && nc <= kBlockRounds) {
+                tail = true;
+                break;
+            }
             if (tid == 0) {
                 flags[F_ROUNDS]++;
                 flags[F_LOST] = 0;
-                flags[F_ROUND + ((round + 1) & 1)] = 0;
             }
-            for (int base = gw * kNetsPerWarp; base < nc; base += nw * kNetsPerWarp) {
-                const int idx = base + grp;
-                if (idx >= nc) continue;
-                const int k = cand[idx];
-                const int sh = c.perm ? c.perm[k] : k;
-                const int e = c.claim_off[sh + 1];
-                for (int i = c.claim_off[sh] + gl; i < e; i += kG) atomicMax(&c.map[c.claim[i]], k);
-            }
-            if (!grid_barrier(bar, err)) return;
-            // commit: members own every point; the others go to the lost list
+            claim_phase(c, cand, nc, blockIdx.x, gridDim.x);
+            if (!grid_sync(bar, err, epoch)) return;
             if (tid == 0) {
                 flags[F_CAND] = 0;
                 if (round == 0) flags[F_LEFT + ((cur + 1) & 1)] = 0;
             }
-            for (int base = gw * kNetsPerWarp; base < nc; base += nw * kNetsPerWarp) {
-                const int idx = base + grp;
-                const bool valid = idx < nc;
-                const int k = valid ? cand[idx] : -1;
-                bool ok = true;
-                if (valid) {
-                    const int sh = c.perm ? c.perm[k] : k;
-                    const int e = c.pt_off[sh + 1];
-                    for (int i = c.pt_off[sh] + gl; i < e; i += kG) ok &= c.map[c.pts[i]] == k;
-                }
-                const unsigned bad = (__ballot_sync(0xffffffffu, !ok) >> (grp * kG)) & kGroupMask;
-                if (valid && bad == 0 && gl == 0) {
-                    c.batch[k] = cur;
-                    flags[F_ROUND + (round & 1)] = 1;
-                }
-                warp_append(c.lost, flags + F_LOST, valid && bad != 0 && gl == 0, k, lane);
-            }
-            if (!grid_barrier(bar, err)) return;
-            if (!vflags[F_ROUND + (round & 1)]) break;
-            // block (and release) or stay a candidate
+            commit_phase(c, st, cand, nc, cur, flags + F_LOST, blockIdx.x, gridDim.x);
+            if (!grid_sync(bar, err, epoch)) return;
             const int nl = vflags[F_LOST];
-            for (int base = gw * kNetsPerWarp; base < nl; base += nw * kNetsPerWarp) {
-                const int idx = base + grp;
-                const bool valid = idx < nl;
-                const int k = valid ? c.lost[idx] : -1;
-                const int sh = valid ? (c.perm ? c.perm[k] : k) : 0;
-                bool hit = false;
-                if (valid) {
-                    const int e = c.pt_off[sh + 1];
-                    for (int i = c.pt_off[sh] + gl; i < e; i += kG) {
-                        const int pre = c.map[c.pts[i]];
-                        hit |= (pre != -1 && c.batch[pre] != -1);
-                    }
-                }
-                const bool blocked = ((__ballot_sync(0xffffffffu, hit) >> (grp * kG)) & kGroupMask) != 0;
-                if (valid && blocked) {
-                    const int e = c.claim_off[sh + 1];
-                    for (int i = c.claim_off[sh] + gl; i < e; i += kG)
-                        if (c.map[c.claim[i]] == k) c.map[c.claim[i]] = -1;
-                }
-                warp_append(c.cand, flags + F_CAND, valid && !blocked && gl == 0, k, lane);
-            }
-            if (!grid_barrier(bar, err)) return;
+            if (nl == nc) break;  // no net joined in this round
+            block_phase(c, st, nl, flags + F_CAND, blockIdx.x, gridDim.x);
+            if (!grid_sync(bar, err, epoch)) return;
             cand = c.cand;
             nc = vflags[F_CAND];
             if (nc == 0) break;
         }
+        if (tail) {
+            if (blockIdx.x == 0) block_rounds(c, st, round, nc, cur, flags + F_ROUNDS);
+            if (!grid_sync(bar, err, epoch)) return;
+        }
         // nets still without a batch stay active; the map is cleared for the next batch
         for (int i = tid; i < XY; i += nth) c.map[i] = -1;
-        if (tid == 0) flags[F_ROUND] = flags[F_ROUND + 1] = 0;
-        for (int base = gw * 32; base < na; base += nw * 32) {
-            const int i = base + lane;
+        int it = 0;
+        for (int b0 = blockIdx.x * kThreads; b0 < na; b0 += nth, it++) {
+            const int i = b0 + threadIdx.x;
             const int k = i < na ? act[i] : -1;
-            warp_append(act2, flags + F_LEFT + (cur & 1), k >= 0 && c.batch[k] == -1, k, lane);
+            stage(st, k >= 0 && __ldcg(c.batch + k) == -1, k, lane);
+            if ((it + 1) % (kBuf / kThreads) == 0) flush(st, act2, flags + F_LEFT + (cur & 1));
         }
-        if (!grid_barrier(bar, err)) return;
+        flush(st, act2, flags + F_LEFT + (cur & 1));
+        if (!grid_sync(bar, err, epoch)) return;
         na = vflags[F_LEFT + (cur & 1)];
         int *t = act; act = act2; act2 = t;
         if (na == 0) {
@@ -228,24 +304,21 @@ int run_coloring(ColorDev &c, int max_batch, cudaStream_t s) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int threads = 1024;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coloring_kernel, threads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coloring_kernel, kThreads, 0);
     int blocks = sms * (per < 1 ? per : 1);
     if (blocks < 1) blocks = 1;
-    Bar bar{reinterpret_cast<unsigned *>(c.flags + 4), reinterpret_cast<unsigned *>(c.flags + 5)};
-    int *err = c.flags + 6;
     cudaMemsetAsync(c.flags, 0, 16 * sizeof(int), s);
     cudaMemsetAsync(c.batch, 0xff, sizeof(int) * (size_t)c.n, s);
     int max_batches = c.n + 1;
-    void *args[] = {&c, &bar, &err, &max_batches};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void *)coloring_kernel, dim3(blocks), dim3(threads), args, 0, s);
+    void *args[] = {&c, &max_batches};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void *)coloring_kernel, dim3(blocks), dim3(kThreads), args, 0, s);
     if (e != cudaSuccess) return -1;
     int h[16];
     if (cudaMemcpyAsync(h, c.flags, sizeof h, cudaMemcpyDeviceToHost, s) != cudaSuccess) return -1;
     if (cudaStreamSynchronize(s) != cudaSuccess) return -1;
-    if (h[6] != 0) return -2;
-    c.rounds = h[8];
-    return h[2];
+    if (h[F_ERR] != 0) return -2;
+    c.rounds = h[F_ROUNDS];
+    return h[F_NB];
 }
 
 }  // namespace igr

@@ -14,7 +14,7 @@
 // waiting forever.  Emitted segments are staged per DAG node and compacted in
 // node order, so route records do not depend on atomic ordering (the
 // reference appends them with atomicAdd).
-#include "kcommon.cuh"
+#include "gridsync.cuh"
 
 namespace igr {
 
@@ -22,45 +22,6 @@ namespace {
 
 constexpr int kML = 10;                      // MAX_LAYER of the reference
 constexpr unsigned long long kInitPacked = 7208259049189261824ULL;  // init_cost_with_road
-
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-struct Bar {
-    unsigned *count;
-    unsigned *gen;
-};
-
-__device__ bool grid_barrier(Bar b, int *err) {
-    __syncthreads();
-    __shared__ int s_ok;
-    if (threadIdx.x == 0) {
-        s_ok = 1;
-        volatile unsigned *vgen = b.gen;
-        const unsigned g = *vgen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(b.count, 1u);
-        if (arrived == gridDim.x - 1) {
-            *b.count = 0;
-            __threadfence();
-            atomicAdd(b.gen, 1u);
-        } else {
-            const unsigned long long t0 = global_ns();
-            while (*vgen == g) {
-                if (*(volatile int *)err) { s_ok = 0; break; }
-                if (global_ns() - t0 > 2000000000ull) { set_error(err, ERR_TIMEOUT); s_ok = 0; break; }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-        if (*(volatile int *)err) s_ok = 0;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
 
 __device__ __forceinline__ int32_t f2o(float f) {
     int32_t i = __float_as_int(f);
@@ -314,15 +275,16 @@ __device__ void trace_node(const GridDev &g, const DagBatchDev &b, int node, int
     if (mnl < mxl) stage2(b, node, (mnl - 1) * XY + cx * Y + cy, (mxl - 1) * XY + cx * Y + cy, g.err);
 }
 
-__global__ void dag_levels_kernel(GridDev g, DagBatchDev b, Bar bar, int stamp) {
+__global__ void dag_levels_kernel(GridDev g, DagBatchDev b, unsigned *bar, int stamp) {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    unsigned epoch = 0;
     for (int d = b.depth - 1; d >= 0; d--) {
         for (int s = b.level_off[d] + tid; s < b.level_off[d + 1]; s += nth) dp_node(g, b, b.level_nodes[s]);
-        if (!grid_barrier(bar, g.err)) return;
+        if (!grid_sync(bar, g.err, epoch)) return;
     }
     for (int d = 0; d < b.depth; d++) {
         for (int s = b.level_off[d] + tid; s < b.level_off[d + 1]; s += nth) trace_node(g, b, b.level_nodes[s], stamp);
-        if (!grid_barrier(bar, g.err)) return;
+        if (!grid_sync(bar, g.err, epoch)) return;
     }
 }
 
@@ -394,7 +356,7 @@ int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, unsigned
         const int need = (int)((b.max_level + 255) / 256);
         if (need < blocks) blocks = need < 1 ? 1 : need;
         cudaMemsetAsync(bar_words, 0, 2 * sizeof(unsigned), s);
-        Bar bar{bar_words, bar_words + 1};
+        unsigned *bar = bar_words;
         GridDev gg = g;
         DagBatchDev bb = b;
         void *args[] = {&gg, &bb, &bar, &stamp};

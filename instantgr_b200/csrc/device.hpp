@@ -146,6 +146,7 @@ struct ColorDev {
     // net lists, [n] each: nets without a batch (two buffers), candidates of a
     // round, nets that lost a point in a round
     int *active = nullptr, *active2 = nullptr, *cand = nullptr, *lost = nullptr;
+    int4 *hdr = nullptr;      // [n] per rank: claim begin/end, point begin/end
     int *flags = nullptr;     // [16] device flags
     int rounds = 0;           // out: colouring rounds run
 };

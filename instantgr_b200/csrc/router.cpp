@@ -537,6 +537,7 @@ void Router::color_nets(const std::vector<int> &order, const ShapeDev &shapes, i
     d_map.alloc((size_t)ns.X * ns.Y);
     d_bat.alloc(n);
     d_act.alloc(4 * (size_t)n);
+    d_hdr.alloc(n);
     d_flags.alloc(16);
     st.h2d_bytes += (int64_t)(n + nshapes) * 4;
     if (sparsity != shapes.sparsity) throw Error(ERR_STATE, "claim lists were built for another sparsity");
@@ -547,6 +548,7 @@ void Router::color_nets(const std::vector<int> &order, const ShapeDev &shapes, i
     cd.h_off = shapes.h_off.p; cd.hseg = shapes.hseg.p; cd.v_off = shapes.v_off.p; cd.vseg = shapes.vseg.p;
     cd.claim_off = shapes.claim_off.p; cd.claim = shapes.claim.p;
     cd.active = d_act.p; cd.active2 = d_act.p + n; cd.cand = d_act.p + 2 * (size_t)n; cd.lost = d_act.p + 3 * (size_t)n;
+    cd.hdr = d_hdr.p;
     cd.npts = shapes.npts; cd.map = d_map.p; cd.batch = d_bat.p; cd.flags = d_flags.p;
     kt.begin(KC_COLOR);
     int nb = run_coloring(cd, 0, s);

@@ -124,6 +124,7 @@ struct Router {
     std::vector<int> h_routes;  // host copy, made on demand
     bool h_routes_valid = false;
     // ---- per-run device buffers (grow-only)
+    DevBuf<int4> d_hdr;
     DevBuf<int> d_ids, d_all_ids, of_sum, d_perm, d_rank, d_map, d_bat, d_act, d_flags, d_queue;
     // launch shape of the tree DP per size class (large, medium, small) and the
     // node count that separates small from medium nets (autotuned, see tune.cpp)
