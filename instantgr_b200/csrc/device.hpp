@@ -55,15 +55,21 @@ struct TreeBatchDev {
     int *routes;             // route records
     double *scratch;         // per-node DP tables of nets larger than the shared-memory tile
     const int64_t *scratch_off;  // [routing nets] offset (in nodes) into scratch, -1 for nets that fit on chip
-    int64_t scratch_nodes;   // nodes covered by scratch: 81 doubles each, then 46 ints each
+    int64_t scratch_nodes;   // nodes covered by scratch: kPatternScratchD doubles each, then kPatternScratchI ints each
     int n;
     const int *order = nullptr;  // [n] positions into net_ids in processing order (null: 0..n-1)
     int *queue = nullptr;        // work counter of this launch (zero before the launch)
     int lanes_per_net = 32;      // 16 or 32
     int tile = 16;               // nodes kept on chip: 6, 16, or 1 (all in scratch)
 };
+// scratch per node of a net kept in global memory: 45 range costs and 36
+// prefetched edge costs (doubles), then 8 via-column costs (floats), 45
+// backtrace codes, the chosen range and 4 decoded position/parent ints
+constexpr int kPatternScratchD = 81, kPatternScratchI = 8 + 45 + 1 + 4;
 // doubles of scratch needed for `nodes` nodes of nets kept in global memory
-inline int64_t pattern_scratch_doubles(int64_t nodes) { return nodes * 81 + (nodes * 46 + 1) / 2; }
+inline int64_t pattern_scratch_doubles(int64_t nodes) {
+    return nodes * kPatternScratchD + (nodes * kPatternScratchI + 1) / 2;
+}
 constexpr int kPatternNodeTile = 16;  // nets with more nodes use global scratch
 void launch_pattern_route(const GridDev &g, const TreeBatchDev &b, int stamp, cudaStream_t s);
 

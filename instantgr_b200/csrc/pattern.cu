@@ -31,6 +31,7 @@ namespace {
 constexpr int kL = kRouteL;                  // 9 routing layers
 constexpr int kR = 45;                       // layer ranges minl <= maxl
 constexpr int kPF = 36;                      // prefetched doubles per edge
+constexpr int kCol = kL - 1;                 // via column per node: vcost of layers 0..7
 
 __host__ __device__ constexpr int tri(int a, int b) { return a * 9 - a * (a - 1) / 2 + (b - a); }
 
@@ -38,8 +39,10 @@ template <int T>
 struct GroupSmem {
     double dist[T * kR];
     double pf[(T > 1 ? T - 1 : 1) * kPF];
+    float col[T * kCol];
     int from[T * kR];
     int lr[T];
+    int nx[T], ny[T], nl[T], np[T];  // decoded node position and parent
     double costc[kL], diag[kL];
     int cf[kL], pdiag[kL];
 };
@@ -95,29 +98,47 @@ __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatch
         const int *nodes = b.nodes + nb;
         const int *par = b.par + nb;
         double *dist, *pf;
-        int *from, *lr;
+        float *col;
+        int *from, *lr, *nx, *ny, *nl, *np;
         if (n <= kNodeTile) {
-            dist = sm.dist; pf = sm.pf; from = sm.from; lr = sm.lr;
+            dist = sm.dist; pf = sm.pf; col = sm.col; from = sm.from; lr = sm.lr;
+            nx = sm.nx; ny = sm.ny; nl = sm.nl; np = sm.np;
         } else {
             const int64_t so = b.scratch_off[net];
             if (so < 0 || so + n > b.scratch_nodes) {
                 if (gl == 0) set_error(g.err, so < 0 ? ERR_STATE : ERR_CAPACITY);
                 continue;
             }
-            dist = b.scratch + so * (kR + kPF);
+            dist = b.scratch + so * kPatternScratchD;
             pf = dist + (int64_t)n * kR;
-            from = reinterpret_cast<int *>(b.scratch + b.scratch_nodes * (kR + kPF)) + so * (kR + 1);
+            int *ib = reinterpret_cast<int *>(b.scratch + b.scratch_nodes * kPatternScratchD) + so * kPatternScratchI;
+            col = reinterpret_cast<float *>(ib);
+            from = ib + (int64_t)n * kCol;
             lr = from + (int64_t)n * kR;
+            nx = lr + n; ny = nx + n; nl = ny + n; np = nl + n;
         }
-        // ---- 1a. via-stack cost of every node and layer range (Lshape_route.hpp:22-32)
+        // ---- 0. node positions and parents, decoded once
+        for (int i = gl; i < n; i += G) {
+            const int v = nodes[i];
+            const int l = v / XY, r = v - l * XY, x = r / Y;
+            nx[i] = x; ny[i] = r - x * Y; nl[i] = l; np[i] = par[i];
+        }
+        __syncwarp(gmask);
+        // ---- 1a. via columns of all nodes, every load in flight at once, then the
+        //          via-stack cost of every node and layer range (Lshape_route.hpp:22-32)
+        for (int p = gl; p < n * kCol; p += G) {
+            const int i = p / kCol;
+            col[p] = g.vcost[cell_at(g, p - i * kCol, nx[i], ny[i])];
+        }
+        __syncwarp(gmask);
         for (int p = gl; p < n * kL; p += G) {
             const int i = p / kL, mn = p % kL;
-            const int v = nodes[i];
-            const int l = v / XY, x = v / Y % X, y = v % Y;
+            const int l = nl[i];
+            const float *cc = col + i * kCol;
             double acc = 0;
             dist[i * kR + tri(mn, mn)] = (l < kL && l != mn) ? kInf : 0.0;
             for (int mx = mn + 1; mx < kL; mx++) {
-                acc = acc + (double)g.vcost[cell_at(g, mx - 1, x, y)];
+                acc = acc + (double)cc[mx - 1];
                 dist[i * kR + tri(mn, mx)] = (l < kL && (mn > l || mx < l)) ? kInf : acc;
             }
         }
@@ -126,10 +147,9 @@ __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatch
         //          [27,36) via column at (px, y)
         for (int t = gl; t < (n - 1) * kPF; t += G) {
             const int e = t / kPF, j = t % kPF, i = e + 1;
-            const int pi = par[i];
+            const int pi = np[i];
             if (pi < 0 || pi >= i) continue;  // reported below
-            const int v = nodes[i], pv = nodes[pi];
-            const int x = v / Y % X, y = v % Y, px = pv / Y % X, py = pv % Y;
+            const int x = nx[i], y = ny[i], px = nx[pi], py = ny[pi];
             const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
             const bool straight = (x == px || y == py);
             double val = 0;
@@ -157,10 +177,9 @@ __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatch
         // ---- 2. bottom-up over tree edges (Lshape_route.hpp:33-97)
         bool bad = false;
         for (int i = n - 1; i >= 1; i--) {
-            const int pi = par[i];
+            const int pi = np[i];
             if (pi < 0 || pi >= i) { bad = true; break; }
-            const int v = nodes[i], pv = nodes[pi];
-            const int x = v / Y % X, y = v % Y, px = pv / Y % X, py = pv % Y;
+            const int x = nx[i], y = ny[i], px = nx[pi], py = ny[pi];
             const double *nd = dist + i * kR;
             double *pd = dist + pi * kR;
             int *prev = from + i * kR;
@@ -267,11 +286,10 @@ __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatch
         r[cnt++] = (B);                                    \
     } while (0)
             for (int i = 0; i < n && ok; i++) {
-                const int v = nodes[i];
-                const int x = v / Y % X, y = v % Y;
+                const int x = nx[i], y = ny[i];
                 int code = 0;
                 if (i > 0) {
-                    const int plr = lr[par[i]];
+                    const int plr = lr[np[i]];
                     code = from[i * kR + tri(plr / kL, plr % kL)];
                     lr[i] = code / (kL * kL);
                 }
@@ -279,8 +297,7 @@ __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatch
                 if (mn > mx || !(dist[i * kR + tri(mn, mx)] < kInf)) { set_error(g.err, ERR_STATE); ok = false; break; }
                 if (mn < mx) EMIT(mn * XY + x * Y + y, mx * XY + x * Y + y);
                 if (!ok || i == 0) continue;
-                const int pv = nodes[par[i]];
-                const int px = pv / Y % X, py = pv % Y;
+                const int px = nx[np[i]], py = ny[np[i]];
                 const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
                 const int curl = code / kL % kL, parl = code % kL;
                 if (px == x || py == y) {
@@ -332,14 +349,15 @@ void launch_g(const GridDev &g, const TreeBatchDev &b, int stamp, cudaStream_t s
 
 }  // namespace
 
-// Tile sizes (nodes kept on chip per group) compiled in: 6 (two- and three-pin
-// nets), 16, and 1 (every net in global scratch).
+// Tile sizes (nodes kept on chip per group) compiled in: 6 (small nets), 16,
+// 32 (32 lanes only) and 1 (every net in global scratch).
 void launch_pattern_route(const GridDev &g, const TreeBatchDev &b, int stamp, cudaStream_t s) {
     if (b.n <= 0) return;
     const bool half = b.lanes_per_net == 16;
     switch (b.tile) {
         case 6: half ? launch_g<16, 6>(g, b, stamp, s) : launch_g<32, 6>(g, b, stamp, s); break;
         case 1: half ? launch_g<16, 1>(g, b, stamp, s) : launch_g<32, 1>(g, b, stamp, s); break;
+        case 32: launch_g<32, 32>(g, b, stamp, s); break;
         default: half ? launch_g<16, 16>(g, b, stamp, s) : launch_g<32, 16>(g, b, stamp, s); break;
     }
 }

@@ -136,6 +136,11 @@ Router::~Router() {
     kt.collect();
     if (graph1_exec) cudaGraphExecDestroy(graph1_exec);
     if (ev0) cudaEventDestroy(ev0);
+    for (int i = 0; i < 2; i++) {
+        if (ev_join[i]) cudaEventDestroy(ev_join[i]);
+        if (s_cls[i]) cudaStreamDestroy(s_cls[i]);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev1) cudaEventDestroy(ev1);
     if (s) cudaStreamDestroy(s);
 }
@@ -182,6 +187,11 @@ void Router::open(const char *cap, const char *net) {
 void Router::ensure_device() {
     if (s) return;
     cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+    for (int i = 0; i < 2; i++) {
+        cuda_check(cudaStreamCreateWithFlags(&s_cls[i], cudaStreamNonBlocking), "stream");
+        cuda_check(cudaEventCreateWithFlags(&ev_join[i], cudaEventDisableTiming), "event");
+    }
+    cuda_check(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming), "event");
     cuda_check(cudaEventCreate(&ev0), "event");
     cuda_check(cudaEventCreate(&ev1), "event");
     const int L = d.L - 1, X = d.X, Y = d.Y;
@@ -329,6 +339,10 @@ void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<in
         launch_cost_refresh(go.g, true, s);
         if (timed) kt.end(KC_COST);
         if (timed) kt.begin(KC_PATTERN);
+        // batched form: the large (c = 0) and small (c = 2) classes are forked
+        // onto their own streams and run beside the medium class (c = 1)
+        bool forked[3] = {false, false, false};
+        if (batched) cuda_check(cudaEventRecord(ev_fork, s), "event");
         for (int c = 0; c < 3; c++) {
             const int a = class_off[3 * bi + c];
             const int e = c < 2 ? class_off[3 * bi + c + 1] : batch_off[bi + 1];
@@ -336,15 +350,27 @@ void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<in
             TreeBatchDev tb{d_ids.p + a, d_tree_off.p, d_tree_nodes.p, d_tree_par.p, d_route_off.p, d_route_cap.p,
                             routes.p, d_scratch.p, d_scratch_off.p, scratch_nodes, e - a};
             tb.queue = d_queue.p + 3 * bi + c;
+            cudaStream_t cs = s;
             if (batched) {
-                tb.tile = c == 0 ? 1 : (c == 1 ? kPatternNodeTile : 6);
+                tb.tile = c == 0 ? 32 : (c == 1 ? kPatternNodeTile : 6);
                 tb.lanes_per_net = tune.lanes[c];
+                if (c != 1) {
+                    cs = s_cls[c == 0 ? 0 : 1];
+                    cuda_check(cudaStreamWaitEvent(cs, ev_fork, 0), "fork");
+                    forked[c] = true;
+                }
             } else {
                 tb.tile = kPatternNodeTile;  // nets beyond the tile use global scratch in the same launch
                 tb.lanes_per_net = 32;
             }
-            launch_pattern_route(go.g, tb, stamp, s);
+            launch_pattern_route(go.g, tb, stamp, cs);
             st.launches += 1;
+        }
+        for (int c : {0, 2}) {
+            if (!forked[c]) continue;
+            const int j = c == 0 ? 0 : 1;
+            cuda_check(cudaEventRecord(ev_join[j], s_cls[j]), "event");
+            cuda_check(cudaStreamWaitEvent(s, ev_join[j], 0), "join");
         }
         if (timed) kt.end(KC_PATTERN);
         if (timed) kt.begin(KC_WIRE_COMMIT);

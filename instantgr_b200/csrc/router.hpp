@@ -99,6 +99,10 @@ struct Router {
     GridOwner go;
     cudaStream_t s = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // batched form: the large and small size classes run beside the medium one
+    // on these streams, forked from and joined back into `s`
+    cudaStream_t s_cls[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     RouterStats st;
     KernelTimer kt;
     int global_stamp = 0;
