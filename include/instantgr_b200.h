@@ -172,7 +172,7 @@ int igr_pattern_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t 
  * written (then call igr_commit_wires as usual).  Results are identical to
  * igr_pattern_route's.
  *
- * The DP's scratch (layer tables of nets with more than 16 tree nodes, 880
+ * The DP's scratch (layer tables of nets with more than 16 tree nodes, 504
  * bytes per such node, plus 12 bytes per net and a work counter) lives in one
  * fixed array of IGR_STATIC_SCRATCH_BYTES in the library's device image, held
  * by every GPU that loads the library until the process exits.  A call with

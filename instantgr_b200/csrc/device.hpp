@@ -62,10 +62,10 @@ struct TreeBatchDev {
     int lanes_per_net = 32;      // 16 or 32
     int tile = 16;               // nodes kept on chip: 6, 16, or 1 (all in scratch)
 };
-// scratch per node of a net kept in global memory: 45 range costs and 36
-// prefetched edge costs (doubles), then 8 via-column costs (floats), 45
-// backtrace codes, the chosen range and 4 decoded position/parent ints
-constexpr int kPatternScratchD = 81, kPatternScratchI = 8 + 45 + 1 + 4;
+// scratch per node of a net kept in global memory: 45 range costs (doubles),
+// then 8 via-column costs (floats), 45 backtrace codes (shorts, padded to 23
+// ints), the chosen range and 4 decoded position/parent ints
+constexpr int kPatternScratchD = 45, kPatternScratchI = 8 + 23 + 1 + 4;
 // doubles of scratch needed for `nodes` nodes of nets kept in global memory
 inline int64_t pattern_scratch_doubles(int64_t nodes) {
     return nodes * kPatternScratchD + (nodes * kPatternScratchI + 1) / 2;
@@ -132,13 +132,27 @@ void launch_from_track_layout_d(const GridDev &g, const double *trk, double *ref
 void launch_to_track_layout_d(const GridDev &g, const double *ref, double *trk, cudaStream_t s);
 void launch_from_track_layout_i(const GridDev &g, const int *trk, int *ref, cudaStream_t s);
 
+// ---- phase-1 plan from the colouring (plan.cu): routing-net ids batch by
+// batch in routing order (batches reversed), each batch split into the size
+// classes of the tree DP, nets of a class by node count (largest first)
+struct PlanArgs {
+    int n = 0, nb = 0;                // ranks, batches
+    const int *bat = nullptr;         // [n] batch of each rank
+    const int *perm = nullptr;        // [n] routing-net id of each rank (null: identity)
+    const int *node_off = nullptr;    // [routing nets+1] tree node offsets
+    int classes = 1, split = 6, big = 16;  // 1 class (all medium), or large (> big) / medium (> split) / small
+};
+// histogram entries launch_plan needs for nb batches
+int64_t plan_hist_size(int nb);
+// ids[n]; offs[3 * rb + c] = first position of class c of routed batch rb, offs[3 * nb] = n
+void launch_plan(const PlanArgs &a, int *hist, int *ids, int *offs, int *err, cudaStream_t s);
+
 // ---- batch colouring (database_cuda.hpp:288-434, made deterministic)
 struct ColorDev {
     int n = 0, X = 0, Y = 0, sparsity = 15;
     // shapes are indexed by shape id s; the colouring ranks k = 0..n-1 (higher
-    // k wins a cell) with perm[k] = shape of rank k and rank[s] = its inverse
-    // (both null: identity)
-    const int *perm = nullptr, *rank = nullptr;
+    // k wins a cell) with perm[k] = shape of rank k (null: identity)
+    const int *perm = nullptr;
     const int *pt_off = nullptr, *pts = nullptr;   // [shapes+1], 2-D cells
     const int *pt_net = nullptr;                   // [points] owner shape
     const int *h_off = nullptr, *hseg = nullptr;   // [shapes+1], pairs

@@ -38,9 +38,9 @@ __host__ __device__ constexpr int tri(int a, int b) { return a * 9 - a * (a - 1)
 template <int T>
 struct GroupSmem {
     double dist[T * kR];
-    double pf[(T > 1 ? T - 1 : 1) * kPF];
+    double pf[2 * kPF];  // geometry-only costs of the current and the next edge
     float col[T * kCol];
-    int from[T * kR];
+    short from[T * kR];  // backtrace code of each range: cf * 81 + child layer * 9 + parent layer
     int lr[T];
     int nx[T], ny[T], nl[T], np[T];  // decoded node position and parent
     double costc[kL], diag[kL];
@@ -50,6 +50,30 @@ struct GroupSmem {
 __device__ __forceinline__ double wire_cost(const GridDev &g, int l, int xa, int xb, int ya, int yb) {
     // presum[IDX(l, xmax, ymax)] - presum[IDX(l, xmin, ymin)]  (graph.hpp:19-21)
     return g.presum[cell_at(g, l, xb, yb)] - g.presum[cell_at(g, l, xa, ya)];
+}
+
+// Geometry-only cost j of the edge from (x, y) to its parent (px, py), 0 when
+// unused: [0,9) child leg (bent) or wire (straight) per layer, [9,18) parent
+// leg, [18,27) via column at (x, py), [27,36) via column at (px, y).
+__device__ __forceinline__ double edge_value(const GridDev &g, int x, int y, int px, int py, int j) {
+    const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
+    const bool straight = (x == px || y == py);
+    if (j < kL) {
+        const int l = j;
+        if (straight) {
+            const int dl = layer_dir(g, l);
+            if (!((dl == 0 && y != py) || (dl == 1 && x != px))) return wire_cost(g, l, minx, maxx, miny, maxy);
+            return 0.0;
+        }
+        return layer_dir(g, l) ? wire_cost(g, l, x, x, miny, maxy) : wire_cost(g, l, minx, maxx, y, y);
+    }
+    if (straight) return 0.0;
+    if (j < 2 * kL) {
+        const int l = j - kL;
+        return layer_dir(g, l) ? wire_cost(g, l, px, px, miny, maxy) : wire_cost(g, l, minx, maxx, py, py);
+    }
+    if (j < 3 * kL) return (double)g.vcost[cell_at(g, j - 2 * kL, x, py)];
+    return (double)g.vcost[cell_at(g, j - 3 * kL, px, y)];
 }
 
 __device__ __forceinline__ void add_wire(const GridDev &g, const int *layer_first, int l, int xa, int xb, int ya,
@@ -97,11 +121,12 @@ __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatch
         const int n = b.node_off[net + 1] - nb;
         const int *nodes = b.nodes + nb;
         const int *par = b.par + nb;
-        double *dist, *pf;
+        double *dist;
         float *col;
-        int *from, *lr, *nx, *ny, *nl, *np;
+        short *from;
+        int *lr, *nx, *ny, *nl, *np;
         if (n <= kNodeTile) {
-            dist = sm.dist; pf = sm.pf; col = sm.col; from = sm.from; lr = sm.lr;
+            dist = sm.dist; col = sm.col; from = sm.from; lr = sm.lr;
             nx = sm.nx; ny = sm.ny; nl = sm.nl; np = sm.np;
         } else {
             const int64_t so = b.scratch_off[net];
@@ -110,11 +135,10 @@ __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatch
                 continue;
             }
             dist = b.scratch + so * kPatternScratchD;
-            pf = dist + (int64_t)n * kR;
             int *ib = reinterpret_cast<int *>(b.scratch + b.scratch_nodes * kPatternScratchD) + so * kPatternScratchI;
             col = reinterpret_cast<float *>(ib);
-            from = ib + (int64_t)n * kCol;
-            lr = from + (int64_t)n * kR;
+            from = reinterpret_cast<short *>(ib + (int64_t)n * kCol);
+            lr = ib + (int64_t)n * (kCol + (kR + 1) / 2);
             nx = lr + n; ny = nx + n; nl = ny + n; np = nl + n;
         }
         // ---- 0. node positions and parents, decoded once
@@ -142,48 +166,45 @@ __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatch
                 dist[i * kR + tri(mn, mx)] = (l < kL && (mn > l || mx < l)) ? kInf : acc;
             }
         }
-        // ---- 1b. geometry-only costs of every edge: [0,9) child leg (bent) or wire
-        //          (straight) per layer, [9,18) parent leg, [18,27) via column at (x, py),
-        //          [27,36) via column at (px, y)
-        for (int t = gl; t < (n - 1) * kPF; t += G) {
-            const int e = t / kPF, j = t % kPF, i = e + 1;
-            const int pi = np[i];
-            if (pi < 0 || pi >= i) continue;  // reported below
-            const int x = nx[i], y = ny[i], px = nx[pi], py = ny[pi];
-            const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
-            const bool straight = (x == px || y == py);
-            double val = 0;
-            if (j < kL) {
-                const int l = j;
-                if (straight) {
-                    const int dl = layer_dir(g, l);
-                    if (!((dl == 0 && y != py) || (dl == 1 && x != px))) val = wire_cost(g, l, minx, maxx, miny, maxy);
-                } else {
-                    val = layer_dir(g, l) ? wire_cost(g, l, x, x, miny, maxy) : wire_cost(g, l, minx, maxx, y, y);
-                }
-            } else if (!straight) {
-                if (j < 2 * kL) {
-                    const int l = j - kL;
-                    val = layer_dir(g, l) ? wire_cost(g, l, px, px, miny, maxy) : wire_cost(g, l, minx, maxx, py, py);
-                } else if (j < 3 * kL) {
-                    val = (double)g.vcost[cell_at(g, j - 2 * kL, x, py)];
-                } else {
-                    val = (double)g.vcost[cell_at(g, j - 3 * kL, px, y)];
-                }
+        // ---- 2. bottom-up over tree edges (Lshape_route.hpp:33-97).  The
+        //      geometry-only costs of edge i-1 are loaded into registers while
+        //      edge i is computed and stored into the other half of sm.pf after it.
+        constexpr int kPer = (kPF + G - 1) / G;
+        double q[kPer];
+        auto load_edge = [&](int i) {
+            int x = 0, y = 0, px = 0, py = 0;
+            bool use = false;
+            if (i >= 1) {
+                const int pi = np[i];
+                if (pi >= 0 && pi < i) { use = true; x = nx[i]; y = ny[i]; px = nx[pi]; py = ny[pi]; }
             }
-            pf[t] = val;
+#pragma unroll
+            for (int u = 0; u < kPer; u++) {
+                const int j = gl + u * G;
+                q[u] = (use && j < kPF) ? edge_value(g, x, y, px, py, j) : 0.0;
+            }
+        };
+        auto store_edge = [&](int i) {
+            double *slot = sm.pf + (i & 1) * kPF;
+#pragma unroll
+            for (int u = 0; u < kPer; u++)
+                if (gl + u * G < kPF) slot[gl + u * G] = q[u];
+        };
+        if (n > 1) {
+            load_edge(n - 1);
+            store_edge(n - 1);
         }
         __syncwarp(gmask);
-        // ---- 2. bottom-up over tree edges (Lshape_route.hpp:33-97)
         bool bad = false;
         for (int i = n - 1; i >= 1; i--) {
             const int pi = np[i];
             if (pi < 0 || pi >= i) { bad = true; break; }
+            load_edge(i - 1);
             const int x = nx[i], y = ny[i], px = nx[pi], py = ny[pi];
             const double *nd = dist + i * kR;
             double *pd = dist + pi * kR;
-            int *prev = from + i * kR;
-            const double *pe = pf + (i - 1) * kPF;
+            short *prev = from + i * kR;
+            const double *pe = sm.pf + (i & 1) * kPF;
             // (a) cheapest range containing each layer
             double mcc = kInf;
             int cf = 0;
@@ -247,6 +268,7 @@ __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatch
                     pd[tri(mn, mx)] += row;
                 }
             }
+            store_edge(i - 1);
             __syncwarp(gmask);
         }
         if (bad) {

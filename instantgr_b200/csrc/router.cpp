@@ -223,6 +223,9 @@ void Router::ensure_device() {
         sh.v_off.push_back((int)(sh.vseg.size() / 2));
     }
     d_shapes1.upload(sh, X, Y, 15, s);  // phase 1 samples every 15th segment cell (database_cuda.hpp:439)
+    // phase-1 colouring ranks: the reversed routing priority (the last rank wins conflicts)
+    std::vector<int> perm1(order1.rbegin(), order1.rend());
+    d_perm1.upload(perm1, s);
     std::vector<int> ids(R);
     std::iota(ids.begin(), ids.end(), 0);
     d_all_ids.upload(ids, s);
@@ -288,44 +291,31 @@ void Router::fetch_routes() {
 // are split into size classes (results do not depend on the order of nets
 // within a batch): large nets (global scratch) first, then medium, then small,
 // each by node count, largest first; one DP launch per class.
-void Router::plan_phase1(const std::vector<std::vector<int>> &batches, std::vector<int> &net_ids,
-                         std::vector<int> &batch_off, std::vector<int> &class_off) const {
-    net_ids.clear();
-    batch_off.assign(1, 0);
-    class_off.clear();
-    auto nodes_of = [&](int id) { return tree_off[id + 1] - tree_off[id]; };
-    for (auto &b : batches) {
-        if (!batched) {
-            class_off.push_back((int)net_ids.size());
-            class_off.push_back((int)net_ids.size());
-            class_off.push_back((int)net_ids.size());
-            net_ids.insert(net_ids.end(), b.begin(), b.end());
-            batch_off.push_back((int)net_ids.size());
-            continue;
-        }
-        // class of a net: one class puts every net in the medium launch (tile 16,
-        // scratch beyond it); within a class, nets by node count, largest first,
-        // ties in batch order (a counting sort: node counts are small integers)
-        auto class_of = [&](int m) {
-            return tune.classes == 1 ? 1 : (m > kPatternNodeTile ? 0 : (m > tune.split ? 1 : 2));
-        };
-        int maxm = 0;
-        for (int id : b) maxm = std::max(maxm, nodes_of(id));
-        std::vector<int> cnt(3 * (size_t)(maxm + 2), 0);  // [class][maxm - m]
-        for (int id : b) {
-            const int m = nodes_of(id);
-            cnt[(size_t)class_of(m) * (maxm + 2) + (maxm - m) + 1]++;
-        }
-        const int base = (int)net_ids.size();
-        for (size_t i = 1; i < cnt.size(); i++) cnt[i] += cnt[i - 1];
-        for (int c = 0; c < 3; c++) class_off.push_back(base + cnt[(size_t)c * (maxm + 2)]);
-        net_ids.resize(base + b.size());
-        for (int id : b) {
-            const int m = nodes_of(id);
-            net_ids[base + cnt[(size_t)class_of(m) * (maxm + 2) + (maxm - m)]++] = id;
-        }
-        batch_off.push_back((int)net_ids.size());
+void Router::plan_phase1(int nb, std::vector<int> &batch_off, std::vector<int> &class_off) {
+    const int R = (int)ns.nets.size();
+    PlanArgs pa;
+    pa.n = R; pa.nb = nb; pa.bat = d_bat.p; pa.perm = d_perm1.p; pa.node_off = d_tree_off.p;
+    pa.classes = batched ? tune.classes : 1;
+    pa.split = tune.split;
+    pa.big = kPatternNodeTile;
+    d_plan_hist.alloc((size_t)plan_hist_size(nb));
+    d_plan_offs.alloc(3 * (size_t)nb + 1);
+    d_ids.alloc(R);
+    launch_plan(pa, d_plan_hist.p, d_ids.p, d_plan_offs.p, go.g.err, s);
+    st.launches += 3;
+    std::vector<int> offs(3 * (size_t)nb + 1);
+    cuda_check(cudaMemcpyAsync(offs.data(), d_plan_offs.p, offs.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaStreamSynchronize(s), "plan");
+    st.d2h_bytes += (int64_t)offs.size() * 4;
+    if (int e = go.check_error(s)) throw Error(e, "a net was left without a batch");
+    batch_off.resize(nb + 1);
+    class_off.resize(3 * (size_t)nb);
+    for (int b = 0; b < nb; b++) {
+        batch_off[b] = offs[3 * b];
+        for (int c = 0; c < 3; c++) class_off[3 * b + c] = offs[3 * b + c];
     }
+    batch_off[nb] = offs[3 * nb];
+    if (batch_off[nb] != R) throw Error(ERR_STATE, "phase-1 plan does not cover every net");
 }
 
 // The per-batch launches of phase 1 (Lshape_route.hpp:235-242), stream-ordered.
@@ -386,19 +376,17 @@ void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<in
 
 void Router::phase1() {
     const int R = (int)ns.nets.size();
-    std::vector<std::vector<int>> batches;
-    color_nets(order1, d_shapes1, 15, batches);
-    std::reverse(batches.begin(), batches.end());
-    st.batches1 = (int)batches.size();
-    if (batched && !tuned) autotune(batches);
-    std::vector<int> net_ids, batch_off, class_off;
-    plan_phase1(batches, net_ids, batch_off, class_off);
+    // colouring and plan stay on the device; only the batch and class offsets
+    // come back to size the launches
+    const int nb = run_color(R, d_perm1.p, d_shapes1, 15);
+    st.batches1 = nb;
+    if (batched && !tuned) autotune(nb);
+    std::vector<int> batch_off, class_off;
+    plan_phase1(nb, batch_off, class_off);
     grow_routes(route_end);
-    d_ids.upload(net_ids, s);
     cuda_check(cudaMemcpyAsync(d_route_off.p, d_route_off1.p, (size_t)R * 8, cudaMemcpyDeviceToDevice, s), "D2D");
     cuda_check(cudaMemcpyAsync(d_route_cap.p, d_route_cap1.p, (size_t)R * 4, cudaMemcpyDeviceToDevice, s), "D2D");
-    d_queue.alloc(3 * batches.size() + 1);
-    st.h2d_bytes += (int64_t)net_ids.size() * 4;
+    d_queue.alloc(3 * (size_t)nb + 1);
     cuda_check(cudaEventRecord(ev0, s), "event");
     if (batched) {
         // the whole phase-1 loop as one CUDA graph, reused while the plan is unchanged
@@ -424,19 +412,19 @@ void Router::phase1() {
     } else {
         emit_phase1(batch_off, class_off, true);
     }
-    global_stamp = (int)batches.size();
+    global_stamp = nb;
     cuda_check(cudaEventRecord(ev1, s), "event");
     cuda_check(cudaGetLastError(), "phase-1 launch");
-    // plan of this run, in routing order (for igr_router_plan)
-    plan_ids.swap(net_ids);
+    // plan of this run, in routing order (for igr_router_plan; ids fetched on demand)
     plan_batch_off.swap(batch_off);
+    plan_ids.clear();
     plan_built = false;
     cuda_check(cudaEventSynchronize(ev1), "phase 1");
     float ms = 0;
     cudaEventElapsedTime(&ms, ev0, ev1);
     st.p1_ms = ms;
     if (int e = go.check_error(s)) throw Error(e, "device error in phase 1");
-    if (verbose) std::fprintf(stderr, "[igr] phase 1: %zu batches, %.2f ms device\n", batches.size(), ms);
+    if (verbose) std::fprintf(stderr, "[igr] phase 1: %d batches, %.2f ms device\n", nb, ms);
 }
 
 // Autotuner of the batched form: picks the node count that separates small
@@ -450,10 +438,10 @@ static std::string tune_cache_path() {
     return std::string(h ? h : "/tmp") + "/.cache/instantgr_b200/tune.txt";
 }
 
-void Router::autotune(const std::vector<std::vector<int>> &batches) {
+void Router::autotune(int nb) {
     const int R = (int)ns.nets.size();
     char key[96];
-    std::snprintf(key, sizeof key, "%d %d %d %d", ns.X, ns.Y, R, (int)batches.size());
+    std::snprintf(key, sizeof key, "%d %d %d %d", ns.X, ns.Y, R, nb);
     const std::string path = tune_cache_path();
     if (FILE *f = std::fopen(path.c_str(), "r")) {
         char line[256];
@@ -488,15 +476,14 @@ void Router::autotune(const std::vector<std::vector<int>> &batches) {
             }
     Tune best = tune;
     float best_ms = 1e30f;
-    std::vector<int> net_ids, batch_off, class_off;
-    d_queue.alloc(3 * batches.size() + 1);
+    std::vector<int> batch_off, class_off;
+    d_queue.alloc(3 * (size_t)nb + 1);
     grow_routes(route_end);
     for (const Tune &cand : cands) {
             {
                 tune = cand;
-                plan_phase1(batches, net_ids, batch_off, class_off);
+                plan_phase1(nb, batch_off, class_off);
                 go.reset_demand(s);
-                d_ids.upload(net_ids, s);
                 cuda_check(cudaMemcpyAsync(d_route_off.p, d_route_off1.p, (size_t)R * 8, cudaMemcpyDeviceToDevice, s), "D2D");
                 cuda_check(cudaMemcpyAsync(d_route_cap.p, d_route_cap1.p, (size_t)R * 4, cudaMemcpyDeviceToDevice, s), "D2D");
                 cuda_check(cudaEventRecord(ev0, s), "event");
@@ -533,6 +520,11 @@ void Router::autotune(const std::vector<std::vector<int>> &batches) {
 // Trees and route capacities of the last phase-1 plan, in routing order.
 void Router::build_plan() {
     if (plan_built) return;
+    if (plan_ids.empty() && !plan_batch_off.empty()) {
+        plan_ids.resize(plan_batch_off.back());
+        cuda_check(cudaMemcpyAsync(plan_ids.data(), d_ids.p, plan_ids.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
+        cuda_check(cudaStreamSynchronize(s), "plan");
+    }
     plan_node_off.assign(1, 0);
     plan_nodes.clear();
     plan_par.clear();
@@ -555,21 +547,31 @@ void Router::color_nets(const std::vector<int> &order, const ShapeDev &shapes, i
     const int n = (int)order.size();
     batches.clear();
     if (n == 0) return;
-    const int nshapes = shapes.nshapes;
-    std::vector<int> perm(order.rbegin(), order.rend()), rank(nshapes, -1);
-    for (int k = 0; k < n; k++) rank[perm[k]] = k;
+    std::vector<int> perm(order.rbegin(), order.rend());
     d_perm.upload(perm, s);
-    d_rank.upload(rank, s);
+    st.h2d_bytes += (int64_t)n * 4;
+    const int nb = run_color(n, d_perm.p, shapes, sparsity);
+    std::vector<int> bid(n);
+    cuda_check(cudaMemcpyAsync(bid.data(), d_bat.p, n * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    st.d2h_bytes += (int64_t)n * 4;
+    batches.assign(nb, {});
+    for (int k = 0; k < n; k++) {
+        if (bid[k] < 0 || bid[k] >= nb) throw Error(ERR_STATE, "a net was left without a batch");
+        batches[bid[k]].push_back(perm[k]);
+    }
+}
+
+int Router::run_color(int n, const int *d_perm_ranks, const ShapeDev &shapes, int sparsity) {
     d_map.alloc((size_t)ns.X * ns.Y);
     d_bat.alloc(n);
     d_act.alloc(4 * (size_t)n);
     d_hdr.alloc(n);
     d_flags.alloc(16);
-    st.h2d_bytes += (int64_t)(n + nshapes) * 4;
     if (sparsity != shapes.sparsity) throw Error(ERR_STATE, "claim lists were built for another sparsity");
     ColorDev cd;
     cd.n = n; cd.X = ns.X; cd.Y = ns.Y; cd.sparsity = sparsity;
-    cd.perm = d_perm.p; cd.rank = d_rank.p;
+    cd.perm = d_perm_ranks;
     cd.pt_off = shapes.pt_off.p; cd.pts = shapes.pts.p; cd.pt_net = shapes.pt_net.p;
     cd.h_off = shapes.h_off.p; cd.hseg = shapes.hseg.p; cd.v_off = shapes.v_off.p; cd.vseg = shapes.vseg.p;
     cd.claim_off = shapes.claim_off.p; cd.claim = shapes.claim.p;
@@ -583,15 +585,7 @@ void Router::color_nets(const std::vector<int> &order, const ShapeDev &shapes, i
     st.launches += 1;
     if (nb == -2) throw Error(ERR_TIMEOUT, "colouring barrier timed out");
     if (nb < 0) throw Error(ERR_CUDA, std::string("colouring failed: ") + cudaGetErrorString(cudaGetLastError()));
-    std::vector<int> bid(n);
-    cuda_check(cudaMemcpyAsync(bid.data(), d_bat.p, n * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
-    cuda_check(cudaStreamSynchronize(s), "sync");
-    st.d2h_bytes += (int64_t)n * 4;
-    batches.assign(nb, {});
-    for (int k = 0; k < n; k++) {
-        if (bid[k] < 0 || bid[k] >= nb) throw Error(ERR_STATE, "a net was left without a batch");
-        batches[bid[k]].push_back(perm[k]);
-    }
+    return nb;
 }
 
 // One rip-up-and-reroute pass (main.cpp:37-68, Lshape_route_detour.hpp:726-1112).
@@ -615,9 +609,8 @@ bool Router::rrr_pass(int iter) {
     ViaBatchDev all{d_all_ids.p, d_route_off.p, routes.p, R};
     kt.begin(KC_RIPUP);
     launch_mark_overflow(go.g, 0, of_sum.p, all, 10, d_is_of.p, s);
-    launch_congestion_view(go.g, d_xsum.p, d_ysum.p, s);
     kt.end(KC_RIPUP);
-    st.launches += 5;
+    st.launches += 2;
     std::vector<uint8_t> is_of(R);
     CongestionView cv;
     cv.X = X; cv.Y = Y;
@@ -633,6 +626,10 @@ bool Router::rrr_pass(int iter) {
     if (verbose) std::fprintf(stderr, "[igr] pass %d: %zu nets to reroute\n", iter, of_nets.size());
     if (of_nets.empty()) return false;
     // the host builds the detour DAGs from the congestion view (Lshape_route_detour.hpp:735-740)
+    kt.begin(KC_RIPUP);
+    launch_congestion_view(go.g, d_xsum.p, d_ysum.p, s);
+    kt.end(KC_RIPUP);
+    st.launches += 3;
     cuda_check(cudaMemcpyAsync(cv.xsum.data(), d_xsum.p, cv.xsum.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaMemcpyAsync(cv.ysum.data(), d_ysum.p, cv.ysum.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
@@ -809,11 +806,14 @@ void Router::compute_score() {
     unsigned long long h[4] = {0, 0, 0, 0};
     double of = 0;
     launch_overflow_cost(go.g, go.score.p, s);
+    st.launches += 2;
     cuda_check(cudaMemcpyAsync(h, go.stats.p, sizeof h, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaMemcpyAsync(&of, go.score.p, sizeof of, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
-    int64_t pin_vias = 0;
-    for (size_t i = 0; i < d.sel.size(); i++) pin_vias += d.sel[i] < d.X * d.Y;
+    if (pin_vias < 0) {
+        pin_vias = 0;
+        for (size_t i = 0; i < d.sel.size(); i++) pin_vias += d.sel[i] < d.X * d.Y;
+    }
     cost_cells = h[2];
     score_wl = (double)(int64_t)h[0] * d.unit_wire;
     score_via = (double)((int64_t)h[1] + pin_vias) * d.unit_via;

@@ -129,7 +129,7 @@ struct Router {
     bool h_routes_valid = false;
     // ---- per-run device buffers (grow-only)
     DevBuf<int4> d_hdr;
-    DevBuf<int> d_ids, d_all_ids, of_sum, d_perm, d_rank, d_map, d_bat, d_act, d_flags, d_queue;
+    DevBuf<int> d_ids, d_all_ids, of_sum, d_perm, d_map, d_bat, d_act, d_flags, d_queue;
     // launch shape of the tree DP per size class (large, medium, small) and the
     // node count that separates small from medium nets (autotuned, see tune.cpp)
     struct Tune {
@@ -145,10 +145,12 @@ struct Router {
     std::vector<int> graph1_batch_off, graph1_class_off;
     int *graph1_routes = nullptr;
     long long graph1_launches = 0;
-    void plan_phase1(const std::vector<std::vector<int>> &batches, std::vector<int> &net_ids,
-                     std::vector<int> &batch_off, std::vector<int> &class_off) const;
+    // device plan of phase 1 from the colouring in d_bat (ranks of d_perm1):
+    // d_ids, and the batch and class offsets on the host
+    void plan_phase1(int nb, std::vector<int> &batch_off, std::vector<int> &class_off);
     void emit_phase1(const std::vector<int> &batch_off, const std::vector<int> &class_off, bool timed);
-    void autotune(const std::vector<std::vector<int>> &batches);
+    void autotune(int nb);
+    DevBuf<int> d_perm1, d_plan_hist, d_plan_offs;  // phase-1 colouring ranks, plan scratch
     DevBuf<uint8_t> d_is_of;
     DevBuf<float> d_xsum, d_ysum;
     DevBuf<unsigned> d_bar;
@@ -165,6 +167,7 @@ struct Router {
     void build_plan();
     // score of the last run: wirelength, vias, overflow (GPU estimate)
     double score_wl = 0, score_via = 0, score_of = 0;
+    int64_t pin_vias = -1;  // selected pins on file layer 0 (one via each), counted once
 
     ~Router();
     void open(const char *cap, const char *net);
@@ -175,6 +178,8 @@ struct Router {
     void ensure_device();
     void color_nets(const std::vector<int> &order, const ShapeDev &shapes, int sparsity,
                     std::vector<std::vector<int>> &batches);
+    // colours n ranks (d_perm_ranks[k] = shape of rank k) into d_bat; returns the batch count
+    int run_color(int n, const int *d_perm_ranks, const ShapeDev &shapes, int sparsity);
     void compute_score();
 
    private:

@@ -76,8 +76,8 @@ def test_static_scratch_rejects_oversized_batches():
     with pytest.raises(ig.IgrError) as e:
         c.pattern_route_static(ig.STATIC_MAX_NETS + 1, p, 0, p, p, p, p, p, 0, 1)
     assert e.value.code == ig.IGR_ERR_CAPACITY and "nets per call" in str(e.value)
-    # 2000 chains of 50 nodes: 100k nodes in scratch need about 83 MB (> 64 MiB)
-    n, k = 2000, 50
+    # 2000 chains of 80 nodes: 160k nodes in scratch need about 80 MB (> 64 MiB)
+    n, k = 2000, 80
     xy = g["X"] * g["Y"]
     node_off = np.arange(n + 1, dtype=np.int32) * k
     nodes = (np.arange(n * k, dtype=np.int64) % xy).astype(np.int32)
