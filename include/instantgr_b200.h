@@ -53,7 +53,9 @@ typedef struct igr_options {
     int verbose;       /* print stage times to stderr */
     int batched;       /* 1 = size-class persistent kernels + CUDA graphs (same results as 0) */
     int profile;       /* 1 = time every kernel launch with CUDA events (igr_router_kstats) */
-    int reserved[7];
+    int split_commit;  /* 1 = phase-1 batches commit wires and vias and refresh costs in three
+                          launches instead of one fused per-track pass (same results) */
+    int reserved[6];
 } igr_options;
 
 /* Fills `o` with the defaults that reproduce InstantGR (1 RRR pass). */
@@ -78,9 +80,10 @@ int igr_router_write(igr_router *r, const char *out_path);
  * [13] host-to-device bytes, [14] device-to-host bytes. */
 int igr_router_stats(igr_router *r, double *out, int n);
 /* Per-kernel-class device time of the last run (needs opt->profile): for
- * class k in {cost refresh, tree DP, wire commit, via commit, DAG DP,
- * colouring, rip-up/marking}, out[3k] = launches, out[3k+1] = milliseconds,
- * out[3k+2] = algorithmic DRAM bytes (cost refresh: 20 per refreshed cell). */
+ * class k in {cost refresh (with the fused phase-1 commit), tree DP, wire
+ * commit, via commit, DAG DP, colouring, rip-up/marking, phase-1 graph},
+ * out[3k] = launches, out[3k+1] = milliseconds, out[3k+2] = algorithmic DRAM
+ * bytes (cost refresh: 20 per refreshed cell + 12 per committed cell). */
 int igr_router_kstats(igr_router *r, double *out, int n);
 /* Phase-1 plan of the last run: routing order, batch offsets and trees.
  * sizes[0..2] receive the number of nets, batches and tree nodes; the arrays

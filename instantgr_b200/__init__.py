@@ -48,7 +48,8 @@ EXPORTS = [
 
 class Options(C.Structure):
     _fields_ = [("rrr_iters", C.c_int), ("threads", C.c_int), ("mode", C.c_int), ("verbose", C.c_int),
-                ("batched", C.c_int), ("profile", C.c_int), ("reserved", C.c_int * 7)]
+                ("batched", C.c_int), ("profile", C.c_int), ("split_commit", C.c_int),
+                ("reserved", C.c_int * 6)]
 
 
 class GridDesc(C.Structure):
@@ -230,6 +231,14 @@ class Router:
         _check(L.igr_router_grid(self.h, p(hdr), p(costs), p(xl), p(yl), p(cap)))
         return dict(L=Lr, X=X, Y=Y, DIR=d0, xlen=xl, ylen=yl, unit_wire=float(costs[0]), unit_via=float(costs[1]),
                     short=costs[2:].copy(), cap=cap, demand=np.zeros_like(cap))
+
+    def demand(self) -> np.ndarray:
+        """Device demand of the routing layers after the last run, [l][x][y]."""
+        hdr = np.zeros(4, np.int32)
+        _check(lib().igr_router_grid(self.h, hdr.ctypes.data_as(C.c_void_p), None, None, None, None))
+        out = np.zeros(int(hdr[0]) * int(hdr[1]) * int(hdr[2]), np.float32)
+        _check(lib().igr_router_demand(self.h, out))
+        return out
 
     def sizes(self):
         a, b = C.c_int64(), C.c_int64()

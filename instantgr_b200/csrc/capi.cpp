@@ -80,6 +80,7 @@ static void apply_options(Router &r, const igr_options *o) {
     r.mode = o->mode;
     r.verbose = o->verbose;
     r.batched = o->batched;
+    r.split_commit = o->split_commit;
     r.kt.on = o->profile != 0;
 }
 
@@ -124,7 +125,8 @@ int igr_router_kstats(igr_router *h, double *o, int n) {
     if (!h || !o) return fail(nullptr, IGR_ERR_INVALID, "null argument");
     const auto &r = h->r;
     for (int k = 0; k < KC_N; k++) {
-        double v[3] = {(double)r.kt.launches[k], r.kt.ms[k], k == KC_COST ? 20.0 * (double)r.cost_cells : 0.0};
+        double v[3] = {(double)r.kt.launches[k], r.kt.ms[k],
+                       k == KC_COST ? 20.0 * (double)r.cost_cells + 12.0 * (double)r.commit_cells : 0.0};
         for (int j = 0; j < 3; j++)
             if (3 * k + j < n) o[3 * k + j] = v[j];
     }

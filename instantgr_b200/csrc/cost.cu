@@ -24,32 +24,19 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Cost model and Sklansky prefix sums of one track whose capacity and demand
+// are staged in s_cap / s_dem; every thread of the block calls it.
 template <int MAXE>
-__global__ void __launch_bounds__(kThreads) cost_refresh_kernel(GridDev g, int only_dirty) {
-    const int tr = blockIdx.x;
-    if (only_dirty) {
-        if (!g.dirty_cost[tr]) return;
-    }
-    const TrackInfo ti = decode_track(g, tr);
+__device__ __forceinline__ void refresh_track(const GridDev &g, const TrackInfo &ti, const float *s_cap,
+                                              const float *s_dem) {
     const int n = ti.len;
     const int E = (n + kThreads - 1) / kThreads;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const double sc = g.short_cost[ti.l];
     const int *elen = ti.dir ? g.ylen : g.xlen;
-
-    __shared__ float s_cap[MAXE * kThreads], s_dem[MAXE * kThreads];
     __shared__ double s_wt[kThreads / 32][MAXE];
     __shared__ double s_rt[MAXE];
-
-    for (int i = tid; i < n; i += kThreads) {
-        s_cap[i] = g.cap[ti.base + i];
-        s_dem[i] = g.demand[ti.base + i];
-    }
-    __syncthreads();
-    if (tid == 0) {
-        if (only_dirty) g.dirty_cost[tr] = 0;
-        atomicAdd(&g.stats[2], (unsigned long long)n);  // refreshed cells, for the roofline
-    }
+    if (tid == 0) atomicAdd(&g.stats[2], (unsigned long long)n);  // refreshed cells, for the roofline
 
     double x[MAXE];
 #pragma unroll
@@ -138,6 +125,117 @@ __global__ void __launch_bounds__(kThreads) cost_refresh_kernel(GridDev g, int o
     }
 }
 
+template <int MAXE>
+__global__ void __launch_bounds__(kThreads) cost_refresh_kernel(GridDev g, int only_dirty) {
+    const int tr = blockIdx.x;
+    if (only_dirty) {
+        if (!g.dirty_cost[tr]) return;
+    }
+    const TrackInfo ti = decode_track(g, tr);
+    __shared__ float s_cap[MAXE * kThreads], s_dem[MAXE * kThreads];
+    for (int i = threadIdx.x; i < ti.len; i += kThreads) {
+        s_cap[i] = g.cap[ti.base + i];
+        s_dem[i] = g.demand[ti.base + i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && only_dirty) g.dirty_cost[tr] = 0;
+    refresh_track<MAXE>(g, ti, s_cap, s_dem);
+}
+
+__device__ __forceinline__ int warp_incl_scan(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Batch commit and cost refresh of one track in one pass (phase 1): the wire
+// difference array is scanned into demand and stamps (compute_presum_general
+// + commit_all_edge, graph.hpp:74-137), the via crossings the tree DP counted
+// per cell are added where this batch's wires left no stamp
+// (commit_via_demand, graph.hpp:496-543: half a unit on each track edge
+// beside the cell, a full unit at the track ends), and the costs and prefix
+// sums are rebuilt from the demand still in shared memory.  Tracks with no
+// pending commit and clean costs are skipped.  With refresh = 0 the costs are
+// only marked dirty.
+template <int MAXE>
+__global__ void __launch_bounds__(kThreads) commit_refresh_kernel(GridDev g, int *vcnt, int stamp, int refresh) {
+    const int tr = blockIdx.x;
+    const bool commit = g.dirty_commit[tr] != 0;
+    if (!commit && !(refresh && g.dirty_cost[tr])) return;
+    const TrackInfo ti = decode_track(g, tr);
+    const int n = ti.len;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __shared__ float s_cap[MAXE * kThreads], s_dem[MAXE * kThreads];
+    __shared__ int s_w[kThreads / 32];
+    __shared__ int s_carry;
+    __shared__ long long s_wl[kThreads / 32];
+    for (int i = tid; i < n; i += kThreads) {
+        if (refresh) s_cap[i] = g.cap[ti.base + i];
+        s_dem[i] = g.demand[ti.base + i];
+    }
+    if (commit) {
+        const int *elen = ti.dir ? g.ylen : g.xlen;
+        if (tid == 0) s_carry = 0;
+        __syncthreads();
+        long long wl = 0;
+        for (int r0 = 0; r0 < n; r0 += kThreads) {
+            const int i = r0 + tid;
+            int v = 0;
+            if (i < n) {
+                v = g.pre[ti.base + i];
+                if (v != 0) g.pre[ti.base + i] = 0;
+            }
+            const int inc = warp_incl_scan(v, lane);
+            if (lane == 31) s_w[warp] = inc;
+            __syncthreads();
+            int wpre = 0;
+            for (int w = 0; w < warp; w++) wpre += s_w[w];
+            const int cnt = s_carry + wpre + inc;  // inclusive prefix at i
+            if (i < n - 1 && cnt > 0) {
+                s_dem[i] += (float)cnt;
+                g.stamp[ti.base + i] = stamp;
+                wl += (long long)cnt * elen[i];
+            }
+            __syncthreads();
+            if (tid == kThreads - 1) s_carry = cnt;
+            __syncthreads();
+        }
+        // vias, after every wire stamp of the track is in place
+        for (int i = tid; i < n; i += kThreads) {
+            const int c = vcnt[ti.base + i];
+            if (c == 0) continue;
+            vcnt[ti.base + i] = 0;
+            if (g.stamp[ti.base + i] >= stamp) continue;
+            if (i == 0) atomicAdd(&s_dem[0], (float)c);
+            else if (i == n - 1) atomicAdd(&s_dem[n - 2], (float)c);
+            else {
+                atomicAdd(&s_dem[i - 1], 0.5f * (float)c);
+                atomicAdd(&s_dem[i], 0.5f * (float)c);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) wl += __shfl_down_sync(0xffffffffu, wl, o);
+        if (lane == 0) s_wl[warp] = wl;
+        __syncthreads();
+        for (int i = tid; i < n; i += kThreads) g.demand[ti.base + i] = s_dem[i];
+        if (tid == 0) {
+            long long t = 0;
+            for (int w = 0; w < kThreads / 32; w++) t += s_wl[w];
+            if (t) atomicAdd(&g.stats[0], (unsigned long long)t);
+            atomicAdd(&g.stats[3], (unsigned long long)n);  // committed cells, for the roofline
+            g.dirty_commit[tr] = 0;
+            g.dirty_cost[tr] = refresh ? 0 : 1;
+        }
+    } else {
+        __syncthreads();
+        if (tid == 0) g.dirty_cost[tr] = 0;
+    }
+    if (refresh) refresh_track<MAXE>(g, ti, s_cap, s_dem);
+}
+
 template <typename T>
 __global__ void ref_to_track_kernel(GridDev g, const T *ref, T *trk) {
     const int64_t n = g.N;
@@ -171,6 +269,17 @@ void launch_cost_refresh(const GridDev &g, bool only_dirty, cudaStream_t s) {
     else if (e <= 4) cost_refresh_kernel<4><<<g.ntracks, kThreads, 0, s>>>(g, od);
     else if (e <= 8) cost_refresh_kernel<8><<<g.ntracks, kThreads, 0, s>>>(g, od);
     else cost_refresh_kernel<16><<<g.ntracks, kThreads, 0, s>>>(g, od);  // tracks of <= 4096 cells
+}
+
+void launch_commit_refresh(const GridDev &g, int *vcnt, int stamp, bool refresh, cudaStream_t s) {
+    const int maxlen = g.X > g.Y ? g.X : g.Y;
+    const int e = (maxlen + kThreads - 1) / kThreads;
+    const int rf = refresh ? 1 : 0;
+    if (e <= 1) commit_refresh_kernel<1><<<g.ntracks, kThreads, 0, s>>>(g, vcnt, stamp, rf);
+    else if (e <= 2) commit_refresh_kernel<2><<<g.ntracks, kThreads, 0, s>>>(g, vcnt, stamp, rf);
+    else if (e <= 4) commit_refresh_kernel<4><<<g.ntracks, kThreads, 0, s>>>(g, vcnt, stamp, rf);
+    else if (e <= 8) commit_refresh_kernel<8><<<g.ntracks, kThreads, 0, s>>>(g, vcnt, stamp, rf);
+    else commit_refresh_kernel<16><<<g.ntracks, kThreads, 0, s>>>(g, vcnt, stamp, rf);
 }
 
 static int grid_for(int64_t n) {

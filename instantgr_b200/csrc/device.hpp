@@ -32,7 +32,8 @@ struct GridDev {
     double *short_cost = nullptr;  // [L]
     uint8_t *dirty_cost = nullptr;    // [ntracks] demand changed since the last cost refresh
     uint8_t *dirty_commit = nullptr;  // [ntracks] difference array holds entries
-    unsigned long long *stats = nullptr;  // [0] wirelength, [1] via count (signed, two's complement)
+    unsigned long long *stats = nullptr;  // [0] wirelength, [1] via count (signed, two's complement),
+                                          // [2] refreshed cells, [3] committed cells
     int *err = nullptr;                   // device error word
 };
 
@@ -44,6 +45,10 @@ struct TrackMap {
 // ---- launchers (stream-ordered; errors are reported through cudaGetLastError)
 void launch_cost_refresh(const GridDev &g, bool only_dirty, cudaStream_t s);
 void launch_wire_commit(const GridDev &g, int stamp, bool only_dirty, cudaStream_t s);
+// Commit of a tree-DP batch (wires from the difference array, vias from the
+// per-cell crossing counts `vcnt`, which it clears) and cost refresh, fused per
+// track; refresh = false only commits and marks the costs dirty.
+void launch_commit_refresh(const GridDev &g, int *vcnt, int stamp, bool refresh, cudaStream_t s);
 
 struct TreeBatchDev {
     const int *net_ids;      // [n] routing-net id of each net of the batch
@@ -60,7 +65,9 @@ struct TreeBatchDev {
     const int *order = nullptr;  // [n] positions into net_ids in processing order (null: 0..n-1)
     int *queue = nullptr;        // work counter of this launch (zero before the launch)
     int lanes_per_net = 32;      // 16 or 32
-    int tile = 16;               // nodes kept on chip: 6, 16, or 1 (all in scratch)
+    int tile = 16;               // nodes kept on chip: 6, 16, 32, or 1 (all in scratch)
+    int *vcnt = nullptr;         // non-null: count via crossings per cell here (and the via
+                                 // count in stats[1]) for launch_commit_refresh
 };
 // scratch per node of a net kept in global memory: 45 range costs (doubles),
 // then 8 via-column costs (floats), 45 backtrace codes (shorts, padded to 23

@@ -91,6 +91,15 @@ __device__ __forceinline__ void add_wire(const GridDev &g, const int *layer_firs
     g.dirty_commit[track_of(g, l, xa, ya, layer_first)] = 1;
 }
 
+// Via crossings of a via span [lo, hi) at (x, y) for the fused batch commit.
+__device__ __forceinline__ void count_vias(const GridDev &g, int *vcnt, const int *layer_first, int lo, int hi, int x,
+                                           int y) {
+    for (int l = lo; l < hi; l++) {
+        atomicAdd(&vcnt[cell_at(g, l, x, y)], 1);
+        g.dirty_commit[track_of(g, l, x, y, layer_first)] = 1;
+    }
+}
+
 template <int G, int T>
 __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatchDev b, int stamp) {
     extern __shared__ unsigned char smem_raw[];
@@ -295,6 +304,7 @@ __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatch
             const int cap = b.route_cap[net];
             int cnt = 1;
             bool ok = true;
+            long long nvias = 0;
             // root range as (minl, maxl)
             int rmn = 0, rmx = 0;
             for (int a = 0, t = 0; a < kL; a++)
@@ -317,7 +327,10 @@ __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatch
                 }
                 const int mn = lr[i] / kL, mx = lr[i] % kL;
                 if (mn > mx || !(dist[i * kR + tri(mn, mx)] < kInf)) { set_error(g.err, ERR_STATE); ok = false; break; }
-                if (mn < mx) EMIT(mn * XY + x * Y + y, mx * XY + x * Y + y);
+                if (mn < mx) {
+                    EMIT(mn * XY + x * Y + y, mx * XY + x * Y + y);
+                    if (ok && b.vcnt) { count_vias(g, b.vcnt, layer_first, mn, mx, x, y); nvias += mx - mn; }
+                }
                 if (!ok || i == 0) continue;
                 const int px = nx[np[i]], py = ny[np[i]];
                 const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
@@ -329,12 +342,20 @@ __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatch
                     EMIT(curl * XY + x * Y + y, curl * XY + x * Y + py);
                     if (ok) add_wire(g, layer_first, curl, x, x, miny, maxy, stamp);
                     EMIT(curl * XY + x * Y + py, parl * XY + x * Y + py);
+                    if (ok && b.vcnt) {
+                        count_vias(g, b.vcnt, layer_first, min(curl, parl), max(curl, parl), x, py);
+                        nvias += max(curl, parl) - min(curl, parl);
+                    }
                     EMIT(parl * XY + x * Y + py, parl * XY + px * Y + py);
                     if (ok) add_wire(g, layer_first, parl, minx, maxx, py, py, stamp);
                 } else {
                     EMIT(curl * XY + x * Y + y, curl * XY + px * Y + y);
                     if (ok) add_wire(g, layer_first, curl, minx, maxx, y, y, stamp);
                     EMIT(curl * XY + px * Y + y, parl * XY + px * Y + y);
+                    if (ok && b.vcnt) {
+                        count_vias(g, b.vcnt, layer_first, min(curl, parl), max(curl, parl), px, y);
+                        nvias += max(curl, parl) - min(curl, parl);
+                    }
                     EMIT(parl * XY + px * Y + y, parl * XY + px * Y + py);
                     if (ok) add_wire(g, layer_first, parl, px, px, miny, maxy, stamp);
                 }
@@ -342,6 +363,7 @@ __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatch
 #undef EMIT
             if (!ok) set_error(g.err, ERR_CAPACITY);
             r[0] = cnt;
+            if (nvias) atomicAdd(&g.stats[1], (unsigned long long)nvias);
         }
         __syncwarp(gmask);
     }

@@ -207,6 +207,8 @@ void Router::ensure_device() {
     d_tree_par.upload(tree_par, s);
     d_scratch_off.upload(scratch_off, s);
     d_scratch.alloc((size_t)pattern_scratch_doubles(scratch_nodes));
+    d_vcnt.alloc((size_t)go.g.N);
+    cuda_check(cudaMemsetAsync(d_vcnt.p, 0, (size_t)go.g.N * sizeof(int), s), "memset");
     d_route_off1.upload(route_off1, s);
     d_route_cap1.upload(route_cap1, s);
     d_route_off.alloc(route_off1.size());
@@ -251,6 +253,7 @@ void Router::run() {
     kt.s = s;
     kt.reset();
     go.reset_demand(s);
+    cuda_check(cudaMemsetAsync(d_vcnt.p, 0, (size_t)go.g.N * sizeof(int), s), "memset");
     global_stamp = 0;
     h_routes_valid = false;
     const int R = (int)ns.nets.size();
@@ -326,7 +329,8 @@ void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<in
         const int off = batch_off[bi], n = batch_off[bi + 1] - off;
         const int stamp = bi + 1;
         if (timed) kt.begin(KC_COST);
-        launch_cost_refresh(go.g, true, s);
+        if (split_commit) launch_cost_refresh(go.g, true, s);
+        else launch_commit_refresh(go.g, d_vcnt.p, bi, true, s);  // commits batch bi-1 (stamp bi)
         if (timed) kt.end(KC_COST);
         if (timed) kt.begin(KC_PATTERN);
         // batched form: the large (c = 0) and small (c = 2) classes are forked
@@ -340,6 +344,7 @@ void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<in
             TreeBatchDev tb{d_ids.p + a, d_tree_off.p, d_tree_nodes.p, d_tree_par.p, d_route_off.p, d_route_cap.p,
                             routes.p, d_scratch.p, d_scratch_off.p, scratch_nodes, e - a};
             tb.queue = d_queue.p + 3 * bi + c;
+            tb.vcnt = split_commit ? nullptr : d_vcnt.p;
             cudaStream_t cs = s;
             if (batched) {
                 tb.tile = c == 0 ? 32 : (c == 1 ? kPatternNodeTile : 6);
@@ -363,6 +368,8 @@ void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<in
             cuda_check(cudaStreamWaitEvent(s, ev_join[j], 0), "join");
         }
         if (timed) kt.end(KC_PATTERN);
+        st.launches += 1;
+        if (!split_commit) continue;
         if (timed) kt.begin(KC_WIRE_COMMIT);
         launch_wire_commit(go.g, stamp, true, s);
         if (timed) kt.end(KC_WIRE_COMMIT);
@@ -370,7 +377,13 @@ void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<in
         if (timed) kt.begin(KC_VIA_COMMIT);
         launch_via_commit(go.g, vb, stamp, 1, s);
         if (timed) kt.end(KC_VIA_COMMIT);
-        st.launches += 3;
+        st.launches += 2;
+    }
+    if (!split_commit && nb > 0) {  // commit of the last batch; its costs are refreshed when next needed
+        if (timed) kt.begin(KC_COST);
+        launch_commit_refresh(go.g, d_vcnt.p, nb, false, s);
+        if (timed) kt.end(KC_COST);
+        st.launches += 1;
     }
 }
 
@@ -815,6 +828,7 @@ void Router::compute_score() {
         for (size_t i = 0; i < d.sel.size(); i++) pin_vias += d.sel[i] < d.X * d.Y;
     }
     cost_cells = h[2];
+    commit_cells = h[3];
     score_wl = (double)(int64_t)h[0] * d.unit_wire;
     score_via = (double)((int64_t)h[1] + pin_vias) * d.unit_via;
     score_of = of;

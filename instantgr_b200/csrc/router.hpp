@@ -94,6 +94,7 @@ struct ShapeDev {
 
 struct Router {
     int rrr_iters = 1, threads = 0, mode = -1, verbose = 0, batched = 0;
+    int split_commit = 0;  // 1: separate cost refresh, wire commit and via commit launches per phase-1 batch
     Design d;
     NetSet ns;
     GridOwner go;
@@ -129,6 +130,7 @@ struct Router {
     bool h_routes_valid = false;
     // ---- per-run device buffers (grow-only)
     DevBuf<int4> d_hdr;
+    DevBuf<int> d_vcnt;  // via crossings per cell of the current phase-1 batch (fused commit)
     DevBuf<int> d_ids, d_all_ids, of_sum, d_perm, d_map, d_bat, d_act, d_flags, d_queue;
     // launch shape of the tree DP per size class (large, medium, small) and the
     // node count that separates small from medium nets (autotuned, see tune.cpp)
@@ -160,7 +162,7 @@ struct Router {
     DevBuf<unsigned long long> dg_best, dg_packed;
     bool cooperative = true;
     std::vector<DagNet> dag;  // detour DAG of every rerouted net (phase 2)
-    unsigned long long cost_cells = 0;
+    unsigned long long cost_cells = 0, commit_cells = 0;
     // phase-1 plan of the last run (routing order, batches, trees, route capacity in order)
     std::vector<int> plan_ids, plan_batch_off, plan_node_off, plan_nodes, plan_par, plan_cap;
     bool plan_built = false;

@@ -68,6 +68,25 @@ def test_batched_form_matches_plain_form(small_design):
     assert outs[0] == outs[1] == outs[2]
 
 
+def test_fused_batch_commit_matches_split_commit(small_design):
+    """The fused per-track commit + cost refresh of phase 1 gives the demand,
+    routes and statistics of separate cost-refresh, wire-commit and via-commit
+    launches (phase 1 only, where the fusion applies)."""
+    cap, net, d = small_design
+    res = []
+    for split in (1, 0):
+        r = ig.Router(cap, net, rrr_iters=0, batched=1, split_commit=split)
+        r.run()
+        out = str(d / f"split{split}.out")
+        r.write(out)
+        s = r.stats()
+        res.append((r.demand(), open(out).read(), s["wirelength"], s["via_cost"], s["overflow_cost"]))
+        r.close()
+    assert np.array_equal(res[0][0], res[1][0]), "demand differs"
+    assert res[0][1] == res[1][1], "route guides differ"
+    assert res[0][2:] == res[1][2:]
+
+
 def test_router_stats_and_gpu_score(small_design):
     cap, net, d = small_design
     r = ig.Router(cap, net, rrr_iters=1)
