@@ -253,7 +253,7 @@ int igr_generate_custom(int X, int Y, int nets, uint64_t seed, int cap_mode, dou
         p.X = X; p.Y = Y; p.nets = nets; p.seed = seed; p.cap_mode = cap_mode; p.block_frac = block_frac;
         p.pin_mode = pin_mode; p.hifanout_frac = hifanout_frac; p.bbox_median = bbox_median;
         p.bbox_sigma = bbox_sigma; p.hotspots = hotspots; p.hotspot_frac = hotspot_frac;
-        p.hotspot_sigma = 0.04 * std::max(X, Y);
+        p.hotspot_sigma = 0.1 * std::max(X, Y);
         generate_design(p, cap_path, net_path);
     });
 }

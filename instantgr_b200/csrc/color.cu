@@ -24,6 +24,7 @@
 // block with block barriers.  Every grid barrier gives up after two seconds
 // and reports ERR_TIMEOUT instead of waiting forever.
 #include "gridsync.cuh"
+#include "host.hpp"
 
 namespace igr {
 
@@ -275,28 +276,42 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
 
 void build_claims(int nshapes, const int *pt_off, const int *pts, const int *h_off, const int *hseg,
                   const int *v_off, const int *vseg, int X, int Y, int sparsity, std::vector<int> &off,
-                  std::vector<int> &cells, int /*threads*/) {
+                  std::vector<int> &cells, int threads) {
     static const int dx[4] = {0, 0, -1, 1}, dy[4] = {0, -1, 0, 0};
-    off.assign(nshapes + 1, 0);
-    cells.clear();
-    for (int k = 0; k < nshapes; k++) {
+    // cells of shape k in claim order; emit(cell) is called for each
+    auto walk = [&](int k, auto &&emit) {
         for (int i = pt_off[k]; i < pt_off[k + 1]; i++) {
             const int x = pts[i] / Y, y = pts[i] % Y;
             for (int j = 0; j < 4; j++) {
                 const int nx = x + dx[j], ny = y + dy[j];
-                if (nx >= 0 && nx < X && ny >= 0 && ny < Y) cells.push_back(nx * Y + ny);
+                if (nx >= 0 && nx < X && ny >= 0 && ny < Y) emit(nx * Y + ny);
             }
         }
         for (int i = h_off[k]; i < h_off[k + 1]; i++) {
-            const int s = hseg[2 * i], e = hseg[2 * i + 1], y = s % Y;
-            for (int x = s / Y; x <= e / Y; x += sparsity) cells.push_back(x * Y + y);
+            const int s0 = hseg[2 * i], e0 = hseg[2 * i + 1], y = s0 % Y;
+            for (int x = s0 / Y; x <= e0 / Y; x += sparsity) emit(x * Y + y);
         }
         for (int i = v_off[k]; i < v_off[k + 1]; i++) {
-            const int s = vseg[2 * i], e = vseg[2 * i + 1], x = s / Y;
-            for (int y = s % Y; y <= e % Y; y += sparsity) cells.push_back(x * Y + y);
+            const int s0 = vseg[2 * i], e0 = vseg[2 * i + 1], x = s0 / Y;
+            for (int y = s0 % Y; y <= e0 % Y; y += sparsity) emit(x * Y + y);
         }
-        off[k + 1] = (int)cells.size();
-    }
+    };
+    off.assign(nshapes + 1, 0);
+    parallel_for(nshapes, threads, [&](int b, int e) {
+        for (int k = b; k < e; k++) {
+            int n = 0;
+            walk(k, [&](int) { n++; });
+            off[k + 1] = n;
+        }
+    });
+    for (int k = 0; k < nshapes; k++) off[k + 1] += off[k];
+    cells.resize(off[nshapes]);
+    parallel_for(nshapes, threads, [&](int b, int e) {
+        for (int k = b; k < e; k++) {
+            int *o = cells.data() + off[k];
+            walk(k, [&](int c) { *o++ = c; });
+        }
+    });
 }
 
 int run_coloring(ColorDev &c, int max_batch, cudaStream_t s) {

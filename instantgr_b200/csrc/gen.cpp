@@ -134,8 +134,17 @@ void generate_design(const GenParams &p, const char *cap_path, const char *net_p
         double cx, cy;
         if (!hx.empty() && rng.uni() < p.hotspot_frac) {
             int h = (int)(rng.next() % hx.size());
-            cx = hx[h] + rng.normal() * p.hotspot_sigma;
-            cy = hy[h] + rng.normal() * p.hotspot_sigma;
+            // centres off the grid are drawn again (clamping them would pile
+            // the boxes of a hotspot near a corner onto the grid boundary)
+            int tries = 0;
+            do {
+                cx = hx[h] + rng.normal() * p.hotspot_sigma;
+                cy = hy[h] + rng.normal() * p.hotspot_sigma;
+            } while ((cx < 0 || cx >= X || cy < 0 || cy >= Y) && ++tries < 16);
+            if (tries == 16) {
+                cx = rng.uni() * X;
+                cy = rng.uni() * Y;
+            }
         } else {
             cx = rng.uni() * X;
             cy = rng.uni() * Y;

@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <numeric>
+#include <thread>
 
 namespace igr {
 
@@ -116,7 +117,7 @@ void KernelTimer::reset() {
     for (int k = 0; k < KC_N; k++) { ms[k] = 0; launches[k] = 0; }
 }
 
-void ShapeDev::upload(const ShapeSet &sh, int X, int Y, int sp, cudaStream_t st) {
+void ShapeDev::upload(const ShapeSet &sh, int X, int Y, int sp, cudaStream_t st, int threads) {
     pt_off.upload(sh.pt_off, st); pts.upload(sh.pts, st); pt_net.upload(sh.pt_net, st);
     h_off.upload(sh.h_off, st); hseg.upload(sh.hseg, st);
     v_off.upload(sh.v_off, st); vseg.upload(sh.vseg, st);
@@ -125,7 +126,7 @@ void ShapeDev::upload(const ShapeSet &sh, int X, int Y, int sp, cudaStream_t st)
     sparsity = sp;
     std::vector<int> co, cl;
     build_claims(nshapes, sh.pt_off.data(), sh.pts.data(), sh.h_off.data(), sh.hseg.data(), sh.v_off.data(),
-                 sh.vseg.data(), X, Y, sp, co, cl, 0);
+                 sh.vseg.data(), X, Y, sp, co, cl, threads);
     claim_off.upload(co, st);
     claim.upload(cl, st);
     cuda_check(cudaStreamSynchronize(st), "claims");  // host vectors go out of scope
@@ -147,6 +148,17 @@ Router::~Router() {
 
 void Router::open(const char *cap, const char *net) {
     const double t0 = now_s();
+    // bring up the CUDA context of the caller's device while the host parses
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+    std::thread ctx_init([dev] {
+        if (dev >= 0 && cudaSetDevice(dev) == cudaSuccess) cudaFree(nullptr);
+        cudaGetLastError();
+    });
+    struct Joiner {
+        std::thread &t;
+        ~Joiner() { if (t.joinable()) t.join(); }
+    } joiner{ctx_init};
     read_design(d, cap, net, threads);
     build_netset(d, ns, threads);
     // trees in DFS preorder, net-id order, and the phase-1 route record layout
@@ -186,6 +198,7 @@ void Router::open(const char *cap, const char *net) {
 // opening a design (parsing, pin selection, trees) needs no GPU.
 void Router::ensure_device() {
     if (s) return;
+    const double t0 = now_s();
     cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
     for (int i = 0; i < 2; i++) {
         cuda_check(cudaStreamCreateWithFlags(&s_cls[i], cudaStreamNonBlocking), "stream");
@@ -215,16 +228,37 @@ void Router::ensure_device() {
     d_route_cap.alloc(route_cap1.size());
     ShapeSet sh;
     const int R = (int)ns.nets.size();
+    sh.pt_off.assign(R + 1, 0);
+    sh.h_off.assign(R + 1, 0);
+    sh.v_off.assign(R + 1, 0);
     for (int i = 0; i < R; i++) {
         const RNet &r = ns.nets[i];
-        for (int q : r.points) { sh.pts.push_back(q); sh.pt_net.push_back(i); }
-        sh.pt_off.push_back((int)sh.pts.size());
-        for (auto &sg : r.hseg) { sh.hseg.push_back(sg.first); sh.hseg.push_back(sg.second); }
-        sh.h_off.push_back((int)(sh.hseg.size() / 2));
-        for (auto &sg : r.vseg) { sh.vseg.push_back(sg.first); sh.vseg.push_back(sg.second); }
-        sh.v_off.push_back((int)(sh.vseg.size() / 2));
+        sh.pt_off[i + 1] = sh.pt_off[i] + (int)r.points.size();
+        sh.h_off[i + 1] = sh.h_off[i] + (int)r.hseg.size();
+        sh.v_off[i + 1] = sh.v_off[i] + (int)r.vseg.size();
     }
-    d_shapes1.upload(sh, X, Y, 15, s);  // phase 1 samples every 15th segment cell (database_cuda.hpp:439)
+    sh.pts.resize(sh.pt_off[R]);
+    sh.pt_net.resize(sh.pt_off[R]);
+    sh.hseg.resize(2 * (size_t)sh.h_off[R]);
+    sh.vseg.resize(2 * (size_t)sh.v_off[R]);
+    parallel_for(R, threads, [&](int b, int e) {
+        for (int i = b; i < e; i++) {
+            const RNet &r = ns.nets[i];
+            for (size_t j = 0; j < r.points.size(); j++) {
+                sh.pts[sh.pt_off[i] + j] = r.points[j];
+                sh.pt_net[sh.pt_off[i] + j] = i;
+            }
+            for (size_t j = 0; j < r.hseg.size(); j++) {
+                sh.hseg[2 * (sh.h_off[i] + j)] = r.hseg[j].first;
+                sh.hseg[2 * (sh.h_off[i] + j) + 1] = r.hseg[j].second;
+            }
+            for (size_t j = 0; j < r.vseg.size(); j++) {
+                sh.vseg[2 * (sh.v_off[i] + j)] = r.vseg[j].first;
+                sh.vseg[2 * (sh.v_off[i] + j) + 1] = r.vseg[j].second;
+            }
+        }
+    });
+    d_shapes1.upload(sh, X, Y, 15, s, threads);  // phase 1 samples every 15th segment cell (database_cuda.hpp:439)
     // phase-1 colouring ranks: the reversed routing priority (the last rank wins conflicts)
     std::vector<int> perm1(order1.rbegin(), order1.rend());
     d_perm1.upload(perm1, s);
@@ -232,6 +266,7 @@ void Router::ensure_device() {
     std::iota(ids.begin(), ids.end(), 0);
     d_all_ids.upload(ids, s);
     cuda_check(cudaStreamSynchronize(s), "inputs");
+    if (verbose) std::fprintf(stderr, "[igr] device setup %.3fs\n", now_s() - t0);
 }
 
 // Grows the route buffer to `need` ints, keeping the records already written.
@@ -682,7 +717,7 @@ bool Router::rrr_pass(int iter) {
         sh.v_off.push_back((int)(sh.vseg.size() / 2));
     }
     ShapeDev shd;
-    shd.upload(sh, X, Y, mode_eff >= 1 ? 2 : 15, s);
+    shd.upload(sh, X, Y, mode_eff >= 1 ? 2 : 15, s, threads);
     st.h2d_bytes += (int64_t)(sh.pts.size() * 2 + sh.hseg.size() + sh.vseg.size() + 3 * of_nets.size()) * 4;
     std::vector<int> local(of_nets.size());
     std::iota(local.begin(), local.end(), 0);  // shape k belongs to of_nets[k]; of_nets is in priority order
@@ -835,10 +870,13 @@ void Router::compute_score() {
 }
 
 void Router::write(const char *out) {
+    const double t0 = now_s();
     fetch_routes();
+    const double t1 = now_s();
     RouteSource rs;
     rs.routes_of = [&](int net) -> const int * { return h_routes.empty() ? nullptr : route_of(net); };
     write_guides(d, ns, rs, out, threads);
+    if (verbose) std::fprintf(stderr, "[igr] routes to host %.3fs, guides written %.3fs\n", t1 - t0, now_s() - t1);
 }
 
 }  // namespace igr

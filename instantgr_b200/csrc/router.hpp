@@ -89,7 +89,7 @@ struct ShapeSet {
 struct ShapeDev {
     DevBuf<int> pt_off, pts, pt_net, h_off, hseg, v_off, vseg, claim_off, claim;
     int npts = 0, nshapes = 0, sparsity = 0;
-    void upload(const ShapeSet &s, int X, int Y, int sparsity, cudaStream_t st);
+    void upload(const ShapeSet &s, int X, int Y, int sparsity, cudaStream_t st, int threads = 0);
 };
 
 struct Router {
