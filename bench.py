@@ -128,7 +128,8 @@ def measured_peaks() -> dict:
 
 
 def profile_traffic() -> dict:
-    """Per-launch DRAM traffic of the cost refresh from the committed ncu summary, if any."""
+    """Per-launch DRAM traffic of the profiled kernels (ncu dram__bytes_read.sum +
+    dram__bytes_write.sum) from the committed summary, if any."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(p):
         return json.load(open(p))
@@ -241,37 +242,49 @@ def main():
     sb, sp = rb.stats(), rp.stats()
     same = all(sb[k] == sp[k] for k in ("wirelength", "via_cost", "overflow_cost"))
 
-    # e2e: the whole `-cap/-net/-out` call with host files (read, route, write), batched form
+    # e2e: the whole `-cap/-net/-out` flow through the public API with host files
+    # (read, upload, route, download, write guides), batched form
     out = os.path.join(args.workdir, f"guides_r{rank}.out")
-    ms_e2e, _, _ = timed(None, lambda: ig.route_files(cap, net, out, rrr_iters=args.rrr_iters, batched=1))
+    e2e_bytes = []
+
+    def e2e_step():
+        r = ig.Router(cap, net, rrr_iters=args.rrr_iters, batched=1)
+        r.run()
+        r.write(out)
+        st = r.stats()
+        e2e_bytes.append((st["setup_h2d_bytes"] + st["h2d_bytes"], st["d2h_bytes"]))
+        r.close()
+
+    ms_e2e, _, _ = timed(None, e2e_step)
 
     result = None
     if rank == 0:
         value = design_nets * args.steps * world / (ms_b / 1e3)
         value_plain = design_nets * args.steps * world / (ms_p / 1e3)
         e2e_value = design_nets * args.steps * world / (ms_e2e / 1e3)
-        L, X, Y = 9, cfg["X"], cfg["Y"]
-        cells = L * X * Y
         plan = rp.plan()
-        # per step: net ordering, batch offsets (route_files also uploads the grid and trees)
-        h2d = cells * 4 + (X + Y) * 4 + (plan["nodes"].size * 2 + plan["node_off"].size * 2
-                                         + plan["net_ids"].size * 3) * 4
-        d2h = int(sum(plan["route_cap"])) * 4
-        # dominant kernel of the plain form and the cost-refresh roofline
-        dom = max(ks_p, key=lambda k: ks_p[k]["ms"])
-        cr = ks_p["cost_refresh"]
+        h2d, d2h = e2e_bytes[-1]
+        # roofline of the dominant kernel class of the plain form (every class is
+        # timed per launch there) and, beside it, of every class with byte counts
         pk = measured_peaks()
         tr = profile_traffic()
-        ach = cr["bytes"] / (cr["ms"] / 1e3) / 1e9 if cr["ms"] else 0.0
-        roof = dict(kernel="cost_refresh (fused wire/via cost + f64 Sklansky prefix sums)", bound="hbm",
-                    achieved=round(ach, 1), peak=pk["hbm_gbs"], unit="GB/s",
-                    frac=round(ach / pk["hbm_gbs"], 4), peak_src=pk["src"],
-                    traffic=tr.get("cost_refresh_bytes_per_launch"),
-                    algorithmic_bytes_per_launch=cr["bytes"] / max(cr["launches"], 1),
-                    avg_launch_us=1e3 * cr["ms"] / max(cr["launches"], 1),
-                    dominant_kernel=dom,
-                    kernel_ms_per_step_plain={k: round(v["ms"] / args.steps, 3) for k, v in ks_p.items()},
-                    kernel_ms_per_step_batched={k: round(v["ms"] / args.steps, 3) for k, v in ks_b.items()})
+
+        def roof_of(k):
+            v = ks_p[k]
+            ach = v["bytes"] / (v["ms"] / 1e3) / 1e9 if v["ms"] else 0.0
+            n = max(v["launches"], 1)
+            return dict(kernel=KERNEL_NAMES.get(k, k), bound="hbm", achieved=round(ach, 1), peak=pk["hbm_gbs"],
+                        unit="GB/s", frac=round(ach / pk["hbm_gbs"], 4), peak_src=pk["src"],
+                        traffic=tr.get(f"{k}_bytes_per_launch"),
+                        algorithmic_bytes_per_launch=round(v["bytes"] / n, 1),
+                        avg_launch_us=round(1e3 * v["ms"] / n, 3))
+
+        dom = max((k for k in ks_p if ks_p[k]["bytes"] > 0), key=lambda k: ks_p[k]["ms"])
+        roof = roof_of(dom)
+        roof["dominant_kernel"] = dom
+        roof["classes"] = {k: roof_of(k) for k in ks_p if ks_p[k]["bytes"] > 0}
+        roof["kernel_ms_per_step_plain"] = {k: round(v["ms"] / args.steps, 3) for k, v in ks_p.items()}
+        roof["kernel_ms_per_step_batched"] = {k: round(v["ms"] / args.steps, 3) for k, v in ks_b.items()}
         cpu = None
         if world == 1:
             try:
@@ -306,6 +319,13 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     return result
+
+
+KERNEL_NAMES = {
+    "cost_refresh": "commit_refresh / cost_refresh (fused batch commit, wire/via cost, f64 Sklansky prefix sums)",
+    "coloring": "coloring_kernel (persistent cooperative batch colouring)",
+    "pattern_dp": "pattern_route_kernel (tree DP per net, phase 1)",
+}
 
 
 def bench_reference(args, rank, world, workload):

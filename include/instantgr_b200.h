@@ -77,13 +77,18 @@ int igr_router_write(igr_router *r, const char *out_path);
  * src/graph.hpp:148-169), [5] route wall seconds, [6] phase-1 batches,
  * [7] phase-1 device ms, [8] rip-up/reroute device ms, [9] host DAG ms,
  * [10] kernel launches, [11] design nets, [12] colouring rounds,
- * [13] host-to-device bytes, [14] device-to-host bytes. */
+ * [13] host-to-device bytes, [14] device-to-host bytes (of the run and the
+ * route download for writing), [15] host-to-device bytes of the one-time
+ * device setup (grid, trees, conflict shapes). */
 int igr_router_stats(igr_router *r, double *out, int n);
 /* Per-kernel-class device time of the last run (needs opt->profile): for
  * class k in {cost refresh (with the fused phase-1 commit), tree DP, wire
  * commit, via commit, DAG DP, colouring, rip-up/marking, phase-1 graph},
  * out[3k] = launches, out[3k+1] = milliseconds, out[3k+2] = algorithmic DRAM
- * bytes (cost refresh: 20 per refreshed cell + 12 per committed cell). */
+ * bytes (cost refresh: 20 per refreshed cell + 12 per committed cell;
+ * colouring: 12 per claimed cell, 8 per commit point check, 12 per blocking
+ * point check, 8 per release check, 8 per active-list entry scanned; tree
+ * DP: 32 per node, 144 per straight and 360 per bent tree edge). */
 int igr_router_kstats(igr_router *r, double *out, int n);
 /* Phase-1 plan of the last run: routing order, batch offsets and trees.
  * sizes[0..2] receive the number of nets, batches and tree nodes; the arrays

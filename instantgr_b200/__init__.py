@@ -176,7 +176,8 @@ KERNEL_CLASSES = ["cost_refresh", "pattern_dp", "wire_commit", "via_commit", "da
                   "phase1_graph"]
 
 STATS = ["routing_nets", "rerouted", "wirelength", "via_cost", "overflow_cost", "route_s", "batches1", "p1_ms",
-         "rrr_ms", "dag_host_ms", "launches", "design_nets", "color_rounds", "h2d_bytes", "d2h_bytes"]
+         "rrr_ms", "dag_host_ms", "launches", "design_nets", "color_rounds", "h2d_bytes", "d2h_bytes",
+         "setup_h2d_bytes"]
 
 
 class Router:

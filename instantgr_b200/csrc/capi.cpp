@@ -113,11 +113,11 @@ int igr_router_write(igr_router *h, const char *out) {
 int igr_router_stats(igr_router *h, double *o, int n) {
     if (!h || !o) return fail(nullptr, IGR_ERR_INVALID, "null argument");
     const auto &r = h->r;
-    double v[15] = {(double)r.ns.nets.size(), (double)r.st.rerouted, r.score_wl, r.score_via, r.score_of,
+    double v[16] = {(double)r.ns.nets.size(), (double)r.st.rerouted, r.score_wl, r.score_via, r.score_of,
                     r.st.wall, (double)r.st.batches1, r.st.p1_ms, r.st.rrr_ms, r.st.dag_host_ms,
                     (double)r.st.launches, (double)r.d.num_nets(), (double)r.st.color_rounds,
-                    (double)r.st.h2d_bytes, (double)r.st.d2h_bytes};
-    for (int k = 0; k < n && k < 15; k++) o[k] = v[k];
+                    (double)r.st.h2d_bytes, (double)r.st.d2h_bytes, (double)r.setup_h2d};
+    for (int k = 0; k < n && k < 16; k++) o[k] = v[k];
     return IGR_OK;
 }
 
@@ -126,7 +126,8 @@ int igr_router_kstats(igr_router *h, double *o, int n) {
     const auto &r = h->r;
     for (int k = 0; k < KC_N; k++) {
         double v[3] = {(double)r.kt.launches[k], r.kt.ms[k],
-                       k == KC_COST ? 20.0 * (double)r.cost_cells + 12.0 * (double)r.commit_cells : 0.0};
+                       k == KC_COST ? 20.0 * (double)r.cost_cells + 12.0 * (double)r.commit_cells
+                                    : (k == KC_COLOR ? r.color_bytes : (k == KC_PATTERN ? r.dp_bytes : 0.0))};
         for (int j = 0; j < 3; j++)
             if (3 * k + j < n) o[3 * k + j] = v[j];
     }

@@ -44,6 +44,13 @@ constexpr int kBlockRounds = 2 * kGroups;
 // (by batch parity)
 enum : int { F_NB = 2, F_BAR = 4, F_ERR = 6, F_ROUNDS = 8, F_LOST = 9, F_CAND = 10, F_LEFT = 11 };
 
+// memory operations of this thread, summed into c.ops at the end (roofline
+// accounting): claimed cells, points checked for commit, points checked for
+// blocking, cells checked for release, list entries scanned
+struct Ops {
+    unsigned long long claims = 0, points = 0, bpoints = 0, releases = 0, scans = 0;
+};
+
 struct Stage {
     int buf[kBuf];
     int n, base;
@@ -78,11 +85,12 @@ __device__ __forceinline__ int owner(const ColorDev &c, int cell) { return __ldc
 
 // Candidates claim their cells, four cells in flight per lane.  Blocks blk,
 // blk+nblk, ... of the workers; group j of a block takes list entry j.
-__device__ __forceinline__ void claim_phase(const ColorDev &c, const int *list, int n, int blk, int nblk) {
+__device__ __forceinline__ void claim_phase(const ColorDev &c, const int *list, int n, int blk, int nblk, Ops &ops) {
     const int gl = threadIdx.x % kG;
     for (int idx = blk * kGroups + threadIdx.x / kG; idx < n; idx += nblk * kGroups) {
         const int k = list[idx];
         const int4 h = c.hdr[k];
+        if (gl == 0) ops.claims += h.y - h.x;
         for (int i = h.x + gl; i < h.y; i += 4 * kG) {
             const int c0 = __ldg(c.claim + i);
             const int c1 = i + kG < h.y ? __ldg(c.claim + i + kG) : -1;
@@ -99,7 +107,7 @@ __device__ __forceinline__ void claim_phase(const ColorDev &c, const int *list, 
 // Candidates owning all their points join batch `cur`; the others go to the
 // lost list.  Block-uniform loop (staging and flushes).
 __device__ __forceinline__ void commit_phase(const ColorDev &c, Stage &st, const int *list, int n, int cur,
-                                             int *lost_cnt, int blk, int nblk) {
+                                             int *lost_cnt, int blk, int nblk, Ops &ops) {
     const int lane = threadIdx.x & 31, grp = lane / kG, gl = lane % kG;
     int it = 0;
     for (int b0 = blk * kGroups; b0 < n; b0 += nblk * kGroups, it++) {
@@ -109,6 +117,7 @@ __device__ __forceinline__ void commit_phase(const ColorDev &c, Stage &st, const
         bool ok = true;
         if (valid) {
             const int4 h = c.hdr[k];
+            if (gl == 0) ops.points += h.w - h.z;
             for (int i = h.z + gl; i < h.w; i += 2 * kG) {
                 const int p0 = __ldg(c.pts + i);
                 const int p1 = i + kG < h.w ? __ldg(c.pts + i + kG) : -1;
@@ -128,7 +137,8 @@ __device__ __forceinline__ void commit_phase(const ColorDev &c, Stage &st, const
 // Lost nets with a point owned by a member are blocked and release their
 // cells at once (a blocked net's cells are no member's points, so the release
 // cannot change another net's check); the others stay candidates.
-__device__ __forceinline__ void block_phase(const ColorDev &c, Stage &st, int n, int *cand_cnt, int blk, int nblk) {
+__device__ __forceinline__ void block_phase(const ColorDev &c, Stage &st, int n, int *cand_cnt, int blk, int nblk,
+                                            Ops &ops) {
     const int lane = threadIdx.x & 31, grp = lane / kG, gl = lane % kG;
     int it = 0;
     for (int b0 = blk * kGroups; b0 < n; b0 += nblk * kGroups, it++) {
@@ -139,6 +149,7 @@ __device__ __forceinline__ void block_phase(const ColorDev &c, Stage &st, int n,
         bool hit = false;
         if (valid) {
             h = c.hdr[k];
+            if (gl == 0) ops.bpoints += h.w - h.z;
             for (int i = h.z + gl; i < h.w; i += 2 * kG) {
                 const int p0 = __ldg(c.pts + i);
                 const int p1 = i + kG < h.w ? __ldg(c.pts + i + kG) : -1;
@@ -151,6 +162,7 @@ __device__ __forceinline__ void block_phase(const ColorDev &c, Stage &st, int n,
         }
         const bool blocked = ((__ballot_sync(0xffffffffu, hit) >> (grp * kG)) & kGroupMask) != 0;
         if (valid && blocked) {
+            if (gl == 0) ops.releases += h.y - h.x;
             for (int i = h.x + gl; i < h.y; i += 4 * kG) {
                 int cl[4], ow[4];
 #pragma unroll
@@ -170,7 +182,7 @@ __device__ __forceinline__ void block_phase(const ColorDev &c, Stage &st, int n,
 
 // Rounds `round`.. of batch `cur` in this block alone, over the nc candidates
 // in c.cand.  Every thread of the block calls it.
-__device__ void block_rounds(const ColorDev &c, Stage &st, int round, int nc, int cur, int *rounds_ctr) {
+__device__ void block_rounds(const ColorDev &c, Stage &st, int round, int nc, int cur, int *rounds_ctr, Ops &ops) {
     __shared__ int s_lost, s_cand;
     for (; round < 30; round++) {
         if (threadIdx.x == 0) {
@@ -179,12 +191,12 @@ __device__ void block_rounds(const ColorDev &c, Stage &st, int round, int nc, in
             (*rounds_ctr)++;
         }
         __syncthreads();
-        claim_phase(c, c.cand, nc, 0, 1);
+        claim_phase(c, c.cand, nc, 0, 1, ops);
         __syncthreads();
-        commit_phase(c, st, c.cand, nc, cur, &s_lost, 0, 1);
+        commit_phase(c, st, c.cand, nc, cur, &s_lost, 0, 1, ops);
         const int nl = s_lost;  // flush ends with a block barrier
         if (nl == nc) break;    // no net joined in this round
-        block_phase(c, st, nl, &s_cand, 0, 1);
+        block_phase(c, st, nl, &s_cand, 0, 1, ops);
         nc = s_cand;
         __syncthreads();  // every thread has read the counters before they are reset
         if (nc == 0) break;
@@ -207,6 +219,17 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
     unsigned *bar = reinterpret_cast<unsigned *>(c.flags + F_BAR);
     int *err = c.flags + F_ERR;
     unsigned epoch = 0;
+    Ops ops;
+    auto sum_ops = [&]() {
+        if (!c.ops) return;
+        unsigned long long v[5] = {ops.claims, ops.points, ops.bpoints, ops.releases, ops.scans};
+#pragma unroll
+        for (int j = 0; j < 5; j++) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_down_sync(0xffffffffu, v[j], o);
+            if (lane == 0 && v[j]) atomicAdd(c.ops + j, v[j]);
+        }
+    };
     if (threadIdx.x == 0) st.n = 0;
     int *act = c.active, *act2 = c.active2;
     for (int k = tid; k < c.n; k += nth) {
@@ -231,24 +254,24 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
                 flags[F_ROUNDS]++;
                 flags[F_LOST] = 0;
             }
-            claim_phase(c, cand, nc, blockIdx.x, gridDim.x);
+            claim_phase(c, cand, nc, blockIdx.x, gridDim.x, ops);
             if (!grid_sync(bar, err, epoch)) return;
             if (tid == 0) {
                 flags[F_CAND] = 0;
                 if (round == 0) flags[F_LEFT + ((cur + 1) & 1)] = 0;
             }
-            commit_phase(c, st, cand, nc, cur, flags + F_LOST, blockIdx.x, gridDim.x);
+            commit_phase(c, st, cand, nc, cur, flags + F_LOST, blockIdx.x, gridDim.x, ops);
             if (!grid_sync(bar, err, epoch)) return;
             const int nl = vflags[F_LOST];
             if (nl == nc) break;  // no net joined in this round
-            block_phase(c, st, nl, flags + F_CAND, blockIdx.x, gridDim.x);
+            block_phase(c, st, nl, flags + F_CAND, blockIdx.x, gridDim.x, ops);
             if (!grid_sync(bar, err, epoch)) return;
             cand = c.cand;
             nc = vflags[F_CAND];
             if (nc == 0) break;
         }
         if (tail) {
-            if (blockIdx.x == 0) block_rounds(c, st, round, nc, cur, flags + F_ROUNDS);
+            if (blockIdx.x == 0) block_rounds(c, st, round, nc, cur, flags + F_ROUNDS, ops);
             if (!grid_sync(bar, err, epoch)) return;
         }
         // nets still without a batch stay active; the map is cleared for the next batch
@@ -257,6 +280,7 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
         for (int b0 = blockIdx.x * kThreads; b0 < na; b0 += nth, it++) {
             const int i = b0 + threadIdx.x;
             const int k = i < na ? act[i] : -1;
+            if (k >= 0) ops.scans++;
             stage(st, k >= 0 && __ldcg(c.batch + k) == -1, k, lane);
             if ((it + 1) % (kBuf / kThreads) == 0) flush(st, act2, flags + F_LEFT + (cur & 1));
         }
@@ -266,10 +290,12 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
         int *t = act; act = act2; act2 = t;
         if (na == 0) {
             if (tid == 0) flags[F_NB] = cur + 1;
+            sum_ops();
             return;
         }
     }
     if (tid == 0) flags[F_NB] = max_batches;
+    sum_ops();
 }
 
 }  // namespace

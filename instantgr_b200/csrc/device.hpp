@@ -174,6 +174,9 @@ struct ColorDev {
     // round, nets that lost a point in a round
     int *active = nullptr, *active2 = nullptr, *cand = nullptr, *lost = nullptr;
     int4 *hdr = nullptr;      // [n] per rank: claim begin/end, point begin/end
+    // optional [5] operation counts, accumulated: claimed cells, commit point
+    // checks, blocking point checks, release checks, list entries scanned
+    unsigned long long *ops = nullptr;
     int *flags = nullptr;     // [16] device flags
     int rounds = 0;           // out: colouring rounds run
 };

@@ -130,6 +130,8 @@ void ShapeDev::upload(const ShapeSet &sh, int X, int Y, int sp, cudaStream_t st,
     claim_off.upload(co, st);
     claim.upload(cl, st);
     cuda_check(cudaStreamSynchronize(st), "claims");  // host vectors go out of scope
+    bytes = 4 * (int64_t)(sh.pt_off.size() + 2 * sh.pts.size() + sh.h_off.size() + sh.hseg.size() +
+                          sh.v_off.size() + sh.vseg.size() + co.size() + cl.size());
 }
 
 // ------------------------------------------------------------------ router
@@ -185,6 +187,21 @@ void Router::open(const char *cap, const char *net) {
     }
     route_off1 = route_off;
     route_cap1 = route_cap;
+    // algorithmic bytes of one phase-1 tree DP pass: per node the 8 via-column
+    // costs (f32); per straight edge 9 layers x 2 presum values (f64); per bent
+    // edge 18 legs x 2 presum values and the two corner via columns (9 x f32 each)
+    dp_bytes = 0;
+    for (int i = 0; i < R; i++) {
+        const int a = tree_off[i], m = tree_off[i + 1] - a;
+        dp_bytes += 32.0 * m;
+        for (int j = 1; j < m; j++) {
+            const int p = tree_par[a + j];
+            if (p < 0 || p >= j) continue;
+            const int v = tree_nodes[a + j], pv = tree_nodes[a + p];
+            const int x = v / ns.Y % ns.X, y = v % ns.Y, px = pv / ns.Y % ns.X, py = pv % ns.Y;
+            dp_bytes += (x == px || y == py) ? 144.0 : 360.0;
+        }
+    }
     // phase-1 routing priority: HPWL, largest first (Lshape_route.hpp:170-172),
     // with the reference's (unstable) std::sort and comparator
     order1.resize(R);
@@ -265,6 +282,10 @@ void Router::ensure_device() {
     std::vector<int> ids(R);
     std::iota(ids.begin(), ids.end(), 0);
     d_all_ids.upload(ids, s);
+    // host-to-device bytes of the setup: grid, trees, record layout, conflict shapes, ranks
+    setup_h2d = (int64_t)go.g.N * 4 + 4 * (int64_t)(X + Y - 2) + 8 * L + 4 * (int64_t)tree_off.size() +
+                8 * (int64_t)tree_nodes.size() + 8 * (int64_t)scratch_off.size() + 12 * (int64_t)R +
+                d_shapes1.bytes + 8 * (int64_t)R;
     cuda_check(cudaStreamSynchronize(s), "inputs");
     if (verbose) std::fprintf(stderr, "[igr] device setup %.3fs\n", now_s() - t0);
 }
@@ -289,6 +310,8 @@ void Router::run() {
     kt.reset();
     go.reset_demand(s);
     cuda_check(cudaMemsetAsync(d_vcnt.p, 0, (size_t)go.g.N * sizeof(int), s), "memset");
+    d_cops.alloc(5);
+    cuda_check(cudaMemsetAsync(d_cops.p, 0, 5 * sizeof(unsigned long long), s), "memset");
     global_stamp = 0;
     h_routes_valid = false;
     const int R = (int)ns.nets.size();
@@ -625,6 +648,7 @@ int Router::run_color(int n, const int *d_perm_ranks, const ShapeDev &shapes, in
     cd.claim_off = shapes.claim_off.p; cd.claim = shapes.claim.p;
     cd.active = d_act.p; cd.active2 = d_act.p + n; cd.cand = d_act.p + 2 * (size_t)n; cd.lost = d_act.p + 3 * (size_t)n;
     cd.hdr = d_hdr.p;
+    cd.ops = d_cops.p;
     cd.npts = shapes.npts; cd.map = d_map.p; cd.batch = d_bat.p; cd.flags = d_flags.p;
     kt.begin(KC_COLOR);
     int nb = run_coloring(cd, 0, s);
@@ -855,6 +879,8 @@ void Router::compute_score() {
     double of = 0;
     launch_overflow_cost(go.g, go.score.p, s);
     st.launches += 2;
+    unsigned long long cops[5] = {0, 0, 0, 0, 0};
+    if (d_cops.p) cuda_check(cudaMemcpyAsync(cops, d_cops.p, sizeof cops, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaMemcpyAsync(h, go.stats.p, sizeof h, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaMemcpyAsync(&of, go.score.p, sizeof of, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
@@ -862,6 +888,10 @@ void Router::compute_score() {
         pin_vias = 0;
         for (size_t i = 0; i < d.sel.size(); i++) pin_vias += d.sel[i] < d.X * d.Y;
     }
+    // per claimed cell: 4-byte index + 8-byte read-modify-write; per point check:
+    // index + owner (+ batch of the owner when blocking); per release check:
+    // index + owner; per list entry scanned: entry + batch
+    color_bytes = 12.0 * cops[0] + 8.0 * cops[1] + 12.0 * cops[2] + 8.0 * cops[3] + 8.0 * cops[4];
     cost_cells = h[2];
     commit_cells = h[3];
     score_wl = (double)(int64_t)h[0] * d.unit_wire;

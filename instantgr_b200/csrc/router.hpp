@@ -89,6 +89,7 @@ struct ShapeSet {
 struct ShapeDev {
     DevBuf<int> pt_off, pts, pt_net, h_off, hseg, v_off, vseg, claim_off, claim;
     int npts = 0, nshapes = 0, sparsity = 0;
+    int64_t bytes = 0;  // host-to-device bytes of the last upload
     void upload(const ShapeSet &s, int X, int Y, int sparsity, cudaStream_t st, int threads = 0);
 };
 
@@ -131,6 +132,10 @@ struct Router {
     // ---- per-run device buffers (grow-only)
     DevBuf<int4> d_hdr;
     DevBuf<int> d_vcnt;  // via crossings per cell of the current phase-1 batch (fused commit)
+    DevBuf<unsigned long long> d_cops;  // colouring operation counts of the current run
+    double color_bytes = 0;             // algorithmic bytes of the colouring kernels of the last run
+    double dp_bytes = 0;                // algorithmic bytes of one phase-1 tree DP pass
+    int64_t setup_h2d = 0;              // host-to-device bytes of the device setup
     DevBuf<int> d_ids, d_all_ids, of_sum, d_perm, d_map, d_bat, d_act, d_flags, d_queue;
     // launch shape of the tree DP per size class (large, medium, small) and the
     // node count that separates small from medium nets (autotuned, see tune.cpp)
