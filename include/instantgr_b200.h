@@ -247,6 +247,43 @@ int igr_build_dag(int X, int Y, int mode, int ntree, const int32_t *pos, const i
 int igr_steiner(int n, const int32_t *x, const int32_t *y, int32_t *node_x, int32_t *node_y, int cap_nodes,
                 int *n_nodes, int32_t *edges, int cap_edges, int *n_edges);
 
+/* ------------------------------------------------------------------ learned congestion seed
+ *
+ * A BF16 convolutional encoder-decoder (six 3x3 convolutions, 32-64
+ * channels, FP32 accumulation in TMEM on the tcgen05 tensor cores) that
+ * predicts the routed demand of every layer from placement features, run on
+ * 256 x 256 GCell tiles with a 16-GCell halo.  No counterpart in InstantGR;
+ * the router uses a model attached with igr_router_set_seed.  Maps are
+ * channels-last [X][Y][16] float arrays: features = pins, RUDY-H, RUDY-V,
+ * blocked-layer fraction, capacity of file layers 0..9 (scaled by 1/8), 0, 0;
+ * predictions/targets = demand of file layers 0..9 (scaled by 1/8), 0 x 6. */
+typedef struct igr_seed igr_seed;
+int igr_seed_create(uint64_t init_seed, igr_seed **out);  /* He-normal initialisation */
+int igr_seed_destroy(igr_seed *m);
+const char *igr_seed_last_error(const igr_seed *m);
+/* Tile size with halo (even) and halo; default 288 and 16. */
+int igr_seed_set_tile(igr_seed *m, int size, int halo);
+/* All parameters (per layer: weights [cout][3][3][cin], then biases); *n gets the count. */
+int igr_seed_params(igr_seed *m, float *out, int64_t cap, int64_t *n);
+int igr_seed_set_params(igr_seed *m, const float *params, int64_t n);
+/* Features of an opened router's design ([X][Y][16]). */
+int igr_seed_features(igr_router *r, float *out);
+/* Training maps kept in device memory: explicit maps, or the features and the
+ * routed demand of a router's last run. */
+int igr_seed_add_map(igr_seed *m, int X, int Y, const float *features, const float *target, int32_t *map_id);
+int igr_seed_add_routed(igr_seed *m, igr_router *r, int32_t *map_id);
+/* `steps` Adam steps on batches of `tiles` random tiles of the training maps;
+ * loss_curve[steps] (optional) receives the mean squared error of each step. */
+int igr_seed_train(igr_seed *m, int steps, int tiles, float lr, uint64_t seed, double *loss_curve);
+/* Mean squared and absolute error of the prediction of training map `map`. */
+int igr_seed_eval(igr_seed *m, int map, double *mse, double *mae);
+/* Prediction of a whole feature map (tiled). */
+int igr_seed_predict(igr_seed *m, int X, int Y, const float *features, float *pred);
+/* One forward and backward pass on T tiles (x, target: [T][size][size][16])
+ * without an update: loss and the gradient of every parameter (layout of
+ * igr_seed_params), for gradient checks. */
+int igr_seed_grad(igr_seed *m, int T, const float *x, const float *target, double *loss, float *grads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,9 @@ EXPORTS = [
     "igr_pattern_route", "igr_pattern_route_static", "igr_commit_wires", "igr_commit_vias", "igr_ripup_wires",
     "igr_mark_overflow",
     "igr_congestion_view", "igr_score", "igr_color_batches", "igr_dag_route", "igr_build_dag", "igr_steiner",
+    "igr_seed_create", "igr_seed_destroy", "igr_seed_last_error", "igr_seed_set_tile", "igr_seed_params",
+    "igr_seed_set_params", "igr_seed_features", "igr_seed_add_map", "igr_seed_add_routed", "igr_seed_train",
+    "igr_seed_eval", "igr_seed_predict", "igr_seed_grad",
 ]
 
 
@@ -121,6 +124,20 @@ def lib() -> C.CDLL:
                                 C.c_int64, C.POINTER(C.c_int64)]
     L.igr_steiner.argtypes = [C.c_int, _i32p, _i32p, _i32p, _i32p, C.c_int, C.POINTER(C.c_int), _i32p,
                               C.c_int, C.POINTER(C.c_int)]
+    L.igr_seed_create.argtypes = [C.c_uint64, C.POINTER(vp)]
+    L.igr_seed_destroy.argtypes = [vp]
+    L.igr_seed_last_error.restype = C.c_char_p
+    L.igr_seed_last_error.argtypes = [vp]
+    L.igr_seed_set_tile.argtypes = [vp, C.c_int, C.c_int]
+    L.igr_seed_params.argtypes = [vp, vp, C.c_int64, C.POINTER(C.c_int64)]
+    L.igr_seed_set_params.argtypes = [vp, _f32p, C.c_int64]
+    L.igr_seed_features.argtypes = [vp, _f32p]
+    L.igr_seed_add_map.argtypes = [vp, C.c_int, C.c_int, _f32p, _f32p, C.POINTER(C.c_int32)]
+    L.igr_seed_add_routed.argtypes = [vp, vp, C.POINTER(C.c_int32)]
+    L.igr_seed_train.argtypes = [vp, C.c_int, C.c_int, C.c_float, C.c_uint64, vp]
+    L.igr_seed_eval.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.igr_seed_predict.argtypes = [vp, C.c_int, C.c_int, _f32p, _f32p]
+    L.igr_seed_grad.argtypes = [vp, C.c_int, _f32p, _f32p, C.POINTER(C.c_double), vp]
     _lib = L
     return L
 
@@ -418,3 +435,90 @@ def steiner(x, y):
     nn, ne = C.c_int(), C.c_int()
     _check(lib().igr_steiner(n, x, y, nx, ny, cap, C.byref(nn), ed, cap, C.byref(ne)))
     return nx[: nn.value], ny[: nn.value], ed[: 2 * ne.value].reshape(-1, 2)
+
+
+class Seed:
+    """Learned congestion seed (igr_seed_*): BF16 convolutional demand predictor
+    trained and run on the tcgen05 tensor cores."""
+
+    def __init__(self, init_seed: int = 1, params=None):
+        self.h = C.c_void_p()
+        self._c(lib().igr_seed_create(init_seed, C.byref(self.h)))
+        if params is not None:
+            self.set_params(params)
+
+    def _c(self, rc):
+        if rc != IGR_OK:
+            raise IgrError(rc, lib().igr_seed_last_error(self.h).decode(errors="replace"))
+
+    def close(self):
+        if self.h:
+            lib().igr_seed_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_tile(self, size: int, halo: int):
+        self._c(lib().igr_seed_set_tile(self.h, size, halo))
+
+    def params(self) -> np.ndarray:
+        n = C.c_int64()
+        self._c(lib().igr_seed_params(self.h, None, 0, C.byref(n)))
+        out = np.zeros(n.value, np.float32)
+        self._c(lib().igr_seed_params(self.h, out.ctypes.data_as(C.c_void_p), n.value, C.byref(n)))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._c(lib().igr_seed_set_params(self.h, p, p.size))
+
+    def add_map(self, features, target) -> int:
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        t = np.ascontiguousarray(target, dtype=np.float32)
+        X, Y = f.shape[0], f.shape[1]
+        i = C.c_int32()
+        self._c(lib().igr_seed_add_map(self.h, X, Y, f.reshape(-1), t.reshape(-1), C.byref(i)))
+        return i.value
+
+    def add_routed(self, router: "Router") -> int:
+        i = C.c_int32()
+        self._c(lib().igr_seed_add_routed(self.h, router.h, C.byref(i)))
+        return i.value
+
+    def train(self, steps: int, tiles: int = 8, lr: float = 1e-3, seed: int = 1) -> np.ndarray:
+        c = np.zeros(max(steps, 1), np.float64)
+        self._c(lib().igr_seed_train(self.h, steps, tiles, lr, seed, c.ctypes.data_as(C.c_void_p)))
+        return c[:steps]
+
+    def evaluate(self, map_id: int):
+        a, b = C.c_double(), C.c_double()
+        self._c(lib().igr_seed_eval(self.h, map_id, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def predict(self, features) -> np.ndarray:
+        f = np.ascontiguousarray(features, dtype=np.float32)
+        out = np.zeros_like(f)
+        self._c(lib().igr_seed_predict(self.h, f.shape[0], f.shape[1], f.reshape(-1), out.reshape(-1)))
+        return out
+
+    def grad(self, x, target):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(target, dtype=np.float32)
+        g = np.zeros(self.params().size, np.float32)
+        loss = C.c_double()
+        self._c(lib().igr_seed_grad(self.h, x.shape[0], x.reshape(-1), t.reshape(-1), C.byref(loss),
+                                    g.ctypes.data_as(C.c_void_p)))
+        return loss.value, g
+
+
+def seed_features(router: "Router") -> np.ndarray:
+    """Input features of an opened router's design, [X][Y][16]."""
+    hdr = np.zeros(4, np.int32)
+    _check(lib().igr_router_grid(router.h, hdr.ctypes.data_as(C.c_void_p), None, None, None, None))
+    out = np.zeros((int(hdr[1]), int(hdr[2]), 16), np.float32)
+    _check(lib().igr_seed_features(router.h, out.reshape(-1)), router.h)
+    return out

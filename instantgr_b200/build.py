@@ -22,8 +22,10 @@ ROOT = os.path.dirname(HERE)
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CUDA_INC = "/usr/local/cuda/include"
 
-CU_SOURCES = ["cost.cu", "commit.cu", "ripup.cu", "pattern.cu", "pattern_static.cu", "color.cu", "dag.cu", "plan.cu"]
-CPP_SOURCES = ["design_io.cpp", "pins.cpp", "netbuild.cpp", "gen.cpp", "dag_build.cpp", "router.cpp", "capi.cpp"]
+CU_SOURCES = ["cost.cu", "commit.cu", "ripup.cu", "pattern.cu", "pattern_static.cu", "color.cu", "dag.cu", "plan.cu",
+              "seed_nn.cu"]
+CPP_SOURCES = ["design_io.cpp", "pins.cpp", "netbuild.cpp", "gen.cpp", "dag_build.cpp", "router.cpp", "capi.cpp",
+               "seed_model.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # --fmad=false: the only multiply-add the reference contracts is written as fma() explicitly
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-Xptxas", "-v"] + ARCH

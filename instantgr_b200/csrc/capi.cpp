@@ -10,6 +10,7 @@
 #include <string>
 
 #include "router.hpp"
+#include "seed_model.hpp"
 
 using namespace igr;
 
@@ -41,6 +42,11 @@ int guard(std::string *slot, F &&f) {
 
 struct igr_router {
     Router r;
+    std::string err;
+};
+
+struct igr_seed {
+    SeedModel m;
     std::string err;
 };
 
@@ -734,6 +740,159 @@ int igr_steiner(int n, const int32_t *x, const int32_t *y, int32_t *nx, int32_t 
         if (*n_nodes > cap_nodes || *n_edges > cap_edges) throw Error(ERR_CAPACITY, "output buffers too small");
         for (int i = 0; i < *n_nodes; i++) { nx[i] = t.x[i]; ny[i] = t.y[i]; }
         for (int i = 0; i < *n_edges; i++) { edges[2 * i] = t.edges[i].first; edges[2 * i + 1] = t.edges[i].second; }
+    });
+}
+
+// ------------------------------------------------------------------ learned congestion seed
+#define SEED_GUARD(m, ...)                                                      \
+    do {                                                                        \
+        if (!(m)) return fail(nullptr, IGR_ERR_INVALID, "null model");          \
+        return guard(&(m)->err, [&] { __VA_ARGS__; });                          \
+    } while (0)
+
+static std::vector<__nv_bfloat16> to_bf16(const float *p, size_t n) {
+    std::vector<__nv_bfloat16> v(n);
+    for (size_t i = 0; i < n; i++) v[i] = __float2bfloat16(p[i]);
+    return v;
+}
+
+int igr_seed_create(uint64_t init_seed, igr_seed **out) {
+    if (!out) return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    *out = nullptr;
+    auto *m = new igr_seed();
+    const int rc = guard(&m->err, [&] { m->m.init(init_seed); });
+    if (rc) { delete m; return rc; }
+    *out = m;
+    return IGR_OK;
+}
+
+int igr_seed_destroy(igr_seed *m) {
+    delete m;
+    return IGR_OK;
+}
+
+const char *igr_seed_last_error(const igr_seed *m) { return m ? m->err.c_str() : g_last_error.c_str(); }
+
+int igr_seed_set_tile(igr_seed *m, int size, int halo) {
+    SEED_GUARD(m, {
+        std::vector<float> p;
+        m->m.get_params(p);
+        m->m.set_tile(size, halo);
+        m->m.set_params(p.data(), p.size());
+    });
+}
+
+int igr_seed_params(igr_seed *m, float *out, int64_t cap, int64_t *n) {
+    SEED_GUARD(m, {
+        if (!n) throw Error(ERR_INVALID, "null count");
+        *n = m->m.params();
+        if (out) {
+            if (cap < *n) throw Error(ERR_CAPACITY, "output buffer too small");
+            std::vector<float> p;
+            m->m.get_params(p);
+            std::memcpy(out, p.data(), p.size() * 4);
+        }
+    });
+}
+
+int igr_seed_set_params(igr_seed *m, const float *p, int64_t n) {
+    SEED_GUARD(m, {
+        if (!p) throw Error(ERR_INVALID, "null parameters");
+        m->m.set_params(p, (size_t)n);
+    });
+}
+
+int igr_seed_features(igr_router *h, float *out) {
+    if (!h || !out) return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    return guard(&h->err, [&] {
+        std::vector<__nv_bfloat16> f;
+        seed_features(h->r.d, h->r.ns, f);
+        for (size_t i = 0; i < f.size(); i++) out[i] = __bfloat162float(f[i]);
+    });
+}
+
+int igr_seed_add_map(igr_seed *m, int X, int Y, const float *feat, const float *target, int32_t *map_id) {
+    SEED_GUARD(m, {
+        if (X < 1 || Y < 1 || !feat || !target) throw Error(ERR_INVALID, "bad map");
+        const size_t n = (size_t)X * Y * 16;
+        const auto f = to_bf16(feat, n), t = to_bf16(target, n);
+        const int id = m->m.add_map(X, Y, f.data(), t.data());
+        if (map_id) *map_id = id;
+    });
+}
+
+int igr_seed_add_routed(igr_seed *m, igr_router *h, int32_t *map_id) {
+    if (!m || !h) return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    return guard(&m->err, [&] {
+        auto &r = h->r;
+        if (!r.ran) throw Error(ERR_STATE, "route before taking the demand");
+        std::vector<__nv_bfloat16> f, t;
+        seed_features(r.d, r.ns, f);
+        const int L = r.go.g.L, X = r.go.g.X, Y = r.go.g.Y;
+        std::vector<float> dem((size_t)L * X * Y);
+        DevBuf<float> tmp;
+        tmp.alloc(dem.size());
+        launch_from_track_layout_f(r.go.g, r.go.demand.p, tmp.p, r.s);
+        cuda_check(cudaMemcpyAsync(dem.data(), tmp.p, dem.size() * 4, cudaMemcpyDeviceToHost, r.s), "D2H");
+        cuda_check(cudaStreamSynchronize(r.s), "sync");
+        seed_targets(X, Y, L, dem.data(), t);
+        const int id = m->m.add_map(X, Y, f.data(), t.data());
+        if (map_id) *map_id = id;
+    });
+}
+
+int igr_seed_train(igr_seed *m, int steps, int tiles, float lr, uint64_t seed, double *loss_curve) {
+    SEED_GUARD(m, {
+        if (steps < 0 || tiles < 1 || tiles > 256) throw Error(ERR_INVALID, "bad training arguments");
+        std::vector<double> c;
+        m->m.train(steps, tiles, lr, seed, &c);
+        if (loss_curve) std::memcpy(loss_curve, c.data(), c.size() * sizeof(double));
+    });
+}
+
+int igr_seed_eval(igr_seed *m, int map, double *mse, double *mae) {
+    SEED_GUARD(m, {
+        if (map < 0 || map >= (int)m->m.maps.size()) throw Error(ERR_INVALID, "no such map");
+        double a = 0;
+        const double e = m->m.evaluate(map, &a);
+        if (mse) *mse = e;
+        if (mae) *mae = a;
+    });
+}
+
+int igr_seed_predict(igr_seed *m, int X, int Y, const float *feat, float *pred) {
+    SEED_GUARD(m, {
+        if (X < 1 || Y < 1 || !feat || !pred) throw Error(ERR_INVALID, "bad map");
+        const size_t n = (size_t)X * Y * 16;
+        const auto f = to_bf16(feat, n);
+        DevBuf<__nv_bfloat16> fd;
+        DevBuf<float> pd;
+        fd.upload(f.data(), n, m->m.s);
+        pd.alloc(n);
+        cuda_check(cudaMemsetAsync(pd.p, 0, n * 4, m->m.s), "memset");
+        m->m.predict(X, Y, fd.p, pd.p);
+        cuda_check(cudaMemcpyAsync(pred, pd.p, n * 4, cudaMemcpyDeviceToHost, m->m.s), "D2H");
+        cuda_check(cudaStreamSynchronize(m->m.s), "sync");
+    });
+}
+
+int igr_seed_grad(igr_seed *m, int T, const float *x, const float *target, double *loss, float *grads) {
+    SEED_GUARD(m, {
+        if (T < 1 || !x || !target) throw Error(ERR_INVALID, "bad arguments");
+        auto &M = m->m;
+        M.ensure(T);
+        const size_t n = (size_t)T * M.S * M.S * 16;
+        const auto xb = to_bf16(x, n);
+        cuda_check(cudaMemcpyAsync(M.x0.p, xb.data(), n * 2, cudaMemcpyHostToDevice, M.s), "H2D");
+        cuda_check(cudaMemcpyAsync(M.tgt32.p, target, n * 4, cudaMemcpyHostToDevice, M.s), "H2D");
+        M.forward(T);
+        const double l = M.backward(T, nullptr);
+        if (loss) *loss = l;
+        if (grads) {
+            std::vector<float> g;
+            M.grads(g);
+            std::memcpy(grads, g.data(), g.size() * 4);
+        }
     });
 }
 

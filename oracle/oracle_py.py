@@ -39,7 +39,8 @@ def build() -> None:
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(os.path.join(HERE, "oracle.c")):
+        srcs = [os.path.join(HERE, f) for f in ("oracle.c", "seed_oracle.c")]
+        if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(f) for f in srcs):
             build()
         L = C.CDLL(LIB)
         gp = C.POINTER(Grid)
@@ -59,8 +60,35 @@ def lib():
         L.orc_color.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, C.c_int, _i32p]
         L.orc_dag_route.argtypes = [gp, _f32p, _f64p, C.c_int, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p,
                                     _i64p, _i32p, _i32p, _i32p, _i32p, C.c_int]
+        L.orc_seed_params.restype = C.c_int
+        L.orc_seed_grad.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, _f32p, _f32p, _f32p, C.c_int]
+        L.orc_seed_grad.restype = C.c_double
         _lib = L
     return _lib
+
+
+def seed_grad(x, target, params, halo, rounded=True):
+    """Loss and parameter gradient of the congestion-seed network (seed_oracle.c),
+    tiles [T][S][S][16]; `rounded` rounds to BF16 where the GPU stores BF16."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    t = np.ascontiguousarray(target, dtype=np.float32)
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    g = np.zeros(lib().orc_seed_params(), np.float32)
+    loss = lib().orc_seed_grad(x.shape[0], x.shape[1], halo, x.reshape(-1), t.reshape(-1), p, g, 1 if rounded else 0)
+    return loss, g
+
+
+SEED_LAYERS = [(16, 32), (32, 64), (64, 64), (64, 64), (64, 32), (32, 16)]  # (cin, cout) of the six convolutions
+
+
+def seed_slices():
+    """(weight slice, bias slice) of each layer in the flat parameter vector."""
+    out, o = [], 0
+    for ci, co in SEED_LAYERS:
+        nw = co * 9 * ci
+        out.append((slice(o, o + nw), slice(o + nw, o + nw + co)))
+        o += nw + co
+    return out
 
 
 def _i32(a):
