@@ -272,13 +272,27 @@ int igr_seed_features(igr_router *r, float *out);
  * routed demand of a router's last run. */
 int igr_seed_add_map(igr_seed *m, int X, int Y, const float *features, const float *target, int32_t *map_id);
 int igr_seed_add_routed(igr_seed *m, igr_router *r, int32_t *map_id);
-/* `steps` Adam steps on batches of `tiles` random tiles of the training maps;
- * loss_curve[steps] (optional) receives the mean squared error of each step. */
-int igr_seed_train(igr_seed *m, int steps, int tiles, float lr, uint64_t seed, double *loss_curve);
-/* Mean squared and absolute error of the prediction of training map `map`. */
-int igr_seed_eval(igr_seed *m, int map, double *mse, double *mae);
+/* `steps` Adam steps on batches of `tiles` random tiles of training maps
+ * 0..nmaps-1 (0: all); loss_curve[steps] (optional) receives the mean squared
+ * error of each step. */
+int igr_seed_train(igr_seed *m, int steps, int tiles, float lr, uint64_t seed, int nmaps, double *loss_curve);
+/* Errors of the prediction of stored map `map`: out[0] mean squared error,
+ * [1] mean absolute error, [2] MAE of predicting zero, [3] MAE of predicting
+ * each layer's mean demand over the map. */
+int igr_seed_eval(igr_seed *m, int map, double *out, int n);
 /* Prediction of a whole feature map (tiled). */
 int igr_seed_predict(igr_seed *m, int X, int Y, const float *features, float *pred);
+/* Attaches a model to a router (mode 0: none, 1: every run seeded, 2: a seeded
+ * run and a plain run, the better total score kept).  Seeding adds alpha x the
+ * predicted demand (kind 0) or alpha x the predicted overflow over capacity
+ * (kind 1), rounded to half units, to the demand during phase 1 and removes
+ * it after; with levels > 0 the seed shrinks in that many steps as the
+ * phase-1 batches commit.  Rip-up-and-reroute then handles the nets of higher
+ * predicted overflow first.  The model must outlive the router's runs. */
+int igr_router_set_seed(igr_router *r, igr_seed *m, double alpha, int mode, int kind, int levels);
+/* Seed statistics of the last run: [0] 1 if the seeded result was kept (mode 2),
+ * [1] seeded total score, [2] plain total score (mode 2), [3] prediction ms. */
+int igr_router_seed_stats(igr_router *r, double *out, int n);
 /* One forward and backward pass on T tiles (x, target: [T][size][size][16])
  * without an update: loss and the gradient of every parameter (layout of
  * igr_seed_params), for gradient checks. */

@@ -45,7 +45,7 @@ EXPORTS = [
     "igr_congestion_view", "igr_score", "igr_color_batches", "igr_dag_route", "igr_build_dag", "igr_steiner",
     "igr_seed_create", "igr_seed_destroy", "igr_seed_last_error", "igr_seed_set_tile", "igr_seed_params",
     "igr_seed_set_params", "igr_seed_features", "igr_seed_add_map", "igr_seed_add_routed", "igr_seed_train",
-    "igr_seed_eval", "igr_seed_predict", "igr_seed_grad",
+    "igr_seed_eval", "igr_seed_predict", "igr_seed_grad", "igr_router_set_seed", "igr_router_seed_stats",
 ]
 
 
@@ -124,6 +124,8 @@ def lib() -> C.CDLL:
                                 C.c_int64, C.POINTER(C.c_int64)]
     L.igr_steiner.argtypes = [C.c_int, _i32p, _i32p, _i32p, _i32p, C.c_int, C.POINTER(C.c_int), _i32p,
                               C.c_int, C.POINTER(C.c_int)]
+    L.igr_router_set_seed.argtypes = [vp, vp, C.c_double, C.c_int, C.c_int, C.c_int]
+    L.igr_router_seed_stats.argtypes = [vp, _f64p, C.c_int]
     L.igr_seed_create.argtypes = [C.c_uint64, C.POINTER(vp)]
     L.igr_seed_destroy.argtypes = [vp]
     L.igr_seed_last_error.restype = C.c_char_p
@@ -134,8 +136,8 @@ def lib() -> C.CDLL:
     L.igr_seed_features.argtypes = [vp, _f32p]
     L.igr_seed_add_map.argtypes = [vp, C.c_int, C.c_int, _f32p, _f32p, C.POINTER(C.c_int32)]
     L.igr_seed_add_routed.argtypes = [vp, vp, C.POINTER(C.c_int32)]
-    L.igr_seed_train.argtypes = [vp, C.c_int, C.c_int, C.c_float, C.c_uint64, vp]
-    L.igr_seed_eval.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.igr_seed_train.argtypes = [vp, C.c_int, C.c_int, C.c_float, C.c_uint64, C.c_int, vp]
+    L.igr_seed_eval.argtypes = [vp, C.c_int, _f64p, C.c_int]
     L.igr_seed_predict.argtypes = [vp, C.c_int, C.c_int, _f32p, _f32p]
     L.igr_seed_grad.argtypes = [vp, C.c_int, _f32p, _f32p, C.POINTER(C.c_double), vp]
     _lib = L
@@ -257,6 +259,17 @@ class Router:
         out = np.zeros(int(hdr[0]) * int(hdr[1]) * int(hdr[2]), np.float32)
         _check(lib().igr_router_demand(self.h, out))
         return out
+
+    def set_seed(self, model, alpha: float = 1.0, mode: int = 1, kind: int = 1, levels: int = 4) -> None:
+        """Attach a learned congestion seed (igr_router_set_seed); mode 0 detaches."""
+        self._seed = model
+        _check(lib().igr_router_set_seed(self.h, model.h if model is not None else None, alpha, mode, kind, levels),
+               self.h)
+
+    def seed_stats(self) -> dict:
+        v = np.zeros(4, np.float64)
+        _check(lib().igr_router_seed_stats(self.h, v, 4))
+        return dict(seed_kept=bool(v[0]), seeded_score=v[1], plain_score=v[2], predict_ms=v[3])
 
     def sizes(self):
         a, b = C.c_int64(), C.c_int64()
@@ -437,9 +450,17 @@ def steiner(x, y):
     return nx[: nn.value], ny[: nn.value], ed[: 2 * ne.value].reshape(-1, 2)
 
 
+SEED_MODEL_PATH = os.path.join(_HERE, "data", "congestion_seed.npz")
+
+
 class Seed:
     """Learned congestion seed (igr_seed_*): BF16 convolutional demand predictor
     trained and run on the tcgen05 tensor cores."""
+
+    @classmethod
+    def load(cls, path: str = SEED_MODEL_PATH) -> "Seed":
+        """The model of a parameter file written by train_seed (default: the shipped model)."""
+        return cls(1, params=np.load(path)["params"])
 
     def __init__(self, init_seed: int = 1, params=None):
         self.h = C.c_void_p()
@@ -489,15 +510,17 @@ class Seed:
         self._c(lib().igr_seed_add_routed(self.h, router.h, C.byref(i)))
         return i.value
 
-    def train(self, steps: int, tiles: int = 8, lr: float = 1e-3, seed: int = 1) -> np.ndarray:
+    def train(self, steps: int, tiles: int = 8, lr: float = 1e-3, seed: int = 1, maps: int = 0) -> np.ndarray:
+        """Adam steps on random tiles of stored maps 0..maps-1 (0: all); per-step MSE."""
         c = np.zeros(max(steps, 1), np.float64)
-        self._c(lib().igr_seed_train(self.h, steps, tiles, lr, seed, c.ctypes.data_as(C.c_void_p)))
+        self._c(lib().igr_seed_train(self.h, steps, tiles, lr, seed, maps, c.ctypes.data_as(C.c_void_p)))
         return c[:steps]
 
-    def evaluate(self, map_id: int):
-        a, b = C.c_double(), C.c_double()
-        self._c(lib().igr_seed_eval(self.h, map_id, C.byref(a), C.byref(b)))
-        return a.value, b.value
+    def evaluate(self, map_id: int) -> dict:
+        """Errors of a stored map's prediction and of the zero / per-layer-mean baselines."""
+        v = np.zeros(4, np.float64)
+        self._c(lib().igr_seed_eval(self.h, map_id, v, 4))
+        return dict(mse=v[0], mae=v[1], mae_zero=v[2], mae_mean=v[3])
 
     def predict(self, features) -> np.ndarray:
         f = np.ascontiguousarray(features, dtype=np.float32)

@@ -744,6 +744,31 @@ int igr_steiner(int n, const int32_t *x, const int32_t *y, int32_t *nx, int32_t 
 }
 
 // ------------------------------------------------------------------ learned congestion seed
+int igr_router_set_seed(igr_router *h, igr_seed *m, double alpha, int mode, int kind, int levels) {
+    if (!h) return fail(nullptr, IGR_ERR_INVALID, "null router");
+    return guard(&h->err, [&] {
+        if (mode < 0 || mode > 2 || !(alpha >= 0) || kind < 0 || kind > 1 || levels < 0)
+            throw Error(ERR_INVALID, "bad seed mode, kind, levels or weight");
+        if (mode && !m) throw Error(ERR_INVALID, "null model");
+        auto &r = h->r;
+        r.seed = mode ? &m->m : nullptr;
+        r.seed_mode = mode;
+        r.seed_alpha = alpha;
+        r.seed_kind = kind;
+        r.seed_levels = levels;
+        r.seed_ready = false;
+        r.seed_used = false;
+    });
+}
+
+int igr_router_seed_stats(igr_router *h, double *out, int n) {
+    if (!h || !out) return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    const auto &r = h->r;
+    double v[4] = {r.seed_used ? 1.0 : 0.0, r.seed_scores[1], r.seed_scores[0], r.seed_ms};
+    for (int k = 0; k < n && k < 4; k++) out[k] = v[k];
+    return IGR_OK;
+}
+
 #define SEED_GUARD(m, ...)                                                      \
     do {                                                                        \
         if (!(m)) return fail(nullptr, IGR_ERR_INVALID, "null model");          \
@@ -841,22 +866,22 @@ int igr_seed_add_routed(igr_seed *m, igr_router *h, int32_t *map_id) {
     });
 }
 
-int igr_seed_train(igr_seed *m, int steps, int tiles, float lr, uint64_t seed, double *loss_curve) {
+int igr_seed_train(igr_seed *m, int steps, int tiles, float lr, uint64_t seed, int nmaps, double *loss_curve) {
     SEED_GUARD(m, {
-        if (steps < 0 || tiles < 1 || tiles > 256) throw Error(ERR_INVALID, "bad training arguments");
+        if (steps < 0 || tiles < 1 || tiles > 256 || nmaps < 0) throw Error(ERR_INVALID, "bad training arguments");
         std::vector<double> c;
-        m->m.train(steps, tiles, lr, seed, &c);
+        m->m.train(steps, tiles, lr, seed, &c, nmaps);
         if (loss_curve) std::memcpy(loss_curve, c.data(), c.size() * sizeof(double));
     });
 }
 
-int igr_seed_eval(igr_seed *m, int map, double *mse, double *mae) {
+int igr_seed_eval(igr_seed *m, int map, double *out, int n) {
     SEED_GUARD(m, {
         if (map < 0 || map >= (int)m->m.maps.size()) throw Error(ERR_INVALID, "no such map");
-        double a = 0;
-        const double e = m->m.evaluate(map, &a);
-        if (mse) *mse = e;
-        if (mae) *mae = a;
+        if (!out) throw Error(ERR_INVALID, "null output");
+        double v[4];
+        m->m.evaluate(map, v);
+        for (int k = 0; k < n && k < 4; k++) out[k] = v[k];
     });
 }
 

@@ -15,6 +15,7 @@
 // phase-2 launch), and no device memory is allocated per run once the
 // buffers have grown to the design's size.
 #include "router.hpp"
+#include "seed_model.hpp"
 
 #include <sys/stat.h>
 
@@ -302,8 +303,141 @@ void Router::grow_routes(int64_t need) {
 }
 
 void Router::run() {
+    if (!seed || seed_mode == 0) {
+        run_once(false);
+        return;
+    }
+    if (seed_mode == 1) {
+        run_once(true);
+        seed_used = true;
+        seed_scores[1] = score_wl + score_via + score_of;
+        return;
+    }
+    // seeded run judged against the plain run: the better total score is kept
+    const double t0 = now_s();
+    run_once(true);
+    const double seeded_score = score_wl + score_via + score_of;
+    RouteBackup bk;
+    save_result(bk);
+    run_once(false);
+    const double plain_score = score_wl + score_via + score_of;
+    seed_used = seeded_score < plain_score;
+    if (seed_used) restore_result(bk);
+    seed_scores[0] = plain_score;
+    seed_scores[1] = seeded_score;
+    st.wall = now_s() - t0;
+    if (verbose)
+        std::fprintf(stderr, "[igr] seeded %.0f vs plain %.0f: %s result kept\n", seeded_score, plain_score,
+                     seed_used ? "seeded" : "plain");
+}
+
+void Router::save_result(RouteBackup &b) {
+    b.routes.alloc(std::max<size_t>(1, (size_t)route_end));
+    if (route_end)
+        cuda_check(cudaMemcpyAsync(b.routes.p, routes.p, route_end * sizeof(int), cudaMemcpyDeviceToDevice, s), "D2D");
+    b.demand.alloc(go.g.N);
+    cuda_check(cudaMemcpyAsync(b.demand.p, go.demand.p, go.g.N * sizeof(float), cudaMemcpyDeviceToDevice, s), "D2D");
+    cuda_check(cudaStreamSynchronize(s), "backup");
+    b.route_off = route_off;
+    b.route_cap = route_cap;
+    b.route_end = route_end;
+    b.st = st;
+    b.kt_ms.assign(kt.ms, kt.ms + KC_N);
+    b.score[0] = score_wl;
+    b.score[1] = score_via;
+    b.score[2] = score_of;
+    b.cost_cells = cost_cells;
+    b.commit_cells = commit_cells;
+    b.color_bytes = color_bytes;
+}
+
+void Router::restore_result(RouteBackup &b) {
+    grow_routes(b.route_end);
+    if (b.route_end)
+        cuda_check(cudaMemcpyAsync(routes.p, b.routes.p, b.route_end * sizeof(int), cudaMemcpyDeviceToDevice, s), "D2D");
+    cuda_check(cudaMemcpyAsync(go.demand.p, b.demand.p, go.g.N * sizeof(float), cudaMemcpyDeviceToDevice, s), "D2D");
+    cuda_check(cudaStreamSynchronize(s), "restore");
+    route_off = b.route_off;
+    route_cap = b.route_cap;
+    route_end = b.route_end;
+    st = b.st;
+    score_wl = b.score[0];
+    score_via = b.score[1];
+    score_of = b.score[2];
+    cost_cells = b.cost_cells;
+    commit_cells = b.commit_cells;
+    color_bytes = b.color_bytes;
+    h_routes_valid = false;
+    go.mark_all_dirty(s);
+}
+
+// Prediction of the attached congestion seed for this design (once), the
+// seed demand in the track layout and the predicted overflow per GCell.
+void Router::prepare_seed() {
+    if (seed_ready) return;
+    const double t0 = now_s();
+    const int L = go.g.L, X = go.g.X, Y = go.g.Y;
+    std::vector<__nv_bfloat16> f;
+    seed_features(d, ns, f);
+    const double t1 = now_s();
+    DevBuf<__nv_bfloat16> feat;
+    DevBuf<float> pred, ref, cap;
+    feat.upload(f.data(), f.size(), seed->s);
+    pred.alloc(f.size());
+    cuda_check(cudaMemsetAsync(pred.p, 0, f.size() * sizeof(float), seed->s), "memset");
+    seed->predict(X, Y, feat.p, pred.p);
+    const double t2 = now_s();
+    cap.alloc((size_t)L * X * Y);
+    launch_from_track_layout_f(go.g, go.cap.p, cap.p, seed->s);
+    ref.alloc((size_t)L * X * Y);
+    launch_seed_demand(X, Y, L, pred.p, (float)seed_alpha, seed_kind, cap.p, ref.p, seed->s);
+    DevBuf<float> over;
+    over.alloc((size_t)X * Y);
+    launch_seed_overflow(X, Y, L, pred.p, cap.p, over.p, seed->s);
+    std::vector<float> ov((size_t)X * Y);
+    cuda_check(cudaMemcpyAsync(ov.data(), over.p, ov.size() * 4, cudaMemcpyDeviceToHost, seed->s), "D2H");
+    cuda_check(cudaStreamSynchronize(seed->s), "seed");
+    d_seed_dem.alloc(go.g.N);
+    launch_to_track_layout(go.g, ref.p, d_seed_dem.p, s);
+    d_seed_cur.alloc(go.g.N);
+    cuda_check(cudaMemsetAsync(d_seed_cur.p, 0, go.g.N * sizeof(float), s), "memset");
+    // summed-area table of the predicted overflow for the rip-up order
+    seed_sat.assign((size_t)(X + 1) * (Y + 1), 0.0);
+    for (int x = 0; x < X; x++)
+        for (int y = 0; y < Y; y++)
+            seed_sat[(size_t)(x + 1) * (Y + 1) + y + 1] = ov[(size_t)x * Y + y] + seed_sat[(size_t)x * (Y + 1) + y + 1] +
+                                                          seed_sat[(size_t)(x + 1) * (Y + 1) + y] -
+                                                          seed_sat[(size_t)x * (Y + 1) + y];
+    cuda_check(cudaStreamSynchronize(s), "seed");
+    seed_ready = true;
+    seed_ms = 1e3 * (now_s() - t0);
+    if (verbose)
+        std::fprintf(stderr, "[igr] congestion seed: %.1f ms (features %.1f, network %.1f)\n", seed_ms,
+                     1e3 * (t1 - t0), 1e3 * (t2 - t1));
+}
+
+// Starts the seed of a phase-1 pass on freshly reset demand: constant seeds are
+// added at once, shrinking ones by the first step of the batch loop.
+void Router::seed_begin() {
+    if (!seed_active) return;
+    cuda_check(cudaMemsetAsync(d_seed_cur.p, 0, go.g.N * sizeof(float), s), "memset");
+    if (seed_levels == 0) launch_seed_step(go.g.N, go.demand.p, d_seed_dem.p, d_seed_cur.p, 1.f, s);
+}
+
+// predicted overflow per GCell over a net's bounding box
+double Router::seed_pressure(int net) const {
+    const RNet &n = ns.nets[net];
+    const int Y1 = ns.Y + 1;
+    auto at = [&](int x, int y) { return seed_sat[(size_t)x * Y1 + y]; };
+    const double s = at(n.maxx + 1, n.maxy + 1) - at(n.minx, n.maxy + 1) - at(n.maxx + 1, n.miny) + at(n.minx, n.miny);
+    return s / ((double)(n.maxx - n.minx + 1) * (n.maxy - n.miny + 1));
+}
+
+void Router::run_once(bool seeded) {
     ensure_device();
     cudaGetLastError();  // start from a clean error state
+    if (seeded) prepare_seed();
+    seed_active = seeded;
     const double t0 = now_s();
     st = RouterStats();
     kt.s = s;
@@ -322,7 +456,12 @@ void Router::run() {
     int m = mode;
     if (m < 0) m = R > 20000000 ? 2 : (R > 5000000 ? 1 : 0);
     mode_eff = m;
+    // the seed demand steers phase 1 only (added in phase1()) and is taken out before rip-up
     phase1();
+    if (seeded) {
+        launch_seed_step(go.g.N, go.demand.p, d_seed_dem.p, d_seed_cur.p, 0.f, s);
+        go.mark_all_dirty(s);
+    }
     for (int it = 0; it < rrr_iters; it++)
         if (!rrr_pass(it)) break;
     cuda_check(cudaStreamSynchronize(s), "sync");
@@ -386,6 +525,15 @@ void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<in
     for (int bi = 0; bi < nb; bi++) {
         const int off = batch_off[bi], n = batch_off[bi + 1] - off;
         const int stamp = bi + 1;
+        if (seed_active && seed_levels > 0) {
+            // the seed shrinks in `seed_levels` steps as the batches commit real demand
+            const int lv = (int)((int64_t)bi * seed_levels / nb);
+            if (bi == 0 || lv != (int)((int64_t)(bi - 1) * seed_levels / nb)) {
+                launch_seed_step(go.g.N, go.demand.p, d_seed_dem.p, d_seed_cur.p, 1.f - (float)lv / seed_levels, s);
+                go.mark_all_dirty(s);
+                st.launches += 1;
+            }
+        }
         if (timed) kt.begin(KC_COST);
         if (split_commit) launch_cost_refresh(go.g, true, s);
         else launch_commit_refresh(go.g, d_vcnt.p, bi, true, s);  // commits batch bi-1 (stamp bi)
@@ -452,6 +600,7 @@ void Router::phase1() {
     const int nb = run_color(R, d_perm1.p, d_shapes1, 15);
     st.batches1 = nb;
     if (batched && !tuned) autotune(nb);
+    seed_begin();
     std::vector<int> batch_off, class_off;
     plan_phase1(nb, batch_off, class_off);
     grow_routes(route_end);
@@ -461,7 +610,9 @@ void Router::phase1() {
     cuda_check(cudaEventRecord(ev0, s), "event");
     if (batched) {
         // the whole phase-1 loop as one CUDA graph, reused while the plan is unchanged
-        if (!graph1_exec || graph1_batch_off != batch_off || graph1_class_off != class_off || graph1_routes != routes.p) {
+        const int gkey = seed_active ? 1 + seed_levels : 0;
+        if (!graph1_exec || graph1_batch_off != batch_off || graph1_class_off != class_off || graph1_routes != routes.p ||
+            graph1_seed != gkey) {
             if (graph1_exec) { cudaGraphExecDestroy(graph1_exec); graph1_exec = nullptr; }
             cudaGraph_t gr = nullptr;
             cuda_check(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed), "capture");
@@ -474,6 +625,7 @@ void Router::phase1() {
             graph1_batch_off = batch_off;
             graph1_class_off = class_off;
             graph1_routes = routes.p;
+            graph1_seed = gkey;
         } else {
             st.launches += graph1_launches;
         }
@@ -555,6 +707,7 @@ void Router::autotune(int nb) {
                 tune = cand;
                 plan_phase1(nb, batch_off, class_off);
                 go.reset_demand(s);
+                seed_begin();
                 cuda_check(cudaMemcpyAsync(d_route_off.p, d_route_off1.p, (size_t)R * 8, cudaMemcpyDeviceToDevice, s), "D2D");
                 cuda_check(cudaMemcpyAsync(d_route_cap.p, d_route_cap1.p, (size_t)R * 4, cudaMemcpyDeviceToDevice, s), "D2D");
                 cuda_check(cudaEventRecord(ev0, s), "event");
@@ -706,7 +859,17 @@ bool Router::rrr_pass(int iter) {
     cuda_check(cudaMemcpyAsync(cv.ysum.data(), d_ysum.p, cv.ysum.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
     st.d2h_bytes += (int64_t)X * Y * 8;
-    std::sort(of_nets.begin(), of_nets.end(), [&](int l, int r) { return ns.nets[l].hpwl > ns.nets[r].hpwl; });
+    if (seed_active) {
+        // predicted congestion first, then HPWL (the reference's order)
+        std::vector<double> pr(R, 0.0);
+        for (int i : of_nets) pr[i] = seed_pressure(i);
+        std::sort(of_nets.begin(), of_nets.end(), [&](int l, int r) {
+            if (pr[l] != pr[r]) return pr[l] > pr[r];
+            return ns.nets[l].hpwl > ns.nets[r].hpwl;
+        });
+    } else {
+        std::sort(of_nets.begin(), of_nets.end(), [&](int l, int r) { return ns.nets[l].hpwl > ns.nets[r].hpwl; });
+    }
     // detour DAGs on host threads (Lshape_route_detour.hpp:702-748)
     const double th0 = now_s();
     dag.resize(R);

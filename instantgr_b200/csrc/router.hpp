@@ -93,6 +93,22 @@ struct ShapeDev {
     void upload(const ShapeSet &s, int X, int Y, int sparsity, cudaStream_t st, int threads = 0);
 };
 
+struct SeedModel;
+
+// result of a run kept aside while another run is made (seeded against plain)
+struct RouteBackup {
+    DevBuf<int> routes;
+    DevBuf<float> demand;
+    std::vector<int64_t> route_off;
+    std::vector<int> route_cap;
+    int64_t route_end = 0;
+    RouterStats st;
+    std::vector<double> kt_ms;
+    double score[3] = {0, 0, 0};
+    unsigned long long cost_cells = 0, commit_cells = 0;
+    double color_bytes = 0;
+};
+
 struct Router {
     int rrr_iters = 1, threads = 0, mode = -1, verbose = 0, batched = 0;
     int split_commit = 0;  // 1: separate cost refresh, wire commit and via commit launches per phase-1 batch
@@ -151,6 +167,7 @@ struct Router {
     cudaGraphExec_t graph1_exec = nullptr;
     std::vector<int> graph1_batch_off, graph1_class_off;
     int *graph1_routes = nullptr;
+    int graph1_seed = 0;  // seeding of the captured loop (0 none, 1 + decay levels)
     long long graph1_launches = 0;
     // device plan of phase 1 from the colouring in d_bat (ranks of d_perm1):
     // d_ids, and the batch and class offsets on the host
@@ -175,6 +192,25 @@ struct Router {
     // score of the last run: wirelength, vias, overflow (GPU estimate)
     double score_wl = 0, score_via = 0, score_of = 0;
     int64_t pin_vias = -1;  // selected pins on file layer 0 (one via each), counted once
+
+    // learned congestion seed (not owned): 1 = seeded runs, 2 = seeded run
+    // judged against a plain run (the better score is kept)
+    SeedModel *seed = nullptr;
+    double seed_alpha = 0.5;
+    int seed_mode = 0;
+    int seed_kind = 0;    // 0 predicted demand, 1 predicted overflow only
+    int seed_levels = 0;  // 0 constant during phase 1, else shrinks in this many steps
+    bool seed_ready = false, seed_active = false, seed_used = false;
+    double seed_ms = 0, seed_scores[2] = {0, 0};
+    DevBuf<float> d_seed_dem;         // seed demand at full strength (unrounded), track layout
+    DevBuf<float> d_seed_cur;         // seed demand currently added to the demand (half units)
+    std::vector<double> seed_sat;     // summed-area table of the predicted overflow
+    void prepare_seed();
+    void seed_begin();
+    double seed_pressure(int net) const;
+    void run_once(bool seeded);
+    void save_result(RouteBackup &b);
+    void restore_result(RouteBackup &b);
 
     ~Router();
     void open(const char *cap, const char *net);

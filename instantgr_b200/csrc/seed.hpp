@@ -56,6 +56,21 @@ void launch_gather_tiles(int T, int S, int halo, const TileRef *tiles, const __n
 // channels-last prediction map pred [X][Y][16] (cells outside the map skipped).
 void launch_scatter_prediction(int T, int S, int halo, const TileRef *tiles, const float *y32, float *pred,
                                cudaStream_t s);
+// Seed demand of the routing layers in the reference layout [l][x][y]: alpha x the
+// predicted demand of file layer l + 1 (pred in units of 8 GCell tracks), rounded
+// to half units (exact in f32 and removable), clamped at 0.
+// kind 1 seeds only the predicted overflow, alpha x max(0, predicted demand - capacity)
+// (cap_ref: capacity of the routing layers, reference layout); kind 0 needs no cap_ref.
+void launch_seed_demand(int X, int Y, int L, const float *pred, float alpha, int kind, const float *cap_ref,
+                        float *out_ref, cudaStream_t s);
+// Seed contribution at fraction `frac`: q = round_half(frac x base); demand += q - cur; cur = q
+// (frac = 0 removes it); track layout, n cells.
+void launch_seed_step(int64_t n, float *demand, const float *base, float *cur, float frac, cudaStream_t s);
+// Predicted overflow per GCell: sum over routing layers of max(0, predicted demand - capacity);
+// cap_ref is the capacity of the routing layers in the reference layout.
+void launch_seed_overflow(int X, int Y, int L, const float *pred, const float *cap_ref, float *out, cudaStream_t s);
+// demand[i] += sign * seed[i] over n cells
+void launch_add_demand(int64_t n, float *demand, const float *seed, float sign, cudaStream_t s);
 // Adam step over n parameters (f32 master, gradient, moments), bias-corrected.
 void launch_adam(int n, float *p, const float *g, float *m, float *v, float lr, float b1, float b2, float eps, int t,
                  cudaStream_t s);

@@ -239,8 +239,9 @@ int SeedModel::add_map(int X, int Y, const __nv_bfloat16 *feat, const __nv_bfloa
     return (int)maps.size() - 1;
 }
 
-double SeedModel::train(int steps, int T, float lr, uint64_t seed, std::vector<double> *curve) {
+double SeedModel::train(int steps, int T, float lr, uint64_t seed, std::vector<double> *curve, int nmaps) {
     if (maps.empty()) throw Error(ERR_STATE, "no training maps");
+    const size_t nm = nmaps > 0 ? std::min<size_t>((size_t)nmaps, maps.size()) : maps.size();
     ensure(T);
     uint64_t r = seed * 0x9E3779B97F4A7C15ull + 3;
     const int inner = S - 2 * halo;
@@ -248,7 +249,7 @@ double SeedModel::train(int steps, int T, float lr, uint64_t seed, std::vector<d
     std::vector<TileRef> tr(T);
     for (int st = 0; st < steps; st++) {
         for (int t = 0; t < T; t++) {
-            const TileRef &m = maps[splitmix(r) % maps.size()];
+            const TileRef &m = maps[splitmix(r) % nm];
             tr[t] = m;
             tr[t].x0 = m.X > inner ? (int)(splitmix(r) % (uint64_t)(m.X - inner + 1)) : 0;
             tr[t].y0 = m.Y > inner ? (int)(splitmix(r) % (uint64_t)(m.Y - inner + 1)) : 0;
@@ -284,7 +285,7 @@ void SeedModel::predict(int X, int Y, const __nv_bfloat16 *feat_dev, float *pred
     check("predict");
 }
 
-double SeedModel::evaluate(int map, double *mae) {
+void SeedModel::evaluate(int map, double *out) {
     const TileRef &m = maps.at(map);
     DevBuf<float> pred;
     pred.alloc((size_t)m.X * m.Y * 16);
@@ -294,16 +295,26 @@ double SeedModel::evaluate(int map, double *mae) {
     cuda_check(cudaMemcpyAsync(p.data(), pred.p, p.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaMemcpyAsync(t.data(), tpool.p + m.base, t.size() * 2, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "evaluate");
-    double se = 0, ae = 0;
-    for (size_t c = 0; c < (size_t)m.X * m.Y; c++)
+    const size_t cells = (size_t)m.X * m.Y;
+    double mean[kSeedLayersOut] = {0};
+    for (size_t c = 0; c < cells; c++)
+        for (int ch = 0; ch < kSeedLayersOut; ch++) mean[ch] += __bfloat162float(t[c * 16 + ch]);
+    for (int ch = 0; ch < kSeedLayersOut; ch++) mean[ch] /= (double)cells;
+    double se = 0, ae = 0, az = 0, am = 0;
+    for (size_t c = 0; c < cells; c++)
         for (int ch = 0; ch < kSeedLayersOut; ch++) {
-            const double e = p[c * 16 + ch] - (double)__bfloat162float(t[c * 16 + ch]);
+            const double tv = __bfloat162float(t[c * 16 + ch]);
+            const double e = p[c * 16 + ch] - tv;
             se += e * e;
             ae += std::fabs(e);
+            az += std::fabs(tv);
+            am += std::fabs(tv - mean[ch]);
         }
-    const double cnt = (double)m.X * m.Y * kSeedLayersOut;
-    if (mae) *mae = ae / cnt;
-    return se / cnt;
+    const double cnt = (double)cells * kSeedLayersOut;
+    out[0] = se / cnt;
+    out[1] = ae / cnt;
+    out[2] = az / cnt;
+    out[3] = am / cnt;
 }
 
 SeedModel::~SeedModel() {
@@ -314,46 +325,59 @@ SeedModel::~SeedModel() {
 void seed_features(const Design &d, const NetSet &ns, std::vector<__nv_bfloat16> &out) {
     const int X = d.X, Y = d.Y, L = d.L;
     const size_t XY = (size_t)X * Y;
-    std::vector<float> f(XY * 16, 0.f);
-    // pins per GCell
-    for (const RNet &n : ns.nets)
-        for (int p : n.pins) f[((size_t)(p % (int)XY)) * 16 + 0] += 0.25f;
-    // RUDY: a net spreads w/(w h) of horizontal and h/(w h) of vertical wire
-    // density over its bounding box (difference arrays in x and y)
+    // pins per GCell, and RUDY: a net spreads w/(w h) of horizontal and h/(w h)
+    // of vertical wire density over its bounding box (2-D difference arrays)
+    std::vector<float> pins(XY, 0.f);
     std::vector<double> dh((X + 1) * (size_t)(Y + 1), 0.0), dv(dh.size(), 0.0);
     auto at = [&](int x, int y) { return (size_t)x * (Y + 1) + y; };
     for (const RNet &n : ns.nets) {
-        const int w = n.maxx - n.minx + 1, h = n.maxy - n.miny + 1;
-        const double vh = 1.0 / h, vv = 1.0 / w;
-        for (auto *da : {&dh, &dv}) {
-            const double v = da == &dh ? vh : vv;
-            (*da)[at(n.minx, n.miny)] += v;
-            (*da)[at(n.maxx + 1, n.miny)] -= v;
-            (*da)[at(n.minx, n.maxy + 1)] -= v;
-            (*da)[at(n.maxx + 1, n.maxy + 1)] += v;
-        }
+        for (int p : n.pins) pins[(size_t)(p % (int)XY)] += 0.25f;
+        const double vh = 1.0 / (n.maxy - n.miny + 1), vv = 1.0 / (n.maxx - n.minx + 1);
+        dh[at(n.minx, n.miny)] += vh;
+        dh[at(n.maxx + 1, n.miny)] -= vh;
+        dh[at(n.minx, n.maxy + 1)] -= vh;
+        dh[at(n.maxx + 1, n.maxy + 1)] += vh;
+        dv[at(n.minx, n.miny)] += vv;
+        dv[at(n.maxx + 1, n.miny)] -= vv;
+        dv[at(n.minx, n.maxy + 1)] -= vv;
+        dv[at(n.maxx + 1, n.maxy + 1)] += vv;
     }
-    for (int x = 0; x <= X; x++)
-        for (int y = 0; y <= Y; y++) {
-            if (x > 0) { dh[at(x, y)] += dh[at(x - 1, y)]; dv[at(x, y)] += dv[at(x - 1, y)]; }
-            if (y > 0) { dh[at(x, y)] += dh[at(x, y - 1)]; dv[at(x, y)] += dv[at(x, y - 1)]; }
-            if (x > 0 && y > 0) { dh[at(x, y)] -= dh[at(x - 1, y - 1)]; dv[at(x, y)] -= dv[at(x - 1, y - 1)]; }
-        }
-    for (int x = 0; x < X; x++)
-        for (int y = 0; y < Y; y++) {
-            float *c = f.data() + ((size_t)x * Y + y) * 16;
-            c[1] = (float)(0.5 * dh[at(x, y)]);
-            c[2] = (float)(0.5 * dv[at(x, y)]);
-            int blocked = 0;
-            for (int l = 0; l < L && l < 10; l++) {
-                const float cap = d.cap[(size_t)l * XY + (size_t)x * Y + y];
-                c[4 + l] = cap / 8.f;
-                if (l > 0 && cap < 0.5f) blocked++;
+    // prefix sums: along y per row (parallel over x), then along x per column (parallel over y)
+    parallel_for(X + 1, 0, [&](int b, int e) {
+        for (int x = b; x < e; x++)
+            for (int y = 1; y <= Y; y++) {
+                dh[at(x, y)] += dh[at(x, y - 1)];
+                dv[at(x, y)] += dv[at(x, y - 1)];
             }
-            c[3] = L > 1 ? (float)blocked / (float)(L - 1) : 0.f;
-        }
-    out.resize(f.size());
-    for (size_t i = 0; i < f.size(); i++) out[i] = __float2bfloat16(f[i]);
+    });
+    parallel_for(Y + 1, 0, [&](int b, int e) {
+        for (int x = 1; x <= X; x++)
+            for (int y = b; y < e; y++) {
+                dh[at(x, y)] += dh[at(x - 1, y)];
+                dv[at(x, y)] += dv[at(x - 1, y)];
+            }
+    });
+    out.resize(XY * 16);
+    const __nv_bfloat16 zero = __float2bfloat16(0.f);
+    parallel_for(X, 0, [&](int b, int e) {
+        for (int x = b; x < e; x++)
+            for (int y = 0; y < Y; y++) {
+                const size_t c = (size_t)x * Y + y;
+                __nv_bfloat16 *o = out.data() + c * 16;
+                o[0] = __float2bfloat16(pins[c]);
+                o[1] = __float2bfloat16((float)(0.5 * dh[at(x, y)]));
+                o[2] = __float2bfloat16((float)(0.5 * dv[at(x, y)]));
+                int blocked = 0;
+                for (int l = 0; l < 10; l++) {
+                    const float cap = l < L ? d.cap[(size_t)l * XY + c] : 0.f;
+                    o[4 + l] = __float2bfloat16(cap / 8.f);
+                    if (l > 0 && l < L && cap < 0.5f) blocked++;
+                }
+                o[3] = __float2bfloat16(L > 1 ? (float)blocked / (float)(L - 1) : 0.f);
+                o[14] = zero;
+                o[15] = zero;
+            }
+    });
 }
 
 void seed_targets(int X, int Y, int routing_layers, const float *demand_ref, std::vector<__nv_bfloat16> &out) {

@@ -40,10 +40,13 @@ struct SeedModel {
     void adam(float lr);
     void grads(std::vector<float> &out);  // dW (as [cout][9][cin]) and db of each layer
     int add_map(int X, int Y, const __nv_bfloat16 *feat, const __nv_bfloat16 *target);  // host maps
-    double train(int steps, int T, float lr, uint64_t seed, std::vector<double> *curve);
+    // Adam steps on random tiles of training maps [0, nmaps) (0: every map)
+    double train(int steps, int T, float lr, uint64_t seed, std::vector<double> *curve, int nmaps = 0);
     // predicted channels-last map [X][Y][16] (f32) of a feature map on the device
     void predict(int X, int Y, const __nv_bfloat16 *feat_dev, float *pred_dev);
-    double evaluate(int map, double *mae);  // MSE (and MAE) of a training map's prediction
+    // errors of a stored map's prediction: out[0] MSE, [1] MAE, [2] MAE of predicting 0,
+    // [3] MAE of predicting each layer's mean demand over the map
+    void evaluate(int map, double *out);
     void check(const char *what);
 
    private:

@@ -384,6 +384,43 @@ __global__ void scatter_prediction_kernel(int T, int S, int halo, const TileRef 
     }
 }
 
+__global__ void seed_demand_kernel(int X, int Y, int L, const float *pred, float alpha, int kind, const float *cap,
+                                   float *out) {
+    const long long n = (long long)L * X * Y;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int l = (int)(i / ((long long)X * Y));
+        const long long c = i - (long long)l * X * Y;
+        float v = 8.f * pred[c * kSeedOut + 1 + l];
+        if (kind == 1) v -= cap[i];
+        out[i] = v > 0.f ? alpha * v : 0.f;
+    }
+}
+
+__global__ void seed_step_kernel(long long n, float *d, const float *base, float *cur, float frac) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float q = 0.5f * rintf(2.f * frac * base[i]);
+        const float c = cur[i];
+        if (q != c) {
+            d[i] += q - c;
+            cur[i] = q;
+        }
+    }
+}
+
+__global__ void seed_overflow_kernel(int X, int Y, int L, const float *pred, const float *cap, float *out) {
+    const long long n = (long long)X * Y;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        float o = 0;
+        for (int l = 0; l < L; l++) o += fmaxf(0.f, 8.f * pred[c * kSeedOut + 1 + l] - cap[(long long)l * n + c]);
+        out[c] = o;
+    }
+}
+
+__global__ void add_demand_kernel(long long n, float *d, const float *seed, float sign) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        d[i] += sign * seed[i];
+}
+
 __global__ void adam_kernel(int n, float *p, const float *g, float *m, float *v, float lr, float b1, float b2, float eps,
                             float c1, float c2) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -462,6 +499,23 @@ void launch_scatter_prediction(int T, int S, int halo, const TileRef *tiles, con
                                cudaStream_t s) {
     const int in = S - 2 * halo;
     scatter_prediction_kernel<<<blocks_for((long long)T * in * in * 4), 256, 0, s>>>(T, S, halo, tiles, y32, pred);
+}
+
+void launch_seed_demand(int X, int Y, int L, const float *pred, float alpha, int kind, const float *cap_ref,
+                        float *out_ref, cudaStream_t s) {
+    seed_demand_kernel<<<blocks_for((long long)L * X * Y), 256, 0, s>>>(X, Y, L, pred, alpha, kind, cap_ref, out_ref);
+}
+
+void launch_seed_step(int64_t n, float *demand, const float *base, float *cur, float frac, cudaStream_t s) {
+    seed_step_kernel<<<blocks_for(n), 256, 0, s>>>(n, demand, base, cur, frac);
+}
+
+void launch_seed_overflow(int X, int Y, int L, const float *pred, const float *cap_ref, float *out, cudaStream_t s) {
+    seed_overflow_kernel<<<blocks_for((long long)X * Y), 256, 0, s>>>(X, Y, L, pred, cap_ref, out);
+}
+
+void launch_add_demand(int64_t n, float *demand, const float *seed, float sign, cudaStream_t s) {
+    add_demand_kernel<<<blocks_for(n), 256, 0, s>>>(n, demand, seed, sign);
 }
 
 void launch_adam(int n, float *p, const float *g, float *m, float *v, float lr, float b1, float b2, float eps, int t,

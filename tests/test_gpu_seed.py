@@ -61,9 +61,9 @@ def test_seed_training_learns_a_smooth_demand_map():
             tg[..., l] = np.maximum(0, 0.6 * f[..., 1] + 0.4 * f[..., 2] - 0.3 * f[..., 4 + l]) + 0.2
         maps.append(m.add_map(f, tg))
         maps_np = tg
-    before = np.mean([m.evaluate(i)[0] for i in maps])
+    before = np.mean([m.evaluate(i)["mse"] for i in maps])
     curve = m.train(300, tiles=4, lr=2e-3, seed=1)
-    after = np.mean([m.evaluate(i)[0] for i in maps])
+    after = np.mean([m.evaluate(i)["mse"] for i in maps])
     const = float(np.var(maps_np[..., :10]))
     assert np.all(np.isfinite(curve))
     assert after < 0.2 * before, (before, after)
