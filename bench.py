@@ -127,6 +127,29 @@ def measured_peaks() -> dict:
     return dict(hbm_gbs=6650.0, src="of fallback")
 
 
+def max_over_ranks(ms: float, dist=None, device: str = "cpu") -> float:
+    """The slowest rank's time: every rank takes part in one MAX all-reduce (the
+    same collective step on every rank); `dist` None means a single rank."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(ms)
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(nets_per_replica: int, steps: int, world: int, max_ms: float) -> float:
+    """Whole-job nets/s of `world` independent replicas that each routed `steps`
+    times, over the slowest replica's time."""
+    return nets_per_replica * steps * world / (max_ms / 1e3)
+
+
+def omp_threads() -> int:
+    """Host threads the OpenMP-parallel oracle uses (all cores unless OMP_NUM_THREADS says otherwise)."""
+    v = os.environ.get("OMP_NUM_THREADS", "")
+    return int(v) if v.isdigit() and int(v) > 0 else (os.cpu_count() or 1)
+
+
 def profile_traffic() -> dict:
     """Per-launch DRAM traffic of the profiled kernels (ncu dram__bytes_read.sum +
     dram__bytes_write.sum) from the committed summary, if any."""
@@ -229,10 +252,7 @@ def main():
                         t[f] += v[f]
         e1.record()
         sync_all()
-        t = torch.tensor([e0.elapsed_time(e1)], device="cuda")
-        if dist:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item()), launches, ks
+        return max_over_ranks(e0.elapsed_time(e1), dist, "cuda"), launches, ks
 
     clk = Clocks(local)
     clk.start()
@@ -259,9 +279,9 @@ def main():
 
     result = None
     if rank == 0:
-        value = design_nets * args.steps * world / (ms_b / 1e3)
-        value_plain = design_nets * args.steps * world / (ms_p / 1e3)
-        e2e_value = design_nets * args.steps * world / (ms_e2e / 1e3)
+        value = replica_throughput(design_nets, args.steps, world, ms_b)
+        value_plain = replica_throughput(design_nets, args.steps, world, ms_p)
+        e2e_value = replica_throughput(design_nets, args.steps, world, ms_e2e)
         plan = rp.plan()
         h2d, d2h = e2e_bytes[-1]
         # roofline of the dominant kernel class of the plain form (every class is
@@ -290,12 +310,12 @@ def main():
             try:
                 g = rp.grid()
                 v, info = cpu_sample(rp, g, plan, args.cpu_batches)
-                cpu = dict(value=round(v, 2), unit="nets/s", cores=1, kind="port",
+                cpu = dict(value=round(v, 2), unit="nets/s", cores=omp_threads(), kind="port",
                            sample=f"oracle phase-1 (cost refresh + tree DP + commit) on the first "
                                   f"{info['batches']} of {info['of_batches']} batches ({info['nets']} nets, "
                                   f"{info['seconds']:.1f} s)")
             except Exception as ex:  # the CPU baseline is reported, never required
-                cpu = dict(value=None, unit="nets/s", cores=1, kind="port", sample=f"failed: {ex}")
+                cpu = dict(value=None, unit="nets/s", cores=omp_threads(), kind="port", sample=f"failed: {ex}")
         result = dict(metric="route throughput (nets/s), batched RRR router", value=round(value, 2), unit="nets/s",
                       n_gpus=world, steps=args.steps, warmup=args.warmup, ms_per_step=round(ms_b / args.steps, 3),
                       higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32/f64 costs, i32 demand",
@@ -340,7 +360,7 @@ def bench_reference(args, rank, world, workload):
     plan = r.plan()
     design_nets, _ = r.sizes()
     vals, infos = [], []
-    nb = args.cpu_batches or 3
+    nb = args.cpu_batches  # 0: every batch of phase 1, within the time budget
     for i in range(args.warmup + args.steps):
         v, info = cpu_sample(r, g, plan, nb)
         if i >= args.warmup:
@@ -354,7 +374,7 @@ def bench_reference(args, rank, world, workload):
                ms_per_step=round(1e3 * infos[0]["nets"] / v, 3), higher_is_better=True, scaling="weak",
                vs_baseline=None, dtype="f32/f64 costs, i32 demand", data="synthetic (seeded generator)",
                config=workload,
-               cpu_baseline=dict(value=round(v, 2), unit="nets/s", cores=1, kind="port", sample=sample),
+               cpu_baseline=dict(value=round(v, 2), unit="nets/s", cores=omp_threads(), kind="port", sample=sample),
                e2e=dict(value=round(v, 2), unit="nets/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(res), flush=True)
     r.close()

@@ -45,6 +45,7 @@ static void sklansky_d(double *s, int n) {
 void orc_cost_refresh(const orc_grid *g, const float *dem, float *wcost, float *vcost, double *presum) {
     const int L = g->L, X = g->X, Y = g->Y;
     /* update_wcost_cuda_ispd24 (graph.hpp:40-47) */
+#pragma omp parallel for collapse(2) schedule(static)
     for (int l = 0; l < L; l++)
         for (int x = 0; x < X; x++)
             for (int y = 0; y < Y; y++) {
@@ -54,6 +55,7 @@ void orc_cost_refresh(const orc_grid *g, const float *dem, float *wcost, float *
                 wcost[IDX(l, x, y)] = w;
             }
     /* update_single_vcost_ispd24 (graph.hpp:52-71), cross_points = 0 */
+#pragma omp parallel for collapse(2) schedule(static)
     for (int l = 0; l < L; l++)
         for (int x = 0; x < X; x++)
             for (int y = 0; y < Y; y++) {
@@ -71,25 +73,29 @@ void orc_cost_refresh(const orc_grid *g, const float *dem, float *wcost, float *
             }
     /* compute_presum */
     int n = X > Y ? X : Y;
-    double *s = (double *)malloc(sizeof(double) * (size_t)n);
-    for (int l = 0; l < L; l++) {
-        if (dir_of(g, l)) {
-            for (int x = 0; x < X; x++) {
-                s[0] = 0;
-                for (int y = 0; y < Y - 1; y++) s[y + 1] = wcost[IDX(l, x, y)];
-                sklansky_d(s, Y);
-                for (int y = 0; y < Y; y++) presum[IDX(l, x, y)] = s[y];
+    /* one track per iteration: (l, t) with t < X on vertical layers, t < Y on horizontal ones */
+#pragma omp parallel
+    {
+        double *s = (double *)malloc(sizeof(double) * (size_t)n);
+#pragma omp for collapse(2) schedule(static)
+        for (int l = 0; l < L; l++)
+            for (int t = 0; t < n; t++) {
+                if (dir_of(g, l)) {
+                    if (t >= X) continue;
+                    s[0] = 0;
+                    for (int y = 0; y < Y - 1; y++) s[y + 1] = wcost[IDX(l, t, y)];
+                    sklansky_d(s, Y);
+                    for (int y = 0; y < Y; y++) presum[IDX(l, t, y)] = s[y];
+                } else {
+                    if (t >= Y) continue;
+                    s[0] = 0;
+                    for (int x = 0; x < X - 1; x++) s[x + 1] = wcost[IDX(l, x, t)];
+                    sklansky_d(s, X);
+                    for (int x = 0; x < X; x++) presum[IDX(l, x, t)] = s[x];
+                }
             }
-        } else {
-            for (int y = 0; y < Y; y++) {
-                s[0] = 0;
-                for (int x = 0; x < X - 1; x++) s[x + 1] = wcost[IDX(l, x, y)];
-                sklansky_d(s, X);
-                for (int x = 0; x < X; x++) presum[IDX(l, x, y)] = s[x];
-            }
-        }
+        free(s);
     }
-    free(s);
 }
 
 static double wseg(const orc_grid *g, const double *presum, int l, int xa, int xb, int ya, int yb) {
@@ -98,9 +104,20 @@ static double wseg(const orc_grid *g, const double *presum, int l, int xa, int x
 
 /* atomic_add_unit_demand_wire_segment (graph.hpp:105-117), K = 1 */
 static void add_seg(const orc_grid *g, int *pre, int *st, int l, int xa, int xb, int ya, int yb, int stamp) {
+#pragma omp atomic
     pre[IDX(l, xa, ya)] += 1;
-    if (xa == xb) { pre[IDX(l, xa, yb)] -= 1; st[IDX(l, xa, yb)] = stamp; }
-    if (ya == yb) { pre[IDX(l, xb, ya)] -= 1; st[IDX(l, xb, ya)] = stamp; }
+    if (xa == xb) {
+#pragma omp atomic
+        pre[IDX(l, xa, yb)] -= 1;
+#pragma omp atomic write
+        st[IDX(l, xa, yb)] = stamp;
+    }
+    if (ya == yb) {
+#pragma omp atomic
+        pre[IDX(l, xb, ya)] -= 1;
+#pragma omp atomic write
+        st[IDX(l, xb, ya)] = stamp;
+    }
 }
 
 int orc_pattern_route(const orc_grid *g, const float *vcost, const double *presum, int n, const int *node_off,
@@ -108,6 +125,8 @@ int orc_pattern_route(const orc_grid *g, const float *vcost, const double *presu
                       int *pre, int *st, int stamp) {
     const int L = g->L, X = g->X, Y = g->Y, XY = X * Y, LL = L * L;
     int status = 0;
+    /* the nets of a batch are independent: one net per iteration, on all cores */
+#pragma omp parallel for schedule(dynamic, 64) reduction(min : status)
     for (int k = 0; k < n; k++) {
         const int nb = node_off[k], cnt = node_off[k + 1] - nb;
         const int *nd = nodes + nb, *pa = par + nb;
@@ -232,9 +251,13 @@ int orc_pattern_route(const orc_grid *g, const float *vcost, const double *presu
 int64_t orc_commit_wires(const orc_grid *g, int *pre, float *dem, int *st, int stamp) {
     const int L = g->L, X = g->X, Y = g->Y;
     int64_t wl = 0;
-    for (int l = 0; l < L; l++) {
+    const int n = X > Y ? X : Y;
+#pragma omp parallel for collapse(2) schedule(static) reduction(+ : wl)
+    for (int l = 0; l < L; l++)
+        for (int t = 0; t < n; t++) {
         if (dir_of(g, l) == 0) {
-            for (int y = 0; y < Y; y++) {
+            if (t < Y) {
+                const int y = t;
                 int acc = 0;
                 for (int x = 0; x < X - 1; x++) {
                     acc += pre[IDX(l, x, y)];
@@ -246,7 +269,8 @@ int64_t orc_commit_wires(const orc_grid *g, int *pre, float *dem, int *st, int s
                 }
             }
         } else {
-            for (int x = 0; x < X; x++) {
+            if (t < X) {
+                const int x = t;
                 int acc = 0;
                 for (int y = 0; y < Y - 1; y++) {
                     acc += pre[IDX(l, x, y)];
@@ -258,15 +282,22 @@ int64_t orc_commit_wires(const orc_grid *g, int *pre, float *dem, int *st, int s
                 }
             }
         }
-    }
+        }
     memset(pre, 0, sizeof(int) * (size_t)L * X * Y);
     return wl;
+}
+
+/* demand values are multiples of 0.5: concurrent additions are exact in any order */
+static inline void addf(float *p, float v) {
+#pragma omp atomic
+    *p += v;
 }
 
 int64_t orc_commit_vias(const orc_grid *g, int n, const int64_t *off, const int *routes, float *dem, const int *st,
                         int stamp, int K) {
     const int X = g->X, Y = g->Y, XY = X * Y;
     int64_t vias = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : vias)
     for (int k = 0; k < n; k++) {
         const int *r = routes + off[k];
         for (int i = 1; i < r[0]; i += 2) {
@@ -277,13 +308,13 @@ int64_t orc_commit_vias(const orc_grid *g, int n, const int64_t *off, const int 
             for (int l = mn; l < mx; l++) {
                 if (st[IDX(l, x, y)] >= stamp) continue;
                 if (dir_of(g, l)) {
-                    if (y == 0) dem[IDX(l, x, y)] += (float)K;
-                    else if (y == Y - 1) dem[IDX(l, x, y - 1)] += (float)K;
-                    else { dem[IDX(l, x, y - 1)] += (float)(0.5 * K); dem[IDX(l, x, y)] += (float)(0.5 * K); }
+                    if (y == 0) addf(&dem[IDX(l, x, y)], (float)K);
+                    else if (y == Y - 1) addf(&dem[IDX(l, x, y - 1)], (float)K);
+                    else { addf(&dem[IDX(l, x, y - 1)], (float)(0.5 * K)); addf(&dem[IDX(l, x, y)], (float)(0.5 * K)); }
                 } else {
-                    if (x == 0) dem[IDX(l, x, y)] += (float)K;
-                    else if (x == X - 1) dem[IDX(l, x - 1, y)] += (float)K;
-                    else { dem[IDX(l, x - 1, y)] += (float)(0.5 * K); dem[IDX(l, x, y)] += (float)(0.5 * K); }
+                    if (x == 0) addf(&dem[IDX(l, x, y)], (float)K);
+                    else if (x == X - 1) addf(&dem[IDX(l, x - 1, y)], (float)K);
+                    else { addf(&dem[IDX(l, x - 1, y)], (float)(0.5 * K)); addf(&dem[IDX(l, x, y)], (float)(0.5 * K)); }
                 }
             }
         }
