@@ -23,6 +23,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <numeric>
 #include <thread>
 
@@ -30,6 +32,64 @@ namespace igr {
 
 void cuda_check(cudaError_t e, const char *what) {
     if (e != cudaSuccess) throw Error(ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ------------------------------------------------------------------ device memory cache
+namespace {
+std::mutex g_cache_mu;
+std::map<std::pair<int, size_t>, std::vector<void *>> g_cache;  // (device, block bytes) -> free blocks
+
+size_t block_bytes(size_t bytes) {
+    const size_t g = bytes >= (size_t(1) << 20) ? (size_t(2) << 20) : 512;  // 2 MiB granules for large blocks
+    return (bytes + g - 1) / g * g;
+}
+}  // namespace
+
+void *dev_alloc(size_t bytes) {
+    const size_t b = block_bytes(bytes);
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    {
+        std::lock_guard<std::mutex> lock(g_cache_mu);
+        // smallest cached block that fits and wastes at most half of itself
+        auto it = g_cache.lower_bound({dev, b});
+        if (it != g_cache.end() && it->first.first == dev && it->first.second <= 2 * b && !it->second.empty()) {
+            void *p = it->second.back();
+            it->second.pop_back();
+            if (it->second.empty()) g_cache.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    if (cudaMalloc(&p, b) != cudaSuccess) {
+        cudaGetLastError();
+        dev_trim();
+        cuda_check(cudaMalloc(&p, b), "cudaMalloc");
+    }
+    return p;
+}
+
+void dev_free(void *p, size_t bytes) {
+    if (!p) return;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(p);
+        return;
+    }
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    g_cache[{dev, block_bytes(bytes)}].push_back(p);
+}
+
+void dev_trim() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    for (auto it = g_cache.begin(); it != g_cache.end();) {
+        if (it->first.first != dev) { ++it; continue; }
+        for (void *p : it->second) cudaFree(p);
+        it = g_cache.erase(it);
+    }
 }
 
 // ------------------------------------------------------------------ grid

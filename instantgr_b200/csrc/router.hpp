@@ -13,6 +13,15 @@ namespace igr {
 
 void cuda_check(cudaError_t e, const char *what);
 
+// Process-wide cache of device memory: blocks given back stay mapped and are
+// handed out again for requests of up to their size (per device), so that
+// routers opened one after another do not pay cudaMalloc/cudaFree each time.
+// A block is cached only after a device synchronisation, as cudaFree would.
+void *dev_alloc(size_t bytes);
+void dev_free(void *p, size_t bytes);
+// returns every cached block of the current device to the driver
+void dev_trim();
+
 template <typename T>
 struct DevBuf {
     T *p = nullptr;
@@ -22,7 +31,7 @@ struct DevBuf {
     DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) dev_free(p, n * sizeof(T));
         p = nullptr;
         n = 0;
     }
@@ -31,7 +40,7 @@ struct DevBuf {
         if (count <= n && p) return;
         release();
         if (count == 0) count = 1;
-        cuda_check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+        p = static_cast<T *>(dev_alloc(count * sizeof(T)));
         n = count;
     }
     void upload(const T *h, size_t count, cudaStream_t s) {
