@@ -61,7 +61,6 @@ struct igr_ctx {
     DevBuf<uint8_t> u8;
     DevBuf<float> f1, f2;
     DevBuf<double> d1;
-    DevBuf<unsigned> bar;
 };
 
 extern "C" {
@@ -627,62 +626,58 @@ int igr_dag_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t *nod
             throw Error(ERR_INVALID, "bad arguments");
         if (n == 0) return;
         const auto &g = c->go.g;
+        if (g.L != kRouteLayers) throw Error(ERR_INVALID, "the DAG DP handles 9 routing layers");
         const int N = node_off[n], E = par_off[N];
         if (node_off[0] != 0 || par_off[0] != 0) throw Error(ERR_INVALID, "CSR offsets must start at 0");
-        int D = 0;
+        for (int k = 0; k < n; k++)
+            if (node_off[k + 1] < node_off[k]) throw Error(ERR_INVALID, "node offsets must not decrease");
         for (int v = 0; v < N; v++) {
             if (depth[v] < 0) throw Error(ERR_INVALID, "negative depth");
             if (child_num[v] < 0 || child_num[v] > 10) throw Error(ERR_INVALID, "at most 10 child slots per node");
             if (nodes[v] < 0 || nodes[v] >= (g.L + 1) * g.X * g.Y) throw Error(ERR_INVALID, "node out of range");
-            D = std::max(D, depth[v] + 1);
         }
         for (int e = 0; e < E; e++) {
             if (par[e] < 0 || par[e] >= N) throw Error(ERR_INVALID, "parent out of range");
             if (child_slot[e] < 0 || child_slot[e] >= child_num[par[e]]) throw Error(ERR_INVALID, "child slot out of range");
         }
         std::vector<int> echild(E), child_off(N + 1, 0), ids(n);
-        for (int v = 0; v < N; v++) {
-            for (int e = par_off[v]; e < par_off[v + 1]; e++) {
-                echild[e] = v;
-                if (depth[par[e]] >= depth[v]) throw Error(ERR_STATE, "a parent must be shallower than its child");
+        for (int k = 0; k < n; k++)
+            for (int v = node_off[k]; v < node_off[k + 1]; v++) {
+                for (int e = par_off[v]; e < par_off[v + 1]; e++) {
+                    echild[e] = v;
+                    if (par[e] < node_off[k] || par[e] >= node_off[k + 1])
+                        throw Error(ERR_INVALID, "a parent must belong to the same net");
+                    if (depth[par[e]] >= depth[v]) throw Error(ERR_STATE, "a parent must be shallower than its child");
+                }
+                child_off[v + 1] = child_off[v] + child_num[v];
             }
-            child_off[v + 1] = child_off[v] + child_num[v];
-        }
         std::iota(ids.begin(), ids.end(), 0);
-        std::vector<int> cnt(D + 1, 0), ln(N);
-        for (int v = 0; v < N; v++) cnt[depth[v] + 1]++;
-        for (int d = 0; d < D; d++) cnt[d + 1] += cnt[d];
-        std::vector<int> level_off(cnt);
-        int ml = 0;
-        for (int d = 0; d < D; d++) ml = std::max(ml, cnt[d + 1] - cnt[d]);
-        for (int v = 0; v < N; v++) ln[cnt[depth[v]]++] = v;
+        std::vector<int> ln, level_off, net_level_off;
+        dag_levels(n, node_off, depth, ln, level_off, net_level_off);
         if ((int64_t)N * 100 + 99 > 0x7fffffffLL) throw Error(ERR_CAPACITY, "too many DAG nodes in one batch");
         const int64_t ext = records_extent(n, route_off, route_cap, nullptr);
-        DevBuf<int> dn, dpo, dp, dcs, dec, dco, dlo, dln, dno, dids, dcap, dlout, dstage, dscnt, dbc;
+        DevBuf<int> dn, dpo, dp, dcs, dec, dco, dlo, dln, dnl, dno, dids, dcap, dlout, dstage, dscnt, dbc;
         DevBuf<int64_t> droff;
         DevBuf<double> dcost, dce;
         DevBuf<unsigned long long> dbest, dpk;
         dn.upload(nodes, N, c->s); dpo.upload(par_off, N + 1, c->s); dp.upload(par, E, c->s);
         dcs.upload(child_slot, E, c->s); dec.upload(echild, c->s); dco.upload(child_off, c->s);
-        dlo.upload(level_off, c->s); dln.upload(ln, c->s); dno.upload(node_off, n + 1, c->s);
+        dlo.upload(level_off, c->s); dln.upload(ln, c->s); dnl.upload(net_level_off, c->s);
+        dno.upload(node_off, n + 1, c->s);
         dids.upload(ids, c->s); dcap.upload(route_cap, n, c->s); droff.upload(route_off, n, c->s);
         dcost.alloc((size_t)N * 10); dce.alloc((size_t)std::max(E, 1) * 81); dbc.alloc((size_t)std::max(E, 1) * 81);
         dbest.alloc((size_t)std::max(child_off[N], 1) * 10); dpk.alloc((size_t)std::max(child_off[N], 1) * 10);
         dlout.alloc(N); dstage.alloc((size_t)N * 8); dscnt.alloc(N);
         c->routes.upload(routes_out, (size_t)ext, c->s);
-        c->bar.alloc(2);
         DagBatchDev db;
-        db.n_nodes = N; db.n_edges = E; db.n_slots = child_off[N]; db.depth = D; db.n_nets = n; db.max_level = ml;
+        db.n_nodes = N; db.n_edges = E; db.n_nets = n;
         db.nodes = dn.p; db.par_off = dpo.p; db.par = dp.p; db.child_slot = dcs.p; db.edge_child = dec.p;
-        db.child_off = dco.p; db.level_off = dlo.p; db.level_nodes = dln.p; db.h_level_off = level_off.data();
+        db.child_off = dco.p; db.level_off = dlo.p; db.level_nodes = dln.p; db.net_level_off = dnl.p;
         db.net_node_off = dno.p; db.net_ids = dids.p; db.costs = dcost.p; db.best_path = dbest.p; db.packed = dpk.p;
         db.cost_edges = dce.p; db.best_change = dbc.p; db.layer_out = dlout.p; db.stage = dstage.p;
         db.stage_cnt = dscnt.p; db.route_off = droff.p; db.route_cap = dcap.p; db.routes = c->routes.p;
-        int nl = launch_dag_route(g, db, stamp, c->bar.p, true, c->s);
-        if (nl < 0) {
-            cudaGetLastError();
-            launch_dag_route(g, db, stamp, c->bar.p, false, c->s);
-        }
+        launch_dag_route(g, db, stamp, c->s);
+        cuda_check(cudaGetLastError(), "DAG launch");
         cuda_check(cudaMemcpyAsync(routes_out, c->routes.p, ext * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
         sync_check(c);
     });

@@ -7,14 +7,17 @@
 //   Lshape_route_node_layer_change_cuda   src/Lshape_route_detour.hpp:281-406
 //   get_routing_tree_layer_change_cuda    src/Lshape_route_detour.hpp:520-694
 //   cost/id packing for atomicMin         src/Lshape_route_detour.hpp:83-112
-// The reference launches two kernels per DAG level with a host synchronisation
-// after each (2 x depth launches per batch).  Here one persistent cooperative
-// kernel walks all levels of a batch, bottom-up then top-down, separated by a
-// grid barrier that gives up after two seconds (ERR_TIMEOUT) rather than
-// waiting forever.  Emitted segments are staged per DAG node and compacted in
-// node order, so route records do not depend on atomic ordering (the
-// reference appends them with atomicAdd).
-#include "gridsync.cuh"
+// The reference launches two kernels per DAG level of the whole batch, with a
+// host synchronisation after each (2 x depth launches per batch).  The nets of
+// a batch share no DAG node, so here one CTA walks one net's levels, bottom-up
+// then top-down, separated by CTA barriers: one launch per batch and no grid
+// synchronisation.  A warp computes the DP of one node; a thread traces one
+// node.  Emitted segments are staged per DAG node and compacted in node order,
+// so route records do not depend on atomic ordering (the reference appends
+// them with atomicAdd).
+#include "kcommon.cuh"
+
+#include <algorithm>
 
 namespace igr {
 
@@ -22,6 +25,8 @@ namespace {
 
 constexpr int kML = 10;                      // MAX_LAYER of the reference
 constexpr unsigned long long kInitPacked = 7208259049189261824ULL;  // init_cost_with_road
+constexpr int kDagWarps = 8;                 // warps of one net's CTA
+constexpr int kDagThreads = 32 * kDagWarps;
 
 __device__ __forceinline__ int32_t f2o(float f) {
     int32_t i = __float_as_int(f);
@@ -31,10 +36,8 @@ __device__ __forceinline__ float o2f(int32_t i) { return __int_as_float((i >= 0)
 __device__ __forceinline__ unsigned long long pack(float cost, int id) {
     return ((unsigned long long)f2o(cost) << 32) | (unsigned int)id;
 }
-__device__ __forceinline__ void unpack(unsigned long long p, double *cost, int *id) {
-    *cost = (double)o2f((int32_t)(p >> 32));
-    *id = (int)(p & 0xFFFFFFFFull);
-}
+__device__ __forceinline__ double packed_cost(unsigned long long p) { return (double)o2f((int32_t)(p >> 32)); }
+__device__ __forceinline__ int packed_id(unsigned long long p) { return (int)(p & 0xFFFFFFFFull); }
 
 __device__ __forceinline__ double wire_cost(const GridDev &g, int l, int xa, int xb, int ya, int yb) {
     return g.presum[cell_at(g, l, xb, yb)] - g.presum[cell_at(g, l, xa, ya)];
@@ -53,13 +56,6 @@ __device__ __forceinline__ void add_wire(const GridDev &g, int l, int xa, int xb
     int first = 0;
     for (int k = 0; k < l; k++) first += layer_dir(g, k) ? g.X : g.Y;
     g.dirty_commit[first + (layer_dir(g, l) ? xa : ya)] = 1;
-}
-
-__global__ void dag_init_kernel(DagBatchDev b) {
-    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, nth = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = tid; i < (int64_t)b.n_nodes * kML; i += nth) b.costs[i] = kInf;
-    for (int64_t i = tid; i < (int64_t)b.n_slots * kML; i += nth) { b.packed[i] = kInitPacked; b.best_path[i] = 0; }
-    for (int64_t i = tid; i < b.n_nodes; i += nth) { b.layer_out[i] = -1; b.stage_cnt[i] = 0; }
 }
 
 // precompute_cost_edge: one thread per (edge, from layer)
@@ -104,82 +100,179 @@ __global__ void dag_edge_cost_kernel(GridDev g, DagBatchDev b) {
     }
 }
 
-// Lshape_route_node_layer_change_cuda for one node
-__device__ void dp_node(const GridDev &g, const DagBatchDev &b, int node) {
+// per-warp scratch of the node DP
+struct NodeScratch {
+    unsigned long long pk[kML][kML];  // [child slot][layer] packed best of each child
+    double row[kML][kML];             // [low][layer] suffix minimum of the candidates of row `low`
+    signed char row_at[kML][kML];     // [low][layer] the candidate's top layer
+    double vcol[kML];                 // via costs of the node's column, layers 0..8
+    double cost[kML];                 // the node's final cost per layer
+    int win[kML];                     // winner low * 16 + top layer per layer, -1 none
+};
+
+constexpr double kNone = __builtin_huge_val();  // no candidate (every real candidate is below kInf)
+
+// what one (parent edge, target layer t) pair needs besides the node's own
+// costs: the parent's packed entry and, per source layer of t's parity
+// (layer = 2 - t % 2 + 2q), the wire cost (layer == t) or the precomputed
+// mid-edge layer change cost, kNone where the reference skips the layer
+struct Offer {
+    int64_t dst;
+    double v[5];
+};
+
+__device__ __forceinline__ void offer_load(const GridDev &g, const DagBatchDev &b, int node, int x, int y, int e,
+                                           int t, Offer &o) {
+    const int parent = b.par[e];
+    const int pv = b.nodes[parent];
+    const int px = pv / g.Y % g.X, py = pv % g.Y;
+    const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
+    const bool far = abs(x - px) + abs(y - py) > 4;
+    o.dst = ((int64_t)b.child_off[parent] + b.child_slot[e]) * kML + t;
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        const int layer = 2 - (t & 1) + 2 * q;
+        o.v[q] = kNone;
+        if (layer >= kML) continue;
+        const int dl = (layer & 1) ^ g.DIR;  // direction test of the reference, on 1-based layers
+        if (dl == 1 && y != py) continue;
+        if (dl == 0 && x != px) continue;
+        if (t == layer) {
+            o.v[q] = wire_cost(g, layer - 1, minx, maxx, miny, maxy);
+        } else if (far) {
+            const double ce = b.cost_edges[(int64_t)e * 81 + (layer - 1) * 9 + (t - 1)];
+            if (ce < kInf) o.v[q] = ce;
+        }
+    }
+}
+
+// the minimum packed offer of the pair over its source layers, then atomicMin
+// into the parent's entry (the minimum does not depend on the order)
+__device__ __forceinline__ void offer_send(const DagBatchDev &b, const Offer &o, const double *cost, int node) {
+    const int t = (int)(o.dst % kML);
+    unsigned long long m = ~0ull;
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        const int layer = 2 - (t & 1) + 2 * q;
+        if (layer >= kML || !(o.v[q] < kNone)) continue;
+        const double c2 = cost[layer] + o.v[q];
+        const int choice = t == layer ? 82 : (layer - 1) * 9 + (t - 1);
+        const unsigned long long nv = pack((float)c2, node * 100 + choice);
+        if (nv < m) m = nv;
+    }
+    if (m != ~0ull) atomicMin(b.packed + o.dst, m);
+}
+
+// Lshape_route_node_layer_change_cuda for one node, computed by one warp.
+//
+// The reference walks low = 1..fixed_low; for each low it scans layer =
+// low..9, keeping per child the first minimum of the packed costs over
+// [low, layer] and the via cost of the column from low to layer, offers the
+// candidate T(low, layer) = via + sum of the children's minima (for layer >=
+// fixed_high, if below INF) to cost[layer] with a strict `<`, then copies
+// cost[layer + 1] down to cost[layer] where strictly smaller, layer 8..low.
+// Unrolling that order, cost[j] ends as the minimum of T(low, J) over
+// low <= j <= J, and of equal candidates the one with the smallest low, then
+// the smallest J, is the one that arrives first and stays; best[c][j] is then
+// child c's first minimum over [low, J] of that winner.  The warp computes the
+// 45 candidates row by row (lane = low, the same additions in the same order),
+// the suffix minima of each row, and per layer the minimum over rows.
+__device__ void dp_node_warp(const GridDev &g, const DagBatchDev &b, int node, int lane, NodeScratch &s) {
     const int X = g.X, Y = g.Y, XY = X * Y;
-    const int pb = b.par_off[node], pn = b.par_off[node + 1] - pb;
     const int v = b.nodes[node];
     const int fixed_low = 1 + v / XY;
-    const int x = v / Y % X, y = v % Y;
     const int fixed_high = fixed_low == 10 ? 0 : fixed_low;
+    const int x = v / Y % X, y = v % Y;
     const int cb = b.child_off[node], cn = b.child_off[node + 1] - cb;
-    unsigned long long *best = b.best_path + (int64_t)cb * kML;
-    const unsigned long long *pk = b.packed + (int64_t)cb * kML;
-    double *cost = b.costs + (int64_t)node * kML;
-    double minc[kML];
-    unsigned long long bp[kML];
-    for (int c = 0; c < kML; c++) bp[c] = 0;
-    for (int low = 1; low <= fixed_low; low++) {
-        for (int c = 0; c < cn; c++) minc[c] = kInf;
+    __syncwarp();  // the previous node's scratch is no longer read
+    {
+        // the children's atomics landed in L2: read past L1
+        const unsigned long long *pk = b.packed + (int64_t)cb * kML;
+        for (int i = lane; i < cn * 9; i += 32) {
+            const int c = i / 9, layer = 1 + i % 9;
+            s.pk[c][layer] = __ldcg(pk + c * kML + layer);
+        }
+        if (lane < 8) s.vcol[lane] = g.vcost[cell_at(g, lane, x, y)];
+    }
+    // the parent-side inputs do not depend on the DP: issue their loads now
+    const int pb = b.par_off[node], pn = b.par_off[node + 1] - pb;
+    Offer o;
+    if (lane < pn * 9) offer_load(g, b, node, x, y, pb + lane / 9, 1 + lane % 9, o);
+    __syncwarp();
+    if (lane < 9) {
+        const int low = lane + 1;
+        double T[kML];
+        double minc[kML];
+#pragma unroll
+        for (int c = 0; c < kML; c++) minc[c] = kInf;
         double via = 0;
-        for (int layer = low; layer < g.L + 1; layer++) {
-            if (layer > low) via += g.vcost[cell_at(g, layer - 2, x, y)];
-            for (int c = 0; c < cn; c++) {
-                double cc;
-                int id;
-                unpack(pk[c * kML + layer], &cc, &id);
-                if (cc < minc[c]) { minc[c] = cc; bp[c] = (unsigned long long)id * kML + layer; }
-            }
-            if (layer >= fixed_high) {
+#pragma unroll
+        for (int J = 1; J < kML; J++) {
+            T[J] = kNone;
+            if (J >= low && low <= fixed_low) {
+                if (J > low) via += s.vcol[J - 2];
                 double t = via;
-                for (int c = 0; c < cn; c++) t += minc[c];
-                if (t < kInf && t < cost[layer]) {
-                    cost[layer] = t;
-                    for (int c = 0; c < cn; c++) best[c * kML + layer] = bp[c];
+#pragma unroll
+                for (int c = 0; c < kML; c++) {
+                    if (c < cn) {
+                        const double cc = packed_cost(s.pk[c][J]);
+                        if (cc < minc[c]) minc[c] = cc;
+                        t += minc[c];
+                    }
                 }
+                if (J >= fixed_high && t < kInf) T[J] = t;
             }
         }
-        for (int layer = g.L + 1 - 2; layer >= low; layer--) {
-            if (cost[layer + 1] < cost[layer]) {
-                cost[layer] = cost[layer + 1];
-                for (int c = 0; c < cn; c++) best[c * kML + layer] = best[c * kML + layer + 1];
-            }
+        double r = kNone;
+        int rj = -1;
+#pragma unroll
+        for (int J = kML - 1; J >= 1; J--) {
+            if (T[J] < kNone && T[J] <= r) { r = T[J]; rj = J; }  // equal: the smaller top layer
+            s.row[low][J] = r;
+            s.row_at[low][J] = (signed char)rj;
         }
     }
-    for (int pi = 0; pi < pn; pi++) {
-        const int e = pb + pi;
-        const int parent = b.par[e];
-        const int slot = b.child_slot[e];
-        unsigned long long *ppk = b.packed + (int64_t)b.child_off[parent] * kML + slot * kML;
-        const int pv = b.nodes[parent];
-        const int px = pv / Y % X, py = pv % Y;
-        const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
-        unsigned long long cache[kML];
-        for (int t = 1; t < kML; t++) cache[t] = ppk[t];
-        for (int layer = 1; layer < kML; layer++) {
-            const int dl = (layer & 1) ^ g.DIR;  // direction test of the reference, on 1-based layers
-            if (dl == 1 && y != py) continue;
-            if (dl == 0 && x != px) continue;
-            const double base = cost[layer];
-            for (int t = 1 + (1 - layer % 2); t < kML; t += 2) {
-                double c2;
-                int choice = 82;
-                if (t == layer) {
-                    c2 = base + wire_cost(g, layer - 1, minx, maxx, miny, maxy);
-                } else if (abs(x - px) + abs(y - py) > 4) {
-                    const int seq = (layer - 1) * 9 + (t - 1);
-                    const double ce = b.cost_edges[(int64_t)e * 81 + seq];
-                    if (ce < kInf) { c2 = base + ce; choice = seq; }
-                    else continue;
-                } else {
-                    continue;
-                }
-                const unsigned long long nv = pack((float)c2, node * 100 + choice);
-                if (nv < cache[t]) cache[t] = nv;
+    __syncwarp();
+    double *cost = b.costs + (int64_t)node * kML;
+    if (lane < 9) {
+        const int j = lane + 1;
+        double m = kNone;
+        int wl = -1, wj = -1;
+        for (int lo = 1; lo <= j; lo++) {
+            const double r = s.row[lo][j];
+            if (r < m) { m = r; wl = lo; wj = s.row_at[lo][j]; }  // equal: the smaller low
+        }
+        const double cj = wl > 0 ? m : kInf;
+        s.cost[j] = cj;
+        s.win[j] = wl > 0 ? wl * 16 + wj : -1;
+        cost[j] = cj;
+    } else if (lane == 9) {
+        s.cost[0] = kInf;
+        s.win[0] = -1;
+        cost[0] = kInf;
+    }
+    __syncwarp();
+    unsigned long long *best = b.best_path + (int64_t)cb * kML;
+    for (int i = lane; i < cn * kML; i += 32) {
+        const int c = i / kML, j = i % kML;
+        const int w = s.win[j];
+        unsigned long long val = 0;
+        if (w >= 0) {
+            double m = kInf;
+            for (int q = w >> 4; q <= (w & 15); q++) {
+                const unsigned long long p = s.pk[c][q];
+                const double cc = packed_cost(p);
+                if (cc < m) { m = cc; val = (unsigned long long)packed_id(p) * kML + q; }
             }
         }
-        for (int t = 1; t < kML; t++) atomicMin(ppk + t, cache[t]);
+        best[c * kML + j] = val;
     }
+    for (int i = lane + 32; i < pn * 9; i += 32) {
+        Offer o2;
+        offer_load(g, b, node, x, y, pb + i / 9, 1 + i % 9, o2);
+        offer_send(b, o2, s.cost, node);
+    }
+    if (lane < pn * 9) offer_send(b, o, s.cost, node);
 }
 
 __device__ __forceinline__ void stage2(const DagBatchDev &b, int node, int a, int c, int *err) {
@@ -275,113 +368,94 @@ __device__ void trace_node(const GridDev &g, const DagBatchDev &b, int node, int
     if (mnl < mxl) stage2(b, node, (mnl - 1) * XY + cx * Y + cy, (mxl - 1) * XY + cx * Y + cy, g.err);
 }
 
-__global__ void dag_levels_kernel(GridDev g, DagBatchDev b, unsigned *bar, int stamp) {
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-    unsigned epoch = 0;
-    for (int d = b.depth - 1; d >= 0; d--) {
-        for (int s = b.level_off[d] + tid; s < b.level_off[d + 1]; s += nth) dp_node(g, b, b.level_nodes[s]);
-        if (!grid_sync(bar, g.err, epoch)) return;
-    }
-    for (int d = 0; d < b.depth; d++) {
-        for (int s = b.level_off[d] + tid; s < b.level_off[d + 1]; s += nth) trace_node(g, b, b.level_nodes[s], stamp);
-        if (!grid_sync(bar, g.err, epoch)) return;
-    }
-}
-
-// one-level launches, used when a cooperative launch is not available
-__global__ void dag_dp_level_kernel(GridDev g, DagBatchDev b, int d) {
-    const int s = b.level_off[d] + blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < b.level_off[d + 1]) dp_node(g, b, b.level_nodes[s]);
-}
-__global__ void dag_trace_level_kernel(GridDev g, DagBatchDev b, int d, int stamp) {
-    const int s = b.level_off[d] + blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < b.level_off[d + 1]) trace_node(g, b, b.level_nodes[s], stamp);
-}
-
-// route records in DAG node order: one warp per net
-__global__ void dag_compact_kernel(GridDev g, DagBatchDev b) {
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < b.n_nets; k += warps) {
-        const int net = b.net_ids[k];
-        int *r = b.routes + b.route_off[net];
-        const int cap = b.route_cap[net];
-        const int n0 = b.net_node_off[k], n1 = b.net_node_off[k + 1];
-        int base = 1;
-        for (int c0 = n0; c0 < n1; c0 += 32) {
-            const int node = c0 + lane;
-            const int cnt = node < n1 ? b.stage_cnt[node] : 0;
-            int inc = cnt;
+// route record of net k in DAG node order, written by one warp
+__device__ void compact_net(const GridDev &g, const DagBatchDev &b, int k, int lane) {
+    const int net = b.net_ids[k];
+    int *r = b.routes + b.route_off[net];
+    const int cap = b.route_cap[net];
+    const int n0 = b.net_node_off[k], n1 = b.net_node_off[k + 1];
+    int base = 1;
+    for (int c0 = n0; c0 < n1; c0 += 32) {
+        const int node = c0 + lane;
+        const int cnt = node < n1 ? b.stage_cnt[node] : 0;
+        int inc = cnt;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, inc, o);
-                if (lane >= o) inc += t;
-            }
-            const int at = base + inc - cnt;
-            if (cnt && at + cnt <= cap)
-                for (int j = 0; j < cnt; j++) r[at + j] = b.stage[(int64_t)node * 8 + j];
-            else if (cnt)
-                set_error(g.err, ERR_CAPACITY);
-            base += __shfl_sync(0xffffffffu, inc, 31);
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
         }
-        if (lane == 0) r[0] = base <= cap ? base : 1;
+        const int at = base + inc - cnt;
+        if (cnt && at + cnt <= cap)
+            for (int j = 0; j < cnt; j++) r[at + j] = b.stage[(int64_t)node * 8 + j];
+        else if (cnt)
+            set_error(g.err, ERR_CAPACITY);
+        base += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    if (lane == 0) r[0] = base <= cap ? base : 1;
+}
+
+// one CTA per net: initialisation, DP levels deepest first, trace levels root
+// first, compaction
+__global__ void __launch_bounds__(kDagThreads) dag_net_kernel(GridDev g, DagBatchDev b, int stamp) {
+    __shared__ NodeScratch scr[kDagWarps];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int k = blockIdx.x; k < b.n_nets; k += gridDim.x) {
+        const int n0 = b.net_node_off[k], n1 = b.net_node_off[k + 1];
+        const int64_t s0 = (int64_t)b.child_off[n0] * kML, s1 = (int64_t)b.child_off[n1] * kML;
+        for (int64_t i = s0 + tid; i < s1; i += kDagThreads) b.packed[i] = kInitPacked;
+        for (int v = n0 + tid; v < n1; v += kDagThreads) {
+            b.layer_out[v] = -1;
+            b.stage_cnt[v] = 0;
+        }
+        __syncthreads();
+        const int l0 = b.net_level_off[k], nl = b.net_level_off[k + 1] - l0 - 1;
+        for (int d = nl - 1; d >= 0; d--) {
+            const int a = b.level_off[l0 + d], e = b.level_off[l0 + d + 1];
+            for (int s = a + warp; s < e; s += kDagWarps) dp_node_warp(g, b, b.level_nodes[s], lane, scr[warp]);
+            __syncthreads();
+        }
+        for (int d = 0; d < nl; d++) {
+            const int a = b.level_off[l0 + d], e = b.level_off[l0 + d + 1];
+            for (int s = a + tid; s < e; s += kDagThreads) trace_node(g, b, b.level_nodes[s], stamp);
+            __syncthreads();
+        }
+        if (warp == 0) compact_net(g, b, k, lane);
+        __syncthreads();
     }
 }
 
 }  // namespace
 
-int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, unsigned *bar_words, bool cooperative,
-                     cudaStream_t s) {
-    if (b.n_nodes <= 0) return 0;
-    int launches = 0;
-    {
-        int64_t work = (int64_t)b.n_slots * kML;
-        if ((int64_t)b.n_nodes * kML > work) work = (int64_t)b.n_nodes * kML;
-        int blocks = (int)((work + 255) / 256);
-        if (blocks > 148 * 16) blocks = 148 * 16;
-        dag_init_kernel<<<blocks < 1 ? 1 : blocks, 256, 0, s>>>(b);
-        launches++;
+void dag_levels(int n, const int *node_off, const int *depth, std::vector<int> &level_nodes,
+                std::vector<int> &level_off, std::vector<int> &net_level_off) {
+    level_nodes.resize(node_off[n] - node_off[0]);
+    level_off.clear();
+    net_level_off.assign(1, 0);
+    std::vector<int> cnt;
+    for (int k = 0; k < n; k++) {
+        const int a = node_off[k], e = node_off[k + 1];
+        int D = 0;
+        for (int v = a; v < e; v++) D = std::max(D, depth[v] + 1);
+        cnt.assign(D + 1, 0);
+        for (int v = a; v < e; v++) cnt[depth[v] + 1]++;
+        cnt[0] = a - node_off[0];
+        for (int d = 0; d < D; d++) cnt[d + 1] += cnt[d];
+        level_off.insert(level_off.end(), cnt.begin(), cnt.end());
+        for (int v = a; v < e; v++) level_nodes[cnt[depth[v]]++] = v;
+        net_level_off.push_back((int)level_off.size());
     }
+}
+
+int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStream_t s) {
+    if (b.n_nodes <= 0 || b.n_nets <= 0) return 0;
+    int launches = 0;
     if (b.n_edges > 0) {
         const int64_t th = (int64_t)b.n_edges * 9;
         dag_edge_cost_kernel<<<(int)((th + 255) / 256), 256, 0, s>>>(g, b);
         launches++;
     }
-    if (cooperative) {
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dag_levels_kernel, 256, 0);
-        int blocks = sms * (per < 2 ? per : 2);
-        const int need = (int)((b.max_level + 255) / 256);
-        if (need < blocks) blocks = need < 1 ? 1 : need;
-        cudaMemsetAsync(bar_words, 0, 2 * sizeof(unsigned), s);
-        unsigned *bar = bar_words;
-        GridDev gg = g;
-        DagBatchDev bb = b;
-        void *args[] = {&gg, &bb, &bar, &stamp};
-        cudaError_t e = cudaLaunchCooperativeKernel((const void *)dag_levels_kernel, dim3(blocks), dim3(256), args, 0, s);
-        if (e != cudaSuccess) return -1;
-        launches++;
-    } else {
-        for (int d = b.depth - 1; d >= 0; d--) {
-            const int w = b.h_level_off[d + 1] - b.h_level_off[d];
-            dag_dp_level_kernel<<<(w + 255) / 256, 256, 0, s>>>(g, b, d);
-            launches++;
-        }
-        for (int d = 0; d < b.depth; d++) {
-            const int w = b.h_level_off[d + 1] - b.h_level_off[d];
-            dag_trace_level_kernel<<<(w + 255) / 256, 256, 0, s>>>(g, b, d, stamp);
-            launches++;
-        }
-    }
-    {
-        int blocks = (b.n_nets + 7) / 8;
-        if (blocks > 148 * 16) blocks = 148 * 16;
-        dag_compact_kernel<<<blocks < 1 ? 1 : blocks, 256, 0, s>>>(g, b);
-        launches++;
-    }
-    return launches;
+    dag_net_kernel<<<b.n_nets, kDagThreads, 0, s>>>(g, b, stamp);
+    return launches + 1;
 }
 
 }  // namespace igr

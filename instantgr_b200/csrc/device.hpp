@@ -103,10 +103,12 @@ void launch_wire_ripup(const GridDev &g, const ViaBatchDev &b, int stamp, int K,
 // slot child_slot[e] of the parent, child node edge_child[e]); the child slots
 // of v are child_off[v]..child_off[v+1].
 struct DagBatchDev {
-    int n_nodes = 0, n_edges = 0, n_slots = 0, depth = 0, n_nets = 0, max_level = 0;
+    int n_nodes = 0, n_edges = 0, n_nets = 0;
     const int *nodes = nullptr, *par_off = nullptr, *par = nullptr, *child_slot = nullptr, *edge_child = nullptr;
-    const int *child_off = nullptr, *level_off = nullptr, *level_nodes = nullptr;
-    const int *h_level_off = nullptr;  // host copy of level_off (per-level launches)
+    const int *child_off = nullptr;
+    // levels of each net (dag_levels): net k's levels are level_off[net_level_off[k] + d],
+    // d = 0..depth_k, positions into level_nodes
+    const int *level_off = nullptr, *level_nodes = nullptr, *net_level_off = nullptr;
     const int *net_node_off = nullptr, *net_ids = nullptr;
     double *costs = nullptr;
     unsigned long long *best_path = nullptr, *packed = nullptr;
@@ -116,9 +118,13 @@ struct DagBatchDev {
     const int *route_cap = nullptr;
     int *routes = nullptr;
 };
-// returns the number of kernel launches, or -1 when the cooperative launch failed
-int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, unsigned *bar_words, bool cooperative,
-                     cudaStream_t s);
+// per-net level lists of n nets whose nodes are node_off[k]..node_off[k+1]:
+// level_nodes holds each net's nodes by depth (stable), level_off the depth_k + 1
+// level boundaries of each net, net_level_off[k] where net k's boundaries start
+void dag_levels(int n, const int *node_off, const int *depth, std::vector<int> &level_nodes,
+                std::vector<int> &level_off, std::vector<int> &net_level_off);
+// edge costs, then one CTA per net; returns the number of kernel launches
+int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStream_t s);
 
 constexpr int kRouteLayers = 9;
 

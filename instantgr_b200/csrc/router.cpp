@@ -883,7 +883,6 @@ bool Router::rrr_pass(int iter) {
     d_is_of.alloc(R);
     d_xsum.alloc((size_t)X * Y);
     d_ysum.alloc((size_t)X * Y);
-    d_bar.alloc(2);
     if (iter > 0) {  // records moved in the previous pass
         d_route_off.upload(route_off, s);
         d_route_cap.upload(route_cap, s);
@@ -975,20 +974,17 @@ bool Router::rrr_pass(int iter) {
         for (int k : lb[b]) batches[b].push_back(of_nets[k]);
     std::reverse(batches.begin(), batches.end());
     // batch-local CSR of all batches, laid end to end
-    struct BInfo { int nb, eb, pb, lb, nnb, nets, n, e, slots, depth, max_level; };
+    struct BInfo { int nb, eb, pb, lb, nnb, nets, n, e, slots; };
     std::vector<BInfo> bi;
     std::vector<int> nodes, par_off, par, cslot, echild, child_off, level_off, level_nodes, net_node_off, net_ids;
+    std::vector<int> net_level_off, b_nodes, b_off, b_net;
     std::vector<int64_t> old_off = route_off;
     for (size_t b = 0; b < batches.size(); b++) {
         BInfo f{};
         f.nb = (int)nodes.size(); f.eb = (int)par.size(); f.pb = (int)par_off.size();
         f.lb = (int)level_off.size(); f.nnb = (int)net_node_off.size(); f.nets = (int)net_ids.size();
-        int n = 0, e = 0, sl = 0, depth = 0;
-        for (int id : batches[b]) {
-            const DagNet &dn = dag[id];
-            n += (int)dn.nodes.size();
-            for (int dv : dn.depth) depth = std::max(depth, dv + 1);
-        }
+        int n = 0, e = 0, sl = 0;
+        for (int id : batches[b]) n += (int)dag[id].nodes.size();
         std::vector<int> dep(n);
         par_off.push_back(0);
         child_off.push_back(0);
@@ -1018,29 +1014,48 @@ bool Router::rrr_pass(int iter) {
             route_off[id] = route_end;
             route_end += route_cap[id];
         }
-        // counting sort of nodes by depth (stable in node order)
-        std::vector<int> cnt(depth + 1, 0);
-        for (int v = 0; v < n; v++) cnt[dep[v] + 1]++;
-        for (int dd = 0; dd < depth; dd++) cnt[dd + 1] += cnt[dd];
-        int ml = 0;
-        for (int dd = 0; dd <= depth; dd++) level_off.push_back(cnt[dd]);
-        for (int dd = 0; dd < depth; dd++) ml = std::max(ml, cnt[dd + 1] - cnt[dd]);
-        std::vector<int> ln(n);
-        for (int v = 0; v < n; v++) ln[cnt[dep[v]]++] = v;
-        level_nodes.insert(level_nodes.end(), ln.begin(), ln.end());
+        // levels of each net of the batch (batch-local positions)
+        dag_levels((int)batches[b].size(), net_node_off.data() + f.nnb, dep.data(), b_nodes, b_off, b_net);
+        level_nodes.insert(level_nodes.end(), b_nodes.begin(), b_nodes.end());
+        level_off.insert(level_off.end(), b_off.begin(), b_off.end());
+        net_level_off.insert(net_level_off.end(), b_net.begin(), b_net.end());
         if ((int64_t)n * 100 + 99 > 0x7fffffffLL) throw Error(ERR_CAPACITY, "DAG batch too large for 32-bit node ids");
-        f.n = n; f.e = e; f.slots = sl; f.depth = depth; f.max_level = ml;
+        f.n = n; f.e = e; f.slots = sl;
         bi.push_back(f);
+    }
+    if (verbose) {
+        // shape of the DAGs: nodes and depth per net, widest level of one net
+        std::vector<int> nn, nd, nw;
+        for (int id : of_nets) {
+            const DagNet &dn = dag[id];
+            int dmax = 0;
+            for (int dv : dn.depth) dmax = std::max(dmax, dv + 1);
+            std::vector<int> w(dmax, 0);
+            for (int dv : dn.depth) w[dv]++;
+            nn.push_back((int)dn.nodes.size());
+            nd.push_back(dmax);
+            nw.push_back(dmax ? *std::max_element(w.begin(), w.end()) : 0);
+        }
+        auto q = [](std::vector<int> v, double p) {
+            std::sort(v.begin(), v.end());
+            return v.empty() ? 0 : v[std::min(v.size() - 1, (size_t)(p * (v.size() - 1) + 0.5))];
+        };
+        std::fprintf(stderr,
+                     "[igr] dags: %zu batches, %zu nets, %zu nodes; per net nodes p50 %d p90 %d p99 %d max %d, "
+                     "depth p50 %d p90 %d p99 %d max %d, widest level p50 %d p99 %d max %d\n",
+                     batches.size(), of_nets.size(), nodes.size(), q(nn, .5), q(nn, .9), q(nn, .99), q(nn, 1),
+                     q(nd, .5), q(nd, .9), q(nd, .99), q(nd, 1), q(nw, .5), q(nw, .99), q(nw, 1));
     }
     grow_routes(route_end);
     dg_nodes.upload(nodes, s); dg_paroff.upload(par_off, s); dg_par.upload(par, s); dg_cslot.upload(cslot, s);
     dg_echild.upload(echild, s); dg_childoff.upload(child_off, s); dg_leveloff.upload(level_off, s);
     dg_levelnodes.upload(level_nodes, s); dg_nno.upload(net_node_off, s); dg_ids.upload(net_ids, s);
+    dg_netlvl.upload(net_level_off, s);
     d_old_off.upload(old_off, s);
     d_route_off.upload(route_off, s);
     d_route_cap.upload(route_cap, s);
     st.h2d_bytes += (int64_t)(nodes.size() * 2 + par_off.size() * 2 + par.size() * 3 + level_off.size() +
-                              net_node_off.size() + net_ids.size()) * 4 + (int64_t)R * 20;
+                              net_level_off.size() + net_node_off.size() + net_ids.size()) * 4 + (int64_t)R * 20;
     int mn = 1, me = 1, ms = 1;
     for (auto &f : bi) { mn = std::max(mn, f.n); me = std::max(me, f.e); ms = std::max(ms, f.slots); }
     dg_costs.alloc((size_t)mn * 10); dg_cedges.alloc((size_t)me * 81);
@@ -1060,23 +1075,17 @@ bool Router::rrr_pass(int iter) {
         launch_cost_refresh(go.g, true, s);
         kt.end(KC_COST);
         DagBatchDev db;
-        db.n_nodes = f.n; db.n_edges = f.e; db.n_slots = f.slots; db.depth = f.depth; db.n_nets = nnet;
-        db.max_level = f.max_level;
+        db.n_nodes = f.n; db.n_edges = f.e; db.n_nets = nnet;
         db.nodes = dg_nodes.p + f.nb; db.par_off = dg_paroff.p + f.pb; db.par = dg_par.p + f.eb;
         db.child_slot = dg_cslot.p + f.eb; db.edge_child = dg_echild.p + f.eb; db.child_off = dg_childoff.p + f.pb;
         db.level_off = dg_leveloff.p + f.lb; db.level_nodes = dg_levelnodes.p + f.nb;
-        db.h_level_off = level_off.data() + f.lb;
+        db.net_level_off = dg_netlvl.p + f.nnb;
         db.net_node_off = dg_nno.p + f.nnb; db.net_ids = dg_ids.p + f.nets;
         db.costs = dg_costs.p; db.best_path = dg_best.p; db.packed = dg_packed.p; db.cost_edges = dg_cedges.p;
         db.best_change = dg_bchange.p; db.layer_out = dg_lout.p; db.stage = dg_stage.p; db.stage_cnt = dg_scnt.p;
         db.route_off = d_route_off.p; db.route_cap = d_route_cap.p; db.routes = routes.p;
         kt.begin(KC_DAG);
-        int nl = launch_dag_route(go.g, db, s2, d_bar.p, cooperative, s);
-        if (nl < 0) {
-            cudaGetLastError();
-            cooperative = false;
-            nl = launch_dag_route(go.g, db, s2, d_bar.p, false, s);
-        }
+        const int nl = launch_dag_route(go.g, db, s2, s);
         kt.end(KC_DAG);
         kt.begin(KC_WIRE_COMMIT);
         launch_wire_commit(go.g, s2, true, s);

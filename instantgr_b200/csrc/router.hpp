@@ -186,12 +186,10 @@ struct Router {
     DevBuf<int> d_perm1, d_plan_hist, d_plan_offs;  // phase-1 colouring ranks, plan scratch
     DevBuf<uint8_t> d_is_of;
     DevBuf<float> d_xsum, d_ysum;
-    DevBuf<unsigned> d_bar;
     DevBuf<int> dg_nodes, dg_paroff, dg_par, dg_cslot, dg_echild, dg_childoff, dg_leveloff, dg_levelnodes, dg_nno,
-        dg_ids, dg_bchange, dg_lout, dg_stage, dg_scnt;
+        dg_netlvl, dg_ids, dg_bchange, dg_lout, dg_stage, dg_scnt;
     DevBuf<double> dg_costs, dg_cedges;
     DevBuf<unsigned long long> dg_best, dg_packed;
-    bool cooperative = true;
     std::vector<DagNet> dag;  // detour DAG of every rerouted net (phase 2)
     unsigned long long cost_cells = 0, commit_cells = 0;
     // phase-1 plan of the last run (routing order, batches, trees, route capacity in order)
