@@ -58,46 +58,83 @@ __device__ __forceinline__ void add_wire(const GridDev &g, int l, int xa, int xb
     g.dirty_commit[first + (layer_dir(g, l) ? xa : ya)] = 1;
 }
 
-// precompute_cost_edge: one thread per (edge, from layer)
-__global__ void dag_edge_cost_kernel(GridDev g, DagBatchDev b) {
-    const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t e = idx / 9;
+constexpr int kEdgeWarps = 4;
+constexpr int kMaxPos = 40;  // mid-edge positions of one edge: at most 38 (see below)
+
+struct EdgeScratch {
+    double vc[kMaxPos][9];  // via cost per position and layer
+    double ps[kMaxPos][9];  // wire prefix sum per position and layer
+    double pf[9], pt[9];    // wire prefix sums at the child and the parent end
+};
+
+// precompute_cost_edge, one warp per edge.  For every source layer f whose
+// direction runs along the edge and every target layer t of the same parity,
+// the cheapest position of the layer change among the positions s0 + k * dd
+// strictly inside the edge (dd = dist / min(dist, 20), so at most 38 of them):
+// via cost of the column from min(f, t) to max(f, t) plus the wire costs of
+// both legs, first minimum in position order.  Source layers across the edge
+// get INF.  Only edges longer than 4 GCells are computed: the DP reads these
+// costs for such edges alone, and the backtrace only where the DP chose them.
+// The positions' via costs and prefix sums are staged in shared memory; each
+// lane then scans the positions for one (f, t) pair with the reference's
+// additions in the reference's order.
+__global__ void __launch_bounds__(32 * kEdgeWarps) dag_edge_cost_kernel(GridDev g, DagBatchDev b) {
+    __shared__ EdgeScratch scr[kEdgeWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t e = (int64_t)blockIdx.x * kEdgeWarps + warp;
     if (e >= b.n_edges) return;
-    const int f = (int)(idx % 9);
-    const int to_node = b.par[e], from_node = b.edge_child[e];
+    EdgeScratch &s = scr[warp];
     const int Y = g.Y, X = g.X;
+    const int to_node = b.par[e], from_node = b.edge_child[e];
     const int tox = b.nodes[to_node] / Y % X, toy = b.nodes[to_node] % Y;
     const int fx = b.nodes[from_node] / Y % X, fy = b.nodes[from_node] % Y;
-    double *ce = b.cost_edges + e * 81 + f * 9;
-    int *bc = b.best_change + e * 81 + f * 9;
-    if ((layer_dir(g, f) == 0 && fy != toy) || (layer_dir(g, f) == 1 && fx != tox)) {
-        for (int t = 0; t < 9; t++) ce[t] = kInf;
-        return;
-    }
     const int dist = abs(tox - fx) + abs(toy - fy);
-    if (dist == 0) return;
-    const int dd = dist / min(dist, 20);
-    const bool vert = (fx == tox);
-    const int s0 = vert ? min(fy, toy) : min(fx, tox);
-    const int s1 = vert ? max(fy, toy) : max(fx, tox);
-    for (int t = 0; t < 9; t++) {
-        if ((t % 2) != (f % 2)) continue;
-        double best = kInf;
-        int pos = -1;
-        for (int sp = s0 + dd; sp < s1; sp += dd) {
-            const int sx = vert ? fx : sp, sy = vert ? sp : fy;
-            double via = 0;
-            for (int ll = min(f, t); ll < max(f, t); ll++) via += g.vcost[cell_at(g, ll, sx, sy)];
-            double c = via;
-            if (vert)
-                c += (wire_cost(g, f, fx, fx, min(fy, sy), max(fy, sy)) + wire_cost(g, t, tox, tox, min(toy, sy), max(toy, sy)));
-            else
-                c += (wire_cost(g, f, min(fx, sx), max(fx, sx), fy, fy) + wire_cost(g, t, min(tox, sx), max(tox, sx), toy, toy));
-            if (c < best) { best = c; pos = sp; }
-        }
-        ce[t] = best;
-        bc[t] = pos;
+    if (dist <= 4) return;
+    double *ce = b.cost_edges + e * 81;
+    int *bc = b.best_change + e * 81;
+    if (lane < 9) {
+        const int f = lane;
+        if ((layer_dir(g, f) == 0 && fy != toy) || (layer_dir(g, f) == 1 && fx != tox))
+            for (int t = 0; t < 9; t++) ce[f * 9 + t] = kInf;
     }
+    const bool vert = fx == tox;
+    if (!vert && fy != toy) return;  // no source layer runs along a bent edge
+    const int dd = dist / min(dist, 20);
+    const int s0 = vert ? min(fy, toy) : min(fx, tox);
+    const int npos = (dist - 1) / dd;  // positions s0 + k * dd < s0 + dist, k >= 1
+    for (int i = lane; i < npos * 9; i += 32) {
+        const int p = i / 9, l = i % 9;
+        const int sp = s0 + (p + 1) * dd;
+        const int sx = vert ? fx : sp, sy = vert ? sp : fy;
+        const int64_t cell = cell_at(g, l, sx, sy);
+        s.vc[p][l] = g.vcost[cell];
+        s.ps[p][l] = g.presum[cell];
+    }
+    if (lane < 9) s.pf[lane] = g.presum[cell_at(g, lane, fx, fy)];
+    else if (lane < 18) s.pt[lane - 9] = g.presum[cell_at(g, lane - 9, tox, toy)];
+    __syncwarp();
+    // the source layers along the edge are one parity class (directions
+    // alternate): f0, f0 + 2, ...; pair i = (f0 + 2 (i / nv), f0 + 2 (i % nv))
+    const int f0 = layer_dir(g, 0) == (vert ? 1 : 0) ? 0 : 1;
+    const int nv = f0 == 0 ? 5 : 4;
+    if (lane >= nv * nv) return;
+    const int f = f0 + 2 * (lane / nv), t = f0 + 2 * (lane % nv);
+    const int lo = min(f, t), hi = max(f, t);
+    const int fa = vert ? fy : fx, ta = vert ? toy : tox;  // the ends along the edge
+    double best = kInf;
+    int pos = -1;
+    for (int p = 0; p < npos; p++) {
+        const int sp = s0 + (p + 1) * dd;
+        double via = 0;
+        for (int ll = lo; ll < hi; ll++) via += s.vc[p][ll];
+        double c = via;
+        const double wf = fa < sp ? s.ps[p][f] - s.pf[f] : s.pf[f] - s.ps[p][f];
+        const double wt = ta < sp ? s.ps[p][t] - s.pt[t] : s.pt[t] - s.ps[p][t];
+        c += (wf + wt);
+        if (c < best) { best = c; pos = sp; }
+    }
+    ce[f * 9 + t] = best;
+    bc[f * 9 + t] = pos;
 }
 
 // per-warp scratch of the node DP
@@ -450,8 +487,7 @@ int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStre
     if (b.n_nodes <= 0 || b.n_nets <= 0) return 0;
     int launches = 0;
     if (b.n_edges > 0) {
-        const int64_t th = (int64_t)b.n_edges * 9;
-        dag_edge_cost_kernel<<<(int)((th + 255) / 256), 256, 0, s>>>(g, b);
+        dag_edge_cost_kernel<<<(int)((b.n_edges + kEdgeWarps - 1) / kEdgeWarps), 32 * kEdgeWarps, 0, s>>>(g, b);
         launches++;
     }
     dag_net_kernel<<<b.n_nets, kDagThreads, 0, s>>>(g, b, stamp);

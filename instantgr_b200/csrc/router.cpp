@@ -863,9 +863,13 @@ int Router::run_color(int n, const int *d_perm_ranks, const ShapeDev &shapes, in
     cd.hdr = d_hdr.p;
     cd.ops = d_cops.p;
     cd.npts = shapes.npts; cd.map = d_map.p; cd.batch = d_bat.p; cd.flags = d_flags.p;
+    const double t0 = verbose ? now_s() : 0;
     kt.begin(KC_COLOR);
     int nb = run_coloring(cd, 0, s);
     kt.end(KC_COLOR);
+    if (verbose)
+        std::fprintf(stderr, "[igr] colouring: %d nets, %zu claim cells, %d points, sparsity %d: %d batches, %d rounds, "
+                     "%.2f ms\n", n, shapes.claim.n, shapes.npts, sparsity, nb, cd.rounds, (now_s() - t0) * 1e3);
     st.color_rounds += cd.rounds;
     st.launches += 1;
     if (nb == -2) throw Error(ERR_TIMEOUT, "colouring barrier timed out");
