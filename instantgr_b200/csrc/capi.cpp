@@ -692,13 +692,16 @@ int igr_build_dag(int X, int Y, int mode, int ntree, const int32_t *pos, const i
         ns.L = 9; ns.X = X; ns.Y = Y;
         RNet r;
         r.tnode.assign(pos, pos + ntree);
-        r.adj.assign(ntree, {});
+        r.adj.off.assign(1, 0);
+        r.adj.nb.clear();
         for (int v = 0; v < ntree; v++) {
             if (pos[v] < 0 || pos[v] >= 10 * X * Y) throw Error(ERR_INVALID, "node position out of range");
+            if (adj_off[v + 1] < adj_off[v]) throw Error(ERR_INVALID, "adjacency offsets must not decrease");
             for (int q = adj_off[v]; q < adj_off[v + 1]; q++) {
                 if (adj[q] < 0 || adj[q] >= ntree) throw Error(ERR_INVALID, "adjacency out of range");
-                r.adj[v].push_back(adj[q]);
+                r.adj.nb.push_back(adj[q]);
             }
+            r.adj.off.push_back((int)r.adj.nb.size());
         }
         CongestionView cv;
         cv.X = X; cv.Y = Y;

@@ -37,7 +37,7 @@ struct Builder {
     int mode;
     DagNet &out;
     int X, Y, XY;
-    const std::vector<std::vector<int>> &G;  // tree adjacency
+    const TreeAdj &G;                        // tree adjacency
     const std::vector<int> &P;               // tree node positions (3-D, Steiner layer 9)
     int ntree;
     float ratio;

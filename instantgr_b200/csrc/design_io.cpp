@@ -12,6 +12,7 @@
 #include "host.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -34,14 +35,22 @@ void parallel_for(int n, int threads, const std::function<void(int, int)> &fn) {
     if (threads <= 0) threads = hw_threads();
     threads = std::min(threads, n);
     if (threads <= 1) { fn(0, n); return; }
-    std::vector<std::thread> ts;
+    // ranges are handed out dynamically, about eight per thread, so that items
+    // of very different cost (a 500-pin net beside two-pin nets) balance
+    const int chunk = std::max(1, n / (threads * 8));
+    std::atomic<int> next{0};
     std::vector<std::exception_ptr> errs(threads);
-    for (int t = 0; t < threads; t++) {
-        int b = (int)((int64_t)n * t / threads), e = (int)((int64_t)n * (t + 1) / threads);
-        ts.emplace_back([&, t, b, e] {
-            try { fn(b, e); } catch (...) { errs[t] = std::current_exception(); }
-        });
-    }
+    auto work = [&](int t) {
+        try {
+            for (int b; (b = next.fetch_add(chunk)) < n;) fn(b, std::min(n, b + chunk));
+        } catch (...) {
+            errs[t] = std::current_exception();
+            next.store(n);
+        }
+    };
+    std::vector<std::thread> ts;
+    for (int t = 1; t < threads; t++) ts.emplace_back(work, t);
+    work(0);
     for (auto &t : ts) t.join();
     for (auto &e : errs) if (e) std::rethrow_exception(e);
 }
@@ -100,9 +109,129 @@ struct Scanner {
     }
 };
 
+inline bool in_run(char c) { return is_dig(c) || c == '.'; }
+
+// The capacity values of all layers, parsed on several threads.  The layer
+// headers are read in order; a layer's values run up to the next layer name.
+// Each value section is cut into pieces at blanks (a blank never lies inside
+// a number, which is a digit followed by digits and dots); the numbers of
+// every piece are counted, then parsed with the scanner's arithmetic into
+// their places.  Returns false, having stored nothing that the sequential
+// reader would not, unless every section holds exactly X*Y numbers and only
+// blanks follow the last one before the next name: the caller then reads the
+// layers sequentially, which also produces the errors of malformed files.
+bool cap_layers_parallel(Design &d, const char *buf, size_t n, size_t p0, int threads) {
+    const int L = d.L;
+    const size_t XY = (size_t)d.X * d.Y;
+    std::vector<size_t> beg(L), end(L);
+    std::vector<int> dir(L);
+    std::vector<double> minlen(L);
+    Scanner t(buf, n);
+    t.p = p0;
+    try {
+        for (int l = 0; l < L; l++) {
+            size_t b, e;
+            t.read_token(b, e);
+            if (std::string(buf + b, buf + e) != "metal" + std::to_string(l + 1)) return false;
+            dir[l] = t.read_int();
+            minlen[l] = t.read_double();
+            if (l && dir[l] == dir[l - 1]) return false;
+            beg[l] = t.p;
+            if (l + 1 < L) {
+                const std::string next = "metal" + std::to_string(l + 2);
+                const void *f = memmem(buf + beg[l], n - beg[l], next.data(), next.size());
+                if (!f) return false;
+                end[l] = (size_t)((const char *)f - buf);
+                t.p = end[l];
+            } else {
+                end[l] = n;
+            }
+        }
+    } catch (const Error &) {
+        return false;
+    }
+    // pieces of 4 KB to 1 MB (about four per thread and section), cut at a blank
+    struct Piece { int l; size_t a, e; int64_t first, count; size_t last; };
+    std::vector<Piece> pc;
+    const size_t T = (size_t)(threads > 0 ? threads : hw_threads());
+    for (int l = 0; l < L; l++) {
+        const size_t len = std::min<size_t>((size_t)1 << 20, std::max<size_t>(4096, (end[l] - beg[l]) / (4 * T)));
+        size_t a = beg[l];
+        while (a < end[l]) {
+            size_t e = std::min(end[l], a + len);
+            while (e < end[l] && buf[e] != ' ' && buf[e] != '\n') e++;
+            pc.push_back({l, a, e, 0, 0, a});
+            a = e;
+        }
+    }
+    const int P = (int)pc.size();
+    parallel_for(P, threads, [&](int b, int e) {
+        for (int i = b; i < e; i++) {
+            Piece &q = pc[i];
+            int64_t c = 0;
+            bool run = false;
+            for (size_t k = q.a; k < q.e; k++) {
+                const char ch = buf[k];
+                if (run) {
+                    run = in_run(ch);
+                } else if (is_dig(ch)) {
+                    run = true;
+                    c++;
+                }
+            }
+            q.count = c;
+        }
+    });
+    for (int l = 0, i = 0; l < L; l++) {
+        int64_t c = 0;
+        for (; i < P && pc[i].l == l; i++) {
+            pc[i].first = c;
+            c += pc[i].count;
+        }
+        if (c != (int64_t)XY) return false;
+    }
+    const int X = d.X, Y = d.Y;
+    parallel_for(P, threads, [&](int b, int e) {
+        for (int i = b; i < e; i++) {
+            Piece &q = pc[i];
+            float *cap = d.cap.data() + (size_t)q.l * XY;
+            int64_t idx = q.first;
+            size_t k = q.a;
+            while (k < q.e) {
+                if (!is_dig(buf[k])) { k++; continue; }
+                double ans = 0, scale = 0;
+                for (; k < q.e && in_run(buf[k]); k++) {
+                    if (buf[k] == '.') scale = 1;
+                    else scale *= 10, ans = ans * 10 + (buf[k] - '0');
+                }
+                const int y = (int)(idx / X), x = (int)(idx % X);
+                cap[(size_t)x * Y + y] = (float)(scale == 0 ? ans : ans / scale);
+                idx++;
+                q.last = k;
+            }
+        }
+    });
+    // only blanks between a section's last number and the next layer name
+    for (int l = 0, i = 0; l + 1 < L; l++) {
+        size_t last = beg[l];
+        for (; i < P && pc[i].l == l; i++)
+            if (pc[i].count) last = pc[i].last;
+        for (size_t k = last; k < end[l]; k++)
+            if (buf[k] != ' ' && buf[k] != '\n') {
+                std::fill(d.cap.begin(), d.cap.end(), 0.f);
+                return false;
+            }
+    }
+    for (int l = 0; l < L; l++) {
+        d.layer_dir[l] = dir[l];
+        d.layer_min_len[l] = minlen[l];
+    }
+    return true;
+}
+
 }  // namespace
 
-void read_cap_buffer(Design &d, const char *buf, size_t n) {
+void read_cap_buffer(Design &d, const char *buf, size_t n, int threads) {
     Scanner s(buf, n);
     d.L = s.read_int();
     d.X = s.read_int();
@@ -129,6 +258,7 @@ void read_cap_buffer(Design &d, const char *buf, size_t n) {
     d.layer_dir.resize(d.L);
     d.layer_min_len.resize(d.L);
     d.cap.assign((size_t)d.L * d.X * d.Y, 0.f);
+    if (cap_layers_parallel(d, buf, n, s.p, threads)) return;
     for (int l = 0; l < d.L; l++) {
         size_t b, e;
         s.read_token(b, e);
@@ -237,7 +367,7 @@ void read_net_buffer(Design &d, const char *buf, size_t n) {
 void read_design(Design &d, const char *cap_path, const char *net_path, int threads) {
     {
         auto b = slurp(cap_path);
-        read_cap_buffer(d, b.data(), b.size() - 1);
+        read_cap_buffer(d, b.data(), b.size() - 1, threads);
     }
     {
         auto b = slurp(net_path);
@@ -289,8 +419,8 @@ void write_guides(const Design &d, const NetSet &ns, const RouteSource &rs, cons
             for (int64_t i = d.sel_off[n]; i < d.sel_off[n + 1]; i++)
                 if (d.sel[i] < XY) seg(d.sel[i], d.sel[i] + XY, out);
             for (int64_t i = d.extra_off[n]; i < d.extra_off[n + 1]; i += 2) seg(d.extra[i], d.extra[i + 1], out);
-            if (n < (int)ns.subnets.size())
-                for (int s : ns.subnets[n]) {
+            if (n + 1 < (int)ns.sub_off.size())
+                for (int s = ns.sub_off[n]; s < ns.sub_off[n + 1]; s++) {
                     const int *r = rs.routes_of(s);
                     if (!r) continue;
                     for (int j = 1; j < r[0]; j += 2) seg(r[j] + XY, r[j + 1] + XY, out);

@@ -63,13 +63,30 @@ struct Design {
 // (src/database.hpp:247-409): digits only (no signs, no exponents), '.' as the
 // only fraction mark, access points "(l, x, y)" grouped in "[...]" pins.
 void read_design(Design &d, const char *cap_path, const char *net_path, int threads);
-void read_cap_buffer(Design &d, const char *buf, size_t n);
+void read_cap_buffer(Design &d, const char *buf, size_t n, int threads = 0);
 void read_net_buffer(Design &d, const char *buf, size_t n);
 
 // Chooses one access point per pin (src/database.hpp:38-243), fills sel/extra.
 void select_pins(Design &d, int threads);
 
 // ---------------------------------------------------------------- routing nets
+// Adjacency of a tree in CSR form: the neighbours of node i are
+// nb[off[i] .. off[i+1]), in the order the edges were added.
+struct TreeAdj {
+    std::vector<int> off{0}, nb;
+    struct Row {
+        const int *b, *e;
+        const int *begin() const { return b; }
+        const int *end() const { return e; }
+        size_t size() const { return (size_t)(e - b); }
+        int operator[](size_t k) const { return b[k]; }
+    };
+    int size() const { return (int)off.size() - 1; }
+    Row operator[](int i) const { return Row{nb.data() + off[i], nb.data() + off[i + 1]}; }
+    // n nodes; each undirected edge (a, b) in order appends b to a's list, then a to b's
+    void from_edges(int n, const std::vector<std::pair<int, int>> &edges);
+};
+
 // A routing net ("subnet") is a net of >= 2 selected pins, split at
 // MAX_PIN_SIZE = 12 pins along its Steiner tree (src/database_cuda.hpp:2111-2237).
 struct RNet {
@@ -77,25 +94,58 @@ struct RNet {
     int hpwl = 0, minx = 0, maxx = 0, miny = 0, maxy = 0;
     std::vector<int> pins;         // routing-layer 3-D positions
     // Steiner tree: adjacency over nodes, node positions (3-D, Steiner -> layer L)
-    std::vector<std::vector<int>> adj;
+    TreeAdj adj;
     std::vector<int> tnode;
-    // 2-D conflict shapes used by batch colouring (src/database_cuda.hpp:746-820)
-    std::vector<std::pair<int, int>> hseg, vseg;
-    std::vector<int> points;
 };
+
+// 2-D conflict shapes of a routing net for batch colouring (net::construct_rsmt,
+// src/database_cuda.hpp:746-820), in the reference's order: the tree nodes as
+// points, then per tree edge (i, j < i) its horizontal and vertical segments
+// (pairs of 2-D cells, lower first) and its end or corner points.
+template <class Pt, class Hs, class Vs>
+void for_each_shape(const RNet &n, int X, int Y, Pt &&point, Hs &&hseg, Vs &&vseg) {
+    const int XY = X * Y;
+    const int m = (int)n.tnode.size();
+    for (int i = 0; i < m; i++) point(n.tnode[i] % XY);
+    for (int i = 0; i < m; i++) {
+        const int pi = n.tnode[i] % XY, xi = pi / Y, yi = pi % Y;
+        for (int j : n.adj[i]) {
+            if (j >= i) continue;
+            const int pj = n.tnode[j] % XY, xj = pj / Y, yj = pj % Y;
+            const int mnx = xi < xj ? xi : xj, mxx = xi < xj ? xj : xi;
+            const int mny = yi < yj ? yi : yj, mxy = yi < yj ? yj : yi;
+            if (xi != xj && yi != yj) {
+                hseg(mnx * Y + mny, mxx * Y + mny);
+                hseg(mnx * Y + mxy, mxx * Y + mxy);
+                vseg(mnx * Y + mny, mnx * Y + mxy);
+                vseg(mxx * Y + mny, mxx * Y + mxy);
+                point(xi * Y + yj);
+                point(xj * Y + yi);
+            } else if (xi != xj) {
+                hseg(mnx * Y + mny, mxx * Y + mny);
+                point(mnx * Y + mny);
+                point(mxx * Y + mny);
+            } else if (yi != yj) {
+                vseg(mnx * Y + mny, mnx * Y + mxy);
+                point(mnx * Y + mny);
+                point(mnx * Y + mxy);
+            }
+        }
+    }
+}
 
 struct NetSet {
     int L = 0, X = 0, Y = 0, DIR = 0;   // routing layers (L = 9)
     std::vector<RNet> nets;
-    std::vector<std::vector<int>> subnets;   // design net -> routing net ids
+    std::vector<int> sub_off;                // [design nets + 1]: routing nets sub_off[n] .. sub_off[n+1]
     std::vector<int> unfinished;             // design net -> subnets still routing
     std::vector<int64_t> pin_sum;            // [n+1] pin prefix sum (route slots)
 };
 
 // Builds routing nets: Steiner trees for every multi-pin net, split >12-pin nets.
 void build_netset(const Design &d, NetSet &ns, int threads);
-// Fills hseg/vseg/points/adj/tnode for one net from its tree (construct_rsmt).
-void construct_rsmt(const Design &d, const NetSet &ns, RNet &n, bool rsmt_only);
+// Tree (adj, tnode with layers) of one net (construct_rsmt, src/database_cuda.hpp:746-820).
+void construct_rsmt(const Design &d, const NetSet &ns, RNet &n);
 void calc_hpwl(const NetSet &ns, RNet &n);
 
 // DFS preorder flattening of a tree (src/Lshape_route.hpp:191-208).

@@ -4,7 +4,7 @@
 // Restates, in this project's own code, the host steps of InstantGR:
 //   build_cuda_database's net split       src/database_cuda.hpp:2111-2237
 //   my_flute (tree -> GCell graph, MST)   src/database_cuda.hpp:696-744
-//   net::construct_rsmt (segments/points) src/database_cuda.hpp:746-820
+//   net::construct_rsmt (tree, layers)    src/database_cuda.hpp:746-820
 //   net::calc_hpwl                        src/database_cuda.hpp:93-103
 //   the DFS flattening of phase 1         src/Lshape_route.hpp:191-208
 // The unstable std::sort calls of the reference (edges keyed on a single
@@ -23,8 +23,8 @@ namespace igr {
 namespace {
 
 // Tree over the distinct 2-D positions of `pos2d` (my_flute, database_cuda.hpp:696-744).
-void tree_from_positions(const Design &d, int Y, const std::vector<int> &pos2d,
-                         std::vector<std::vector<int>> &graph, std::vector<int> &nodes) {
+void tree_from_positions(const Design &d, int Y, const std::vector<int> &pos2d, TreeAdj &graph,
+                         std::vector<int> &nodes) {
     std::vector<int> x, y;
     x.reserve(pos2d.size()); y.reserve(pos2d.size());
     for (int e : pos2d) { x.push_back(d.dr_x[e / Y]); y.push_back(d.dr_y[e % Y]); }
@@ -52,19 +52,37 @@ void tree_from_positions(const Design &d, int Y, const std::vector<int> &pos2d,
     std::sort(edges.begin(), edges.end());
     std::vector<int> parent(nodes.size());
     std::iota(parent.begin(), parent.end(), 0);
-    std::function<int(int)> find = [&](int v) { return v == parent[v] ? v : parent[v] = find(parent[v]); };
-    graph.assign(nodes.size(), {});
+    auto find = [&](int v) {
+        int r = v;
+        while (parent[r] != r) r = parent[r];
+        while (parent[v] != r) { const int n = parent[v]; parent[v] = r; v = n; }
+        return r;
+    };
+    std::vector<std::pair<int, int>> kept;
+    kept.reserve(nodes.size());
     for (auto &e : edges) {
         int u = std::get<1>(e), v = std::get<2>(e), pu = find(u), pv = find(v);
         if (pu != pv) {
-            graph[u].push_back(v);
-            graph[v].push_back(u);
+            kept.push_back({u, v});
             parent[pu] = pv;
         }
     }
+    graph.from_edges((int)nodes.size(), kept);
 }
 
 }  // namespace
+
+void TreeAdj::from_edges(int n, const std::vector<std::pair<int, int>> &edges) {
+    off.assign(n + 1, 0);
+    for (auto &e : edges) { off[e.first + 1]++; off[e.second + 1]++; }
+    for (int i = 0; i < n; i++) off[i + 1] += off[i];
+    nb.resize(off[n]);
+    std::vector<int> at(off.begin(), off.end() - 1);
+    for (auto &e : edges) {
+        nb[at[e.first]++] = e.second;
+        nb[at[e.second]++] = e.first;
+    }
+}
 
 void steiner_tree(const std::vector<int> &x, const std::vector<int> &y, SteinerTree &t) {
     igr_steiner::Tree s;
@@ -85,52 +103,29 @@ void calc_hpwl(const NetSet &ns, RNet &n) {
     n.hpwl = n.maxx - n.minx + n.maxy - n.miny;
 }
 
-void construct_rsmt(const Design &d, const NetSet &ns, RNet &n, bool rsmt_only) {
+void construct_rsmt(const Design &d, const NetSet &ns, RNet &n) {
     const int X = ns.X, Y = ns.Y, XY = X * Y, L = ns.L;
-    std::unordered_map<int, int> layer;
+    // pins are distinct in 2-D (checked below); the layer of each 2-D position
+    std::vector<std::pair<int, int>> layer;
+    layer.reserve(n.pins.size());
     std::vector<int> pos;
+    pos.reserve(n.pins.size());
     for (int p : n.pins) {
-        int q = p % XY;
-        if (!layer.count(q)) pos.push_back(q);
-        layer[q] = p / XY;
+        layer.push_back({p % XY, p / XY});
+        pos.push_back(p % XY);
     }
-    if (pos.size() != n.pins.size()) throw Error(ERR_STATE, "two pins of a routing net share a 2-D position");
+    std::sort(layer.begin(), layer.end());
+    for (size_t i = 1; i < layer.size(); i++)
+        if (layer[i].first == layer[i - 1].first)
+            throw Error(ERR_STATE, "two pins of a routing net share a 2-D position");
     if (n.tnode.empty()) {
         tree_from_positions(d, Y, pos, n.adj, n.tnode);
     } else {
         for (auto &e : n.tnode) e %= XY;
     }
-    if (!rsmt_only) {
-        n.hseg.clear(); n.vseg.clear();
-        n.points = n.tnode;
-        for (int i = 0; i < (int)n.tnode.size(); i++) {
-            int xi = n.tnode[i] / Y, yi = n.tnode[i] % Y;
-            for (int j : n.adj[i]) {
-                if (j >= i) continue;
-                int xj = n.tnode[j] / Y, yj = n.tnode[j] % Y;
-                int mnx = std::min(xi, xj), mxx = std::max(xi, xj), mny = std::min(yi, yj), mxy = std::max(yi, yj);
-                if (xi != xj && yi != yj) {
-                    n.hseg.push_back({mnx * Y + mny, mxx * Y + mny});
-                    n.hseg.push_back({mnx * Y + mxy, mxx * Y + mxy});
-                    n.vseg.push_back({mnx * Y + mny, mnx * Y + mxy});
-                    n.vseg.push_back({mxx * Y + mny, mxx * Y + mxy});
-                    n.points.push_back(xi * Y + yj);
-                    n.points.push_back(xj * Y + yi);
-                } else if (xi != xj) {
-                    n.hseg.push_back({mnx * Y + mny, mxx * Y + mny});
-                    n.points.push_back(mnx * Y + mny);
-                    n.points.push_back(mxx * Y + mny);
-                } else if (yi != yj) {
-                    n.vseg.push_back({mnx * Y + mny, mnx * Y + mxy});
-                    n.points.push_back(mnx * Y + mny);
-                    n.points.push_back(mnx * Y + mxy);
-                }
-            }
-        }
-    }
     for (auto &e : n.tnode) {
-        auto it = layer.find(e);
-        e += (it != layer.end() ? it->second : L) * XY;
+        auto it = std::lower_bound(layer.begin(), layer.end(), std::make_pair(e, -1));
+        e += (it != layer.end() && it->first == e ? it->second : L) * XY;
     }
 }
 
@@ -147,7 +142,7 @@ void split_net(const Design &d, const NetSet &ns, int db_id, std::vector<RNet> &
         tmp.pins.push_back(p >= XY ? p - XY : p);
     }
     tmp.orig = db_id;
-    construct_rsmt(d, ns, tmp, true);
+    construct_rsmt(d, ns, tmp);
     const auto &tn = tmp.tnode;
     const int n = (int)tn.size();
     std::vector<char> not_steiner(n);
@@ -155,7 +150,12 @@ void split_net(const Design &d, const NetSet &ns, int db_id, std::vector<RNet> &
     std::vector<int> sz(n, 1), par(n);
     std::vector<std::tuple<int, int, int>> edges;
     edges.reserve(n);
-    std::function<int(int)> find = [&](int v) { return v == par[v] ? v : par[v] = find(par[v]); };
+    auto find = [&](int v) {
+        int r = v;
+        while (par[r] != r) r = par[r];
+        while (par[v] != r) { const int q = par[v]; par[v] = r; v = q; }
+        return r;
+    };
     for (int i = 0; i < n; i++) {
         par[i] = i;
         for (int j : tmp.adj[i])
@@ -198,16 +198,16 @@ void split_net(const Design &d, const NetSet &ns, int db_id, std::vector<RNet> &
             if (new_pins[i][j] < L * XY) s.pins.push_back(new_pins[i][j]);
             indx[new_pins[i][j]] = j;
         }
-        s.adj.assign(new_pins[i].size(), {});
         s.tnode = new_pins[i];
+        std::vector<std::pair<int, int>> se;
+        se.reserve(net_edge[i].size());
         for (int j : net_edge[i]) {
             auto &e = edges[j];
             int u = std::get<0>(e), v = std::get<1>(e);
             if (find(v) == i) std::swap(u, v);
-            int a = indx[tn[u]], b = indx[tn[v]];
-            s.adj[a].push_back(b);
-            s.adj[b].push_back(a);
+            se.push_back({indx[tn[u]], indx[tn[v]]});
         }
+        s.adj.from_edges((int)new_pins[i].size(), se);
         out.push_back(std::move(s));
     }
 }
@@ -217,44 +217,53 @@ void split_net(const Design &d, const NetSet &ns, int db_id, std::vector<RNet> &
 void build_netset(const Design &d, NetSet &ns, int threads) {
     ns.L = d.L - 1; ns.X = d.X; ns.Y = d.Y; ns.DIR = d.layer_dir[1];
     const int N = d.num_nets(), XY = d.X * d.Y;
-    std::vector<std::vector<RNet>> tmp(N);
+    // nets of more than 12 pins are split first (in parallel); every other
+    // multi-pin net is one routing net
+    std::vector<int> big;
+    for (int id = 0; id < N; id++)
+        if (d.sel_off[id + 1] - d.sel_off[id] > 12) big.push_back(id);
+    std::vector<std::vector<RNet>> parts(big.size());
+    parallel_for((int)big.size(), threads, [&](int b, int e) {
+        for (int k = b; k < e; k++) split_net(d, ns, big[k], parts[k]);
+    });
     ns.unfinished.assign(N, 0);
+    ns.sub_off.assign(N + 1, 0);
+    for (int id = 0, k = 0; id < N; id++) {
+        const int64_t np = d.sel_off[id + 1] - d.sel_off[id];
+        const int cnt = np == 1 ? 0 : (np <= 12 ? 1 : (int)parts[k++].size());
+        ns.unfinished[id] = cnt;
+        ns.sub_off[id + 1] = ns.sub_off[id] + cnt;
+    }
+    const int R = ns.sub_off[N];
+    ns.nets.clear();
+    ns.nets.resize(R);
+    std::vector<int> part_of(N, -1);
+    for (int k = 0; k < (int)big.size(); k++) part_of[big[k]] = k;
+    // routing nets in design-net order; trees of every routing net (Lshape_route.hpp:159-163)
     parallel_for(N, threads, [&](int b, int e) {
         for (int id = b; id < e; id++) {
-            int64_t np = d.sel_off[id + 1] - d.sel_off[id];
-            if (np == 1) continue;
-            if (np <= 12) {
-                RNet r;
+            const int r0 = ns.sub_off[id], r1 = ns.sub_off[id + 1];
+            if (r0 == r1) continue;
+            if (part_of[id] >= 0) {
+                auto &pv = parts[part_of[id]];
+                for (int r = r0; r < r1; r++) ns.nets[r] = std::move(pv[r - r0]);
+            } else {
+                RNet &r = ns.nets[r0];
                 r.orig = id;
+                r.pins.reserve(d.sel_off[id + 1] - d.sel_off[id]);
                 for (int64_t i = d.sel_off[id]; i < d.sel_off[id + 1]; i++) {
                     int p = d.sel[i];
                     r.pins.push_back(p >= XY ? p - XY : p);
                 }
-                tmp[id].push_back(std::move(r));
-                ns.unfinished[id] = 1;
-                continue;
             }
-            split_net(d, ns, id, tmp[id]);
-            ns.unfinished[id] = (int)tmp[id].size();
+            for (int r = r0; r < r1; r++) {
+                calc_hpwl(ns, ns.nets[r]);
+                construct_rsmt(d, ns, ns.nets[r]);
+            }
         }
-    });
-    ns.nets.clear();
-    ns.subnets.assign(N, {});
-    for (int id = 0; id < N; id++)
-        for (auto &r : tmp[id]) {
-            ns.subnets[id].push_back((int)ns.nets.size());
-            ns.nets.push_back(std::move(r));
-        }
-    const int R = (int)ns.nets.size();
-    parallel_for(R, threads, [&](int b, int e) {
-        for (int i = b; i < e; i++) calc_hpwl(ns, ns.nets[i]);
     });
     ns.pin_sum.assign(R + 1, 0);
     for (int i = 0; i < R; i++) ns.pin_sum[i + 1] = ns.pin_sum[i] + (int64_t)ns.nets[i].pins.size();
-    // trees, segments and points of every routing net (Lshape_route.hpp:159-163)
-    parallel_for(R, threads, [&](int b, int e) {
-        for (int i = b; i < e; i++) construct_rsmt(d, ns, ns.nets[i], false);
-    });
 }
 
 void flatten_tree(const RNet &n, int *nodes, int *par) {

@@ -223,7 +223,9 @@ void Router::open(const char *cap, const char *net) {
         ~Joiner() { if (t.joinable()) t.join(); }
     } joiner{ctx_init};
     read_design(d, cap, net, threads);
+    const double t_read = now_s();
     build_netset(d, ns, threads);
+    const double t_nets = now_s();
     // trees in DFS preorder, net-id order, and the phase-1 route record layout
     const int R = (int)ns.nets.size();
     tree_off.assign(R + 1, 0);
@@ -268,8 +270,9 @@ void Router::open(const char *cap, const char *net) {
     order1.resize(R);
     std::iota(order1.begin(), order1.end(), 0);
     std::sort(order1.begin(), order1.end(), [&](int l, int r) { return ns.nets[l].hpwl > ns.nets[r].hpwl; });
-    if (verbose) std::fprintf(stderr, "[igr] read+trees %.2fs: %d nets, %d routing nets\n", now_s() - t0,
-                              d.num_nets(), R);
+    if (verbose)
+        std::fprintf(stderr, "[igr] read+trees %.2fs (read %.3f, pins+trees %.3f, layout %.3f): %d nets, %d routing nets\n",
+                     now_s() - t0, t_read - t0, t_nets - t_read, now_s() - t_nets, d.num_nets(), R);
 }
 
 // Device state is created and the inputs uploaded on the first run, so that
@@ -292,6 +295,7 @@ void Router::ensure_device() {
     for (int l = 0; l < L; l++) sc[l] = d.short_cost[l + 1];
     go.create(L, X, Y, d.layer_dir[1], d.x_edge_len.data(), d.y_edge_len.data(), d.unit_wire, d.unit_via, sc.data(),
               capr.data(), s);
+    const double t_grid = now_s();
     // resident inputs
     d_tree_off.upload(tree_off, s);
     d_tree_nodes.upload(tree_nodes, s);
@@ -304,16 +308,25 @@ void Router::ensure_device() {
     d_route_cap1.upload(route_cap1, s);
     d_route_off.alloc(route_off1.size());
     d_route_cap.alloc(route_cap1.size());
+    const double t_trees = now_s();
     ShapeSet sh;
     const int R = (int)ns.nets.size();
     sh.pt_off.assign(R + 1, 0);
     sh.h_off.assign(R + 1, 0);
     sh.v_off.assign(R + 1, 0);
+    parallel_for(R, threads, [&](int b, int e) {
+        for (int i = b; i < e; i++) {
+            int np = 0, nh = 0, nv = 0;
+            for_each_shape(ns.nets[i], X, Y, [&](int) { np++; }, [&](int, int) { nh++; }, [&](int, int) { nv++; });
+            sh.pt_off[i + 1] = np;
+            sh.h_off[i + 1] = nh;
+            sh.v_off[i + 1] = nv;
+        }
+    });
     for (int i = 0; i < R; i++) {
-        const RNet &r = ns.nets[i];
-        sh.pt_off[i + 1] = sh.pt_off[i] + (int)r.points.size();
-        sh.h_off[i + 1] = sh.h_off[i] + (int)r.hseg.size();
-        sh.v_off[i + 1] = sh.v_off[i] + (int)r.vseg.size();
+        sh.pt_off[i + 1] += sh.pt_off[i];
+        sh.h_off[i + 1] += sh.h_off[i];
+        sh.v_off[i + 1] += sh.v_off[i];
     }
     sh.pts.resize(sh.pt_off[R]);
     sh.pt_net.resize(sh.pt_off[R]);
@@ -321,22 +334,16 @@ void Router::ensure_device() {
     sh.vseg.resize(2 * (size_t)sh.v_off[R]);
     parallel_for(R, threads, [&](int b, int e) {
         for (int i = b; i < e; i++) {
-            const RNet &r = ns.nets[i];
-            for (size_t j = 0; j < r.points.size(); j++) {
-                sh.pts[sh.pt_off[i] + j] = r.points[j];
-                sh.pt_net[sh.pt_off[i] + j] = i;
-            }
-            for (size_t j = 0; j < r.hseg.size(); j++) {
-                sh.hseg[2 * (sh.h_off[i] + j)] = r.hseg[j].first;
-                sh.hseg[2 * (sh.h_off[i] + j) + 1] = r.hseg[j].second;
-            }
-            for (size_t j = 0; j < r.vseg.size(); j++) {
-                sh.vseg[2 * (sh.v_off[i] + j)] = r.vseg[j].first;
-                sh.vseg[2 * (sh.v_off[i] + j) + 1] = r.vseg[j].second;
-            }
+            int *pt = sh.pts.data() + sh.pt_off[i], *pn = sh.pt_net.data() + sh.pt_off[i];
+            int *hs = sh.hseg.data() + 2 * (size_t)sh.h_off[i], *vs = sh.vseg.data() + 2 * (size_t)sh.v_off[i];
+            for_each_shape(
+                ns.nets[i], X, Y, [&](int q) { *pt++ = q; *pn++ = i; },
+                [&](int a, int c) { *hs++ = a; *hs++ = c; }, [&](int a, int c) { *vs++ = a; *vs++ = c; });
         }
     });
+    const double t_shapes = now_s();
     d_shapes1.upload(sh, X, Y, 15, s, threads);  // phase 1 samples every 15th segment cell (database_cuda.hpp:439)
+    const double t_claims = now_s();
     // phase-1 colouring ranks: the reversed routing priority (the last rank wins conflicts)
     std::vector<int> perm1(order1.rbegin(), order1.rend());
     d_perm1.upload(perm1, s);
@@ -348,7 +355,10 @@ void Router::ensure_device() {
                 8 * (int64_t)tree_nodes.size() + 8 * (int64_t)scratch_off.size() + 12 * (int64_t)R +
                 d_shapes1.bytes + 8 * (int64_t)R;
     cuda_check(cudaStreamSynchronize(s), "inputs");
-    if (verbose) std::fprintf(stderr, "[igr] device setup %.3fs\n", now_s() - t0);
+    if (verbose)
+        std::fprintf(stderr, "[igr] device setup %.3fs (grid %.3f, trees %.3f, shapes %.3f, claims+upload %.3f, rest %.3f)\n",
+                     now_s() - t0, t_grid - t0, t_trees - t_grid, t_shapes - t_trees, t_claims - t_shapes,
+                     now_s() - t_claims);
 }
 
 // Grows the route buffer to `need` ints, keeping the records already written.
@@ -961,9 +971,10 @@ bool Router::rrr_pass(int iter) {
         const RNet &r = ns.nets[id];
         for (int q : dag[id].points) { sh.pts.push_back(q); sh.pt_net.push_back((int)sh.pt_off.size() - 1); }
         sh.pt_off.push_back((int)sh.pts.size());
-        for (auto &sg : r.hseg) { sh.hseg.push_back(sg.first); sh.hseg.push_back(sg.second); }
+        for_each_shape(
+            r, X, Y, [](int) {}, [&](int a, int c) { sh.hseg.push_back(a); sh.hseg.push_back(c); },
+            [&](int a, int c) { sh.vseg.push_back(a); sh.vseg.push_back(c); });
         sh.h_off.push_back((int)(sh.hseg.size() / 2));
-        for (auto &sg : r.vseg) { sh.vseg.push_back(sg.first); sh.vseg.push_back(sg.second); }
         sh.v_off.push_back((int)(sh.vseg.size() / 2));
     }
     ShapeDev shd;

@@ -22,7 +22,8 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdlib>
-#include <map>
+#include <climits>
+#include <stdexcept>
 #include <numeric>
 #include <unordered_map>
 #include <utility>
@@ -59,73 +60,124 @@ inline void build(const std::vector<int> &xin, const std::vector<int> &yin, Tree
         for (int i = 0; i < 3; i++) if (i != c) t.edges.push_back({std::min(i, c), std::max(i, c)});
         return;
     }
-    // ---- candidate edges
-    struct E { int w, a, b; };
-    std::vector<E> cand;
+    // ---- minimum spanning tree under the edge order (length, lo, hi).  The
+    // order is strict, so the tree is unique: Prim over all pairs up to 64
+    // points; above, Kruskal over the sweep candidates (which contain it).
+    std::vector<std::vector<int>> adj(P);
     if (P <= 64) {
-        cand.reserve((size_t)P * (P - 1) / 2);
-        for (int i = 0; i < P; i++)
-            for (int j = i + 1; j < P; j++) cand.push_back({dist(i, j), i, j});
+        // Prim: key of the best edge from the tree to each outside point
+        long long key[64];
+        int from[64];
+        bool in[64];
+        auto ek = [&](int a, int b) {  // (length, lo, hi) as one integer: lengths < 2^31, ids < 64
+            const int lo = a < b ? a : b, hi = a < b ? b : a;
+            return ((long long)dist(a, b) << 12) | (lo << 6) | hi;
+        };
+        for (int i = 0; i < P; i++) { key[i] = ek(0, i); from[i] = 0; in[i] = false; }
+        in[0] = true;
+        for (int k = 1; k < P; k++) {
+            int best = -1;
+            for (int i = 0; i < P; i++)
+                if (!in[i] && (best < 0 || key[i] < key[best])) best = i;
+            in[best] = true;
+            adj[from[best]].push_back(best);
+            adj[best].push_back(from[best]);
+            for (int i = 0; i < P; i++)
+                if (!in[i]) {
+                    const long long q = ek(best, i);
+                    if (q < key[i]) { key[i] = q; from[i] = best; }
+                }
+        }
     } else {
+        // candidate edges as keys length << 32 | lo << 16 | hi (points < 2^16)
+        // or, above that, as (length, lo, hi) triples; both sort in the same order
+        const bool packed = P < (1 << 16);
+        struct E { int w, a, b; };
+        std::vector<E> cand;
+        std::vector<uint64_t> ckey;
+        auto add = [&](int i, int j) {
+            const int lo = std::min(i, j), hi = std::max(i, j), w = dist(i, j);
+            if (packed) ckey.push_back((uint64_t)(uint32_t)w << 32 | (uint64_t)lo << 16 | (uint64_t)hi);
+            else cand.push_back({w, lo, hi});
+        };
+        (packed ? (void)ckey.reserve((size_t)8 * P) : cand.reserve((size_t)8 * P));
         std::vector<int> px(t.x), py(t.y), id(P);
+        std::vector<int64_t> order(P);
+        std::vector<std::pair<int, int>> sweep;  // (-y, point), ascending
+        sweep.reserve(P);
         for (int k = 0; k < 4; k++) {
-            std::iota(id.begin(), id.end(), 0);
-            std::sort(id.begin(), id.end(), [&](int a, int b) {
-                int64_t sa = (int64_t)px[a] + py[a], sb = (int64_t)px[b] + py[b];
-                return sa != sb ? sa < sb : a < b;
-            });
-            std::map<int, int> sweep;  // key -y -> point
+            // points by x + y, then by index; sums fit 33 bits, indices 31
+            for (int i = 0; i < P; i++) order[i] = (((int64_t)px[i] + py[i]) << 31) + i;
+            std::sort(order.begin(), order.end());
+            for (int i = 0; i < P; i++) id[i] = (int)(order[i] & 0x7fffffff);
+            sweep.clear();
             for (int i : id) {
-                for (auto it = sweep.lower_bound(-py[i]); it != sweep.end();) {
+                auto lo = std::lower_bound(sweep.begin(), sweep.end(), std::make_pair(-py[i], INT32_MIN));
+                auto it = lo;
+                for (; it != sweep.end(); ++it) {
                     int j = it->second;
                     int dx = px[i] - px[j], dy = py[i] - py[j];
                     if (dy > dx) break;
-                    cand.push_back({dist(i, j), std::min(i, j), std::max(i, j)});
-                    it = sweep.erase(it);
+                    add(i, j);
                 }
-                sweep[-py[i]] = i;
+                // the keys from lo on are >= -py[i]; an equal key was erased above
+                // (dy == 0 <= dx for a point swept earlier), so i goes in at lo
+                if (it != lo) {
+                    *lo = {-py[i], i};
+                    sweep.erase(lo + 1, it);
+                } else {
+                    sweep.insert(lo, {-py[i], i});
+                }
             }
             for (int i = 0; i < P; i++) {
                 if (k & 1) px[i] = -px[i];
                 else std::swap(px[i], py[i]);
             }
         }
-    }
-    std::sort(cand.begin(), cand.end(), [](const E &l, const E &r) {
-        if (l.w != r.w) return l.w < r.w;
-        if (l.a != r.a) return l.a < r.a;
-        return l.b < r.b;
-    });
-    std::vector<int> uf(P);
-    std::iota(uf.begin(), uf.end(), 0);
-    auto find = [&](int v) {
-        while (uf[v] != v) v = uf[v] = uf[uf[v]];
-        return v;
-    };
-    std::vector<std::vector<int>> adj(P);
-    int used = 0;
-    for (auto &e : cand) {
-        int ra = find(e.a), rb = find(e.b);
-        if (ra == rb) continue;
-        uf[ra] = rb;
-        adj[e.a].push_back(e.b);
-        adj[e.b].push_back(e.a);
-        if (++used == P - 1) break;
+        if (packed) {
+            std::sort(ckey.begin(), ckey.end());
+            cand.resize(ckey.size());
+            for (size_t q = 0; q < ckey.size(); q++)
+                cand[q] = {(int)(ckey[q] >> 32), (int)(ckey[q] >> 16 & 0xffff), (int)(ckey[q] & 0xffff)};
+        } else {
+            std::sort(cand.begin(), cand.end(), [](const E &l, const E &r) {
+                if (l.w != r.w) return l.w < r.w;
+                if (l.a != r.a) return l.a < r.a;
+                return l.b < r.b;
+            });
+        }
+        std::vector<int> uf(P);
+        std::iota(uf.begin(), uf.end(), 0);
+        auto find = [&](int v) {
+            while (uf[v] != v) v = uf[v] = uf[uf[v]];
+            return v;
+        };
+        int used = 0;
+        for (auto &e : cand) {
+            int ra = find(e.a), rb = find(e.b);
+            if (ra == rb) continue;
+            uf[ra] = rb;
+            adj[e.a].push_back(e.b);
+            adj[e.b].push_back(e.a);
+            if (++used == P - 1) break;
+        }
     }
     // ---- Steinerisation
     std::unordered_map<int64_t, int> at;
+    at.reserve((size_t)2 * P);
     auto key = [](int x, int y) { return ((int64_t)x << 32) ^ (uint32_t)y; };
     for (int i = 0; i < P; i++) at[key(t.x[i], t.y[i])] = i;
     auto drop = [&](int u, int v) {
         auto &a = adj[u];
         a.erase(std::find(a.begin(), a.end(), v));
     };
+    std::vector<int> sn;
     for (int pass = 0; pass < 4; pass++) {
         bool changed = false;
         for (int v = 0; v < (int)adj.size(); v++) {
             auto &nb = adj[v];
             if (nb.size() < 2) continue;
-            std::vector<int> sn(nb);
+            sn.assign(nb.begin(), nb.end());
             std::sort(sn.begin(), sn.end());
             int best_gain = 0, ba = -1, bb = -1, bx = 0, by = 0;
             for (size_t i = 0; i < sn.size(); i++)
@@ -214,17 +266,26 @@ inline void to_branches(const std::vector<int> &xin, const std::vector<int> &yin
             if (par[w] < 0) { par[w] = order[i]; order.push_back(w); }
     // branch index of each tree node: first input point at that position, or a Steiner slot
     std::vector<int> bidx(V, -1);
-    std::map<std::pair<int, int>, int> pos2node;
-    for (int v = 0; v < t.npins; v++) pos2node[{t.x[v], t.y[v]}] = v;
+    // tree node of each input point: the pins come first in (x, y) order, distinct
+    auto node_at = [&](int x, int y) {
+        int lo = 0, hi = t.npins;
+        while (lo < hi) {
+            const int m = (lo + hi) >> 1;
+            if (t.x[m] < x || (t.x[m] == x && t.y[m] < y)) lo = m + 1;
+            else hi = m;
+        }
+        if (lo == t.npins || t.x[lo] != x || t.y[lo] != y) throw std::out_of_range("point not in the tree");
+        return lo;
+    };
     for (int i = 0; i < d; i++) {
-        int v = pos2node.at({xin[i], yin[i]});
+        int v = node_at(xin[i], yin[i]);
         if (bidx[v] < 0) bidx[v] = i;
     }
     int slot = d;
     for (int v = t.npins; v < V; v++) bidx[v] = slot++;
     for (int v = 0; v < V; v++) br[bidx[v]] = Branch{t.x[v], t.y[v], bidx[par[v]]};
     for (int i = 0; i < d; i++) {
-        int v = pos2node.at({xin[i], yin[i]});
+        int v = node_at(xin[i], yin[i]);
         if (bidx[v] != i) br[i] = Branch{xin[i], yin[i], bidx[v]};  // duplicate input point
     }
     for (int s = slot; s < 2 * d - 2; s++) br[s] = Branch{t.x[0], t.y[0], bidx[0]};

@@ -135,3 +135,99 @@ def test_generator_is_deterministic(tmp_path):
     assert open(a[1], "rb").read() == open(b[1], "rb").read()
     ig.generate(0, 8, 0.05, *b)
     assert open(a[1], "rb").read() != open(b[1], "rb").read()
+
+
+def _scan_cap(text: str):
+    """Sequential restatement of the .cap scanner (src/database.hpp:247-330):
+    integers and reals are runs starting at a digit (reals also take dots),
+    anything else between them is skipped; names run to the next blank."""
+    p = 0
+    n = len(text)
+
+    def num(real):
+        nonlocal p
+        while p < n and not text[p].isdigit():
+            p += 1
+        if p >= n:
+            raise ValueError("end of input")
+        ans, scale = 0.0, 0.0
+        while p < n and (text[p].isdigit() or (real and text[p] == ".")):
+            if text[p] == ".":
+                scale = 1.0
+            else:
+                scale *= 10
+                ans = ans * 10 + int(text[p])
+            p += 1
+        return (ans if scale == 0 else ans / scale) if real else int(ans)
+
+    def token():
+        nonlocal p
+        while p < n and text[p] in " \n":
+            p += 1
+        b = p
+        while p < n and text[p] not in " \n":
+            p += 1
+        return text[b:p]
+
+    L, X, Y = num(False), num(False), num(False)
+    for _ in range(2 + L):
+        num(True)
+    for _ in range(X - 1 + Y - 1):
+        num(False)
+    cap = np.zeros((L, X, Y), np.float32)
+    for lay in range(L):
+        if token() != f"metal{lay + 1}":
+            raise ValueError("layer name")
+        num(False)
+        num(True)
+        for y in range(Y):
+            for x in range(X):
+                cap[lay, x, y] = np.float32(num(True))
+    return cap
+
+
+def _cap_text(r, X, Y, style):
+    vals = r.integers(0, 40, size=(10, Y, X)) / r.choice([1, 2, 4, 8], size=(10, Y, X))
+    out = [f"10 {X} {Y}\n1 4\n" + " ".join("0.5" for _ in range(10)) + "\n"]
+    out.append(" ".join(str(int(v)) for v in r.integers(1, 4, X - 1)) + "\n")
+    out.append(" ".join(str(int(v)) for v in r.integers(1, 4, Y - 1)) + "\n")
+    for lay in range(10):
+        out.append(f"metal{lay + 1} {lay % 2} 1.5\n")
+        rows = []
+        for y in range(Y):
+            items = [f"{v:g}" if v != int(v) else str(int(v)) for v in vals[lay, y]]
+            if style == 1:
+                items = [("." + i[2:]) if i.startswith("0.") else i for i in items]  # ".5" reads as 5
+                rows.append("  ".join(items) + " ")
+            elif style == 2:
+                rows.append(",\t".join(items))
+            else:
+                rows.append(" ".join(items))
+        out.append((" " if style == 1 else "\n").join(rows) + "\n")
+    return "".join(out)
+
+
+@pytest.mark.parametrize("style", [0, 1, 2])
+def test_capacity_reader_matches_the_sequential_scanner(tmp_path, style):
+    """The capacity values are parsed in pieces on several threads; the result is
+    the sequential scanner's for any spacing, separators and number forms."""
+    r = np.random.default_rng(11 + style)
+    X, Y = 97, 131
+    text = _cap_text(r, X, Y, style)
+    cap, net = tmp_path / "t.cap", tmp_path / "t.net"
+    cap.write_text(text)
+    net.write_text("n0\n(\n[(1, 0, 0)]\n[(1, 3, 4)]\n)\n")
+    ref = _scan_cap(text)
+    g = ig.Router(str(cap), str(net)).grid()
+    assert np.array_equal(g["cap"].reshape(9, X, Y), ref[1:])
+
+
+def test_capacity_reader_rejects_junk_before_a_layer_name(tmp_path):
+    r = np.random.default_rng(5)
+    text = _cap_text(r, 40, 30, 0).replace("\nmetal4 ", "\nx metal4 ", 1)
+    cap, net = tmp_path / "t.cap", tmp_path / "t.net"
+    cap.write_text(text)
+    net.write_text("n0\n(\n[(1, 0, 0)]\n[(1, 3, 4)]\n)\n")
+    with pytest.raises(ig.IgrError) as e:
+        ig.Router(str(cap), str(net))
+    assert e.value.code == -3
