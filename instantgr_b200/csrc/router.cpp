@@ -309,41 +309,33 @@ void Router::ensure_device() {
     d_route_off.alloc(route_off1.size());
     d_route_cap.alloc(route_cap1.size());
     const double t_trees = now_s();
-    ShapeSet sh;
     const int R = (int)ns.nets.size();
-    sh.pt_off.assign(R + 1, 0);
-    sh.h_off.assign(R + 1, 0);
-    sh.v_off.assign(R + 1, 0);
-    parallel_for(R, threads, [&](int b, int e) {
-        for (int i = b; i < e; i++) {
-            int np = 0, nh = 0, nv = 0;
-            for_each_shape(ns.nets[i], X, Y, [&](int) { np++; }, [&](int, int) { nh++; }, [&](int, int) { nv++; });
-            sh.pt_off[i + 1] = np;
-            sh.h_off[i + 1] = nh;
-            sh.v_off[i + 1] = nv;
-        }
-    });
-    for (int i = 0; i < R; i++) {
-        sh.pt_off[i + 1] += sh.pt_off[i];
-        sh.h_off[i + 1] += sh.h_off[i];
-        sh.v_off[i + 1] += sh.v_off[i];
+    {
+        // phase-1 conflict shapes and claim lists from the resident trees; phase 1
+        // samples every 15th segment cell (database_cuda.hpp:439)
+        ShapeDev &sd = d_shapes1;
+        sd.pt_off.alloc(R + 1);
+        sd.claim_off.alloc(R + 1);
+        DevBuf<long long> tot;
+        tot.alloc(2);
+        launch_shape_count(d_tree_off.p, d_tree_nodes.p, d_tree_par.p, R, X, Y, 15, sd.pt_off.p, sd.claim_off.p, tot.p,
+                           s);
+        long long h_tot[2] = {0, 0};
+        cuda_check(cudaMemcpyAsync(h_tot, tot.p, sizeof h_tot, cudaMemcpyDeviceToHost, s), "D2H");
+        cuda_check(cudaStreamSynchronize(s), "shape counts");
+        if (h_tot[0] > INT32_MAX || h_tot[1] > INT32_MAX)
+            throw Error(ERR_CAPACITY, "conflict shapes exceed 32-bit offsets");
+        sd.pts.alloc((size_t)h_tot[0]);
+        sd.claim.alloc((size_t)h_tot[1]);
+        launch_shape_fill(d_tree_off.p, d_tree_nodes.p, d_tree_par.p, R, X, Y, 15, sd.pt_off.p, sd.claim_off.p,
+                          sd.pts.p, sd.claim.p, s);
+        sd.npts = (int)h_tot[0];
+        sd.nshapes = R;
+        sd.sparsity = 15;
+        sd.bytes = 0;
     }
-    sh.pts.resize(sh.pt_off[R]);
-    sh.pt_net.resize(sh.pt_off[R]);
-    sh.hseg.resize(2 * (size_t)sh.h_off[R]);
-    sh.vseg.resize(2 * (size_t)sh.v_off[R]);
-    parallel_for(R, threads, [&](int b, int e) {
-        for (int i = b; i < e; i++) {
-            int *pt = sh.pts.data() + sh.pt_off[i], *pn = sh.pt_net.data() + sh.pt_off[i];
-            int *hs = sh.hseg.data() + 2 * (size_t)sh.h_off[i], *vs = sh.vseg.data() + 2 * (size_t)sh.v_off[i];
-            for_each_shape(
-                ns.nets[i], X, Y, [&](int q) { *pt++ = q; *pn++ = i; },
-                [&](int a, int c) { *hs++ = a; *hs++ = c; }, [&](int a, int c) { *vs++ = a; *vs++ = c; });
-        }
-    });
     const double t_shapes = now_s();
-    d_shapes1.upload(sh, X, Y, 15, s, threads);  // phase 1 samples every 15th segment cell (database_cuda.hpp:439)
-    const double t_claims = now_s();
+    const double t_claims = t_shapes;
     // phase-1 colouring ranks: the reversed routing priority (the last rank wins conflicts)
     std::vector<int> perm1(order1.rbegin(), order1.rend());
     d_perm1.upload(perm1, s);
@@ -352,13 +344,11 @@ void Router::ensure_device() {
     d_all_ids.upload(ids, s);
     // host-to-device bytes of the setup: grid, trees, record layout, conflict shapes, ranks
     setup_h2d = (int64_t)go.g.N * 4 + 4 * (int64_t)(X + Y - 2) + 8 * L + 4 * (int64_t)tree_off.size() +
-                8 * (int64_t)tree_nodes.size() + 8 * (int64_t)scratch_off.size() + 12 * (int64_t)R +
-                d_shapes1.bytes + 8 * (int64_t)R;
+                8 * (int64_t)tree_nodes.size() + 8 * (int64_t)scratch_off.size() + 12 * (int64_t)R + 8 * (int64_t)R;
     cuda_check(cudaStreamSynchronize(s), "inputs");
     if (verbose)
-        std::fprintf(stderr, "[igr] device setup %.3fs (grid %.3f, trees %.3f, shapes %.3f, claims+upload %.3f, rest %.3f)\n",
-                     now_s() - t0, t_grid - t0, t_trees - t_grid, t_shapes - t_trees, t_claims - t_shapes,
-                     now_s() - t_claims);
+        std::fprintf(stderr, "[igr] device setup %.3fs (grid %.3f, trees %.3f, shapes and claims %.3f, rest %.3f)\n",
+                     now_s() - t0, t_grid - t0, t_trees - t_grid, t_shapes - t_trees, now_s() - t_claims);
 }
 
 // Grows the route buffer to `need` ints, keeping the records already written.

@@ -162,7 +162,7 @@ void SeedModel::forward(int T) {
     for (int i = 0; i < kSeedConvs; i++) {
         const bool last = i == kSeedConvs - 1;
         launch_conv_fwd(spec[i], T, in, W[i].p, bias[i].p, last ? y16.p : act[i].p, last ? y32.p : nullptr, err.p, s);
-        in = act[i].p;
+        if (!last) in = act[i].p;
     }
 }
 

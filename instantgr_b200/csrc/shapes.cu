@@ -1,0 +1,150 @@
+// Phase-1 conflict shapes and claim lists of the batch colouring, built on the
+// device from the flattened trees already resident there.
+//
+// The shapes of a routing net (net::construct_rsmt, src/database_cuda.hpp:
+// 746-820) are its tree nodes as points and, per tree edge, its segments and
+// end or corner points; the claims (generate_batches_rsmt_gpu,
+// src/database_cuda.hpp:288-434) are the cell, left, right and lower cells of
+// every point and every `sparsity`-th cell of every segment.  They depend only
+// on the set of tree edges, so they are generated here from the (node,
+// parent) pairs of the DFS-ordered trees; the colouring treats points and
+// claims as sets, so the order inside a net is free.  Two passes: counts per
+// net with an exclusive scan (one block), then the fill.
+#include "kcommon.cuh"
+
+namespace igr {
+
+namespace {
+
+constexpr int kScanThreads = 1024;
+
+template <class Pt, class Hs, class Vs>
+__device__ __forceinline__ void net_shapes(const int *nodes, const int *par, int m, int X, int Y, Pt &&point,
+                                           Hs &&hseg, Vs &&vseg) {
+    const int XY = X * Y;
+    for (int i = 0; i < m; i++) {
+        const int p = nodes[i] % XY;
+        point(p / Y, p % Y);
+    }
+    for (int i = 1; i < m; i++) {
+        const int j = par[i];
+        if (j < 0) continue;
+        const int pi = nodes[i] % XY, pj = nodes[j] % XY;
+        const int xi = pi / Y, yi = pi % Y, xj = pj / Y, yj = pj % Y;
+        const int mnx = min(xi, xj), mxx = max(xi, xj), mny = min(yi, yj), mxy = max(yi, yj);
+        if (xi != xj && yi != yj) {
+            hseg(mnx, mxx, mny);
+            hseg(mnx, mxx, mxy);
+            vseg(mny, mxy, mnx);
+            vseg(mny, mxy, mxx);
+            point(xi, yj);
+            point(xj, yi);
+        } else if (xi != xj) {
+            hseg(mnx, mxx, mny);
+            point(mnx, mny);
+            point(mxx, mny);
+        } else if (yi != yj) {
+            vseg(mny, mxy, mnx);
+            point(mnx, mny);
+            point(mnx, mxy);
+        }
+    }
+}
+
+// claimed cells of a point: the cell, the one below, left and right (in the grid)
+__device__ __forceinline__ int point_claims(int x, int y, int X, int Y) {
+    return 1 + (y > 0) + (x > 0) + (x + 1 < X);
+}
+
+__global__ void shape_count_kernel(const int *tree_off, const int *tree_nodes, const int *tree_par, int R, int X,
+                                   int Y, int sp, int *pt_cnt, int *claim_cnt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= R) return;
+    const int a = tree_off[i], m = tree_off[i + 1] - a;
+    int np = 0, nc = 0;
+    net_shapes(
+        tree_nodes + a, tree_par + a, m, X, Y,
+        [&](int x, int y) {
+            np++;
+            nc += point_claims(x, y, X, Y);
+        },
+        [&](int lo, int hi, int) { nc += (hi - lo) / sp + 1; }, [&](int lo, int hi, int) { nc += (hi - lo) / sp + 1; });
+    pt_cnt[i + 1] = np;
+    claim_cnt[i + 1] = nc;
+}
+
+// exclusive scan of a[1..n] into a[0..n] (a[0] = 0) in one block; the total
+// goes to *total (64-bit, so that an overflow of the 32-bit offsets is seen)
+__device__ void block_scan(int *a, int n, long long *total) {
+    __shared__ long long part[kScanThreads];
+    const int t = threadIdx.x;
+    const int chunk = (n + kScanThreads - 1) / kScanThreads;
+    const int lo = min(n, t * chunk), hi = min(n, lo + chunk);
+    long long sum = 0;
+    for (int i = lo; i < hi; i++) sum += a[i + 1];
+    part[t] = sum;
+    __syncthreads();
+    for (int d = 1; d < kScanThreads; d <<= 1) {
+        const long long v = t >= d ? part[t - d] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    long long run = part[t] - sum;
+    for (int i = lo; i < hi; i++) {
+        run += a[i + 1];
+        a[i + 1] = (int)run;
+    }
+    if (t == 0) a[0] = 0;
+    if (t == kScanThreads - 1) *total = part[t];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kScanThreads) shape_scan_kernel(int R, int *pt_off, int *claim_off,
+                                                                   long long *totals) {
+    block_scan(pt_off, R, totals);
+    block_scan(claim_off, R, totals + 1);
+}
+
+__global__ void shape_fill_kernel(const int *tree_off, const int *tree_nodes, const int *tree_par, int R, int X,
+                                  int Y, int sp, const int *pt_off, const int *claim_off, int *pts, int *claim) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= R) return;
+    const int a = tree_off[i], m = tree_off[i + 1] - a;
+    int *pt = pts + pt_off[i];
+    int *cl = claim + claim_off[i];
+    net_shapes(
+        tree_nodes + a, tree_par + a, m, X, Y,
+        [&](int x, int y) {
+            *pt++ = x * Y + y;
+            *cl++ = x * Y + y;
+            if (y > 0) *cl++ = x * Y + y - 1;
+            if (x > 0) *cl++ = (x - 1) * Y + y;
+            if (x + 1 < X) *cl++ = (x + 1) * Y + y;
+        },
+        [&](int lo, int hi, int y) {
+            for (int x = lo; x <= hi; x += sp) *cl++ = x * Y + y;
+        },
+        [&](int lo, int hi, int x) {
+            for (int y = lo; y <= hi; y += sp) *cl++ = x * Y + y;
+        });
+}
+
+}  // namespace
+
+void launch_shape_count(const int *tree_off, const int *tree_nodes, const int *tree_par, int R, int X, int Y,
+                        int sparsity, int *pt_off, int *claim_off, long long *totals, cudaStream_t s) {
+    if (R > 0)
+        shape_count_kernel<<<(R + 255) / 256, 256, 0, s>>>(tree_off, tree_nodes, tree_par, R, X, Y, sparsity, pt_off,
+                                                           claim_off);
+    shape_scan_kernel<<<1, kScanThreads, 0, s>>>(R, pt_off, claim_off, totals);
+}
+
+void launch_shape_fill(const int *tree_off, const int *tree_nodes, const int *tree_par, int R, int X, int Y,
+                       int sparsity, const int *pt_off, const int *claim_off, int *pts, int *claim, cudaStream_t s) {
+    if (R > 0)
+        shape_fill_kernel<<<(R + 255) / 256, 256, 0, s>>>(tree_off, tree_nodes, tree_par, R, X, Y, sparsity, pt_off,
+                                                          claim_off, pts, claim);
+}
+
+}  // namespace igr
