@@ -308,7 +308,9 @@ struct Builder {
                         of += ys(std::max(cx, x2), std::max(cy, y2)) - ys(std::min(cx, x2), std::min(cy, y2));
                         road[k - 1] = std::make_pair((float)of, k);
                     }
-                    if (mz - 1 > 0) std::sort(road, road + mz - 1);
+                    // ascending (the entries are distinct or equal as pairs, so any sort agrees)
+                    for (int a = 1; a < mz - 1; a++)
+                        for (int b = a; b > 0 && road[b] < road[b - 1]; b--) std::swap(road[b], road[b - 1]);
                     for (int ii = 0; ii < sel; ii++) {
                         const int k = road[ii].second;
                         int x1, y1, x2, y2;

@@ -13,10 +13,18 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cerrno>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <thread>
+
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <memory>
 
 namespace igr {
 
@@ -364,15 +372,64 @@ void read_net_buffer(Design &d, const char *buf, size_t n) {
     }
 }
 
+namespace {
+
+// read-only view of a whole file: a private mapping, or a copy where mapping fails
+struct FileView {
+    const char *data = nullptr;
+    size_t size = 0;
+    void *map = nullptr;
+    std::vector<char> copy;
+    explicit FileView(const char *path) {
+        const int fd = ::open(path, O_RDONLY);
+        if (fd < 0) throw Error(ERR_IO, std::string("cannot open ") + path);
+        struct stat st;
+        if (::fstat(fd, &st) == 0 && st.st_size > 0) {
+            void *m = ::mmap(nullptr, (size_t)st.st_size, PROT_READ, MAP_PRIVATE | MAP_POPULATE, fd, 0);
+            if (m != MAP_FAILED) {
+                map = m;
+                data = static_cast<const char *>(m);
+                size = (size_t)st.st_size;
+            }
+        }
+        ::close(fd);
+        if (!map) {
+            copy = slurp(path);
+            data = copy.data();
+            size = copy.size() - 1;
+        }
+    }
+    ~FileView() {
+        if (map) ::munmap(map, size);
+    }
+    FileView(const FileView &) = delete;
+    FileView &operator=(const FileView &) = delete;
+};
+
+}  // namespace
+
 void read_design(Design &d, const char *cap_path, const char *net_path, int threads) {
-    {
-        auto b = slurp(cap_path);
-        read_cap_buffer(d, b.data(), b.size() - 1, threads);
+    // the .net file is mapped while the capacities are parsed
+    std::unique_ptr<FileView> net;
+    std::exception_ptr net_err;
+    std::thread loader([&] {
+        try {
+            net.reset(new FileView(net_path));
+        } catch (...) {
+            net_err = std::current_exception();
+        }
+    });
+    try {
+        FileView cap(cap_path);
+        read_cap_buffer(d, cap.data, cap.size, threads);
+    } catch (...) {
+        loader.join();
+        throw;
     }
-    {
-        auto b = slurp(net_path);
-        read_net_buffer(d, b.data(), b.size() - 1);
-    }
+    loader.join();
+    if (net_err) std::rethrow_exception(net_err);
+    read_net_buffer(d, net->data, net->size);
+    net.reset();
     select_pins(d, threads);
 }
 
@@ -390,14 +447,38 @@ inline char *put_int(char *o, int v) {
 
 }  // namespace
 
+namespace {
+
+// writes all of buf at file offset `at`
+bool pwrite_all(int fd, const char *buf, size_t n, off_t at) {
+    while (n > 0) {
+        const ssize_t w = ::pwrite(fd, buf, n, at);
+        if (w < 0) {
+            if (errno == EINTR) continue;
+            return false;
+        }
+        buf += w;
+        n -= (size_t)w;
+        at += w;
+    }
+    return true;
+}
+
+}  // namespace
+
 void write_guides(const Design &d, const NetSet &ns, const RouteSource &rs, const char *path, int threads) {
-    FILE *f = std::fopen(path, "wb");
-    if (!f) throw Error(ERR_IO, std::string("cannot open ") + path + " for writing");
+    const int fd = ::open(path, O_WRONLY | O_CREAT | O_TRUNC, 0666);
+    if (fd < 0) throw Error(ERR_IO, std::string("cannot open ") + path + " for writing");
+    struct Closer {
+        int fd;
+        ~Closer() { if (fd >= 0) ::close(fd); }
+    } closer{fd};
     const int X = d.X, Y = d.Y, XY = X * Y;
     const int N = d.num_nets();
     if (threads <= 0) threads = hw_threads();
-    // Chunks of nets are formatted in parallel into private buffers, then written in order.
-    const int CH = 4096;
+    // Windows of chunks of nets: the chunks of a window are formatted in
+    // parallel into private buffers, then written in parallel at their offsets.
+    const int CH = 2048;
     int nch = (N + CH - 1) / CH;
     auto fmt = [&](int c, std::vector<char> &out) {
         out.clear();
@@ -428,19 +509,27 @@ void write_guides(const Design &d, const NetSet &ns, const RouteSource &rs, cons
             out.push_back(')'); out.push_back('\n');
         }
     };
-    std::vector<std::vector<char>> bufs(std::max(1, threads));
-    for (int c0 = 0; c0 < nch; c0 += threads) {
-        int k = std::min(threads, nch - c0);
-        parallel_for(k, k, [&](int b, int e) {
+    const int W = 8 * std::max(1, threads);
+    std::vector<std::vector<char>> bufs(W);
+    std::vector<off_t> at(W + 1);
+    off_t pos = 0;
+    for (int c0 = 0; c0 < nch; c0 += W) {
+        const int k = std::min(W, nch - c0);
+        parallel_for(k, threads, [&](int b, int e) {
             for (int i = b; i < e; i++) fmt(c0 + i, bufs[i]);
         });
-        for (int i = 0; i < k; i++)
-            if (!bufs[i].empty() && std::fwrite(bufs[i].data(), 1, bufs[i].size(), f) != bufs[i].size()) {
-                std::fclose(f);
-                throw Error(ERR_IO, "write failed");
-            }
+        at[0] = pos;
+        for (int i = 0; i < k; i++) at[i + 1] = at[i] + (off_t)bufs[i].size();
+        std::atomic<bool> ok{true};
+        parallel_for(k, threads, [&](int b, int e) {
+            for (int i = b; i < e; i++)
+                if (!pwrite_all(fd, bufs[i].data(), bufs[i].size(), at[i])) ok = false;
+        });
+        if (!ok) throw Error(ERR_IO, std::string("write failed on ") + path);
+        pos = at[k];
     }
-    std::fclose(f);
+    closer.fd = -1;
+    if (::close(fd) != 0) throw Error(ERR_IO, std::string("write failed on ") + path);
 }
 
 }  // namespace igr

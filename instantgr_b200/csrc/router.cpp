@@ -92,6 +92,34 @@ void dev_trim() {
     }
 }
 
+namespace {
+std::mutex g_pinned_mu;
+std::map<size_t, std::vector<void *>> g_pinned;  // block bytes -> free page-locked blocks
+}  // namespace
+
+void *pinned_alloc(size_t bytes) {
+    const size_t b = block_bytes(bytes);
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_mu);
+        auto it = g_pinned.lower_bound(b);
+        if (it != g_pinned.end() && it->first <= 2 * b && !it->second.empty()) {
+            void *p = it->second.back();
+            it->second.pop_back();
+            if (it->second.empty()) g_pinned.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    cuda_check(cudaMallocHost(&p, b), "cudaMallocHost");
+    return p;
+}
+
+void pinned_free(void *p, size_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    g_pinned[block_bytes(bytes)].push_back(p);
+}
+
 // ------------------------------------------------------------------ grid
 void GridOwner::create(int L, int X, int Y, int DIR, const int *xl, const int *yl, double unit_wire,
                        double unit_via, const double *sc, const float *cap_ref, cudaStream_t s) {
@@ -232,14 +260,31 @@ void Router::open(const char *cap, const char *net) {
     for (int i = 0; i < R; i++) tree_off[i + 1] = tree_off[i] + (int)ns.nets[i].tnode.size();
     tree_nodes.resize(tree_off[R]);
     tree_par.resize(tree_off[R]);
+    // algorithmic bytes of one phase-1 tree DP pass: per node the 8 via-column
+    // costs (f32); per straight edge 9 layers x 2 presum values (f64); per bent
+    // edge 18 legs x 2 presum values and the two corner via columns (9 x f32 each)
+    std::vector<int64_t> net_bytes(R);
     parallel_for(R, threads, [&](int b, int e) {
-        for (int i = b; i < e; i++) flatten_tree(ns.nets[i], tree_nodes.data() + tree_off[i], tree_par.data() + tree_off[i]);
+        for (int i = b; i < e; i++) {
+            const int a = tree_off[i], m = tree_off[i + 1] - a;
+            flatten_tree(ns.nets[i], tree_nodes.data() + a, tree_par.data() + a);
+            int64_t nb = 32 * (int64_t)m;
+            for (int j = 1; j < m; j++) {
+                const int p = tree_par[a + j];
+                if (p < 0 || p >= j) continue;
+                const int v = tree_nodes[a + j], pv = tree_nodes[a + p];
+                const int x = v / ns.Y % ns.X, y = v % ns.Y, px = pv / ns.Y % ns.X, py = pv % ns.Y;
+                nb += (x == px || y == py) ? 144 : 360;
+            }
+            net_bytes[i] = nb;
+        }
     });
     route_off.assign(R, 0);
     route_cap.assign(R, 0);
     route_end1 = 0;
     scratch_off.assign(R, -1);
     scratch_nodes = 0;
+    int64_t dpb = 0;
     for (int i = 0; i < R; i++) {
         const auto &n = ns.nets[i];
         route_cap[i] = (int)std::max<int64_t>(12 * (int64_t)n.pins.size(), 8 * (int64_t)n.tnode.size() + 1);
@@ -247,24 +292,11 @@ void Router::open(const char *cap, const char *net) {
         route_end1 += route_cap[i];
         const int cnt = tree_off[i + 1] - tree_off[i];
         if (cnt > kPatternNodeTile) { scratch_off[i] = scratch_nodes; scratch_nodes += cnt; }
+        dpb += net_bytes[i];
     }
     route_off1 = route_off;
     route_cap1 = route_cap;
-    // algorithmic bytes of one phase-1 tree DP pass: per node the 8 via-column
-    // costs (f32); per straight edge 9 layers x 2 presum values (f64); per bent
-    // edge 18 legs x 2 presum values and the two corner via columns (9 x f32 each)
-    dp_bytes = 0;
-    for (int i = 0; i < R; i++) {
-        const int a = tree_off[i], m = tree_off[i + 1] - a;
-        dp_bytes += 32.0 * m;
-        for (int j = 1; j < m; j++) {
-            const int p = tree_par[a + j];
-            if (p < 0 || p >= j) continue;
-            const int v = tree_nodes[a + j], pv = tree_nodes[a + p];
-            const int x = v / ns.Y % ns.X, y = v % ns.Y, px = pv / ns.Y % ns.X, py = pv % ns.Y;
-            dp_bytes += (x == px || y == py) ? 144.0 : 360.0;
-        }
-    }
+    dp_bytes = (double)dpb;
     // phase-1 routing priority: HPWL, largest first (Lshape_route.hpp:170-172),
     // with the reference's (unstable) std::sort and comparator
     order1.resize(R);
@@ -537,9 +569,9 @@ void Router::run_once(bool seeded) {
 
 void Router::fetch_routes() {
     if (h_routes_valid) return;
-    h_routes.resize(route_end);
+    h_routes.alloc((size_t)route_end);
     if (route_end)
-        cuda_check(cudaMemcpyAsync(h_routes.data(), routes.p, route_end * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
+        cuda_check(cudaMemcpyAsync(h_routes.p, routes.p, route_end * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
     st.d2h_bytes += route_end * 4;
     h_routes_valid = true;
@@ -1141,7 +1173,7 @@ void Router::write(const char *out) {
     fetch_routes();
     const double t1 = now_s();
     RouteSource rs;
-    rs.routes_of = [&](int net) -> const int * { return h_routes.empty() ? nullptr : route_of(net); };
+    rs.routes_of = [&](int net) -> const int * { return route_end == 0 ? nullptr : route_of(net); };
     write_guides(d, ns, rs, out, threads);
     if (verbose) std::fprintf(stderr, "[igr] routes to host %.3fs, guides written %.3fs\n", t1 - t0, now_s() - t1);
 }

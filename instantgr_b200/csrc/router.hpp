@@ -21,6 +21,33 @@ void *dev_alloc(size_t bytes);
 void dev_free(void *p, size_t bytes);
 // returns every cached block of the current device to the driver
 void dev_trim();
+// The same for page-locked host memory (cudaMallocHost), used for the copies
+// of results to the host.
+void *pinned_alloc(size_t bytes);
+void pinned_free(void *p, size_t bytes);
+
+template <typename T>
+struct PinnedBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf &) = delete;
+    PinnedBuf &operator=(const PinnedBuf &) = delete;
+    ~PinnedBuf() { release(); }
+    void release() {
+        if (p) pinned_free(p, n * sizeof(T));
+        p = nullptr;
+        n = 0;
+    }
+    // grow-only
+    void alloc(size_t count) {
+        if (count <= n && p) return;
+        release();
+        if (count == 0) count = 1;
+        p = static_cast<T *>(pinned_alloc(count * sizeof(T)));
+        n = count;
+    }
+};
 
 template <typename T>
 struct DevBuf {
@@ -152,7 +179,7 @@ struct Router {
     DevBuf<int> routes;
     DevBuf<int64_t> d_route_off, d_old_off;
     DevBuf<int> d_route_cap;
-    std::vector<int> h_routes;  // host copy, made on demand
+    PinnedBuf<int> h_routes;    // host copy of the route records, made on demand
     bool h_routes_valid = false;
     // ---- per-run device buffers (grow-only)
     DevBuf<int4> d_hdr;
@@ -224,7 +251,7 @@ struct Router {
     void run();
     void write(const char *out);
     void fetch_routes();
-    const int *route_of(int net) const { return h_routes.data() + route_off[net]; }
+    const int *route_of(int net) const { return h_routes.p + route_off[net]; }
     void ensure_device();
     void color_nets(const std::vector<int> &order, const ShapeDev &shapes, int sparsity,
                     std::vector<std::vector<int>> &batches);
