@@ -436,13 +436,29 @@ void read_design(Design &d, const char *cap_path, const char *net_path, int thre
 // ------------------------------------------------------------------ writer
 namespace {
 
+// decimal digits of a non-negative value, two at a time
 inline char *put_int(char *o, int v) {
+    static const char kPairs[] =
+        "00010203040506070809101112131415161718192021222324252627282930313233343536373839"
+        "40414243444546474849505152535455565758596061626364656667686970717273747576777879"
+        "8081828384858687888990919293949596979899";
     char t[12];
-    int k = 0;
-    if (v == 0) { *o++ = '0'; return o; }
-    while (v) t[k++] = (char)('0' + v % 10), v /= 10;
-    while (k) *o++ = t[--k];
-    return o;
+    char *e = t + sizeof t, *p = e;
+    unsigned u = (unsigned)v;
+    while (u >= 100) {
+        const unsigned r = u % 100;
+        u /= 100;
+        p -= 2;
+        std::memcpy(p, kPairs + 2 * r, 2);
+    }
+    if (u >= 10) {
+        p -= 2;
+        std::memcpy(p, kPairs + 2 * u, 2);
+    } else {
+        *--p = (char)('0' + u);
+    }
+    std::memcpy(o, p, (size_t)(e - p));
+    return o + (e - p);
 }
 
 }  // namespace
@@ -480,37 +496,57 @@ void write_guides(const Design &d, const NetSet &ns, const RouteSource &rs, cons
     // parallel into private buffers, then written in parallel at their offsets.
     const int CH = 2048;
     int nch = (N + CH - 1) / CH;
-    auto fmt = [&](int c, std::vector<char> &out) {
-        out.clear();
-        auto seg = [&](int p0, int p1, std::vector<char> &o) {
+    // a line of six values of at most 10 digits
+    constexpr size_t kSegBytes = 6 * 11;
+    struct Buf {
+        std::unique_ptr<char[]> p;
+        size_t cap = 0, size = 0;
+    };
+    auto fmt = [&](int c, Buf &out) {
+        const int n0 = c * CH, n1 = std::min(N, (c + 1) * CH);
+        // bytes of the chunk at most, so that the lines go straight into the buffer
+        size_t ub = 0;
+        for (int n = n0; n < n1; n++) {
+            size_t segs = (size_t)(d.sel_off[n + 1] - d.sel_off[n]) + (size_t)(d.extra_off[n + 1] - d.extra_off[n]) / 2;
+            if (n + 1 < (int)ns.sub_off.size())
+                for (int s = ns.sub_off[n]; s < ns.sub_off[n + 1]; s++)
+                    if (const int *r = rs.routes_of(s)) segs += (size_t)(r[0] > 1 ? r[0] / 2 : 0);
+            ub += (size_t)(d.name_off[n + 1] - d.name_off[n]) + 5 + segs * kSegBytes;
+        }
+        if (out.cap < ub) {
+            out.p.reset(new char[ub]);  // uninitialised: only the written part is touched
+            out.cap = ub;
+        }
+        char *q = out.p.get();
+        auto seg = [&](int p0, int p1) {
             if (p0 > p1) std::swap(p0, p1);
-            char tmp[96];
-            char *q = tmp;
             q = put_int(q, p0 / Y % X); *q++ = ' ';
             q = put_int(q, p0 % Y); *q++ = ' ';
             q = put_int(q, p0 / XY); *q++ = ' ';
             q = put_int(q, p1 / Y % X); *q++ = ' ';
             q = put_int(q, p1 % Y); *q++ = ' ';
             q = put_int(q, p1 / XY); *q++ = '\n';
-            o.insert(o.end(), tmp, q);
         };
-        for (int n = c * CH; n < std::min(N, (c + 1) * CH); n++) {
-            out.insert(out.end(), d.name_pool.data() + d.name_off[n], d.name_pool.data() + d.name_off[n + 1]);
-            out.push_back('\n'); out.push_back('('); out.push_back('\n');
+        for (int n = n0; n < n1; n++) {
+            const size_t nl = (size_t)(d.name_off[n + 1] - d.name_off[n]);
+            std::memcpy(q, d.name_pool.data() + d.name_off[n], nl);
+            q += nl;
+            *q++ = '\n'; *q++ = '('; *q++ = '\n';
             for (int64_t i = d.sel_off[n]; i < d.sel_off[n + 1]; i++)
-                if (d.sel[i] < XY) seg(d.sel[i], d.sel[i] + XY, out);
-            for (int64_t i = d.extra_off[n]; i < d.extra_off[n + 1]; i += 2) seg(d.extra[i], d.extra[i + 1], out);
+                if (d.sel[i] < XY) seg(d.sel[i], d.sel[i] + XY);
+            for (int64_t i = d.extra_off[n]; i < d.extra_off[n + 1]; i += 2) seg(d.extra[i], d.extra[i + 1]);
             if (n + 1 < (int)ns.sub_off.size())
                 for (int s = ns.sub_off[n]; s < ns.sub_off[n + 1]; s++) {
                     const int *r = rs.routes_of(s);
                     if (!r) continue;
-                    for (int j = 1; j < r[0]; j += 2) seg(r[j] + XY, r[j + 1] + XY, out);
+                    for (int j = 1; j < r[0]; j += 2) seg(r[j] + XY, r[j + 1] + XY);
                 }
-            out.push_back(')'); out.push_back('\n');
+            *q++ = ')'; *q++ = '\n';
         }
+        out.size = (size_t)(q - out.p.get());
     };
     const int W = 8 * std::max(1, threads);
-    std::vector<std::vector<char>> bufs(W);
+    std::vector<Buf> bufs(W);
     std::vector<off_t> at(W + 1);
     off_t pos = 0;
     for (int c0 = 0; c0 < nch; c0 += W) {
@@ -519,11 +555,11 @@ void write_guides(const Design &d, const NetSet &ns, const RouteSource &rs, cons
             for (int i = b; i < e; i++) fmt(c0 + i, bufs[i]);
         });
         at[0] = pos;
-        for (int i = 0; i < k; i++) at[i + 1] = at[i] + (off_t)bufs[i].size();
+        for (int i = 0; i < k; i++) at[i + 1] = at[i] + (off_t)bufs[i].size;
         std::atomic<bool> ok{true};
         parallel_for(k, threads, [&](int b, int e) {
             for (int i = b; i < e; i++)
-                if (!pwrite_all(fd, bufs[i].data(), bufs[i].size(), at[i])) ok = false;
+                if (!pwrite_all(fd, bufs[i].p.get(), bufs[i].size, at[i])) ok = false;
         });
         if (!ok) throw Error(ERR_IO, std::string("write failed on ") + path);
         pos = at[k];

@@ -225,6 +225,7 @@ void ShapeDev::upload(const ShapeSet &sh, int X, int Y, int sp, cudaStream_t st,
 
 // ------------------------------------------------------------------ router
 Router::~Router() {
+    if (grid_thread.joinable()) grid_thread.join();
     kt.collect();
     if (graph1_exec) cudaGraphExecDestroy(graph1_exec);
     if (ev0) cudaEventDestroy(ev0);
@@ -252,6 +253,16 @@ void Router::open(const char *cap, const char *net) {
     } joiner{ctx_init};
     read_design(d, cap, net, threads);
     const double t_read = now_s();
+    // the grid goes to the device while the trees are built
+    if (dev >= 0)
+        grid_thread = std::thread([this, dev] {
+            try {
+                cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+                create_grid();
+            } catch (...) {
+                grid_err = std::current_exception();
+            }
+        });
     build_netset(d, ns, threads);
     const double t_nets = now_s();
     // trees in DFS preorder, net-id order, and the phase-1 route record layout
@@ -309,9 +320,7 @@ void Router::open(const char *cap, const char *net) {
 
 // Device state is created and the inputs uploaded on the first run, so that
 // opening a design (parsing, pin selection, trees) needs no GPU.
-void Router::ensure_device() {
-    if (s) return;
-    const double t0 = now_s();
+void Router::create_grid() {
     cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
     for (int i = 0; i < 2; i++) {
         cuda_check(cudaStreamCreateWithFlags(&s_cls[i], cudaStreamNonBlocking), "stream");
@@ -321,12 +330,29 @@ void Router::ensure_device() {
     cuda_check(cudaEventCreate(&ev0), "event");
     cuda_check(cudaEventCreate(&ev1), "event");
     const int L = d.L - 1, X = d.X, Y = d.Y;
-    std::vector<float> capr((size_t)L * X * Y);
-    std::memcpy(capr.data(), d.cap.data() + (size_t)X * Y, capr.size() * sizeof(float));
     std::vector<double> sc(L);
     for (int l = 0; l < L; l++) sc[l] = d.short_cost[l + 1];
+    // routing layers are file layers 1..L, contiguous in d.cap
     go.create(L, X, Y, d.layer_dir[1], d.x_edge_len.data(), d.y_edge_len.data(), d.unit_wire, d.unit_via, sc.data(),
-              capr.data(), s);
+              d.cap.data() + (size_t)X * Y, s);
+    grid_ready = true;
+}
+
+void Router::join_grid() {
+    if (grid_thread.joinable()) grid_thread.join();
+    if (grid_err) {
+        std::exception_ptr e = grid_err;
+        grid_err = nullptr;
+        std::rethrow_exception(e);
+    }
+}
+
+void Router::ensure_device() {
+    if (device_ready) return;
+    const double t0 = now_s();
+    join_grid();
+    if (!grid_ready) create_grid();
+    const int L = d.L - 1, X = d.X, Y = d.Y;
     const double t_grid = now_s();
     // resident inputs
     d_tree_off.upload(tree_off, s);
@@ -378,6 +404,7 @@ void Router::ensure_device() {
     setup_h2d = (int64_t)go.g.N * 4 + 4 * (int64_t)(X + Y - 2) + 8 * L + 4 * (int64_t)tree_off.size() +
                 8 * (int64_t)tree_nodes.size() + 8 * (int64_t)scratch_off.size() + 12 * (int64_t)R + 8 * (int64_t)R;
     cuda_check(cudaStreamSynchronize(s), "inputs");
+    device_ready = true;
     if (verbose)
         std::fprintf(stderr, "[igr] device setup %.3fs (grid %.3f, trees %.3f, shapes and claims %.3f, rest %.3f)\n",
                      now_s() - t0, t_grid - t0, t_trees - t_grid, t_shapes - t_trees, now_s() - t_claims);

@@ -2,8 +2,10 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <exception>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "device.hpp"
@@ -253,6 +255,13 @@ struct Router {
     void fetch_routes();
     const int *route_of(int net) const { return h_routes.p + route_off[net]; }
     void ensure_device();
+    // stream, events and the routing grid on the device; started on a thread of
+    // its own by open() as soon as the capacities are read
+    void create_grid();
+    void join_grid();
+    std::thread grid_thread;
+    std::exception_ptr grid_err;
+    bool grid_ready = false, device_ready = false;
     void color_nets(const std::vector<int> &order, const ShapeDev &shapes, int sparsity,
                     std::vector<std::vector<int>> &batches);
     // colours n ranks (d_perm_ranks[k] = shape of rank k) into d_bat; returns the batch count
