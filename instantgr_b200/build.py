@@ -74,7 +74,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
         list(ex.map(lambda c: _run(c, log), jobs_list))
     so = os.path.join(LIB, "libigr_b200.so")
     if jobs_list or not os.path.exists(so):
-        _run([NVCC, "-shared", "-o", so] + objs + ARCH + ["-lpthread"], log)
+        _run([NVCC, "-shared", "-o", so] + objs + ARCH + ["-lpthread", "-ldl"], log)
     exe = os.path.join(BIN, "igr_route")
     main_src = os.path.join(CSRC, "main_route.cpp")
     if _stale(main_src, exe, max(hdr, os.path.getmtime(so))):

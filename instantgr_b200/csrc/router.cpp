@@ -17,12 +17,14 @@
 #include "router.hpp"
 #include "seed_model.hpp"
 
+#include <dlfcn.h>
 #include <sys/stat.h>
 
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <future>
 #include <map>
 #include <mutex>
 #include <numeric>
@@ -118,6 +120,20 @@ void pinned_free(void *p, size_t bytes) {
     if (!p) return;
     std::lock_guard<std::mutex> lock(g_pinned_mu);
     g_pinned[block_bytes(bytes)].push_back(p);
+}
+
+// True when this process has initialised the CUDA driver already, found
+// without initialising it: cuCtxGetCurrent of an already loaded driver
+// library answers CUDA_ERROR_NOT_INITIALIZED (3) before cuInit.
+bool cuda_driver_ready() {
+    void *h = dlopen("libcuda.so.1", RTLD_NOW | RTLD_NOLOAD);
+    if (!h) return false;
+    using GetCurrent = int (*)(void **);
+    auto f = reinterpret_cast<GetCurrent>(dlsym(h, "cuCtxGetCurrent"));
+    void *ctx = nullptr;
+    const bool ready = f && f(&ctx) == 0;
+    dlclose(h);
+    return ready;
 }
 
 // ------------------------------------------------------------------ grid
@@ -240,29 +256,37 @@ Router::~Router() {
 
 void Router::open(const char *cap, const char *net) {
     const double t0 = now_s();
-    // bring up the CUDA context of the caller's device while the host parses
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
-    std::thread ctx_init([dev] {
-        if (dev >= 0 && cudaSetDevice(dev) == cudaSuccess) cudaFree(nullptr);
+    // The CUDA driver, the caller's device context and the routing grid are
+    // brought up on a side thread while the host parses and builds trees (the
+    // first CUDA call of a process can take a second).  The device is the
+    // calling thread's current one; before the driver is initialised no thread
+    // can have chosen one, so it is the runtime's default, device 0.
+    int dev = 0;
+    if (cuda_driver_ready() && cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
+        dev = 0;
+    }
+    std::promise<bool> cap_read;  // true: the capacities are parsed; false: open failed
+    std::future<bool> cap_ok = cap_read.get_future();
+    grid_thread = std::thread([this, dev, f = std::move(cap_ok)]() mutable {
+        try {
+            const double c0 = now_s();
+            cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+            cuda_check(cudaFree(nullptr), "device context");
+            ctx_seconds = now_s() - c0;
+            if (f.get()) create_grid();
+        } catch (...) {
+            grid_err = std::current_exception();
+        }
     });
-    struct Joiner {
-        std::thread &t;
-        ~Joiner() { if (t.joinable()) t.join(); }
-    } joiner{ctx_init};
-    read_design(d, cap, net, threads);
+    try {
+        read_design(d, cap, net, threads);
+    } catch (...) {
+        cap_read.set_value(false);
+        throw;
+    }
+    cap_read.set_value(true);
     const double t_read = now_s();
-    // the grid goes to the device while the trees are built
-    if (dev >= 0)
-        grid_thread = std::thread([this, dev] {
-            try {
-                cuda_check(cudaSetDevice(dev), "cudaSetDevice");
-                create_grid();
-            } catch (...) {
-                grid_err = std::current_exception();
-            }
-        });
     build_netset(d, ns, threads);
     const double t_nets = now_s();
     // trees in DFS preorder, net-id order, and the phase-1 route record layout
@@ -406,8 +430,10 @@ void Router::ensure_device() {
     cuda_check(cudaStreamSynchronize(s), "inputs");
     device_ready = true;
     if (verbose)
-        std::fprintf(stderr, "[igr] device setup %.3fs (grid %.3f, trees %.3f, shapes and claims %.3f, rest %.3f)\n",
-                     now_s() - t0, t_grid - t0, t_trees - t_grid, t_shapes - t_trees, now_s() - t_claims);
+        std::fprintf(stderr,
+                     "[igr] device setup %.3fs (waiting for the context and grid %.3f, trees %.3f, shapes and claims "
+                     "%.3f, rest %.3f; the context took %.3f on the side thread)\n",
+                     now_s() - t0, t_grid - t0, t_trees - t_grid, t_shapes - t_trees, now_s() - t_claims, ctx_seconds);
 }
 
 // Grows the route buffer to `need` ints, keeping the records already written.

@@ -14,6 +14,7 @@
 namespace igr {
 
 void cuda_check(cudaError_t e, const char *what);
+bool cuda_driver_ready();
 
 // Process-wide cache of device memory: blocks given back stay mapped and are
 // handed out again for requests of up to their size (per device), so that
@@ -262,6 +263,7 @@ struct Router {
     std::thread grid_thread;
     std::exception_ptr grid_err;
     bool grid_ready = false, device_ready = false;
+    double ctx_seconds = 0;  // context creation on the side thread (verbose report)
     void color_nets(const std::vector<int> &order, const ShapeDev &shapes, int sparsity,
                     std::vector<std::vector<int>> &batches);
     // colours n ranks (d_perm_ranks[k] = shape of rank k) into d_bat; returns the batch count
