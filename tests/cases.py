@@ -213,3 +213,45 @@ def grid_arrays(g: dict):
             np.array([g["unit_wire"], g["unit_via"]], np.float64), np.asarray(g["short"], np.float64),
             np.asarray(g["xlen"], np.int32), np.asarray(g["ylen"], np.int32), np.asarray(g["cap"], np.float32),
             np.asarray(g["demand"], np.float32)]
+
+
+def dag_records_batch(ref, nets=None) -> dict:
+    """Batch in the layout of dag_batch from flat detour-DAG records
+    [m, nodes, par_num, child_num, depth, E, par, child_idx, npoints, points]
+    (the output of igr_build_dag), nets in record order."""
+    node_off, nodes, depth, par_off, par, slot, child_num = [0], [], [], [0], [], [], []
+    p = 0
+    k = 0
+    while p < ref.size:
+        m = int(ref[p])
+        nd = ref[p + 1:p + 1 + m]
+        pn = ref[p + 1 + m:p + 1 + 2 * m]
+        cn = ref[p + 1 + 2 * m:p + 1 + 3 * m]
+        dep = ref[p + 1 + 3 * m:p + 1 + 4 * m]
+        E = int(ref[p + 1 + 4 * m])
+        pr = ref[p + 2 + 4 * m:p + 2 + 4 * m + E]
+        ci = ref[p + 2 + 4 * m + E:p + 2 + 4 * m + 2 * E]
+        npt = int(ref[p + 2 + 4 * m + 2 * E])
+        p += 3 + 4 * m + 2 * E + npt
+        if nets is not None and k not in nets:
+            k += 1
+            continue
+        k += 1
+        base = len(nodes)
+        nodes += nd.tolist()
+        depth += dep.tolist()
+        child_num += cn.tolist()
+        q = 0
+        for v in range(m):
+            for _ in range(int(pn[v])):
+                par.append(base + int(pr[q]))
+                slot.append(int(ci[q]))
+                q += 1
+            par_off.append(len(par))
+        node_off.append(len(nodes))
+    node_off = np.array(node_off, np.int32)
+    cap = (8 * np.diff(node_off) + 1).astype(np.int32)
+    return dict(node_off=node_off, nodes=np.array(nodes, np.int32), depth=np.array(depth, np.int32),
+                par_off=np.array(par_off, np.int32), par=np.array(par, np.int32),
+                child_slot=np.array(slot, np.int32), child_num=np.array(child_num, np.int32), route_cap=cap,
+                route_off=np.concatenate([[0], np.cumsum(cap)[:-1]]).astype(np.int64))

@@ -150,6 +150,46 @@ def test_coloring_matches_oracle(seed, n):
         assert len(cells) == len(set(cells))
 
 
+def _dag_vs_oracle(g, d, stamp=11):
+    """GPU DAG DP, backtrace and demand against the oracle; returns the nets compared."""
+    n = len(d["node_off"]) - 1
+    c = ctx_for(g)
+    c.cost_refresh()
+    vc, ps = c.costs()
+    total = int(d["route_off"][-1] + d["route_cap"][-1])
+    r_gpu = np.zeros(total, np.int32)
+    c.dag_route(d["node_off"], d["nodes"], d["depth"], d["par_off"], d["par"], d["child_slot"], d["child_num"],
+                d["route_off"], d["route_cap"], r_gpu, stamp)
+    pre_gpu = c.pre()
+    c.close()
+    o = Oracle(g)
+    r_orc = np.zeros(total, np.int32)
+    pre = np.zeros(o.N, np.int32)
+    st = np.zeros(o.N, np.int32)
+    assert o.dag_route(vc, ps, d, d["route_off"], d["route_cap"], r_orc, pre, st, stamp) == 0
+    for k in range(n):
+        a = int(d["route_off"][k])
+        m = int(r_orc[a])
+        assert np.array_equal(r_gpu[a:a + m], r_orc[a:a + m]), f"net {k}"
+    assert np.array_equal(pre_gpu, pre)
+    return n
+
+
+@pytest.mark.parametrize("seed,dir0,load", [(43, 0, 1.0), (44, 1, 2.5)])
+def test_dag_route_on_detour_builder_dags(seed, dir0, load):
+    """The DAGs of the detour builder (golden records of the reference builder:
+    mirrored trunks, Z-shape alternatives, split long edges; nodes with up to 36
+    parents and 5 child slots, depth up to 13) through the DAG DP, against the
+    oracle on two cost maps."""
+    from conftest import golden
+    f = golden("dagbuild.npz")
+    X, Y = int(f["X"]), int(f["Y"])
+    g = cases.grid_case(seed, X=X, Y=Y, dir0=dir0, load=load)
+    d = cases.dag_records_batch(f["ref"])
+    assert int(np.max(np.diff(d["par_off"]))) >= 30
+    assert _dag_vs_oracle(g, d) == len(f["tree_off"]) - 1
+
+
 @pytest.mark.parametrize("seed,X,Y,dir0,n", [(41, 48, 40, 0, 50), (42, 70, 60, 1, 120)])
 def test_dag_route_matches_oracle(seed, X, Y, dir0, n):
     g = cases.grid_case(seed, X=X, Y=Y, dir0=dir0)
