@@ -30,6 +30,18 @@ namespace igr {
 
 namespace {
 
+// Working arrays of one builder, kept per host thread so that their capacity
+// carries over from net to net.
+struct Scratch {
+    std::vector<int> region[2];
+    std::vector<std::pair<int, int>> range[2];
+    std::vector<std::vector<int>> stems[2];
+    std::vector<int> nodes, child_pre, points;
+    std::vector<std::pair<int, int>> links;
+    std::vector<int> poff, pcode, at, visit, newid, stk;
+    std::vector<std::pair<int, int>> st;
+};
+
 struct Builder {
     const NetSet &ns;
     const RNet &net;
@@ -43,21 +55,27 @@ struct Builder {
     float ratio;
     int num_tracks;
     int root = -1;
-    std::vector<int> region[2];
-    std::vector<std::pair<int, int>> range[2];
-    std::vector<std::vector<int>> stems[2];
+    Scratch &sc;
+    std::vector<int> (&region)[2];
+    std::vector<std::pair<int, int>> (&range)[2];
+    std::vector<std::vector<int>> (&stems)[2];
     // DAG under construction
-    std::vector<int> nodes;
-    std::vector<std::vector<int>> parents;  // parent*10 + slot
-    std::vector<int> child_pre;
-    std::vector<int> points;
+    std::vector<int> &nodes;
+    std::vector<std::pair<int, int>> &links;  // (child, parent*10 + slot) in creation order
+    std::vector<int> &child_pre;
+    std::vector<int> &points;
 
-    Builder(const NetSet &n_, const RNet &r, const CongestionView &c, int m, DagNet &o)
+    Builder(const NetSet &n_, const RNet &r, const CongestionView &c, int m, DagNet &o, Scratch &s)
         : ns(n_), net(r), cv(c), mode(m), out(o), X(n_.X), Y(n_.Y), XY(n_.X * n_.Y), G(r.adj), P(r.tnode),
-          ntree((int)r.tnode.size()) {
+          ntree((int)r.tnode.size()), sc(s), region(s.region), range(s.range), stems(s.stems), nodes(s.nodes),
+          links(s.links), child_pre(s.child_pre), points(s.points) {
         ratio = 0.15f;
         num_tracks = 9;
         if (mode == 0 || mode == 1) { ratio = 0.1f; num_tracks = 6; }
+        nodes.clear();
+        links.clear();
+        child_pre.clear();
+        points.clear();
     }
 
     int px_(int v) const { return v / Y % X; }
@@ -160,7 +178,6 @@ struct Builder {
 
     int create(int l, int x, int y) {
         nodes.push_back(l * XY + x * Y + y);
-        parents.emplace_back();
         child_pre.push_back(0);
         return (int)nodes.size() - 1;
     }
@@ -168,7 +185,7 @@ struct Builder {
     void connect_pre(int p, int c, int slot) {
         points.push_back(px_(nodes[c]) * Y + py_(nodes[c]));
         points.push_back(px_(nodes[p]) * Y + py_(nodes[p]));
-        parents[c].push_back(p * 10 + slot);
+        links.push_back({c, p * 10 + slot});
         child_pre[p]++;
     }
 
@@ -228,9 +245,10 @@ struct Builder {
         return sh;
     }
 
-    void dfs(int x, int par, int par_node, int slot, int depth, std::vector<std::vector<int>> mirrors,
-             std::vector<std::vector<int>> old_places) {
-        if (mirrors.empty()) mirrors.resize(2);
+    void dfs(int x, int par, int par_node, int slot, int depth, const std::vector<std::vector<int>> &mirrors_in,
+             const std::vector<std::vector<int>> &old_places) {
+        static const std::vector<std::vector<int>> kNone(2);
+        const std::vector<std::vector<int>> &mirrors = mirrors_in.empty() ? kNone : mirrors_in;
         const int v = P[x];
         const int cl = v / XY, cx = px_(v), cy = py_(v);
         const int me = create(cl, cx, cy);
@@ -368,7 +386,8 @@ struct Builder {
         for (int dir = 0; dir < 2; dir++) {
             region[dir].assign(ntree, -1);
             range[dir].assign(ntree, {0, 0});
-            stems[dir].assign(ntree, {});
+            if ((int)stems[dir].size() < ntree) stems[dir].resize(ntree);
+            for (int i = 0; i < ntree; i++) stems[dir][i].clear();
         }
         for (int x = 0; x < ntree; x++) {
             const int v = P[x], cl = v / XY, cx = px_(v), cy = py_(v);
@@ -385,24 +404,33 @@ struct Builder {
         // renumber: a node is placed once all of its children are placed (post order
         // on a stack), then popped so that parents precede children (:2027-2085)
         const int cnt = (int)nodes.size();
-        std::vector<int> visit(cnt, 0), newid(cnt, 0);
-        std::vector<int> stk;
-        stk.reserve(cnt);
-        std::vector<int> work;
+        // parents of every node in creation order (CSR)
+        std::vector<int> &poff = sc.poff, &pcode = sc.pcode, &at = sc.at;
+        poff.assign(cnt + 1, 0);
+        pcode.resize(links.size());
+        for (auto &l : links) poff[l.first + 1]++;
+        for (int i = 0; i < cnt; i++) poff[i + 1] += poff[i];
+        at.assign(poff.begin(), poff.end() - 1);
+        for (auto &l : links) pcode[at[l.first]++] = l.second;
+        std::vector<int> &visit = sc.visit, &newid = sc.newid, &stk = sc.stk;
+        visit.assign(cnt, 0);
+        newid.assign(cnt, 0);
+        stk.clear();
+        std::vector<std::pair<int, int>> &st = sc.st;
         for (int i = 0; i < cnt; i++) {
             if (child_pre[i] != 0) continue;
             // iterative form of determinSequence: push i, then every parent whose
             // children are all pushed, depth first in parent order
-            std::vector<std::pair<int, size_t>> st;
+            st.clear();
             stk.push_back(i);
-            st.push_back({i, 0});
+            st.push_back({i, poff[i]});
             while (!st.empty()) {
                 auto &f = st.back();
-                if (f.second >= parents[f.first].size()) { st.pop_back(); continue; }
-                const int p = parents[f.first][f.second++] / 10;
+                if (f.second >= poff[f.first + 1]) { st.pop_back(); continue; }
+                const int p = pcode[f.second++] / 10;
                 if (++visit[p] == child_pre[p]) {
                     stk.push_back(p);
-                    st.push_back({p, 0});
+                    st.push_back({p, poff[p]});
                 }
             }
         }
@@ -418,7 +446,8 @@ struct Builder {
         while (!stk.empty()) {
             const int idx = stk.back();
             stk.pop_back();
-            for (int c : parents[idx]) {
+            for (int q = poff[idx]; q < poff[idx + 1]; q++) {
+                const int c = pcode[q];
                 const int p = c / 10, sl = c % 10;
                 const int sp = newid[p];
                 out.child_num[sp] = std::max(out.child_num[sp], sl + 1);
@@ -427,7 +456,7 @@ struct Builder {
                 out.depth[k] = std::max(out.depth[k], out.depth[sp] + 1);
             }
             newid[idx] = k;
-            out.par_num[k] = (int)parents[idx].size();
+            out.par_num[k] = poff[idx + 1] - poff[idx];
             out.par_sum[k + 1] = out.par_sum[k] + out.par_num[k];
             out.nodes[k] = nodes[idx];
             k++;
@@ -439,8 +468,9 @@ struct Builder {
 }  // namespace
 
 void build_dag(const NetSet &ns, const RNet &n, const CongestionView &cv, int mode, DagNet &out) {
+    thread_local Scratch scratch;
     out = DagNet();
-    Builder b(ns, n, cv, mode, out);
+    Builder b(ns, n, cv, mode, out, scratch);
     b.build();
 }
 
