@@ -145,12 +145,19 @@ void launch_from_track_layout_d(const GridDev &g, const double *trk, double *ref
 void launch_to_track_layout_d(const GridDev &g, const double *ref, double *trk, cudaStream_t s);
 void launch_from_track_layout_i(const GridDev &g, const int *trk, int *ref, cudaStream_t s);
 
-// ---- phase-1 conflict shapes from the flattened trees (shapes.cu): counts and
-// offsets (pt_off, claim_off: [R+1]; totals: points, claims), then the fill
-void launch_shape_count(const int *tree_off, const int *tree_nodes, const int *tree_par, int R, int X, int Y,
-                        int sparsity, int *pt_off, int *claim_off, long long *totals, cudaStream_t s);
-void launch_shape_fill(const int *tree_off, const int *tree_nodes, const int *tree_par, int R, int X, int Y,
-                       int sparsity, const int *pt_off, const int *claim_off, int *pts, int *claim, cudaStream_t s);
+// ---- conflict shapes and claim lists from the flattened trees (shapes.cu).
+// Shape k is routing net ids[k] (k when ids is null); its points are its tree's
+// nodes and edge points, or ext_pts[ext_off[k] .. ext_off[k+1]) when ext_off is
+// given; its segments are its tree's.  Counts and offsets first (pt_off,
+// claim_off: [n+1]; totals: points, claims), then the fill.
+struct ShapeArgs {
+    const int *tree_off = nullptr, *tree_nodes = nullptr, *tree_par = nullptr;
+    const int *ids = nullptr, *ext_off = nullptr, *ext_pts = nullptr;
+    int n = 0, X = 0, Y = 0, sparsity = 15;
+};
+void launch_shape_count(const ShapeArgs &a, int *pt_off, int *claim_off, long long *totals, cudaStream_t s);
+void launch_shape_fill(const ShapeArgs &a, const int *pt_off, const int *claim_off, int *pts, int *claim,
+                       cudaStream_t s);
 
 // ---- phase-1 plan from the colouring (plan.cu): routing-net ids batch by
 // batch in routing order (batches reversed), each batch split into the size

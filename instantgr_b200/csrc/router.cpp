@@ -371,6 +371,26 @@ void Router::join_grid() {
     }
 }
 
+// Conflict shapes and claim lists on the device (shapes.cu): counts and
+// offsets, the totals to the host for the allocation, then the fill.
+void Router::device_shapes(const ShapeArgs &a, ShapeDev &sd) {
+    sd.pt_off.alloc((size_t)a.n + 1);
+    sd.claim_off.alloc((size_t)a.n + 1);
+    d_shape_tot.alloc(2);
+    launch_shape_count(a, sd.pt_off.p, sd.claim_off.p, d_shape_tot.p, s);
+    long long h_tot[2] = {0, 0};
+    cuda_check(cudaMemcpyAsync(h_tot, d_shape_tot.p, sizeof h_tot, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaStreamSynchronize(s), "shape counts");
+    if (h_tot[0] > INT32_MAX || h_tot[1] > INT32_MAX) throw Error(ERR_CAPACITY, "conflict shapes exceed 32-bit offsets");
+    sd.pts.alloc((size_t)h_tot[0]);
+    sd.claim.alloc((size_t)h_tot[1]);
+    launch_shape_fill(a, sd.pt_off.p, sd.claim_off.p, sd.pts.p, sd.claim.p, s);
+    sd.npts = (int)h_tot[0];
+    sd.nshapes = a.n;
+    sd.sparsity = a.sparsity;
+    sd.bytes = 0;
+}
+
 void Router::ensure_device() {
     if (device_ready) return;
     const double t0 = now_s();
@@ -395,26 +415,10 @@ void Router::ensure_device() {
     {
         // phase-1 conflict shapes and claim lists from the resident trees; phase 1
         // samples every 15th segment cell (database_cuda.hpp:439)
-        ShapeDev &sd = d_shapes1;
-        sd.pt_off.alloc(R + 1);
-        sd.claim_off.alloc(R + 1);
-        DevBuf<long long> tot;
-        tot.alloc(2);
-        launch_shape_count(d_tree_off.p, d_tree_nodes.p, d_tree_par.p, R, X, Y, 15, sd.pt_off.p, sd.claim_off.p, tot.p,
-                           s);
-        long long h_tot[2] = {0, 0};
-        cuda_check(cudaMemcpyAsync(h_tot, tot.p, sizeof h_tot, cudaMemcpyDeviceToHost, s), "D2H");
-        cuda_check(cudaStreamSynchronize(s), "shape counts");
-        if (h_tot[0] > INT32_MAX || h_tot[1] > INT32_MAX)
-            throw Error(ERR_CAPACITY, "conflict shapes exceed 32-bit offsets");
-        sd.pts.alloc((size_t)h_tot[0]);
-        sd.claim.alloc((size_t)h_tot[1]);
-        launch_shape_fill(d_tree_off.p, d_tree_nodes.p, d_tree_par.p, R, X, Y, 15, sd.pt_off.p, sd.claim_off.p,
-                          sd.pts.p, sd.claim.p, s);
-        sd.npts = (int)h_tot[0];
-        sd.nshapes = R;
-        sd.sparsity = 15;
-        sd.bytes = 0;
+        ShapeArgs a;
+        a.tree_off = d_tree_off.p; a.tree_nodes = d_tree_nodes.p; a.tree_par = d_tree_par.p;
+        a.n = R; a.X = X; a.Y = Y; a.sparsity = 15;
+        device_shapes(a, d_shapes1);
     }
     const double t_shapes = now_s();
     const double t_claims = t_shapes;
@@ -1020,11 +1024,14 @@ bool Router::rrr_pass(int iter) {
     }
     // detour DAGs on host threads (Lshape_route_detour.hpp:702-748)
     const double th0 = now_s();
-    dag.resize(R);
+    // DAGs of the rerouted nets only, by their position in of_nets
+    dag.resize(of_nets.size());
+    dag_slot.assign(R, -1);
+    for (size_t k = 0; k < of_nets.size(); k++) dag_slot[of_nets[k]] = (int)k;
     std::vector<char> keep(of_nets.size(), 1);
     parallel_for((int)of_nets.size(), threads, [&](int b, int e) {
         for (int k = b; k < e; k++) {
-            DagNet &dn = dag[of_nets[k]];
+            DagNet &dn = dag[k];
             build_dag(ns, ns.nets[of_nets[k]], cv, mode_eff, dn);
             // the DP keeps at most 10 child slots per node (the reference packs the
             // slot as a decimal digit); nets beyond that keep their current route
@@ -1039,85 +1046,128 @@ bool Router::rrr_pass(int iter) {
         of_nets.swap(kept);
     }
     st.dag_host_ms += (now_s() - th0) * 1e3;
+    const double t_dag = now_s();
     if (of_nets.empty()) return false;
     // colouring on DAG points and tree segments (Lshape_route_detour.hpp:751)
-    ShapeSet sh;
-    for (int id : of_nets) {
-        const RNet &r = ns.nets[id];
-        for (int q : dag[id].points) { sh.pts.push_back(q); sh.pt_net.push_back((int)sh.pt_off.size() - 1); }
-        sh.pt_off.push_back((int)sh.pts.size());
-        for_each_shape(
-            r, X, Y, [](int) {}, [&](int a, int c) { sh.hseg.push_back(a); sh.hseg.push_back(c); },
-            [&](int a, int c) { sh.vseg.push_back(a); sh.vseg.push_back(c); });
-        sh.h_off.push_back((int)(sh.hseg.size() / 2));
-        sh.v_off.push_back((int)(sh.vseg.size() / 2));
-    }
+    // conflict shapes of the rerouted nets: their DAG points and their trees'
+    // segments; claim lists built on the device
+    std::vector<int> pt_off(of_nets.size() + 1, 0), pts;
+    for (size_t k = 0; k < of_nets.size(); k++) pt_off[k + 1] = pt_off[k] + (int)dag[dag_slot[of_nets[k]]].points.size();
+    pts.resize(pt_off.back());
+    parallel_for((int)of_nets.size(), threads, [&](int b, int e) {
+        for (int k = b; k < e; k++) {
+            const auto &p = dag[dag_slot[of_nets[k]]].points;
+            std::copy(p.begin(), p.end(), pts.begin() + pt_off[k]);
+        }
+    });
+    d2_ptoff.upload(pt_off, s);
+    d2_pts.upload(pts, s);
+    d2_ids.upload(of_nets, s);
+    st.h2d_bytes += (int64_t)(pt_off.size() + pts.size() + of_nets.size()) * 4;
     ShapeDev shd;
-    shd.upload(sh, X, Y, mode_eff >= 1 ? 2 : 15, s, threads);
-    st.h2d_bytes += (int64_t)(sh.pts.size() * 2 + sh.hseg.size() + sh.vseg.size() + 3 * of_nets.size()) * 4;
+    {
+        ShapeArgs a;
+        a.tree_off = d_tree_off.p; a.tree_nodes = d_tree_nodes.p; a.tree_par = d_tree_par.p;
+        a.ids = d2_ids.p; a.ext_off = d2_ptoff.p; a.ext_pts = d2_pts.p;
+        a.n = (int)of_nets.size(); a.X = X; a.Y = Y; a.sparsity = mode_eff >= 1 ? 2 : 15;
+        device_shapes(a, shd);
+    }
     std::vector<int> local(of_nets.size());
     std::iota(local.begin(), local.end(), 0);  // shape k belongs to of_nets[k]; of_nets is in priority order
     std::vector<std::vector<int>> lb;
+    const double t_shapes = now_s();
     color_nets(local, shd, mode_eff >= 1 ? 2 : 15, lb);
+    const double t_color = now_s();
     std::vector<std::vector<int>> batches(lb.size());
     for (size_t b = 0; b < lb.size(); b++)
         for (int k : lb[b]) batches[b].push_back(of_nets[k]);
     std::reverse(batches.begin(), batches.end());
-    // batch-local CSR of all batches, laid end to end
+    // batch-local CSR of all batches, laid end to end: sizes per net and batch
+    // first, then every batch filled on its own thread
     struct BInfo { int nb, eb, pb, lb, nnb, nets, n, e, slots; };
-    std::vector<BInfo> bi;
-    std::vector<int> nodes, par_off, par, cslot, echild, child_off, level_off, level_nodes, net_node_off, net_ids;
-    std::vector<int> net_level_off, b_nodes, b_off, b_net;
+    const int B = (int)batches.size();
+    std::vector<BInfo> bi(B);
     std::vector<int64_t> old_off = route_off;
-    for (size_t b = 0; b < batches.size(); b++) {
-        BInfo f{};
-        f.nb = (int)nodes.size(); f.eb = (int)par.size(); f.pb = (int)par_off.size();
-        f.lb = (int)level_off.size(); f.nnb = (int)net_node_off.size(); f.nets = (int)net_ids.size();
-        int n = 0, e = 0, sl = 0;
-        for (int id : batches[b]) n += (int)dag[id].nodes.size();
-        std::vector<int> dep(n);
-        par_off.push_back(0);
-        child_off.push_back(0);
-        net_node_off.push_back(0);
-        int base = 0;
-        for (int id : batches[b]) {
-            const DagNet &dn = dag[id];
-            const int m = (int)dn.nodes.size();
-            for (int v = 0; v < m; v++) {
-                nodes.push_back(dn.nodes[v]);
-                for (int q = dn.par_sum[v]; q < dn.par_sum[v + 1]; q++) {
-                    par.push_back(base + dn.par_nodes[q]);
-                    cslot.push_back(dn.child_idx[q]);
-                    echild.push_back(base + v);
-                    e++;
-                }
-                par_off.push_back(e);
-                sl += dn.child_num[v];
-                child_off.push_back(sl);
-                dep[base + v] = dn.depth[v];
-            }
-            base += m;
-            net_ids.push_back(id);
-            net_node_off.push_back(base);
-            // new route record of the net (appended)
-            route_cap[id] = 8 * m + 1;
-            route_off[id] = route_end;
-            route_end += route_cap[id];
+    std::vector<int> net_levels(of_nets.size());  // depth + 1 of each net's DAG
+    parallel_for((int)of_nets.size(), threads, [&](int b0, int e0) {
+        for (int k = b0; k < e0; k++) {
+            int D = 0;
+            for (int dv : dag[k].depth) D = std::max(D, dv + 1);
+            net_levels[k] = D;
         }
-        // levels of each net of the batch (batch-local positions)
-        dag_levels((int)batches[b].size(), net_node_off.data() + f.nnb, dep.data(), b_nodes, b_off, b_net);
-        level_nodes.insert(level_nodes.end(), b_nodes.begin(), b_nodes.end());
-        level_off.insert(level_off.end(), b_off.begin(), b_off.end());
-        net_level_off.insert(net_level_off.end(), b_net.begin(), b_net.end());
-        if ((int64_t)n * 100 + 99 > 0x7fffffffLL) throw Error(ERR_CAPACITY, "DAG batch too large for 32-bit node ids");
-        f.n = n; f.e = e; f.slots = sl;
-        bi.push_back(f);
+    });
+    BInfo tot{};
+    {
+        BInfo acc{};
+        for (int b = 0; b < B; b++) {
+            BInfo &f = bi[b];
+            f = acc;
+            f.n = f.e = f.slots = 0;
+            int lv = 0;
+            for (int id : batches[b]) {
+                const int k = dag_slot[id];
+                const DagNet &dn = dag[k];
+                f.n += (int)dn.nodes.size();
+                f.e += (int)dn.par_nodes.size();
+                for (int c : dn.child_num) f.slots += c;
+                lv += net_levels[k] + 1;
+                // new route record of the net (appended)
+                route_cap[id] = 8 * (int)dn.nodes.size() + 1;
+                route_off[id] = route_end;
+                route_end += route_cap[id];
+            }
+            if ((int64_t)f.n * 100 + 99 > 0x7fffffffLL) throw Error(ERR_CAPACITY, "DAG batch too large for 32-bit node ids");
+            const int nn = (int)batches[b].size();
+            acc.nb += f.n; acc.eb += f.e; acc.pb += f.n + 1; acc.lb += lv; acc.nnb += nn + 1; acc.nets += nn;
+        }
+        tot = acc;
     }
+    std::vector<int> nodes(tot.nb), par_off(tot.pb), par(tot.eb), cslot(tot.eb), echild(tot.eb), child_off(tot.pb);
+    std::vector<int> level_off(tot.lb), level_nodes(tot.nb), net_node_off(tot.nnb), net_ids(tot.nets),
+        net_level_off(tot.nnb);
+    parallel_for(B, threads, [&](int b0, int e0) {
+        std::vector<int> dep, b_nodes, b_off, b_net;
+        for (int b = b0; b < e0; b++) {
+            const BInfo &f = bi[b];
+            dep.resize(f.n);
+            int e = 0, sl = 0, base = 0;
+            par_off[f.pb] = 0;
+            child_off[f.pb] = 0;
+            net_node_off[f.nnb] = 0;
+            int j = 0;
+            for (int id : batches[b]) {
+                const DagNet &dn = dag[dag_slot[id]];
+                const int m = (int)dn.nodes.size();
+                for (int v = 0; v < m; v++) {
+                    nodes[f.nb + base + v] = dn.nodes[v];
+                    for (int q = dn.par_sum[v]; q < dn.par_sum[v + 1]; q++) {
+                        par[f.eb + e] = base + dn.par_nodes[q];
+                        cslot[f.eb + e] = dn.child_idx[q];
+                        echild[f.eb + e] = base + v;
+                        e++;
+                    }
+                    par_off[f.pb + base + v + 1] = e;
+                    sl += dn.child_num[v];
+                    child_off[f.pb + base + v + 1] = sl;
+                    dep[base + v] = dn.depth[v];
+                }
+                base += m;
+                net_ids[f.nets + j] = id;
+                net_node_off[f.nnb + j + 1] = base;
+                j++;
+            }
+            // levels of each net of the batch (batch-local positions)
+            dag_levels(j, net_node_off.data() + f.nnb, dep.data(), b_nodes, b_off, b_net);
+            std::copy(b_nodes.begin(), b_nodes.end(), level_nodes.begin() + f.nb);
+            std::copy(b_off.begin(), b_off.end(), level_off.begin() + f.lb);
+            std::copy(b_net.begin(), b_net.end(), net_level_off.begin() + f.nnb);
+        }
+    });
     if (verbose) {
         // shape of the DAGs: nodes and depth per net, widest level of one net
         std::vector<int> nn, nd, nw;
         for (int id : of_nets) {
-            const DagNet &dn = dag[id];
+            const DagNet &dn = dag[dag_slot[id]];
             int dmax = 0;
             for (int dv : dn.depth) dmax = std::max(dmax, dv + 1);
             std::vector<int> w(dmax, 0);
@@ -1136,6 +1186,7 @@ bool Router::rrr_pass(int iter) {
                      batches.size(), of_nets.size(), nodes.size(), q(nn, .5), q(nn, .9), q(nn, .99), q(nn, 1),
                      q(nd, .5), q(nd, .9), q(nd, .99), q(nd, 1), q(nw, .5), q(nw, .99), q(nw, 1));
     }
+    const double t_csr = now_s();
     grow_routes(route_end);
     dg_nodes.upload(nodes, s); dg_paroff.upload(par_off, s); dg_par.upload(par, s); dg_cslot.upload(cslot, s);
     dg_echild.upload(echild, s); dg_childoff.upload(child_off, s); dg_leveloff.upload(level_off, s);
@@ -1193,6 +1244,11 @@ bool Router::rrr_pass(int iter) {
     cudaEventElapsedTime(&ms_, ev0, ev1);
     st.rrr_ms += ms_;
     if (int e = go.check_error(s)) throw Error(e, "device error in rip-up and reroute");
+    if (verbose)
+        std::fprintf(stderr,
+                     "[igr] pass %d host: DAGs %.3f s, conflict shapes %.3f s, colouring %.3f s, batch arrays %.3f s, "
+                     "batches on the device %.3f s\n",
+                     iter, t_dag - th0, t_shapes - t_dag, t_color - t_shapes, t_csr - t_color, now_s() - t_csr);
     return true;
 }
 

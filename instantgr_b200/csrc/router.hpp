@@ -220,7 +220,8 @@ struct Router {
         dg_netlvl, dg_ids, dg_bchange, dg_lout, dg_stage, dg_scnt;
     DevBuf<double> dg_costs, dg_cedges;
     DevBuf<unsigned long long> dg_best, dg_packed;
-    std::vector<DagNet> dag;  // detour DAG of every rerouted net (phase 2)
+    std::vector<DagNet> dag;     // detour DAGs of the nets rerouted in the current pass
+    std::vector<int> dag_slot;   // routing net -> its DAG in `dag`, -1 when not rerouted
     unsigned long long cost_cells = 0, commit_cells = 0;
     // phase-1 plan of the last run (routing order, batches, trees, route capacity in order)
     std::vector<int> plan_ids, plan_batch_off, plan_node_off, plan_nodes, plan_par, plan_cap;
@@ -256,6 +257,9 @@ struct Router {
     void fetch_routes();
     const int *route_of(int net) const { return h_routes.p + route_off[net]; }
     void ensure_device();
+    void device_shapes(const ShapeArgs &a, ShapeDev &sd);
+    DevBuf<long long> d_shape_tot;
+    DevBuf<int> d2_ptoff, d2_pts, d2_ids;  // DAG points and net ids of the rerouted nets
     // stream, events and the routing grid on the device; started on a thread of
     // its own by open() as soon as the capacities are read
     void create_grid();

@@ -9,7 +9,9 @@
 // on the set of tree edges, so they are generated here from the (node,
 // parent) pairs of the DFS-ordered trees; the colouring treats points and
 // claims as sets, so the order inside a net is free.  Two passes: counts per
-// net with an exclusive scan (one block), then the fill.
+// net with an exclusive scan (one block), then the fill.  The rip-up passes
+// use the same kernels for the rerouted nets, with the DAG points given and
+// the segments of their trees.
 #include "kcommon.cuh"
 
 namespace igr {
@@ -56,21 +58,40 @@ __device__ __forceinline__ int point_claims(int x, int y, int X, int Y) {
     return 1 + (y > 0) + (x > 0) + (x + 1 < X);
 }
 
-__global__ void shape_count_kernel(const int *tree_off, const int *tree_nodes, const int *tree_par, int R, int X,
-                                   int Y, int sp, int *pt_cnt, int *claim_cnt) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= R) return;
-    const int a = tree_off[i], m = tree_off[i + 1] - a;
+// shape k: routing net ids[k] (k when ids is null); its points are the tree's
+// (nodes and edge points) or, when ext_off is given, ext_pts[ext_off[k] ..
+// ext_off[k+1]); its segments are always the tree's
+struct ShapeSrc {
+    const int *tree_off, *tree_nodes, *tree_par, *ids, *ext_off, *ext_pts;
+    int n, X, Y, sp;
+};
+
+template <class Pt, class Hs, class Vs>
+__device__ __forceinline__ void shape_of(const ShapeSrc &a, int k, Pt &&point, Hs &&hseg, Vs &&vseg) {
+    const int net = a.ids ? a.ids[k] : k;
+    const int t = a.tree_off[net], m = a.tree_off[net + 1] - t;
+    if (a.ext_off) {
+        for (int q = a.ext_off[k]; q < a.ext_off[k + 1]; q++) point(a.ext_pts[q] / a.Y, a.ext_pts[q] % a.Y);
+        net_shapes(a.tree_nodes + t, a.tree_par + t, m, a.X, a.Y, [](int, int) {}, hseg, vseg);
+    } else {
+        net_shapes(a.tree_nodes + t, a.tree_par + t, m, a.X, a.Y, point, hseg, vseg);
+    }
+}
+
+__global__ void shape_count_kernel(ShapeSrc a, int *pt_cnt, int *claim_cnt) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.n) return;
+    const int X = a.X, Y = a.Y, sp = a.sp;
     int np = 0, nc = 0;
-    net_shapes(
-        tree_nodes + a, tree_par + a, m, X, Y,
+    shape_of(
+        a, k,
         [&](int x, int y) {
             np++;
             nc += point_claims(x, y, X, Y);
         },
         [&](int lo, int hi, int) { nc += (hi - lo) / sp + 1; }, [&](int lo, int hi, int) { nc += (hi - lo) / sp + 1; });
-    pt_cnt[i + 1] = np;
-    claim_cnt[i + 1] = nc;
+    pt_cnt[k + 1] = np;
+    claim_cnt[k + 1] = nc;
 }
 
 // exclusive scan of a[1..n] into a[0..n] (a[0] = 0) in one block; the total
@@ -106,15 +127,14 @@ __global__ void __launch_bounds__(kScanThreads) shape_scan_kernel(int R, int *pt
     block_scan(claim_off, R, totals + 1);
 }
 
-__global__ void shape_fill_kernel(const int *tree_off, const int *tree_nodes, const int *tree_par, int R, int X,
-                                  int Y, int sp, const int *pt_off, const int *claim_off, int *pts, int *claim) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= R) return;
-    const int a = tree_off[i], m = tree_off[i + 1] - a;
-    int *pt = pts + pt_off[i];
-    int *cl = claim + claim_off[i];
-    net_shapes(
-        tree_nodes + a, tree_par + a, m, X, Y,
+__global__ void shape_fill_kernel(ShapeSrc a, const int *pt_off, const int *claim_off, int *pts, int *claim) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.n) return;
+    const int X = a.X, Y = a.Y, sp = a.sp;
+    int *pt = pts + pt_off[k];
+    int *cl = claim + claim_off[k];
+    shape_of(
+        a, k,
         [&](int x, int y) {
             *pt++ = x * Y + y;
             *cl++ = x * Y + y;
@@ -132,19 +152,16 @@ __global__ void shape_fill_kernel(const int *tree_off, const int *tree_nodes, co
 
 }  // namespace
 
-void launch_shape_count(const int *tree_off, const int *tree_nodes, const int *tree_par, int R, int X, int Y,
-                        int sparsity, int *pt_off, int *claim_off, long long *totals, cudaStream_t s) {
-    if (R > 0)
-        shape_count_kernel<<<(R + 255) / 256, 256, 0, s>>>(tree_off, tree_nodes, tree_par, R, X, Y, sparsity, pt_off,
-                                                           claim_off);
-    shape_scan_kernel<<<1, kScanThreads, 0, s>>>(R, pt_off, claim_off, totals);
+void launch_shape_count(const ShapeArgs &a, int *pt_off, int *claim_off, long long *totals, cudaStream_t s) {
+    const ShapeSrc src{a.tree_off, a.tree_nodes, a.tree_par, a.ids, a.ext_off, a.ext_pts, a.n, a.X, a.Y, a.sparsity};
+    if (a.n > 0) shape_count_kernel<<<(a.n + 255) / 256, 256, 0, s>>>(src, pt_off, claim_off);
+    shape_scan_kernel<<<1, kScanThreads, 0, s>>>(a.n, pt_off, claim_off, totals);
 }
 
-void launch_shape_fill(const int *tree_off, const int *tree_nodes, const int *tree_par, int R, int X, int Y,
-                       int sparsity, const int *pt_off, const int *claim_off, int *pts, int *claim, cudaStream_t s) {
-    if (R > 0)
-        shape_fill_kernel<<<(R + 255) / 256, 256, 0, s>>>(tree_off, tree_nodes, tree_par, R, X, Y, sparsity, pt_off,
-                                                          claim_off, pts, claim);
+void launch_shape_fill(const ShapeArgs &a, const int *pt_off, const int *claim_off, int *pts, int *claim,
+                       cudaStream_t s) {
+    const ShapeSrc src{a.tree_off, a.tree_nodes, a.tree_par, a.ids, a.ext_off, a.ext_pts, a.n, a.X, a.Y, a.sparsity};
+    if (a.n > 0) shape_fill_kernel<<<(a.n + 255) / 256, 256, 0, s>>>(src, pt_off, claim_off, pts, claim);
 }
 
 }  // namespace igr
