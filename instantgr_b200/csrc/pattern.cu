@@ -15,8 +15,9 @@
 //      looping over the 4-5 bend layers of opposite parity in the reference's
 //      order), the nine range rows (with the reference's <= rule) and the
 //      accumulation into the parent (in the reference's order of additions);
-//   3. one lane walks the nodes in preorder, emits the route record and writes
-//      the difference array.
+//   3. one lane fixes every node's layer range in preorder (shared memory
+//      only); then all lanes emit the route record and write the difference
+//      array, each node's segments placed by a prefix sum over the nodes.
 // Nets are taken from a per-batch queue in the order given (largest first),
 // so the long nets of a batch start early.  The 45 valid layer ranges of a
 // node live in shared memory (global scratch for nets of more than kNodeTile
@@ -298,71 +299,101 @@ __global__ void __launch_bounds__(128) pattern_route_kernel(GridDev g, TreeBatch
             const int oi = __shfl_down_sync(gmask, bi, o, G);
             if (ov < bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
         }
-        // ---- 4. backtrace, route emission and demand (Lshape_route.hpp:99-152)
+        // ---- 4. backtrace, route emission and demand (Lshape_route.hpp:99-152).
+        //      One lane walks the nodes in preorder and fixes each node's layer
+        //      range from its parent's (shared memory only), stopping at the
+        //      first node without a finite range; then every lane takes nodes:
+        //      the segments of a node (its via stack, then the straight wire or
+        //      the leg, corner via and leg of a bend) get their positions in the
+        //      record from a prefix sum over nodes, in the reference's order, and
+        //      the demand of each segment that fits the record is applied.
+        __shared__ int s_stop[128 / G];
         if (gl == 0) {
-            int *r = b.routes + b.route_off[net];
-            const int cap = b.route_cap[net];
-            int cnt = 1;
-            bool ok = true;
-            long long nvias = 0;
-            // root range as (minl, maxl)
             int rmn = 0, rmx = 0;
             for (int a = 0, t = 0; a < kL; a++)
                 for (int c = a; c < kL; c++, t++)
                     if (t == bi) { rmn = a; rmx = c; }
             lr[0] = rmn * kL + rmx;
-#define EMIT(A, B)                                         \
-    do {                                                   \
-        if (!ok || cnt + 2 > cap) { ok = false; break; }   \
-        r[cnt++] = (A);                                    \
-        r[cnt++] = (B);                                    \
-    } while (0)
-            for (int i = 0; i < n && ok; i++) {
-                const int x = nx[i], y = ny[i];
-                int code = 0;
+            int stop = n;
+            for (int i = 0; i < n; i++) {
                 if (i > 0) {
                     const int plr = lr[np[i]];
-                    code = from[i * kR + tri(plr / kL, plr % kL)];
-                    lr[i] = code / (kL * kL);
+                    lr[i] = from[i * kR + tri(plr / kL, plr % kL)] / (kL * kL);
                 }
                 const int mn = lr[i] / kL, mx = lr[i] % kL;
-                if (mn > mx || !(dist[i * kR + tri(mn, mx)] < kInf)) { set_error(g.err, ERR_STATE); ok = false; break; }
-                if (mn < mx) {
-                    EMIT(mn * XY + x * Y + y, mx * XY + x * Y + y);
-                    if (ok && b.vcnt) { count_vias(g, b.vcnt, layer_first, mn, mx, x, y); nvias += mx - mn; }
-                }
-                if (!ok || i == 0) continue;
-                const int px = nx[np[i]], py = ny[np[i]];
-                const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
-                const int curl = code / kL % kL, parl = code % kL;
-                if (px == x || py == y) {
-                    EMIT(curl * XY + minx * Y + miny, curl * XY + maxx * Y + maxy);
-                    if (ok) add_wire(g, layer_first, curl, minx, maxx, miny, maxy, stamp);
-                } else if (layer_dir(g, curl)) {
-                    EMIT(curl * XY + x * Y + y, curl * XY + x * Y + py);
-                    if (ok) add_wire(g, layer_first, curl, x, x, miny, maxy, stamp);
-                    EMIT(curl * XY + x * Y + py, parl * XY + x * Y + py);
-                    if (ok && b.vcnt) {
-                        count_vias(g, b.vcnt, layer_first, min(curl, parl), max(curl, parl), x, py);
-                        nvias += max(curl, parl) - min(curl, parl);
-                    }
-                    EMIT(parl * XY + x * Y + py, parl * XY + px * Y + py);
-                    if (ok) add_wire(g, layer_first, parl, minx, maxx, py, py, stamp);
-                } else {
-                    EMIT(curl * XY + x * Y + y, curl * XY + px * Y + y);
-                    if (ok) add_wire(g, layer_first, curl, minx, maxx, y, y, stamp);
-                    EMIT(curl * XY + px * Y + y, parl * XY + px * Y + y);
-                    if (ok && b.vcnt) {
-                        count_vias(g, b.vcnt, layer_first, min(curl, parl), max(curl, parl), px, y);
-                        nvias += max(curl, parl) - min(curl, parl);
-                    }
-                    EMIT(parl * XY + px * Y + y, parl * XY + px * Y + py);
-                    if (ok) add_wire(g, layer_first, parl, px, px, miny, maxy, stamp);
-                }
+                if (mn > mx || !(dist[i * kR + tri(mn, mx)] < kInf)) { stop = i; break; }
             }
-#undef EMIT
-            if (!ok) set_error(g.err, ERR_CAPACITY);
-            r[0] = cnt;
+            s_stop[threadIdx.x / G] = stop;
+        }
+        __syncwarp(gmask);
+        const int stop = s_stop[threadIdx.x / G];
+        int *r = b.routes + b.route_off[net];
+        const int cap = b.route_cap[net];
+        const int smax = cap >= 1 ? (cap - 1) / 2 : 0;  // segments that fit the record
+        // segments of node i: emit(k, a, b, kind) for k = 0.. in record order;
+        // kind 0: via stack at the node, 1: wire (l, xa, xb, ya, yb), 2: corner via
+        auto node_segments = [&](int i, auto &&emit) {
+            const int x = nx[i], y = ny[i];
+            const int mn = lr[i] / kL, mx = lr[i] % kL;
+            int k = 0;
+            if (mn < mx) emit(k++, mn * XY + x * Y + y, mx * XY + x * Y + y, 0, mn, mx, x, y, 0);
+            if (i == 0) return k;
+            const int plr = lr[np[i]];
+            const int code = from[i * kR + tri(plr / kL, plr % kL)];
+            const int px = nx[np[i]], py = ny[np[i]];
+            const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
+            const int curl = code / kL % kL, parl = code % kL;
+            const int vlo = min(curl, parl), vhi = max(curl, parl);
+            if (px == x || py == y) {
+                emit(k++, curl * XY + minx * Y + miny, curl * XY + maxx * Y + maxy, 1, curl, minx, maxx, miny, maxy);
+            } else if (layer_dir(g, curl)) {
+                emit(k++, curl * XY + x * Y + y, curl * XY + x * Y + py, 1, curl, x, x, miny, maxy);
+                emit(k++, curl * XY + x * Y + py, parl * XY + x * Y + py, 2, vlo, vhi, x, py, 0);
+                emit(k++, parl * XY + x * Y + py, parl * XY + px * Y + py, 1, parl, minx, maxx, py, py);
+            } else {
+                emit(k++, curl * XY + x * Y + y, curl * XY + px * Y + y, 1, curl, minx, maxx, y, y);
+                emit(k++, curl * XY + px * Y + y, parl * XY + px * Y + y, 2, vlo, vhi, px, y, 0);
+                emit(k++, parl * XY + px * Y + y, parl * XY + px * Y + py, 1, parl, px, px, miny, maxy);
+            }
+            return k;
+        };
+        auto no_emit = [](int, int, int, int, int, int, int, int, int) {};
+        int carry = 0;  // segments of the nodes before this round
+        long long nvias = 0;
+        for (int i0 = 0; i0 < stop; i0 += G) {
+            const int i = i0 + gl;
+            const int cnt = i < stop ? node_segments(i, no_emit) : 0;
+            int inc = cnt;
+#pragma unroll
+            for (int o = 1; o < G; o <<= 1) {
+                const int t = __shfl_up_sync(gmask, inc, o, G);
+                if (gl >= o) inc += t;
+            }
+            const int first = carry + inc - cnt;  // global index of this node's first segment
+            if (i < stop && first < smax) {
+                node_segments(i, [&](int k, int a, int c, int kind, int p0, int p1, int p2, int p3, int p4) {
+                    const int sidx = first + k;
+                    if (sidx >= smax) return;
+                    r[1 + 2 * sidx] = a;
+                    r[2 + 2 * sidx] = c;
+                    if (kind == 1) {
+                        add_wire(g, layer_first, p0, p1, p2, p3, p4, stamp);
+                    } else if (b.vcnt) {  // kinds 0 and 2: a via stack from layer p0 to p1 at (p2, p3)
+                        count_vias(g, b.vcnt, layer_first, p0, p1, p2, p3);
+                        nvias += p1 - p0;
+                    }
+                });
+            }
+            carry += __shfl_sync(gmask, inc, G - 1, G);
+        }
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) nvias += __shfl_down_sync(gmask, nvias, o, G);
+        if (gl == 0) {
+            // the reference meets whichever comes first: a record overflow at a node
+            // before `stop` ends the walk there; otherwise the state error at `stop`
+            if (carry > smax) set_error(g.err, ERR_CAPACITY);
+            else if (stop < n) set_error(g.err, ERR_STATE);
+            r[0] = 1 + 2 * min(carry, smax);
             if (nvias) atomicAdd(&g.stats[1], (unsigned long long)nvias);
         }
         __syncwarp(gmask);

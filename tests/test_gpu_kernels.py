@@ -101,6 +101,27 @@ def test_pattern_route_and_commit_match_oracle(seed, X, Y, dir0, n, kmax):
     assert wl_gpu == wl
 
 
+def test_pattern_route_reports_a_record_too_short():
+    """A route record that cannot hold a net's segments: the oracle stops there
+    (status -1) and the kernel reports IGR_ERR_CAPACITY."""
+    g, tb = _pattern_case(14, 40, 30, 0, 60, 8)
+    cap = tb["route_cap"].copy()
+    k = int(np.argmax(np.diff(tb["node_off"])))  # the net with the most nodes
+    cap[k] = 3
+    c = ctx_for(g)
+    c.cost_refresh()
+    vc, ps = c.costs()
+    total = int(tb["route_off"][-1] + tb["route_cap"][-1])
+    with pytest.raises(ig.IgrError) as e:
+        c.pattern_route(tb["node_off"], tb["nodes"], tb["par"], tb["route_off"], cap, np.zeros(total, np.int32), 7)
+    assert e.value.code == -5
+    c.close()
+    o = Oracle(g)
+    z = np.zeros(o.N, np.int32)
+    assert o.pattern_route(vc, ps, tb["node_off"], tb["nodes"], tb["par"], tb["route_off"], cap,
+                           np.zeros(total, np.int32), z, z.copy(), 7) == -1
+
+
 def test_ripup_and_overflow_marking_match_oracle():
     g, tb = _pattern_case(21, 60, 50, 0, 250, 8)
     c = ctx_for(g)
