@@ -72,6 +72,15 @@ int igr_router_open(const char *cap_path, const char *net_path, const igr_option
 int igr_router_run(igr_router *r);
 /* Writes the route guides (src/graph.hpp:179-235). */
 int igr_router_write(igr_router *r, const char *out_path);
+/* Scores the last run on the device with the rules of the ISPD2024 evaluator
+ * (run/evaluator.cpp:462-633, read_gr_solution), on the guides that
+ * igr_router_write would write, without writing them: out[0] wirelength cost,
+ * out[1] via cost, out[2] overflow cost, out[3] total (the evaluator's FOR_STAT
+ * values before rounding); layer_loss[0..8] (may be null) the overflow loss of
+ * each routing layer before its weight.  Connectivity is not checked (the
+ * evaluator stops at the first open net instead of scoring).  No reference
+ * counterpart in the router: it replaces running the evaluator on the file. */
+int igr_router_evaluate(igr_router *r, double *out, double *layer_loss);
 /* Statistics of the last run: [0] routing nets, [1] nets rerouted in the last
  * pass, [2] wirelength, [3] via count, [4] overflow cost (GPU estimate,
  * src/graph.hpp:148-169), [5] route wall seconds, [6] phase-1 batches,

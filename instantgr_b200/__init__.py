@@ -36,6 +36,7 @@ _u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
 # every symbol of include/instantgr_b200.h
 EXPORTS = [
     "igr_default_options", "igr_route_files", "igr_router_open", "igr_router_run", "igr_router_write",
+    "igr_router_evaluate",
     "igr_router_stats", "igr_router_kstats", "igr_router_sizes", "igr_router_route", "igr_router_pins",
     "igr_router_demand", "igr_router_close", "igr_router_plan", "igr_router_grid", "igr_set_device",
     "igr_generate", "igr_generate_custom", "igr_create", "igr_destroy", "igr_last_error", "igr_set_demand",
@@ -84,6 +85,7 @@ def lib() -> C.CDLL:
     L.igr_router_open.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(Options), C.POINTER(vp)]
     L.igr_router_run.argtypes = [vp]
     L.igr_router_write.argtypes = [vp, C.c_char_p]
+    L.igr_router_evaluate.argtypes = [vp, C.c_void_p, C.c_void_p]
     L.igr_router_stats.argtypes = [vp, _f64p, C.c_int]
     L.igr_router_kstats.argtypes = [vp, _f64p, C.c_int]
     L.igr_router_plan.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
@@ -212,6 +214,15 @@ class Router:
 
     def write(self, out: str) -> None:
         _check(lib().igr_router_write(self.h, out.encode()))
+
+    def evaluate(self) -> dict:
+        """Scores the last run on the device with the ISPD2024 evaluator's rules
+        (the FOR_STAT values before rounding, and the overflow loss per layer)."""
+        out = np.zeros(4, np.float64)
+        layers = np.zeros(9, np.float64)
+        _check(lib().igr_router_evaluate(self.h, out.ctypes.data_as(C.c_void_p), layers.ctypes.data_as(C.c_void_p)))
+        return dict(wirelength=float(out[0]), via=float(out[1]), overflow=float(out[2]), total=float(out[3]),
+                    layer_loss=layers)
 
     def stats(self) -> dict:
         v = np.zeros(len(STATS), dtype=np.float64)

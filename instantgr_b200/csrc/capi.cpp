@@ -115,6 +115,11 @@ int igr_router_write(igr_router *h, const char *out) {
     });
 }
 
+int igr_router_evaluate(igr_router *h, double *out, double *layer_loss) {
+    if (!h || !out) return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    return guard(&h->err, [&] { h->r.evaluate(out, layer_loss); });
+}
+
 int igr_router_stats(igr_router *h, double *o, int n) {
     if (!h || !o) return fail(nullptr, IGR_ERR_INVALID, "null argument");
     const auto &r = h->r;

@@ -199,6 +199,7 @@ bool cap_layers_parallel(Design &d, const char *buf, size_t n, size_t p0, int th
         if (c != (int64_t)XY) return false;
     }
     const int X = d.X, Y = d.Y;
+    std::atomic<bool> inexact{false};
     parallel_for(P, threads, [&](int b, int e) {
         for (int i = b; i < e; i++) {
             Piece &q = pc[i];
@@ -213,7 +214,9 @@ bool cap_layers_parallel(Design &d, const char *buf, size_t n, size_t p0, int th
                     else scale *= 10, ans = ans * 10 + (buf[k] - '0');
                 }
                 const int y = (int)(idx / X), x = (int)(idx % X);
-                cap[(size_t)x * Y + y] = (float)(scale == 0 ? ans : ans / scale);
+                const double v = scale == 0 ? ans : ans / scale;
+                cap[(size_t)x * Y + y] = (float)v;
+                if ((double)(float)v != v) inexact = true;
                 idx++;
                 q.last = k;
             }
@@ -233,6 +236,26 @@ bool cap_layers_parallel(Design &d, const char *buf, size_t n, size_t p0, int th
     for (int l = 0; l < L; l++) {
         d.layer_dir[l] = dir[l];
         d.layer_min_len[l] = minlen[l];
+    }
+    if (inexact) {  // rare: the exact values as well
+        d.cap_d.assign(d.cap.size(), 0.0);
+        parallel_for(P, threads, [&](int b, int e) {
+            for (int i = b; i < e; i++) {
+                const Piece &q = pc[i];
+                double *cap = d.cap_d.data() + (size_t)q.l * XY;
+                int64_t idx = q.first;
+                for (size_t k = q.a; k < q.e;) {
+                    if (!is_dig(buf[k])) { k++; continue; }
+                    double ans = 0, scale = 0;
+                    for (; k < q.e && in_run(buf[k]); k++) {
+                        if (buf[k] == '.') scale = 1;
+                        else scale *= 10, ans = ans * 10 + (buf[k] - '0');
+                    }
+                    cap[(size_t)(idx % X) * Y + (size_t)(idx / X)] = scale == 0 ? ans : ans / scale;
+                    idx++;
+                }
+            }
+        });
     }
     return true;
 }
@@ -266,6 +289,7 @@ void read_cap_buffer(Design &d, const char *buf, size_t n, int threads) {
     d.layer_dir.resize(d.L);
     d.layer_min_len.resize(d.L);
     d.cap.assign((size_t)d.L * d.X * d.Y, 0.f);
+    d.cap_d.clear();
     if (cap_layers_parallel(d, buf, n, s.p, threads)) return;
     for (int l = 0; l < d.L; l++) {
         size_t b, e;
@@ -276,7 +300,17 @@ void read_cap_buffer(Design &d, const char *buf, size_t n, int threads) {
         d.layer_min_len[l] = s.read_double();
         float *c = d.cap.data() + (size_t)l * d.X * d.Y;
         for (int y = 0; y < d.Y; y++)
-            for (int x = 0; x < d.X; x++) c[(size_t)x * d.Y + y] = (float)s.read_double();
+            for (int x = 0; x < d.X; x++) {
+                const double v = s.read_double();
+                c[(size_t)x * d.Y + y] = (float)v;
+                if ((double)(float)v != v) {
+                    if (d.cap_d.empty()) {  // rare: keep the exact values as well
+                        d.cap_d.resize(d.cap.size());
+                        for (size_t i = 0; i < d.cap.size(); i++) d.cap_d[i] = d.cap[i];
+                    }
+                }
+                if (!d.cap_d.empty()) d.cap_d[(size_t)l * d.X * d.Y + (size_t)x * d.Y + y] = v;
+            }
         if (l && d.layer_dir[l] == d.layer_dir[l - 1])
             throw Error(ERR_FORMAT, "layer directions must alternate");
     }

@@ -159,6 +159,34 @@ void launch_shape_count(const ShapeArgs &a, int *pt_off, int *claim_off, long lo
 void launch_shape_fill(const ShapeArgs &a, const int *pt_off, const int *claim_off, int *pts, int *claim,
                        cudaStream_t s);
 
+// ---- evaluation of a routing result with the ISPD2024 evaluator's rules (eval.cu)
+constexpr int kEvalLayers = 10;  // file layers: 0 (pins) and the 9 routing layers
+struct EvalDev {
+    int n = 0, L = 0, X = 0, Y = 0, DIR = 0;      // design nets, routing layers, grid
+    const int64_t *sel_off = nullptr, *extra_off = nullptr;  // pins and stacked-pin pairs per design net
+    const int *sel = nullptr, *extra = nullptr;   // file-layer 3-D positions
+    const int *sub_off = nullptr;                 // [n+1] routing nets of each design net
+    const int64_t *route_off = nullptr;           // route record of each routing net
+    const int *routes = nullptr;
+    const float *cap = nullptr;                   // routing-layer capacity (track layout)
+    const double *cap_d = nullptr;                // the same in double where a value is not a float
+    const int *xlen = nullptr, *ylen = nullptr;   // GCell widths along x and y
+    int *wire = nullptr, *stacked = nullptr;      // per routing cell (track layout)
+    unsigned long long *total_vias = nullptr;     // [kEvalLayers]
+    unsigned long long *wl = nullptr;             // [L] wire length per routing layer
+    unsigned long long *wkeys = nullptr, *vkeys = nullptr;  // hash sets of wire cells and via locations
+    unsigned long long wmask = 0, vmask = 0;      // table sizes - 1 (powers of two)
+    unsigned *vfirst = nullptr;                   // first position of each via location (by slot)
+    unsigned long long *vloc = nullptr;           // via locations in order
+    unsigned *vord = nullptr;                     // their line positions
+    int *err = nullptr;
+};
+void launch_eval_count(const EvalDev &e, long long *via_cnt, long long *cell_cnt, cudaStream_t s);
+void launch_eval_marks(const EvalDev &e, const long long *via_off, long long nloc, cudaStream_t s);
+int eval_blocks_per_layer(int64_t XY);
+// per (routing layer, block) overflow-loss partial sums into part[L * blocks]
+void launch_eval_cells(const EvalDev &e, int blocks_per_layer, double *part, cudaStream_t s);
+
 // ---- phase-1 plan from the colouring (plan.cu): routing-net ids batch by
 // batch in routing order (batches reversed), each batch split into the size
 // classes of the tree DP, nets of a class by node count (largest first)

@@ -37,6 +37,7 @@ struct Design {
     std::vector<int> layer_dir;             // [L] 0 = horizontal, 1 = vertical
     std::vector<double> layer_min_len;      // [L]
     std::vector<float> cap;                 // [L][X][Y] capacity (file layers)
+    std::vector<double> cap_d;              // the capacities as read, kept only when one is not a float
 
     // nets as read: CSR net -> pins -> access points
     std::vector<char> name_pool;

@@ -1277,6 +1277,88 @@ void Router::compute_score() {
     score_of = of;
 }
 
+void Router::evaluate(double *out, double *layer_loss) {
+    if (!ran) throw Error(ERR_STATE, "route before evaluating");
+    const int N = d.num_nets(), L = go.g.L, X = d.X, Y = d.Y;
+    const int64_t XY = (int64_t)X * Y;
+    EvalDev e;
+    e.n = N; e.L = L; e.X = X; e.Y = Y; e.DIR = go.g.DIR;
+    ev_sel_off.upload(d.sel_off, s); ev_sel.upload(d.sel, s);
+    ev_extra_off.upload(d.extra_off, s); ev_extra.upload(d.extra, s);
+    ev_sub_off.upload(ns.sub_off, s);
+    ev_route_off.upload(route_off, s);
+    e.sel_off = ev_sel_off.p; e.sel = ev_sel.p; e.extra_off = ev_extra_off.p; e.extra = ev_extra.p;
+    e.sub_off = ev_sub_off.p; e.route_off = ev_route_off.p; e.routes = routes.p;
+    e.cap = go.g.cap; e.xlen = go.g.xlen; e.ylen = go.g.ylen; e.err = go.g.err;
+    if (!d.cap_d.empty()) {  // capacities that are not floats: the exact values, in the track layout
+        ev_capd_ref.upload(d.cap_d.data() + XY, (size_t)L * XY, s);
+        ev_capd.alloc((size_t)L * XY);
+        launch_to_track_layout_d(go.g, ev_capd_ref.p, ev_capd.p, s);
+        e.cap_d = ev_capd.p;
+    }
+    ev_wire.alloc((size_t)go.g.N);
+    ev_stacked.alloc((size_t)go.g.N);
+    cuda_check(cudaMemsetAsync(ev_wire.p, 0, (size_t)go.g.N * sizeof(int), s), "memset");
+    cuda_check(cudaMemsetAsync(ev_stacked.p, 0, (size_t)go.g.N * sizeof(int), s), "memset");
+    ev_cnt.alloc(kEvalLayers + L);
+    cuda_check(cudaMemsetAsync(ev_cnt.p, 0, (kEvalLayers + L) * sizeof(unsigned long long), s), "memset");
+    e.wire = ev_wire.p; e.stacked = ev_stacked.p; e.total_vias = ev_cnt.p; e.wl = ev_cnt.p + kEvalLayers;
+    // counts per design net, then the via-location offsets and the table sizes
+    ev_vcnt.alloc(std::max(N, 1)); ev_ccnt.alloc(std::max(N, 1));
+    launch_eval_count(e, ev_vcnt.p, ev_ccnt.p, s);
+    std::vector<long long> vc(N), cc(N);
+    if (N) {
+        cuda_check(cudaMemcpyAsync(vc.data(), ev_vcnt.p, N * sizeof(long long), cudaMemcpyDeviceToHost, s), "D2H");
+        cuda_check(cudaMemcpyAsync(cc.data(), ev_ccnt.p, N * sizeof(long long), cudaMemcpyDeviceToHost, s), "D2H");
+    }
+    cuda_check(cudaStreamSynchronize(s), "evaluation counts");
+    std::vector<long long> voff(N + 1, 0);
+    long long ncell = 0;
+    for (int i = 0; i < N; i++) { voff[i + 1] = voff[i] + vc[i]; ncell += cc[i]; }
+    const long long nloc = voff[N];
+    if (N > (1 << 28) || X > 65535 || Y > 65535) throw Error(ERR_CAPACITY, "design too large for the evaluation keys");
+    auto table = [](long long n) {
+        unsigned long long t = 64;
+        while (t < 2ull * (unsigned long long)n) t <<= 1;
+        return t;
+    };
+    const unsigned long long wt = table(ncell), vt = table(nloc);
+    ev_voff.upload(voff.data(), N + 1, s);
+    ev_wkeys.alloc(wt); ev_vkeys.alloc(vt); ev_vfirst.alloc(vt);
+    ev_vloc.alloc(std::max<long long>(nloc, 1)); ev_vord.alloc(std::max<long long>(nloc, 1));
+    cuda_check(cudaMemsetAsync(ev_wkeys.p, 0xff, wt * 8, s), "memset");
+    cuda_check(cudaMemsetAsync(ev_vkeys.p, 0xff, vt * 8, s), "memset");
+    cuda_check(cudaMemsetAsync(ev_vfirst.p, 0xff, vt * 4, s), "memset");
+    e.wkeys = ev_wkeys.p; e.wmask = wt - 1; e.vkeys = ev_vkeys.p; e.vmask = vt - 1;
+    e.vfirst = ev_vfirst.p; e.vloc = ev_vloc.p; e.vord = ev_vord.p;
+    launch_eval_marks(e, ev_voff.p, nloc, s);
+    const int bpl = eval_blocks_per_layer(XY);
+    ev_part.alloc((size_t)bpl * L);
+    launch_eval_cells(e, bpl, ev_part.p, s);
+    std::vector<double> part((size_t)bpl * L);
+    std::vector<unsigned long long> cnt(kEvalLayers + L);
+    cuda_check(cudaMemcpyAsync(part.data(), ev_part.p, part.size() * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaMemcpyAsync(cnt.data(), ev_cnt.p, cnt.size() * 8, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaStreamSynchronize(s), "evaluation");
+    cuda_check(cudaGetLastError(), "evaluation launch");
+    if (int err = go.check_error(s)) throw Error(err, "device error in the evaluation");
+    // per file layer in the evaluator's order: layer 0 is not a routing layer
+    double wl_cost = 0, via_cost = 0, of_cost = 0;
+    via_cost += double(cnt[0]) * d.unit_via;
+    for (int z = 1; z <= L; z++) {
+        double layer = 0;
+        for (int b = 0; b < bpl; b++) layer += part[(size_t)(z - 1) * bpl + b];
+        if (layer_loss) layer_loss[z - 1] = layer;
+        of_cost += layer * d.short_cost[z];
+        via_cost += double(cnt[z < kEvalLayers ? z : kEvalLayers - 1]) * d.unit_via;
+        wl_cost += double(cnt[kEvalLayers + z - 1]) * d.unit_wire;
+    }
+    out[0] = wl_cost;
+    out[1] = via_cost;
+    out[2] = of_cost;
+    out[3] = of_cost + via_cost + wl_cost;
+}
+
 void Router::write(const char *out) {
     const double t0 = now_s();
     fetch_routes();

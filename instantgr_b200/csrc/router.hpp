@@ -254,6 +254,16 @@ struct Router {
     void open(const char *cap, const char *net);
     void run();
     void write(const char *out);
+    // Scores the last run with the ISPD2024 evaluator's rules on the device
+    // (run/evaluator.cpp:462-633): out = {wirelength cost, via cost, overflow
+    // cost, total}; layer_loss (optional, L entries) = overflow loss per routing layer.
+    void evaluate(double *out, double *layer_loss);
+    DevBuf<int64_t> ev_sel_off, ev_extra_off, ev_route_off;
+    DevBuf<int> ev_sel, ev_extra, ev_sub_off, ev_wire, ev_stacked;
+    DevBuf<long long> ev_vcnt, ev_ccnt, ev_voff;
+    DevBuf<unsigned long long> ev_cnt, ev_wkeys, ev_vkeys, ev_vloc;
+    DevBuf<unsigned> ev_vfirst, ev_vord;
+    DevBuf<double> ev_part, ev_capd, ev_capd_ref;
     void fetch_routes();
     const int *route_of(int net) const { return h_routes.p + route_off[net]; }
     void ensure_device();

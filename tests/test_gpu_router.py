@@ -43,6 +43,37 @@ def test_route_files_produces_connected_guides(small_design):
     assert tot == wl + via + of or abs(tot - (wl + via + of)) <= 2
 
 
+@pytest.mark.parametrize("rrr", [0, 3])
+def test_device_evaluation_matches_the_evaluator(small_design, rrr):
+    """igr_router_evaluate against the reference evaluator run on the written
+    guides: wire length and via costs exactly, overflow and total to the
+    evaluator's printed integers (sums of exp terms in another order)."""
+    cap, net, d = small_design
+    r = ig.Router(cap, net, rrr_iters=rrr)
+    r.run()
+    out = str(d / f"eval{rrr}.out")
+    r.write(out)
+    mine = r.evaluate()
+    r.close()
+    wl, via, of, tot = evaluate(cap, net, out)
+    assert round(mine["wirelength"]) == wl and round(mine["via"]) == via, (mine, wl, via)
+    assert abs(mine["overflow"] - of) <= 1 and abs(mine["total"] - tot) <= 1, (mine, of, tot)
+
+
+def test_device_evaluation_on_a_rerouted_design(tmp_path):
+    """The 256x256, 20k-net configuration with rip-up and reroute passes."""
+    cap, net, out = str(tmp_path / "c0.cap"), str(tmp_path / "c0.net"), str(tmp_path / "c0.out")
+    ig.generate(0, 3, 1.0, cap, net)
+    r = ig.Router(cap, net, rrr_iters=3)
+    r.run()
+    r.write(out)
+    mine = r.evaluate()
+    r.close()
+    wl, via, of, tot = evaluate(cap, net, out)
+    assert round(mine["wirelength"]) == wl and round(mine["via"]) == via, (mine, wl, via)
+    assert abs(mine["overflow"] - of) <= 1 and abs(mine["total"] - tot) <= 1, (mine, of, tot)
+
+
 def test_cli_matches_library(small_design):
     cap, net, d = small_design
     out1, out2 = str(d / "a.out"), str(d / "b.out")
