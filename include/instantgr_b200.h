@@ -300,7 +300,8 @@ int igr_seed_predict(igr_seed *m, int X, int Y, const float *features, float *pr
  * predicted overflow first.  The model must outlive the router's runs. */
 int igr_router_set_seed(igr_router *r, igr_seed *m, double alpha, int mode, int kind, int levels);
 /* Seed statistics of the last run: [0] 1 if the seeded result was kept (mode 2),
- * [1] seeded total score, [2] plain total score (mode 2), [3] prediction ms. */
+ * [1] seeded total score, [2] plain total score (mode 2), [3] prediction ms.
+ * Scores are the evaluator's totals (igr_router_evaluate). */
 int igr_router_seed_stats(igr_router *r, double *out, int n);
 /* One forward and backward pass on T tiles (x, target: [T][size][size][16])
  * without an update: loss and the gradient of every parameter (layout of

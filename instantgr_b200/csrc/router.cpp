@@ -456,20 +456,26 @@ void Router::run() {
         run_once(false);
         return;
     }
+    // scores are the evaluator's totals, computed on the device
+    auto total = [&] {
+        double v[4];
+        evaluate(v, nullptr);
+        return v[3];
+    };
     if (seed_mode == 1) {
         run_once(true);
         seed_used = true;
-        seed_scores[1] = score_wl + score_via + score_of;
+        seed_scores[1] = total();
         return;
     }
     // seeded run judged against the plain run: the better total score is kept
     const double t0 = now_s();
     run_once(true);
-    const double seeded_score = score_wl + score_via + score_of;
+    const double seeded_score = total();
     RouteBackup bk;
     save_result(bk);
     run_once(false);
-    const double plain_score = score_wl + score_via + score_of;
+    const double plain_score = total();
     seed_used = seeded_score < plain_score;
     if (seed_used) restore_result(bk);
     seed_scores[0] = plain_score;
