@@ -231,3 +231,18 @@ def test_capacity_reader_rejects_junk_before_a_layer_name(tmp_path):
     with pytest.raises(ig.IgrError) as e:
         ig.Router(str(cap), str(net))
     assert e.value.code == -3
+
+
+def test_router_refuses_to_write_or_evaluate_before_routing(tmp_path):
+    """Writing guides or scoring needs a routed result; both fail with IGR_ERR_STATE
+    (no GPU is needed to open a design or to get these errors)."""
+    cap, net = str(tmp_path / "t.cap"), str(tmp_path / "t.net")
+    ig.generate_custom(32, 32, 50, seed=3, cap_mode=0, block_frac=0.0, cap=cap, net=net)
+    r = ig.Router(cap, net)
+    with pytest.raises(ig.IgrError) as e:
+        r.evaluate()
+    assert e.value.code == -7
+    with pytest.raises(ig.IgrError) as e:
+        r.write(str(tmp_path / "t.out"))
+    assert e.value.code == -7
+    r.close()
