@@ -116,6 +116,13 @@ void *pinned_alloc(size_t bytes) {
     return p;
 }
 
+bool pinned_cached(size_t bytes) {
+    const size_t b = block_bytes(bytes);
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    auto it = g_pinned.lower_bound(b);
+    return it != g_pinned.end() && it->first <= 2 * b && !it->second.empty();
+}
+
 void pinned_free(void *p, size_t bytes) {
     if (!p) return;
     std::lock_guard<std::mutex> lock(g_pinned_mu);
@@ -632,9 +639,18 @@ void Router::run_once(bool seeded) {
 
 void Router::fetch_routes() {
     if (h_routes_valid) return;
-    h_routes.alloc((size_t)route_end);
+    // Page-locked memory copies fastest, but locking a large new block costs
+    // more than the copy it speeds up: a large first copy goes to pageable memory.
+    const size_t bytes = (size_t)route_end * sizeof(int);
+    if (bytes <= ((size_t)64 << 20) || (h_routes.p && h_routes.n >= (size_t)route_end) || pinned_cached(bytes)) {
+        h_routes.alloc((size_t)route_end);
+        h_routes_ptr = h_routes.p;
+    } else {
+        h_routes_pageable.resize((size_t)route_end);
+        h_routes_ptr = h_routes_pageable.data();
+    }
     if (route_end)
-        cuda_check(cudaMemcpyAsync(h_routes.p, routes.p, route_end * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
+        cuda_check(cudaMemcpyAsync(const_cast<int *>(h_routes_ptr), routes.p, bytes, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
     st.d2h_bytes += route_end * 4;
     h_routes_valid = true;

@@ -28,6 +28,8 @@ void dev_trim();
 // of results to the host.
 void *pinned_alloc(size_t bytes);
 void pinned_free(void *p, size_t bytes);
+// true when the cache holds a page-locked block for `bytes`
+bool pinned_cached(size_t bytes);
 
 template <typename T>
 struct PinnedBuf {
@@ -182,7 +184,9 @@ struct Router {
     DevBuf<int> routes;
     DevBuf<int64_t> d_route_off, d_old_off;
     DevBuf<int> d_route_cap;
-    PinnedBuf<int> h_routes;    // host copy of the route records, made on demand
+    PinnedBuf<int> h_routes;    // host copy of the route records, made on demand: page-locked ...
+    std::vector<int> h_routes_pageable;  // ... or, for a large first copy, pageable
+    const int *h_routes_ptr = nullptr;
     bool h_routes_valid = false;
     // ---- per-run device buffers (grow-only)
     DevBuf<int4> d_hdr;
@@ -265,7 +269,7 @@ struct Router {
     DevBuf<unsigned> ev_vfirst, ev_vord;
     DevBuf<double> ev_part, ev_capd, ev_capd_ref;
     void fetch_routes();
-    const int *route_of(int net) const { return h_routes.p + route_off[net]; }
+    const int *route_of(int net) const { return h_routes_ptr + route_off[net]; }
     void ensure_device();
     void device_shapes(const ShapeArgs &a, ShapeDev &sd);
     DevBuf<long long> d_shape_tot;
