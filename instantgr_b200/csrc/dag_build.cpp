@@ -50,7 +50,7 @@ struct Builder {
     DagNet &out;
     int X, Y, XY;
     const TreeAdj &G;                        // tree adjacency
-    const std::vector<int> &P;               // tree node positions (3-D, Steiner layer 9)
+    const std::pmr::vector<int> &P;          // tree node positions (3-D, Steiner layer 9)
     int ntree;
     float ratio;
     int num_tracks;

@@ -12,10 +12,12 @@
 //     direction (r & 1) ^ DIR with DIR = direction of file layer 1.
 #pragma once
 #include <cstdint>
+#include <functional>
+#include <memory>
+#include <memory_resource>
+#include <stdexcept>
 #include <string>
 #include <vector>
-#include <stdexcept>
-#include <functional>
 
 #include "status.hpp"
 
@@ -74,7 +76,8 @@ void select_pins(Design &d, int threads);
 // Adjacency of a tree in CSR form: the neighbours of node i are
 // nb[off[i] .. off[i+1]), in the order the edges were added.
 struct TreeAdj {
-    std::vector<int> off{0}, nb;
+    std::pmr::vector<int> off, nb;
+    explicit TreeAdj(std::pmr::memory_resource *r = std::pmr::get_default_resource()) : off(1, 0, r), nb(r) {}
     struct Row {
         const int *b, *e;
         const int *begin() const { return b; }
@@ -90,13 +93,16 @@ struct TreeAdj {
 
 // A routing net ("subnet") is a net of >= 2 selected pins, split at
 // MAX_PIN_SIZE = 12 pins along its Steiner tree (src/database_cuda.hpp:2111-2237).
+// Its arrays come from the memory resource it is made with (the net set's pool,
+// so that a whole net set is freed at once).
 struct RNet {
     int orig = -1;                 // design net id
     int hpwl = 0, minx = 0, maxx = 0, miny = 0, maxy = 0;
-    std::vector<int> pins;         // routing-layer 3-D positions
+    std::pmr::vector<int> pins;    // routing-layer 3-D positions
     // Steiner tree: adjacency over nodes, node positions (3-D, Steiner -> layer L)
     TreeAdj adj;
-    std::vector<int> tnode;
+    std::pmr::vector<int> tnode;
+    explicit RNet(std::pmr::memory_resource *r = std::pmr::get_default_resource()) : pins(r), adj(r), tnode(r) {}
 };
 
 // 2-D conflict shapes of a routing net for batch colouring (net::construct_rsmt,
@@ -137,6 +143,9 @@ void for_each_shape(const RNet &n, int X, int Y, Pt &&point, Hs &&hseg, Vs &&vse
 
 struct NetSet {
     int L = 0, X = 0, Y = 0, DIR = 0;   // routing layers (L = 9)
+    // the nets' arrays: one arena per range of design nets, filled by one thread
+    // at a time and freed as a whole (declared before the nets: freed after them)
+    std::vector<std::unique_ptr<std::pmr::monotonic_buffer_resource>> arenas;
     std::vector<RNet> nets;
     std::vector<int> sub_off;                // [design nets + 1]: routing nets sub_off[n] .. sub_off[n+1]
     std::vector<int> unfinished;             // design net -> subnets still routing

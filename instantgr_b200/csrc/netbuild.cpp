@@ -14,6 +14,8 @@
 #include "steiner_core.hpp"
 
 #include <algorithm>
+#include <mutex>
+#include <new>
 #include <numeric>
 #include <tuple>
 #include <unordered_map>
@@ -24,7 +26,7 @@ namespace {
 
 // Tree over the distinct 2-D positions of `pos2d` (my_flute, database_cuda.hpp:696-744).
 void tree_from_positions(const Design &d, int Y, const std::vector<int> &pos2d, TreeAdj &graph,
-                         std::vector<int> &nodes) {
+                         std::pmr::vector<int> &nodes) {
     std::vector<int> x, y;
     x.reserve(pos2d.size()); y.reserve(pos2d.size());
     for (int e : pos2d) { x.push_back(d.dr_x[e / Y]); y.push_back(d.dr_y[e % Y]); }
@@ -68,6 +70,43 @@ void tree_from_positions(const Design &d, int Y, const std::vector<int> &pos2d, 
         }
     }
     graph.from_edges((int)nodes.size(), kept);
+}
+
+// Upstream of the net arenas: blocks given back stay mapped and are handed out
+// again (rounded up to powers of two), so that the next design opened in this
+// process reuses them instead of faulting in new pages.
+class BlockCache final : public std::pmr::memory_resource {
+    std::mutex mu_;
+    std::vector<std::vector<void *>> free_;  // by log2 of the block size
+    static int cls(size_t b) {
+        int c = 12;
+        while (((size_t)1 << c) < b) c++;
+        return c;
+    }
+    void *do_allocate(size_t bytes, size_t align) override {
+        const int c = cls(std::max(bytes, align));
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            if (c < (int)free_.size() && !free_[c].empty()) {
+                void *p = free_[c].back();
+                free_[c].pop_back();
+                return p;
+            }
+        }
+        return ::operator new((size_t)1 << c, std::align_val_t(std::max<size_t>(align, 64)));
+    }
+    void do_deallocate(void *p, size_t bytes, size_t align) override {
+        const int c = cls(std::max(bytes, align));
+        std::lock_guard<std::mutex> lock(mu_);
+        if ((int)free_.size() <= c) free_.resize(c + 1);
+        free_[c].push_back(p);
+    }
+    bool do_is_equal(const std::pmr::memory_resource &o) const noexcept override { return this == &o; }
+};
+
+std::pmr::memory_resource *block_cache() {
+    static BlockCache *c = new BlockCache;  // never destroyed: arenas may outlive static destruction
+    return c;
 }
 
 }  // namespace
@@ -134,6 +173,7 @@ namespace {
 // Splits one design net with more than MAX_PIN_SIZE pins along its tree
 // (database_cuda.hpp:2130-2228).
 void split_net(const Design &d, const NetSet &ns, int db_id, std::vector<RNet> &out) {
+    std::pmr::memory_resource *res = std::pmr::get_default_resource();
     const int MAX_PIN_SIZE = 12;
     const int X = ns.X, Y = ns.Y, XY = X * Y, L = ns.L;
     RNet tmp;
@@ -191,14 +231,14 @@ void split_net(const Design &d, const NetSet &ns, int db_id, std::vector<RNet> &
     }
     for (int i = 0; i < n; i++) {
         if (find(i) != i) continue;
-        RNet s;
+        RNet s(res);
         s.orig = db_id;
         std::unordered_map<int, int> indx;
         for (int j = 0; j < (int)new_pins[i].size(); j++) {
             if (new_pins[i][j] < L * XY) s.pins.push_back(new_pins[i][j]);
             indx[new_pins[i][j]] = j;
         }
-        s.tnode = new_pins[i];
+        s.tnode.assign(new_pins[i].begin(), new_pins[i].end());
         std::vector<std::pair<int, int>> se;
         se.reserve(net_edge[i].size());
         for (int j : net_edge[i]) {
@@ -216,7 +256,15 @@ void split_net(const Design &d, const NetSet &ns, int db_id, std::vector<RNet> &
 
 void build_netset(const Design &d, NetSet &ns, int threads) {
     ns.L = d.L - 1; ns.X = d.X; ns.Y = d.Y; ns.DIR = d.layer_dir[1];
+    ns.nets.clear();
+    ns.arenas.clear();
     const int N = d.num_nets(), XY = d.X * d.Y;
+    if (threads <= 0) threads = hw_threads();
+    // tasks: ranges of design nets, each with its own arena
+    const int T = std::max(1, std::min(N, 8 * threads));
+    for (int t = 0; t < T; t++)
+        ns.arenas.push_back(std::make_unique<std::pmr::monotonic_buffer_resource>(block_cache()));
+    auto task_begin = [&](int t) { return (int)((int64_t)N * t / T); };
     // nets of more than 12 pins are split first (in parallel); every other
     // multi-pin net is one routing net
     std::vector<int> big;
@@ -236,12 +284,15 @@ void build_netset(const Design &d, NetSet &ns, int threads) {
     }
     const int R = ns.sub_off[N];
     ns.nets.clear();
-    ns.nets.resize(R);
+    ns.nets.reserve(R);
+    for (int t = 0; t < T; t++)
+        for (int r = ns.sub_off[task_begin(t)]; r < ns.sub_off[task_begin(t + 1)]; r++)
+            ns.nets.emplace_back(ns.arenas[t].get());
     std::vector<int> part_of(N, -1);
     for (int k = 0; k < (int)big.size(); k++) part_of[big[k]] = k;
     // routing nets in design-net order; trees of every routing net (Lshape_route.hpp:159-163)
-    parallel_for(N, threads, [&](int b, int e) {
-        for (int id = b; id < e; id++) {
+    parallel_for(T, threads, [&](int tb, int te) {
+        for (int id = task_begin(tb); id < task_begin(te); id++) {
             const int r0 = ns.sub_off[id], r1 = ns.sub_off[id + 1];
             if (r0 == r1) continue;
             if (part_of[id] >= 0) {
