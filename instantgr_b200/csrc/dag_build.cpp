@@ -461,7 +461,7 @@ struct Builder {
             out.nodes[k] = nodes[idx];
             k++;
         }
-        out.points = points;
+        out.points.assign(points.begin(), points.end());
     }
 };
 
@@ -469,7 +469,10 @@ struct Builder {
 
 void build_dag(const NetSet &ns, const RNet &n, const CongestionView &cv, int mode, DagNet &out) {
     thread_local Scratch scratch;
-    out = DagNet();
+    // the arrays are rewritten below; out keeps its memory resource
+    out.par_nodes.clear();
+    out.child_idx.clear();
+    out.points.clear();
     Builder b(ns, n, cv, mode, out, scratch);
     b.build();
 }

@@ -163,22 +163,28 @@ void flatten_tree(const RNet &n, int *nodes, int *par);
 
 // ---------------------------------------------------------------- detour DAG
 // Per-net detour DAG (src/database_cuda.hpp:1429-2086), in topological order.
+// Its arrays come from the memory resource it is made with.
 struct DagNet {
-    std::vector<int> nodes;        // 3-D positions (routing layer; virtual = 9)
-    std::vector<int> par_num;      // parents per node
-    std::vector<int> par_sum;      // [n+1]
-    std::vector<int> par_nodes;    // parent node (local index) per parent slot
-    std::vector<int> child_idx;    // child slot of this node in the parent
-    std::vector<int> child_num;    // children per node
-    std::vector<int> depth;        // depth per node
-    std::vector<int> points;       // 2-D conflict points
-    std::vector<std::pair<int, int>> hseg, vseg;
+    std::pmr::vector<int> nodes;      // 3-D positions (routing layer; virtual = 9)
+    std::pmr::vector<int> par_num;    // parents per node
+    std::pmr::vector<int> par_sum;    // [n+1]
+    std::pmr::vector<int> par_nodes;  // parent node (local index) per parent slot
+    std::pmr::vector<int> child_idx;  // child slot of this node in the parent
+    std::pmr::vector<int> child_num;  // children per node
+    std::pmr::vector<int> depth;      // depth per node
+    std::pmr::vector<int> points;     // 2-D conflict points
+    explicit DagNet(std::pmr::memory_resource *r = std::pmr::get_default_resource())
+        : nodes(r), par_num(r), par_sum(r), par_nodes(r), child_idx(r), child_num(r), depth(r), points(r) {}
 };
 struct CongestionView {            // host copy of the 2-D congestion prefix sums
     int X = 0, Y = 0;
     std::vector<float> xsum, ysum;
 };
 void build_dag(const NetSet &ns, const RNet &n, const CongestionView &cv, int mode, DagNet &out);
+// Process-wide cache of host memory blocks for arenas: blocks given back stay
+// mapped and are handed out again (powers of two), so that arenas made one
+// after another reuse their pages.
+std::pmr::memory_resource *host_block_cache();
 
 // ---------------------------------------------------------------- Steiner provider
 // Rectilinear Steiner tree of a point set; deterministic and independent of the

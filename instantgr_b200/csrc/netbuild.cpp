@@ -104,12 +104,12 @@ class BlockCache final : public std::pmr::memory_resource {
     bool do_is_equal(const std::pmr::memory_resource &o) const noexcept override { return this == &o; }
 };
 
-std::pmr::memory_resource *block_cache() {
+}  // namespace
+
+std::pmr::memory_resource *host_block_cache() {
     static BlockCache *c = new BlockCache;  // never destroyed: arenas may outlive static destruction
     return c;
 }
-
-}  // namespace
 
 void TreeAdj::from_edges(int n, const std::vector<std::pair<int, int>> &edges) {
     off.assign(n + 1, 0);
@@ -263,7 +263,7 @@ void build_netset(const Design &d, NetSet &ns, int threads) {
     // tasks: ranges of design nets, each with its own arena
     const int T = std::max(1, std::min(N, 8 * threads));
     for (int t = 0; t < T; t++)
-        ns.arenas.push_back(std::make_unique<std::pmr::monotonic_buffer_resource>(block_cache()));
+        ns.arenas.push_back(std::make_unique<std::pmr::monotonic_buffer_resource>(host_block_cache()));
     auto task_begin = [&](int t) { return (int)((int64_t)N * t / T); };
     // nets of more than 12 pins are split first (in parallel); every other
     // multi-pin net is one routing net

@@ -143,6 +143,22 @@ bool cuda_driver_ready() {
     return ready;
 }
 
+namespace {
+// host array without value initialisation
+template <typename T>
+struct HostArray {
+    std::unique_ptr<T[]> p;
+    size_t n = 0;
+    explicit HostArray(size_t count) : p(new T[count ? count : 1]), n(count) {}
+    T *data() { return p.get(); }
+    const T *data() const { return p.get(); }
+    size_t size() const { return n; }
+    T &operator[](size_t i) { return p[i]; }
+    const T &operator[](size_t i) const { return p[i]; }
+    T *begin() { return p.get(); }
+};
+}  // namespace
+
 // ------------------------------------------------------------------ grid
 void GridOwner::create(int L, int X, int Y, int DIR, const int *xl, const int *yl, double unit_wire,
                        double unit_via, const double *sc, const float *cap_ref, cudaStream_t s) {
@@ -1046,13 +1062,23 @@ bool Router::rrr_pass(int iter) {
     }
     // detour DAGs on host threads (Lshape_route_detour.hpp:702-748)
     const double th0 = now_s();
-    // DAGs of the rerouted nets only, by their position in of_nets
-    dag.resize(of_nets.size());
+    // DAGs of the rerouted nets only, by their position in of_nets; their arrays
+    // come from one arena per range of nets, emptied at the next pass
+    const int K = (int)of_nets.size();
+    const int T = std::max(1, std::min(K, 8 * (threads > 0 ? threads : hw_threads())));
+    auto task_begin = [&](int t) { return (int)((int64_t)K * t / T); };
+    dag.clear();
+    for (auto &a : dag_arenas) a->release();
+    while ((int)dag_arenas.size() < T)
+        dag_arenas.push_back(std::make_unique<std::pmr::monotonic_buffer_resource>(host_block_cache()));
+    dag.reserve(K);
+    for (int t = 0; t < T; t++)
+        for (int k = task_begin(t); k < task_begin(t + 1); k++) dag.emplace_back(dag_arenas[t].get());
     dag_slot.assign(R, -1);
     for (size_t k = 0; k < of_nets.size(); k++) dag_slot[of_nets[k]] = (int)k;
     std::vector<char> keep(of_nets.size(), 1);
-    parallel_for((int)of_nets.size(), threads, [&](int b, int e) {
-        for (int k = b; k < e; k++) {
+    parallel_for(T, threads, [&](int tb, int te) {
+        for (int k = task_begin(tb); k < task_begin(te); k++) {
             DagNet &dn = dag[k];
             build_dag(ns, ns.nets[of_nets[k]], cv, mode_eff, dn);
             // the DP keeps at most 10 child slots per node (the reference packs the
@@ -1144,8 +1170,9 @@ bool Router::rrr_pass(int iter) {
         }
         tot = acc;
     }
-    std::vector<int> nodes(tot.nb), par_off(tot.pb), par(tot.eb), cslot(tot.eb), echild(tot.eb), child_off(tot.pb);
-    std::vector<int> level_off(tot.lb), level_nodes(tot.nb), net_node_off(tot.nnb), net_ids(tot.nets),
+    // every entry is written below: left uninitialised (these reach billions of entries)
+    HostArray<int> nodes(tot.nb), par_off(tot.pb), par(tot.eb), cslot(tot.eb), echild(tot.eb), child_off(tot.pb);
+    HostArray<int> level_off(tot.lb), level_nodes(tot.nb), net_node_off(tot.nnb), net_ids(tot.nets),
         net_level_off(tot.nnb);
     parallel_for(B, threads, [&](int b0, int e0) {
         std::vector<int> dep, b_nodes, b_off, b_net;
@@ -1198,8 +1225,16 @@ bool Router::rrr_pass(int iter) {
             nd.push_back(dmax);
             nw.push_back(dmax ? *std::max_element(w.begin(), w.end()) : 0);
         }
-        auto q = [](std::vector<int> v, double p) {
-            std::sort(v.begin(), v.end());
+        for (auto *v : {&nn, &nd, &nw}) {  // counting sort: the values are small
+            int mx = 0;
+            for (int x : *v) mx = std::max(mx, x);
+            std::vector<int64_t> h((size_t)mx + 2, 0);
+            for (int x : *v) h[x]++;
+            size_t k = 0;
+            for (int x = 0; x <= mx; x++)
+                for (int64_t c = 0; c < h[x]; c++) (*v)[k++] = x;
+        }
+        auto q = [](const std::vector<int> &v, double p) {  // v sorted
             return v.empty() ? 0 : v[std::min(v.size() - 1, (size_t)(p * (v.size() - 1) + 0.5))];
         };
         std::fprintf(stderr,
@@ -1210,10 +1245,13 @@ bool Router::rrr_pass(int iter) {
     }
     const double t_csr = now_s();
     grow_routes(route_end);
-    dg_nodes.upload(nodes, s); dg_paroff.upload(par_off, s); dg_par.upload(par, s); dg_cslot.upload(cslot, s);
-    dg_echild.upload(echild, s); dg_childoff.upload(child_off, s); dg_leveloff.upload(level_off, s);
-    dg_levelnodes.upload(level_nodes, s); dg_nno.upload(net_node_off, s); dg_ids.upload(net_ids, s);
-    dg_netlvl.upload(net_level_off, s);
+    dg_nodes.upload(nodes.data(), nodes.size(), s); dg_paroff.upload(par_off.data(), par_off.size(), s);
+    dg_par.upload(par.data(), par.size(), s); dg_cslot.upload(cslot.data(), cslot.size(), s);
+    dg_echild.upload(echild.data(), echild.size(), s); dg_childoff.upload(child_off.data(), child_off.size(), s);
+    dg_leveloff.upload(level_off.data(), level_off.size(), s);
+    dg_levelnodes.upload(level_nodes.data(), level_nodes.size(), s);
+    dg_nno.upload(net_node_off.data(), net_node_off.size(), s); dg_ids.upload(net_ids.data(), net_ids.size(), s);
+    dg_netlvl.upload(net_level_off.data(), net_level_off.size(), s);
     d_old_off.upload(old_off, s);
     d_route_off.upload(route_off, s);
     d_route_cap.upload(route_cap, s);

@@ -224,6 +224,8 @@ struct Router {
         dg_netlvl, dg_ids, dg_bchange, dg_lout, dg_stage, dg_scnt;
     DevBuf<double> dg_costs, dg_cedges;
     DevBuf<unsigned long long> dg_best, dg_packed;
+    // arenas of the DAG arrays (declared before the DAGs: freed after them)
+    std::vector<std::unique_ptr<std::pmr::monotonic_buffer_resource>> dag_arenas;
     std::vector<DagNet> dag;     // detour DAGs of the nets rerouted in the current pass
     std::vector<int> dag_slot;   // routing net -> its DAG in `dag`, -1 when not rerouted
     unsigned long long cost_cells = 0, commit_cells = 0;
