@@ -144,18 +144,22 @@ bool cuda_driver_ready() {
 }
 
 namespace {
-// host array without value initialisation
+// host staging array without value initialisation, in cached page-locked
+// memory (uploads at full speed; pages reused by the next pass)
 template <typename T>
 struct HostArray {
-    std::unique_ptr<T[]> p;
+    T *p = nullptr;
     size_t n = 0;
-    explicit HostArray(size_t count) : p(new T[count ? count : 1]), n(count) {}
-    T *data() { return p.get(); }
-    const T *data() const { return p.get(); }
+    explicit HostArray(size_t count) : p(static_cast<T *>(pinned_alloc((count ? count : 1) * sizeof(T)))), n(count) {}
+    ~HostArray() { pinned_free(p, (n ? n : 1) * sizeof(T)); }
+    HostArray(const HostArray &) = delete;
+    HostArray &operator=(const HostArray &) = delete;
+    T *data() { return p; }
+    const T *data() const { return p; }
     size_t size() const { return n; }
     T &operator[](size_t i) { return p[i]; }
     const T &operator[](size_t i) const { return p[i]; }
-    T *begin() { return p.get(); }
+    T *begin() { return p; }
 };
 }  // namespace
 
@@ -1136,12 +1140,14 @@ bool Router::rrr_pass(int iter) {
     const int B = (int)batches.size();
     std::vector<BInfo> bi(B);
     std::vector<int64_t> old_off = route_off;
-    std::vector<int> net_levels(of_nets.size());  // depth + 1 of each net's DAG
+    std::vector<int> net_levels(of_nets.size()), net_slots(of_nets.size());  // depth + 1, child slots
     parallel_for((int)of_nets.size(), threads, [&](int b0, int e0) {
         for (int k = b0; k < e0; k++) {
-            int D = 0;
+            int D = 0, sl = 0;
             for (int dv : dag[k].depth) D = std::max(D, dv + 1);
+            for (int c : dag[k].child_num) sl += c;
             net_levels[k] = D;
+            net_slots[k] = sl;
         }
     });
     BInfo tot{};
@@ -1157,7 +1163,7 @@ bool Router::rrr_pass(int iter) {
                 const DagNet &dn = dag[k];
                 f.n += (int)dn.nodes.size();
                 f.e += (int)dn.par_nodes.size();
-                for (int c : dn.child_num) f.slots += c;
+                f.slots += net_slots[k];
                 lv += net_levels[k] + 1;
                 // new route record of the net (appended)
                 route_cap[id] = 8 * (int)dn.nodes.size() + 1;
@@ -1166,6 +1172,9 @@ bool Router::rrr_pass(int iter) {
             }
             if ((int64_t)f.n * 100 + 99 > 0x7fffffffLL) throw Error(ERR_CAPACITY, "DAG batch too large for 32-bit node ids");
             const int nn = (int)batches[b].size();
+            const int64_t big = std::max({(int64_t)acc.pb + f.n + 1, (int64_t)acc.eb + f.e, (int64_t)acc.lb + lv,
+                                          (int64_t)acc.nnb + nn + 1});
+            if (big > 0x7fffffffLL) throw Error(ERR_CAPACITY, "DAG arrays of one rip-up pass exceed 32-bit offsets");
             acc.nb += f.n; acc.eb += f.e; acc.pb += f.n + 1; acc.lb += lv; acc.nnb += nn + 1; acc.nets += nn;
         }
         tot = acc;
