@@ -159,6 +159,13 @@ void launch_shape_count(const ShapeArgs &a, int *pt_off, int *claim_off, long lo
 void launch_shape_fill(const ShapeArgs &a, const int *pt_off, const int *claim_off, int *pts, int *claim,
                        cudaStream_t s);
 
+// ---- dense copy of the live route records (records.cu): record lengths and
+// their exclusive scan into off[0..n] (off: [n+1]), then the copy into dense
+void launch_record_offsets(const int *routes, const int64_t *route_off, int n, int64_t end, int64_t *off,
+                           cudaStream_t s);
+void launch_record_copy(const int *routes, const int64_t *route_off, int n, const int64_t *off, int *dense,
+                        cudaStream_t s);
+
 // ---- evaluation of a routing result with the ISPD2024 evaluator's rules (eval.cu)
 constexpr int kEvalLayers = 10;  // file layers: 0 (pins) and the 9 routing layers
 struct EvalDev {

@@ -659,20 +659,40 @@ void Router::run_once(bool seeded) {
 
 void Router::fetch_routes() {
     if (h_routes_valid) return;
+    const int R = (int)route_off.size();
+    h_route_at.assign((size_t)R + 1, 0);
+    if (route_end == 0 || R == 0) {
+        h_routes_ptr = nullptr;
+        h_routes_valid = true;
+        return;
+    }
+    // Records sit at offsets with room for their largest size, and each
+    // rip-up pass appends new ones: pack the live records on the device
+    // (lengths, scan, copy) and bring only those and their offsets back.
+    d_fetch_off.upload(route_off, s);
+    d_dense_off.alloc((size_t)R + 1);
+    launch_record_offsets(routes.p, d_fetch_off.p, R, route_end, d_dense_off.p, s);
+    cuda_check(cudaMemcpyAsync(h_route_at.data(), d_dense_off.p, ((size_t)R + 1) * 8, cudaMemcpyDeviceToHost, s),
+               "D2H");
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    const int64_t live = h_route_at[R];
+    d_dense.alloc((size_t)live);
+    launch_record_copy(routes.p, d_fetch_off.p, R, d_dense_off.p, d_dense.p, s);
     // Page-locked memory copies fastest, but locking a large new block costs
     // more than the copy it speeds up: a large first copy goes to pageable memory.
-    const size_t bytes = (size_t)route_end * sizeof(int);
-    if (bytes <= ((size_t)64 << 20) || (h_routes.p && h_routes.n >= (size_t)route_end) || pinned_cached(bytes)) {
-        h_routes.alloc((size_t)route_end);
+    const size_t bytes = (size_t)live * sizeof(int);
+    if (bytes <= ((size_t)64 << 20) || (h_routes.p && h_routes.n >= (size_t)live) || pinned_cached(bytes)) {
+        h_routes.alloc((size_t)live);
         h_routes_ptr = h_routes.p;
     } else {
-        h_routes_pageable.resize((size_t)route_end);
+        h_routes_pageable.resize((size_t)live);
         h_routes_ptr = h_routes_pageable.data();
     }
-    if (route_end)
-        cuda_check(cudaMemcpyAsync(const_cast<int *>(h_routes_ptr), routes.p, bytes, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaMemcpyAsync(const_cast<int *>(h_routes_ptr), d_dense.p, bytes, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
-    st.d2h_bytes += route_end * 4;
+    if (bytes > ((size_t)256 << 20)) d_dense.release();  // a large packed copy gives its HBM back
+    st.d2h_bytes += (int64_t)bytes + ((int64_t)R + 1) * 8;
+    st.launches += 3;
     h_routes_valid = true;
 }
 

@@ -184,10 +184,15 @@ struct Router {
     DevBuf<int> routes;
     DevBuf<int64_t> d_route_off, d_old_off;
     DevBuf<int> d_route_cap;
-    PinnedBuf<int> h_routes;    // host copy of the route records, made on demand: page-locked ...
+    // host copy of the live route records, packed on the device and made on
+    // demand: page-locked ...
+    PinnedBuf<int> h_routes;
     std::vector<int> h_routes_pageable;  // ... or, for a large first copy, pageable
     const int *h_routes_ptr = nullptr;
+    std::vector<int64_t> h_route_at;     // [R+1] record of each routing net in the host copy
     bool h_routes_valid = false;
+    DevBuf<int64_t> d_fetch_off, d_dense_off;
+    DevBuf<int> d_dense;
     // ---- per-run device buffers (grow-only)
     DevBuf<int4> d_hdr;
     DevBuf<int> d_vcnt;  // via crossings per cell of the current phase-1 batch (fused commit)
@@ -271,7 +276,7 @@ struct Router {
     DevBuf<unsigned> ev_vfirst, ev_vord;
     DevBuf<double> ev_part, ev_capd, ev_capd_ref;
     void fetch_routes();
-    const int *route_of(int net) const { return h_routes_ptr + route_off[net]; }
+    const int *route_of(int net) const { return h_routes_ptr + h_route_at[net]; }
     void ensure_device();
     void device_shapes(const ShapeArgs &a, ShapeDev &sd);
     DevBuf<long long> d_shape_tot;

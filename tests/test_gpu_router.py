@@ -159,3 +159,30 @@ def test_score_close_to_reference_router(tmp_path):
         mine = evaluate(cap, net, out)[3]
         theirs = float(rec["for_stat"].split()[4])
         assert mine <= theirs * 1.005, (name, mine, theirs)
+
+
+def test_route_records_after_rerouting(tmp_path):
+    """Records read back one net at a time after rip-up passes on the 256x256,
+    20k-net configuration (the records are packed on the device before the
+    copy): every record well formed, wires straight, vias on one GCell, and
+    the same records from a second router."""
+    cap, net = str(tmp_path / "c0.cap"), str(tmp_path / "c0.net")
+    ig.generate(0, 3, 1.0, cap, net)
+    X = Y = 256
+    recs = []
+    for _ in range(2):
+        r = ig.Router(cap, net, rrr_iters=3)
+        r.run()
+        _, rn = r.sizes()
+        recs.append([r.route(k) for k in range(rn)])
+        assert r.stats()["rerouted"] > 0
+        r.close()
+    assert all(np.array_equal(a, b) for a, b in zip(*recs))
+    XY = X * Y
+    for rec in recs[0]:
+        assert rec[0] == len(rec) and rec[0] % 2 == 1
+        a, b = rec[1::2], rec[2::2]
+        xa, ya, xb, yb = a % XY // Y, a % Y, b % XY // Y, b % Y
+        via = a // XY != b // XY
+        assert np.all(~via | ((xa == xb) & (ya == yb)))
+        assert np.all(via | (xa == xb) | (ya == yb))
