@@ -55,7 +55,9 @@ typedef struct igr_options {
     int profile;       /* 1 = time every kernel launch with CUDA events (igr_router_kstats) */
     int split_commit;  /* 1 = phase-1 batches commit wires and vias and refresh costs in three
                           launches instead of one fused per-track pass (same results) */
-    int reserved[6];
+    int host_dags;     /* 1 = detour DAGs and the per-batch DAG arrays of the rip-up passes are
+                          built on the host threads instead of the device (same results) */
+    int reserved[5];
 } igr_options;
 
 /* Fills `o` with the defaults that reproduce InstantGR (1 RRR pass). */
@@ -249,6 +251,20 @@ int igr_dag_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t *nod
  * cap < *len. */
 int igr_build_dag(int X, int Y, int mode, int ntree, const int32_t *pos, const int32_t *adj_off, const int32_t *adj,
                   const float *xsum, const float *ysum, int32_t *out, int64_t cap, int64_t *len);
+
+/* Detour DAGs of n trees built on the device, one thread per tree (the
+ * construction of igr_build_dag, which it replaces for the rip-up passes of
+ * the router: Lshape_route_detour.hpp:702-748 calls
+ * net::generate_detours_reconstruct, src/database_cuda.hpp:1429-2086, per
+ * net on host threads).  Tree k: nodes tree_off[k] .. tree_off[k+1]-1 of
+ * pos[]; node v's neighbours adj[adj_off[v] .. adj_off[v+1]) as indices
+ * local to its tree (adj_off has tree_off[n] + 1 entries).  The records, in
+ * igr_build_dag's format, are written end to end to out; rec_off[n+1]
+ * receives their offsets and *len the total length; nothing is written to
+ * out when cap < *len.  Needs a GPU. */
+int igr_build_dags(int X, int Y, int mode, int n, const int32_t *tree_off, const int32_t *pos,
+                   const int32_t *adj_off, const int32_t *adj, const float *xsum, const float *ysum, int32_t *out,
+                   int64_t cap, int64_t *rec_off, int64_t *len);
 
 /* Steiner provider used in place of FLUTE (flute::flute, src/flute.hpp:1239;
  * its POST9.dat table is absent).  Nodes: distinct input points in ascending

@@ -43,7 +43,8 @@ EXPORTS = [
     "igr_get_demand", "igr_get_stamp", "igr_get_pre", "igr_cost_refresh", "igr_get_costs", "igr_set_costs",
     "igr_pattern_route", "igr_pattern_route_static", "igr_commit_wires", "igr_commit_vias", "igr_ripup_wires",
     "igr_mark_overflow",
-    "igr_congestion_view", "igr_score", "igr_color_batches", "igr_dag_route", "igr_build_dag", "igr_steiner",
+    "igr_congestion_view", "igr_score", "igr_color_batches", "igr_dag_route", "igr_build_dag", "igr_build_dags",
+    "igr_steiner",
     "igr_seed_create", "igr_seed_destroy", "igr_seed_last_error", "igr_seed_set_tile", "igr_seed_params",
     "igr_seed_set_params", "igr_seed_features", "igr_seed_add_map", "igr_seed_add_routed", "igr_seed_train",
     "igr_seed_eval", "igr_seed_predict", "igr_seed_grad", "igr_router_set_seed", "igr_router_seed_stats",
@@ -53,7 +54,7 @@ EXPORTS = [
 class Options(C.Structure):
     _fields_ = [("rrr_iters", C.c_int), ("threads", C.c_int), ("mode", C.c_int), ("verbose", C.c_int),
                 ("batched", C.c_int), ("profile", C.c_int), ("split_commit", C.c_int),
-                ("reserved", C.c_int * 6)]
+                ("host_dags", C.c_int), ("reserved", C.c_int * 5)]
 
 
 class GridDesc(C.Structure):
@@ -124,6 +125,8 @@ def lib() -> C.CDLL:
                                 _i32p, C.c_int32]
     L.igr_build_dag.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _i32p, _f32p, _f32p, _i32p,
                                 C.c_int64, C.POINTER(C.c_int64)]
+    L.igr_build_dags.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _i32p, _i32p, _f32p, _f32p,
+                                 vp, C.c_int64, _i64p, C.POINTER(C.c_int64)]
     L.igr_steiner.argtypes = [C.c_int, _i32p, _i32p, _i32p, _i32p, C.c_int, C.POINTER(C.c_int), _i32p,
                               C.c_int, C.POINTER(C.c_int)]
     L.igr_router_set_seed.argtypes = [vp, vp, C.c_double, C.c_int, C.c_int, C.c_int]
@@ -430,6 +433,23 @@ class Ctx:
                                     _i32(par_off), _i32(par), _i32(child_slot), _i32(child_num), _i64(route_off),
                                     _i32(route_cap), routes, stamp))
         return routes
+
+
+def build_dags(X, Y, mode, tree_off, pos, adj_off, adj, xsum, ysum):
+    """Detour DAGs of many trees built on the device (igr_build_dags); returns the
+    records of build_dag end to end and their offsets [n+1]."""
+    tree_off, pos, adj_off, adj = _i32(tree_off), _i32(pos), _i32(adj_off), _i32(adj)
+    xs = np.ascontiguousarray(xsum, dtype=np.float32)
+    ys = np.ascontiguousarray(ysum, dtype=np.float32)
+    n = len(tree_off) - 1
+    rec_off = np.zeros(n + 1, dtype=np.int64)
+    total = C.c_int64()
+    _check(lib().igr_build_dags(X, Y, mode, n, tree_off, pos, adj_off, adj, xs, ys, None, 0, rec_off,
+                                C.byref(total)))
+    out = np.zeros(max(total.value, 1), dtype=np.int32)
+    _check(lib().igr_build_dags(X, Y, mode, n, tree_off, pos, adj_off, adj, xs, ys,
+                                out.ctypes.data_as(C.c_void_p), total.value, rec_off, C.byref(total)))
+    return out[: total.value], rec_off
 
 
 def build_dag(X, Y, mode, pos, adj_off, adj, xsum, ysum):

@@ -23,9 +23,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CUDA_INC = "/usr/local/cuda/include"
 
 CU_SOURCES = ["cost.cu", "commit.cu", "ripup.cu", "pattern.cu", "pattern_static.cu", "color.cu", "dag.cu", "plan.cu",
-              "seed_nn.cu", "shapes.cu", "eval.cu", "records.cu"]
-CPP_SOURCES = ["design_io.cpp", "pins.cpp", "netbuild.cpp", "gen.cpp", "dag_build.cpp", "router.cpp", "capi.cpp",
-               "seed_model.cpp"]
+              "seed_nn.cu", "shapes.cu", "eval.cu", "records.cu", "dagbuild.cu"]
+CPP_SOURCES = ["design_io.cpp", "pins.cpp", "netbuild.cpp", "gen.cpp", "dag_build.cpp", "dag_device.cpp", "router.cpp",
+               "capi.cpp", "seed_model.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # --fmad=false: the only multiply-add the reference contracts is written as fma() explicitly
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-Xptxas", "-v"] + ARCH

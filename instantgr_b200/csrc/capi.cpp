@@ -86,6 +86,7 @@ static void apply_options(Router &r, const igr_options *o) {
     r.verbose = o->verbose;
     r.batched = o->batched;
     r.split_commit = o->split_commit;
+    r.host_dags = o->host_dags;
     r.kt.on = o->profile != 0;
 }
 
@@ -728,6 +729,80 @@ int igr_build_dag(int X, int Y, int mode, int ntree, const int32_t *pos, const i
         v.insert(v.end(), dn.points.begin(), dn.points.end());
         *len = (int64_t)v.size();
         if (out && cap >= *len) std::memcpy(out, v.data(), v.size() * 4);
+    });
+}
+
+int igr_build_dags(int X, int Y, int mode, int n, const int32_t *tree_off, const int32_t *pos,
+                   const int32_t *adj_off, const int32_t *adj, const float *xsum, const float *ysum, int32_t *out,
+                   int64_t cap, int64_t *rec_off, int64_t *len) {
+    if (n < 0 || !tree_off || !xsum || !ysum || !len || !rec_off || X < 2 || Y < 2 || (n > 0 && (!pos || !adj_off || !adj)))
+        return fail(nullptr, IGR_ERR_INVALID, "bad arguments");
+    return guard(nullptr, [&] {
+        if (tree_off[0] != 0) throw Error(ERR_INVALID, "tree offsets must start at 0");
+        for (int k = 0; k < n; k++) {
+            const int a = tree_off[k], b = tree_off[k + 1];
+            if (b - a < 2) throw Error(ERR_INVALID, "a tree needs at least two nodes");
+            for (int v = a; v < b; v++) {
+                if (pos[v] < 0 || pos[v] >= 10 * X * Y) throw Error(ERR_INVALID, "node position out of range");
+                if (adj_off[v + 1] < adj_off[v]) throw Error(ERR_INVALID, "adjacency offsets must not decrease");
+                for (int q = adj_off[v]; q < adj_off[v + 1]; q++)
+                    if (adj[q] < 0 || adj[q] >= b - a) throw Error(ERR_INVALID, "adjacency out of range");
+            }
+        }
+        const int total = n ? tree_off[n] : 0;
+        cudaStream_t s = nullptr;
+        cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+        struct StreamGuard {
+            cudaStream_t s;
+            ~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+        } sg{s};
+        DevBuf<int> d_off, d_pos, d_aoff, d_adj, d_ids;
+        DevBuf<float> d_xs, d_ys;
+        std::vector<int> ids(n);
+        std::iota(ids.begin(), ids.end(), 0);
+        d_off.upload(tree_off, (size_t)n + 1, s);
+        d_pos.upload(pos, (size_t)std::max(total, 1), s);
+        d_aoff.upload(adj_off, (size_t)total + 1, s);
+        d_adj.upload(adj, (size_t)std::max(adj_off[total], 1), s);
+        d_ids.upload(ids, s);
+        d_xs.upload(xsum, (size_t)X * Y, s);
+        d_ys.upload(ysum, (size_t)X * Y, s);
+        DagBuildArgs a;
+        a.tree_off = d_off.p; a.pos = d_pos.p; a.adj_off = d_aoff.p; a.adj = d_adj.p;
+        a.xsum = d_xs.p; a.ysum = d_ys.p; a.X = X; a.Y = Y; a.mode = mode;
+        a.ids = d_ids.p; a.n_list = n;
+        DeviceDags dd;
+        dd.measure(a, s);
+        dd.write(a, ids, s);  // every DAG, in order (no slot rule here)
+        const size_t nn = (size_t)dd.h_node_at[n], ne = (size_t)dd.h_edge_at[n], np = (size_t)dd.h_point_at[n];
+        std::vector<int> nodes(nn), pnum(nn), cnum(nn), dep(nn), par(ne), cidx(ne), pts(np);
+        auto down = [&](std::vector<int> &h, const DevBuf<int> &d) {
+            if (!h.empty()) cuda_check(cudaMemcpyAsync(h.data(), d.p, h.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
+        };
+        down(nodes, dd.nodes); down(pnum, dd.par_num); down(cnum, dd.child_num); down(dep, dd.depth);
+        down(par, dd.par); down(cidx, dd.child_idx); down(pts, dd.points);
+        cuda_check(cudaStreamSynchronize(s), "sync");
+        int64_t L = 0;
+        for (int k = 0; k < n; k++) {
+            rec_off[k] = L;
+            L += 3 + 4 * (dd.h_node_at[k + 1] - dd.h_node_at[k]) + 2 * (dd.h_edge_at[k + 1] - dd.h_edge_at[k]) +
+                 (dd.h_point_at[k + 1] - dd.h_point_at[k]);
+        }
+        rec_off[n] = L;
+        *len = L;
+        if (!out || cap < L) return;
+        for (int k = 0; k < n; k++) {
+            int32_t *o = out + rec_off[k];
+            const int64_t a0 = dd.h_node_at[k], m = dd.h_node_at[k + 1] - a0;
+            const int64_t e0 = dd.h_edge_at[k], E = dd.h_edge_at[k + 1] - e0;
+            const int64_t p0 = dd.h_point_at[k], P = dd.h_point_at[k + 1] - p0;
+            *o++ = (int32_t)m;
+            for (auto *v : {&nodes, &pnum, &cnum, &dep}) o = std::copy(v->begin() + a0, v->begin() + a0 + m, o);
+            *o++ = (int32_t)E;
+            for (auto *v : {&par, &cidx}) o = std::copy(v->begin() + e0, v->begin() + e0 + E, o);
+            *o++ = (int32_t)P;
+            o = std::copy(pts.begin() + p0, pts.begin() + p0 + P, o);
+        }
     });
 }
 

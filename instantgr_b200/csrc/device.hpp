@@ -159,6 +159,55 @@ void launch_shape_count(const ShapeArgs &a, int *pt_off, int *claim_off, long lo
 void launch_shape_fill(const ShapeArgs &a, const int *pt_off, const int *claim_off, int *pts, int *claim,
                        cudaStream_t s);
 
+// ---- detour DAGs on the device (dagbuild.cu)
+// slice sizes of one builder thread's work area: tree nodes, stem entries,
+// mirror entries, DAG nodes, links, conflict points (before deduplication)
+struct DagCaps {
+    int tc = 32, sc = 512, mc = 512, nc = 512, ec = 1024, pc = 2048;
+};
+constexpr int kDagSizeFields = 7;  // per DAG: nodes, links, points, depth levels, child slots, widest slot, status
+struct DagBuildArgs {
+    int n_list = 0;
+    const int *list = nullptr;      // DAGs to build (positions k); null: 0..n_list-1
+    const int *ids = nullptr;       // [k] routing net of DAG k
+    const int *tree_off = nullptr;  // [R+1] tree nodes of each routing net, in adjacency order
+    const int *pos = nullptr;       // tree node positions (3-D; Steiner nodes on layer 9)
+    const int *adj_off = nullptr;   // [tree nodes + 1] neighbour list of each tree node
+    const int *adj = nullptr;       // neighbours (net-local indices)
+    const float *xsum = nullptr, *ysum = nullptr;  // congestion view [X][Y]
+    int X = 0, Y = 0, mode = 2;
+    DagCaps caps;
+    int *work = nullptr;            // threads x dag_work_ints(caps)
+    int *sizes = nullptr;           // size pass: [k][kDagSizeFields]
+    // write pass: layout [k+1] and the per-DAG arrays
+    const long long *node_at = nullptr, *edge_at = nullptr, *point_at = nullptr;
+    int *out_nodes = nullptr, *out_par_num = nullptr, *out_child_num = nullptr, *out_depth = nullptr;
+    int *out_par = nullptr, *out_child_idx = nullptr, *out_points = nullptr;
+    int *err = nullptr;
+};
+long long dag_work_ints(const DagCaps &c);
+void launch_dag_build(const DagBuildArgs &a, int threads, cudaStream_t s);
+// one builder per block: work area in shared memory (a.work null, at most
+// dag_solo_smem_limit() bytes) or in global memory (builders x slices)
+void launch_dag_build_solo(const DagBuildArgs &a, int builders, cudaStream_t s);
+int dag_solo_smem_limit();
+// batch layout: per net (in batch order) its DAG k, batch-local node base,
+// edge base, slot base, level base, position in the batch and batch; per
+// batch its first node, edge, node+1, level and net entries and first net
+constexpr int kDagDescFields = 7;
+constexpr int kDagBatchFields = 6;
+struct DagGatherArgs {
+    int n = 0;
+    const int *desc = nullptr, *batch = nullptr, *ids = nullptr;
+    const long long *node_at = nullptr, *edge_at = nullptr;
+    const int *src_nodes = nullptr, *src_par_num = nullptr, *src_child_num = nullptr, *src_depth = nullptr;
+    const int *src_par = nullptr, *src_child_idx = nullptr;
+    int *nodes = nullptr, *par_off = nullptr, *par = nullptr, *child_slot = nullptr, *edge_child = nullptr,
+        *child_off = nullptr, *level_off = nullptr, *level_nodes = nullptr, *net_node_off = nullptr,
+        *net_ids = nullptr, *net_level_off = nullptr;
+};
+void launch_dag_gather(const DagGatherArgs &a, cudaStream_t s);
+
 // ---- dense copy of the live route records (records.cu): record lengths and
 // their exclusive scan into off[0..n] (off: [n+1]), then the copy into dense
 void launch_record_offsets(const int *routes, const int64_t *route_off, int n, int64_t end, int64_t *off,

@@ -29,6 +29,7 @@ int main(int argc, char **argv) {
         else if (a == "--threads") o.threads = std::atoi(val("--threads"));
         else if (a == "--mode") o.mode = std::atoi(val("--mode"));
         else if (a == "--batched") o.batched = 1;
+        else if (a == "--host-dags") o.host_dags = 1;
         else if (a == "--verbose") o.verbose = 1;
         else {
             std::fprintf(stderr, "unknown argument %s\n", a.c_str());

@@ -1053,8 +1053,10 @@ bool Router::rrr_pass(int iter) {
     std::vector<uint8_t> is_of(R);
     CongestionView cv;
     cv.X = X; cv.Y = Y;
-    cv.xsum.resize((size_t)X * Y);
-    cv.ysum.resize((size_t)X * Y);
+    if (host_dags) {
+        cv.xsum.resize((size_t)X * Y);
+        cv.ysum.resize((size_t)X * Y);
+    }
     cuda_check(cudaMemcpyAsync(is_of.data(), d_is_of.p, R, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
     st.d2h_bytes += R;
@@ -1069,10 +1071,12 @@ bool Router::rrr_pass(int iter) {
     launch_congestion_view(go.g, d_xsum.p, d_ysum.p, s);
     kt.end(KC_RIPUP);
     st.launches += 3;
-    cuda_check(cudaMemcpyAsync(cv.xsum.data(), d_xsum.p, cv.xsum.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
-    cuda_check(cudaMemcpyAsync(cv.ysum.data(), d_ysum.p, cv.ysum.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
-    cuda_check(cudaStreamSynchronize(s), "sync");
-    st.d2h_bytes += (int64_t)X * Y * 8;
+    if (host_dags) {  // the host builder reads the view from host memory
+        cuda_check(cudaMemcpyAsync(cv.xsum.data(), d_xsum.p, cv.xsum.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
+        cuda_check(cudaMemcpyAsync(cv.ysum.data(), d_ysum.p, cv.ysum.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
+        cuda_check(cudaStreamSynchronize(s), "sync");
+        st.d2h_bytes += (int64_t)X * Y * 8;
+    }
     if (seed_active) {
         // predicted congestion first, then HPWL (the reference's order)
         std::vector<double> pr(R, 0.0);
@@ -1084,215 +1088,224 @@ bool Router::rrr_pass(int iter) {
     } else {
         std::sort(of_nets.begin(), of_nets.end(), [&](int l, int r) { return ns.nets[l].hpwl > ns.nets[r].hpwl; });
     }
-    // detour DAGs on host threads (Lshape_route_detour.hpp:702-748)
-    const double th0 = now_s();
-    // DAGs of the rerouted nets only, by their position in of_nets; their arrays
-    // come from one arena per range of nets, emptied at the next pass
-    const int K = (int)of_nets.size();
-    const int T = std::max(1, std::min(K, 8 * (threads > 0 ? threads : hw_threads())));
-    auto task_begin = [&](int t) { return (int)((int64_t)K * t / T); };
-    dag.clear();
-    for (auto &a : dag_arenas) a->release();
-    while ((int)dag_arenas.size() < T)
-        dag_arenas.push_back(std::make_unique<std::pmr::monotonic_buffer_resource>(host_block_cache()));
-    dag.reserve(K);
-    for (int t = 0; t < T; t++)
-        for (int k = task_begin(t); k < task_begin(t + 1); k++) dag.emplace_back(dag_arenas[t].get());
-    dag_slot.assign(R, -1);
-    for (size_t k = 0; k < of_nets.size(); k++) dag_slot[of_nets[k]] = (int)k;
-    std::vector<char> keep(of_nets.size(), 1);
-    parallel_for(T, threads, [&](int tb, int te) {
-        for (int k = task_begin(tb); k < task_begin(te); k++) {
-            DagNet &dn = dag[k];
-            build_dag(ns, ns.nets[of_nets[k]], cv, mode_eff, dn);
-            // the DP keeps at most 10 child slots per node (the reference packs the
-            // slot as a decimal digit); nets beyond that keep their current route
-            for (int c : dn.child_num)
-                if (c > 10) keep[k] = 0;
-        }
-    });
-    {
-        std::vector<int> kept;
-        for (size_t k = 0; k < of_nets.size(); k++)
-            if (keep[k]) kept.push_back(of_nets[k]);
-        of_nets.swap(kept);
-    }
-    st.dag_host_ms += (now_s() - th0) * 1e3;
-    const double t_dag = now_s();
-    if (of_nets.empty()) return false;
-    // colouring on DAG points and tree segments (Lshape_route_detour.hpp:751)
-    // conflict shapes of the rerouted nets: their DAG points and their trees'
-    // segments; claim lists built on the device
-    std::vector<int> pt_off(of_nets.size() + 1, 0), pts;
-    for (size_t k = 0; k < of_nets.size(); k++) pt_off[k + 1] = pt_off[k] + (int)dag[dag_slot[of_nets[k]]].points.size();
-    pts.resize(pt_off.back());
-    parallel_for((int)of_nets.size(), threads, [&](int b, int e) {
-        for (int k = b; k < e; k++) {
-            const auto &p = dag[dag_slot[of_nets[k]]].points;
-            std::copy(p.begin(), p.end(), pts.begin() + pt_off[k]);
-        }
-    });
-    d2_ptoff.upload(pt_off, s);
-    d2_pts.upload(pts, s);
-    d2_ids.upload(of_nets, s);
-    st.h2d_bytes += (int64_t)(pt_off.size() + pts.size() + of_nets.size()) * 4;
-    ShapeDev shd;
-    {
-        ShapeArgs a;
-        a.tree_off = d_tree_off.p; a.tree_nodes = d_tree_nodes.p; a.tree_par = d_tree_par.p;
-        a.ids = d2_ids.p; a.ext_off = d2_ptoff.p; a.ext_pts = d2_pts.p;
-        a.n = (int)of_nets.size(); a.X = X; a.Y = Y; a.sparsity = mode_eff >= 1 ? 2 : 15;
-        device_shapes(a, shd);
-    }
-    std::vector<int> local(of_nets.size());
-    std::iota(local.begin(), local.end(), 0);  // shape k belongs to of_nets[k]; of_nets is in priority order
-    std::vector<std::vector<int>> lb;
-    const double t_shapes = now_s();
-    color_nets(local, shd, mode_eff >= 1 ? 2 : 15, lb);
-    const double t_color = now_s();
-    std::vector<std::vector<int>> batches(lb.size());
-    for (size_t b = 0; b < lb.size(); b++)
-        for (int k : lb[b]) batches[b].push_back(of_nets[k]);
-    std::reverse(batches.begin(), batches.end());
-    // batch-local CSR of all batches, laid end to end: sizes per net and batch
-    // first, then every batch filled on its own thread
-    struct BInfo { int nb, eb, pb, lb, nnb, nets, n, e, slots; };
-    const int B = (int)batches.size();
-    std::vector<BInfo> bi(B);
+    // per colour batch: its first entries in the arrays of the pass and its sizes
+    std::vector<std::vector<int>> batches;
+    std::vector<DagBatchInfo> bi;
     std::vector<int64_t> old_off = route_off;
-    std::vector<int> net_levels(of_nets.size()), net_slots(of_nets.size());  // depth + 1, child slots
-    parallel_for((int)of_nets.size(), threads, [&](int b0, int e0) {
-        for (int k = b0; k < e0; k++) {
-            int D = 0, sl = 0;
-            for (int dv : dag[k].depth) D = std::max(D, dv + 1);
-            for (int c : dag[k].child_num) sl += c;
-            net_levels[k] = D;
-            net_slots[k] = sl;
-        }
-    });
-    BInfo tot{};
-    {
-        BInfo acc{};
-        for (int b = 0; b < B; b++) {
-            BInfo &f = bi[b];
-            f = acc;
-            f.n = f.e = f.slots = 0;
-            int lv = 0;
-            for (int id : batches[b]) {
-                const int k = dag_slot[id];
-                const DagNet &dn = dag[k];
-                f.n += (int)dn.nodes.size();
-                f.e += (int)dn.par_nodes.size();
-                f.slots += net_slots[k];
-                lv += net_levels[k] + 1;
-                // new route record of the net (appended)
-                route_cap[id] = 8 * (int)dn.nodes.size() + 1;
-                route_off[id] = route_end;
-                route_end += route_cap[id];
+    double th0 = now_s(), t_dag = 0, t_shapes = 0, t_color = 0, t_csr = 0;
+    if (!host_dags) {
+        double tm[4];
+        if (!dags_on_device(of_nets, batches, bi, old_off, tm)) return false;
+        t_dag = tm[0]; t_shapes = tm[1]; t_color = tm[2]; t_csr = tm[3];
+    } else {
+        // detour DAGs on host threads (Lshape_route_detour.hpp:702-748)
+        th0 = now_s();
+        // DAGs of the rerouted nets only, by their position in of_nets; their arrays
+        // come from one arena per range of nets, emptied at the next pass
+        const int K = (int)of_nets.size();
+        const int T = std::max(1, std::min(K, 8 * (threads > 0 ? threads : hw_threads())));
+        auto task_begin = [&](int t) { return (int)((int64_t)K * t / T); };
+        dag.clear();
+        for (auto &a : dag_arenas) a->release();
+        while ((int)dag_arenas.size() < T)
+            dag_arenas.push_back(std::make_unique<std::pmr::monotonic_buffer_resource>(host_block_cache()));
+        dag.reserve(K);
+        for (int t = 0; t < T; t++)
+            for (int k = task_begin(t); k < task_begin(t + 1); k++) dag.emplace_back(dag_arenas[t].get());
+        dag_slot.assign(R, -1);
+        for (size_t k = 0; k < of_nets.size(); k++) dag_slot[of_nets[k]] = (int)k;
+        std::vector<char> keep(of_nets.size(), 1);
+        parallel_for(T, threads, [&](int tb, int te) {
+            for (int k = task_begin(tb); k < task_begin(te); k++) {
+                DagNet &dn = dag[k];
+                build_dag(ns, ns.nets[of_nets[k]], cv, mode_eff, dn);
+                // the DP keeps at most 10 child slots per node (the reference packs the
+                // slot as a decimal digit); nets beyond that keep their current route
+                for (int c : dn.child_num)
+                    if (c > 10) keep[k] = 0;
             }
-            if ((int64_t)f.n * 100 + 99 > 0x7fffffffLL) throw Error(ERR_CAPACITY, "DAG batch too large for 32-bit node ids");
-            const int nn = (int)batches[b].size();
-            const int64_t big = std::max({(int64_t)acc.pb + f.n + 1, (int64_t)acc.eb + f.e, (int64_t)acc.lb + lv,
-                                          (int64_t)acc.nnb + nn + 1});
-            if (big > 0x7fffffffLL) throw Error(ERR_CAPACITY, "DAG arrays of one rip-up pass exceed 32-bit offsets");
-            acc.nb += f.n; acc.eb += f.e; acc.pb += f.n + 1; acc.lb += lv; acc.nnb += nn + 1; acc.nets += nn;
+        });
+        {
+            std::vector<int> kept;
+            for (size_t k = 0; k < of_nets.size(); k++)
+                if (keep[k]) kept.push_back(of_nets[k]);
+            of_nets.swap(kept);
         }
-        tot = acc;
-    }
-    // every entry is written below: left uninitialised (these reach billions of entries)
-    HostArray<int> nodes(tot.nb), par_off(tot.pb), par(tot.eb), cslot(tot.eb), echild(tot.eb), child_off(tot.pb);
-    HostArray<int> level_off(tot.lb), level_nodes(tot.nb), net_node_off(tot.nnb), net_ids(tot.nets),
-        net_level_off(tot.nnb);
-    parallel_for(B, threads, [&](int b0, int e0) {
-        std::vector<int> dep, b_nodes, b_off, b_net;
-        for (int b = b0; b < e0; b++) {
-            const BInfo &f = bi[b];
-            dep.resize(f.n);
-            int e = 0, sl = 0, base = 0;
-            par_off[f.pb] = 0;
-            child_off[f.pb] = 0;
-            net_node_off[f.nnb] = 0;
-            int j = 0;
-            for (int id : batches[b]) {
-                const DagNet &dn = dag[dag_slot[id]];
-                const int m = (int)dn.nodes.size();
-                for (int v = 0; v < m; v++) {
-                    nodes[f.nb + base + v] = dn.nodes[v];
-                    for (int q = dn.par_sum[v]; q < dn.par_sum[v + 1]; q++) {
-                        par[f.eb + e] = base + dn.par_nodes[q];
-                        cslot[f.eb + e] = dn.child_idx[q];
-                        echild[f.eb + e] = base + v;
-                        e++;
-                    }
-                    par_off[f.pb + base + v + 1] = e;
-                    sl += dn.child_num[v];
-                    child_off[f.pb + base + v + 1] = sl;
-                    dep[base + v] = dn.depth[v];
+        st.dag_host_ms += (now_s() - th0) * 1e3;
+        t_dag = now_s();
+        if (of_nets.empty()) return false;
+        // colouring on DAG points and tree segments (Lshape_route_detour.hpp:751)
+        // conflict shapes of the rerouted nets: their DAG points and their trees'
+        // segments; claim lists built on the device
+        std::vector<int> pt_off(of_nets.size() + 1, 0), pts;
+        for (size_t k = 0; k < of_nets.size(); k++) pt_off[k + 1] = pt_off[k] + (int)dag[dag_slot[of_nets[k]]].points.size();
+        pts.resize(pt_off.back());
+        parallel_for((int)of_nets.size(), threads, [&](int b, int e) {
+            for (int k = b; k < e; k++) {
+                const auto &p = dag[dag_slot[of_nets[k]]].points;
+                std::copy(p.begin(), p.end(), pts.begin() + pt_off[k]);
+            }
+        });
+        d2_ptoff.upload(pt_off, s);
+        d2_pts.upload(pts, s);
+        d2_ids.upload(of_nets, s);
+        st.h2d_bytes += (int64_t)(pt_off.size() + pts.size() + of_nets.size()) * 4;
+        ShapeDev shd;
+        {
+            ShapeArgs a;
+            a.tree_off = d_tree_off.p; a.tree_nodes = d_tree_nodes.p; a.tree_par = d_tree_par.p;
+            a.ids = d2_ids.p; a.ext_off = d2_ptoff.p; a.ext_pts = d2_pts.p;
+            a.n = (int)of_nets.size(); a.X = X; a.Y = Y; a.sparsity = mode_eff >= 1 ? 2 : 15;
+            device_shapes(a, shd);
+        }
+        std::vector<int> local(of_nets.size());
+        std::iota(local.begin(), local.end(), 0);  // shape k belongs to of_nets[k]; of_nets is in priority order
+        std::vector<std::vector<int>> lb;
+        t_shapes = now_s();
+        color_nets(local, shd, mode_eff >= 1 ? 2 : 15, lb);
+        t_color = now_s();
+        batches.assign(lb.size(), {});
+        for (size_t b = 0; b < lb.size(); b++)
+            for (int k : lb[b]) batches[b].push_back(of_nets[k]);
+        std::reverse(batches.begin(), batches.end());
+        // batch-local CSR of all batches, laid end to end: sizes per net and batch
+        // first, then every batch filled on its own thread
+        const int B = (int)batches.size();
+        bi.assign(B, DagBatchInfo{});
+        std::vector<int> net_levels(of_nets.size()), net_slots(of_nets.size());  // depth + 1, child slots
+        parallel_for((int)of_nets.size(), threads, [&](int b0, int e0) {
+            for (int k = b0; k < e0; k++) {
+                int D = 0, sl = 0;
+                for (int dv : dag[k].depth) D = std::max(D, dv + 1);
+                for (int c : dag[k].child_num) sl += c;
+                net_levels[k] = D;
+                net_slots[k] = sl;
+            }
+        });
+        DagBatchInfo tot{};
+        {
+            DagBatchInfo acc{};
+            for (int b = 0; b < B; b++) {
+                DagBatchInfo &f = bi[b];
+                f = acc;
+                f.n = f.e = f.slots = 0;
+                int lv = 0;
+                for (int id : batches[b]) {
+                    const int k = dag_slot[id];
+                    const DagNet &dn = dag[k];
+                    f.n += (int)dn.nodes.size();
+                    f.e += (int)dn.par_nodes.size();
+                    f.slots += net_slots[k];
+                    lv += net_levels[k] + 1;
+                    // new route record of the net (appended)
+                    route_cap[id] = 8 * (int)dn.nodes.size() + 1;
+                    route_off[id] = route_end;
+                    route_end += route_cap[id];
                 }
-                base += m;
-                net_ids[f.nets + j] = id;
-                net_node_off[f.nnb + j + 1] = base;
-                j++;
+                if ((int64_t)f.n * 100 + 99 > 0x7fffffffLL) throw Error(ERR_CAPACITY, "DAG batch too large for 32-bit node ids");
+                const int nn = (int)batches[b].size();
+                const int64_t big = std::max({(int64_t)acc.pb + f.n + 1, (int64_t)acc.eb + f.e, (int64_t)acc.lb + lv,
+                                              (int64_t)acc.nnb + nn + 1});
+                if (big > 0x7fffffffLL) throw Error(ERR_CAPACITY, "DAG arrays of one rip-up pass exceed 32-bit offsets");
+                acc.nb += f.n; acc.eb += f.e; acc.pb += f.n + 1; acc.lb += lv; acc.nnb += nn + 1; acc.nets += nn;
             }
-            // levels of each net of the batch (batch-local positions)
-            dag_levels(j, net_node_off.data() + f.nnb, dep.data(), b_nodes, b_off, b_net);
-            std::copy(b_nodes.begin(), b_nodes.end(), level_nodes.begin() + f.nb);
-            std::copy(b_off.begin(), b_off.end(), level_off.begin() + f.lb);
-            std::copy(b_net.begin(), b_net.end(), net_level_off.begin() + f.nnb);
+            tot = acc;
         }
-    });
-    if (verbose) {
-        // shape of the DAGs: nodes and depth per net, widest level of one net
-        std::vector<int> nn, nd, nw;
-        for (int id : of_nets) {
-            const DagNet &dn = dag[dag_slot[id]];
-            int dmax = 0;
-            for (int dv : dn.depth) dmax = std::max(dmax, dv + 1);
-            std::vector<int> w(dmax, 0);
-            for (int dv : dn.depth) w[dv]++;
-            nn.push_back((int)dn.nodes.size());
-            nd.push_back(dmax);
-            nw.push_back(dmax ? *std::max_element(w.begin(), w.end()) : 0);
+        // every entry is written below: left uninitialised (these reach billions of entries)
+        HostArray<int> nodes(tot.nb), par_off(tot.pb), par(tot.eb), cslot(tot.eb), echild(tot.eb), child_off(tot.pb);
+        HostArray<int> level_off(tot.lb), level_nodes(tot.nb), net_node_off(tot.nnb), net_ids(tot.nets),
+            net_level_off(tot.nnb);
+        parallel_for(B, threads, [&](int b0, int e0) {
+            std::vector<int> dep, b_nodes, b_off, b_net;
+            for (int b = b0; b < e0; b++) {
+                const DagBatchInfo &f = bi[b];
+                dep.resize(f.n);
+                int e = 0, sl = 0, base = 0;
+                par_off[f.pb] = 0;
+                child_off[f.pb] = 0;
+                net_node_off[f.nnb] = 0;
+                int j = 0;
+                for (int id : batches[b]) {
+                    const DagNet &dn = dag[dag_slot[id]];
+                    const int m = (int)dn.nodes.size();
+                    for (int v = 0; v < m; v++) {
+                        nodes[f.nb + base + v] = dn.nodes[v];
+                        for (int q = dn.par_sum[v]; q < dn.par_sum[v + 1]; q++) {
+                            par[f.eb + e] = base + dn.par_nodes[q];
+                            cslot[f.eb + e] = dn.child_idx[q];
+                            echild[f.eb + e] = base + v;
+                            e++;
+                        }
+                        par_off[f.pb + base + v + 1] = e;
+                        sl += dn.child_num[v];
+                        child_off[f.pb + base + v + 1] = sl;
+                        dep[base + v] = dn.depth[v];
+                    }
+                    base += m;
+                    net_ids[f.nets + j] = id;
+                    net_node_off[f.nnb + j + 1] = base;
+                    j++;
+                }
+                // levels of each net of the batch (batch-local positions)
+                dag_levels(j, net_node_off.data() + f.nnb, dep.data(), b_nodes, b_off, b_net);
+                std::copy(b_nodes.begin(), b_nodes.end(), level_nodes.begin() + f.nb);
+                std::copy(b_off.begin(), b_off.end(), level_off.begin() + f.lb);
+                std::copy(b_net.begin(), b_net.end(), net_level_off.begin() + f.nnb);
+            }
+        });
+        if (verbose) {
+            // shape of the DAGs: nodes and depth per net, widest level of one net
+            std::vector<int> nn, nd, nw;
+            for (int id : of_nets) {
+                const DagNet &dn = dag[dag_slot[id]];
+                int dmax = 0;
+                for (int dv : dn.depth) dmax = std::max(dmax, dv + 1);
+                std::vector<int> w(dmax, 0);
+                for (int dv : dn.depth) w[dv]++;
+                nn.push_back((int)dn.nodes.size());
+                nd.push_back(dmax);
+                nw.push_back(dmax ? *std::max_element(w.begin(), w.end()) : 0);
+            }
+            for (auto *v : {&nn, &nd, &nw}) {  // counting sort: the values are small
+                int mx = 0;
+                for (int x : *v) mx = std::max(mx, x);
+                std::vector<int64_t> h((size_t)mx + 2, 0);
+                for (int x : *v) h[x]++;
+                size_t k = 0;
+                for (int x = 0; x <= mx; x++)
+                    for (int64_t c = 0; c < h[x]; c++) (*v)[k++] = x;
+            }
+            auto q = [](const std::vector<int> &v, double p) {  // v sorted
+                return v.empty() ? 0 : v[std::min(v.size() - 1, (size_t)(p * (v.size() - 1) + 0.5))];
+            };
+            std::fprintf(stderr,
+                         "[igr] dags: %zu batches, %zu nets, %zu nodes; per net nodes p50 %d p90 %d p99 %d max %d, "
+                         "depth p50 %d p90 %d p99 %d max %d, widest level p50 %d p99 %d max %d\n",
+                         batches.size(), of_nets.size(), nodes.size(), q(nn, .5), q(nn, .9), q(nn, .99), q(nn, 1),
+                         q(nd, .5), q(nd, .9), q(nd, .99), q(nd, 1), q(nw, .5), q(nw, .99), q(nw, 1));
         }
-        for (auto *v : {&nn, &nd, &nw}) {  // counting sort: the values are small
-            int mx = 0;
-            for (int x : *v) mx = std::max(mx, x);
-            std::vector<int64_t> h((size_t)mx + 2, 0);
-            for (int x : *v) h[x]++;
-            size_t k = 0;
-            for (int x = 0; x <= mx; x++)
-                for (int64_t c = 0; c < h[x]; c++) (*v)[k++] = x;
-        }
-        auto q = [](const std::vector<int> &v, double p) {  // v sorted
-            return v.empty() ? 0 : v[std::min(v.size() - 1, (size_t)(p * (v.size() - 1) + 0.5))];
-        };
-        std::fprintf(stderr,
-                     "[igr] dags: %zu batches, %zu nets, %zu nodes; per net nodes p50 %d p90 %d p99 %d max %d, "
-                     "depth p50 %d p90 %d p99 %d max %d, widest level p50 %d p99 %d max %d\n",
-                     batches.size(), of_nets.size(), nodes.size(), q(nn, .5), q(nn, .9), q(nn, .99), q(nn, 1),
-                     q(nd, .5), q(nd, .9), q(nd, .99), q(nd, 1), q(nw, .5), q(nw, .99), q(nw, 1));
+        t_csr = now_s();
+        grow_routes(route_end);
+        dg_nodes.upload(nodes.data(), nodes.size(), s); dg_paroff.upload(par_off.data(), par_off.size(), s);
+        dg_par.upload(par.data(), par.size(), s); dg_cslot.upload(cslot.data(), cslot.size(), s);
+        dg_echild.upload(echild.data(), echild.size(), s); dg_childoff.upload(child_off.data(), child_off.size(), s);
+        dg_leveloff.upload(level_off.data(), level_off.size(), s);
+        dg_levelnodes.upload(level_nodes.data(), level_nodes.size(), s);
+        dg_nno.upload(net_node_off.data(), net_node_off.size(), s); dg_ids.upload(net_ids.data(), net_ids.size(), s);
+        dg_netlvl.upload(net_level_off.data(), net_level_off.size(), s);
+        d_old_off.upload(old_off, s);
+        d_route_off.upload(route_off, s);
+        d_route_cap.upload(route_cap, s);
+        st.h2d_bytes += (int64_t)(nodes.size() * 2 + par_off.size() * 2 + par.size() * 3 + level_off.size() +
+                                  net_level_off.size() + net_node_off.size() + net_ids.size()) * 4 + (int64_t)R * 20;
     }
-    const double t_csr = now_s();
-    grow_routes(route_end);
-    dg_nodes.upload(nodes.data(), nodes.size(), s); dg_paroff.upload(par_off.data(), par_off.size(), s);
-    dg_par.upload(par.data(), par.size(), s); dg_cslot.upload(cslot.data(), cslot.size(), s);
-    dg_echild.upload(echild.data(), echild.size(), s); dg_childoff.upload(child_off.data(), child_off.size(), s);
-    dg_leveloff.upload(level_off.data(), level_off.size(), s);
-    dg_levelnodes.upload(level_nodes.data(), level_nodes.size(), s);
-    dg_nno.upload(net_node_off.data(), net_node_off.size(), s); dg_ids.upload(net_ids.data(), net_ids.size(), s);
-    dg_netlvl.upload(net_level_off.data(), net_level_off.size(), s);
-    d_old_off.upload(old_off, s);
-    d_route_off.upload(route_off, s);
-    d_route_cap.upload(route_cap, s);
-    st.h2d_bytes += (int64_t)(nodes.size() * 2 + par_off.size() * 2 + par.size() * 3 + level_off.size() +
-                              net_level_off.size() + net_node_off.size() + net_ids.size()) * 4 + (int64_t)R * 20;
     int mn = 1, me = 1, ms = 1;
     for (auto &f : bi) { mn = std::max(mn, f.n); me = std::max(me, f.e); ms = std::max(ms, f.slots); }
     dg_costs.alloc((size_t)mn * 10); dg_cedges.alloc((size_t)me * 81);
     dg_best.alloc((size_t)ms * 10); dg_packed.alloc((size_t)ms * 10);
     dg_bchange.alloc((size_t)me * 81); dg_lout.alloc(mn); dg_stage.alloc((size_t)mn * 8); dg_scnt.alloc(mn);
     for (size_t b = 0; b < bi.size(); b++) {
-        const BInfo &f = bi[b];
+        const DagBatchInfo &f = bi[b];
         const int nnet = (int)batches[b].size();
         ViaBatchDev old{dg_ids.p + f.nets, d_old_off.p, routes.p, nnet};
         const int s1 = ++global_stamp;
@@ -1338,6 +1351,194 @@ bool Router::rrr_pass(int iter) {
                      "[igr] pass %d host: DAGs %.3f s, conflict shapes %.3f s, colouring %.3f s, batch arrays %.3f s, "
                      "batches on the device %.3f s\n",
                      iter, t_dag - th0, t_shapes - t_dag, t_color - t_shapes, t_csr - t_color, now_s() - t_csr);
+    return true;
+}
+
+void Router::upload_dag_trees() {
+    if (dt_ready) return;
+    const int R = (int)ns.nets.size();
+    std::vector<int64_t> off((size_t)R + 1, 0), aoff((size_t)R + 1, 0);
+    for (int r = 0; r < R; r++) {
+        off[r + 1] = off[r] + (int64_t)ns.nets[r].tnode.size();
+        aoff[r + 1] = aoff[r] + (int64_t)ns.nets[r].adj.nb.size();
+    }
+    if (off[R] + 1 > INT32_MAX || aoff[R] > INT32_MAX) throw Error(ERR_CAPACITY, "trees exceed 32-bit offsets");
+    std::vector<int> h_off((size_t)R + 1), h_pos((size_t)off[R]), h_aoff((size_t)off[R] + 1), h_adj((size_t)aoff[R]);
+    parallel_for(R, threads, [&](int b, int e) {
+        for (int r = b; r < e; r++) {
+            const RNet &n = ns.nets[r];
+            const int base = (int)off[r], nbase = (int)aoff[r], T = (int)n.tnode.size();
+            h_off[r] = base;
+            for (int i = 0; i < T; i++) {
+                h_pos[base + i] = n.tnode[i];
+                h_aoff[base + i] = nbase + n.adj.off[i];
+            }
+            std::copy(n.adj.nb.begin(), n.adj.nb.end(), h_adj.begin() + nbase);
+        }
+    });
+    h_off[R] = (int)off[R];
+    h_aoff[off[R]] = (int)aoff[R];
+    d_dt_off.upload(h_off, s);
+    d_dt_pos.upload(h_pos, s);
+    d_dt_aoff.upload(h_aoff, s);
+    d_dt_adj.upload(h_adj, s);
+    cuda_check(cudaStreamSynchronize(s), "tree upload");
+    st.h2d_bytes += (int64_t)(h_off.size() + h_pos.size() + h_aoff.size() + h_adj.size()) * 4;
+    dt_ready = true;
+}
+
+// Detour DAGs of the rerouted nets built on the device (dagbuild.cu), their
+// conflict shapes and colouring, and the batch-local arrays of every colour
+// batch gathered on the device: the batches and arrays of the host path.
+bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<int>> &batches,
+                            std::vector<DagBatchInfo> &bi, const std::vector<int64_t> &old_off, double *tm) {
+    const int X = ns.X, Y = ns.Y, R = (int)ns.nets.size();
+    const double th0 = now_s();
+    upload_dag_trees();
+    DagBuildArgs a;
+    a.tree_off = d_dt_off.p; a.pos = d_dt_pos.p; a.adj_off = d_dt_aoff.p; a.adj = d_dt_adj.p;
+    a.xsum = d_xsum.p; a.ysum = d_ysum.p; a.X = X; a.Y = Y; a.mode = mode_eff;
+    d2_ids.upload(of_nets, s);
+    st.h2d_bytes += (int64_t)of_nets.size() * 4;
+    a.ids = d2_ids.p;
+    a.n_list = (int)of_nets.size();
+    const double tb0 = now_s();
+    ddag.measure(a, s);
+    const double tb1 = now_s();
+    st.d2h_bytes += (int64_t)of_nets.size() * kDagSizeFields * 4;
+    // the DP keeps at most 10 child slots per node (the reference packs the
+    // slot as a decimal digit); nets beyond that keep their current route
+    std::vector<int> kept;
+    kept.reserve(of_nets.size());
+    for (int k = 0; k < (int)of_nets.size(); k++)
+        if (ddag.sz(k, 5) <= 10) kept.push_back(k);
+    {
+        std::vector<int> ids(kept.size());
+        for (size_t i = 0; i < kept.size(); i++) ids[i] = of_nets[kept[i]];
+        of_nets.swap(ids);
+    }
+    if (of_nets.empty()) return false;
+    const int n = (int)of_nets.size();
+    d_kept.upload(of_nets, s);
+    a.ids = d_kept.p;
+    const double tb2 = now_s();
+    ddag.write(a, kept, s);
+    const double tb3 = now_s();
+    st.h2d_bytes += (int64_t)n * (4 + 24);
+    st.dag_host_ms += (now_s() - th0) * 1e3;
+    tm[0] = now_s();
+    // conflict shapes of the rerouted nets: their DAG points and their trees'
+    // segments (Lshape_route_detour.hpp:751)
+    if (ddag.h_point_at[n] > INT32_MAX) throw Error(ERR_CAPACITY, "DAG points exceed 32-bit offsets");
+    std::vector<int> pt_off((size_t)n + 1);
+    for (int i = 0; i <= n; i++) pt_off[i] = (int)ddag.h_point_at[i];
+    d2_ptoff.upload(pt_off, s);
+    st.h2d_bytes += (int64_t)(n + 1) * 4;
+    ShapeDev shd;
+    {
+        ShapeArgs sa;
+        sa.tree_off = d_tree_off.p; sa.tree_nodes = d_tree_nodes.p; sa.tree_par = d_tree_par.p;
+        sa.ids = d_kept.p; sa.ext_off = d2_ptoff.p; sa.ext_pts = ddag.points.p;
+        sa.n = n; sa.X = X; sa.Y = Y; sa.sparsity = mode_eff >= 1 ? 2 : 15;
+        device_shapes(sa, shd);
+    }
+    tm[1] = now_s();
+    std::vector<int> local(n);
+    std::iota(local.begin(), local.end(), 0);  // shape i belongs to of_nets[i]; of_nets is in priority order
+    std::vector<std::vector<int>> lb;
+    color_nets(local, shd, mode_eff >= 1 ? 2 : 15, lb);
+    tm[2] = now_s();
+    // batches in the host path's order (last colour first), as ids and as positions
+    const int B = (int)lb.size();
+    batches.assign(B, {});
+    std::vector<std::vector<int>> bpos(B);
+    for (int b = 0; b < B; b++) {
+        bpos[B - 1 - b] = lb[b];
+        for (int i : lb[b]) batches[B - 1 - b].push_back(of_nets[i]);
+    }
+    auto m_of = [&](int i) { return (int)(ddag.h_node_at[i + 1] - ddag.h_node_at[i]); };
+    auto e_of = [&](int i) { return (int)(ddag.h_edge_at[i + 1] - ddag.h_edge_at[i]); };
+    auto d_of = [&](int i) { return ddag.sz(kept[i], 3); };
+    auto s_of = [&](int i) { return ddag.sz(kept[i], 4); };
+    bi.assign(B, DagBatchInfo{});
+    DagBatchInfo tot{};
+    {
+        DagBatchInfo acc{};
+        for (int b = 0; b < B; b++) {
+            DagBatchInfo &f = bi[b];
+            f = acc;
+            f.n = f.e = f.slots = 0;
+            int64_t lv = 0;
+            for (int i : bpos[b]) {
+                const int id = of_nets[i];
+                f.n += m_of(i);
+                f.e += e_of(i);
+                f.slots += s_of(i);
+                lv += d_of(i) + 1;
+                // new route record of the net (appended)
+                route_cap[id] = 8 * m_of(i) + 1;
+                route_off[id] = route_end;
+                route_end += route_cap[id];
+            }
+            if ((int64_t)f.n * 100 + 99 > 0x7fffffffLL) throw Error(ERR_CAPACITY, "DAG batch too large for 32-bit node ids");
+            const int nn = (int)bpos[b].size();
+            const int64_t big = std::max({(int64_t)acc.pb + f.n + 1, (int64_t)acc.eb + f.e, (int64_t)acc.lb + lv,
+                                          (int64_t)acc.nnb + nn + 1});
+            if (big > 0x7fffffffLL) throw Error(ERR_CAPACITY, "DAG arrays of one rip-up pass exceed 32-bit offsets");
+            acc.nb += f.n; acc.eb += f.e; acc.pb += f.n + 1; acc.lb += (int)lv; acc.nnb += nn + 1; acc.nets += nn;
+        }
+        tot = acc;
+    }
+    // gather layout: per net (batch order) its DAG and its bases in the batch
+    std::vector<int> desc((size_t)n * kDagDescFields), bat((size_t)std::max(B, 1) * kDagBatchFields);
+    parallel_for(B, threads, [&](int b0, int e0) {
+        for (int b = b0; b < e0; b++) {
+            const DagBatchInfo &f = bi[b];
+            int base = 0, ebl = 0, sl = 0, lvb = 0, jl = 0;
+            for (int i : bpos[b]) {
+                int *d = desc.data() + (size_t)(f.nets + jl) * kDagDescFields;
+                d[0] = i; d[1] = base; d[2] = ebl; d[3] = sl; d[4] = lvb; d[5] = jl; d[6] = b;
+                base += m_of(i); ebl += e_of(i); sl += s_of(i); lvb += d_of(i) + 1; jl++;
+            }
+            int *t = bat.data() + (size_t)b * kDagBatchFields;
+            t[0] = f.nb; t[1] = f.eb; t[2] = f.pb; t[3] = f.lb; t[4] = f.nnb; t[5] = f.nets;
+        }
+    });
+    d_gdesc.upload(desc, s);
+    d_gbatch.upload(bat, s);
+    st.h2d_bytes += (int64_t)(desc.size() + bat.size()) * 4;
+    dg_nodes.alloc(std::max(1, tot.nb)); dg_paroff.alloc(std::max(1, tot.pb)); dg_par.alloc(std::max(1, tot.eb));
+    dg_cslot.alloc(std::max(1, tot.eb)); dg_echild.alloc(std::max(1, tot.eb)); dg_childoff.alloc(std::max(1, tot.pb));
+    dg_leveloff.alloc(std::max(1, tot.lb)); dg_levelnodes.alloc(std::max(1, tot.nb));
+    dg_nno.alloc(std::max(1, tot.nnb)); dg_ids.alloc(std::max(1, tot.nets)); dg_netlvl.alloc(std::max(1, tot.nnb));
+    DagGatherArgs g;
+    g.n = n; g.desc = d_gdesc.p; g.batch = d_gbatch.p; g.ids = d_kept.p;
+    g.node_at = ddag.node_at.p; g.edge_at = ddag.edge_at.p;
+    g.src_nodes = ddag.nodes.p; g.src_par_num = ddag.par_num.p; g.src_child_num = ddag.child_num.p;
+    g.src_depth = ddag.depth.p; g.src_par = ddag.par.p; g.src_child_idx = ddag.child_idx.p;
+    g.nodes = dg_nodes.p; g.par_off = dg_paroff.p; g.par = dg_par.p; g.child_slot = dg_cslot.p;
+    g.edge_child = dg_echild.p; g.child_off = dg_childoff.p; g.level_off = dg_leveloff.p;
+    g.level_nodes = dg_levelnodes.p; g.net_node_off = dg_nno.p; g.net_ids = dg_ids.p; g.net_level_off = dg_netlvl.p;
+    launch_dag_gather(g, s);
+    cuda_check(cudaGetLastError(), "DAG gather launch");
+    st.launches += 1;
+    if (verbose) {
+        int64_t mx = 0, dmx = 0;
+        for (int i = 0; i < n; i++) { mx = std::max<int64_t>(mx, m_of(i)); dmx = std::max<int64_t>(dmx, d_of(i)); }
+        int cls[3] = {0, 0, 0};
+        for (int k : kept) cls[ddag.tier[k]]++;
+        std::fprintf(stderr,
+                     "[igr] dags on the device: %d batches, %d nets, %lld nodes, %lld edges, %lld points; max %lld nodes, "
+                     "depth %lld; work-area classes %d/%d/%d; trees %.3f s, sizes %.3f s, arrays %.3f s\n",
+                     B, n, (long long)ddag.h_node_at[n], (long long)ddag.h_edge_at[n], (long long)ddag.h_point_at[n],
+                     (long long)mx, (long long)dmx, cls[0], cls[1], cls[2], tb0 - th0, tb1 - tb0, tb3 - tb2);
+    }
+    tm[3] = now_s();
+    grow_routes(route_end);
+    d_old_off.upload(old_off, s);
+    d_route_off.upload(route_off, s);
+    d_route_cap.upload(route_cap, s);
+    st.h2d_bytes += (int64_t)R * 20;
     return true;
 }
 

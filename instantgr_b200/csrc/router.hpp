@@ -82,6 +82,33 @@ struct DevBuf {
     void upload(const std::vector<T> &v, cudaStream_t s) { upload(v.data(), v.size(), s); }
 };
 
+// Colour batch of a rip-up pass: its first entries in the pass-wide DAG
+// arrays (nodes, edges, nodes + 1 per net, depth levels, nets + 1, nets) and
+// its node, edge and child-slot counts.
+struct DagBatchInfo {
+    int nb, eb, pb, lb, nnb, nets, n, e, slots;
+};
+
+// Detour DAGs built on the device (dagbuild.cu) for a list of routing nets:
+// a size pass (nets whose DAG outgrows a thread's work area are built again
+// with larger slices), then, for the nets kept, a write pass into arrays laid
+// out end to end in list order.
+struct DeviceDags {
+    DevBuf<int> work, sizes, list, err;
+    DevBuf<long long> node_at, edge_at, point_at;
+    DevBuf<int> nodes, par_num, child_num, depth, par, child_idx, points;
+    std::vector<int> hs;    // [k][kDagSizeFields] after measure()
+    std::vector<int> tier;  // work-area size class each DAG fits
+    std::vector<long long> h_node_at, h_edge_at, h_point_at;  // [kept+1] after write()
+    // a.ids, a.n_list and the tree, congestion and grid fields set; list,
+    // sizes, work and the outputs are filled in here
+    void measure(DagBuildArgs a, cudaStream_t s);
+    // DAGs `kept` (positions of the measured list, ascending) written in that
+    // order; a.ids holds the kept nets' ids in the same order
+    void write(DagBuildArgs a, const std::vector<int> &kept, cudaStream_t s);
+    int sz(int k, int f) const { return hs[(size_t)k * kDagSizeFields + f]; }
+};
+
 // Device arrays of one routing grid (build_cuda_database, database_cuda.hpp:2096-2362).
 struct GridOwner {
     GridDev g;
@@ -153,6 +180,7 @@ struct RouteBackup {
 struct Router {
     int rrr_iters = 1, threads = 0, mode = -1, verbose = 0, batched = 0;
     int split_commit = 0;  // 1: separate cost refresh, wire commit and via commit launches per phase-1 batch
+    int host_dags = 0;     // 1: detour DAGs and batch arrays of the rip-up passes built on host threads
     Design d;
     NetSet ns;
     GridOwner go;
@@ -281,6 +309,11 @@ struct Router {
     void device_shapes(const ShapeArgs &a, ShapeDev &sd);
     DevBuf<long long> d_shape_tot;
     DevBuf<int> d2_ptoff, d2_pts, d2_ids;  // DAG points and net ids of the rerouted nets
+    // device DAG construction: trees in adjacency order (positions, neighbour
+    // lists), the builder, kept nets and the batch layout of the gather
+    DevBuf<int> d_dt_off, d_dt_pos, d_dt_aoff, d_dt_adj, d_kept, d_gdesc, d_gbatch;
+    bool dt_ready = false;
+    DeviceDags ddag;
     // stream, events and the routing grid on the device; started on a thread of
     // its own by open() as soon as the capacities are read
     void create_grid();
@@ -294,6 +327,12 @@ struct Router {
     // colours n ranks (d_perm_ranks[k] = shape of rank k) into d_bat; returns the batch count
     int run_color(int n, const int *d_perm_ranks, const ShapeDev &shapes, int sparsity);
     void compute_score();
+    // detour DAGs of the rerouted nets built, coloured and laid out per batch
+    // on the device; false when no net is left to reroute.  tm: times at which
+    // the DAGs, conflict shapes, colouring and batch arrays were done
+    bool dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<int>> &batches,
+                        std::vector<DagBatchInfo> &bi, const std::vector<int64_t> &old_off, double *tm);
+    void upload_dag_trees();  // trees in adjacency order, once per router
 
    private:
     void phase1();
