@@ -772,9 +772,18 @@ int igr_build_dags(int X, int Y, int mode, int n, const int32_t *tree_off, const
         a.xsum = d_xs.p; a.ysum = d_ys.p; a.X = X; a.Y = Y; a.mode = mode;
         a.ids = d_ids.p; a.n_list = n;
         DeviceDags dd;
-        dd.measure(a, s);
-        dd.write(a, ids, s);  // every DAG, in order (no slot rule here)
-        const size_t nn = (size_t)dd.h_node_at[n], ne = (size_t)dd.h_edge_at[n], np = (size_t)dd.h_point_at[n];
+        dd.build(a, s);
+        std::vector<long long> nat(n), eat(n), pat(n);
+        unsigned long long u[3];
+        auto down64 = [&](std::vector<long long> &h, const DevBuf<long long> &d) {
+            if (!h.empty()) cuda_check(cudaMemcpyAsync(h.data(), d.p, h.size() * 8, cudaMemcpyDeviceToHost, s), "D2H");
+        };
+        down64(nat, dd.node_at); down64(eat, dd.edge_at); down64(pat, dd.point_at);
+        cuda_check(cudaMemcpyAsync(u, dd.used.p, sizeof u, cudaMemcpyDeviceToHost, s), "D2H");
+        cuda_check(cudaStreamSynchronize(s), "sync");
+        // the pools up to what was used (holes left by rebuilt DAGs included)
+        const size_t nn = std::min<size_t>(u[0], dd.nodes.n), ne = std::min<size_t>(u[1], dd.par.n),
+                     np = std::min<size_t>(u[2], dd.points.n);
         std::vector<int> nodes(nn), pnum(nn), cnum(nn), dep(nn), par(ne), cidx(ne), pts(np);
         auto down = [&](std::vector<int> &h, const DevBuf<int> &d) {
             if (!h.empty()) cuda_check(cudaMemcpyAsync(h.data(), d.p, h.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
@@ -785,17 +794,14 @@ int igr_build_dags(int X, int Y, int mode, int n, const int32_t *tree_off, const
         int64_t L = 0;
         for (int k = 0; k < n; k++) {
             rec_off[k] = L;
-            L += 3 + 4 * (dd.h_node_at[k + 1] - dd.h_node_at[k]) + 2 * (dd.h_edge_at[k + 1] - dd.h_edge_at[k]) +
-                 (dd.h_point_at[k + 1] - dd.h_point_at[k]);
+            L += 3 + 4 * (int64_t)dd.sz(k, 0) + 2 * (int64_t)dd.sz(k, 1) + dd.sz(k, 2);
         }
         rec_off[n] = L;
         *len = L;
         if (!out || cap < L) return;
         for (int k = 0; k < n; k++) {
             int32_t *o = out + rec_off[k];
-            const int64_t a0 = dd.h_node_at[k], m = dd.h_node_at[k + 1] - a0;
-            const int64_t e0 = dd.h_edge_at[k], E = dd.h_edge_at[k + 1] - e0;
-            const int64_t p0 = dd.h_point_at[k], P = dd.h_point_at[k + 1] - p0;
+            const int64_t a0 = nat[k], m = dd.sz(k, 0), e0 = eat[k], E = dd.sz(k, 1), p0 = pat[k], P = dd.sz(k, 2);
             *o++ = (int32_t)m;
             for (auto *v : {&nodes, &pnum, &cnum, &dep}) o = std::copy(v->begin() + a0, v->begin() + a0 + m, o);
             *o++ = (int32_t)E;

@@ -58,71 +58,85 @@ void run_class(DeviceDags &d, DagBuildArgs a, int cls, const std::vector<int> &m
     cuda_check(cudaGetLastError(), "DAG build launch");
 }
 
+// grows a pool to `count` entries, keeping its first `keep`
+void grow_keep(DevBuf<int> &b, size_t count, size_t keep, cudaStream_t s) {
+    if (count <= b.n && b.p) return;
+    int *np = static_cast<int *>(dev_alloc(count * sizeof(int)));
+    if (keep && b.p) cuda_check(cudaMemcpyAsync(np, b.p, keep * sizeof(int), cudaMemcpyDeviceToDevice, s), "D2D");
+    b.release();  // synchronises the device first
+    b.p = np;
+    b.n = count;
+}
+
 }  // namespace
 
-void DeviceDags::measure(DagBuildArgs a, cudaStream_t s) {
+void DeviceDags::build(DagBuildArgs a, cudaStream_t s) {
     const int n = a.n_list;
     hs.assign((size_t)n * kDagSizeFields, 0);
     tier.assign(n, 0);
     if (n == 0) return;
     sizes.alloc((size_t)n * kDagSizeFields);
+    node_at.alloc(n); edge_at.alloc(n); point_at.alloc(n);
+    used.alloc(3);
+    cuda_check(cudaMemsetAsync(used.p, 0, 3 * sizeof(unsigned long long), s), "memset");
+    // pools sized from the last build's entries per DAG, with a margin
+    auto want = [&](double per) { return (size_t)(per * 1.25 * n) + 4096; };
+    const size_t cn = want(per_node), ce = want(per_edge), cp = want(per_point);
+    grow_keep(nodes, cn, 0, s); grow_keep(par_num, cn, 0, s); grow_keep(child_num, cn, 0, s);
+    grow_keep(depth, cn, 0, s); grow_keep(par, ce, 0, s); grow_keep(child_idx, ce, 0, s); grow_keep(points, cp, 0, s);
     a.sizes = sizes.p;
-    a.out_nodes = nullptr;
-    std::vector<int> members(n);
+    a.node_at = node_at.p; a.edge_at = edge_at.p; a.point_at = point_at.p;
+    a.used = used.p;
+    auto set_pools = [&]() {
+        a.cap_nodes = (long long)nodes.n; a.cap_edges = (long long)par.n; a.cap_points = (long long)points.n;
+        a.out_nodes = nodes.p; a.out_par_num = par_num.p; a.out_child_num = child_num.p; a.out_depth = depth.p;
+        a.out_par = par.p; a.out_child_idx = child_idx.p; a.out_points = points.p;
+    };
+    set_pools();
+    std::vector<int> members(n), next;  // DAGs to build in this class; for the next class
     for (int k = 0; k < n; k++) members[k] = k;
-    for (int cls = 0; cls < kNumClasses && !members.empty(); cls++) {
+    int cls = 0, regrow = 0;
+    while (true) {
         run_class(*this, a, cls, members, s);
+        unsigned long long u[3];
         cuda_check(cudaMemcpyAsync(hs.data(), sizes.p, hs.size() * 4, cudaMemcpyDeviceToHost, s), "D2H");
-        cuda_check(cudaStreamSynchronize(s), "DAG sizes");
-        std::vector<int> again;
+        cuda_check(cudaMemcpyAsync(u, used.p, sizeof u, cudaMemcpyDeviceToHost, s), "D2H");
+        cuda_check(cudaStreamSynchronize(s), "DAG build");
+        std::vector<int> full;
         for (int k : members) {
             const int status = sz(k, 6);
             if (status == 2) throw Error(ERR_STATE, "malformed tree or detour DAG");
-            if (status == 1) again.push_back(k);
+            if (status == 1) next.push_back(k);
+            if (status == 3) full.push_back(k);
             tier[k] = cls;
         }
-        members.swap(again);
+        if (!full.empty()) {  // grow the pools past what was asked for and build those DAGs again
+            if (++regrow > 8) throw Error(ERR_CAPACITY, "detour DAG pools keep overflowing");
+            const double f = 2.0 * (double)full.size() + 4096;
+            grow_keep(nodes, (size_t)(u[0] + f * per_node), nodes.n, s);
+            grow_keep(par_num, nodes.n, par_num.n, s);
+            grow_keep(child_num, nodes.n, child_num.n, s);
+            grow_keep(depth, nodes.n, depth.n, s);
+            grow_keep(par, (size_t)(u[1] + f * per_edge), par.n, s);
+            grow_keep(child_idx, par.n, child_idx.n, s);
+            grow_keep(points, (size_t)(u[2] + f * per_point), points.n, s);
+            set_pools();
+            members.swap(full);
+            continue;  // same class
+        }
+        if (next.empty()) break;
+        if (++cls >= kNumClasses) throw Error(ERR_CAPACITY, "a detour DAG outgrows the largest work area");
+        std::sort(next.begin(), next.end());
+        members.swap(next);
+        next.clear();
     }
-    if (!members.empty()) throw Error(ERR_CAPACITY, "a detour DAG outgrows the largest work area");
-}
-
-void DeviceDags::write(DagBuildArgs a, const std::vector<int> &kept, cudaStream_t s) {
-    const int n = (int)kept.size();
-    h_node_at.assign((size_t)n + 1, 0);
-    h_edge_at.assign((size_t)n + 1, 0);
-    h_point_at.assign((size_t)n + 1, 0);
-    for (int i = 0; i < n; i++) {
-        const int k = kept[i];
-        h_node_at[i + 1] = h_node_at[i] + sz(k, 0);
-        h_edge_at[i + 1] = h_edge_at[i] + sz(k, 1);
-        h_point_at[i + 1] = h_point_at[i] + sz(k, 2);
-    }
-    if (n == 0) return;
-    node_at.upload(h_node_at, s);
-    edge_at.upload(h_edge_at, s);
-    point_at.upload(h_point_at, s);
-    const size_t nn = (size_t)std::max<long long>(1, h_node_at[n]), ne = (size_t)std::max<long long>(1, h_edge_at[n]),
-                 np = (size_t)std::max<long long>(1, h_point_at[n]);
-    nodes.alloc(nn); par_num.alloc(nn); child_num.alloc(nn); depth.alloc(nn);
-    par.alloc(ne); child_idx.alloc(ne); points.alloc(np);
-    err.alloc(1);
-    cuda_check(cudaMemsetAsync(err.p, 0, sizeof(int), s), "memset");
-    a.sizes = nullptr;
-    a.node_at = node_at.p; a.edge_at = edge_at.p; a.point_at = point_at.p;
-    a.out_nodes = nodes.p; a.out_par_num = par_num.p; a.out_child_num = child_num.p; a.out_depth = depth.p;
-    a.out_par = par.p; a.out_child_idx = child_idx.p; a.out_points = points.p;
-    a.err = err.p;
-    a.n_list = n;
-    for (int cls = 0; cls < kNumClasses; cls++) {
-        std::vector<int> members;
-        for (int i = 0; i < n; i++)
-            if (tier[kept[i]] == cls) members.push_back(i);
-        run_class(*this, a, cls, members, s);
-    }
-    int h_err = 0;
-    cuda_check(cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
-    cuda_check(cudaStreamSynchronize(s), "DAG write");
-    if (h_err) throw Error(ERR_STATE, "a detour DAG changed between the size and write passes");
+    for (int k = 0; k < n; k++)
+        if (sz(k, 6) != 0) throw Error(ERR_STATE, "a detour DAG was left unbuilt");
+    double tn = 0, te = 0, tp = 0;
+    for (int k = 0; k < n; k++) { tn += sz(k, 0); te += sz(k, 1); tp += sz(k, 2); }
+    per_node = std::max(8.0, tn / n);
+    per_edge = std::max(8.0, te / n);
+    per_point = std::max(8.0, tp / n);
 }
 
 }  // namespace igr

@@ -12,10 +12,11 @@
 //   (:2027-2085).
 // The recursions become explicit stacks and the growing containers become
 // slices of a per-thread work area.  A net whose DAG does not fit its slices
-// reports so and is built again with larger ones.  Two passes over the same
-// nets: the first returns the size of every DAG, the second, once the host has
-// laid the DAGs out end to end, writes them.  A third kernel gathers the DAGs
-// of each colour batch into the batch-local arrays of the DAG router.
+// reports so and is built again with larger ones.  A finished DAG reserves its
+// ranges of the node, edge and point pools with one atomic add each and is
+// written there; a DAG that finds a pool full is built again once the pools
+// have grown.  A second kernel gathers the DAGs of each colour batch into the
+// batch-local arrays of the DAG router.
 #include "kcommon.cuh"
 
 namespace igr {
@@ -69,7 +70,7 @@ __device__ Work carve(int *p, const DagCaps &c) {
     return w;
 }
 
-enum : int { kOk = 0, kTooLarge = 1, kMalformed = 2 };
+enum : int { kOk = 0, kTooLarge = 1, kMalformed = 2, kPoolFull = 3 };
 
 // in-place ascending heap sort of a[0..n)
 __device__ void heap_sort(int *a, int n) {
@@ -698,38 +699,30 @@ __device__ void build_dags(const DagBuildArgs &a, const Work &w, int t, int nt) 
             for (int q = 0; q < B.np; q++)
                 if (npu == 0 || w.pts[q] != w.pts[npu - 1]) w.pts[npu++] = w.pts[q];
         }
-        const bool write = a.out_nodes != nullptr;
-        if (write) {
-            // the layout was made from the sizes of the same construction
-            const bool fits = !B.bad && a.node_at[k + 1] - a.node_at[k] == B.nn &&
-                              a.edge_at[k + 1] - a.edge_at[k] == B.nl && a.point_at[k + 1] - a.point_at[k] == npu;
-            if (!fits) {
-                atomicExch(a.err, 1);
-                continue;
-            }
-            B.renumber(a.out_par + a.edge_at[k], a.out_child_idx + a.edge_at[k]);
-            if (B.bad) {
-                atomicExch(a.err, 1);
-                continue;
-            }
-            const long long no = a.node_at[k], po = a.point_at[k];
+        // place the DAG: node, edge and point ranges reserved in the pools
+        // (their order varies from run to run; every reader goes through the
+        // per-DAG offsets, so results do not)
+        long long no = 0, eo = 0, po = 0;
+        if (!B.bad) {
+            no = (long long)atomicAdd(a.used + 0, (unsigned long long)B.nn);
+            eo = (long long)atomicAdd(a.used + 1, (unsigned long long)B.nl);
+            po = (long long)atomicAdd(a.used + 2, (unsigned long long)npu);
+            if (no + B.nn > a.cap_nodes || eo + B.nl > a.cap_edges || po + npu > a.cap_points) B.bad = kPoolFull;
+        }
+        if (!B.bad) B.renumber(a.out_par + eo, a.out_child_idx + eo);
+        int D = 0, S = 0, mc = 0;
+        if (!B.bad) {
             for (int v = 0; v < B.nn; v++) {
                 a.out_nodes[no + v] = w.onode[v];
                 a.out_par_num[no + v] = w.pn[v];
                 a.out_child_num[no + v] = w.cn[v];
                 a.out_depth[no + v] = w.dep[v];
-            }
-            for (int q = 0; q < npu; q++) a.out_points[po + q] = w.pts[q];
-            continue;
-        }
-        if (!B.bad) B.renumber(nullptr, nullptr);
-        int D = 0, S = 0, mc = 0;
-        if (!B.bad)
-            for (int v = 0; v < B.nn; v++) {
                 D = max(D, w.dep[v] + 1);
                 S += w.cn[v];
                 mc = max(mc, w.cn[v]);
             }
+            for (int q = 0; q < npu; q++) a.out_points[po + q] = w.pts[q];
+        }
         int *sz = a.sizes + (size_t)k * kDagSizeFields;
         sz[0] = B.bad ? 0 : B.nn;
         sz[1] = B.bad ? 0 : B.nl;
@@ -738,6 +731,9 @@ __device__ void build_dags(const DagBuildArgs &a, const Work &w, int t, int nt) 
         sz[4] = S;
         sz[5] = mc;
         sz[6] = B.bad;
+        a.node_at[k] = no;
+        a.edge_at[k] = eo;
+        a.point_at[k] = po;
     }
 }
 
@@ -765,10 +761,10 @@ __global__ void dag_gather_kernel(DagGatherArgs a) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= a.n) return;
     const int *d = a.desc + (size_t)j * kDagDescFields;
-    const int i = d[0], base = d[1], ebl = d[2], sl0 = d[3], lvb = d[4], jl = d[5], b = d[6];
+    const int k = d[0], base = d[1], ebl = d[2], sl0 = d[3], lvb = d[4], jl = d[5], b = d[6];
     const int *bi = a.batch + (size_t)b * kDagBatchFields;  // nb, eb, pb, lb, nnb, nets
-    const long long no = a.node_at[i], eo = a.edge_at[i];
-    const int m = (int)(a.node_at[i + 1] - no);
+    const long long no = a.node_at[k], eo = a.edge_at[k];
+    const int m = a.sizes[(size_t)k * kDagSizeFields];
     const int nb0 = bi[0] + base, eb0 = bi[1] + ebl, pb0 = bi[2] + base, lb0 = bi[3] + lvb, nnb0 = bi[4] + jl;
     if (jl == 0) {
         a.par_off[bi[2]] = 0;
@@ -801,7 +797,7 @@ __global__ void dag_gather_kernel(DagGatherArgs a) {
     }
     a.level_off[lb0 + D] = pos;
     a.net_node_off[nnb0 + 1] = base + m;
-    a.net_ids[bi[5] + jl] = a.ids[i];
+    a.net_ids[bi[5] + jl] = a.ids[k];
     a.net_level_off[nnb0 + 1] = lvb + D + 1;
 }
 

@@ -153,6 +153,10 @@ void launch_from_track_layout_i(const GridDev &g, const int *trk, int *ref, cuda
 struct ShapeArgs {
     const int *tree_off = nullptr, *tree_nodes = nullptr, *tree_par = nullptr;
     const int *ids = nullptr, *ext_off = nullptr, *ext_pts = nullptr;
+    // instead of ext_off: shape k's points start at ext_at[k], ext_cnt[k * ext_stride] of them
+    const long long *ext_at = nullptr;
+    const int *ext_cnt = nullptr;
+    int ext_stride = 1;
     int n = 0, X = 0, Y = 0, sparsity = 15;
 };
 void launch_shape_count(const ShapeArgs &a, int *pt_off, int *claim_off, long long *totals, cudaStream_t s);
@@ -178,12 +182,13 @@ struct DagBuildArgs {
     int X = 0, Y = 0, mode = 2;
     DagCaps caps;
     int *work = nullptr;            // threads x dag_work_ints(caps)
-    int *sizes = nullptr;           // size pass: [k][kDagSizeFields]
-    // write pass: layout [k+1] and the per-DAG arrays
-    const long long *node_at = nullptr, *edge_at = nullptr, *point_at = nullptr;
+    int *sizes = nullptr;           // [k][kDagSizeFields]; status 1: work area too small, 2: malformed, 3: pool full
+    long long *node_at = nullptr, *edge_at = nullptr, *point_at = nullptr;  // [k] where DAG k was placed
+    // pools: entries used so far (nodes, edges, points) and their capacities
+    unsigned long long *used = nullptr;
+    long long cap_nodes = 0, cap_edges = 0, cap_points = 0;
     int *out_nodes = nullptr, *out_par_num = nullptr, *out_child_num = nullptr, *out_depth = nullptr;
     int *out_par = nullptr, *out_child_idx = nullptr, *out_points = nullptr;
-    int *err = nullptr;
 };
 long long dag_work_ints(const DagCaps &c);
 void launch_dag_build(const DagBuildArgs &a, int threads, cudaStream_t s);
@@ -198,7 +203,7 @@ constexpr int kDagDescFields = 7;
 constexpr int kDagBatchFields = 6;
 struct DagGatherArgs {
     int n = 0;
-    const int *desc = nullptr, *batch = nullptr, *ids = nullptr;
+    const int *desc = nullptr, *batch = nullptr, *ids = nullptr, *sizes = nullptr;
     const long long *node_at = nullptr, *edge_at = nullptr;
     const int *src_nodes = nullptr, *src_par_num = nullptr, *src_child_num = nullptr, *src_depth = nullptr;
     const int *src_par = nullptr, *src_child_idx = nullptr;

@@ -1358,12 +1358,21 @@ void Router::upload_dag_trees() {
     if (dt_ready) return;
     const int R = (int)ns.nets.size();
     std::vector<int64_t> off((size_t)R + 1, 0), aoff((size_t)R + 1, 0);
+    parallel_for(R, threads, [&](int b, int e) {
+        for (int r = b; r < e; r++) {
+            off[r + 1] = (int64_t)ns.nets[r].tnode.size();
+            aoff[r + 1] = (int64_t)ns.nets[r].adj.nb.size();
+        }
+    });
     for (int r = 0; r < R; r++) {
-        off[r + 1] = off[r] + (int64_t)ns.nets[r].tnode.size();
-        aoff[r + 1] = aoff[r] + (int64_t)ns.nets[r].adj.nb.size();
+        off[r + 1] += off[r];
+        aoff[r + 1] += aoff[r];
     }
     if (off[R] + 1 > INT32_MAX || aoff[R] > INT32_MAX) throw Error(ERR_CAPACITY, "trees exceed 32-bit offsets");
-    std::vector<int> h_off((size_t)R + 1), h_pos((size_t)off[R]), h_aoff((size_t)off[R] + 1), h_adj((size_t)aoff[R]);
+    // written in full below, by the threads that fill them
+    const size_t nt = (size_t)off[R], na = (size_t)aoff[R];
+    std::unique_ptr<int[]> h_off(new int[(size_t)R + 1]), h_pos(new int[nt ? nt : 1]), h_aoff(new int[nt + 1]),
+        h_adj(new int[na ? na : 1]);
     parallel_for(R, threads, [&](int b, int e) {
         for (int r = b; r < e; r++) {
             const RNet &n = ns.nets[r];
@@ -1373,17 +1382,17 @@ void Router::upload_dag_trees() {
                 h_pos[base + i] = n.tnode[i];
                 h_aoff[base + i] = nbase + n.adj.off[i];
             }
-            std::copy(n.adj.nb.begin(), n.adj.nb.end(), h_adj.begin() + nbase);
+            std::copy(n.adj.nb.begin(), n.adj.nb.end(), h_adj.get() + nbase);
         }
     });
     h_off[R] = (int)off[R];
-    h_aoff[off[R]] = (int)aoff[R];
-    d_dt_off.upload(h_off, s);
-    d_dt_pos.upload(h_pos, s);
-    d_dt_aoff.upload(h_aoff, s);
-    d_dt_adj.upload(h_adj, s);
+    h_aoff[nt] = (int)na;
+    d_dt_off.upload(h_off.get(), (size_t)R + 1, s);
+    d_dt_pos.upload(h_pos.get(), nt, s);
+    d_dt_aoff.upload(h_aoff.get(), nt + 1, s);
+    d_dt_adj.upload(h_adj.get(), na, s);
     cuda_check(cudaStreamSynchronize(s), "tree upload");
-    st.h2d_bytes += (int64_t)(h_off.size() + h_pos.size() + h_aoff.size() + h_adj.size()) * 4;
+    st.h2d_bytes += (int64_t)(R + 1 + 2 * nt + 1 + na) * 4;
     dt_ready = true;
 }
 
@@ -1403,7 +1412,7 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
     a.ids = d2_ids.p;
     a.n_list = (int)of_nets.size();
     const double tb0 = now_s();
-    ddag.measure(a, s);
+    ddag.build(a, s);
     const double tb1 = now_s();
     st.d2h_bytes += (int64_t)of_nets.size() * kDagSizeFields * 4;
     // the DP keeps at most 10 child slots per node (the reference packs the
@@ -1412,6 +1421,7 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
     kept.reserve(of_nets.size());
     for (int k = 0; k < (int)of_nets.size(); k++)
         if (ddag.sz(k, 5) <= 10) kept.push_back(k);
+    const bool all_kept = kept.size() == of_nets.size();
     {
         std::vector<int> ids(kept.size());
         for (size_t i = 0; i < kept.size(); i++) ids[i] = of_nets[kept[i]];
@@ -1419,26 +1429,31 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
     }
     if (of_nets.empty()) return false;
     const int n = (int)of_nets.size();
-    d_kept.upload(of_nets, s);
-    a.ids = d_kept.p;
-    const double tb2 = now_s();
-    ddag.write(a, kept, s);
-    const double tb3 = now_s();
-    st.h2d_bytes += (int64_t)n * (4 + 24);
     st.dag_host_ms += (now_s() - th0) * 1e3;
     tm[0] = now_s();
     // conflict shapes of the rerouted nets: their DAG points and their trees'
     // segments (Lshape_route_detour.hpp:751)
-    if (ddag.h_point_at[n] > INT32_MAX) throw Error(ERR_CAPACITY, "DAG points exceed 32-bit offsets");
-    std::vector<int> pt_off((size_t)n + 1);
-    for (int i = 0; i <= n; i++) pt_off[i] = (int)ddag.h_point_at[i];
-    d2_ptoff.upload(pt_off, s);
-    st.h2d_bytes += (int64_t)(n + 1) * 4;
     ShapeDev shd;
     {
         ShapeArgs sa;
         sa.tree_off = d_tree_off.p; sa.tree_nodes = d_tree_nodes.p; sa.tree_par = d_tree_par.p;
-        sa.ids = d_kept.p; sa.ext_off = d2_ptoff.p; sa.ext_pts = ddag.points.p;
+        sa.ext_pts = ddag.points.p;
+        if (all_kept) {  // shape i is DAG i
+            sa.ids = d2_ids.p;
+            sa.ext_at = ddag.point_at.p; sa.ext_cnt = ddag.sizes.p + 2; sa.ext_stride = kDagSizeFields;
+        } else {         // shape i is DAG kept[i]
+            std::vector<long long> at(n);
+            std::vector<long long> all_at(kept.back() + 1);
+            cuda_check(cudaMemcpyAsync(all_at.data(), ddag.point_at.p, all_at.size() * 8, cudaMemcpyDeviceToHost, s),
+                       "D2H");
+            cuda_check(cudaStreamSynchronize(s), "sync");
+            std::vector<int> cnt(n);
+            for (int i = 0; i < n; i++) { at[i] = all_at[kept[i]]; cnt[i] = ddag.sz(kept[i], 2); }
+            d_kept.upload(of_nets, s);
+            d2_extat.upload(at, s);
+            d2_ptoff.upload(cnt, s);
+            sa.ids = d_kept.p; sa.ext_at = d2_extat.p; sa.ext_cnt = d2_ptoff.p; sa.ext_stride = 1;
+        }
         sa.n = n; sa.X = X; sa.Y = Y; sa.sparsity = mode_eff >= 1 ? 2 : 15;
         device_shapes(sa, shd);
     }
@@ -1456,8 +1471,8 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
         bpos[B - 1 - b] = lb[b];
         for (int i : lb[b]) batches[B - 1 - b].push_back(of_nets[i]);
     }
-    auto m_of = [&](int i) { return (int)(ddag.h_node_at[i + 1] - ddag.h_node_at[i]); };
-    auto e_of = [&](int i) { return (int)(ddag.h_edge_at[i + 1] - ddag.h_edge_at[i]); };
+    auto m_of = [&](int i) { return ddag.sz(kept[i], 0); };
+    auto e_of = [&](int i) { return ddag.sz(kept[i], 1); };
     auto d_of = [&](int i) { return ddag.sz(kept[i], 3); };
     auto s_of = [&](int i) { return ddag.sz(kept[i], 4); };
     bi.assign(B, DagBatchInfo{});
@@ -1497,7 +1512,7 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
             int base = 0, ebl = 0, sl = 0, lvb = 0, jl = 0;
             for (int i : bpos[b]) {
                 int *d = desc.data() + (size_t)(f.nets + jl) * kDagDescFields;
-                d[0] = i; d[1] = base; d[2] = ebl; d[3] = sl; d[4] = lvb; d[5] = jl; d[6] = b;
+                d[0] = kept[i]; d[1] = base; d[2] = ebl; d[3] = sl; d[4] = lvb; d[5] = jl; d[6] = b;
                 base += m_of(i); ebl += e_of(i); sl += s_of(i); lvb += d_of(i) + 1; jl++;
             }
             int *t = bat.data() + (size_t)b * kDagBatchFields;
@@ -1512,7 +1527,7 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
     dg_leveloff.alloc(std::max(1, tot.lb)); dg_levelnodes.alloc(std::max(1, tot.nb));
     dg_nno.alloc(std::max(1, tot.nnb)); dg_ids.alloc(std::max(1, tot.nets)); dg_netlvl.alloc(std::max(1, tot.nnb));
     DagGatherArgs g;
-    g.n = n; g.desc = d_gdesc.p; g.batch = d_gbatch.p; g.ids = d_kept.p;
+    g.n = n; g.desc = d_gdesc.p; g.batch = d_gbatch.p; g.ids = d2_ids.p; g.sizes = ddag.sizes.p;
     g.node_at = ddag.node_at.p; g.edge_at = ddag.edge_at.p;
     g.src_nodes = ddag.nodes.p; g.src_par_num = ddag.par_num.p; g.src_child_num = ddag.child_num.p;
     g.src_depth = ddag.depth.p; g.src_par = ddag.par.p; g.src_child_idx = ddag.child_idx.p;
@@ -1523,15 +1538,19 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
     cuda_check(cudaGetLastError(), "DAG gather launch");
     st.launches += 1;
     if (verbose) {
-        int64_t mx = 0, dmx = 0;
-        for (int i = 0; i < n; i++) { mx = std::max<int64_t>(mx, m_of(i)); dmx = std::max<int64_t>(dmx, d_of(i)); }
+        int64_t mx = 0, dmx = 0, tn = 0, te = 0, tp = 0;
+        for (int i = 0; i < n; i++) {
+            mx = std::max<int64_t>(mx, m_of(i));
+            dmx = std::max<int64_t>(dmx, d_of(i));
+            tn += m_of(i); te += e_of(i); tp += ddag.sz(kept[i], 2);
+        }
         int cls[3] = {0, 0, 0};
         for (int k : kept) cls[ddag.tier[k]]++;
         std::fprintf(stderr,
                      "[igr] dags on the device: %d batches, %d nets, %lld nodes, %lld edges, %lld points; max %lld nodes, "
-                     "depth %lld; work-area classes %d/%d/%d; trees %.3f s, sizes %.3f s, arrays %.3f s\n",
-                     B, n, (long long)ddag.h_node_at[n], (long long)ddag.h_edge_at[n], (long long)ddag.h_point_at[n],
-                     (long long)mx, (long long)dmx, cls[0], cls[1], cls[2], tb0 - th0, tb1 - tb0, tb3 - tb2);
+                     "depth %lld; work-area classes %d/%d/%d; trees %.3f s, build %.3f s\n",
+                     B, n, (long long)tn, (long long)te, (long long)tp, (long long)mx, (long long)dmx, cls[0], cls[1],
+                     cls[2], tb0 - th0, tb1 - tb0);
     }
     tm[3] = now_s();
     grow_routes(route_end);

@@ -89,23 +89,21 @@ struct DagBatchInfo {
     int nb, eb, pb, lb, nnb, nets, n, e, slots;
 };
 
-// Detour DAGs built on the device (dagbuild.cu) for a list of routing nets:
-// a size pass (nets whose DAG outgrows a thread's work area are built again
-// with larger slices), then, for the nets kept, a write pass into arrays laid
-// out end to end in list order.
+// Detour DAGs built on the device (dagbuild.cu) for a list of routing nets,
+// placed in node, edge and point pools.  DAGs that outgrow a thread's work
+// area are built again with larger slices; DAGs that find a pool full are
+// built again after the pools have grown (keeping what they hold).
 struct DeviceDags {
-    DevBuf<int> work, sizes, list, err;
+    DevBuf<int> work, sizes, list;
     DevBuf<long long> node_at, edge_at, point_at;
+    DevBuf<unsigned long long> used;
     DevBuf<int> nodes, par_num, child_num, depth, par, child_idx, points;
-    std::vector<int> hs;    // [k][kDagSizeFields] after measure()
+    double per_node = 64, per_edge = 80, per_point = 48;  // entries per DAG of the last build
+    std::vector<int> hs;    // [k][kDagSizeFields] after build()
     std::vector<int> tier;  // work-area size class each DAG fits
-    std::vector<long long> h_node_at, h_edge_at, h_point_at;  // [kept+1] after write()
-    // a.ids, a.n_list and the tree, congestion and grid fields set; list,
-    // sizes, work and the outputs are filled in here
-    void measure(DagBuildArgs a, cudaStream_t s);
-    // DAGs `kept` (positions of the measured list, ascending) written in that
-    // order; a.ids holds the kept nets' ids in the same order
-    void write(DagBuildArgs a, const std::vector<int> &kept, cudaStream_t s);
+    // a.ids, a.n_list and the tree, congestion and grid fields set; the rest
+    // is filled in here
+    void build(DagBuildArgs a, cudaStream_t s);
     int sz(int k, int f) const { return hs[(size_t)k * kDagSizeFields + f]; }
 };
 
@@ -312,6 +310,7 @@ struct Router {
     // device DAG construction: trees in adjacency order (positions, neighbour
     // lists), the builder, kept nets and the batch layout of the gather
     DevBuf<int> d_dt_off, d_dt_pos, d_dt_aoff, d_dt_adj, d_kept, d_gdesc, d_gbatch;
+    DevBuf<long long> d2_extat;
     bool dt_ready = false;
     DeviceDags ddag;
     // stream, events and the routing grid on the device; started on a thread of

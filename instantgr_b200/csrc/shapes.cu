@@ -63,15 +63,19 @@ __device__ __forceinline__ int point_claims(int x, int y, int X, int Y) {
 // ext_off[k+1]); its segments are always the tree's
 struct ShapeSrc {
     const int *tree_off, *tree_nodes, *tree_par, *ids, *ext_off, *ext_pts;
-    int n, X, Y, sp;
+    const long long *ext_at;
+    const int *ext_cnt;
+    int ext_stride, n, X, Y, sp;
 };
 
 template <class Pt, class Hs, class Vs>
 __device__ __forceinline__ void shape_of(const ShapeSrc &a, int k, Pt &&point, Hs &&hseg, Vs &&vseg) {
     const int net = a.ids ? a.ids[k] : k;
     const int t = a.tree_off[net], m = a.tree_off[net + 1] - t;
-    if (a.ext_off) {
-        for (int q = a.ext_off[k]; q < a.ext_off[k + 1]; q++) point(a.ext_pts[q] / a.Y, a.ext_pts[q] % a.Y);
+    if (a.ext_off || a.ext_at) {
+        const long long q0 = a.ext_at ? a.ext_at[k] : a.ext_off[k];
+        const long long q1 = a.ext_at ? q0 + a.ext_cnt[(size_t)k * a.ext_stride] : a.ext_off[k + 1];
+        for (long long q = q0; q < q1; q++) point(a.ext_pts[q] / a.Y, a.ext_pts[q] % a.Y);
         net_shapes(a.tree_nodes + t, a.tree_par + t, m, a.X, a.Y, [](int, int) {}, hseg, vseg);
     } else {
         net_shapes(a.tree_nodes + t, a.tree_par + t, m, a.X, a.Y, point, hseg, vseg);
@@ -153,14 +157,16 @@ __global__ void shape_fill_kernel(ShapeSrc a, const int *pt_off, const int *clai
 }  // namespace
 
 void launch_shape_count(const ShapeArgs &a, int *pt_off, int *claim_off, long long *totals, cudaStream_t s) {
-    const ShapeSrc src{a.tree_off, a.tree_nodes, a.tree_par, a.ids, a.ext_off, a.ext_pts, a.n, a.X, a.Y, a.sparsity};
+    const ShapeSrc src{a.tree_off, a.tree_nodes, a.tree_par, a.ids, a.ext_off, a.ext_pts, a.ext_at,
+                       a.ext_cnt, a.ext_stride, a.n, a.X, a.Y, a.sparsity};
     if (a.n > 0) shape_count_kernel<<<(a.n + 255) / 256, 256, 0, s>>>(src, pt_off, claim_off);
     shape_scan_kernel<<<1, kScanThreads, 0, s>>>(a.n, pt_off, claim_off, totals);
 }
 
 void launch_shape_fill(const ShapeArgs &a, const int *pt_off, const int *claim_off, int *pts, int *claim,
                        cudaStream_t s) {
-    const ShapeSrc src{a.tree_off, a.tree_nodes, a.tree_par, a.ids, a.ext_off, a.ext_pts, a.n, a.X, a.Y, a.sparsity};
+    const ShapeSrc src{a.tree_off, a.tree_nodes, a.tree_par, a.ids, a.ext_off, a.ext_pts, a.ext_at,
+                       a.ext_cnt, a.ext_stride, a.n, a.X, a.Y, a.sparsity};
     if (a.n > 0) shape_fill_kernel<<<(a.n + 255) / 256, 256, 0, s>>>(src, pt_off, claim_off, pts, claim);
 }
 
