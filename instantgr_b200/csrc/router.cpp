@@ -1034,6 +1034,7 @@ bool Router::rrr_pass(int iter) {
     const int R = (int)ns.nets.size();
     const int X = ns.X, Y = ns.Y;
     if (R == 0) return false;
+    const double tp0 = now_s();
     of_sum.alloc(go.g.N);
     d_is_of.alloc(R);
     d_xsum.alloc((size_t)X * Y);
@@ -1086,7 +1087,12 @@ bool Router::rrr_pass(int iter) {
             return ns.nets[l].hpwl > ns.nets[r].hpwl;
         });
     } else {
-        std::sort(of_nets.begin(), of_nets.end(), [&](int l, int r) { return ns.nets[l].hpwl > ns.nets[r].hpwl; });
+        // the comparisons of the reference's sort, on a contiguous copy of the keys
+        std::vector<int> hp(R);
+        parallel_for(R, threads, [&](int b, int e) {
+            for (int i = b; i < e; i++) hp[i] = ns.nets[i].hpwl;
+        });
+        std::sort(of_nets.begin(), of_nets.end(), [&](int l, int r) { return hp[l] > hp[r]; });
     }
     // per colour batch: its first entries in the arrays of the pass and its sizes
     std::vector<std::vector<int>> batches;
@@ -1348,9 +1354,9 @@ bool Router::rrr_pass(int iter) {
     if (int e = go.check_error(s)) throw Error(e, "device error in rip-up and reroute");
     if (verbose)
         std::fprintf(stderr,
-                     "[igr] pass %d host: DAGs %.3f s, conflict shapes %.3f s, colouring %.3f s, batch arrays %.3f s, "
-                     "batches on the device %.3f s\n",
-                     iter, t_dag - th0, t_shapes - t_dag, t_color - t_shapes, t_csr - t_color, now_s() - t_csr);
+                     "[igr] pass %d host: marking and order %.3f s, DAGs %.3f s, conflict shapes %.3f s, colouring %.3f s, "
+                     "batch arrays %.3f s, batches on the device %.3f s\n",
+                     iter, th0 - tp0, t_dag - th0, t_shapes - t_dag, t_color - t_shapes, t_csr - t_color, now_s() - t_csr);
     return true;
 }
 
