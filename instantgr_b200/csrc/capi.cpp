@@ -614,6 +614,13 @@ int igr_color_batches(igr_ctx *c, int n, const int32_t *pt_off, const int32_t *p
         cd.claim_off = dco.p; cd.claim = dcl.p;
         cd.active = act.p; cd.active2 = act.p + n; cd.cand = act.p + 2 * (size_t)n; cd.lost = act.p + 3 * (size_t)n;
         cd.hdr = hdr.p;
+        DevBuf<int> rev_off, rev_cnt, rev, snap, dirty, part;
+        if (cl.size() < (size_t)INT32_MAX) {  // round-0 map kept up to date across batches
+            rev_off.alloc(XY); rev_cnt.alloc(XY); rev.alloc(std::max<size_t>(1, cl.size()));
+            snap.alloc(XY); dirty.alloc(XY); part.alloc(1024);
+            cd.rev_off = rev_off.p; cd.rev_cnt = rev_cnt.p; cd.rev = rev.p; cd.snap = snap.p; cd.dirty = dirty.p;
+            cd.part = part.p;
+        }
         const int nb = run_coloring(cd, 0, c->s);
         if (nb == -2) throw Error(ERR_TIMEOUT, "colouring barrier timed out");
         if (nb < 0) throw Error(ERR_CUDA, std::string("colouring launch failed: ") + cudaGetErrorString(cudaGetLastError()));

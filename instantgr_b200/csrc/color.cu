@@ -23,6 +23,14 @@
 // kernel; the last rounds of a batch, which have few candidates, run in one
 // block with block barriers.  Every grid barrier gives up after two seconds
 // and reports ERR_TIMEOUT instead of waiting forever.
+//
+// Optionally (ColorDev::rev set) the round-0 map of every batch is kept up to
+// date instead of being cleared and re-claimed by every net without a batch:
+// the claimers of each cell are grouped by cell once; after a batch, each cell
+// whose round-0 owner joined gets as new owner its highest claimer still
+// without a batch (one warp per such cell, assigned claimers dropped from the
+// list), which is the max the re-claim would give, since every other cell's
+// owner is still without a batch and still the highest of a smaller set.
 #include "gridsync.cuh"
 #include "host.hpp"
 
@@ -42,7 +50,7 @@ constexpr int kBlockRounds = 2 * kGroups;
 // flags (ints): [2] batches, [4] barrier counter, [6] error, [8] rounds run,
 // [9] lost count, [10] next candidate count, [11..12] nets left after a batch
 // (by batch parity)
-enum : int { F_NB = 2, F_BAR = 4, F_ERR = 6, F_ROUNDS = 8, F_LOST = 9, F_CAND = 10, F_LEFT = 11 };
+enum : int { F_NB = 2, F_BAR = 4, F_ERR = 6, F_ROUNDS = 8, F_LOST = 9, F_CAND = 10, F_LEFT = 11, F_DIRTY = 13 };
 
 // memory operations of this thread, summed into c.ops at the end (roofline
 // accounting): claimed cells, points checked for commit, points checked for
@@ -78,6 +86,35 @@ __device__ __forceinline__ void flush(Stage &st, int *list, int *count) {
     }
     if (threadIdx.x == 0) st.n = 0;
     __syncthreads();
+}
+
+// exclusive prefix of v over the block's threads (all threads call it); *total
+// receives the block's sum
+__device__ int block_exclusive(int v, int *total) {
+    __shared__ int warp_sum[kThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int t = lane < kThreads / 32 ? warp_sum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < kThreads / 32) warp_sum[lane] = t;  // inclusive over warps
+    }
+    __syncthreads();
+    const int before = (wid ? warp_sum[wid - 1] : 0) + x - v;
+    *total = warp_sum[kThreads / 32 - 1];
+    __syncthreads();
+    return before;
 }
 
 // map and batch change during the kernel: read them from L2
@@ -237,8 +274,54 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
         c.hdr[k] = make_int4(c.claim_off[sh], c.claim_off[sh + 1], c.pt_off[sh], c.pt_off[sh + 1]);
         act[k] = k;
     }
-    for (int i = tid; i < XY; i += nth) c.map[i] = -1;
+    const bool inc = c.rev != nullptr;
+    for (int i = tid; i < XY; i += nth) {
+        c.map[i] = -1;
+        if (inc) c.rev_cnt[i] = 0;
+    }
     if (!grid_sync(bar, err, epoch)) return;
+    if (inc) {
+        // claimers of every cell (ranks), grouped by cell: counts, an exclusive
+        // scan over the cells (a chunk per block), then the entries
+        for (int k = tid; k < c.n; k += nth) {
+            const int4 h = c.hdr[k];
+            for (int i = h.x; i < h.y; i++) atomicAdd(c.rev_cnt + __ldg(c.claim + i), 1);
+        }
+        if (!grid_sync(bar, err, epoch)) return;
+        const int chunk = (XY + gridDim.x - 1) / gridDim.x;
+        const int lo = min(XY, blockIdx.x * chunk), hi = min(XY, lo + chunk);
+        const int per = (hi - lo + kThreads - 1) / kThreads;
+        const int a0 = min(hi, lo + threadIdx.x * per), a1 = min(hi, a0 + per);
+        int mine = 0, total = 0;
+        for (int i = a0; i < a1; i++) mine += c.rev_cnt[i];
+        int run = block_exclusive(mine, &total);
+        if (threadIdx.x == 0) c.part[blockIdx.x] = total;
+        if (!grid_sync(bar, err, epoch)) return;
+        if (tid == 0) {
+            int acc = 0;
+            for (int b = 0; b < (int)gridDim.x; b++) {
+                const int t = c.part[b];
+                c.part[b] = acc;
+                acc += t;
+            }
+        }
+        if (!grid_sync(bar, err, epoch)) return;
+        run += c.part[blockIdx.x];
+        for (int i = a0; i < a1; i++) {
+            c.rev_off[i] = run;
+            run += c.rev_cnt[i];
+            c.rev_cnt[i] = 0;
+        }
+        if (!grid_sync(bar, err, epoch)) return;
+        for (int k = tid; k < c.n; k += nth) {
+            const int4 h = c.hdr[k];
+            for (int i = h.x; i < h.y; i++) {
+                const int cell = __ldg(c.claim + i);
+                c.rev[c.rev_off[cell] + atomicAdd(c.rev_cnt + cell, 1)] = k;
+            }
+        }
+        if (!grid_sync(bar, err, epoch)) return;
+    }
     int na = c.n;
     for (int cur = 0; cur < max_batches; cur++) {
         const int *cand = act;  // round 0: every net without a batch
@@ -250,16 +333,23 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
                 tail = true;
                 break;
             }
+            // with the round-0 map kept up to date, round 0 of a later batch
+            // starts from it (its counters were reset before the last barrier)
+            const bool kept = inc && round == 0 && cur > 0;
             if (tid == 0) {
                 flags[F_ROUNDS]++;
-                flags[F_LOST] = 0;
+                if (!kept) flags[F_LOST] = 0;
             }
-            claim_phase(c, cand, nc, blockIdx.x, gridDim.x, ops);
-            if (!grid_sync(bar, err, epoch)) return;
-            if (tid == 0) {
-                flags[F_CAND] = 0;
-                if (round == 0) flags[F_LEFT + ((cur + 1) & 1)] = 0;
+            if (!kept) {
+                claim_phase(c, cand, nc, blockIdx.x, gridDim.x, ops);
+                if (!grid_sync(bar, err, epoch)) return;
+                if (tid == 0) {
+                    flags[F_CAND] = 0;
+                    if (round == 0) flags[F_LEFT + ((cur + 1) & 1)] = 0;
+                }
             }
+            if (inc && round == 0 && cur == 0)  // the first round-0 map, before any release
+                for (int i = tid; i < XY; i += nth) c.snap[i] = __ldcg(c.map + i);
             commit_phase(c, st, cand, nc, cur, flags + F_LOST, blockIdx.x, gridDim.x, ops);
             if (!grid_sync(bar, err, epoch)) return;
             const int nl = vflags[F_LOST];
@@ -274,14 +364,29 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
             if (blockIdx.x == 0) block_rounds(c, st, round, nc, cur, flags + F_ROUNDS, ops);
             if (!grid_sync(bar, err, epoch)) return;
         }
-        // nets still without a batch stay active; the map is cleared for the next batch
-        for (int i = tid; i < XY; i += nth) c.map[i] = -1;
+        // nets still without a batch stay active; the map is cleared for the
+        // next batch, or, when the round-0 map is kept, the cells whose
+        // round-0 owner joined this batch are marked for recomputation
+        if (!inc)
+            for (int i = tid; i < XY; i += nth) c.map[i] = -1;
         int it = 0;
         for (int b0 = blockIdx.x * kThreads; b0 < na; b0 += nth, it++) {
             const int i = b0 + threadIdx.x;
             const int k = i < na ? act[i] : -1;
+            const int bk = k >= 0 ? __ldcg(c.batch + k) : -2;
             if (k >= 0) ops.scans++;
-            stage(st, k >= 0 && __ldcg(c.batch + k) == -1, k, lane);
+            if (inc && bk == cur) {
+                const int4 h = c.hdr[k];
+                ops.releases += h.y - h.x;
+                for (int q = h.x; q < h.y; q++) {
+                    const int cell = __ldg(c.claim + q);
+                    if (c.snap[cell] == k) {
+                        c.snap[cell] = -1;
+                        c.dirty[atomicAdd(flags + F_DIRTY, 1)] = cell;
+                    }
+                }
+            }
+            stage(st, bk == -1, k, lane);
             if ((it + 1) % (kBuf / kThreads) == 0) flush(st, act2, flags + F_LEFT + (cur & 1));
         }
         flush(st, act2, flags + F_LEFT + (cur & 1));
@@ -292,6 +397,45 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
             if (tid == 0) flags[F_NB] = cur + 1;
             sum_ops();
             return;
+        }
+        if (inc) {
+            // new round-0 owner of every marked cell: its highest claimer
+            // still without a batch (claimers with a batch leave the list)
+            // one warp per marked cell: 32 claimers per step, compacted in place
+            // (a step writes only below the entries it has read)
+            const int nd = vflags[F_DIRTY];
+            for (int i = tid >> 5; i < nd; i += nth >> 5) {
+                const int cell = c.dirty[i];
+                const int base = c.rev_off[cell], len = c.rev_cnt[cell];
+                int best = -1, w = 0;
+                for (int q0 = 0; q0 < len; q0 += 32) {
+                    const int q = q0 + lane;
+                    const int k = q < len ? c.rev[base + q] : -1;
+                    const bool live = k >= 0 && __ldcg(c.batch + k) == -1;
+                    const unsigned m = __ballot_sync(0xffffffffu, live);
+                    if (live) {
+                        c.rev[base + w + __popc(m & ((1u << lane) - 1))] = k;
+                        best = max(best, k);
+                    }
+                    w += __popc(m);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+                if (lane == 0) {
+                    ops.scans += len;
+                    c.rev_cnt[cell] = w;
+                    c.snap[cell] = best;
+                }
+            }
+            if (!grid_sync(bar, err, epoch)) return;
+            for (int i = tid; i < XY; i += nth) c.map[i] = c.snap[i];
+            if (tid == 0) {  // counters of round 0 of the next batch
+                flags[F_DIRTY] = 0;
+                flags[F_LOST] = 0;
+                flags[F_CAND] = 0;
+                flags[F_LEFT + ((cur + 2) & 1)] = 0;
+            }
+            if (!grid_sync(bar, err, epoch)) return;
         }
     }
     if (tid == 0) flags[F_NB] = max_batches;

@@ -288,6 +288,10 @@ struct ColorDev {
     unsigned long long *ops = nullptr;
     int *flags = nullptr;     // [16] device flags
     int rounds = 0;           // out: colouring rounds run
+    // optional (all or none): the round-0 map of every batch kept up to date
+    // instead of re-claimed.  rev_off/rev_cnt [X*Y]: claimers of each cell in
+    // rev[] (ranks; [total claims]); snap/dirty [X*Y]; part [1024]
+    int *rev_off = nullptr, *rev_cnt = nullptr, *rev = nullptr, *snap = nullptr, *dirty = nullptr, *part = nullptr;
 };
 // Claim lists of shapes (pt_off/pts/h_off/hseg/v_off/vseg as in ColorDev).
 void build_claims(int nshapes, const int *pt_off, const int *pts, const int *h_off, const int *hseg,

@@ -997,6 +997,10 @@ void Router::color_nets(const std::vector<int> &order, const ShapeDev &shapes, i
     }
 }
 
+namespace {
+constexpr int kColorKeepMapNets = 2000000;
+}  // namespace
+
 int Router::run_color(int n, const int *d_perm_ranks, const ShapeDev &shapes, int sparsity) {
     d_map.alloc((size_t)ns.X * ns.Y);
     d_bat.alloc(n);
@@ -1014,6 +1018,18 @@ int Router::run_color(int n, const int *d_perm_ranks, const ShapeDev &shapes, in
     cd.hdr = d_hdr.p;
     cd.ops = d_cops.p;
     cd.npts = shapes.npts; cd.map = d_map.p; cd.batch = d_bat.p; cd.flags = d_flags.p;
+    // Round-0 map kept up to date across batches instead of re-claimed: it
+    // pays on the largest colourings only (10M-net design: 1.57 s to 1.28 s
+    // in phase 1, 12% in the rip-up passes), while the recomputation of the
+    // cells whose owner joined costs about as much as the claims it saves on
+    // designs of up to a million nets (130k-net design: 3.5 ms to 7.2 ms).
+    if (n >= kColorKeepMapNets && shapes.claim.n < (size_t)INT32_MAX) {
+        const size_t XY = (size_t)ns.X * ns.Y;
+        d_rev_off.alloc(XY); d_rev_cnt.alloc(XY); d_rev.alloc(std::max<size_t>(1, shapes.claim.n));
+        d_snap.alloc(XY); d_dirty.alloc(XY); d_part.alloc(1024);
+        cd.rev_off = d_rev_off.p; cd.rev_cnt = d_rev_cnt.p; cd.rev = d_rev.p; cd.snap = d_snap.p;
+        cd.dirty = d_dirty.p; cd.part = d_part.p;
+    }
     const double t0 = verbose ? now_s() : 0;
     kt.begin(KC_COLOR);
     int nb = run_coloring(cd, 0, s);

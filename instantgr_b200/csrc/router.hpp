@@ -227,6 +227,7 @@ struct Router {
     double dp_bytes = 0;                // algorithmic bytes of one phase-1 tree DP pass
     int64_t setup_h2d = 0;              // host-to-device bytes of the device setup
     DevBuf<int> d_ids, d_all_ids, of_sum, d_perm, d_map, d_bat, d_act, d_flags, d_queue;
+    DevBuf<int> d_rev_off, d_rev_cnt, d_rev, d_snap, d_dirty, d_part;  // colouring: claimers per cell, round-0 map
     // launch shape of the tree DP per size class (large, medium, small) and the
     // node count that separates small from medium nets (autotuned, see tune.cpp)
     struct Tune {

@@ -154,7 +154,7 @@ def test_ripup_and_overflow_marking_match_oracle():
     np.testing.assert_allclose(of, o.overflow_cost(d2), rtol=RTOL)
 
 
-@pytest.mark.parametrize("seed,n", [(31, 300), (32, 1500)])
+@pytest.mark.parametrize("seed,n", [(31, 300), (32, 1500), (33, 6000)])
 def test_coloring_matches_oracle(seed, n):
     X, Y = 64, 48
     args = cases.color_case(seed, X, Y, n)
