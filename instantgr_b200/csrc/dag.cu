@@ -27,6 +27,9 @@ constexpr int kML = 10;                      // MAX_LAYER of the reference
 constexpr unsigned long long kInitPacked = 7208259049189261824ULL;  // init_cost_with_road
 constexpr int kDagWarps = 8;                 // warps of one net's CTA
 constexpr int kDagThreads = 32 * kDagWarps;
+constexpr int kSmallWarps = 2;               // warps of a small net's CTA
+constexpr int kSmallNodes = 64;              // a small net's DAG has at most this many nodes
+constexpr int kSplitNets = 4096;             // batches of at least this many nets split by size
 
 __device__ __forceinline__ int32_t f2o(float f) {
     int32_t i = __float_as_int(f);
@@ -431,16 +434,22 @@ __device__ void compact_net(const GridDev &g, const DagBatchDev &b, int k, int l
     if (lane == 0) r[0] = base <= cap ? base : 1;
 }
 
-// one CTA per net: initialisation, DP levels deepest first, trace levels root
-// first, compaction
-__global__ void __launch_bounds__(kDagThreads) dag_net_kernel(GridDev g, DagBatchDev b, int stamp) {
-    __shared__ NodeScratch scr[kDagWarps];
+// one CTA of W warps per net: initialisation, DP levels deepest first, trace
+// levels root first, compaction.  Sizes: 0 every net, 1 nets of at most
+// kSmallNodes nodes, 2 the larger ones (small DAGs have narrow levels, so a
+// 2-warp CTA leaves fewer warps waiting at the level barriers and more CTAs
+// fit an SM)
+template <int W, int Sizes>
+__global__ void __launch_bounds__(32 * W) dag_net_kernel(GridDev g, DagBatchDev b, int stamp) {
+    constexpr int kThreadsW = 32 * W;
+    __shared__ NodeScratch scr[W];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     for (int k = blockIdx.x; k < b.n_nets; k += gridDim.x) {
         const int n0 = b.net_node_off[k], n1 = b.net_node_off[k + 1];
+        if ((Sizes == 1 && n1 - n0 > kSmallNodes) || (Sizes == 2 && n1 - n0 <= kSmallNodes)) continue;
         const int64_t s0 = (int64_t)b.child_off[n0] * kML, s1 = (int64_t)b.child_off[n1] * kML;
-        for (int64_t i = s0 + tid; i < s1; i += kDagThreads) b.packed[i] = kInitPacked;
-        for (int v = n0 + tid; v < n1; v += kDagThreads) {
+        for (int64_t i = s0 + tid; i < s1; i += kThreadsW) b.packed[i] = kInitPacked;
+        for (int v = n0 + tid; v < n1; v += kThreadsW) {
             b.layer_out[v] = -1;
             b.stage_cnt[v] = 0;
         }
@@ -448,12 +457,12 @@ __global__ void __launch_bounds__(kDagThreads) dag_net_kernel(GridDev g, DagBatc
         const int l0 = b.net_level_off[k], nl = b.net_level_off[k + 1] - l0 - 1;
         for (int d = nl - 1; d >= 0; d--) {
             const int a = b.level_off[l0 + d], e = b.level_off[l0 + d + 1];
-            for (int s = a + warp; s < e; s += kDagWarps) dp_node_warp(g, b, b.level_nodes[s], lane, scr[warp]);
+            for (int s = a + warp; s < e; s += W) dp_node_warp(g, b, b.level_nodes[s], lane, scr[warp]);
             __syncthreads();
         }
         for (int d = 0; d < nl; d++) {
             const int a = b.level_off[l0 + d], e = b.level_off[l0 + d + 1];
-            for (int s = a + tid; s < e; s += kDagThreads) trace_node(g, b, b.level_nodes[s], stamp);
+            for (int s = a + tid; s < e; s += kThreadsW) trace_node(g, b, b.level_nodes[s], stamp);
             __syncthreads();
         }
         if (warp == 0) compact_net(g, b, k, lane);
@@ -483,15 +492,28 @@ void dag_levels(int n, const int *node_off, const int *depth, std::vector<int> &
     }
 }
 
-int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStream_t s) {
+int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStream_t s, cudaStream_t aux,
+                     cudaEvent_t fork, cudaEvent_t join) {
     if (b.n_nodes <= 0 || b.n_nets <= 0) return 0;
     int launches = 0;
     if (b.n_edges > 0) {
         dag_edge_cost_kernel<<<(int)((b.n_edges + kEdgeWarps - 1) / kEdgeWarps), 32 * kEdgeWarps, 0, s>>>(g, b);
         launches++;
     }
-    dag_net_kernel<<<b.n_nets, kDagThreads, 0, s>>>(g, b, stamp);
-    return launches + 1;
+    if (!aux || b.n_nets < kSplitNets) {
+        dag_net_kernel<kDagWarps, 0><<<b.n_nets, kDagThreads, 0, s>>>(g, b, stamp);
+        return launches + 1;
+    }
+    // a batch of many nets: the large nets' CTAs on the side stream, beside
+    // the small nets' 2-warp CTAs (the nets of a batch share no state); a
+    // smaller batch is bound by its largest net and gains nothing from it
+    cudaEventRecord(fork, s);
+    cudaStreamWaitEvent(aux, fork, 0);
+    dag_net_kernel<kDagWarps, 2><<<b.n_nets, kDagThreads, 0, aux>>>(g, b, stamp);
+    dag_net_kernel<kSmallWarps, 1><<<b.n_nets, 32 * kSmallWarps, 0, s>>>(g, b, stamp);
+    cudaEventRecord(join, aux);
+    cudaStreamWaitEvent(s, join, 0);
+    return launches + 2;
 }
 
 }  // namespace igr

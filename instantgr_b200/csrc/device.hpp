@@ -124,7 +124,10 @@ struct DagBatchDev {
 void dag_levels(int n, const int *node_off, const int *depth, std::vector<int> &level_nodes,
                 std::vector<int> &level_off, std::vector<int> &net_level_off);
 // edge costs, then one CTA per net; returns the number of kernel launches
-int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStream_t s);
+// aux, fork, join (optional): in batches of 4096 nets or more, the DAGs of
+// more than 64 nodes run on `aux` beside the smaller ones
+int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStream_t s, cudaStream_t aux = nullptr,
+                     cudaEvent_t fork = nullptr, cudaEvent_t join = nullptr);
 
 constexpr int kRouteLayers = 9;
 
