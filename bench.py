@@ -1,19 +1,33 @@
 #!/usr/bin/env python
-"""Benchmark of the GPU global-routing hot path (InstantGR's metric: route
-wall time and nets/s at equal evaluator score).
+"""Benchmark of the GPU global-routing hot path, on InstantGR's metric: route
+wall time and nets/s at equal evaluator score, plain form against the batched
+form with the learned congestion seed.
 
-One step = one complete route of the synthetic design with the design already
-read and its trees built (inputs resident): phase 1 (colouring, per-batch
-cost refresh, tree DP, commit) and `--rrr-iters` rip-up-and-reroute passes.
-Default workload: 10 layers, 840x1140 GCells, 130,000 nets, 3 RRR passes.
+One step = one complete route of the design with the design read and its trees
+built (inputs resident): colouring, phase 1 (per batch: cost refresh, tree DP,
+commit) and `--rrr-iters` rip-up-and-reroute passes (overflow marking, detour
+DAGs, colouring, per batch: rip-up, cost refresh, DAG DP, commit).
+Default workload: 10 layers, 1600x1600 GCells, 800,000 nets (pin-count mixture,
+6 hotspots), 3 RRR passes.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+`value` = design nets per second of the plain drop-in form (K CUDA-event-timed
+steps); the batched form and the batched form with the learned seed are timed
+beside it, each with its evaluator total.  `e2e` = the same
+metric through the public API with host files every step (open: read, pins,
+trees, device set-up; route; write the guides).  `reference_gpu` = the
+reference's own sm_100a build (oracle/_ref/instantgr_ref) and this project's
+command line on the same design, wall time and evaluator totals.
+
 N > 1 runs N independent replicas (the router does not shard), one per GPU;
 `value` is the nets of all replicas over the slowest replica's time.
-`--impl reference` times the CPU restatement of the same hot path (the
-oracle: cost refresh, tree DP and commit per batch, phase 1 only) on the host
-cores, on a bounded sample of the same plan.
+
+`--impl reference` times the reference's CPU implementation of the path
+(oracle/_ref/ref_cpu: the reference's own host code, and the oracle for the
+stages it runs only as CUDA kernels) on the host cores, on a window of the same
+design: the nets whose access points all lie in a centred window covering
+`--ref-window` of each side.  It loads none of this project's router code.
 """
 from __future__ import annotations
 
@@ -28,39 +42,72 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+GEN_BIN = os.path.join(ROOT, "instantgr_b200", "bin", "igr_generate")
+ROUTE_BIN = os.path.join(ROOT, "instantgr_b200", "bin", "igr_route")
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 
 CONFIGS = {
     0: dict(name="256x256x10, 20k nets", X=256, Y=256, nets=20000),
-    1: dict(name="840x1140x10, 130k nets, 1% 65-500-pin nets, 3 RRR passes", X=840, Y=1140, nets=130000),
-    2: dict(name="1600x1600x10, 800k nets, pin mixture, 6 hotspots", X=1600, Y=1600, nets=800000),
+    1: dict(name="840x1140x10, 130k nets, 1% 65-500-pin nets", X=840, Y=1140, nets=130000),
+    2: dict(name="1600x1600x10, 800k nets, pin mixture 70/20/9.5/0.5%, 6 hotspots", X=1600, Y=1600, nets=800000),
+    4: dict(name="3000x3000x10, 10M nets, 4 clusters", X=3000, Y=3000, nets=10000000),
 }
+METRIC = "route throughput (design nets/s): plain vs batched+learned at equal evaluator score"
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=1)
+    ap.add_argument("--config", type=int, default=2)
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--rrr-iters", type=int, default=3)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--ref-window", type=float, default=0.5,
+                    help="side of the reference arm's centred window, as a fraction of the grid's sides")
     ap.add_argument("--workdir", default=os.environ.get("IGR_BENCH_DIR", "/tmp/igr_bench"))
-    ap.add_argument("--cpu-batches", type=int, default=0, help="batches in the CPU sample (0 = auto)")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference sm_100a build's run")
     ap.add_argument("--route-only", action="store_true",
                     help="route --warmup + --steps times and print the router statistics (profiling runs)")
+    ap.add_argument("--form", default="plain", choices=["plain", "batched", "learned"],
+                    help="router form of --route-only")
     return ap.parse_args()
 
 
-def route_only(args):
-    import instantgr_b200 as ig
-    cap, net = design_files(args)
-    r = ig.Router(cap, net, rrr_iters=args.rrr_iters, profile=1)
-    for _ in range(args.warmup + args.steps):
-        r.run()
-    print(json.dumps(dict(stats=r.stats(), kernels=r.kstats())), flush=True)
-    r.close()
+def workload(args) -> dict:
+    cfg = CONFIGS[args.config]
+    return dict(workload=f"global routing, {cfg['name']}, {args.rrr_iters} RRR passes", headline_form="plain",
+                config_index=args.config,
+                scale=args.scale, rrr_iters=args.rrr_iters, seed=args.seed,
+                l2="per-step state exceeds L2 (inputs larger than L2)")
+
+
+def design_files(args, window=None) -> tuple[str, str]:
+    """The seeded design (or a window of it), written by the stand-alone generator."""
+    os.makedirs(args.workdir, exist_ok=True)
+    tag = "" if window is None else "_w%d_%d_%d_%d" % tuple(window)
+    base = os.path.join(args.workdir, f"c{args.config}_s{args.seed}_x{args.scale:g}{tag}")
+    cap, net = base + ".cap", base + ".net"
+    if not (os.path.exists(cap) and os.path.exists(net)):
+        tmpc, tmpn = cap + f".{os.getpid()}", net + f".{os.getpid()}"
+        cmd = [GEN_BIN, "--config", str(args.config), "--seed", str(args.seed), "--scale", str(args.scale),
+               "--cap", tmpc, "--net", tmpn]
+        if window is not None:
+            cmd += ["--window"] + [str(v) for v in window]
+        subprocess.run(cmd, check=True)
+        os.replace(tmpc, cap)
+        os.replace(tmpn, net)
+    return cap, net
+
+
+def ref_window(args) -> list[int]:
+    """Centred window of the reference arm's sample: [x0, y0, w, h]."""
+    cfg = CONFIGS[args.config]
+    w = max(2, int(round(cfg["X"] * args.ref_window)))
+    h = max(2, int(round(cfg["Y"] * args.ref_window)))
+    return [(cfg["X"] - w) // 2, (cfg["Y"] - h) // 2, w, h]
 
 
 class Clocks:
@@ -106,19 +153,6 @@ class Clocks:
                     reasons=reasons, samples=len(self.rows))
 
 
-def design_files(args) -> tuple[str, str]:
-    os.makedirs(args.workdir, exist_ok=True)
-    base = os.path.join(args.workdir, f"c{args.config}_s{args.seed}_x{args.scale:g}")
-    cap, net = base + ".cap", base + ".net"
-    if not (os.path.exists(cap) and os.path.exists(net)):
-        import instantgr_b200 as ig
-        tmpc, tmpn = cap + f".{os.getpid()}", net + f".{os.getpid()}"
-        ig.generate(args.config, args.seed, args.scale, tmpc, tmpn)
-        os.replace(tmpc, cap)
-        os.replace(tmpn, net)
-    return cap, net
-
-
 def measured_peaks() -> dict:
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -144,8 +178,8 @@ def replica_throughput(nets_per_replica: int, steps: int, world: int, max_ms: fl
     return nets_per_replica * steps * world / (max_ms / 1e3)
 
 
-def omp_threads() -> int:
-    """Host threads the OpenMP-parallel oracle uses (all cores unless OMP_NUM_THREADS says otherwise)."""
+def host_threads() -> int:
+    """Host threads the CPU baselines use (all cores unless OMP_NUM_THREADS says otherwise)."""
     v = os.environ.get("OMP_NUM_THREADS", "")
     return int(v) if v.isdigit() and int(v) > 0 else (os.cpu_count() or 1)
 
@@ -159,40 +193,95 @@ def profile_traffic() -> dict:
     return {}
 
 
-def cpu_sample(router, grid, plan, max_batches: int, budget_s: float = 20.0):
-    """CPU restatement (oracle) of the phase-1 hot path on the first batches of the
-    same plan: per batch a full cost refresh, the tree DP and the commits."""
-    import numpy as np
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from oracle_py import Oracle
-    o = Oracle(grid)
-    N = o.N
-    dem = np.zeros(N, np.float32)
-    pre = np.zeros(N, np.int32)
-    st = np.zeros(N, np.int32)
-    w = np.zeros(N, np.float32)
-    boff = plan["batch_off"]
-    nb = len(boff) - 1
-    cap = plan["route_cap"].astype(np.int64)
-    roff = np.concatenate([[0], np.cumsum(cap)[:-1]]).astype(np.int64)
-    routes = np.zeros(int(cap.sum()) + 1, np.int32)
-    t0 = time.perf_counter()
-    nets = 0
-    b = 0
-    while b < nb and (max_batches == 0 or b < max_batches):
-        a, e = int(boff[b]), int(boff[b + 1])
-        _, vc, ps = o.cost_refresh(dem)
-        n0, n1 = int(plan["node_off"][a]), int(plan["node_off"][e])
-        o.pattern_route(vc, ps, plan["node_off"][a:e + 1] - n0, plan["nodes"][n0:n1], plan["par"][n0:n1],
-                        roff[a:e], plan["route_cap"][a:e], routes, pre, st, b + 1)
-        o.commit_wires(pre, dem, st, b + 1)
-        o.commit_vias(roff[a:e], routes, dem, st, b + 1, 1)
-        nets += e - a
-        b += 1
-        if max_batches == 0 and time.perf_counter() - t0 > budget_s:
-            break
-    dt = time.perf_counter() - t0
-    return nets / dt, dict(batches=b, of_batches=nb, nets=nets, seconds=dt)
+def run_ref_cpu(cap: str, net: str, steps: int, warmup: int, rrr: int, threads: int, timeout: float = 1500) -> dict:
+    """The reference route on the host cores (oracle/_ref/ref_cpu); its setup
+    record and per-step records."""
+    exe = os.path.join(REF_DIR, "ref_cpu")
+    if not os.path.exists(exe):
+        raise RuntimeError(f"{exe} missing (built by `make -C oracle ref` where the reference tree is present)")
+    p = subprocess.run([exe, cap, net, str(steps), str(warmup), str(rrr), str(threads)], capture_output=True,
+                       text=True, timeout=timeout)
+    recs = [json.loads(line[7:]) for line in p.stdout.splitlines() if line.startswith("REFCPU ")]
+    if p.returncode != 0 or not recs:
+        raise RuntimeError(f"ref_cpu failed (rc {p.returncode}): {p.stderr[-400:]}")
+    setup = recs[0]
+    timed = [r for r in recs[1:] if r.get("timed")]
+    if len(timed) != steps:
+        raise RuntimeError(f"ref_cpu printed {len(timed)} timed steps of {steps}")
+    return dict(setup=setup, steps=timed)
+
+
+def evaluator_total(cap: str, net: str, out: str) -> dict:
+    """The reference evaluator's FOR_STAT (run/evaluator.cpp) of a guide file."""
+    p = subprocess.run([os.path.join(REF_DIR, "evaluator"), cap, net, out], capture_output=True, text=True,
+                       timeout=900)
+    for line in p.stdout.splitlines():
+        if line.startswith("FOR_STAT"):
+            wl, via, of, tot = (float(v) for v in line.split()[1:5])
+            return dict(wirelength=wl, via=via, overflow=of, total=tot)
+    return dict(error=f"no FOR_STAT (rc {p.returncode})")
+
+
+def reference_gpu(cap: str, net: str, workdir: str, rrr_iters: int) -> dict:
+    """CLI wall time of the reference's own sm_100a build and of this project's
+    command line on the same design, and the reference evaluator's totals of both
+    guide files.  The reference does one rip-up pass (src/main.cpp:45-68)."""
+    exe = os.path.join(REF_DIR, "instantgr_ref")
+    if not os.path.exists(exe):
+        return dict(unavailable=f"{exe} missing")
+    res = {}
+    outs = {}
+    for name, cmd in (("reference", [exe, "-cap", cap, "-net", net, "-out"]),
+                      ("this_build", [ROUTE_BIN, "-cap", cap, "-net", net, "--rrr-iters", "1", "-out"])):
+        out = os.path.join(workdir, f"guides_{name}.out")
+        t0 = time.perf_counter()
+        p = subprocess.run(cmd + [out], capture_output=True, text=True, timeout=900)
+        dt = time.perf_counter() - t0
+        outs[name] = out
+        res[name] = dict(cli_wall_s=round(dt, 3), rc=p.returncode)
+    evs = {}
+    th = [threading.Thread(target=lambda k: evs.__setitem__(k, evaluator_total(cap, net, outs[k])), args=(k,))
+          for k in outs]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for k in outs:
+        res[k]["evaluator"] = evs.get(k)
+    if res["reference"]["rc"] == 0 and res["this_build"]["rc"] == 0:
+        res["cli_speedup"] = round(res["reference"]["cli_wall_s"] / res["this_build"]["cli_wall_s"], 3)
+        a, b = evs.get("this_build", {}).get("total"), evs.get("reference", {}).get("total")
+        if a and b:
+            res["score_delta_pct"] = round(100.0 * (a - b) / b, 5)
+    res["note"] = "both with one rip-up-and-reroute pass, as the reference's main.cpp; wall clock of the process"
+    return res
+
+
+def route_only(args):
+    import instantgr_b200 as ig
+    cap, net = design_files(args)
+    r = ig.Router(cap, net, rrr_iters=args.rrr_iters, profile=1, verbose=1,
+                  batched=0 if args.form == "plain" else 1)
+    m = None
+    if args.form == "learned":
+        m = ig.Seed.load()
+        r.set_seed(m, alpha=1.0, mode=1, kind=1, levels=4)
+    for _ in range(args.warmup + args.steps):
+        r.run()
+    print(json.dumps(dict(form=args.form, stats=r.stats(), kernels=r.kstats(), evaluator=r.evaluate()["total"])),
+          flush=True)
+    r.close()
+    if m is not None:
+        m.close()
+
+
+KERNEL_NAMES = {
+    "cost_refresh": "commit_refresh / cost_refresh (fused batch commit, wire/via cost, f64 Sklansky prefix sums)",
+    "coloring": "coloring_kernel (persistent cooperative batch colouring)",
+    "pattern_dp": "pattern_route_kernel (tree DP per net, phase 1)",
+    "dag_dp": "dag_edge_cost + dag_net_kernel (detour-DAG DP and backtrace per net, reroute passes)",
+    "ripup": "rip-up: overflow marking, congestion view, wire/via rip-up",
+}
 
 
 def main():
@@ -200,22 +289,20 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    cfg = CONFIGS[args.config]
-    workload = dict(workload=f"global routing, {cfg['name']}", config_index=args.config, scale=args.scale,
-                    rrr_iters=args.rrr_iters, seed=args.seed, l2="per-step state exceeds L2 (inputs larger than L2)")
+    wl = workload(args)
     if args.route_only:
         return route_only(args)
     if args.impl == "reference":
-        return bench_reference(args, rank, world, workload)
+        return bench_reference(args, rank, world, wl)
 
     import torch
-    import numpy as np
     import instantgr_b200 as ig
     dist = None
     if world > 1:
+        import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local)
     ig.set_device(local)
     cap, net = design_files(args) if rank == 0 or world == 1 else (None, None)
@@ -223,10 +310,14 @@ def main():
         dist.barrier()
         cap, net = design_files(args)
 
-    rb = ig.Router(cap, net, rrr_iters=args.rrr_iters, profile=1, batched=1)  # batched form (headline)
+    model = ig.Seed.load()
     rp = ig.Router(cap, net, rrr_iters=args.rrr_iters, profile=1, batched=0)  # plain drop-in form
-    design_nets, routing_nets = rb.sizes()
+    rb = ig.Router(cap, net, rrr_iters=args.rrr_iters, profile=1, batched=1)  # batched form
+    rl = ig.Router(cap, net, rrr_iters=args.rrr_iters, profile=1, batched=1)  # batched + learned seed
+    rl.set_seed(model, alpha=1.0, mode=1, kind=1, levels=4)
+    design_nets, routing_nets = rp.sizes()
     for _ in range(max(args.warmup, 0)):
+        rl.run()
         rb.run()
         rp.run()
 
@@ -256,19 +347,20 @@ def main():
 
     clk = Clocks(local)
     clk.start()
+    ms_l, launches_l, ks_l = timed(rl, rl.run)
     ms_b, launches_b, ks_b = timed(rb, rb.run)
     ms_p, launches_p, ks_p = timed(rp, rp.run)
     clocks = clk.stop()
-    sb, sp = rb.stats(), rp.stats()
-    same = all(sb[k] == sp[k] for k in ("wirelength", "via_cost", "overflow_cost"))
+    ev_l, ev_b, ev_p = rl.evaluate(), rb.evaluate(), rp.evaluate()
+    sl, sb, sp = rl.stats(), rb.stats(), rp.stats()
 
     # e2e: the whole `-cap/-net/-out` flow through the public API with host files
-    # (read, upload, route, download, write guides), batched form
+    # (read, pins, trees, upload, route, download, write guides), plain form
     out = os.path.join(args.workdir, f"guides_r{rank}.out")
     e2e_bytes = []
 
     def e2e_step():
-        r = ig.Router(cap, net, rrr_iters=args.rrr_iters, batched=1)
+        r = ig.Router(cap, net, rrr_iters=args.rrr_iters, batched=0)
         r.run()
         r.write(out)
         st = r.stats()
@@ -279,18 +371,13 @@ def main():
 
     result = None
     if rank == 0:
-        value = replica_throughput(design_nets, args.steps, world, ms_b)
-        value_plain = replica_throughput(design_nets, args.steps, world, ms_p)
-        e2e_value = replica_throughput(design_nets, args.steps, world, ms_e2e)
-        plan = rp.plan()
+        value = replica_throughput(design_nets, args.steps, world, ms_p)
         h2d, d2h = e2e_bytes[-1]
-        # roofline of the dominant kernel class of the plain form (every class is
-        # timed per launch there) and, beside it, of every class with byte counts
         pk = measured_peaks()
         tr = profile_traffic()
 
-        def roof_of(k):
-            v = ks_p[k]
+        def roof_of(ks, k):
+            v = ks[k]
             ach = v["bytes"] / (v["ms"] / 1e3) / 1e9 if v["ms"] else 0.0
             n = max(v["launches"], 1)
             return dict(kernel=KERNEL_NAMES.get(k, k), bound="hbm", achieved=round(ach, 1), peak=pk["hbm_gbs"],
@@ -299,85 +386,115 @@ def main():
                         algorithmic_bytes_per_launch=round(v["bytes"] / n, 1),
                         avg_launch_us=round(1e3 * v["ms"] / n, 3))
 
-        dom = max((k for k in ks_p if ks_p[k]["bytes"] > 0), key=lambda k: ks_p[k]["ms"])
-        roof = roof_of(dom)
-        roof["dominant_kernel"] = dom
-        roof["classes"] = {k: roof_of(k) for k in ks_p if ks_p[k]["bytes"] > 0}
+        # every class is timed per launch in the plain form; the roofline object is
+        # the HBM-bound class with the largest share (the cost refresh), every
+        # class with its time and bound beside it
+        roof = roof_of(ks_p, "cost_refresh")
+        roof["dominant_kernel"] = "cost_refresh"
+        roof["classes"] = {k: roof_of(ks_p, k) for k in ks_p if ks_p[k]["bytes"] > 0}
         roof["kernel_ms_per_step_plain"] = {k: round(v["ms"] / args.steps, 3) for k, v in ks_p.items()}
-        roof["kernel_ms_per_step_batched"] = {k: round(v["ms"] / args.steps, 3) for k, v in ks_b.items()}
+        roof["kernel_ms_per_step_batched_learned"] = {k: round(v["ms"] / args.steps, 3) for k, v in ks_l.items()}
+        roof["latency_bound_classes"] = {
+            "coloring": "grid barriers and dependent L2 accesses; DRAM nearly idle (profiles/coloring_kernel_c1.md)",
+            "pattern_dp": "issue/latency bound tree DP (profiles/pattern_route_kernel_c1_largest_batch.md)",
+            "dag_dp": "bound by the dependent levels of the largest DAGs (profiles/dag_net_kernel_c2.md)",
+        }
         cpu = None
+        rgpu = None
         if world == 1:
             try:
-                g = rp.grid()
-                v, info = cpu_sample(rp, g, plan, args.cpu_batches)
-                cpu = dict(value=round(v, 2), unit="nets/s", cores=omp_threads(), kind="port",
-                           sample=f"oracle phase-1 (cost refresh + tree DP + commit) on the first "
-                                  f"{info['batches']} of {info['of_batches']} batches ({info['nets']} nets, "
-                                  f"{info['seconds']:.1f} s)")
+                win = ref_window(args)
+                wc, wn = design_files(args, win)
+                r = run_ref_cpu(wc, wn, 1, 0, args.rrr_iters, host_threads())
+                s0 = r["steps"][0]
+                cpu = dict(value=round(r["setup"]["design_nets"] / s0["seconds"], 2), unit="nets/s",
+                           cores=r["setup"]["threads"], kind="reference",
+                           sample=cpu_sample_text(args, win, r))
             except Exception as ex:  # the CPU baseline is reported, never required
-                cpu = dict(value=None, unit="nets/s", cores=omp_threads(), kind="port", sample=f"failed: {ex}")
-        result = dict(metric="route throughput (nets/s), batched RRR router", value=round(value, 2), unit="nets/s",
-                      n_gpus=world, steps=args.steps, warmup=args.warmup, ms_per_step=round(ms_b / args.steps, 3),
+                cpu = dict(value=None, unit="nets/s", cores=host_threads(), kind="reference", sample=f"failed: {ex}")
+            if not args.no_reference_gpu:
+                try:
+                    rgpu = reference_gpu(cap, net, args.workdir, args.rrr_iters)
+                except Exception as ex:
+                    rgpu = dict(unavailable=f"failed: {ex}")
+
+        def form(ms, launches, ev, st):
+            return dict(value=round(replica_throughput(design_nets, args.steps, world, ms), 2),
+                        ms_per_step=round(ms / args.steps, 3), gpu_launches=launches,
+                        evaluator_total=round(ev["total"], 1), rerouted_last_pass=int(st["rerouted"]),
+                        phase1_ms=round(st["p1_ms"], 3), rrr_ms=round(st["rrr_ms"], 3))
+
+        plain = form(ms_p, launches_p, ev_p, sp)
+        result = dict(metric=METRIC, value=round(value, 2), unit="nets/s",
+                      n_gpus=world, steps=args.steps, warmup=args.warmup, ms_per_step=round(ms_p / args.steps, 3),
                       higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32/f64 costs, i32 demand",
-                      data="synthetic (seeded generator, ISPD2024 format)", config=workload,
+                      data="synthetic (seeded generator, ISPD2024 format)", config=wl,
                       parallelism="replicas" if world > 1 else "single GPU",
-                      e2e=dict(value=round(e2e_value, 2), unit="nets/s", h2d_bytes_per_step=int(h2d),
-                               d2h_bytes_per_step=int(d2h)),
-                      roofline=roof, cpu_baseline=cpu, clocks=clocks, gpu_launches=launches_b,
-                      plain=dict(value=round(value_plain, 2), ms_per_step=round(ms_p / args.steps, 3),
-                                 gpu_launches=launches_p, same_result_as_batched=same),
+                      e2e=dict(value=round(replica_throughput(design_nets, args.steps, world, ms_e2e), 2),
+                               unit="nets/s", h2d_bytes_per_step=int(h2d), d2h_bytes_per_step=int(d2h)),
+                      roofline=roof, cpu_baseline=cpu, clocks=clocks, gpu_launches=launches_p,
+                      forms=dict(
+                          batched_learned=form(ms_l, launches_l, ev_l, sl),
+                          batched=form(ms_b, launches_b, ev_b, sb),
+                          plain=plain),
+                      plain_over_batched_learned_time=round(ms_p / ms_l, 3),
+                      score_batched_learned_vs_plain_pct=round(100.0 * (ev_l["total"] - ev_p["total"])
+                                                               / ev_p["total"], 5),
+                      reference_gpu=rgpu,
                       detail=dict(design_nets=design_nets, routing_nets=routing_nets,
-                                  wirelength=sb["wirelength"], via_cost=sb["via_cost"],
-                                  overflow_cost=sb["overflow_cost"], batches1=sb["batches1"],
-                                  rerouted_last=sb["rerouted"], p1_ms=sb["p1_ms"], rrr_ms=sb["rrr_ms"],
-                                  dag_host_ms=sb["dag_host_ms"], route_s=sb["route_s"],
-                                  host_cores=os.cpu_count()))
+                                  batches1=sp["batches1"], rerouted_last=sp["rerouted"], host_cores=os.cpu_count(),
+                                  e2e_ms_per_step=round(ms_e2e / args.steps, 3)))
         print(json.dumps(result), flush=True)
+    rl.close()
     rb.close()
     rp.close()
+    model.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return result
 
 
-KERNEL_NAMES = {
-    "cost_refresh": "commit_refresh / cost_refresh (fused batch commit, wire/via cost, f64 Sklansky prefix sums)",
-    "coloring": "coloring_kernel (persistent cooperative batch colouring)",
-    "pattern_dp": "pattern_route_kernel (tree DP per net, phase 1)",
-}
+def cpu_sample_text(args, win, r) -> str:
+    st = r["setup"]
+    s = r["steps"]
+    secs = [x["seconds"] for x in s]
+    return (f"oracle/_ref/ref_cpu: the reference's host code (reader, pin selection, net split, Steiner trees, "
+            f"host colouring generate_batches_rsmt, detour-DAG builder on {st['threads']} threads) and the oracle's "
+            f"restatement of its kernels (OpenMP, {st['threads']} threads), one complete route with "
+            f"{args.rrr_iters} RRR passes of the {win[2]}x{win[3]} window at ({win[0]}, {win[1]}) of the same design: "
+            f"{st['design_nets']} design nets, {st['routing_nets']} routing nets; rerouted per pass "
+            f"{s[0]['rerouted']}; {len(s)} step(s) of {statistics.mean(secs):.2f} s")
 
 
-def bench_reference(args, rank, world, workload):
-    """CPU restatement of the hot path (oracle port) on the host cores, rank 0 only."""
+def bench_reference(args, rank, world, wl):
+    """The reference's CPU implementation of the path on the host cores (rank 0 only)."""
     if rank != 0:
         return None
-    import instantgr_b200 as ig
-    cap, net = design_files(args)
-    r = ig.Router(cap, net, rrr_iters=0)
-    r.run()  # plan (batches and trees) of the same design
-    g = r.grid()
-    plan = r.plan()
-    design_nets, _ = r.sizes()
-    vals, infos = [], []
-    nb = args.cpu_batches  # 0: every batch of phase 1, within the time budget
-    for i in range(args.warmup + args.steps):
-        v, info = cpu_sample(r, g, plan, nb)
-        if i >= args.warmup:
-            vals.append(v)
-            infos.append(info)
-    v = statistics.median(vals)
-    sample = (f"oracle phase-1 (cost refresh + tree DP + commit) on the first {infos[0]['batches']} of "
-              f"{infos[0]['of_batches']} batches ({infos[0]['nets']} nets) per step")
-    res = dict(impl="reference", metric="route throughput (nets/s), plain RRR router", value=round(v, 2),
-               unit="nets/s", n_gpus=world, steps=args.steps, warmup=args.warmup,
-               ms_per_step=round(1e3 * infos[0]["nets"] / v, 3), higher_is_better=True, scaling="weak",
-               vs_baseline=None, dtype="f32/f64 costs, i32 demand", data="synthetic (seeded generator)",
-               config=workload,
-               cpu_baseline=dict(value=round(v, 2), unit="nets/s", cores=omp_threads(), kind="port", sample=sample),
-               e2e=dict(value=round(v, 2), unit="nets/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    win = ref_window(args)
+    cap, net = design_files(args, win)
+    try:
+        r = run_ref_cpu(cap, net, args.steps, max(args.warmup, 0), args.rrr_iters, host_threads())
+    except Exception as ex:
+        res = dict(impl="reference", unavailable=f"reference CPU route failed: {ex}")
+        print(json.dumps(res), flush=True)
+        return res
+    secs = [s["seconds"] for s in r["steps"]]
+    ms = 1e3 * sum(secs) / len(secs)
+    nets = r["setup"]["design_nets"]
+    v = nets / (ms / 1e3)
+    cpu = dict(value=round(v, 2), unit="nets/s", cores=r["setup"]["threads"], kind="reference",
+               sample=cpu_sample_text(args, win, r))
+    res = dict(impl="reference", metric=METRIC, value=round(v, 2), unit="nets/s", n_gpus=world, steps=args.steps,
+               warmup=args.warmup, ms_per_step=round(ms, 3), higher_is_better=True, scaling="weak",
+               vs_baseline=None, dtype="f32/f64 costs, i32 demand", data="synthetic (seeded generator, ISPD2024 format)",
+               config=wl, cpu_baseline=cpu,
+               e2e=dict(value=round(v, 2), unit="nets/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+               detail=dict(window=win, design_nets=nets, routing_nets=r["setup"]["routing_nets"],
+                           read_s=r["setup"]["read_s"], nets_trees_s=r["setup"]["nets_trees_s"],
+                           batches1=r["steps"][0]["batches1"], rerouted=r["steps"][0]["rerouted"],
+                           step_seconds=[round(x, 3) for x in secs]))
     print(json.dumps(res), flush=True)
-    r.close()
     return res
 
 

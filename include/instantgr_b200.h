@@ -118,7 +118,8 @@ int igr_router_sizes(igr_router *r, int64_t *design_nets, int64_t *routing_nets)
 /* Route record of routing net `net` (phase 1 or its latest reroute). */
 int igr_router_route(igr_router *r, int net, int32_t *out, int cap, int *len);
 /* Selected pins of design net `net` (net::init, src/database.hpp:38-243):
- * record npins, pins (file-layer positions, ascending), nextra, extra pairs.
+ * record npins, pins (file-layer positions, in the order net::init leaves
+ * them: the iteration order of its robin_hood sets), nextra, extra pairs.
  * Available right after igr_router_open (no GPU needed). */
 int igr_router_pins(igr_router *r, int net, int32_t *out, int cap, int *len);
 /* Device demand of the grid ([l][x][y], routing layers). */
@@ -151,6 +152,39 @@ typedef struct igr_grid_desc {
 int igr_create(const igr_grid_desc *g, igr_ctx **out);
 int igr_destroy(igr_ctx *c);
 const char *igr_last_error(const igr_ctx *c);
+
+/* Test hooks (no counterpart in InstantGR, whose failures end the process):
+ * process-wide settings that let tests reach paths the default sizes do not,
+ * and make the device's bounded waits run out without faulting anything.
+ * Every setting applies to launches made after the call, from any context.
+ *   IGR_HOOK_RESET            every hook back to its default (value ignored)
+ *   IGR_HOOK_WAIT_NS          limit of every grid-barrier and tensor-core
+ *                             mbarrier wait in ns (default 2e9); a wait that
+ *                             runs out sets IGR_ERR_TIMEOUT, the kernel drains
+ *                             its own work in flight and returns
+ *   IGR_HOOK_BARRIER_PHANTOM  arrivals the colouring's grid barriers wait for
+ *                             that never come (default 0): its first barrier
+ *                             then runs out by construction
+ *   IGR_HOOK_MBAR_PROBE       1: every seed-network GEMM first waits on an
+ *                             mbarrier phase that nothing completes, before it
+ *                             issues any MMA (default 0)
+ *   IGR_HOOK_COLOR_KEEP_MAP   igr_color_batches keeps the round-0 claim map up
+ *                             to date across batches (1, default) or clears
+ *                             and re-claims it every batch (0); the batches
+ *                             are the same
+ *   IGR_HOOK_DAG_SPLIT_NETS   DAG batches of at least this many nets (default
+ *                             4096) run their DAGs of at most 64 nodes in
+ *                             2-warp CTAs beside the larger ones on a second
+ *                             stream; the routes are the same */
+enum {
+    IGR_HOOK_RESET = 0,
+    IGR_HOOK_WAIT_NS = 1,
+    IGR_HOOK_BARRIER_PHANTOM = 2,
+    IGR_HOOK_MBAR_PROBE = 3,
+    IGR_HOOK_COLOR_KEEP_MAP = 4,
+    IGR_HOOK_DAG_SPLIT_NETS = 5,
+};
+int igr_test_hook(int key, int64_t value);
 
 /* Demand in and out ([l][x][y]).  Setting demand marks every track dirty. */
 int igr_set_demand(igr_ctx *c, const float *demand);
@@ -192,7 +226,9 @@ int igr_pattern_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t 
  * igr_pattern_route's.
  *
  * The DP's scratch (layer tables of nets with more than 16 tree nodes, 504
- * bytes per such node, plus 12 bytes per net and a work counter) lives in one
+ * bytes per such node, plus 12 bytes per net and a work counter: room for
+ * about 133,000 such nodes in a small call and about 108,000 at
+ * IGR_STATIC_MAX_NETS nets) lives in one
  * fixed array of IGR_STATIC_SCRATCH_BYTES in the library's device image, held
  * by every GPU that loads the library until the process exits.  A call with
  * more than IGR_STATIC_MAX_NETS nets, or whose large nets need more scratch

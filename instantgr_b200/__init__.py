@@ -48,6 +48,7 @@ EXPORTS = [
     "igr_seed_create", "igr_seed_destroy", "igr_seed_last_error", "igr_seed_set_tile", "igr_seed_params",
     "igr_seed_set_params", "igr_seed_features", "igr_seed_add_map", "igr_seed_add_routed", "igr_seed_train",
     "igr_seed_eval", "igr_seed_predict", "igr_seed_grad", "igr_router_set_seed", "igr_router_seed_stats",
+    "igr_test_hook",
 ]
 
 
@@ -145,6 +146,7 @@ def lib() -> C.CDLL:
     L.igr_seed_eval.argtypes = [vp, C.c_int, _f64p, C.c_int]
     L.igr_seed_predict.argtypes = [vp, C.c_int, C.c_int, _f32p, _f32p]
     L.igr_seed_grad.argtypes = [vp, C.c_int, _f32p, _f32p, C.POINTER(C.c_double), vp]
+    L.igr_test_hook.argtypes = [C.c_int, C.c_int64]
     _lib = L
     return L
 
@@ -161,6 +163,14 @@ def _i32(a) -> np.ndarray:
 
 def _i64(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.int64)
+
+
+HOOK_RESET, HOOK_WAIT_NS, HOOK_BARRIER_PHANTOM, HOOK_MBAR_PROBE, HOOK_COLOR_KEEP_MAP, HOOK_DAG_SPLIT_NETS = range(6)
+
+
+def set_test_hook(key: int, value: int = 0) -> None:
+    """Process-wide test hook (igr_test_hook); HOOK_RESET restores every default."""
+    _check(lib().igr_test_hook(key, value))
 
 
 def set_device(device: int) -> None:

@@ -3,6 +3,7 @@
 Outputs (in-tree, so that they travel with the source tree):
   instantgr_b200/lib/libigr_b200.so   C ABI of include/instantgr_b200.h
   instantgr_b200/bin/igr_route         `-cap/-net/-out` command line
+  instantgr_b200/bin/igr_generate      synthetic design generator (stand-alone)
 CUDA sources are compiled for sm_100a only; objects are rebuilt when a source
 or any header under csrc/ is newer than the object.
 """
@@ -23,7 +24,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CUDA_INC = "/usr/local/cuda/include"
 
 CU_SOURCES = ["cost.cu", "commit.cu", "ripup.cu", "pattern.cu", "pattern_static.cu", "color.cu", "dag.cu", "plan.cu",
-              "seed_nn.cu", "shapes.cu", "eval.cu", "records.cu", "dagbuild.cu"]
+              "seed_nn.cu", "shapes.cu", "eval.cu", "records.cu", "dagbuild.cu", "launch.cu"]
 CPP_SOURCES = ["design_io.cpp", "pins.cpp", "netbuild.cpp", "gen.cpp", "dag_build.cpp", "dag_device.cpp", "router.cpp",
                "capi.cpp", "seed_model.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -80,6 +81,11 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
     if _stale(main_src, exe, max(hdr, os.path.getmtime(so))):
         _run(["g++", "-std=c++17", "-O2", main_src, "-o", exe, "-L" + LIB, "-ligr_b200",
               "-Wl,-rpath,$ORIGIN/../lib"], log)
+    # the design generator alone, without the router library
+    gen = os.path.join(BIN, "igr_generate")
+    gen_srcs = [os.path.join(CSRC, "gen_main.cpp"), os.path.join(CSRC, "gen.cpp")]
+    if not os.path.exists(gen) or os.path.getmtime(gen) < max(hdr, *(os.path.getmtime(s) for s in gen_srcs)):
+        _run(["g++"] + CXX_FLAGS + gen_srcs + ["-o", gen], log)
     if verbose:
         sys.stdout.write("\n".join(log))
     return so

@@ -9,6 +9,7 @@
 #include <numeric>
 #include <string>
 
+#include "hooks.hpp"
 #include "router.hpp"
 #include "seed_model.hpp"
 
@@ -53,6 +54,9 @@ struct igr_seed {
 struct igr_ctx {
     GridOwner go;
     cudaStream_t s = nullptr;
+    // side stream and its fork/join events for the split DAG DP (made on first use)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     std::string err;
     // staging buffers reused across calls
     DevBuf<int> a, b, c, d, e, f, h, i, routes;
@@ -218,7 +222,6 @@ int igr_router_pins(igr_router *h, int net, int32_t *out, int cap, int *len) {
         const auto &d = h->r.d;
         if (net < 0 || net >= d.num_nets()) throw Error(ERR_INVALID, "net id out of range");
         std::vector<int> p(d.sel.begin() + d.sel_off[net], d.sel.begin() + d.sel_off[net + 1]);
-        std::sort(p.begin(), p.end());
         std::vector<int> v{(int)p.size()};
         v.insert(v.end(), p.begin(), p.end());
         v.push_back((int)(d.extra_off[net + 1] - d.extra_off[net]) / 2);
@@ -261,26 +264,15 @@ int igr_generate_custom(int X, int Y, int nets, uint64_t seed, int cap_mode, dou
                         double hotspot_frac, const char *cap_path, const char *net_path) {
     if (!cap_path || !net_path) return fail(nullptr, IGR_ERR_INVALID, "null path");
     return guard(nullptr, [&] {
-        GenParams p;
-        p.X = X; p.Y = Y; p.nets = nets; p.seed = seed; p.cap_mode = cap_mode; p.block_frac = block_frac;
-        p.pin_mode = pin_mode; p.hifanout_frac = hifanout_frac; p.bbox_median = bbox_median;
-        p.bbox_sigma = bbox_sigma; p.hotspots = hotspots; p.hotspot_frac = hotspot_frac;
-        p.hotspot_sigma = 0.1 * std::max(X, Y);
-        generate_design(p, cap_path, net_path);
+        generate_design(custom_params(X, Y, nets, seed, cap_mode, block_frac, pin_mode, hifanout_frac, bbox_median,
+                                      bbox_sigma, hotspots, hotspot_frac),
+                        cap_path, net_path);
     });
 }
 
 int igr_generate(int cfg, uint64_t seed, double scale, const char *cap_path, const char *net_path) {
-    if (scale <= 0 || scale > 1) return fail(nullptr, IGR_ERR_INVALID, "scale must be in (0, 1]");
-    auto nn = [&](int n) { return std::max(2, (int)(n * scale)); };
-    switch (cfg) {
-        case 0: return igr_generate_custom(256, 256, nn(20000), seed, 0, 0.05, 0, 0, 8, 1.0, 0, 0, cap_path, net_path);
-        case 1: return igr_generate_custom(840, 1140, nn(130000), seed, 1, 0, 0, 0.01, 8, 1.0, 0, 0, cap_path, net_path);
-        case 2: return igr_generate_custom(1600, 1600, nn(800000), seed, 1, 0, 1, 0, 10, 1.2, 6, 0.35, cap_path, net_path);
-        case 3: return igr_generate_custom(512, 512, nn(40000), seed, 1, 0, 1, 0, 10, 1.2, 6, 0.35, cap_path, net_path);
-        case 4: return igr_generate_custom(3000, 3000, nn(10000000), seed, 1, 0, 1, 0, 10, 1.2, 4, 0.40, cap_path, net_path);
-        default: return fail(nullptr, IGR_ERR_INVALID, "unknown configuration");
-    }
+    if (!cap_path || !net_path) return fail(nullptr, IGR_ERR_INVALID, "null path");
+    return guard(nullptr, [&] { generate_design(config_params(cfg, seed, scale), cap_path, net_path); });
 }
 
 // ------------------------------------------------------------------ device operators
@@ -306,13 +298,39 @@ int igr_create(const igr_grid_desc *g, igr_ctx **out) {
 int igr_destroy(igr_ctx *c) {
     if (!c) return IGR_OK;
     cudaStreamSynchronize(c->s);
-    cudaStream_t s = c->s;
+    cudaStream_t s = c->s, aux = c->aux;
+    cudaEvent_t fork = c->fork, join = c->join;
     delete c;
+    if (aux) cudaStreamDestroy(aux);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
     if (s) cudaStreamDestroy(s);
     return IGR_OK;
 }
 
 const char *igr_last_error(const igr_ctx *c) { return c ? c->err.c_str() : g_last_error.c_str(); }
+
+int igr_test_hook(int key, int64_t value) {
+    TestHooks &h = test_hooks();
+    switch (key) {
+        case IGR_HOOK_RESET: h.reset(); return IGR_OK;
+        case IGR_HOOK_WAIT_NS:
+            if (value < 0) return fail(nullptr, IGR_ERR_INVALID, "negative wait limit");
+            h.wait_ns = (long long)value;
+            return IGR_OK;
+        case IGR_HOOK_BARRIER_PHANTOM:
+            if (value < 0 || value > 1024) return fail(nullptr, IGR_ERR_INVALID, "phantom arrivals in 0..1024");
+            h.barrier_phantom = (int)value;
+            return IGR_OK;
+        case IGR_HOOK_MBAR_PROBE: h.mbar_probe = value != 0; return IGR_OK;
+        case IGR_HOOK_COLOR_KEEP_MAP: h.color_keep_map = value != 0; return IGR_OK;
+        case IGR_HOOK_DAG_SPLIT_NETS:
+            if (value < 1) return fail(nullptr, IGR_ERR_INVALID, "split threshold must be at least 1");
+            h.dag_split_nets = (int)std::min<int64_t>(value, INT32_MAX);
+            return IGR_OK;
+        default: return fail(nullptr, IGR_ERR_INVALID, "unknown test hook");
+    }
+}
 
 #define CTX_GUARD(c, ...)                                                       \
     do {                                                                        \
@@ -615,7 +633,7 @@ int igr_color_batches(igr_ctx *c, int n, const int32_t *pt_off, const int32_t *p
         cd.active = act.p; cd.active2 = act.p + n; cd.cand = act.p + 2 * (size_t)n; cd.lost = act.p + 3 * (size_t)n;
         cd.hdr = hdr.p;
         DevBuf<int> rev_off, rev_cnt, rev, snap, dirty, part;
-        if (cl.size() < (size_t)INT32_MAX) {  // round-0 map kept up to date across batches
+        if (cl.size() < (size_t)INT32_MAX && test_hooks().color_keep_map.load()) {  // round-0 map kept up to date
             rev_off.alloc(XY); rev_cnt.alloc(XY); rev.alloc(std::max<size_t>(1, cl.size()));
             snap.alloc(XY); dirty.alloc(XY); part.alloc(1024);
             cd.rev_off = rev_off.p; cd.rev_cnt = rev_cnt.p; cd.rev = rev.p; cd.snap = snap.p; cd.dirty = dirty.p;
@@ -689,7 +707,12 @@ int igr_dag_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t *nod
         db.net_node_off = dno.p; db.net_ids = dids.p; db.costs = dcost.p; db.best_path = dbest.p; db.packed = dpk.p;
         db.cost_edges = dce.p; db.best_change = dbc.p; db.layer_out = dlout.p; db.stage = dstage.p;
         db.stage_cnt = dscnt.p; db.route_off = droff.p; db.route_cap = dcap.p; db.routes = c->routes.p;
-        launch_dag_route(g, db, stamp, c->s);
+        if (!c->aux) {
+            cuda_check(cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking), "stream");
+            cuda_check(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming), "event");
+            cuda_check(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming), "event");
+        }
+        launch_dag_route(g, db, stamp, c->s, c->aux, c->fork, c->join, test_hooks().dag_split_nets.load());
         cuda_check(cudaGetLastError(), "DAG launch");
         cuda_check(cudaMemcpyAsync(routes_out, c->routes.p, ext * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
         sync_check(c);

@@ -32,6 +32,7 @@
 // list), which is the max the re-claim would give, since every other cell's
 // owner is still without a batch and still the highest of a smaller set.
 #include "gridsync.cuh"
+#include "hooks.hpp"
 #include "host.hpp"
 
 namespace igr {
@@ -279,7 +280,7 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
         c.map[i] = -1;
         if (inc) c.rev_cnt[i] = 0;
     }
-    if (!grid_sync(bar, err, epoch)) return;
+    if (!grid_sync(bar, err, epoch, c.wait_ns, c.phantom)) return;
     if (inc) {
         // claimers of every cell (ranks), grouped by cell: counts, an exclusive
         // scan over the cells (a chunk per block), then the entries
@@ -287,7 +288,7 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
             const int4 h = c.hdr[k];
             for (int i = h.x; i < h.y; i++) atomicAdd(c.rev_cnt + __ldg(c.claim + i), 1);
         }
-        if (!grid_sync(bar, err, epoch)) return;
+        if (!grid_sync(bar, err, epoch, c.wait_ns, c.phantom)) return;
         const int chunk = (XY + gridDim.x - 1) / gridDim.x;
         const int lo = min(XY, blockIdx.x * chunk), hi = min(XY, lo + chunk);
         const int per = (hi - lo + kThreads - 1) / kThreads;
@@ -296,7 +297,7 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
         for (int i = a0; i < a1; i++) mine += c.rev_cnt[i];
         int run = block_exclusive(mine, &total);
         if (threadIdx.x == 0) c.part[blockIdx.x] = total;
-        if (!grid_sync(bar, err, epoch)) return;
+        if (!grid_sync(bar, err, epoch, c.wait_ns, c.phantom)) return;
         if (tid == 0) {
             int acc = 0;
             for (int b = 0; b < (int)gridDim.x; b++) {
@@ -305,14 +306,14 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
                 acc += t;
             }
         }
-        if (!grid_sync(bar, err, epoch)) return;
+        if (!grid_sync(bar, err, epoch, c.wait_ns, c.phantom)) return;
         run += c.part[blockIdx.x];
         for (int i = a0; i < a1; i++) {
             c.rev_off[i] = run;
             run += c.rev_cnt[i];
             c.rev_cnt[i] = 0;
         }
-        if (!grid_sync(bar, err, epoch)) return;
+        if (!grid_sync(bar, err, epoch, c.wait_ns, c.phantom)) return;
         for (int k = tid; k < c.n; k += nth) {
             const int4 h = c.hdr[k];
             for (int i = h.x; i < h.y; i++) {
@@ -320,7 +321,7 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
                 c.rev[c.rev_off[cell] + atomicAdd(c.rev_cnt + cell, 1)] = k;
             }
         }
-        if (!grid_sync(bar, err, epoch)) return;
+        if (!grid_sync(bar, err, epoch, c.wait_ns, c.phantom)) return;
     }
     int na = c.n;
     for (int cur = 0; cur < max_batches; cur++) {
@@ -342,7 +343,7 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
             }
             if (!kept) {
                 claim_phase(c, cand, nc, blockIdx.x, gridDim.x, ops);
-                if (!grid_sync(bar, err, epoch)) return;
+                if (!grid_sync(bar, err, epoch, c.wait_ns, c.phantom)) return;
                 if (tid == 0) {
                     flags[F_CAND] = 0;
                     if (round == 0) flags[F_LEFT + ((cur + 1) & 1)] = 0;
@@ -351,18 +352,18 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
             if (inc && round == 0 && cur == 0)  // the first round-0 map, before any release
                 for (int i = tid; i < XY; i += nth) c.snap[i] = __ldcg(c.map + i);
             commit_phase(c, st, cand, nc, cur, flags + F_LOST, blockIdx.x, gridDim.x, ops);
-            if (!grid_sync(bar, err, epoch)) return;
+            if (!grid_sync(bar, err, epoch, c.wait_ns, c.phantom)) return;
             const int nl = vflags[F_LOST];
             if (nl == nc) break;  // no net joined in this round
             block_phase(c, st, nl, flags + F_CAND, blockIdx.x, gridDim.x, ops);
-            if (!grid_sync(bar, err, epoch)) return;
+            if (!grid_sync(bar, err, epoch, c.wait_ns, c.phantom)) return;
             cand = c.cand;
             nc = vflags[F_CAND];
             if (nc == 0) break;
         }
         if (tail) {
             if (blockIdx.x == 0) block_rounds(c, st, round, nc, cur, flags + F_ROUNDS, ops);
-            if (!grid_sync(bar, err, epoch)) return;
+            if (!grid_sync(bar, err, epoch, c.wait_ns, c.phantom)) return;
         }
         // nets still without a batch stay active; the map is cleared for the
         // next batch, or, when the round-0 map is kept, the cells whose
@@ -390,7 +391,7 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
             if ((it + 1) % (kBuf / kThreads) == 0) flush(st, act2, flags + F_LEFT + (cur & 1));
         }
         flush(st, act2, flags + F_LEFT + (cur & 1));
-        if (!grid_sync(bar, err, epoch)) return;
+        if (!grid_sync(bar, err, epoch, c.wait_ns, c.phantom)) return;
         na = vflags[F_LEFT + (cur & 1)];
         int *t = act; act = act2; act2 = t;
         if (na == 0) {
@@ -427,7 +428,7 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
                     c.snap[cell] = best;
                 }
             }
-            if (!grid_sync(bar, err, epoch)) return;
+            if (!grid_sync(bar, err, epoch, c.wait_ns, c.phantom)) return;
             for (int i = tid; i < XY; i += nth) c.map[i] = c.snap[i];
             if (tid == 0) {  // counters of round 0 of the next batch
                 flags[F_DIRTY] = 0;
@@ -435,7 +436,7 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
                 flags[F_CAND] = 0;
                 flags[F_LEFT + ((cur + 2) & 1)] = 0;
             }
-            if (!grid_sync(bar, err, epoch)) return;
+            if (!grid_sync(bar, err, epoch, c.wait_ns, c.phantom)) return;
         }
     }
     if (tid == 0) flags[F_NB] = max_batches;
@@ -492,6 +493,8 @@ int run_coloring(ColorDev &c, int max_batch, cudaStream_t s) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coloring_kernel, kThreads, 0);
     int blocks = sms * (per < 1 ? per : 1);
     if (blocks < 1) blocks = 1;
+    c.wait_ns = (unsigned long long)test_hooks().wait_ns.load();
+    c.phantom = (unsigned)test_hooks().barrier_phantom.load();
     cudaMemsetAsync(c.flags, 0, 16 * sizeof(int), s);
     cudaMemsetAsync(c.batch, 0xff, sizeof(int) * (size_t)c.n, s);
     int max_batches = c.n + 1;

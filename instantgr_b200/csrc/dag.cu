@@ -29,7 +29,6 @@ constexpr int kDagWarps = 8;                 // warps of one net's CTA
 constexpr int kDagThreads = 32 * kDagWarps;
 constexpr int kSmallWarps = 2;               // warps of a small net's CTA
 constexpr int kSmallNodes = 64;              // a small net's DAG has at most this many nodes
-constexpr int kSplitNets = 4096;             // batches of at least this many nets split by size
 
 __device__ __forceinline__ int32_t f2o(float f) {
     int32_t i = __float_as_int(f);
@@ -493,14 +492,14 @@ void dag_levels(int n, const int *node_off, const int *depth, std::vector<int> &
 }
 
 int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStream_t s, cudaStream_t aux,
-                     cudaEvent_t fork, cudaEvent_t join) {
+                     cudaEvent_t fork, cudaEvent_t join, int split_nets) {
     if (b.n_nodes <= 0 || b.n_nets <= 0) return 0;
     int launches = 0;
     if (b.n_edges > 0) {
         dag_edge_cost_kernel<<<(int)((b.n_edges + kEdgeWarps - 1) / kEdgeWarps), 32 * kEdgeWarps, 0, s>>>(g, b);
         launches++;
     }
-    if (!aux || b.n_nets < kSplitNets) {
+    if (!aux || b.n_nets < split_nets) {
         dag_net_kernel<kDagWarps, 0><<<b.n_nets, kDagThreads, 0, s>>>(g, b, stamp);
         return launches + 1;
     }

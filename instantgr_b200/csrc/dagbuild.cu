@@ -826,7 +826,7 @@ void launch_dag_build_solo(const DagBuildArgs &a, int builders, cudaStream_t s) 
     size_t smem = 0;
     if (!a.work) {
         smem = (size_t)work_ints(a.caps) * sizeof(int);
-        cudaFuncSetAttribute(dag_build_solo_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kernel_setup((const void *)dag_build_solo_kernel, 32, smem);
     }
     dag_build_solo_kernel<<<blocks, 32, smem, s>>>(a);
 }

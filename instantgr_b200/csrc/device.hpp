@@ -42,6 +42,18 @@ struct TrackMap {
     std::vector<int> first;  // [L+1] first track id of each layer
 };
 
+// Launch set-up of one kernel that is a per-device setting: the dynamic
+// shared-memory limit (raised to the largest `smem` asked for so far), the SM
+// count and the resident blocks per SM for `threads` threads and `smem` bytes.
+// Done once per (kernel, device, smem) under a lock, so that contexts on
+// several devices and host threads each get their own; a failing CUDA call
+// throws igr::Error (ERR_CUDA).
+struct KernelShape {
+    int sms = 0;
+    int blocks_per_sm = 0;
+};
+KernelShape kernel_setup(const void *kernel, int threads, size_t smem);
+
 // ---- launchers (stream-ordered; errors are reported through cudaGetLastError)
 void launch_cost_refresh(const GridDev &g, bool only_dirty, cudaStream_t s);
 void launch_wire_commit(const GridDev &g, int stamp, bool only_dirty, cudaStream_t s);
@@ -126,8 +138,12 @@ void dag_levels(int n, const int *node_off, const int *depth, std::vector<int> &
 // edge costs, then one CTA per net; returns the number of kernel launches
 // aux, fork, join (optional): in batches of 4096 nets or more, the DAGs of
 // more than 64 nodes run on `aux` beside the smaller ones
+// Batches of `split_nets` nets or more (4096 by default) run the DAGs of at
+// most 64 nodes in 2-warp CTAs on `s` beside the larger ones on `aux`
+// (forked and joined through the two events); smaller batches, or no `aux`,
+// run one launch.
 int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStream_t s, cudaStream_t aux = nullptr,
-                     cudaEvent_t fork = nullptr, cudaEvent_t join = nullptr);
+                     cudaEvent_t fork = nullptr, cudaEvent_t join = nullptr, int split_nets = 4096);
 
 constexpr int kRouteLayers = 9;
 
@@ -295,6 +311,10 @@ struct ColorDev {
     // instead of re-claimed.  rev_off/rev_cnt [X*Y]: claimers of each cell in
     // rev[] (ranks; [total claims]); snap/dirty [X*Y]; part [1024]
     int *rev_off = nullptr, *rev_cnt = nullptr, *rev = nullptr, *snap = nullptr, *dirty = nullptr, *part = nullptr;
+    // bound of every grid-barrier wait, and arrivals it waits for that never
+    // come (test hook; run_coloring takes both from the process's test hooks)
+    unsigned long long wait_ns = 2000000000ull;
+    unsigned phantom = 0;
 };
 // Claim lists of shapes (pt_off/pts/h_off/hseg/v_off/vseg as in ColorDev).
 void build_claims(int nshapes, const int *pt_off, const int *pts, const int *h_off, const int *hseg,

@@ -9,6 +9,7 @@
 #include "host.hpp"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -101,23 +102,28 @@ void generate_design(const GenParams &p, const char *cap_path, const char *net_p
                     if (c[(size_t)x * Y + y] != 0) { c[(size_t)x * Y + y] = 0; zeroed += 1; }
         }
     }
+    // window written (the whole grid by default)
+    const bool win = p.win_w > 0 && p.win_h > 0;
+    const int wx0 = win ? p.win_x0 : 0, wy0 = win ? p.win_y0 : 0, WX = win ? p.win_w : X, WY = win ? p.win_h : Y;
+    if (wx0 < 0 || wy0 < 0 || WX < 2 || WY < 2 || wx0 + WX > X || wy0 + WY > Y)
+        throw Error(ERR_INVALID, "window must lie inside the grid and be at least 2x2");
     {
         Out o(cap_path);
-        o.i(L); o.c(' '); o.i(X); o.c(' '); o.i(Y); o.c('\n');
+        o.i(L); o.c(' '); o.i(WX); o.c(' '); o.i(WY); o.c('\n');
         o.s("1 2");
         for (int l = 0; l < L; l++) o.s(" 1");
         o.c('\n');
-        for (int x = 0; x < X - 1; x++) { if (x) o.c(' '); o.c('1'); }
+        for (int x = 0; x < WX - 1; x++) { if (x) o.c(' '); o.c('1'); }
         o.c('\n');
-        for (int y = 0; y < Y - 1; y++) { if (y) o.c(' '); o.c('1'); }
+        for (int y = 0; y < WY - 1; y++) { if (y) o.c(' '); o.c('1'); }
         o.c('\n');
         for (int l = 0; l < L; l++) {
             o.s("metal"); o.i(l + 1); o.c(' ');
             o.i(l == 0 ? 1 : ((l - 1) & 1));  // layer 1 horizontal, alternate; layer 0 opposite of layer 1
             o.s(" 0\n");
             const int *c = cap.data() + (size_t)l * X * Y;
-            for (int y = 0; y < Y; y++) {
-                for (int x = 0; x < X; x++) { if (x) o.c(' '); o.i(c[(size_t)x * Y + y]); }
+            for (int y = wy0; y < wy0 + WY; y++) {
+                for (int x = wx0; x < wx0 + WX; x++) { if (x > wx0) o.c(' '); o.i(c[(size_t)x * Y + y]); }
                 o.c('\n');
             }
         }
@@ -127,6 +133,8 @@ void generate_design(const GenParams &p, const char *cap_path, const char *net_p
     for (int h = 0; h < p.hotspots; h++) { hx.push_back(rng.uni() * X); hy.push_back(rng.uni() * Y); }
     Out o(net_path);
     std::vector<std::pair<int, int>> used;
+    std::vector<std::array<int, 3>> aps;  // access points (layer, x, y) of the net being drawn
+    std::vector<int> pin_end;             // end of each pin's access points in aps
     for (int n = 0; n < p.nets; n++) {
         int k = pin_count(p, rng);
         bool hf = k < 0;
@@ -167,8 +175,9 @@ void generate_design(const GenParams &p, const char *cap_path, const char *net_p
         }
         int x0 = std::max(0, std::min(X - w, (int)std::lround(cx - w / 2.0)));
         int y0 = std::max(0, std::min(Y - h, (int)std::lround(cy - h / 2.0)));
-        o.s("net"); o.i(n); o.s("\n(\n");
         used.clear();
+        aps.clear();
+        pin_end.clear();
         auto taken = [&](int x, int y) { return std::find(used.begin(), used.end(), std::make_pair(x, y)) != used.end(); };
         for (int q = 0; q < k; q++) {
             int px = -1, py = -1;
@@ -182,7 +191,6 @@ void generate_design(const GenParams &p, const char *cap_path, const char *net_p
                         if (!taken(x, y)) { px = x; py = y; break; }
             if (px < 0) break;  // the whole box is used: fewer pins
             int nap = rng.range(1, 3);
-            o.c('[');
             static const int dx[4] = {1, -1, 0, 0}, dy[4] = {0, 0, 1, -1};
             int ax = px, ay = py;
             for (int a = 0; a < nap; a++) {
@@ -196,14 +204,50 @@ void generate_design(const GenParams &p, const char *cap_path, const char *net_p
                         ax = nx; ay = ny; ok = true;
                     }
                     if (!ok) break;
-                    o.s(", ");
                 }
                 used.push_back({ax, ay});
-                o.c('('); o.i(rng.range(0, 1)); o.s(", "); o.i(ax); o.s(", "); o.i(ay); o.c(')');
+                aps.push_back({rng.range(0, 1), ax, ay});
+            }
+            pin_end.push_back((int)aps.size());
+        }
+        bool inside = true;
+        for (auto &a : aps)
+            inside = inside && a[1] >= wx0 && a[1] < wx0 + WX && a[2] >= wy0 && a[2] < wy0 + WY;
+        if (!inside) continue;
+        o.s("net"); o.i(n); o.s("\n(\n");
+        for (size_t q = 0, a = 0; q < pin_end.size(); q++) {
+            o.c('[');
+            for (size_t b = a; b < (size_t)pin_end[q]; b++) {
+                if (b > a) o.s(", ");
+                o.c('('); o.i(aps[b][0]); o.s(", "); o.i(aps[b][1] - wx0); o.s(", "); o.i(aps[b][2] - wy0); o.c(')');
             }
             o.s("]\n");
+            a = (size_t)pin_end[q];
         }
         o.s(")\n");
+    }
+}
+
+GenParams custom_params(int X, int Y, int nets, uint64_t seed, int cap_mode, double block_frac, int pin_mode,
+                        double hifanout_frac, double bbox_median, double bbox_sigma, int hotspots, double hotspot_frac) {
+    GenParams p;
+    p.X = X; p.Y = Y; p.nets = nets; p.seed = seed; p.cap_mode = cap_mode; p.block_frac = block_frac;
+    p.pin_mode = pin_mode; p.hifanout_frac = hifanout_frac; p.bbox_median = bbox_median;
+    p.bbox_sigma = bbox_sigma; p.hotspots = hotspots; p.hotspot_frac = hotspot_frac;
+    p.hotspot_sigma = 0.1 * std::max(X, Y);
+    return p;
+}
+
+GenParams config_params(int cfg, uint64_t seed, double scale) {
+    if (scale <= 0 || scale > 1) throw Error(ERR_INVALID, "scale must be in (0, 1]");
+    auto nn = [&](int n) { return std::max(2, (int)(n * scale)); };
+    switch (cfg) {
+        case 0: return custom_params(256, 256, nn(20000), seed, 0, 0.05, 0, 0, 8, 1.0, 0, 0);
+        case 1: return custom_params(840, 1140, nn(130000), seed, 1, 0, 0, 0.01, 8, 1.0, 0, 0);
+        case 2: return custom_params(1600, 1600, nn(800000), seed, 1, 0, 1, 0, 10, 1.2, 6, 0.35);
+        case 3: return custom_params(512, 512, nn(40000), seed, 1, 0, 1, 0, 10, 1.2, 6, 0.35);
+        case 4: return custom_params(3000, 3000, nn(10000000), seed, 1, 0, 1, 0, 10, 1.2, 4, 0.40);
+        default: throw Error(ERR_INVALID, "unknown configuration");
     }
 }
 

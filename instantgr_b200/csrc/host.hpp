@@ -217,8 +217,16 @@ struct GenParams {
     int hotspots = 0;          // Gaussian hotspots
     double hotspot_frac = 0;   // fraction of nets centred on a hotspot
     double hotspot_sigma = 0;  // GCells
+    // window written (0 x 0: the whole grid): the design is drawn in full, and
+    // only the capacities of the window and the nets whose access points all
+    // lie in it are written, shifted to the window's origin
+    int win_x0 = 0, win_y0 = 0, win_w = 0, win_h = 0;
 };
 void generate_design(const GenParams &p, const char *cap_path, const char *net_path);
+// parameters of the benchmark configurations 0..4 (nets scaled by `scale`)
+GenParams config_params(int cfg, uint64_t seed, double scale);
+GenParams custom_params(int X, int Y, int nets, uint64_t seed, int cap_mode, double block_frac, int pin_mode,
+                        double hifanout_frac, double bbox_median, double bbox_sigma, int hotspots, double hotspot_frac);
 
 int hw_threads();
 void parallel_for(int n, int threads, const std::function<void(int, int)> &fn);  // fn(begin, end)

@@ -19,6 +19,7 @@
 #include <numeric>
 #include <tuple>
 #include <unordered_map>
+#include <unordered_set>
 
 namespace igr {
 
@@ -147,12 +148,17 @@ void construct_rsmt(const Design &d, const NetSet &ns, RNet &n) {
     // pins are distinct in 2-D (checked below); the layer of each 2-D position
     std::vector<std::pair<int, int>> layer;
     layer.reserve(n.pins.size());
-    std::vector<int> pos;
-    pos.reserve(n.pins.size());
+    // the Steiner provider sees the 2-D positions in the iteration order of a
+    // std::unordered_set filled in pin order, as my_flute does
+    // (src/database_cuda.hpp:696-708, 746-756); FLUTE's and the provider's
+    // tie-breaking follow the input order
+    // (no reserve: the bucket count, and with it the order, grows as the reference's does)
+    std::unordered_set<int> pos_set;
     for (int p : n.pins) {
         layer.push_back({p % XY, p / XY});
-        pos.push_back(p % XY);
+        pos_set.insert(p % XY);
     }
+    std::vector<int> pos(pos_set.begin(), pos_set.end());
     std::sort(layer.begin(), layer.end());
     for (size_t i = 1; i < layer.size(); i++)
         if (layer[i].first == layer[i - 1].first)

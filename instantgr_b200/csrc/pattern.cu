@@ -404,17 +404,8 @@ template <int G, int T>
 void launch_g(const GridDev &g, const TreeBatchDev &b, int stamp, cudaStream_t s) {
     constexpr int kThreads = 128;
     const size_t smem = sizeof(GroupSmem<T>) * (kThreads / G);
-    static bool attr = false;
-    static int sms = 0, per = 0;
-    if (!attr) {
-        cudaFuncSetAttribute(pattern_route_kernel<G, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, pattern_route_kernel<G, T>, kThreads, smem);
-        attr = true;
-    }
-    if (per < 1) per = 1;
+    const KernelShape ks = kernel_setup((const void *)pattern_route_kernel<G, T>, kThreads, smem);
+    const int sms = ks.sms, per = ks.blocks_per_sm;
     const int groups_per_block = kThreads / G;
     int blocks = (b.n + groups_per_block - 1) / groups_per_block;
     if (blocks > sms * per) blocks = sms * per;

@@ -8,14 +8,19 @@
 //  * > 4 pins: greedy rounds pick the 2-D position shared by the most
 //    unvisited pins (running counts, then x/y coordinate repetition, then
 //    centre distance), then every remaining pin takes its access point with the
-//    most coordinate repetition (src/database.hpp:98-223).  The reference walks
-//    the candidate pins in the iteration order of a robin_hood hash set; here
-//    they are walked in ascending pin order, which only matters when two
-//    positions tie on all three keys.
+//    most coordinate repetition (src/database.hpp:98-223).  The running counts
+//    make the choice depend on the order in which the pins are walked: the
+//    reference walks them in the iteration order of a robin_hood hash set
+//    filled from a robin_hood hash map, and so do these rounds (RobinOrder,
+//    robin_order.hpp).
 //  * Pins that end up stacked on one 2-D position keep the highest one as the
 //    pin and emit a via (lowest, highest) as an extra route
 //    (src/database.hpp:225-242).
+//  * The pins come out in the iteration order of the reference's robin_hood
+//    sets of chosen positions (3-D, or 2-D when pins were stacked), the order in
+//    which its later steps (the Steiner provider's input, the net split) see them.
 #include "host.hpp"
+#include "robin_order.hpp"
 
 #include <algorithm>
 #include <unordered_map>
@@ -30,6 +35,10 @@ struct PinScratch {
     std::unordered_map<int, int> xcnt, ycnt;
     std::vector<char> visited;
     std::vector<int> p, p2;
+    std::vector<int> order;        // walk order of the pins in the greedy rounds
+    RobinOrder keys2d, walk, rp, rp2;
+    std::vector<int> first2d;            // 2-D keys in first-seen order; pins per key (CSR below)
+    std::vector<int> list_off, list_pin;
 };
 
 void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, std::vector<int> &extra) {
@@ -41,7 +50,17 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
     const int c2x = d.bminx[n] + d.bmaxx[n], c2y = d.bminy[n] + d.bmaxy[n];
     std::vector<int> &p = s.p, &p2 = s.p2;  // chosen 3-D positions, chosen 2-D positions
     p.clear(); p2.clear();
+    s.rp.reset(); s.rp2.reset();  // net::init's sets are declared anew for every net
     auto has2 = [&](int v) { return std::find(p2.begin(), p2.end(), v) != p2.end(); };
+    // the reference's robin_hood sets p and p2D (their insertion sequences)
+    auto add3 = [&](int v) {
+        if (std::find(p.begin(), p.end(), v) == p.end()) p.push_back(v);
+        s.rp.insert(v);
+    };
+    auto add2 = [&](int v) {
+        p2.push_back(v);
+        s.rp2.insert(v);
+    };
 
     if (num <= 4) {
         s.idx.assign(num, 0);
@@ -77,8 +96,8 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
         }
         for (int i = 0; i < num; i++) {
             int v = apv(i, s.best[i]);
-            if (std::find(p.begin(), p.end(), v) == p.end()) p.push_back(v);
-            if (!has2(v % XY)) p2.push_back(v % XY);
+            add3(v);
+            if (!has2(v % XY)) add2(v % XY);
         }
     } else {
         s.visited.assign(num, 0);
@@ -87,10 +106,46 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
             auto it = m.find(k);
             return it == m.end() ? 0 : it->second;
         };
+        // walk order (src/database.hpp:101-117): the 2-D keys of all access
+        // points enter a robin_hood map in first-seen order, each with the pins
+        // that have an access point there (ascending); the pins of every key, in
+        // the map's iteration order, fill a robin_hood set, whose iteration order
+        // every round then follows
+        s.keys2d.reset();
+        s.first2d.clear();
+        for (int i = 0; i < num; i++)
+            for (int j = 0; j < nap(i); j++) {
+                const int q = apv(i, j) % XY;
+                if (s.keys2d.insert(q)) s.first2d.push_back(q);
+            }
+        {
+            // pins per 2-D key, in push order (i ascending, then j)
+            std::vector<std::pair<int, int>> kp;  // (key rank in first2d, pin)
+            std::unordered_map<int, int> rank;
+            for (size_t r = 0; r < s.first2d.size(); r++) rank[s.first2d[r]] = (int)r;
+            for (int i = 0; i < num; i++)
+                for (int j = 0; j < nap(i); j++) kp.push_back({rank[apv(i, j) % XY], i});
+            std::stable_sort(kp.begin(), kp.end(),
+                             [](const std::pair<int, int> &a, const std::pair<int, int> &b) { return a.first < b.first; });
+            s.list_off.assign(s.first2d.size() + 1, 0);
+            s.list_pin.clear();
+            for (auto &e : kp) {
+                s.list_off[e.first + 1]++;
+                s.list_pin.push_back(e.second);
+            }
+            for (size_t r = 0; r < s.first2d.size(); r++) s.list_off[r + 1] += s.list_off[r];
+            s.walk.reset();
+            s.keys2d.for_each([&](int q) {
+                const int r = rank[q];
+                for (int t = s.list_off[r]; t < s.list_off[r + 1]; t++) s.walk.insert(s.list_pin[t]);
+            });
+            s.order.clear();
+            s.walk.for_each([&](int i) { s.order.push_back(i); });
+        }
         for (int round = 0; round < num; round++) {
             int max_pos = -1, cnt_repeat = 0, max_coord = -1, min_dist = 1000000000;
             s.cnt2d.clear();
-            for (int i = 0; i < num; i++) {
+            for (int i : s.order) {
                 if (s.visited[i]) continue;
                 for (int j = 0; j < nap(i); j++) {
                     int q = apv(i, j) % XY;
@@ -110,7 +165,7 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
             }
             if (cnt_repeat <= 1) break;
             if (!has2(max_pos)) {
-                p2.push_back(max_pos);
+                add2(max_pos);
                 s.xcnt[max_pos / Y % X]++;
                 s.ycnt[max_pos % Y]++;
             }
@@ -119,8 +174,7 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
                 s.visited[pin] = 1;
                 for (int j = 0; j < nap(pin); j++)
                     if (apv(pin, j) % XY == max_pos) {
-                        int v = apv(pin, j);
-                        if (std::find(p.begin(), p.end(), v) == p.end()) p.push_back(v);
+                        add3(apv(pin, j));
                         break;
                     }
             }
@@ -136,18 +190,17 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
                 else if (coord == max_overlap && dist < min_dist) { min_dist = dist; chosen = v; }
             }
             if (chosen < 0) throw Error(ERR_FORMAT, "pin without access points");
-            if (std::find(p.begin(), p.end(), chosen) == p.end()) p.push_back(chosen);
+            add3(chosen);
             if (!has2(chosen % XY)) {
-                p2.push_back(chosen % XY);
+                add2(chosen % XY);
                 s.xcnt[chosen / Y % X]++;
                 s.ycnt[chosen % Y]++;
             }
         }
     }
-    std::sort(p.begin(), p.end());
+    // output in the iteration order of the reference's sets (src/database.hpp:225-242)
     if (p2.size() < p.size()) {
-        std::sort(p2.begin(), p2.end());
-        for (int q : p2) {
+        s.rp2.for_each([&](int q) {
             int mn = -1, mx = -1;
             for (int v : p)
                 if (v % XY == q) {
@@ -156,9 +209,9 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
                 }
             pins.push_back(mx);
             if (mn != mx) { extra.push_back(mn); extra.push_back(mx); }
-        }
+        });
     } else {
-        pins.insert(pins.end(), p.begin(), p.end());
+        s.rp.for_each([&](int v) { pins.push_back(v); });
     }
 }
 

@@ -16,6 +16,7 @@
 // buffers have grown to the design's size.
 #include "router.hpp"
 #include "seed_model.hpp"
+#include "hooks.hpp"
 
 #include <dlfcn.h>
 #include <sys/stat.h>
@@ -1350,7 +1351,8 @@ bool Router::rrr_pass(int iter) {
         db.best_change = dg_bchange.p; db.layer_out = dg_lout.p; db.stage = dg_stage.p; db.stage_cnt = dg_scnt.p;
         db.route_off = d_route_off.p; db.route_cap = d_route_cap.p; db.routes = routes.p;
         kt.begin(KC_DAG);
-        const int nl = launch_dag_route(go.g, db, s2, s, s_cls[0], ev_fork, ev_join[0]);
+        const int nl = launch_dag_route(go.g, db, s2, s, s_cls[0], ev_fork, ev_join[0],
+                                        test_hooks().dag_split_nets.load());
         kt.end(KC_DAG);
         kt.begin(KC_WIRE_COMMIT);
         launch_wire_commit(go.g, s2, true, s);

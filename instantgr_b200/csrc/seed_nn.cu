@@ -20,6 +20,7 @@
 #include "kcommon.cuh"
 #include "seed.hpp"
 #include "umma.cuh"
+#include "hooks.hpp"
 
 #include <algorithm>
 
@@ -211,7 +212,8 @@ struct WgradOp {
 };
 
 template <int BN, class Op>
-__global__ void __launch_bounds__(128) umma_gemm_kernel(Op op, int kchunk, int *err) {
+__global__ void __launch_bounds__(128) umma_gemm_kernel(Op op, int kchunk, int *err, unsigned long long wait_ns,
+                                                         int probe) {
     constexpr int kCols = BN < 32 ? 32 : BN;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     __nv_bfloat16 *sA = reinterpret_cast<__nv_bfloat16 *>(smem_raw);   // [2][4][128 * 16]
@@ -235,10 +237,15 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(Op op, int kchunk, int *
     constexpr uint32_t idesc = umma::idesc_bf16(128, BN);
     int issued = 0;
     bool ok = true;
-    for (int kb = 0; kb < nk; kb++) {
+    if (probe) {  // test hook: a wait on a phase that nothing completes, before any MMA is issued
+        bool w = true;
+        if (tid == 0) w = umma::mbar_wait(&bar[0], 0, wait_ns);
+        ok = __syncthreads_and(w) != 0;
+    }
+    for (int kb = 0; kb < nk && ok; kb++) {
         const int s = kb & 1;
         bool w = true;
-        if (kb >= 2 && tid == 0) w = umma::mbar_wait(&bar[s], ((kb - 2) >> 1) & 1, kWaitNs);
+        if (kb >= 2 && tid == 0) w = umma::mbar_wait(&bar[s], ((kb - 2) >> 1) & 1, wait_ns);
         ok = __syncthreads_and(w) != 0;
         if (!ok) break;
         __nv_bfloat16 *a = sA + s * 4 * 128 * 16, *b = sB + s * 4 * BN * 16;
@@ -284,14 +291,12 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(Op op, int kchunk, int *
 template <int BN, class Op>
 void launch_gemm(const Op &op, int N, int kchunk, int *err, cudaStream_t s) {
     const size_t smem = 2 * stage_bytes<BN>();
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(umma_gemm_kernel<BN, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
+    kernel_setup((const void *)umma_gemm_kernel<BN, Op>, 128, smem);
     if (kchunk <= 0) kchunk = op.K;
     dim3 grid((op.M + 127) / 128, (N + BN - 1) / BN, (op.K + kchunk - 1) / kchunk);
-    umma_gemm_kernel<BN, Op><<<grid, 128, smem, s>>>(op, kchunk, err);
+    umma_gemm_kernel<BN, Op><<<grid, 128, smem, s>>>(op, kchunk, err,
+                                                      (unsigned long long)test_hooks().wait_ns.load(),
+                                                      test_hooks().mbar_probe.load());
 }
 
 template <class Op>

@@ -292,6 +292,10 @@ static inline void addf(float *p, float v) {
 #pragma omp atomic
     *p += v;
 }
+static inline void setst(int *p, int v) {
+#pragma omp atomic write
+    *p = v;
+}
 
 int64_t orc_commit_vias(const orc_grid *g, int n, const int64_t *off, const int *routes, float *dem, const int *st,
                         int stamp, int K) {
@@ -326,14 +330,20 @@ int64_t orc_ripup_wires(const orc_grid *g, int n, const int64_t *off, const int 
                         int stamp, int K) {
     const int X = g->X, Y = g->Y, XY = X * Y;
     int64_t wl = 0;
+    /* demand changes by whole units and every writer stores the same stamp:
+     * nets in any order give the same arrays */
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : wl)
     for (int k = 0; k < n; k++) {
         const int *r = routes + off[k];
         for (int i = 1; i < r[0]; i += 2) {
             if (r[i] / XY != r[i + 1] / XY) continue;
             int l = r[i] / XY, x0 = r[i] / Y % X, y0 = r[i] % Y, x1 = r[i + 1] / Y % X, y1 = r[i + 1] % Y;
-            for (int x = MIN(x0, x1); x < MAX(x0, x1); x++) { dem[IDX(l, x, y0)] += (float)K; wl += g->xlen[x]; st[IDX(l, x, y0)] = stamp; }
-            for (int y = MIN(y0, y1); y < MAX(y0, y1); y++) { dem[IDX(l, x0, y)] += (float)K; wl += g->ylen[y]; st[IDX(l, x0, y)] = stamp; }
-            st[IDX(l, x0, y0)] = st[IDX(l, x0, y1)] = st[IDX(l, x1, y0)] = st[IDX(l, x1, y1)] = stamp;
+            for (int x = MIN(x0, x1); x < MAX(x0, x1); x++) { addf(&dem[IDX(l, x, y0)], (float)K); wl += g->xlen[x]; setst(&st[IDX(l, x, y0)], stamp); }
+            for (int y = MIN(y0, y1); y < MAX(y0, y1); y++) { addf(&dem[IDX(l, x0, y)], (float)K); wl += g->ylen[y]; setst(&st[IDX(l, x0, y)], stamp); }
+            setst(&st[IDX(l, x0, y0)], stamp);
+            setst(&st[IDX(l, x0, y1)], stamp);
+            setst(&st[IDX(l, x1, y0)], stamp);
+            setst(&st[IDX(l, x1, y1)], stamp);
         }
     }
     return wl * K;
@@ -345,6 +355,7 @@ void orc_mark_overflow(const orc_grid *g, const float *dem, int n, const int64_t
     int *of = (int *)calloc((size_t)L * XY, sizeof(int));
     for (int l = 0; l < L; l++) {
         if (dir_of(g, l) == 0) {
+#pragma omp parallel for schedule(static)
             for (int y = 0; y < Y; y++) {
                 int acc = 0;
                 for (int x = 0; x < X; x++) {
@@ -353,6 +364,7 @@ void orc_mark_overflow(const orc_grid *g, const float *dem, int n, const int64_t
                 }
             }
         } else {
+#pragma omp parallel for schedule(static)
             for (int x = 0; x < X; x++) {
                 int acc = 0;
                 for (int y = 0; y < Y; y++) {
@@ -362,6 +374,7 @@ void orc_mark_overflow(const orc_grid *g, const float *dem, int n, const int64_t
             }
         }
     }
+#pragma omp parallel for schedule(dynamic, 256)
     for (int k = 0; k < n; k++) {
         const int *r = routes + off[k];
         int c = 0;
@@ -378,6 +391,7 @@ void orc_mark_overflow(const orc_grid *g, const float *dem, int n, const int64_t
 
 void orc_congestion_view(const orc_grid *g, const float *dem, float *xsum, float *ysum) {
     const int L = g->L, X = g->X, Y = g->Y;
+#pragma omp parallel for schedule(static)
     for (int x = 0; x < X; x++)
         for (int y = 0; y < Y; y++) {
             float m = 0;
@@ -388,6 +402,7 @@ void orc_congestion_view(const orc_grid *g, const float *dem, float *xsum, float
             xsum[x * Y + y] = m;
             ysum[x * Y + y] = m;
         }
+#pragma omp parallel for schedule(static)
     for (int y = 0; y < Y; y++) {
         float acc = 0;
         for (int x = 0; x < X; x++) {
@@ -396,6 +411,7 @@ void orc_congestion_view(const orc_grid *g, const float *dem, float *xsum, float
             if (x < X - 1) acc += v;
         }
     }
+#pragma omp parallel for schedule(static)
     for (int x = 0; x < X; x++) {
         float acc = 0;
         for (int y = 0; y < Y; y++) {
@@ -498,199 +514,227 @@ int orc_dag_route(const orc_grid *g, const float *vcost, const double *presum, i
     int *coff = (int *)malloc(sizeof(int) * (size_t)(N + 1));
     coff[0] = 0;
     for (int v = 0; v < N; v++) coff[v + 1] = coff[v] + child_num[v];
-    double *costs = (double *)malloc(sizeof(double) * (size_t)N * ML);
+    double *costs = (double *)malloc(sizeof(double) * ((size_t)N * ML + 1));
     uint64_t *best = (uint64_t *)calloc((size_t)coff[N] * ML + 1, 8);
     uint64_t *pk = (uint64_t *)malloc(8 * ((size_t)coff[N] * ML + 1));
     double *ce = (double *)malloc(sizeof(double) * ((size_t)E * 81 + 1));
     int *bc = (int *)malloc(sizeof(int) * ((size_t)E * 81 + 1));
-    int *lo = (int *)malloc(sizeof(int) * (size_t)N);
-    int *stage = (int *)malloc(sizeof(int) * (size_t)N * 8);
-    int *scnt = (int *)calloc((size_t)N, sizeof(int));
-    int D = 0, status = 0;
-    for (int v = 0; v < N; v++) { if (depth[v] + 1 > D) D = depth[v] + 1; lo[v] = -1; }
-    for (int64_t i = 0; i < (int64_t)N * ML; i++) costs[i] = ORC_INF;
-    for (int64_t i = 0; i < (int64_t)coff[N] * ML; i++) pk[i] = 7208259049189261824ULL;
-    for (int64_t i = 0; i < (int64_t)E * 81; i++) { ce[i] = 0; bc[i] = -1; }
-    /* precompute_cost_edge (Lshape_route_detour.hpp:123-195) */
-    for (int v = 0; v < N; v++)
-        for (int e = par_off[v]; e < par_off[v + 1]; e++)
-            for (int f = 0; f < 9; f++) {
-                int tn = par[e];
-                int tox = nodes[tn] / Y % X, toy = nodes[tn] % Y, fx = nodes[v] / Y % X, fy = nodes[v] % Y;
-                if ((dir_of(g, f) == 0 && fy != toy) || (dir_of(g, f) == 1 && fx != tox)) {
-                    for (int t = 0; t < 9; t++) ce[(int64_t)e * 81 + f * 9 + t] = ORC_INF;
-                    continue;
-                }
-                int dist = abs(tox - fx) + abs(toy - fy);
-                if (dist == 0) continue;
-                int dd = dist / MIN(dist, 20);
-                int vert = fx == tox;
-                int s0 = vert ? MIN(fy, toy) : MIN(fx, tox), s1 = vert ? MAX(fy, toy) : MAX(fx, tox);
-                for (int t = 0; t < 9; t++) {
-                    if (t % 2 != f % 2) continue;
-                    double bestc = ORC_INF;
-                    int pos = -1;
-                    for (int sp = s0 + dd; sp < s1; sp += dd) {
-                        int sx = vert ? fx : sp, sy = vert ? sp : fy;
-                        double via = 0;
-                        for (int ll = MIN(f, t); ll < MAX(f, t); ll++) via += vcost[IDX(ll, sx, sy)];
-                        double c = via;
-                        if (vert)
-                            c += (wseg(g, presum, f, fx, fx, MIN(fy, sy), MAX(fy, sy)) + wseg(g, presum, t, tox, tox, MIN(toy, sy), MAX(toy, sy)));
-                        else
-                            c += (wseg(g, presum, f, MIN(fx, sx), MAX(fx, sx), fy, fy) + wseg(g, presum, t, MIN(tox, sx), MAX(tox, sx), toy, toy));
-                        if (c < bestc) { bestc = c; pos = sp; }
+    int *lo = (int *)malloc(sizeof(int) * ((size_t)N + 1));
+    int *stage = (int *)malloc(sizeof(int) * ((size_t)N * 8 + 1));
+    int *scnt = (int *)calloc((size_t)N + 1, sizeof(int));
+    int status = 0;
+    /* The nets of a batch share no DAG node (each node's parents and children
+     * belong to its own net), so the nets are routed one per iteration on all
+     * cores.  Within a net the nodes are visited level by level, deepest level
+     * first, as the reference's per-level launches do; the offers to a parent
+     * are minima and the backtrace reads only earlier levels, so the order of
+     * the nodes inside a level does not change the result. */
+#pragma omp parallel for schedule(dynamic, 1) reduction(min : status)
+    for (int k = 0; k < n; k++) {
+        const int a = node_off[k], b = node_off[k + 1];
+        int sk = 0, D = 0;
+        for (int v = a; v < b; v++) {
+            if (depth[v] + 1 > D) D = depth[v] + 1;
+            lo[v] = -1;
+            for (int j = 0; j < ML; j++) costs[(int64_t)v * ML + j] = ORC_INF;
+        }
+        for (int64_t i = (int64_t)coff[a] * ML; i < (int64_t)coff[b] * ML; i++) pk[i] = 7208259049189261824ULL;
+        for (int64_t i = (int64_t)par_off[a] * 81; i < (int64_t)par_off[b] * 81; i++) { ce[i] = 0; bc[i] = -1; }
+        /* nodes of the net by level (ascending node index inside a level) */
+        int *lv_off = (int *)calloc((size_t)D + 1, sizeof(int));
+        int *lv = (int *)malloc(sizeof(int) * (size_t)(b - a + 1));
+        for (int v = a; v < b; v++) lv_off[depth[v] + 1]++;
+        for (int d = 0; d < D; d++) lv_off[d + 1] += lv_off[d];
+        {
+            int *fill = (int *)malloc(sizeof(int) * (size_t)(D + 1));
+            for (int d = 0; d <= D; d++) fill[d] = lv_off[d];
+            for (int v = a; v < b; v++) lv[fill[depth[v]]++] = v;
+            free(fill);
+        }
+        /* precompute_cost_edge (Lshape_route_detour.hpp:123-195) */
+        for (int v = a; v < b; v++)
+            for (int e = par_off[v]; e < par_off[v + 1]; e++)
+                for (int f = 0; f < 9; f++) {
+                    int tn = par[e];
+                    int tox = nodes[tn] / Y % X, toy = nodes[tn] % Y, fx = nodes[v] / Y % X, fy = nodes[v] % Y;
+                    if ((dir_of(g, f) == 0 && fy != toy) || (dir_of(g, f) == 1 && fx != tox)) {
+                        for (int t = 0; t < 9; t++) ce[(int64_t)e * 81 + f * 9 + t] = ORC_INF;
+                        continue;
                     }
-                    ce[(int64_t)e * 81 + f * 9 + t] = bestc;
-                    bc[(int64_t)e * 81 + f * 9 + t] = pos;
-                }
-            }
-    /* bottom-up (Lshape_route_detour.hpp:281-406) */
-    for (int d = D - 1; d >= 0; d--)
-        for (int v = 0; v < N; v++) {
-            if (depth[v] != d) continue;
-            int fl = 1 + nodes[v] / XY, x = nodes[v] / Y % X, y = nodes[v] % Y;
-            int fh = fl == 10 ? 0 : fl, cb = coff[v], cn = coff[v + 1] - cb;
-            double minc[10];
-            uint64_t bp[10] = {0};
-            for (int low = 1; low <= fl; low++) {
-                for (int c = 0; c < cn; c++) minc[c] = ORC_INF;
-                double via = 0;
-                for (int layer = low; layer < g->L + 1; layer++) {
-                    if (layer > low) via += vcost[IDX(layer - 2, x, y)];
-                    for (int c = 0; c < cn; c++) {
-                        uint64_t p = pk[(int64_t)(cb + c) * ML + layer];
-                        double cc = (double)o2f((int32_t)(p >> 32));
-                        int id = (int)(p & 0xFFFFFFFFu);
-                        if (cc < minc[c]) { minc[c] = cc; bp[c] = (uint64_t)id * ML + layer; }
+                    int dist = abs(tox - fx) + abs(toy - fy);
+                    if (dist == 0) continue;
+                    int dd = dist / MIN(dist, 20);
+                    int vert = fx == tox;
+                    int s0 = vert ? MIN(fy, toy) : MIN(fx, tox), s1 = vert ? MAX(fy, toy) : MAX(fx, tox);
+                    for (int t = 0; t < 9; t++) {
+                        if (t % 2 != f % 2) continue;
+                        double bestc = ORC_INF;
+                        int pos = -1;
+                        for (int sp = s0 + dd; sp < s1; sp += dd) {
+                            int sx = vert ? fx : sp, sy = vert ? sp : fy;
+                            double via = 0;
+                            for (int ll = MIN(f, t); ll < MAX(f, t); ll++) via += vcost[IDX(ll, sx, sy)];
+                            double c = via;
+                            if (vert)
+                                c += (wseg(g, presum, f, fx, fx, MIN(fy, sy), MAX(fy, sy)) + wseg(g, presum, t, tox, tox, MIN(toy, sy), MAX(toy, sy)));
+                            else
+                                c += (wseg(g, presum, f, MIN(fx, sx), MAX(fx, sx), fy, fy) + wseg(g, presum, t, MIN(tox, sx), MAX(tox, sx), toy, toy));
+                            if (c < bestc) { bestc = c; pos = sp; }
+                        }
+                        ce[(int64_t)e * 81 + f * 9 + t] = bestc;
+                        bc[(int64_t)e * 81 + f * 9 + t] = pos;
                     }
-                    if (layer >= fh) {
-                        double t = via;
-                        for (int c = 0; c < cn; c++) t += minc[c];
-                        if (t < ORC_INF && t < costs[(int64_t)v * ML + layer]) {
-                            costs[(int64_t)v * ML + layer] = t;
-                            for (int c = 0; c < cn; c++) best[(int64_t)(cb + c) * ML + layer] = bp[c];
+                }
+        /* bottom-up (Lshape_route_detour.hpp:281-406) */
+        for (int d = D - 1; d >= 0; d--)
+            for (int q = lv_off[d]; q < lv_off[d + 1]; q++) {
+                const int v = lv[q];
+                int fl = 1 + nodes[v] / XY, x = nodes[v] / Y % X, y = nodes[v] % Y;
+                int fh = fl == 10 ? 0 : fl, cb = coff[v], cn = coff[v + 1] - cb;
+                double minc[10];
+                uint64_t bp[10] = {0};
+                for (int low = 1; low <= fl; low++) {
+                    for (int c = 0; c < cn; c++) minc[c] = ORC_INF;
+                    double via = 0;
+                    for (int layer = low; layer < g->L + 1; layer++) {
+                        if (layer > low) via += vcost[IDX(layer - 2, x, y)];
+                        for (int c = 0; c < cn; c++) {
+                            uint64_t p = pk[(int64_t)(cb + c) * ML + layer];
+                            double cc = (double)o2f((int32_t)(p >> 32));
+                            int id = (int)(p & 0xFFFFFFFFu);
+                            if (cc < minc[c]) { minc[c] = cc; bp[c] = (uint64_t)id * ML + layer; }
+                        }
+                        if (layer >= fh) {
+                            double t = via;
+                            for (int c = 0; c < cn; c++) t += minc[c];
+                            if (t < ORC_INF && t < costs[(int64_t)v * ML + layer]) {
+                                costs[(int64_t)v * ML + layer] = t;
+                                for (int c = 0; c < cn; c++) best[(int64_t)(cb + c) * ML + layer] = bp[c];
+                            }
+                        }
+                    }
+                    for (int layer = g->L - 1; layer >= low; layer--)
+                        if (costs[(int64_t)v * ML + layer + 1] < costs[(int64_t)v * ML + layer]) {
+                            costs[(int64_t)v * ML + layer] = costs[(int64_t)v * ML + layer + 1];
+                            for (int c = 0; c < cn; c++) best[(int64_t)(cb + c) * ML + layer] = best[(int64_t)(cb + c) * ML + layer + 1];
+                        }
+                }
+                for (int e = par_off[v]; e < par_off[v + 1]; e++) {
+                    int p = par[e], sl = child_slot[e];
+                    uint64_t *pp = pk + (int64_t)(coff[p] + sl) * ML;
+                    int px = nodes[p] / Y % X, py = nodes[p] % Y;
+                    int minx = MIN(x, px), maxx = MAX(x, px), miny = MIN(y, py), maxy = MAX(y, py);
+                    for (int layer = 1; layer < ML; layer++) {
+                        int dl = (layer & 1) ^ g->DIR;
+                        if (dl == 1 && y != py) continue;
+                        if (dl == 0 && x != px) continue;
+                        double base = costs[(int64_t)v * ML + layer];
+                        for (int t = 1 + (1 - layer % 2); t < ML; t += 2) {
+                            double c2;
+                            int ch = 82;
+                            if (t == layer) c2 = base + wseg(g, presum, layer - 1, minx, maxx, miny, maxy);
+                            else if (abs(x - px) + abs(y - py) > 4) {
+                                int seq = (layer - 1) * 9 + (t - 1);
+                                double c = ce[(int64_t)e * 81 + seq];
+                                if (c < ORC_INF) { c2 = base + c; ch = seq; }
+                                else continue;
+                            } else continue;
+                            uint64_t nv = pack((float)c2, v * 100 + ch);
+                            if (nv < pp[t]) pp[t] = nv;
                         }
                     }
                 }
-                for (int layer = g->L - 1; layer >= low; layer--)
-                    if (costs[(int64_t)v * ML + layer + 1] < costs[(int64_t)v * ML + layer]) {
-                        costs[(int64_t)v * ML + layer] = costs[(int64_t)v * ML + layer + 1];
-                        for (int c = 0; c < cn; c++) best[(int64_t)(cb + c) * ML + layer] = best[(int64_t)(cb + c) * ML + layer + 1];
-                    }
             }
-            for (int e = par_off[v]; e < par_off[v + 1]; e++) {
-                int p = par[e], sl = child_slot[e];
-                uint64_t *pp = pk + (int64_t)(coff[p] + sl) * ML;
-                int px = nodes[p] / Y % X, py = nodes[p] % Y;
-                int minx = MIN(x, px), maxx = MAX(x, px), miny = MIN(y, py), maxy = MAX(y, py);
-                for (int layer = 1; layer < ML; layer++) {
-                    int dl = (layer & 1) ^ g->DIR;
-                    if (dl == 1 && y != py) continue;
-                    if (dl == 0 && x != px) continue;
-                    double base = costs[(int64_t)v * ML + layer];
-                    for (int t = 1 + (1 - layer % 2); t < ML; t += 2) {
-                        double c2;
-                        int ch = 82;
-                        if (t == layer) c2 = base + wseg(g, presum, layer - 1, minx, maxx, miny, maxy);
-                        else if (abs(x - px) + abs(y - py) > 4) {
-                            int seq = (layer - 1) * 9 + (t - 1);
-                            double c = ce[(int64_t)e * 81 + seq];
-                            if (c < ORC_INF) { c2 = base + c; ch = seq; }
-                            else continue;
-                        } else continue;
-                        uint64_t nv = pack((float)c2, v * 100 + ch);
-                        if (nv < pp[t]) pp[t] = nv;
-                    }
-                }
-            }
-        }
-    /* top-down (Lshape_route_detour.hpp:520-694) */
+        /* top-down (Lshape_route_detour.hpp:520-694) */
 #define STAGE(a, b)                                                    \
     do {                                                               \
-        if (scnt[v] + 2 > 8) { status = -1; } else {                   \
+        if (scnt[v] + 2 > 8) { sk = -1; } else {                       \
             stage[(int64_t)v * 8 + scnt[v]] = (a);                     \
             stage[(int64_t)v * 8 + scnt[v] + 1] = (b);                 \
             scnt[v] += 2; }                                            \
     } while (0)
-    for (int d = 0; d < D; d++)
-        for (int v = 0; v < N; v++) {
-            if (depth[v] != d) continue;
-            int l = nodes[v] / XY, cx = nodes[v] / Y % X, cy = nodes[v] % Y;
-            int pn = par_off[v + 1] - par_off[v];
-            if (pn == 0) {
-                int ml = 0;
-                double mc = costs[(int64_t)v * ML];
-                for (int layer = 1; layer < ML; layer++)
-                    if (costs[(int64_t)v * ML + layer] < mc) { mc = costs[(int64_t)v * ML + layer]; ml = layer; }
-                lo[v] = ml;
-            } else {
-                int pl = -1, pidx = -1, pseq = -1;
-                for (int pi = 0; pi < pn; pi++) {
-                    int e = par_off[v] + pi, pnode = par[e];
-                    if (lo[pnode] <= 0) continue;
-                    pidx = pnode; pseq = pi; pl = lo[pnode];
-                    uint64_t path = best[(int64_t)(coff[pidx] + child_slot[par_off[v] + pseq]) * ML + pl];
-                    uint64_t cid = path / ML / 100, ch = (path / ML) % 100;
-                    if (cid == (uint64_t)v) {
-                        lo[v] = ch == 82 ? (int)(path % ML) : (int)(ch / 9 + 1);
-                        int px = nodes[pidx] / Y % X, py = nodes[pidx] % Y, L1 = lo[v] - 1;
-                        if (px == cx && cy != py) {
-                            if (ch == 82) {
-                                add_seg(g, pre, st, L1, px, px, MIN(py, cy), MAX(py, cy), stamp);
-                                STAGE((int)IDX(L1, px, MIN(py, cy)), (int)IDX(L1, px, MAX(py, cy)));
-                            } else {
-                                int f = (int)(ch / 9), t = (int)(ch % 9), cp = bc[(int64_t)e * 81 + f * 9 + t];
-                                add_seg(g, pre, st, f, cx, cx, MIN(cy, cp), MAX(cy, cp), stamp);
-                                add_seg(g, pre, st, t, cx, cx, MIN(py, cp), MAX(py, cp), stamp);
-                                STAGE((int)IDX(f, cx, MIN(cy, cp)), (int)IDX(f, cx, MAX(cy, cp)));
-                                STAGE((int)IDX(MIN(f, t), cx, cp), (int)IDX(MAX(f, t), cx, cp));
-                                STAGE((int)IDX(t, cx, MIN(py, cp)), (int)IDX(t, cx, MAX(py, cp)));
+        for (int d = 0; d < D; d++)
+            for (int q = lv_off[d]; q < lv_off[d + 1]; q++) {
+                const int v = lv[q];
+                int l = nodes[v] / XY, cx = nodes[v] / Y % X, cy = nodes[v] % Y;
+                int pn = par_off[v + 1] - par_off[v];
+                if (pn == 0) {
+                    int ml = 0;
+                    double mc = costs[(int64_t)v * ML];
+                    for (int layer = 1; layer < ML; layer++)
+                        if (costs[(int64_t)v * ML + layer] < mc) { mc = costs[(int64_t)v * ML + layer]; ml = layer; }
+                    lo[v] = ml;
+                } else {
+                    int pl = -1, pidx = -1, pseq = -1;
+                    for (int pi = 0; pi < pn; pi++) {
+                        int e = par_off[v] + pi, pnode = par[e];
+                        if (lo[pnode] <= 0) continue;
+                        pidx = pnode; pseq = pi; pl = lo[pnode];
+                        uint64_t path = best[(int64_t)(coff[pidx] + child_slot[par_off[v] + pseq]) * ML + pl];
+                        uint64_t cid = path / ML / 100, ch = (path / ML) % 100;
+                        if (cid == (uint64_t)v) {
+                            lo[v] = ch == 82 ? (int)(path % ML) : (int)(ch / 9 + 1);
+                            int px = nodes[pidx] / Y % X, py = nodes[pidx] % Y, L1 = lo[v] - 1;
+                            if (px == cx && cy != py) {
+                                if (ch == 82) {
+                                    add_seg(g, pre, st, L1, px, px, MIN(py, cy), MAX(py, cy), stamp);
+                                    STAGE((int)IDX(L1, px, MIN(py, cy)), (int)IDX(L1, px, MAX(py, cy)));
+                                } else {
+                                    int f = (int)(ch / 9), t = (int)(ch % 9), cp = bc[(int64_t)e * 81 + f * 9 + t];
+                                    add_seg(g, pre, st, f, cx, cx, MIN(cy, cp), MAX(cy, cp), stamp);
+                                    add_seg(g, pre, st, t, cx, cx, MIN(py, cp), MAX(py, cp), stamp);
+                                    STAGE((int)IDX(f, cx, MIN(cy, cp)), (int)IDX(f, cx, MAX(cy, cp)));
+                                    STAGE((int)IDX(MIN(f, t), cx, cp), (int)IDX(MAX(f, t), cx, cp));
+                                    STAGE((int)IDX(t, cx, MIN(py, cp)), (int)IDX(t, cx, MAX(py, cp)));
+                                }
+                            } else if (py == cy && cx != px) {
+                                if (ch == 82) {
+                                    add_seg(g, pre, st, L1, MIN(px, cx), MAX(px, cx), py, py, stamp);
+                                    STAGE((int)IDX(L1, MIN(px, cx), py), (int)IDX(L1, MAX(px, cx), py));
+                                } else {
+                                    int f = (int)(ch / 9), t = (int)(ch % 9), cp = bc[(int64_t)e * 81 + f * 9 + t];
+                                    add_seg(g, pre, st, f, MIN(cx, cp), MAX(cx, cp), cy, cy, stamp);
+                                    add_seg(g, pre, st, t, MIN(px, cp), MAX(px, cp), cy, cy, stamp);
+                                    STAGE((int)IDX(f, MIN(cx, cp), cy), (int)IDX(f, MAX(cx, cp), cy));
+                                    STAGE((int)IDX(MIN(f, t), cp, cy), (int)IDX(MAX(f, t), cp, cy));
+                                    STAGE((int)IDX(t, MIN(px, cp), cy), (int)IDX(t, MAX(px, cp), cy));
+                                }
                             }
-                        } else if (py == cy && cx != px) {
-                            if (ch == 82) {
-                                add_seg(g, pre, st, L1, MIN(px, cx), MAX(px, cx), py, py, stamp);
-                                STAGE((int)IDX(L1, MIN(px, cx), py), (int)IDX(L1, MAX(px, cx), py));
-                            } else {
-                                int f = (int)(ch / 9), t = (int)(ch % 9), cp = bc[(int64_t)e * 81 + f * 9 + t];
-                                add_seg(g, pre, st, f, MIN(cx, cp), MAX(cx, cp), cy, cy, stamp);
-                                add_seg(g, pre, st, t, MIN(px, cp), MAX(px, cp), cy, cy, stamp);
-                                STAGE((int)IDX(f, MIN(cx, cp), cy), (int)IDX(f, MAX(cx, cp), cy));
-                                STAGE((int)IDX(MIN(f, t), cp, cy), (int)IDX(MAX(f, t), cp, cy));
-                                STAGE((int)IDX(t, MIN(px, cp), cy), (int)IDX(t, MAX(px, cp), cy));
-                            }
+                            break;
+                        } else {
+                            lo[v] = -1;
                         }
-                        break;
-                    } else {
-                        lo[v] = -1;
                     }
+                    if (pl == -1) { lo[v] = -1; continue; }
+                    uint64_t path = best[(int64_t)(coff[pidx] + child_slot[par_off[v] + pseq]) * ML + pl];
+                    if (path / ML / 100 != (uint64_t)v) { lo[v] = -1; continue; }
                 }
-                if (pl == -1) { lo[v] = -1; continue; }
-                uint64_t path = best[(int64_t)(coff[pidx] + child_slot[par_off[v] + pseq]) * ML + pl];
-                if (path / ML / 100 != (uint64_t)v) { lo[v] = -1; continue; }
+                int cn = coff[v + 1] - coff[v];
+                int mnl = l + 1, mxl = (l + 1) == ML ? 1 : l + 1;
+                mnl = MIN(mnl, lo[v]);
+                mxl = MAX(mxl, lo[v]);
+                for (int c = 0; c < cn; c++) {
+                    int lc = (int)(best[(int64_t)(coff[v] + c) * ML + lo[v]] % ML);
+                    mnl = MIN(lc, mnl);
+                    mxl = MAX(lc, mxl);
+                }
+                if (mnl < mxl) STAGE((int)IDX(mnl - 1, cx, cy), (int)IDX(mxl - 1, cx, cy));
             }
-            int cn = coff[v + 1] - coff[v];
-            int mnl = l + 1, mxl = (l + 1) == ML ? 1 : l + 1;
-            mnl = MIN(mnl, lo[v]);
-            mxl = MAX(mxl, lo[v]);
-            for (int c = 0; c < cn; c++) {
-                int lc = (int)(best[(int64_t)(coff[v] + c) * ML + lo[v]] % ML);
-                mnl = MIN(lc, mnl);
-                mxl = MAX(lc, mxl);
-            }
-            if (mnl < mxl) STAGE((int)IDX(mnl - 1, cx, cy), (int)IDX(mxl - 1, cx, cy));
-        }
 #undef STAGE
-    /* route records in node order */
-    for (int k = 0; k < n; k++) {
-        int *r = routes + route_off[k];
-        int c = 1;
-        for (int v = node_off[k]; v < node_off[k + 1]; v++)
-            for (int j = 0; j < scnt[v]; j++) {
-                if (c + 1 > route_cap[k]) { status = -1; break; }
-                r[c++] = stage[(int64_t)v * 8 + j];
-            }
-        r[0] = c;
+        /* route record in node order */
+        {
+            int *r = routes + route_off[k];
+            int c = 1, full = 0;
+            for (int v = a; v < b && !full; v++)
+                for (int j = 0; j < scnt[v]; j++) {
+                    if (c + 1 > route_cap[k]) { full = 1; sk = -1; break; }
+                    r[c++] = stage[(int64_t)v * 8 + j];
+                }
+            r[0] = c;
+        }
+        free(lv_off);
+        free(lv);
+        if (sk < status) status = sk;
     }
     free(coff); free(costs); free(best); free(pk); free(ce); free(bc); free(lo); free(stage); free(scnt);
     return status;

@@ -3,7 +3,8 @@
 // Runs InstantGR's own .cap/.net reader and pin access-point selection
 // (db::read and net::init, src/database.hpp:38-415, compiled unmodified from
 // the reference tree by oracle/Makefile) and prints, per net, the chosen pins
-// in ascending order, then '|', then the stacked-pin vias as pairs.  Runs on
+// in the order net::init leaves them (the iteration order of its robin_hood
+// sets), then '|', then the stacked-pin vias as pairs in their order.  Runs on
 // the CPU; its output pins the reader and pin selection of this project.
 #include "database.hpp"
 
@@ -19,14 +20,10 @@ int main(int argc, char **argv) {
     FILE *f = fopen(argv[3], "w");
     if (!f) return 2;
     for (auto &n : db::nets) {
-        std::vector<int> p(n.pins);
-        std::sort(p.begin(), p.end());
-        for (int v : p) fprintf(f, "%d ", v);
+        for (int v : n.pins) fprintf(f, "%d ", v);
         fprintf(f, "|");
-        std::vector<std::pair<int, int>> ex;
-        for (size_t i = 0; i + 1 < n.extra_routes.size(); i += 2) ex.push_back({n.extra_routes[i], n.extra_routes[i + 1]});
-        std::sort(ex.begin(), ex.end());
-        for (auto &e : ex) fprintf(f, "%d %d ", e.first, e.second);
+        for (size_t i = 0; i + 1 < n.extra_routes.size(); i += 2)
+            fprintf(f, "%d %d ", n.extra_routes[i], n.extra_routes[i + 1]);
         fprintf(f, "\n");
     }
     fclose(f);

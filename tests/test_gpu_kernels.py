@@ -154,13 +154,21 @@ def test_ripup_and_overflow_marking_match_oracle():
     np.testing.assert_allclose(of, o.overflow_cost(d2), rtol=RTOL)
 
 
+@pytest.mark.parametrize("keep_map", [1, 0])
 @pytest.mark.parametrize("seed,n", [(31, 300), (32, 1500), (33, 6000)])
-def test_coloring_matches_oracle(seed, n):
+def test_coloring_matches_oracle(seed, n, keep_map):
+    """Both forms of the colouring: the round-0 claim map kept up to date across
+    batches (the default of igr_color_batches), and cleared and re-claimed for
+    every batch (the router's form below 2M nets)."""
     X, Y = 64, 48
     args = cases.color_case(seed, X, Y, n)
     g = cases.grid_case(1, X=X, Y=Y)
     c = ctx_for(g)
-    b_gpu, nb_gpu = c.color_batches(*args, sparsity=3)
+    ig.set_test_hook(ig.HOOK_COLOR_KEEP_MAP, keep_map)
+    try:
+        b_gpu, nb_gpu = c.color_batches(*args, sparsity=3)
+    finally:
+        ig.set_test_hook(ig.HOOK_RESET)
     b_orc, nb_orc = orc_color(X, Y, *args, sparsity=3)
     assert nb_gpu == nb_orc
     assert np.array_equal(b_gpu, b_orc)
@@ -235,3 +243,20 @@ def test_dag_route_matches_oracle(seed, X, Y, dir0, n):
         assert m > 1, f"net {k} produced no route"
         assert np.array_equal(r_gpu[a:a + m], r_orc[a:a + m]), f"net {k}"
     assert np.array_equal(pre_gpu, pre)
+
+
+@pytest.mark.parametrize("split", [2, 4096])
+def test_dag_route_split_by_size_matches_oracle(split):
+    """A batch of DAGs of 3 to about 110 nodes through the DAG DP with the
+    size split on (the DAGs of at most 64 nodes in 2-warp CTAs beside the
+    larger ones on a second stream, which the router uses for batches of 4096
+    nets or more) and off, against the oracle."""
+    g = cases.grid_case(45, X=90, Y=80, dir0=0)
+    d = cases.dag_batch(g, 46, n=120, kmax=40)
+    sizes = np.diff(d["node_off"])
+    assert (sizes <= 64).sum() > 0 and (sizes > 64).sum() > 0
+    ig.set_test_hook(ig.HOOK_DAG_SPLIT_NETS, split)
+    try:
+        assert _dag_vs_oracle(g, d) == 120
+    finally:
+        ig.set_test_hook(ig.HOOK_RESET)
