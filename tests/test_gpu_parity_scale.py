@@ -258,3 +258,58 @@ def test_score_within_half_percent_of_reference_router_at_130k_nets(work):
                    stdout=subprocess.DEVNULL, timeout=900)
     mine, theirs = _for_stat(cap, net, mine_out), _for_stat(cap, net, ref_out)
     assert abs(mine - theirs) <= 0.005 * theirs, (mine, theirs)
+
+
+def _conflict_points(nodes, par, Y, XY):
+    """2-D conflict points of one tree (net::construct_rsmt, src/database_cuda.hpp:
+    746-820): its nodes, and per edge its end points or its two bend corners."""
+    pts = set(int(v) % XY for v in nodes)
+    for i in range(1, len(nodes)):
+        a, b = int(nodes[i]) % XY, int(nodes[int(par[i])]) % XY
+        xa, ya, xb, yb = a // Y, a % Y, b // Y, b % Y
+        if xa != xb and ya != yb:
+            pts.add(xa * Y + yb)
+            pts.add(xb * Y + ya)
+    return pts
+
+
+def _reference_phase1_batches(cap, net, runs):
+    """Phase-1 batch counts of the reference router (its colouring is
+    nondeterministic: database_cuda.hpp:437), from its log."""
+    counts = []
+    for _ in range(runs):
+        p = subprocess.run([os.path.join(REF, "instantgr_ref"), "-cap", cap, "-net", net, "-out", os.devnull],
+                           capture_output=True, text=True, timeout=900)
+        gen = [line.split() for line in p.stdout.splitlines() if line.strip().startswith("Generation")]
+        assert gen, p.stdout[-1500:]
+        counts.append(int(gen[0][2]))
+    return counts
+
+
+def test_phase1_colouring_properties_and_batch_count_at_130k_nets(work):
+    """The deterministic colouring on the 840x1140, 130k-net design: no two nets
+    of a batch share a conflict point, every net is in exactly one batch, and the
+    number of batches lies within the range of the reference's (racy) colouring
+    over three runs of the reference router, widened by 10%."""
+    cap, net = _design(work, 1)
+    r = ig.Router(cap, net, rrr_iters=0)
+    r.run()
+    plan = r.plan()
+    nb = int(r.stats()["batches1"])
+    _, R = r.sizes()
+    g = r.grid()
+    r.close()
+    Y, XY = g["Y"], g["X"] * g["Y"]
+    boff, noff = plan["batch_off"], plan["node_off"]
+    assert len(boff) - 1 == nb and int(boff[-1]) == R
+    assert sorted(plan["net_ids"].tolist()) == list(range(R))
+    for b in range(nb):
+        seen = set()
+        for k in range(int(boff[b]), int(boff[b + 1])):
+            a, e = int(noff[k]), int(noff[k + 1])
+            pts = _conflict_points(plan["nodes"][a:e], plan["par"][a:e], Y, XY)
+            assert not (pts & seen), f"batch {b}: nets share a conflict point"
+            seen |= pts
+    ref = _reference_phase1_batches(cap, net, 3)
+    lo, hi = min(ref), max(ref)
+    assert 0.9 * lo <= nb <= 1.1 * hi, (nb, ref)
