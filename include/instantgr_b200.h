@@ -175,7 +175,13 @@ const char *igr_last_error(const igr_ctx *c);
  *   IGR_HOOK_DAG_SPLIT_NETS   DAG batches of at least this many nets (default
  *                             4096) run their DAGs of at most 64 nodes in
  *                             2-warp CTAs beside the larger ones on a second
- *                             stream; the routes are the same */
+ *                             stream; the routes are the same
+ *   IGR_HOOK_COLOR_KEEP_MIN_NETS  the router keeps the round-0 claim map up
+ *                             to date in colourings of at least this many nets
+ *                             (default 2,000,000); the batches are the same
+ *   IGR_HOOK_SHAPE_DEDUPE     the router keeps each conflict point and each
+ *                             claimed cell of a net once (1, default) or
+ *                             every repetition (0); the batches are the same */
 enum {
     IGR_HOOK_RESET = 0,
     IGR_HOOK_WAIT_NS = 1,
@@ -183,6 +189,8 @@ enum {
     IGR_HOOK_MBAR_PROBE = 3,
     IGR_HOOK_COLOR_KEEP_MAP = 4,
     IGR_HOOK_DAG_SPLIT_NETS = 5,
+    IGR_HOOK_COLOR_KEEP_MIN_NETS = 6,
+    IGR_HOOK_SHAPE_DEDUPE = 7,
 };
 int igr_test_hook(int key, int64_t value);
 

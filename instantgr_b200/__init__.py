@@ -165,7 +165,8 @@ def _i64(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.int64)
 
 
-HOOK_RESET, HOOK_WAIT_NS, HOOK_BARRIER_PHANTOM, HOOK_MBAR_PROBE, HOOK_COLOR_KEEP_MAP, HOOK_DAG_SPLIT_NETS = range(6)
+(HOOK_RESET, HOOK_WAIT_NS, HOOK_BARRIER_PHANTOM, HOOK_MBAR_PROBE, HOOK_COLOR_KEEP_MAP, HOOK_DAG_SPLIT_NETS,
+ HOOK_COLOR_KEEP_MIN_NETS, HOOK_SHAPE_DEDUPE) = range(8)
 
 
 def set_test_hook(key: int, value: int = 0) -> None:

@@ -324,6 +324,11 @@ int igr_test_hook(int key, int64_t value) {
             return IGR_OK;
         case IGR_HOOK_MBAR_PROBE: h.mbar_probe = value != 0; return IGR_OK;
         case IGR_HOOK_COLOR_KEEP_MAP: h.color_keep_map = value != 0; return IGR_OK;
+        case IGR_HOOK_COLOR_KEEP_MIN_NETS:
+            if (value < 1) return fail(nullptr, IGR_ERR_INVALID, "threshold must be at least 1");
+            h.color_keep_min_nets = (int)std::min<int64_t>(value, INT32_MAX);
+            return IGR_OK;
+        case IGR_HOOK_SHAPE_DEDUPE: h.shape_dedupe = value != 0; return IGR_OK;
         case IGR_HOOK_DAG_SPLIT_NETS:
             if (value < 1) return fail(nullptr, IGR_ERR_INVALID, "split threshold must be at least 1");
             h.dag_split_nets = (int)std::min<int64_t>(value, INT32_MAX);

@@ -272,7 +272,9 @@ __global__ void __launch_bounds__(kThreads, 1) coloring_kernel(ColorDev c, int m
     int *act = c.active, *act2 = c.active2;
     for (int k = tid; k < c.n; k += nth) {
         const int sh = c.perm ? c.perm[k] : k;
-        c.hdr[k] = make_int4(c.claim_off[sh], c.claim_off[sh + 1], c.pt_off[sh], c.pt_off[sh + 1]);
+        const int c0 = c.claim_off[sh], p0 = c.pt_off[sh];
+        c.hdr[k] = make_int4(c0, c.claim_n ? c0 + c.claim_n[sh] : c.claim_off[sh + 1], p0,
+                             c.pt_n ? p0 + c.pt_n[sh] : c.pt_off[sh + 1]);
         act[k] = k;
     }
     const bool inc = c.rev != nullptr;

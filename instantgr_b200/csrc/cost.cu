@@ -17,12 +17,48 @@
 // lane shuffles, levels 5-7 go through shared memory between warps, and levels
 // >= 8 combine whole rows, whose running totals every thread tracks itself.
 #include "kcommon.cuh"
+#include "host.hpp"
+
+#include <algorithm>
+#include <cstdint>
 
 namespace igr {
 
 namespace {
 
 constexpr int kThreads = 256;
+
+// Cost model of cell i of a track staged in s_cap / s_dem: writes its via cost
+// and returns the scan input, the wire cost of edge i-1 (0 for i = 0).
+__device__ __forceinline__ double cell_costs(const GridDev &g, const TrackInfo &ti, const float *s_cap,
+                                             const float *s_dem, int i, double sc, const int *elen) {
+    const int n = ti.len;
+    const float c = s_cap[i], d = s_dem[i];
+    const double of0 = of_cost(c, d);
+    const double bh = fmin(1e12, (of_cost(c, (float)((double)d + 0.5)) - of0) * sc);
+    float v;
+    double x = 0;
+    if (i == 0) {
+        v = (float)fmin(1e12, (of_cost(c, (float)((double)d + 1.0)) - of0) * sc);
+    } else {
+        const float cp = s_cap[i - 1], dp = s_dem[i - 1];
+        const double ofp = of_cost(cp, dp);
+        const double a1p = fmin(1e12, (of_cost(cp, (float)((double)dp + 1.0)) - ofp) * sc);
+        if (i == n - 1) {
+            v = (float)a1p;
+        } else {
+            const double bhp = fmin(1e12, (of_cost(cp, (float)((double)dp + 0.5)) - ofp) * sc);
+            v = (float)(bh + bhp);
+        }
+        // scan input: wire cost of edge i-1 (graph.hpp:44-46)
+        float w = (float)a1p;
+        w = (float)fma(g.unit_wire, (double)elen[i - 1], (double)w);
+        x = (double)w;
+    }
+    v = (float)((double)v + g.unit_via);
+    g.vcost[ti.base + i] = v;
+    return x;
+}
 
 // Cost model and Sklansky prefix sums of one track whose capacity and demand
 // are staged in s_cap / s_dem; every thread of the block calls it.
@@ -43,31 +79,7 @@ __device__ __forceinline__ void refresh_track(const GridDev &g, const TrackInfo 
     for (int r = 0; r < MAXE; r++) {
         x[r] = 0;
         const int i = tid + r * kThreads;
-        if (r < E && i < n) {
-            const float c = s_cap[i], d = s_dem[i];
-            const double of0 = of_cost(c, d);
-            const double bh = fmin(1e12, (of_cost(c, (float)((double)d + 0.5)) - of0) * sc);
-            float v;
-            if (i == 0) {
-                v = (float)fmin(1e12, (of_cost(c, (float)((double)d + 1.0)) - of0) * sc);
-            } else {
-                const float cp = s_cap[i - 1], dp = s_dem[i - 1];
-                const double ofp = of_cost(cp, dp);
-                const double a1p = fmin(1e12, (of_cost(cp, (float)((double)dp + 1.0)) - ofp) * sc);
-                if (i == n - 1) {
-                    v = (float)a1p;
-                } else {
-                    const double bhp = fmin(1e12, (of_cost(cp, (float)((double)dp + 0.5)) - ofp) * sc);
-                    v = (float)(bh + bhp);
-                }
-                // scan input: wire cost of edge i-1 (graph.hpp:44-46)
-                float w = (float)a1p;
-                w = (float)fma(g.unit_wire, (double)elen[i - 1], (double)w);
-                x[r] = (double)w;
-            }
-            v = (float)((double)v + g.unit_via);
-            g.vcost[ti.base + i] = v;
-        }
+        if (r < E && i < n) x[r] = cell_costs(g, ti, s_cap, s_dem, i, sc, elen);
     }
     // ---- Sklansky levels 0..4: lanes
 #pragma unroll
@@ -125,21 +137,97 @@ __device__ __forceinline__ void refresh_track(const GridDev &g, const TrackInfo 
     }
 }
 
+// Copies n floats of a track's capacity (when `a` is non-null) and demand into
+// shared memory in one loop, so that the loads of both arrays are in flight
+// together: 16 bytes per load where the track starts on a 16-byte boundary
+// (every track of a grid whose X*Y and track lengths are multiples of 4), else
+// one float per load.
+__device__ __forceinline__ void stage_track(const float *a, const float *b, float *da, float *db, int n, int tid,
+                                            int nthreads) {
+    if ((reinterpret_cast<uintptr_t>(b) & 15) == 0) {
+        const int n4 = n >> 2;
+        const float4 *a4 = reinterpret_cast<const float4 *>(a), *b4 = reinterpret_cast<const float4 *>(b);
+        float4 *da4 = reinterpret_cast<float4 *>(da), *db4 = reinterpret_cast<float4 *>(db);
+        for (int i = tid; i < n4; i += nthreads) {
+            const float4 vb = b4[i];
+            if (a) da4[i] = a4[i];
+            db4[i] = vb;
+        }
+        for (int i = (n4 << 2) + tid; i < n; i += nthreads) {
+            if (a) da[i] = a[i];
+            db[i] = b[i];
+        }
+    } else {
+        for (int i = tid; i < n; i += nthreads) {
+            if (a) da[i] = a[i];
+            db[i] = b[i];
+        }
+    }
+}
+
 template <int MAXE>
-__global__ void __launch_bounds__(kThreads) cost_refresh_kernel(GridDev g, int only_dirty) {
+__global__ void __launch_bounds__(kThreads, 5) cost_refresh_kernel(GridDev g, int only_dirty) {
     const int tr = blockIdx.x;
     if (only_dirty) {
         if (!g.dirty_cost[tr]) return;
     }
     const TrackInfo ti = decode_track(g, tr);
-    __shared__ float s_cap[MAXE * kThreads], s_dem[MAXE * kThreads];
-    for (int i = threadIdx.x; i < ti.len; i += kThreads) {
-        s_cap[i] = g.cap[ti.base + i];
-        s_dem[i] = g.demand[ti.base + i];
-    }
+    __shared__ __align__(16) float s_cap[MAXE * kThreads];
+    __shared__ __align__(16) float s_dem[MAXE * kThreads];
+    stage_track(g.cap + ti.base, g.demand + ti.base, s_cap, s_dem, ti.len, threadIdx.x, kThreads);
     __syncthreads();
     if (threadIdx.x == 0 && only_dirty) g.dirty_cost[tr] = 0;
     refresh_track<MAXE>(g, ti, s_cap, s_dem);
+}
+
+// Tracks of more than 4096 cells (up to the reference's 15,360, main.cpp:28):
+// a CTA of kLongThreads per track, the costs evaluated into registers, then
+// the reference's in-place Sklansky scan level by level in shared memory
+// (graph.hpp:421-428; at level d an element reads an element whose bit d is
+// clear, which that level never writes).  The f64 scan array reuses the
+// shared memory of the staged capacity and demand.
+constexpr int kLongThreads = 1024;
+constexpr int kLongMaxE = kMaxTrackCells / kLongThreads;  // 15
+
+__global__ void __launch_bounds__(kLongThreads) cost_refresh_long_kernel(GridDev g, int only_dirty) {
+    extern __shared__ __align__(16) unsigned char long_smem[];
+    float *s_cap = reinterpret_cast<float *>(long_smem);
+    float *s_dem = s_cap + kMaxTrackCells;
+    double *s_x = reinterpret_cast<double *>(long_smem);  // after the costs: 8 bytes per cell
+    const int tid = threadIdx.x;
+    const int tr = blockIdx.x;
+    if (only_dirty && !g.dirty_cost[tr]) return;
+    {
+        const TrackInfo ti = decode_track(g, tr);
+        const int n = ti.len;
+        stage_track(g.cap + ti.base, g.demand + ti.base, s_cap, s_dem, n, tid, kLongThreads);
+        __syncthreads();
+        if (tid == 0) {
+            if (only_dirty) g.dirty_cost[tr] = 0;
+            atomicAdd(&g.stats[2], (unsigned long long)n);
+        }
+        const double sc = g.short_cost[ti.l];
+        const int *elen = ti.dir ? g.ylen : g.xlen;
+        double x[kLongMaxE];
+#pragma unroll
+        for (int r = 0; r < kLongMaxE; r++) {
+            const int i = tid + r * kLongThreads;
+            x[r] = i < n ? cell_costs(g, ti, s_cap, s_dem, i, sc, elen) : 0.0;
+        }
+        __syncthreads();  // every read of the staged capacity and demand is done
+#pragma unroll
+        for (int r = 0; r < kLongMaxE; r++) {
+            const int i = tid + r * kLongThreads;
+            if (i < n) s_x[i] = x[r];
+        }
+        __syncthreads();
+        for (int d = 0; (1 << d) < n; d++) {
+            for (int i = tid; i < n; i += kLongThreads)
+                if ((i >> d) & 1) s_x[i] += s_x[((i >> d) << d) - 1];
+            __syncthreads();
+        }
+        for (int i = tid; i < n; i += kLongThreads) g.presum[ti.base + i] = s_x[i];
+    }
 }
 
 __device__ __forceinline__ int warp_incl_scan(int v, int lane) {
@@ -161,21 +249,19 @@ __device__ __forceinline__ int warp_incl_scan(int v, int lane) {
 // pending commit and clean costs are skipped.  With refresh = 0 the costs are
 // only marked dirty.
 template <int MAXE>
-__global__ void __launch_bounds__(kThreads) commit_refresh_kernel(GridDev g, int *vcnt, int stamp, int refresh) {
+__global__ void __launch_bounds__(kThreads, 5) commit_refresh_kernel(GridDev g, int *vcnt, int stamp, int refresh) {
+    __shared__ __align__(16) float s_cap[MAXE * kThreads];
+    __shared__ __align__(16) float s_dem[MAXE * kThreads];
+    __shared__ int s_w[kThreads / 32];
+    __shared__ int s_carry;
+    __shared__ long long s_wl[kThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int tr = blockIdx.x;
     const bool commit = g.dirty_commit[tr] != 0;
     if (!commit && !(refresh && g.dirty_cost[tr])) return;
     const TrackInfo ti = decode_track(g, tr);
     const int n = ti.len;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    __shared__ float s_cap[MAXE * kThreads], s_dem[MAXE * kThreads];
-    __shared__ int s_w[kThreads / 32];
-    __shared__ int s_carry;
-    __shared__ long long s_wl[kThreads / 32];
-    for (int i = tid; i < n; i += kThreads) {
-        if (refresh) s_cap[i] = g.cap[ti.base + i];
-        s_dem[i] = g.demand[ti.base + i];
-    }
+    stage_track(refresh ? g.cap + ti.base : nullptr, g.demand + ti.base, s_cap, s_dem, n, tid, kThreads);
     if (commit) {
         const int *elen = ti.dir ? g.ylen : g.xlen;
         if (tid == 0) s_carry = 0;
@@ -260,26 +346,46 @@ __global__ void track_to_ref_kernel(GridDev g, const T *trk, T *ref) {
 
 }  // namespace
 
+// One CTA per track: the hardware block scheduler hands the dirty tracks to
+// the SMs as they free up (a resident grid striding over the tracks balanced
+// the uneven dirty tracks worse: 11.9 -> 15.8 ms per step on the 800k-net
+// design), and a CTA that finds its track clean exits at once.
+template <int E>
+static void cost_refresh_e(const GridDev &g, int od, cudaStream_t s) {
+    cost_refresh_kernel<E><<<g.ntracks, kThreads, 0, s>>>(g, od);
+}
+
 void launch_cost_refresh(const GridDev &g, bool only_dirty, cudaStream_t s) {
     const int maxlen = g.X > g.Y ? g.X : g.Y;
     const int e = (maxlen + kThreads - 1) / kThreads;
     const int od = only_dirty ? 1 : 0;
-    if (e <= 1) cost_refresh_kernel<1><<<g.ntracks, kThreads, 0, s>>>(g, od);
-    else if (e <= 2) cost_refresh_kernel<2><<<g.ntracks, kThreads, 0, s>>>(g, od);
-    else if (e <= 4) cost_refresh_kernel<4><<<g.ntracks, kThreads, 0, s>>>(g, od);
-    else if (e <= 8) cost_refresh_kernel<8><<<g.ntracks, kThreads, 0, s>>>(g, od);
-    else cost_refresh_kernel<16><<<g.ntracks, kThreads, 0, s>>>(g, od);  // tracks of <= 4096 cells
+    if (e <= 1) cost_refresh_e<1>(g, od, s);
+    else if (e <= 2) cost_refresh_e<2>(g, od, s);
+    else if (e <= 4) cost_refresh_e<4>(g, od, s);
+    else if (e <= 8) cost_refresh_e<8>(g, od, s);
+    else if (e <= 16) cost_refresh_e<16>(g, od, s);  // tracks of <= 4096 cells
+    else {
+        const size_t smem = (size_t)kMaxTrackCells * 8;
+        kernel_setup((const void *)cost_refresh_long_kernel, kLongThreads, smem);
+        cost_refresh_long_kernel<<<g.ntracks, kLongThreads, smem, s>>>(g, od);
+    }
+}
+
+template <int E>
+static void commit_refresh_e(const GridDev &g, int *vcnt, int stamp, int rf, cudaStream_t s) {
+    commit_refresh_kernel<E><<<g.ntracks, kThreads, 0, s>>>(g, vcnt, stamp, rf);
 }
 
 void launch_commit_refresh(const GridDev &g, int *vcnt, int stamp, bool refresh, cudaStream_t s) {
     const int maxlen = g.X > g.Y ? g.X : g.Y;
+    if (maxlen > kMaxFusedTrackCells) throw Error(ERR_STATE, "fused batch commit on tracks longer than 4096 cells");
     const int e = (maxlen + kThreads - 1) / kThreads;
     const int rf = refresh ? 1 : 0;
-    if (e <= 1) commit_refresh_kernel<1><<<g.ntracks, kThreads, 0, s>>>(g, vcnt, stamp, rf);
-    else if (e <= 2) commit_refresh_kernel<2><<<g.ntracks, kThreads, 0, s>>>(g, vcnt, stamp, rf);
-    else if (e <= 4) commit_refresh_kernel<4><<<g.ntracks, kThreads, 0, s>>>(g, vcnt, stamp, rf);
-    else if (e <= 8) commit_refresh_kernel<8><<<g.ntracks, kThreads, 0, s>>>(g, vcnt, stamp, rf);
-    else commit_refresh_kernel<16><<<g.ntracks, kThreads, 0, s>>>(g, vcnt, stamp, rf);
+    if (e <= 1) commit_refresh_e<1>(g, vcnt, stamp, rf, s);
+    else if (e <= 2) commit_refresh_e<2>(g, vcnt, stamp, rf, s);
+    else if (e <= 4) commit_refresh_e<4>(g, vcnt, stamp, rf, s);
+    else if (e <= 8) commit_refresh_e<8>(g, vcnt, stamp, rf, s);
+    else commit_refresh_e<16>(g, vcnt, stamp, rf, s);  // longer tracks commit with the split launches
 }
 
 static int grid_for(int64_t n) {

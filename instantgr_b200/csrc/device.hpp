@@ -18,6 +18,13 @@
 
 namespace igr {
 
+// longest track: the reference's compute_presum holds a track in at most
+// 120 KB of shared memory, 15,360 doubles (src/main.cpp:28)
+constexpr int kMaxTrackCells = 15360;
+// longest track of the fused batch commit (commit_refresh); grids with longer
+// tracks commit with the separate wire and via launches
+constexpr int kMaxFusedTrackCells = 4096;
+
 struct GridDev {
     int L = 0, X = 0, Y = 0, DIR = 0;  // routing layers, grid, direction of routing layer 0
     int64_t N = 0;                      // L*X*Y cells
@@ -179,8 +186,10 @@ struct ShapeArgs {
     int n = 0, X = 0, Y = 0, sparsity = 15;
 };
 void launch_shape_count(const ShapeArgs &a, int *pt_off, int *claim_off, long long *totals, cudaStream_t s);
+// pt_n / claim_n (optional, [n]): per shape the number of distinct points and
+// claimed cells, which the fill sorts and moves to the front of each range
 void launch_shape_fill(const ShapeArgs &a, const int *pt_off, const int *claim_off, int *pts, int *claim,
-                       cudaStream_t s);
+                       int *pt_n, int *claim_n, cudaStream_t s);
 
 // ---- detour DAGs on the device (dagbuild.cu)
 // slice sizes of one builder thread's work area: tree nodes, stem entries,
@@ -295,6 +304,9 @@ struct ColorDev {
     // cells claimed by each shape: 4-neighbourhood of its points, every
     // `sparsity`-th cell of its segments (CSR over shapes)
     const int *claim_off = nullptr, *claim = nullptr;
+    // optional [shapes]: the shape's distinct claims / points are the first
+    // claim_n[s] / pt_n[s] entries of its range (else the whole range)
+    const int *claim_n = nullptr, *pt_n = nullptr;
     int npts = 0;
     int *map = nullptr;       // [X*Y]
     int *batch = nullptr;     // [n]

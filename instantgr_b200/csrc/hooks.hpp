@@ -12,12 +12,16 @@ struct TestHooks {
     std::atomic<int> mbar_probe{0};       // seed GEMM: first waits on an mbarrier that nothing arrives on
     std::atomic<int> color_keep_map{1};   // igr_color_batches: keep the round-0 map (1) or re-claim (0)
     std::atomic<int> dag_split_nets{4096};  // DAG DP: batches of this many nets or more run split by DAG size
+    std::atomic<int> color_keep_min_nets{2000000};  // router: colourings of this many nets or more keep the map
+    std::atomic<int> shape_dedupe{1};  // router: each shape's conflict points and claims kept once
     void reset() {
         wait_ns = 2000000000LL;
         barrier_phantom = 0;
         mbar_probe = 0;
         color_keep_map = 1;
         dag_split_nets = 4096;
+        color_keep_min_nets = 2000000;
+        shape_dedupe = 1;
     }
 };
 TestHooks &test_hooks();

@@ -169,7 +169,8 @@ void GridOwner::create(int L, int X, int Y, int DIR, const int *xl, const int *y
                        double unit_via, const double *sc, const float *cap_ref, cudaStream_t s) {
     if (L != kRouteLayers) throw Error(ERR_INVALID, "the router handles 9 routing layers");
     if (X < 2 || Y < 2) throw Error(ERR_INVALID, "grid must be at least 2x2");
-    if (X > 4096 || Y > 4096) throw Error(ERR_CAPACITY, "tracks longer than 4096 GCells are not supported");
+    if (X > kMaxTrackCells || Y > kMaxTrackCells)
+        throw Error(ERR_CAPACITY, "tracks longer than 15360 GCells are not supported (the reference's limit)");
     g = GridDev();
     g.L = L; g.X = X; g.Y = Y; g.DIR = DIR;
     g.N = (int64_t)L * X * Y;
@@ -251,6 +252,8 @@ void KernelTimer::reset() {
 }
 
 void ShapeDev::upload(const ShapeSet &sh, int X, int Y, int sp, cudaStream_t st, int threads) {
+    pt_n.release();  // whole ranges: host-built lists are used as they are
+    claim_n.release();
     pt_off.upload(sh.pt_off, st); pts.upload(sh.pts, st); pt_net.upload(sh.pt_net, st);
     h_off.upload(sh.h_off, st); hseg.upload(sh.hseg, st);
     v_off.upload(sh.v_off, st); vseg.upload(sh.vseg, st);
@@ -412,7 +415,14 @@ void Router::device_shapes(const ShapeArgs &a, ShapeDev &sd) {
     if (h_tot[0] > INT32_MAX || h_tot[1] > INT32_MAX) throw Error(ERR_CAPACITY, "conflict shapes exceed 32-bit offsets");
     sd.pts.alloc((size_t)h_tot[0]);
     sd.claim.alloc((size_t)h_tot[1]);
-    launch_shape_fill(a, sd.pt_off.p, sd.claim_off.p, sd.pts.p, sd.claim.p, s);
+    if (test_hooks().shape_dedupe.load()) {
+        sd.pt_n.alloc((size_t)std::max(a.n, 1));
+        sd.claim_n.alloc((size_t)std::max(a.n, 1));
+    } else {
+        sd.pt_n.release();
+        sd.claim_n.release();
+    }
+    launch_shape_fill(a, sd.pt_off.p, sd.claim_off.p, sd.pts.p, sd.claim.p, sd.pt_n.p, sd.claim_n.p, s);
     sd.npts = (int)h_tot[0];
     sd.nshapes = a.n;
     sd.sparsity = a.sparsity;
@@ -733,6 +743,8 @@ void Router::plan_phase1(int nb, std::vector<int> &batch_off, std::vector<int> &
 // The per-batch launches of phase 1 (Lshape_route.hpp:235-242), stream-ordered.
 void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<int> &class_off, bool timed) {
     const int nb = (int)batch_off.size() - 1;
+    // the fused per-track commit holds tracks of up to kMaxFusedTrackCells cells
+    const bool split = split || std::max(go.g.X, go.g.Y) > kMaxFusedTrackCells;
     cuda_check(cudaMemsetAsync(d_queue.p, 0, (3 * (size_t)nb + 1) * sizeof(int), s), "memset");
     for (int bi = 0; bi < nb; bi++) {
         const int off = batch_off[bi], n = batch_off[bi + 1] - off;
@@ -747,7 +759,7 @@ void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<in
             }
         }
         if (timed) kt.begin(KC_COST);
-        if (split_commit) launch_cost_refresh(go.g, true, s);
+        if (split) launch_cost_refresh(go.g, true, s);
         else launch_commit_refresh(go.g, d_vcnt.p, bi, true, s);  // commits batch bi-1 (stamp bi)
         if (timed) kt.end(KC_COST);
         if (timed) kt.begin(KC_PATTERN);
@@ -762,7 +774,7 @@ void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<in
             TreeBatchDev tb{d_ids.p + a, d_tree_off.p, d_tree_nodes.p, d_tree_par.p, d_route_off.p, d_route_cap.p,
                             routes.p, d_scratch.p, d_scratch_off.p, scratch_nodes, e - a};
             tb.queue = d_queue.p + 3 * bi + c;
-            tb.vcnt = split_commit ? nullptr : d_vcnt.p;
+            tb.vcnt = split ? nullptr : d_vcnt.p;
             cudaStream_t cs = s;
             if (batched) {
                 tb.tile = c == 0 ? 32 : (c == 1 ? kPatternNodeTile : 6);
@@ -787,7 +799,7 @@ void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<in
         }
         if (timed) kt.end(KC_PATTERN);
         st.launches += 1;
-        if (!split_commit) continue;
+        if (!split) continue;
         if (timed) kt.begin(KC_WIRE_COMMIT);
         launch_wire_commit(go.g, stamp, true, s);
         if (timed) kt.end(KC_WIRE_COMMIT);
@@ -797,7 +809,7 @@ void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<in
         if (timed) kt.end(KC_VIA_COMMIT);
         st.launches += 2;
     }
-    if (!split_commit && nb > 0) {  // commit of the last batch; its costs are refreshed when next needed
+    if (!split && nb > 0) {  // commit of the last batch; its costs are refreshed when next needed
         if (timed) kt.begin(KC_COST);
         launch_commit_refresh(go.g, d_vcnt.p, nb, false, s);
         if (timed) kt.end(KC_COST);
@@ -998,10 +1010,6 @@ void Router::color_nets(const std::vector<int> &order, const ShapeDev &shapes, i
     }
 }
 
-namespace {
-constexpr int kColorKeepMapNets = 2000000;
-}  // namespace
-
 int Router::run_color(int n, const int *d_perm_ranks, const ShapeDev &shapes, int sparsity) {
     d_map.alloc((size_t)ns.X * ns.Y);
     d_bat.alloc(n);
@@ -1015,6 +1023,8 @@ int Router::run_color(int n, const int *d_perm_ranks, const ShapeDev &shapes, in
     cd.pt_off = shapes.pt_off.p; cd.pts = shapes.pts.p; cd.pt_net = shapes.pt_net.p;
     cd.h_off = shapes.h_off.p; cd.hseg = shapes.hseg.p; cd.v_off = shapes.v_off.p; cd.vseg = shapes.vseg.p;
     cd.claim_off = shapes.claim_off.p; cd.claim = shapes.claim.p;
+    cd.claim_n = shapes.claim_n.n ? shapes.claim_n.p : nullptr;
+    cd.pt_n = shapes.pt_n.n ? shapes.pt_n.p : nullptr;
     cd.active = d_act.p; cd.active2 = d_act.p + n; cd.cand = d_act.p + 2 * (size_t)n; cd.lost = d_act.p + 3 * (size_t)n;
     cd.hdr = d_hdr.p;
     cd.ops = d_cops.p;
@@ -1024,7 +1034,7 @@ int Router::run_color(int n, const int *d_perm_ranks, const ShapeDev &shapes, in
     // in phase 1, 12% in the rip-up passes), while the recomputation of the
     // cells whose owner joined costs about as much as the claims it saves on
     // designs of up to a million nets (130k-net design: 3.5 ms to 7.2 ms).
-    if (n >= kColorKeepMapNets && shapes.claim.n < (size_t)INT32_MAX) {
+    if (n >= test_hooks().color_keep_min_nets.load() && shapes.claim.n < (size_t)INT32_MAX) {
         const size_t XY = (size_t)ns.X * ns.Y;
         d_rev_off.alloc(XY); d_rev_cnt.alloc(XY); d_rev.alloc(std::max<size_t>(1, shapes.claim.n));
         d_snap.alloc(XY); d_dirty.alloc(XY); d_part.alloc(1024);

@@ -154,6 +154,7 @@ struct ShapeSet {
 };
 struct ShapeDev {
     DevBuf<int> pt_off, pts, pt_net, h_off, hseg, v_off, vseg, claim_off, claim;
+    DevBuf<int> pt_n, claim_n;  // distinct points / claims per shape (shapes built on the device)
     int npts = 0, nshapes = 0, sparsity = 0;
     int64_t bytes = 0;  // host-to-device bytes of the last upload
     void upload(const ShapeSet &s, int X, int Y, int sparsity, cudaStream_t st, int threads = 0);

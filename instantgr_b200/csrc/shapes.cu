@@ -131,7 +131,36 @@ __global__ void __launch_bounds__(kScanThreads) shape_scan_kernel(int R, int *pt
     block_scan(claim_off, R, totals + 1);
 }
 
-__global__ void shape_fill_kernel(ShapeSrc a, const int *pt_off, const int *claim_off, int *pts, int *claim) {
+// Sorts a[0..n) (Shell's method, Ciura's gaps) and moves its distinct values
+// to the front; returns their number.
+__device__ int sort_unique(int *a, int n) {
+    constexpr int kGaps[8] = {701, 301, 132, 57, 23, 10, 4, 1};
+#pragma unroll 1
+    for (int gi = 0; gi < 8; gi++) {
+        const int gap = kGaps[gi];
+        for (int i = gap; i < n; i++) {
+            const int v = a[i];
+            int j = i;
+            while (j >= gap && a[j - gap] > v) {
+                a[j] = a[j - gap];
+                j -= gap;
+            }
+            a[j] = v;
+        }
+    }
+    int m = 0;
+    for (int i = 0; i < n; i++)
+        if (m == 0 || a[i] != a[m - 1]) a[m++] = a[i];
+    return m;
+}
+
+// pt_n / claim_n (optional): the number of distinct points and claimed cells of
+// each shape, moved to the front of its range.  A node of a tree is a point
+// once for itself and again for every straight edge it ends, and the claims of
+// neighbouring points and of segment samples overlap; the colouring only asks
+// whether a cell is claimed and whether a point is owned, so each is kept once.
+__global__ void shape_fill_kernel(ShapeSrc a, const int *pt_off, const int *claim_off, int *pts, int *claim,
+                                  int *pt_n, int *claim_n) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.n) return;
     const int X = a.X, Y = a.Y, sp = a.sp;
@@ -152,6 +181,8 @@ __global__ void shape_fill_kernel(ShapeSrc a, const int *pt_off, const int *clai
         [&](int lo, int hi, int x) {
             for (int y = lo; y <= hi; y += sp) *cl++ = x * Y + y;
         });
+    if (pt_n) pt_n[k] = sort_unique(pts + pt_off[k], (int)(pt - (pts + pt_off[k])));
+    if (claim_n) claim_n[k] = sort_unique(claim + claim_off[k], (int)(cl - (claim + claim_off[k])));
 }
 
 }  // namespace
@@ -164,10 +195,11 @@ void launch_shape_count(const ShapeArgs &a, int *pt_off, int *claim_off, long lo
 }
 
 void launch_shape_fill(const ShapeArgs &a, const int *pt_off, const int *claim_off, int *pts, int *claim,
-                       cudaStream_t s) {
+                       int *pt_n, int *claim_n, cudaStream_t s) {
     const ShapeSrc src{a.tree_off, a.tree_nodes, a.tree_par, a.ids, a.ext_off, a.ext_pts, a.ext_at,
                        a.ext_cnt, a.ext_stride, a.n, a.X, a.Y, a.sparsity};
-    if (a.n > 0) shape_fill_kernel<<<(a.n + 255) / 256, 256, 0, s>>>(src, pt_off, claim_off, pts, claim);
+    if (a.n > 0)
+        shape_fill_kernel<<<(a.n + 255) / 256, 256, 0, s>>>(src, pt_off, claim_off, pts, claim, pt_n, claim_n);
 }
 
 }  // namespace igr

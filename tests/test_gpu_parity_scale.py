@@ -313,3 +313,44 @@ def test_phase1_colouring_properties_and_batch_count_at_130k_nets(work):
     ref = _reference_phase1_batches(cap, net, 3)
     lo, hi = min(ref), max(ref)
     assert 0.9 * lo <= nb <= 1.1 * hi, (nb, ref)
+
+
+@pytest.mark.parametrize("X,Y,dir0", [(5000, 8, 0), (8, 5000, 1), (15360, 4, 0)])
+def test_long_track_costs_bit_exact_vs_reference(work, X, Y, dir0):
+    """Tracks longer than 4096 GCells (up to the reference's 15,360): the cost
+    model and the f64 Sklansky prefix sums bit-identical to the reference's
+    kernels on the same demand."""
+    g = cases.grid_case(61, X=X, Y=Y, dir0=dir0)
+    _, vc, ps = _harness("cost", cases.grid_arrays(g), [np.float32, np.float32, np.float64], work)
+    c = _ctx(g)
+    c.cost_refresh()
+    v2, p2 = c.costs()
+    c.close()
+    assert np.array_equal(v2, vc), f"vcost: {np.count_nonzero(v2 != vc)} cells differ"
+    assert np.array_equal(p2, ps), f"presum: {np.count_nonzero(p2 != ps)} cells differ"
+
+
+def test_grid_with_5000_gcell_tracks_routes(work):
+    """A 5000x1000 design (horizontal tracks of 5000 GCells, beyond the fused
+    batch commit's 4096, so phase 1 commits with the separate launches):
+    routed with a rip-up pass, records well formed, and the device
+    evaluation's wire length equal to the router's own count."""
+    X, Y = 5000, 1000
+    cap, net = os.path.join(work, "g5k.cap"), os.path.join(work, "g5k.net")
+    ig.generate_custom(X, Y, 40000, seed=77, cap_mode=1, block_frac=0.0, pin_mode=1, bbox_median=10,
+                       bbox_sigma=1.2, hotspots=4, hotspot_frac=0.4, cap=cap, net=net)
+    r = ig.Router(cap, net, rrr_iters=1)
+    r.run()
+    ev = r.evaluate()
+    st = r.stats()
+    _, R = r.sizes()
+    XY = X * Y
+    for k in range(0, R, max(1, R // 2000)):
+        rec = r.route(k)
+        assert rec[0] == len(rec) and rec[0] % 2 == 1
+        a, b = rec[1::2], rec[2::2]
+        via = a // XY != b // XY
+        assert np.all(~via | ((a % XY) == (b % XY)))
+    r.close()
+    assert np.isfinite(ev["total"]) and ev["total"] > 0
+    assert abs(ev["wirelength"] - st["wirelength"]) <= 1e-6 * st["wirelength"]

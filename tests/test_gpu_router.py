@@ -186,3 +186,31 @@ def test_route_records_after_rerouting(tmp_path):
         via = a // XY != b // XY
         assert np.all(~via | ((xa == xb) & (ya == yb)))
         assert np.all(via | (xa == xb) | (ya == yb))
+
+
+@pytest.mark.parametrize("hook,values", [("HOOK_SHAPE_DEDUPE", (0, 1)), ("HOOK_COLOR_KEEP_MIN_NETS", (2000000, 1))])
+def test_colouring_variants_give_the_same_routing(tmp_path, hook, values):
+    """Conflict points and claims kept once per net or with every repetition,
+    and the round-0 claim map cleared per batch or kept up to date: the same
+    phase-1 batches, and the same demand after three rip-up passes (whose
+    colourings use the same variants).  The order of the nets inside a batch
+    comes from an atomic scatter and does not matter (they share no state)."""
+    cap, net = str(tmp_path / "d.cap"), str(tmp_path / "d.net")
+    ig.generate(1, 5, 0.2, cap, net)
+    res = []
+    for v in values:
+        ig.set_test_hook(getattr(ig, hook), v)
+        try:
+            r = ig.Router(cap, net, rrr_iters=3)
+            r.run()
+            p = r.plan()
+            res.append((p["batch_off"], p["net_ids"], r.demand(), r.stats()["color_rounds"]))
+            r.close()
+        finally:
+            ig.set_test_hook(ig.HOOK_RESET)
+    (b0, i0, d0, c0), (b1, i1, d1, c1) = res
+    assert np.array_equal(b0, b1)
+    for b in range(len(b0) - 1):
+        assert np.array_equal(np.sort(i0[b0[b]:b0[b + 1]]), np.sort(i1[b1[b]:b1[b + 1]])), f"batch {b}"
+    assert np.array_equal(d0, d1)
+    assert c0 == c1
