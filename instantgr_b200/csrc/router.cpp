@@ -287,6 +287,7 @@ Router::~Router() {
 
 void Router::open(const char *cap, const char *net) {
     const double t0 = now_s();
+    hpwl_keys.clear();
     // The CUDA driver, the caller's device context and the routing grid are
     // brought up on a side thread while the host parses and builds trees (the
     // first CUDA call of a process can take a second).  The device is the
@@ -1114,12 +1115,20 @@ bool Router::rrr_pass(int iter) {
             return ns.nets[l].hpwl > ns.nets[r].hpwl;
         });
     } else {
-        // the comparisons of the reference's sort, on a contiguous copy of the keys
-        std::vector<int> hp(R);
-        parallel_for(R, threads, [&](int b, int e) {
-            for (int i = b; i < e; i++) hp[i] = ns.nets[i].hpwl;
-        });
-        std::sort(of_nets.begin(), of_nets.end(), [&](int l, int r) { return hp[l] > hp[r]; });
+        // the comparisons of the reference's sort (Lshape_route_detour.hpp:732-734):
+        // (key, id) pairs compared on the key alone give the same sequence of
+        // comparisons, hence the same order, as the ids compared through a key table
+        if ((int)hpwl_keys.size() != R) {  // the trees (and their HPWL) are fixed after open
+            hpwl_keys.resize(R);
+            parallel_for(R, threads, [&](int b, int e) {
+                for (int i = b; i < e; i++) hpwl_keys[i] = ns.nets[i].hpwl;
+            });
+        }
+        std::vector<std::pair<int, int>> kv(of_nets.size());
+        for (size_t k = 0; k < of_nets.size(); k++) kv[k] = {hpwl_keys[of_nets[k]], of_nets[k]};
+        std::sort(kv.begin(), kv.end(),
+                  [](const std::pair<int, int> &l, const std::pair<int, int> &r) { return l.first > r.first; });
+        for (size_t k = 0; k < of_nets.size(); k++) of_nets[k] = kv[k].second;
     }
     // per colour batch: its first entries in the arrays of the pass and its sizes
     std::vector<std::vector<int>> batches;

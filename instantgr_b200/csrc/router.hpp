@@ -282,6 +282,7 @@ struct Router {
     DevBuf<float> d_seed_dem;         // seed demand at full strength (unrounded), track layout
     DevBuf<float> d_seed_cur;         // seed demand currently added to the demand (half units)
     std::vector<double> seed_sat;     // summed-area table of the predicted overflow
+    std::vector<int> hpwl_keys;       // HPWL of every routing net, contiguous (rip-up order keys)
     void prepare_seed();
     void seed_begin();
     double seed_pressure(int net) const;
