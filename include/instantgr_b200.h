@@ -93,10 +93,11 @@ int igr_router_evaluate(igr_router *r, double *out, double *layer_loss);
  * device setup (grid, trees, conflict shapes). */
 int igr_router_stats(igr_router *r, double *out, int n);
 /* Per-kernel-class device time of the last run (needs opt->profile): for
- * class k in {cost refresh (with the fused phase-1 commit), tree DP, wire
- * commit, via commit, DAG DP, colouring, rip-up/marking, phase-1 graph},
- * out[3k] = launches, out[3k+1] = milliseconds, out[3k+2] = algorithmic DRAM
- * bytes (cost refresh: 20 per refreshed cell + 12 per committed cell;
+ * class k in {cost refresh, tree DP, wire commit, via commit, DAG DP,
+ * colouring, rip-up/marking, phase-1 graph, fused phase-1 commit and cost
+ * refresh}, out[3k] = launches, out[3k+1] = milliseconds, out[3k+2] =
+ * algorithmic DRAM bytes (cost refresh: 20 per refreshed cell; fused commit
+ * and refresh: 20 per refreshed cell + 12 per committed cell;
  * colouring: 12 per claimed cell, 8 per commit point check, 12 per blocking
  * point check, 8 per release check, 8 per active-list entry scanned; tree
  * DP: 32 per node, 144 per straight and 360 per bent tree edge). */

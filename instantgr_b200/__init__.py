@@ -208,7 +208,7 @@ STATIC_SCRATCH_BYTES = 64 << 20
 STATIC_MAX_NETS = 1 << 20
 
 KERNEL_CLASSES = ["cost_refresh", "pattern_dp", "wire_commit", "via_commit", "dag_dp", "coloring", "ripup",
-                  "phase1_graph"]
+                  "phase1_graph", "commit_refresh"]
 
 STATS = ["routing_nets", "rerouted", "wirelength", "via_cost", "overflow_cost", "route_s", "batches1", "p1_ms",
          "rrr_ms", "dag_host_ms", "launches", "design_nets", "color_rounds", "h2d_bytes", "d2h_bytes",

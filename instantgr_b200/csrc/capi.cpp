@@ -141,8 +141,11 @@ int igr_router_kstats(igr_router *h, double *o, int n) {
     const auto &r = h->r;
     for (int k = 0; k < KC_N; k++) {
         double v[3] = {(double)r.kt.launches[k], r.kt.ms[k],
-                       k == KC_COST ? 20.0 * (double)r.cost_cells + 12.0 * (double)r.commit_cells
-                                    : (k == KC_COLOR ? r.color_bytes : (k == KC_PATTERN ? r.dp_bytes : 0.0))};
+                       k == KC_COST             ? 20.0 * (double)r.cost_cells
+                       : k == KC_COMMIT_REFRESH ? 20.0 * (double)r.commit_refresh_cells + 12.0 * (double)r.commit_cells
+                       : k == KC_COLOR          ? r.color_bytes
+                       : k == KC_PATTERN        ? r.dp_bytes
+                                                : 0.0};
         for (int j = 0; j < 3; j++)
             if (3 * k + j < n) o[3 * k + j] = v[j];
     }

@@ -21,12 +21,13 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <type_traits>
 
 namespace igr {
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kTrackThreads = 256;
 
 // Cost model of cell i of a track staged in s_cap / s_dem: writes its via cost
 // and returns the scan input, the wire cost of edge i-1 (0 for i = 0).
@@ -60,26 +61,79 @@ __device__ __forceinline__ double cell_costs(const GridDev &g, const TrackInfo &
     return x;
 }
 
-// Cost model and Sklansky prefix sums of one track whose capacity and demand
-// are staged in s_cap / s_dem; every thread of the block calls it.
-template <int MAXE>
-__device__ __forceinline__ void refresh_track(const GridDev &g, const TrackInfo &ti, const float *s_cap,
-                                              const float *s_dem) {
+// of_cost_scaled (graph.hpp:23-27, of_cost_scale = 1) in float: the
+// reference's exponent arguments 0.5 * (d - c) and 1.5 * d are formed in
+// double from float operands, where both products are exact, and rounded to
+// float, which is the correctly rounded float product 0.5f * (d - c) or
+// 1.5f * d; the comparison with 0.001 stays in double.
+__device__ __forceinline__ float of_cost_f(bool has_cap, float c, float d) {
+    if (has_cap) return __expf(0.5f * (d - c));
+    return d > 0.f ? __expf(1.5f * d) : 0.f;
+}
+
+// Cost model and Sklansky prefix sums of one track of n cells whose capacity
+// and demand are staged in s_cap / s_dem (and s_of1 has room for n floats);
+// every thread of the block calls it and tallies n in g.stats[slot].  Cell i lives at thread i % T, row i / T.
+//
+// Each cell's overflow costs at demand d, d + 0.5 and d + 1 are evaluated once
+// and left in shared memory (over its staged capacity and demand), so that
+// cell i reads its left neighbour's instead of evaluating them again:
+// vcost(i) needs the half-unit costs of cells i-1 and i, the wire cost of edge
+// i-1 the unit cost of cell i-1 (graph.hpp:40-71).
+template <int T, int MAXE>
+__device__ __forceinline__ void refresh_track(const GridDev &g, const TrackInfo &ti, float *s_cap, float *s_dem,
+                                              float *s_of1, int slot) {
+    constexpr int W = T / 32;
     const int n = ti.len;
-    const int E = (n + kThreads - 1) / kThreads;
+    const int E = (n + T - 1) / T;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const double sc = g.short_cost[ti.l];
     const int *elen = ti.dir ? g.ylen : g.xlen;
-    __shared__ double s_wt[kThreads / 32][MAXE];
+    __shared__ double s_wt[W][MAXE];
     __shared__ double s_rt[MAXE];
-    if (tid == 0) atomicAdd(&g.stats[2], (unsigned long long)n);  // refreshed cells, for the roofline
+    if (tid == 0) atomicAdd(&g.stats[slot], (unsigned long long)n);  // refreshed cells, for the roofline
 
+#pragma unroll
+    for (int r = 0; r < MAXE; r++) {
+        const int i = tid + r * T;
+        if (r < E && i < n) {
+            const float c = s_cap[i], d = s_dem[i];
+            const bool has_cap = (double)c > 0.001;
+            const double dd = (double)d;
+            s_cap[i] = of_cost_f(has_cap, c, d);
+            s_dem[i] = of_cost_f(has_cap, c, (float)(dd + 0.5));
+            s_of1[i] = of_cost_f(has_cap, c, (float)(dd + 1.0));
+        }
+    }
+    __syncthreads();
     double x[MAXE];
 #pragma unroll
     for (int r = 0; r < MAXE; r++) {
         x[r] = 0;
-        const int i = tid + r * kThreads;
-        if (r < E && i < n) x[r] = cell_costs(g, ti, s_cap, s_dem, i, sc, elen);
+        const int i = tid + r * T;
+        if (r < E && i < n) {
+            const double of0 = (double)s_cap[i];
+            const double bh = fmin(1e12, ((double)s_dem[i] - of0) * sc);
+            float v;
+            if (i == 0) {
+                v = (float)fmin(1e12, ((double)s_of1[0] - of0) * sc);
+            } else {
+                const double ofp = (double)s_cap[i - 1];
+                const double a1p = fmin(1e12, ((double)s_of1[i - 1] - ofp) * sc);
+                if (i == n - 1) {
+                    v = (float)a1p;
+                } else {
+                    const double bhp = fmin(1e12, ((double)s_dem[i - 1] - ofp) * sc);
+                    v = (float)(bh + bhp);
+                }
+                // scan input: wire cost of edge i-1 (graph.hpp:44-46)
+                float w = (float)a1p;
+                w = (float)fma(g.unit_wire, (double)elen[i - 1], (double)w);
+                x[r] = (double)w;
+            }
+            v = (float)((double)v + g.unit_via);
+            g.vcost[ti.base + i] = v;
+        }
     }
     // ---- Sklansky levels 0..4: lanes
 #pragma unroll
@@ -92,9 +146,9 @@ __device__ __forceinline__ void refresh_track(const GridDev &g, const TrackInfo 
             if (take) x[r] += o;
         }
     }
-    // ---- levels 5..7: warps
+    // ---- levels 5..log2(T)-1: warps
 #pragma unroll
-    for (int m = 0; m < 3; m++) {
+    for (int m = 0; (1 << m) < W; m++) {
         if (lane == 31) {
 #pragma unroll
             for (int r = 0; r < MAXE; r++) s_wt[warp][r] = x[r];
@@ -107,9 +161,9 @@ __device__ __forceinline__ void refresh_track(const GridDev &g, const TrackInfo 
         }
         __syncthreads();
     }
-    // ---- levels >= 8: rows
+    // ---- levels >= log2(T): rows
     if (E > 1) {
-        if (tid == kThreads - 1) {
+        if (tid == T - 1) {
 #pragma unroll
             for (int r = 0; r < MAXE; r++) s_rt[r] = x[r];
         }
@@ -132,7 +186,7 @@ __device__ __forceinline__ void refresh_track(const GridDev &g, const TrackInfo 
     }
 #pragma unroll
     for (int r = 0; r < MAXE; r++) {
-        const int i = tid + r * kThreads;
+        const int i = tid + r * T;
         if (r < E && i < n) g.presum[ti.base + i] = x[r];
     }
 }
@@ -165,19 +219,25 @@ __device__ __forceinline__ void stage_track(const float *a, const float *b, floa
     }
 }
 
-template <int MAXE>
-__global__ void __launch_bounds__(kThreads, 5) cost_refresh_kernel(GridDev g, int only_dirty) {
+// Threads per track of the per-track kernels: five CTAs of 256 per SM (a
+// CTA of 512 or 1024 threads per track shortens each track's chain but keeps
+// fewer tracks in flight per SM, and the refresh is issue-bound: 17.2 and
+// 28.2 ms against 11.5 ms per route of the 800k-net design).
+#define IGR_TRACK_BOUNDS(T) __launch_bounds__(T, 5)
+
+template <int T, int MAXE>
+__global__ void IGR_TRACK_BOUNDS(T) cost_refresh_kernel(GridDev g, int only_dirty) {
     const int tr = blockIdx.x;
     if (only_dirty) {
         if (!g.dirty_cost[tr]) return;
     }
     const TrackInfo ti = decode_track(g, tr);
-    __shared__ __align__(16) float s_cap[MAXE * kThreads];
-    __shared__ __align__(16) float s_dem[MAXE * kThreads];
-    stage_track(g.cap + ti.base, g.demand + ti.base, s_cap, s_dem, ti.len, threadIdx.x, kThreads);
+    extern __shared__ __align__(16) float s_track[];  // capacity, demand, unit-step cost: MAXE * T each
+    float *s_cap = s_track, *s_dem = s_track + MAXE * T, *s_of1 = s_track + 2 * MAXE * T;
+    stage_track(g.cap + ti.base, g.demand + ti.base, s_cap, s_dem, ti.len, threadIdx.x, T);
     __syncthreads();
     if (threadIdx.x == 0 && only_dirty) g.dirty_cost[tr] = 0;
-    refresh_track<MAXE>(g, ti, s_cap, s_dem);
+    refresh_track<T, MAXE>(g, ti, s_cap, s_dem, s_of1, 2);
 }
 
 // Tracks of more than 4096 cells (up to the reference's 15,360, main.cpp:28):
@@ -248,26 +308,26 @@ __device__ __forceinline__ int warp_incl_scan(int v, int lane) {
 // sums are rebuilt from the demand still in shared memory.  Tracks with no
 // pending commit and clean costs are skipped.  With refresh = 0 the costs are
 // only marked dirty.
-template <int MAXE>
-__global__ void __launch_bounds__(kThreads, 5) commit_refresh_kernel(GridDev g, int *vcnt, int stamp, int refresh) {
-    __shared__ __align__(16) float s_cap[MAXE * kThreads];
-    __shared__ __align__(16) float s_dem[MAXE * kThreads];
-    __shared__ int s_w[kThreads / 32];
+template <int T, int MAXE>
+__global__ void IGR_TRACK_BOUNDS(T) commit_refresh_kernel(GridDev g, int *vcnt, int stamp, int refresh) {
+    extern __shared__ __align__(16) float s_track[];  // capacity, demand, unit-step cost: MAXE * T each
+    float *s_cap = s_track, *s_dem = s_track + MAXE * T, *s_of1 = s_track + 2 * MAXE * T;
+    __shared__ int s_w[T / 32];
     __shared__ int s_carry;
-    __shared__ long long s_wl[kThreads / 32];
+    __shared__ long long s_wl[T / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int tr = blockIdx.x;
     const bool commit = g.dirty_commit[tr] != 0;
     if (!commit && !(refresh && g.dirty_cost[tr])) return;
     const TrackInfo ti = decode_track(g, tr);
     const int n = ti.len;
-    stage_track(refresh ? g.cap + ti.base : nullptr, g.demand + ti.base, s_cap, s_dem, n, tid, kThreads);
+    stage_track(refresh ? g.cap + ti.base : nullptr, g.demand + ti.base, s_cap, s_dem, n, tid, T);
     if (commit) {
         const int *elen = ti.dir ? g.ylen : g.xlen;
         if (tid == 0) s_carry = 0;
         __syncthreads();
         long long wl = 0;
-        for (int r0 = 0; r0 < n; r0 += kThreads) {
+        for (int r0 = 0; r0 < n; r0 += T) {
             const int i = r0 + tid;
             int v = 0;
             if (i < n) {
@@ -286,11 +346,11 @@ __global__ void __launch_bounds__(kThreads, 5) commit_refresh_kernel(GridDev g, 
                 wl += (long long)cnt * elen[i];
             }
             __syncthreads();
-            if (tid == kThreads - 1) s_carry = cnt;
+            if (tid == T - 1) s_carry = cnt;
             __syncthreads();
         }
         // vias, after every wire stamp of the track is in place
-        for (int i = tid; i < n; i += kThreads) {
+        for (int i = tid; i < n; i += T) {
             const int c = vcnt[ti.base + i];
             if (c == 0) continue;
             vcnt[ti.base + i] = 0;
@@ -306,10 +366,10 @@ __global__ void __launch_bounds__(kThreads, 5) commit_refresh_kernel(GridDev g, 
         for (int o = 16; o > 0; o >>= 1) wl += __shfl_down_sync(0xffffffffu, wl, o);
         if (lane == 0) s_wl[warp] = wl;
         __syncthreads();
-        for (int i = tid; i < n; i += kThreads) g.demand[ti.base + i] = s_dem[i];
+        for (int i = tid; i < n; i += T) g.demand[ti.base + i] = s_dem[i];
         if (tid == 0) {
             long long t = 0;
-            for (int w = 0; w < kThreads / 32; w++) t += s_wl[w];
+            for (int w = 0; w < T / 32; w++) t += s_wl[w];
             if (t) atomicAdd(&g.stats[0], (unsigned long long)t);
             atomicAdd(&g.stats[3], (unsigned long long)n);  // committed cells, for the roofline
             g.dirty_commit[tr] = 0;
@@ -319,7 +379,7 @@ __global__ void __launch_bounds__(kThreads, 5) commit_refresh_kernel(GridDev g, 
         __syncthreads();
         if (tid == 0) g.dirty_cost[tr] = 0;
     }
-    if (refresh) refresh_track<MAXE>(g, ti, s_cap, s_dem);
+    if (refresh) refresh_track<T, MAXE>(g, ti, s_cap, s_dem, s_of1, 4);
 }
 
 template <typename T>
@@ -346,46 +406,62 @@ __global__ void track_to_ref_kernel(GridDev g, const T *trk, T *ref) {
 
 }  // namespace
 
+// dynamic shared memory of a track kernel: capacity, demand and unit-step
+// cost of T * E cells
+template <int T, int E>
+constexpr size_t track_smem() { return (size_t)3 * T * E * sizeof(float); }
+
 // One CTA per track: the hardware block scheduler hands the dirty tracks to
-// the SMs as they free up (a resident grid striding over the tracks balanced
-// the uneven dirty tracks worse: 11.9 -> 15.8 ms per step on the 800k-net
-// design), and a CTA that finds its track clean exits at once.
-template <int E>
+// the SMs as they free up, and a CTA that finds its track clean exits at once
+// (a resident grid striding over the tracks balanced the uneven dirty tracks
+// worse: 11.9 -> 15.8 ms per route of the 800k-net design; a resident grid
+// over a list of the dirty tracks made by a one-CTA pass saved nothing).
+template <int T, int E>
 static void cost_refresh_e(const GridDev &g, int od, cudaStream_t s) {
-    cost_refresh_kernel<E><<<g.ntracks, kThreads, 0, s>>>(g, od);
+    constexpr size_t smem = track_smem<T, E>();
+    kernel_setup((const void *)cost_refresh_kernel<T, E>, T, smem);
+    cost_refresh_kernel<T, E><<<g.ntracks, T, smem, s>>>(g, od);
+}
+
+template <int T, int E>
+static void commit_refresh_e(const GridDev &g, int *vcnt, int stamp, int rf, cudaStream_t s) {
+    constexpr size_t smem = track_smem<T, E>();
+    kernel_setup((const void *)commit_refresh_kernel<T, E>, T, smem);
+    commit_refresh_kernel<T, E><<<g.ntracks, T, smem, s>>>(g, vcnt, stamp, rf);
+}
+
+// Calls f(E) with E = the rows per thread of a 256-thread CTA for tracks of
+// maxlen <= kMaxFusedTrackCells cells, exactly ceil(maxlen / 256): rows that
+// hold no cell of any track would still be scanned.
+template <int E, class F>
+static void with_rows(int e, F &&f) {
+    if constexpr (E * kTrackThreads >= kMaxFusedTrackCells) {
+        f(std::integral_constant<int, E>());
+    } else {
+        if (e <= E) f(std::integral_constant<int, E>());
+        else with_rows<E + 1>(e, f);
+    }
 }
 
 void launch_cost_refresh(const GridDev &g, bool only_dirty, cudaStream_t s) {
     const int maxlen = g.X > g.Y ? g.X : g.Y;
-    const int e = (maxlen + kThreads - 1) / kThreads;
     const int od = only_dirty ? 1 : 0;
-    if (e <= 1) cost_refresh_e<1>(g, od, s);
-    else if (e <= 2) cost_refresh_e<2>(g, od, s);
-    else if (e <= 4) cost_refresh_e<4>(g, od, s);
-    else if (e <= 8) cost_refresh_e<8>(g, od, s);
-    else if (e <= 16) cost_refresh_e<16>(g, od, s);  // tracks of <= 4096 cells
-    else {
+    if (maxlen <= kMaxFusedTrackCells) {
+        with_rows<1>((maxlen + kTrackThreads - 1) / kTrackThreads,
+                     [&](auto ec) { cost_refresh_e<kTrackThreads, decltype(ec)::value>(g, od, s); });
+    } else {
         const size_t smem = (size_t)kMaxTrackCells * 8;
         kernel_setup((const void *)cost_refresh_long_kernel, kLongThreads, smem);
         cost_refresh_long_kernel<<<g.ntracks, kLongThreads, smem, s>>>(g, od);
     }
 }
 
-template <int E>
-static void commit_refresh_e(const GridDev &g, int *vcnt, int stamp, int rf, cudaStream_t s) {
-    commit_refresh_kernel<E><<<g.ntracks, kThreads, 0, s>>>(g, vcnt, stamp, rf);
-}
-
 void launch_commit_refresh(const GridDev &g, int *vcnt, int stamp, bool refresh, cudaStream_t s) {
     const int maxlen = g.X > g.Y ? g.X : g.Y;
     if (maxlen > kMaxFusedTrackCells) throw Error(ERR_STATE, "fused batch commit on tracks longer than 4096 cells");
-    const int e = (maxlen + kThreads - 1) / kThreads;
     const int rf = refresh ? 1 : 0;
-    if (e <= 1) commit_refresh_e<1>(g, vcnt, stamp, rf, s);
-    else if (e <= 2) commit_refresh_e<2>(g, vcnt, stamp, rf, s);
-    else if (e <= 4) commit_refresh_e<4>(g, vcnt, stamp, rf, s);
-    else if (e <= 8) commit_refresh_e<8>(g, vcnt, stamp, rf, s);
-    else commit_refresh_e<16>(g, vcnt, stamp, rf, s);  // longer tracks commit with the split launches
+    with_rows<1>((maxlen + kTrackThreads - 1) / kTrackThreads,
+                 [&](auto ec) { commit_refresh_e<kTrackThreads, decltype(ec)::value>(g, vcnt, stamp, rf, s); });
 }
 
 static int grid_for(int64_t n) {

@@ -25,6 +25,8 @@ constexpr int kMaxTrackCells = 15360;
 // tracks commit with the separate wire and via launches
 constexpr int kMaxFusedTrackCells = 4096;
 
+constexpr int kStatSlots = 5;  // entries of GridDev::stats
+
 struct GridDev {
     int L = 0, X = 0, Y = 0, DIR = 0;  // routing layers, grid, direction of routing layer 0
     int64_t N = 0;                      // L*X*Y cells
@@ -40,7 +42,8 @@ struct GridDev {
     uint8_t *dirty_cost = nullptr;    // [ntracks] demand changed since the last cost refresh
     uint8_t *dirty_commit = nullptr;  // [ntracks] difference array holds entries
     unsigned long long *stats = nullptr;  // [0] wirelength, [1] via count (signed, two's complement),
-                                          // [2] refreshed cells, [3] committed cells
+                                          // [2] cells refreshed by cost_refresh, [3] cells committed and
+                                          // [4] cells refreshed by commit_refresh
     int *err = nullptr;                   // device error word
 };
 

@@ -184,7 +184,7 @@ void GridOwner::create(int L, int X, int Y, int DIR, const int *xl, const int *y
     xlen.upload(xl, X - 1, s); ylen.upload(yl, Y - 1, s);
     short_cost.upload(sc, L, s);
     dirty_cost.alloc(g.ntracks); dirty_commit.alloc(g.ntracks);
-    stats.alloc(4); err.alloc(1);
+    stats.alloc(kStatSlots); err.alloc(1);
     score.alloc(g.ntracks + 1);
     g.cap = cap.p; g.demand = demand.p; g.vcost = vcost.p; g.presum = presum.p;
     g.pre = pre.p; g.stamp = stamp.p; g.xlen = xlen.p; g.ylen = ylen.p; g.short_cost = short_cost.p;
@@ -204,7 +204,7 @@ void GridOwner::reset_demand(cudaStream_t s) {
     cuda_check(cudaMemsetAsync(demand.p, 0, g.N * sizeof(float), s), "memset");
     cuda_check(cudaMemsetAsync(pre.p, 0, g.N * sizeof(int), s), "memset");
     cuda_check(cudaMemsetAsync(stamp.p, 0, g.N * sizeof(int), s), "memset");
-    cuda_check(cudaMemsetAsync(stats.p, 0, 4 * sizeof(unsigned long long), s), "memset");
+    cuda_check(cudaMemsetAsync(stats.p, 0, kStatSlots * sizeof(unsigned long long), s), "memset");
     cuda_check(cudaMemsetAsync(dirty_commit.p, 0, g.ntracks, s), "memset");
     mark_all_dirty(s);
 }
@@ -542,6 +542,7 @@ void Router::save_result(RouteBackup &b) {
     b.score[2] = score_of;
     b.cost_cells = cost_cells;
     b.commit_cells = commit_cells;
+    b.commit_refresh_cells = commit_refresh_cells;
     b.color_bytes = color_bytes;
 }
 
@@ -560,6 +561,7 @@ void Router::restore_result(RouteBackup &b) {
     score_of = b.score[2];
     cost_cells = b.cost_cells;
     commit_cells = b.commit_cells;
+    commit_refresh_cells = b.commit_refresh_cells;
     color_bytes = b.color_bytes;
     h_routes_valid = false;
     go.mark_all_dirty(s);
@@ -759,10 +761,10 @@ void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<in
                 st.launches += 1;
             }
         }
-        if (timed) kt.begin(KC_COST);
+        if (timed) kt.begin(split ? KC_COST : KC_COMMIT_REFRESH);
         if (split) launch_cost_refresh(go.g, true, s);
         else launch_commit_refresh(go.g, d_vcnt.p, bi, true, s);  // commits batch bi-1 (stamp bi)
-        if (timed) kt.end(KC_COST);
+        if (timed) kt.end(split ? KC_COST : KC_COMMIT_REFRESH);
         if (timed) kt.begin(KC_PATTERN);
         // batched form: the large (c = 0) and small (c = 2) classes are forked
         // onto their own streams and run beside the medium class (c = 1)
@@ -811,9 +813,9 @@ void Router::emit_phase1(const std::vector<int> &batch_off, const std::vector<in
         st.launches += 2;
     }
     if (!split && nb > 0) {  // commit of the last batch; its costs are refreshed when next needed
-        if (timed) kt.begin(KC_COST);
+        if (timed) kt.begin(KC_COMMIT_REFRESH);
         launch_commit_refresh(go.g, d_vcnt.p, nb, false, s);
-        if (timed) kt.end(KC_COST);
+        if (timed) kt.end(KC_COMMIT_REFRESH);
         st.launches += 1;
     }
 }
@@ -1605,7 +1607,7 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
 }
 
 void Router::compute_score() {
-    unsigned long long h[4] = {0, 0, 0, 0};
+    unsigned long long h[kStatSlots] = {0, 0, 0, 0, 0};
     double of = 0;
     launch_overflow_cost(go.g, go.score.p, s);
     st.launches += 2;
@@ -1624,6 +1626,7 @@ void Router::compute_score() {
     color_bytes = 12.0 * cops[0] + 8.0 * cops[1] + 12.0 * cops[2] + 8.0 * cops[3] + 8.0 * cops[4];
     cost_cells = h[2];
     commit_cells = h[3];
+    commit_refresh_cells = h[4];
     score_wl = (double)(int64_t)h[0] * d.unit_wire;
     score_via = (double)((int64_t)h[1] + pin_vias) * d.unit_via;
     score_of = of;

@@ -135,7 +135,9 @@ struct RouterStats {
 
 // Per-kernel-class device time, measured with CUDA events around each launch
 // when profiling is on.
-enum KernelClass { KC_COST = 0, KC_PATTERN, KC_WIRE_COMMIT, KC_VIA_COMMIT, KC_DAG, KC_COLOR, KC_RIPUP, KC_GRAPH1, KC_N };
+enum KernelClass {
+    KC_COST = 0, KC_PATTERN, KC_WIRE_COMMIT, KC_VIA_COMMIT, KC_DAG, KC_COLOR, KC_RIPUP, KC_GRAPH1, KC_COMMIT_REFRESH, KC_N
+};
 struct KernelTimer {
     bool on = false;
     cudaStream_t s = nullptr;
@@ -172,7 +174,7 @@ struct RouteBackup {
     RouterStats st;
     std::vector<double> kt_ms;
     double score[3] = {0, 0, 0};
-    unsigned long long cost_cells = 0, commit_cells = 0;
+    unsigned long long cost_cells = 0, commit_cells = 0, commit_refresh_cells = 0;
     double color_bytes = 0;
 };
 
@@ -261,7 +263,7 @@ struct Router {
     std::vector<std::unique_ptr<std::pmr::monotonic_buffer_resource>> dag_arenas;
     std::vector<DagNet> dag;     // detour DAGs of the nets rerouted in the current pass
     std::vector<int> dag_slot;   // routing net -> its DAG in `dag`, -1 when not rerouted
-    unsigned long long cost_cells = 0, commit_cells = 0;
+    unsigned long long cost_cells = 0, commit_cells = 0, commit_refresh_cells = 0;
     // phase-1 plan of the last run (routing order, batches, trees, route capacity in order)
     std::vector<int> plan_ids, plan_batch_off, plan_node_off, plan_nodes, plan_par, plan_cap;
     bool plan_built = false;
