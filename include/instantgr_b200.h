@@ -352,6 +352,15 @@ int igr_seed_train(igr_seed *m, int steps, int tiles, float lr, uint64_t seed, i
 int igr_seed_eval(igr_seed *m, int map, double *out, int n);
 /* Prediction of a whole feature map (tiled). */
 int igr_seed_predict(igr_seed *m, int X, int Y, const float *features, float *pred);
+/* Device time of the network's forward convolutions (the tcgen05 implicit
+ * GEMMs) over `tiles` tiles of the current tile size, averaged over `reps`
+ * passes after one untimed pass: layer_ms[i] = milliseconds of convolution i
+ * per pass (CUDA events on the model's stream), layer_flops[i] = its
+ * multiply-add FLOPs per pass (2 x output pixels x 9 x cin x cout); both
+ * arrays hold IGR_SEED_CONVS entries.  The tiles hold the last inputs loaded
+ * (zeros at first): the time does not depend on the values. */
+#define IGR_SEED_CONVS 6
+int igr_seed_time_forward(igr_seed *m, int tiles, int reps, double *layer_ms, double *layer_flops);
 /* Attaches a model to a router (mode 0: none, 1: every run seeded, 2: a seeded
  * run and a plain run, the better total score kept).  Seeding adds alpha x the
  * predicted demand (kind 0) or alpha x the predicted overflow over capacity

@@ -47,7 +47,7 @@ EXPORTS = [
     "igr_steiner",
     "igr_seed_create", "igr_seed_destroy", "igr_seed_last_error", "igr_seed_set_tile", "igr_seed_params",
     "igr_seed_set_params", "igr_seed_features", "igr_seed_add_map", "igr_seed_add_routed", "igr_seed_train",
-    "igr_seed_eval", "igr_seed_predict", "igr_seed_grad", "igr_router_set_seed", "igr_router_seed_stats",
+    "igr_seed_eval", "igr_seed_predict", "igr_seed_time_forward", "igr_seed_grad", "igr_router_set_seed", "igr_router_seed_stats",
     "igr_test_hook",
 ]
 
@@ -145,6 +145,7 @@ def lib() -> C.CDLL:
     L.igr_seed_train.argtypes = [vp, C.c_int, C.c_int, C.c_float, C.c_uint64, C.c_int, vp]
     L.igr_seed_eval.argtypes = [vp, C.c_int, _f64p, C.c_int]
     L.igr_seed_predict.argtypes = [vp, C.c_int, C.c_int, _f32p, _f32p]
+    L.igr_seed_time_forward.argtypes = [vp, C.c_int, C.c_int, _f64p, _f64p]
     L.igr_seed_grad.argtypes = [vp, C.c_int, _f32p, _f32p, C.POINTER(C.c_double), vp]
     L.igr_test_hook.argtypes = [C.c_int, C.c_int64]
     _lib = L
@@ -206,6 +207,7 @@ def generate_custom(X, Y, nets, seed=1, cap_mode=0, block_frac=0.05, pin_mode=0,
 # limits of igr_pattern_route_static (IGR_STATIC_SCRATCH_BYTES, IGR_STATIC_MAX_NETS)
 STATIC_SCRATCH_BYTES = 64 << 20
 STATIC_MAX_NETS = 1 << 20
+SEED_CONVS = 6  # convolutions of the learned seed (IGR_SEED_CONVS)
 
 KERNEL_CLASSES = ["cost_refresh", "pattern_dp", "wire_commit", "via_commit", "dag_dp", "coloring", "ripup",
                   "phase1_graph", "commit_refresh"]
@@ -569,6 +571,16 @@ class Seed:
         out = np.zeros_like(f)
         self._c(lib().igr_seed_predict(self.h, f.shape[0], f.shape[1], f.reshape(-1), out.reshape(-1)))
         return out
+
+    def time_forward(self, tiles: int = 16, reps: int = 5) -> dict:
+        """Device time of the forward convolutions (tcgen05 implicit GEMMs) over
+        `tiles` tiles: per convolution ms per pass and FLOPs per pass, and the
+        whole pass's TFLOP/s (igr_seed_time_forward)."""
+        ms = np.zeros(SEED_CONVS, np.float64)
+        fl = np.zeros(SEED_CONVS, np.float64)
+        self._c(lib().igr_seed_time_forward(self.h, tiles, reps, ms, fl))
+        return dict(layer_ms=ms.tolist(), layer_flops=fl.tolist(),
+                    tflops=float(fl.sum() / (ms.sum() * 1e-3) / 1e12) if ms.sum() > 0 else 0.0)
 
     def grad(self, x, target):
         x = np.ascontiguousarray(x, dtype=np.float32)

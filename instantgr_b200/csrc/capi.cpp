@@ -1007,6 +1007,16 @@ int igr_seed_eval(igr_seed *m, int map, double *out, int n) {
     });
 }
 
+int igr_seed_time_forward(igr_seed *m, int tiles, int reps, double *layer_ms, double *layer_flops) {
+    SEED_GUARD(m, {
+        if (!layer_ms || !layer_flops) throw Error(ERR_INVALID, "null output");
+        static_assert(IGR_SEED_CONVS == kSeedConvs, "convolution count of the header");
+        double f[kSeedConvs];
+        m->m.time_forward(tiles, 1, layer_ms, f);  // untimed first pass (set-up, first launch)
+        m->m.time_forward(tiles, reps, layer_ms, layer_flops);
+    });
+}
+
 int igr_seed_predict(igr_seed *m, int X, int Y, const float *feat, float *pred) {
     SEED_GUARD(m, {
         if (X < 1 || Y < 1 || !feat || !pred) throw Error(ERR_INVALID, "bad map");

@@ -386,24 +386,44 @@ void read_net_buffer(Design &d, const char *buf, size_t n) {
     parallel_for(parts, parts, [&](int b, int e) {
         for (int i = b; i < e; i++) parse_net_chunk(d, buf + cut[i], cut[i + 1] - cut[i], ch[i]);
     });
-    d.name_pool.clear(); d.name_off.assign(1, 0);
-    d.pin_off.assign(1, 0); d.ap_off.assign(1, 0); d.ap.clear();
-    d.bminx.clear(); d.bmaxx.clear(); d.bminy.clear(); d.bmaxy.clear();
-    size_t nn = 0;
-    for (auto &c : ch) nn += c.pins_per_net.size();
-    d.name_off.reserve(nn + 1); d.pin_off.reserve(nn + 1);
-    for (auto &c : ch) {
-        d.name_pool.insert(d.name_pool.end(), c.names.begin(), c.names.end());
-        for (auto len : c.name_len) d.name_off.push_back(d.name_off.back() + len);
-        for (auto np : c.pins_per_net) d.pin_off.push_back(d.pin_off.back() + np);
-        for (auto na : c.aps_per_pin) d.ap_off.push_back(d.ap_off.back() + na);
-        d.ap.insert(d.ap.end(), c.ap.begin(), c.ap.end());
-        for (size_t i = 0; i < c.pins_per_net.size(); i++) {
-            d.bminx.push_back(c.bb[4 * i]); d.bmaxx.push_back(c.bb[4 * i + 1]);
-            d.bminy.push_back(c.bb[4 * i + 2]); d.bmaxy.push_back(c.bb[4 * i + 3]);
-        }
-        c = NetChunk();
+    // the chunks' arrays concatenated: each chunk copies into its own slice
+    struct Base { size_t name = 0, net = 0, pin = 0, ap = 0; };
+    std::vector<Base> base(parts + 1);
+    for (int i = 0; i < parts; i++) {
+        base[i + 1].name = base[i].name + ch[i].names.size();
+        base[i + 1].net = base[i].net + ch[i].pins_per_net.size();
+        base[i + 1].pin = base[i].pin + ch[i].aps_per_pin.size();
+        base[i + 1].ap = base[i].ap + ch[i].ap.size();
     }
+    const Base &tot = base[parts];
+    d.name_pool.resize(tot.name);
+    d.name_off.assign(tot.net + 1, 0);
+    d.pin_off.assign(tot.net + 1, 0);
+    d.ap_off.assign(tot.pin + 1, 0);
+    d.ap.resize(tot.ap);
+    d.bminx.resize(tot.net); d.bmaxx.resize(tot.net); d.bminy.resize(tot.net); d.bmaxy.resize(tot.net);
+    parallel_for(parts, parts, [&](int b, int e) {
+        for (int i = b; i < e; i++) {
+            NetChunk &c = ch[i];
+            const Base &o = base[i];
+            std::copy(c.names.begin(), c.names.end(), d.name_pool.begin() + o.name);
+            int64_t at = (int64_t)o.name, pin = (int64_t)o.pin, ap = (int64_t)o.ap;
+            for (size_t k = 0; k < c.pins_per_net.size(); k++) {
+                at += c.name_len[k];
+                pin += c.pins_per_net[k];
+                d.name_off[o.net + k + 1] = at;
+                d.pin_off[o.net + k + 1] = pin;
+                d.bminx[o.net + k] = c.bb[4 * k]; d.bmaxx[o.net + k] = c.bb[4 * k + 1];
+                d.bminy[o.net + k] = c.bb[4 * k + 2]; d.bmaxy[o.net + k] = c.bb[4 * k + 3];
+            }
+            for (size_t k = 0; k < c.aps_per_pin.size(); k++) {
+                ap += c.aps_per_pin[k];
+                d.ap_off[o.pin + k + 1] = ap;
+            }
+            std::copy(c.ap.begin(), c.ap.end(), d.ap.begin() + o.ap);
+            c = NetChunk();
+        }
+    });
 }
 
 namespace {

@@ -28,21 +28,30 @@ namespace {
 // Tree over the distinct 2-D positions of `pos2d` (my_flute, database_cuda.hpp:696-744).
 void tree_from_positions(const Design &d, int Y, const std::vector<int> &pos2d, TreeAdj &graph,
                          std::pmr::vector<int> &nodes) {
-    std::vector<int> x, y;
-    x.reserve(pos2d.size()); y.reserve(pos2d.size());
+    // containers of one tree, kept per thread
+    struct Scratch {
+        std::vector<int> x, y, parent;
+        igr_steiner::Tree t;
+        std::vector<igr_steiner::Branch> br;
+        std::vector<std::tuple<int, int, int>> edges;
+        std::vector<std::pair<int, int>> kept;
+    };
+    thread_local Scratch sc;
+    std::vector<int> &x = sc.x, &y = sc.y;
+    x.clear(); y.clear();
     for (int e : pos2d) { x.push_back(d.dr_x[e / Y]); y.push_back(d.dr_y[e % Y]); }
     const int cnt = (int)pos2d.size();
-    igr_steiner::Tree t;
+    igr_steiner::Tree &t = sc.t;
     igr_steiner::build(x, y, t);
-    std::vector<igr_steiner::Branch> br;
+    std::vector<igr_steiner::Branch> &br = sc.br;
     igr_steiner::to_branches(x, y, t, br);
     const int nb = 2 * cnt - 2;
     nodes.clear();
     for (int i = 0; i < nb; i++) nodes.push_back(d.dr2gr_x[br[i].x] * Y + d.dr2gr_y[br[i].y]);
     std::sort(nodes.begin(), nodes.end());
     nodes.erase(std::unique(nodes.begin(), nodes.end()), nodes.end());
-    std::vector<std::tuple<int, int, int>> edges;
-    edges.reserve(nb);
+    std::vector<std::tuple<int, int, int>> &edges = sc.edges;
+    edges.clear();
     auto where = [&](int g) { return (int)(std::lower_bound(nodes.begin(), nodes.end(), g) - nodes.begin()); };
     for (int i = 0; i < nb; i++)
         if (br[i].n < nb) {
@@ -53,7 +62,8 @@ void tree_from_positions(const Design &d, int Y, const std::vector<int> &pos2d, 
             edges.emplace_back(std::abs(b1.x - b2.x) + std::abs(b1.y - b2.y), u, v);
         }
     std::sort(edges.begin(), edges.end());
-    std::vector<int> parent(nodes.size());
+    std::vector<int> &parent = sc.parent;
+    parent.resize(nodes.size());
     std::iota(parent.begin(), parent.end(), 0);
     auto find = [&](int v) {
         int r = v;
@@ -61,8 +71,8 @@ void tree_from_positions(const Design &d, int Y, const std::vector<int> &pos2d, 
         while (parent[v] != r) { const int n = parent[v]; parent[v] = r; v = n; }
         return r;
     };
-    std::vector<std::pair<int, int>> kept;
-    kept.reserve(nodes.size());
+    std::vector<std::pair<int, int>> &kept = sc.kept;
+    kept.clear();
     for (auto &e : edges) {
         int u = std::get<1>(e), v = std::get<2>(e), pu = find(u), pv = find(v);
         if (pu != pv) {
@@ -145,20 +155,32 @@ void calc_hpwl(const NetSet &ns, RNet &n) {
 
 void construct_rsmt(const Design &d, const NetSet &ns, RNet &n) {
     const int X = ns.X, Y = ns.Y, XY = X * Y, L = ns.L;
+    if (n.pins.size() == 2 && n.tnode.empty()) {
+        // two pins: the provider's tree is the one edge between them whatever
+        // the input order (FLUTE's degree-2 branches), so the nodes are the two
+        // GCells in ascending order, each the other's neighbour
+        const int a = n.pins[0], b = n.pins[1];
+        if (a % XY == b % XY) throw Error(ERR_STATE, "two pins of a routing net share a 2-D position");
+        const int lo = a % XY < b % XY ? a : b, hi = lo == a ? b : a;
+        n.tnode.assign({lo, hi});
+        n.adj.off.assign({0, 1, 2});
+        n.adj.nb.assign({1, 0});
+        return;
+    }
     // pins are distinct in 2-D (checked below); the layer of each 2-D position
-    std::vector<std::pair<int, int>> layer;
-    layer.reserve(n.pins.size());
-    // the Steiner provider sees the 2-D positions in the iteration order of a
-    // std::unordered_set filled in pin order, as my_flute does
-    // (src/database_cuda.hpp:696-708, 746-756); FLUTE's and the provider's
-    // tie-breaking follow the input order
-    // (no reserve: the bucket count, and with it the order, grows as the reference's does)
-    std::unordered_set<int> pos_set;
+    thread_local std::vector<std::pair<int, int>> layer;
+    thread_local std::vector<int> pos;
+    layer.clear();
+    pos.clear();
+    // my_flute hands FLUTE the 2-D positions in the iteration order of a
+    // std::unordered_set (src/database_cuda.hpp:696-708, 746-756).  The tree
+    // does not depend on that order here: the provider sorts its points, and
+    // tree_from_positions keys every edge by its GCells and sorts the edges
+    // completely, so the positions go in pin order.
     for (int p : n.pins) {
         layer.push_back({p % XY, p / XY});
-        pos_set.insert(p % XY);
+        pos.push_back(p % XY);
     }
-    std::vector<int> pos(pos_set.begin(), pos_set.end());
     std::sort(layer.begin(), layer.end());
     for (size_t i = 1; i < layer.size(); i++)
         if (layer[i].first == layer[i - 1].first)
@@ -182,7 +204,19 @@ void split_net(const Design &d, const NetSet &ns, int db_id, std::vector<RNet> &
     std::pmr::memory_resource *res = std::pmr::get_default_resource();
     const int MAX_PIN_SIZE = 12;
     const int X = ns.X, Y = ns.Y, XY = X * Y, L = ns.L;
-    RNet tmp;
+    // containers of one split, kept per thread
+    struct Scratch {
+        RNet tmp;
+        std::vector<char> not_steiner;
+        std::vector<int> sz, par;
+        std::vector<std::tuple<int, int, int>> edges;
+        std::vector<std::vector<int>> new_pins, net_edge;
+        std::vector<std::pair<int, int>> se;
+    };
+    thread_local Scratch sc;
+    RNet &tmp = sc.tmp;
+    tmp.pins.clear();
+    tmp.tnode.clear();
     for (int64_t i = d.sel_off[db_id]; i < d.sel_off[db_id + 1]; i++) {
         int p = d.sel[i];
         tmp.pins.push_back(p >= XY ? p - XY : p);
@@ -191,11 +225,14 @@ void split_net(const Design &d, const NetSet &ns, int db_id, std::vector<RNet> &
     construct_rsmt(d, ns, tmp);
     const auto &tn = tmp.tnode;
     const int n = (int)tn.size();
-    std::vector<char> not_steiner(n);
+    std::vector<char> &not_steiner = sc.not_steiner;
+    not_steiner.resize(n);
     for (int i = 0; i < n; i++) not_steiner[i] = tn[i] < L * XY;
-    std::vector<int> sz(n, 1), par(n);
-    std::vector<std::tuple<int, int, int>> edges;
-    edges.reserve(n);
+    std::vector<int> &sz = sc.sz, &par = sc.par;
+    sz.assign(n, 1);
+    par.resize(n);
+    std::vector<std::tuple<int, int, int>> &edges = sc.edges;
+    edges.clear();
     auto find = [&](int v) {
         int r = v;
         while (par[r] != r) r = par[r];
@@ -221,7 +258,15 @@ void split_net(const Design &d, const NetSet &ns, int db_id, std::vector<RNet> &
         par[u] = v;
         sz[v] += sz[u];
     }
-    std::vector<std::vector<int>> new_pins(n), net_edge(n);
+    std::vector<std::vector<int>> &new_pins = sc.new_pins, &net_edge = sc.net_edge;
+    if ((int)new_pins.size() < n) {
+        new_pins.resize(n);
+        net_edge.resize(n);
+    }
+    for (int i = 0; i < n; i++) {
+        new_pins[i].clear();
+        net_edge[i].clear();
+    }
     for (int i = 0; i < n; i++) new_pins[find(i)].push_back(tn[i]);
     for (int i = 0; i < (int)edges.size(); i++) {
         auto &e = edges[i];
@@ -239,21 +284,26 @@ void split_net(const Design &d, const NetSet &ns, int db_id, std::vector<RNet> &
         if (find(i) != i) continue;
         RNet s(res);
         s.orig = db_id;
-        std::unordered_map<int, int> indx;
-        for (int j = 0; j < (int)new_pins[i].size(); j++) {
-            if (new_pins[i][j] < L * XY) s.pins.push_back(new_pins[i][j]);
-            indx[new_pins[i][j]] = j;
-        }
-        s.tnode.assign(new_pins[i].begin(), new_pins[i].end());
-        std::vector<std::pair<int, int>> se;
-        se.reserve(net_edge[i].size());
+        const std::vector<int> &np = new_pins[i];
+        for (int j = 0; j < (int)np.size(); j++)
+            if (np[j] < L * XY) s.pins.push_back(np[j]);
+        // index of a node in the subnet: its last position in np (a map filled
+        // in order keeps the last)
+        auto index_of = [&](int v) {
+            for (int j = (int)np.size() - 1; j >= 0; j--)
+                if (np[j] == v) return j;
+            return 0;  // every edge end is in np
+        };
+        s.tnode.assign(np.begin(), np.end());
+        std::vector<std::pair<int, int>> &se = sc.se;
+        se.clear();
         for (int j : net_edge[i]) {
             auto &e = edges[j];
             int u = std::get<0>(e), v = std::get<1>(e);
             if (find(v) == i) std::swap(u, v);
-            se.push_back({indx[tn[u]], indx[tn[v]]});
+            se.push_back({index_of(tn[u]), index_of(tn[v])});
         }
-        s.adj.from_edges((int)new_pins[i].size(), se);
+        s.adj.from_edges((int)np.size(), se);
         out.push_back(std::move(s));
     }
 }

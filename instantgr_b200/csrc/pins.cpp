@@ -23,22 +23,98 @@
 #include "robin_order.hpp"
 
 #include <algorithm>
-#include <unordered_map>
+#include <cstdint>
 
 namespace igr {
 
 namespace {
 
+// Map of one net's non-negative keys to values (open addressing, linear
+// probing); reset() empties it for the next net by a generation stamp.
+class KeyIndex {
+public:
+    void reset(size_t expected) {
+        size_t cap = 16;
+        while (cap < 2 * expected) cap <<= 1;
+        if (keys_.size() < cap) {
+            keys_.assign(cap, 0);
+            vals_.assign(cap, 0);
+            gen_.assign(cap, 0);
+            cur_ = 0;
+        }
+        mask_ = cap - 1;
+        if (++cur_ == 0) {
+            std::fill(gen_.begin(), gen_.end(), 0u);
+            cur_ = 1;
+        }
+    }
+    // value of `key`, inserting `val` when absent
+    int find_or_insert(int key, int val) {
+        for (size_t h = slot(key);; h = (h + 1) & mask_) {
+            if (gen_[h] != cur_) {
+                gen_[h] = cur_;
+                keys_[h] = key;
+                vals_[h] = val;
+                return val;
+            }
+            if (keys_[h] == key) return vals_[h];
+        }
+    }
+    int find(int key) const {
+        for (size_t h = slot(key);; h = (h + 1) & mask_) {
+            if (gen_[h] != cur_) return -1;
+            if (keys_[h] == key) return vals_[h];
+        }
+    }
+
+private:
+    std::vector<int> keys_, vals_;
+    std::vector<uint32_t> gen_;
+    uint32_t cur_ = 0;
+    size_t mask_ = 0;
+    size_t slot(int key) const { return (size_t)(((uint64_t)(uint32_t)key * 0x9E3779B97F4A7C15ull) >> 40) & mask_; }
+};
+
+// Counts per grid column or row for one net at a time (a stamp per entry
+// marks the counts of the current net).
+struct StampedCounts {
+    std::vector<int> val;
+    std::vector<uint32_t> st;
+    uint32_t cur = 0;
+    void next(int n) {
+        if ((int)val.size() < n) {
+            val.assign(n, 0);
+            st.assign(n, 0);
+            cur = 0;
+        }
+        if (++cur == 0) {
+            std::fill(st.begin(), st.end(), 0u);
+            cur = 1;
+        }
+    }
+    int get(int k) const { return st[k] == cur ? val[k] : 0; }
+    void inc(int k) {
+        if (st[k] != cur) { st[k] = cur; val[k] = 0; }
+        val[k]++;
+    }
+};
+
 struct PinScratch {
     std::vector<int> idx, best;
-    std::unordered_map<int, std::vector<int>> cnt2d;
-    std::unordered_map<int, int> xcnt, ycnt;
     std::vector<char> visited;
     std::vector<int> p, p2;
     std::vector<int> order;        // walk order of the pins in the greedy rounds
     RobinOrder keys2d, walk, rp, rp2;
-    std::vector<int> first2d;            // 2-D keys in first-seen order; pins per key (CSR below)
-    std::vector<int> list_off, list_pin;
+    std::vector<int> first2d;      // 2-D keys of the access points in first-seen order
+    KeyIndex rank;                 // 2-D key -> its index in first2d
+    std::vector<int> ap_rank;      // per access point of the net (pin-major): rank of its 2-D key
+    std::vector<int> list_off, list_pin;  // pins per 2-D key (CSR by rank, push order)
+    std::vector<int> cnt;          // running count per 2-D key in the current round
+    std::vector<uint32_t> cnt_st;  // round stamp of cnt
+    uint32_t round_st = 0;
+    std::vector<int> lst;          // pins at the chosen key in a round
+    std::vector<int> mn, mx;       // lowest / highest chosen position per 2-D key
+    StampedCounts xcnt, ycnt;
 };
 
 void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, std::vector<int> &extra) {
@@ -51,11 +127,11 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
     std::vector<int> &p = s.p, &p2 = s.p2;  // chosen 3-D positions, chosen 2-D positions
     p.clear(); p2.clear();
     s.rp.reset(); s.rp2.reset();  // net::init's sets are declared anew for every net
-    auto has2 = [&](int v) { return std::find(p2.begin(), p2.end(), v) != p2.end(); };
-    // the reference's robin_hood sets p and p2D (their insertion sequences)
+    // the reference's robin_hood sets p and p2D (their insertion sequences);
+    // p and p2 hold their elements in first-insertion order
+    auto has2 = [&](int v) { return s.rp2.contains(v); };
     auto add3 = [&](int v) {
-        if (std::find(p.begin(), p.end(), v) == p.end()) p.push_back(v);
-        s.rp.insert(v);
+        if (s.rp.insert(v)) p.push_back(v);
     };
     auto add2 = [&](int v) {
         p2.push_back(v);
@@ -101,11 +177,10 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
         }
     } else {
         s.visited.assign(num, 0);
-        s.xcnt.clear(); s.ycnt.clear();
-        auto cnt_of = [](std::unordered_map<int, int> &m, int k) {
-            auto it = m.find(k);
-            return it == m.end() ? 0 : it->second;
-        };
+        s.xcnt.next(X);
+        s.ycnt.next(Y);
+        const int64_t a0 = d.ap_off[pb];
+        const int A = (int)(d.ap_off[pb + num] - a0);
         // walk order (src/database.hpp:101-117): the 2-D keys of all access
         // points enter a robin_hood map in first-seen order, each with the pins
         // that have an access point there (ascending); the pins of every key, in
@@ -113,63 +188,80 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
         // every round then follows
         s.keys2d.reset();
         s.first2d.clear();
+        s.rank.reset((size_t)A);
+        s.ap_rank.resize(A);
         for (int i = 0; i < num; i++)
             for (int j = 0; j < nap(i); j++) {
                 const int q = apv(i, j) % XY;
-                if (s.keys2d.insert(q)) s.first2d.push_back(q);
+                const int r = s.rank.find_or_insert(q, (int)s.first2d.size());
+                if (r == (int)s.first2d.size()) {
+                    s.first2d.push_back(q);
+                    s.keys2d.insert(q);
+                }
+                s.ap_rank[d.ap_off[pb + i] - a0 + j] = r;
             }
+        const int K = (int)s.first2d.size();
+        // pins per 2-D key in push order (i ascending, then j): a counting sort
+        s.list_off.assign(K + 1, 0);
+        for (int a = 0; a < A; a++) s.list_off[s.ap_rank[a] + 1]++;
+        for (int r = 0; r < K; r++) s.list_off[r + 1] += s.list_off[r];
+        s.list_pin.resize(A);
         {
-            // pins per 2-D key, in push order (i ascending, then j)
-            std::vector<std::pair<int, int>> kp;  // (key rank in first2d, pin)
-            std::unordered_map<int, int> rank;
-            for (size_t r = 0; r < s.first2d.size(); r++) rank[s.first2d[r]] = (int)r;
+            std::vector<int> &fill = s.cnt;  // write cursors
+            fill.assign(s.list_off.begin(), s.list_off.end() - 1);
             for (int i = 0; i < num; i++)
-                for (int j = 0; j < nap(i); j++) kp.push_back({rank[apv(i, j) % XY], i});
-            std::stable_sort(kp.begin(), kp.end(),
-                             [](const std::pair<int, int> &a, const std::pair<int, int> &b) { return a.first < b.first; });
-            s.list_off.assign(s.first2d.size() + 1, 0);
-            s.list_pin.clear();
-            for (auto &e : kp) {
-                s.list_off[e.first + 1]++;
-                s.list_pin.push_back(e.second);
-            }
-            for (size_t r = 0; r < s.first2d.size(); r++) s.list_off[r + 1] += s.list_off[r];
-            s.walk.reset();
-            s.keys2d.for_each([&](int q) {
-                const int r = rank[q];
-                for (int t = s.list_off[r]; t < s.list_off[r + 1]; t++) s.walk.insert(s.list_pin[t]);
-            });
-            s.order.clear();
-            s.walk.for_each([&](int i) { s.order.push_back(i); });
+                for (int j = 0; j < nap(i); j++) s.list_pin[fill[s.ap_rank[d.ap_off[pb + i] - a0 + j]]++] = i;
         }
+        s.walk.reset();
+        s.keys2d.for_each([&](int q) {
+            const int r = s.rank.find(q);
+            for (int t = s.list_off[r]; t < s.list_off[r + 1]; t++) s.walk.insert(s.list_pin[t]);
+        });
+        s.order.clear();
+        s.walk.for_each([&](int i) { s.order.push_back(i); });
+        s.cnt.assign(K, 0);
+        s.cnt_st.assign(K, 0);
+        s.round_st = 0;
         for (int round = 0; round < num; round++) {
-            int max_pos = -1, cnt_repeat = 0, max_coord = -1, min_dist = 1000000000;
-            s.cnt2d.clear();
+            int max_pos = -1, max_rank = -1, cnt_repeat = 0, max_coord = -1, min_dist = 1000000000;
+            ++s.round_st;  // every key's running count starts at zero
             for (int i : s.order) {
                 if (s.visited[i]) continue;
+                const int *rk = s.ap_rank.data() + (d.ap_off[pb + i] - a0);
                 for (int j = 0; j < nap(i); j++) {
-                    int q = apv(i, j) % XY;
-                    auto &lst = s.cnt2d[q];
-                    lst.push_back(i);
+                    const int r = rk[j], q = s.first2d[r];
+                    if (s.cnt_st[r] != s.round_st) {
+                        s.cnt_st[r] = s.round_st;
+                        s.cnt[r] = 0;
+                    }
+                    const int sz = ++s.cnt[r];
                     int dist = std::abs(q / Y * 2 - c2x) + std::abs(q % Y * 2 - c2y);
-                    int coord = cnt_of(s.xcnt, q / Y) + cnt_of(s.ycnt, q % Y);
-                    int sz = (int)lst.size();
+                    int coord = s.xcnt.get(q / Y) + s.ycnt.get(q % Y);
                     if (sz > cnt_repeat) {
-                        max_pos = q; cnt_repeat = sz; max_coord = coord; min_dist = dist;
+                        max_pos = q; max_rank = r; cnt_repeat = sz; max_coord = coord; min_dist = dist;
                     } else if (sz == cnt_repeat && coord > max_coord) {
-                        max_pos = q; max_coord = coord; min_dist = dist;
+                        max_pos = q; max_rank = r; max_coord = coord; min_dist = dist;
                     } else if (sz == cnt_repeat && coord == max_coord && dist < min_dist) {
-                        max_pos = q; min_dist = dist;
+                        max_pos = q; max_rank = r; min_dist = dist;
                     }
                 }
             }
             if (cnt_repeat <= 1) break;
             if (!has2(max_pos)) {
                 add2(max_pos);
-                s.xcnt[max_pos / Y % X]++;
-                s.ycnt[max_pos % Y]++;
+                s.xcnt.inc(max_pos / Y % X);
+                s.ycnt.inc(max_pos % Y);
             }
-            for (int pin : s.cnt2d[max_pos]) {
+            // the pins that had an access point at max_pos this round, in the
+            // order of the walk (a pin twice when two of its points are there)
+            s.lst.clear();
+            for (int i : s.order) {
+                if (s.visited[i]) continue;
+                const int *rk = s.ap_rank.data() + (d.ap_off[pb + i] - a0);
+                for (int j = 0; j < nap(i); j++)
+                    if (rk[j] == max_rank) s.lst.push_back(i);
+            }
+            for (int pin : s.lst) {
                 if (s.visited[pin]) throw Error(ERR_FORMAT, "a pin has two access points on one 2-D position");
                 s.visited[pin] = 1;
                 for (int j = 0; j < nap(pin); j++)
@@ -185,7 +277,7 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
             for (int j = 0; j < nap(i); j++) {
                 int v = apv(i, j), q = v % XY;
                 int dist = std::abs(v / Y % X * 2 - c2x) + std::abs(v % Y * 2 - c2y);
-                int coord = cnt_of(s.xcnt, q / Y) + cnt_of(s.ycnt, q % Y);
+                int coord = s.xcnt.get(q / Y) + s.ycnt.get(q % Y);
                 if (coord > max_overlap) { max_overlap = coord; min_dist = dist; chosen = v; }
                 else if (coord == max_overlap && dist < min_dist) { min_dist = dist; chosen = v; }
             }
@@ -193,10 +285,28 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
             add3(chosen);
             if (!has2(chosen % XY)) {
                 add2(chosen % XY);
-                s.xcnt[chosen / Y % X]++;
-                s.ycnt[chosen % Y]++;
+                s.xcnt.inc(chosen / Y % X);
+                s.ycnt.inc(chosen % Y);
             }
         }
+        if (p2.size() < p.size()) {
+            // stacked pins: per 2-D key the lowest and highest chosen position
+            s.mn.assign(K, -1);
+            s.mx.assign(K, -1);
+            for (int v : p) {
+                const int r = s.rank.find(v % XY);
+                if (s.mn[r] < 0 || v < s.mn[r]) s.mn[r] = v;
+                if (s.mx[r] < 0 || v > s.mx[r]) s.mx[r] = v;
+            }
+            s.rp2.for_each([&](int q) {
+                const int r = s.rank.find(q);
+                pins.push_back(s.mx[r]);
+                if (s.mn[r] != s.mx[r]) { extra.push_back(s.mn[r]); extra.push_back(s.mx[r]); }
+            });
+        } else {
+            s.rp.for_each([&](int v) { pins.push_back(v); });
+        }
+        return;
     }
     // output in the iteration order of the reference's sets (src/database.hpp:225-242)
     if (p2.size() < p.size()) {
@@ -220,12 +330,14 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
 void select_pins(Design &d, int threads) {
     const int N = d.num_nets();
     if (threads <= 0) threads = hw_threads();
-    int T = std::max(1, std::min(threads, N / 256 + 1));
+    // ranges of nets, many per thread and handed out dynamically: a few nets
+    // of hundreds of pins cost as much as thousands of two-pin nets
+    int T = std::max(1, std::min(threads * 32, N / 256 + 1));
     std::vector<std::vector<int>> pins(T), extra(T);
     std::vector<std::vector<int64_t>> pcount(T), ecount(T);
     std::vector<int> lo(T + 1);
     for (int t = 0; t <= T; t++) lo[t] = (int)((int64_t)N * t / T);
-    parallel_for(T, T, [&](int b, int e) {
+    parallel_for(T, threads, [&](int b, int e) {
         PinScratch s;
         for (int t = b; t < e; t++)
             for (int n = lo[t]; n < lo[t + 1]; n++) {

@@ -287,7 +287,6 @@ Router::~Router() {
 
 void Router::open(const char *cap, const char *net) {
     const double t0 = now_s();
-    hpwl_keys.clear();
     // The CUDA driver, the caller's device context and the routing grid are
     // brought up on a side thread while the host parses and builds trees (the
     // first CUDA call of a process can take a second).  The device is the
@@ -365,10 +364,22 @@ void Router::open(const char *cap, const char *net) {
     route_cap1 = route_cap;
     dp_bytes = (double)dpb;
     // phase-1 routing priority: HPWL, largest first (Lshape_route.hpp:170-172),
-    // with the reference's (unstable) std::sort and comparator
-    order1.resize(R);
-    std::iota(order1.begin(), order1.end(), 0);
-    std::sort(order1.begin(), order1.end(), [&](int l, int r) { return ns.nets[l].hpwl > ns.nets[r].hpwl; });
+    // with the reference's (unstable) std::sort and comparator: (key, id)
+    // pairs compared on the key alone take the same sequence of comparisons
+    // and moves, hence give the same order, as the ids compared through the
+    // nets; the keys stay for the rip-up order of the reroute passes
+    hpwl_keys.resize(R);
+    parallel_for(R, threads, [&](int b, int e) {
+        for (int i = b; i < e; i++) hpwl_keys[i] = ns.nets[i].hpwl;
+    });
+    {
+        std::vector<std::pair<int, int>> kv(R);
+        for (int i = 0; i < R; i++) kv[i] = {hpwl_keys[i], i};
+        std::sort(kv.begin(), kv.end(),
+                  [](const std::pair<int, int> &l, const std::pair<int, int> &r) { return l.first > r.first; });
+        order1.resize(R);
+        for (int i = 0; i < R; i++) order1[i] = kv[i].second;
+    }
     if (verbose)
         std::fprintf(stderr, "[igr] read+trees %.2fs (read %.3f, pins+trees %.3f, layout %.3f): %d nets, %d routing nets\n",
                      now_s() - t0, t_read - t0, t_nets - t_read, now_s() - t_nets, d.num_nets(), R);
@@ -1119,13 +1130,8 @@ bool Router::rrr_pass(int iter) {
     } else {
         // the comparisons of the reference's sort (Lshape_route_detour.hpp:732-734):
         // (key, id) pairs compared on the key alone give the same sequence of
-        // comparisons, hence the same order, as the ids compared through a key table
-        if ((int)hpwl_keys.size() != R) {  // the trees (and their HPWL) are fixed after open
-            hpwl_keys.resize(R);
-            parallel_for(R, threads, [&](int b, int e) {
-                for (int i = b; i < e; i++) hpwl_keys[i] = ns.nets[i].hpwl;
-            });
-        }
+        // comparisons, hence the same order, as the ids compared through a key
+        // table (the HPWL of every routing net, kept since open)
         std::vector<std::pair<int, int>> kv(of_nets.size());
         for (size_t k = 0; k < of_nets.size(); k++) kv[k] = {hpwl_keys[of_nets[k]], of_nets[k]};
         std::sort(kv.begin(), kv.end(),

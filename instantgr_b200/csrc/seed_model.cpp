@@ -166,6 +166,37 @@ void SeedModel::forward(int T) {
     }
 }
 
+void SeedModel::time_forward(int T, int reps, double *layer_ms, double *layer_flops) {
+    if (T < 1 || reps < 1) throw Error(ERR_INVALID, "tiles and repetitions must be positive");
+    ensure(T);
+    cudaEvent_t ev[kSeedConvs + 1];
+    for (auto &e : ev) cuda_check(cudaEventCreate(&e), "event");
+    double ms[kSeedConvs] = {0};
+    for (int r = 0; r < reps; r++) {
+        const __nv_bfloat16 *in = x0.p;
+        cuda_check(cudaEventRecord(ev[0], s), "event");
+        for (int i = 0; i < kSeedConvs; i++) {
+            const bool last = i == kSeedConvs - 1;
+            launch_conv_fwd(spec[i], T, in, W[i].p, bias[i].p, last ? y16.p : act[i].p, last ? y32.p : nullptr,
+                            err.p, s);
+            if (!last) in = act[i].p;
+            cuda_check(cudaEventRecord(ev[i + 1], s), "event");
+        }
+        cuda_check(cudaEventSynchronize(ev[kSeedConvs]), "sync");
+        for (int i = 0; i < kSeedConvs; i++) {
+            float t = 0;
+            cuda_check(cudaEventElapsedTime(&t, ev[i], ev[i + 1]), "event time");
+            ms[i] += t;
+        }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    check("timed forward");
+    for (int i = 0; i < kSeedConvs; i++) {
+        layer_ms[i] = ms[i] / reps;
+        layer_flops[i] = 2.0 * T * spec[i].hout * spec[i].wout * 9.0 * spec[i].cin * spec[i].cout;
+    }
+}
+
 double SeedModel::backward(int T, double *mae) {
     cuda_check(cudaMemsetAsync(sums.p, 0, 2 * sizeof(double), s), "memset");
     launch_seed_loss(T, S, halo, y32.p, tgt32.p, grad[5].p, sums.p, s);

@@ -36,6 +36,10 @@ struct SeedModel {
     void set_params(const float *p, size_t n);
     void ensure(int T);
     void forward(int T);              // x0 -> y32
+    // device time of `reps` forward passes over T tiles, per convolution
+    // (ms per pass, CUDA events on the model's stream) and its multiply-add
+    // FLOPs per pass (2 x output pixels x 9 x cin x cout)
+    void time_forward(int T, int reps, double *layer_ms, double *layer_flops);
     double backward(int T, double *mae);  // loss of y32 vs tgt32 and every gradient
     void adam(float lr);
     void grads(std::vector<float> &out);  // dW (as [cout][9][cin]) and db of each layer

@@ -39,10 +39,42 @@ struct Tree {
 
 inline int med3(int a, int b, int c) { return std::max(std::min(a, b), std::min(std::max(a, b), c)); }
 
+// Containers of one build, kept per thread so that the small trees of most
+// nets allocate nothing.
+struct BuildScratch {
+    std::vector<std::pair<int, int>> pts;
+    std::vector<std::vector<int>> adj;  // only the first `used` lists are live
+    size_t used = 0;
+    std::vector<int> sn, nid, nx, ny;
+    std::vector<long long> key;
+    std::vector<int> from, out, touched, clean;
+    std::unordered_map<int64_t, int> at;
+    // n empty adjacency lists
+    void lists(size_t n) {
+        for (size_t v = 0; v < std::min(n, adj.size()); v++) adj[v].clear();
+        if (adj.size() < n) adj.resize(n);
+        used = n;
+    }
+    void add_list() {
+        if (adj.size() <= used) adj.emplace_back();
+        adj[used++].clear();
+    }
+};
+
+inline BuildScratch &build_scratch() {
+    thread_local BuildScratch s;
+    return s;
+}
+
 inline void build(const std::vector<int> &xin, const std::vector<int> &yin, Tree &t) {
-    t = Tree();
+    t.x.clear();
+    t.y.clear();
+    t.edges.clear();
+    t.npins = 0;
+    BuildScratch &bs = build_scratch();
     const int n0 = (int)xin.size();
-    std::vector<std::pair<int, int>> pts(n0);
+    std::vector<std::pair<int, int>> &pts = bs.pts;
+    pts.resize(n0);
     for (int i = 0; i < n0; i++) pts[i] = {xin[i], yin[i]};
     std::sort(pts.begin(), pts.end());
     pts.erase(std::unique(pts.begin(), pts.end()), pts.end());
@@ -60,33 +92,50 @@ inline void build(const std::vector<int> &xin, const std::vector<int> &yin, Tree
         for (int i = 0; i < 3; i++) if (i != c) t.edges.push_back({std::min(i, c), std::max(i, c)});
         return;
     }
-    // ---- minimum spanning tree under the edge order (length, lo, hi).  The
-    // order is strict, so the tree is unique: Prim over all pairs up to 64
-    // points; above, Kruskal over the sweep candidates (which contain it).
-    std::vector<std::vector<int>> adj(P);
-    if (P <= 64) {
-        // Prim: key of the best edge from the tree to each outside point
-        long long key[64];
-        int from[64];
-        bool in[64];
-        auto ek = [&](int a, int b) {  // (length, lo, hi) as one integer: lengths < 2^31, ids < 64
+    // ---- spanning tree: up to kPrimMax points the minimum spanning tree
+    // under the strict edge order (length, lo, hi), by Prim over all pairs;
+    // above, Kruskal in that order over the sweep candidates (a minimum
+    // spanning tree, which can settle ties of length otherwise).  Nothing
+    // below depends on the order of a node's neighbour list.
+    bs.lists(P);
+    std::vector<std::vector<int>> &adj = bs.adj;
+    constexpr int kPrimMax = 64;  // (ids fit the 10 bits of the edge key)
+    if (P <= kPrimMax) {
+        // Prim: key of the best edge from the tree to each outside point, as
+        // (length, lo, hi) in one integer (lengths < 2^31)
+        std::vector<long long> &key = bs.key;
+        std::vector<int> &from = bs.from, &out = bs.out;
+        key.resize(P);
+        from.resize(P);
+        out.resize(P);
+        const int *xs = t.x.data(), *ys = t.y.data();
+        auto ek = [&](int a, int b) {
             const int lo = a < b ? a : b, hi = a < b ? b : a;
-            return ((long long)dist(a, b) << 12) | (lo << 6) | hi;
+            const long long w = std::abs(xs[a] - xs[b]) + std::abs(ys[a] - ys[b]);
+            return (w << 20) | ((long long)lo << 10) | hi;
         };
-        for (int i = 0; i < P; i++) { key[i] = ek(0, i); from[i] = 0; in[i] = false; }
-        in[0] = true;
-        for (int k = 1; k < P; k++) {
-            int best = -1;
-            for (int i = 0; i < P; i++)
-                if (!in[i] && (best < 0 || key[i] < key[best])) best = i;
-            in[best] = true;
+        // points still outside the tree, compacted as they join; the scan
+        // that lowers their keys also finds the next point to join
+        int nout = P - 1, bi = 0;
+        for (int i = 1; i < P; i++) {
+            key[i] = ek(0, i);
+            from[i] = 0;
+            out[i - 1] = i;
+            if (key[i] < key[out[bi]]) bi = i - 1;
+        }
+        while (nout > 0) {
+            const int best = out[bi];
+            out[bi] = out[--nout];
             adj[from[best]].push_back(best);
             adj[best].push_back(from[best]);
-            for (int i = 0; i < P; i++)
-                if (!in[i]) {
-                    const long long q = ek(best, i);
-                    if (q < key[i]) { key[i] = q; from[i] = best; }
-                }
+            bi = 0;
+            long long bk = LLONG_MAX;
+            for (int k = 0; k < nout; k++) {
+                const int i = out[k];
+                const long long q = ek(best, i);
+                if (q < key[i]) { key[i] = q; from[i] = best; }
+                if (key[i] < bk) { bk = key[i]; bi = k; }
+            }
         }
     } else {
         // candidate edges as keys length << 32 | lo << 16 | hi (points < 2^16)
@@ -162,21 +211,47 @@ inline void build(const std::vector<int> &xin, const std::vector<int> &yin, Tree
             if (++used == P - 1) break;
         }
     }
-    // ---- Steinerisation
-    std::unordered_map<int64_t, int> at;
-    at.reserve((size_t)2 * P);
+    // ---- Steinerisation.  The node at a position: a scan over the nodes for
+    // small trees, a hash map above (positions are distinct: the pins are, and
+    // a Steiner point is only made where no node is)
+    const bool scan = P <= 64;  // (independent of the MST method)
+    std::unordered_map<int64_t, int> &at = bs.at;
     auto key = [](int x, int y) { return ((int64_t)x << 32) ^ (uint32_t)y; };
-    for (int i = 0; i < P; i++) at[key(t.x[i], t.y[i])] = i;
+    if (!scan) {
+        at.clear();
+        at.reserve((size_t)2 * P);
+        for (int i = 0; i < P; i++) at[key(t.x[i], t.y[i])] = i;
+    }
+    auto node_at_pos = [&](int x, int y) {
+        if (!scan) {
+            auto it = at.find(key(x, y));
+            return it == at.end() ? -1 : it->second;
+        }
+        for (int v = 0; v < (int)t.x.size(); v++)
+            if (t.x[v] == x && t.y[v] == y) return v;
+        return -1;
+    };
     auto drop = [&](int u, int v) {
         auto &a = adj[u];
         a.erase(std::find(a.begin(), a.end(), v));
     };
-    std::vector<int> sn;
+    std::vector<int> &sn = bs.sn;
+    // a node evaluated without a saving is skipped until its neighbour list
+    // changes: the positions never move, so its best saving stays <= 0
+    std::vector<int> &touched = bs.touched, &clean = bs.clean;
+    touched.assign(bs.used, 0);
+    clean.assign(bs.used, -1);
+    int tick = 0;
+    auto touch = [&](int v) {
+        if ((int)touched.size() <= v) { touched.resize(v + 1, 0); clean.resize(v + 1, -1); }
+        touched[v] = ++tick;
+    };
     for (int pass = 0; pass < 4; pass++) {
         bool changed = false;
-        for (int v = 0; v < (int)adj.size(); v++) {
+        for (int v = 0; v < (int)bs.used; v++) {
             auto &nb = adj[v];
             if (nb.size() < 2) continue;
+            if (clean[v] >= touched[v]) continue;
             sn.assign(nb.begin(), nb.end());
             std::sort(sn.begin(), sn.end());
             int best_gain = 0, ba = -1, bb = -1, bx = 0, by = 0;
@@ -189,23 +264,26 @@ inline void build(const std::vector<int> &xin, const std::vector<int> &yin, Tree
                              std::abs(sy - t.y[a]) + std::abs(sx - t.x[b]) + std::abs(sy - t.y[b]));
                     if (g > best_gain) { best_gain = g; ba = a; bb = b; bx = sx; by = sy; }
                 }
-            if (best_gain <= 0) continue;
-            auto it = at.find(key(bx, by));
-            int s;
-            if (it != at.end()) {
-                s = it->second;
+            if (best_gain <= 0) {
+                clean[v] = tick;
+                continue;
+            }
+            int s = node_at_pos(bx, by);
+            if (s >= 0) {
                 if (s != ba && s != bb) continue;  // would merge with an unrelated node
                 // s coincides with a neighbour: reattach the other neighbour to it
                 int o = (s == ba) ? bb : ba;
                 drop(v, o); drop(o, v);
                 adj[s].push_back(o); adj[o].push_back(s);
+                touch(v); touch(o); touch(s);
             } else {
                 s = (int)t.x.size();
                 t.x.push_back(bx); t.y.push_back(by);
-                adj.emplace_back();
-                at[key(bx, by)] = s;
+                bs.add_list();
+                if (!scan) at[key(bx, by)] = s;
                 drop(v, ba); drop(ba, v); drop(v, bb); drop(bb, v);
                 for (int w : {v, ba, bb}) { adj[s].push_back(w); adj[w].push_back(s); }
+                touch(v); touch(ba); touch(bb); touch(s);
             }
             changed = true;
         }
@@ -215,7 +293,7 @@ inline void build(const std::vector<int> &xin, const std::vector<int> &yin, Tree
     bool again = true;
     while (again) {
         again = false;
-        for (int s = P; s < (int)adj.size(); s++) {
+        for (int s = P; s < (int)bs.used; s++) {
             if (adj[s].size() == 1) {
                 int a = adj[s][0];
                 drop(a, s); adj[s].clear(); again = true;
@@ -228,19 +306,23 @@ inline void build(const std::vector<int> &xin, const std::vector<int> &yin, Tree
         }
     }
     // compact node ids (drop emptied Steiner points)
-    std::vector<int> nid(adj.size(), -1);
+    const int V = (int)bs.used;
+    std::vector<int> &nid = bs.nid;
+    nid.assign(V, -1);
     int k = 0;
-    for (int v = 0; v < (int)adj.size(); v++)
+    for (int v = 0; v < V; v++)
         if (v < P || !adj[v].empty()) nid[v] = k++;
-    std::vector<int> nx(k), ny(k);
-    for (int v = 0; v < (int)adj.size(); v++)
+    std::vector<int> &nx = bs.nx, &ny = bs.ny;
+    nx.resize(k);
+    ny.resize(k);
+    for (int v = 0; v < V; v++)
         if (nid[v] >= 0) { nx[nid[v]] = t.x[v]; ny[nid[v]] = t.y[v]; }
-    for (int v = 0; v < (int)adj.size(); v++)
+    for (int v = 0; v < V; v++)
         for (int w : adj[v])
             if (v < w) t.edges.push_back({nid[v], nid[w]});
     std::sort(t.edges.begin(), t.edges.end());
-    t.x.swap(nx);
-    t.y.swap(ny);
+    t.x.assign(nx.begin(), nx.end());
+    t.y.assign(ny.begin(), ny.end());
 }
 
 // FLUTE-style branch list for d input points (d >= 2): 2d-2 branches, branch i
@@ -256,16 +338,26 @@ inline void to_branches(const std::vector<int> &xin, const std::vector<int> &yin
     br.assign(std::max(0, 2 * d - 2), Branch{0, 0, 0});
     if (d < 2) return;
     const int V = (int)t.x.size();
-    std::vector<std::vector<int>> adj(V);
+    struct Scratch {
+        std::vector<std::vector<int>> adj;
+        std::vector<int> par, order, bidx;
+    };
+    thread_local Scratch ts;
+    std::vector<std::vector<int>> &adj = ts.adj;
+    if ((int)adj.size() < V) adj.resize(V);
+    for (int v = 0; v < V; v++) adj[v].clear();
     for (auto &e : t.edges) { adj[e.first].push_back(e.second); adj[e.second].push_back(e.first); }
-    std::vector<int> par(V, -1), order;
+    std::vector<int> &par = ts.par, &order = ts.order;
+    par.assign(V, -1);
+    order.clear();
     order.push_back(0);
     par[0] = 0;
     for (size_t i = 0; i < order.size(); i++)
         for (int w : adj[order[i]])
             if (par[w] < 0) { par[w] = order[i]; order.push_back(w); }
     // branch index of each tree node: first input point at that position, or a Steiner slot
-    std::vector<int> bidx(V, -1);
+    std::vector<int> &bidx = ts.bidx;
+    bidx.assign(V, -1);
     // tree node of each input point: the pins come first in (x, y) order, distinct
     auto node_at = [&](int x, int y) {
         int lo = 0, hi = t.npins;
