@@ -40,6 +40,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 GEN_BIN = os.path.join(ROOT, "instantgr_b200", "bin", "igr_generate")
@@ -73,6 +75,10 @@ def parse():
                     help="route --warmup + --steps times and print the router statistics (profiling runs)")
     ap.add_argument("--form", default="plain", choices=["plain", "batched", "learned"],
                     help="router form of --route-only")
+    ap.add_argument("--micro", choices=["refresh", "seed"],
+                    help="kernel cases for profiling: cost refresh on a seeded 1600x1600x9 grid (every track "
+                         "dirty, none, a sixth, every track), or the learned seed's forward convolutions")
+    ap.add_argument("--tiles", type=int, default=16, help="tiles of --micro seed")
     return ap.parse_args()
 
 
@@ -285,6 +291,62 @@ KERNEL_NAMES = {
 }
 
 
+def micro(args):
+    """Kernel cases for profiling (CUDA events or ncu), one JSON line.
+
+    refresh: a 1600x1600x9 grid with seeded capacity (0..8, 5% zero) and demand
+    (half units): cost refresh with every track dirty, then with none, then
+    after via commits that dirty about a sixth of the tracks (twice), then two
+    full refreshes.  seed: two forward passes of the shipped seed network over
+    --tiles tiles (the first untimed), per convolution."""
+    import instantgr_b200 as ig
+    if args.micro == "seed":
+        m = ig.Seed.load()
+        r = m.time_forward(tiles=args.tiles, reps=2)
+        m.close()
+        print(json.dumps(dict(micro="seed", tiles=args.tiles, **r)), flush=True)
+        return r
+    X = Y = 1600
+    L = 9
+    rng = np.random.default_rng(7)
+    cap = rng.integers(0, 9, size=(L, X, Y)).astype(np.float32)
+    cap[rng.random((L, X, Y)) < 0.05] = 0.0
+    dem = (rng.integers(0, 20, size=(L, X, Y)) * 0.5).astype(np.float32)
+    dem[rng.random((L, X, Y)) < 0.4] = 0.0
+    xlen = rng.integers(1, 3, size=X - 1).astype(np.int32)
+    ylen = rng.integers(1, 3, size=Y - 1).astype(np.int32)
+    short = np.round(rng.uniform(0.5, 2.0, size=L), 3)
+    c = ig.Ctx(L, X, Y, 0, xlen, ylen, 1.0, 2.0, short, cap.reshape(-1))
+    c.set_demand(dem.reshape(-1))
+    nv = 300  # vias from layer 0 to layer 8 at random GCells: 8 tracks dirty each
+    xs, ys = rng.integers(0, X, nv), rng.integers(0, Y, nv)
+    routes = np.zeros(3 * nv, np.int32)
+    routes[0::3] = 3
+    routes[1::3] = xs * Y + ys
+    routes[2::3] = 8 * X * Y + xs * Y + ys
+    off = np.arange(nv, dtype=np.int64) * 3
+
+    def wall_us(f):
+        t0 = time.perf_counter()
+        f()
+        return round((time.perf_counter() - t0) * 1e6, 1)
+
+    res = dict(micro="refresh", grid=[L, X, Y], cells=L * X * Y)
+    res["all_dirty_us"] = wall_us(lambda: c.cost_refresh(True))
+    res["none_dirty_us"] = wall_us(lambda: c.cost_refresh(True))
+    res["partial_us"] = []
+    for k in range(2):
+        c.commit_vias(off, routes, stamp=10 + k, K=1)
+        res["partial_us"].append(wall_us(lambda: c.cost_refresh(True)))
+        c.commit_vias(off, routes, stamp=20 + k, K=-1)
+        c.cost_refresh(True)
+    res["full_us"] = [wall_us(lambda: c.cost_refresh(False)) for _ in range(2)]
+    res["note"] = "host wall time of each call, including its launch and synchronisation"
+    c.close()
+    print(json.dumps(res), flush=True)
+    return res
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -293,6 +355,8 @@ def main():
     wl = workload(args)
     if args.route_only:
         return route_only(args)
+    if args.micro:
+        return micro(args)
     if args.impl == "reference":
         return bench_reference(args, rank, world, wl)
 
@@ -382,7 +446,7 @@ def main():
         e2e_bytes.append((st["setup_h2d_bytes"] + st["h2d_bytes"], st["d2h_bytes"]))
         r.close()
 
-    ms_e2e, _, _ = timed(None, e2e_step)
+    ms_e2e, _ = timed(None, e2e_step)
 
     result = None
     if rank == 0:
@@ -395,9 +459,14 @@ def main():
             v = ks[k]
             ach = v["bytes"] / (v["ms"] / 1e3) / 1e9 if v["ms"] else 0.0
             n = max(v["launches"], 1)
+            traffic = tr.get(f"{k}_bytes_per_launch")
+            if traffic is None and f"{k}_bytes_per_cell" in tr:
+                # measured DRAM bytes per refreshed cell x the cells of an average
+                # launch (20 algorithmic bytes per refreshed cell)
+                traffic = round(tr[f"{k}_bytes_per_cell"] * v["bytes"] / n / 20.0)
             return dict(kernel=KERNEL_NAMES.get(k, k), bound="hbm", achieved=round(ach, 1), peak=pk["hbm_gbs"],
                         unit="GB/s", frac=round(ach / pk["hbm_gbs"], 4), peak_src=pk["src"],
-                        traffic=tr.get(f"{k}_bytes_per_launch"),
+                        traffic=traffic,
                         algorithmic_bytes_per_launch=round(v["bytes"] / n, 1),
                         avg_launch_us=round(1e3 * v["ms"] / n, 3))
 

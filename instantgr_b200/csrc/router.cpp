@@ -1390,6 +1390,7 @@ bool Router::rrr_pass(int iter) {
         kt.end(KC_VIA_COMMIT);
         st.launches += 5 + nl;
     }
+    const double t_enq = now_s();  // every batch of the pass enqueued
     cuda_check(cudaEventRecord(ev1, s), "event");
     cuda_check(cudaGetLastError(), "reroute launch");
     cuda_check(cudaEventSynchronize(ev1), "reroute");
@@ -1400,8 +1401,9 @@ bool Router::rrr_pass(int iter) {
     if (verbose)
         std::fprintf(stderr,
                      "[igr] pass %d host: marking and order %.3f s, DAGs %.3f s, conflict shapes %.3f s, colouring %.3f s, "
-                     "batch arrays %.3f s, batches on the device %.3f s\n",
-                     iter, th0 - tp0, t_dag - th0, t_shapes - t_dag, t_color - t_shapes, t_csr - t_color, now_s() - t_csr);
+                     "batch arrays %.3f s, batches on the device %.3f s (of it enqueueing %zu batches %.3f s)\n",
+                     iter, th0 - tp0, t_dag - th0, t_shapes - t_dag, t_color - t_shapes, t_csr - t_color, now_s() - t_csr,
+                     bi.size(), t_enq - t_csr);
     return true;
 }
 
