@@ -211,6 +211,16 @@ int igr_cost_refresh(igr_ctx *c, int only_dirty);
 int igr_get_costs(igr_ctx *c, float *vcost, double *presum);
 /* Loads a cost map (for replaying a reference cost map into the DP). */
 int igr_set_costs(igr_ctx *c, const float *vcost, const double *presum);
+/* Grid state to a file and back, for parity checks and replay: the file holds
+ * "IGRSTAT1", int32 L, X, Y, then demand (f32), vcost (f32), presum (f64),
+ * stamp (i32) and the wire difference array (i32), each [l][x][y], in the
+ * host's byte order.  Loading needs a context of the same L, X, Y
+ * (IGR_ERR_INVALID otherwise; IGR_ERR_IO / IGR_ERR_FORMAT for an unreadable
+ * or short file); the loaded costs count as fresh and every track as holding
+ * a pending wire commit.  Replaces the dump hooks planned for the reference
+ * (the survey's replay patch); InstantGR itself has none. */
+int igr_dump_state(igr_ctx *c, const char *path);
+int igr_load_state(igr_ctx *c, const char *path);
 
 /* Phase-1 tree DP (Lshape_route_cuda, src/Lshape_route.hpp:9-153) for a
  * batch of n nets.  Trees: nodes in DFS preorder (node_off[n+1] CSR), node

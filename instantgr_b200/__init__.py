@@ -40,7 +40,7 @@ EXPORTS = [
     "igr_router_stats", "igr_router_kstats", "igr_router_sizes", "igr_router_route", "igr_router_pins",
     "igr_router_demand", "igr_router_close", "igr_router_plan", "igr_router_grid", "igr_set_device",
     "igr_generate", "igr_generate_custom", "igr_create", "igr_destroy", "igr_last_error", "igr_set_demand",
-    "igr_get_demand", "igr_get_stamp", "igr_get_pre", "igr_cost_refresh", "igr_get_costs", "igr_set_costs",
+    "igr_get_demand", "igr_get_stamp", "igr_get_pre", "igr_cost_refresh", "igr_get_costs", "igr_set_costs", "igr_dump_state", "igr_load_state",
     "igr_pattern_route", "igr_pattern_route_static", "igr_commit_wires", "igr_commit_vias", "igr_ripup_wires",
     "igr_mark_overflow",
     "igr_congestion_view", "igr_score", "igr_color_batches", "igr_dag_route", "igr_build_dag", "igr_build_dags",
@@ -112,6 +112,8 @@ def lib() -> C.CDLL:
     L.igr_cost_refresh.argtypes = [vp, C.c_int]
     L.igr_get_costs.argtypes = [vp, _f32p, _f64p]
     L.igr_set_costs.argtypes = [vp, _f32p, _f64p]
+    L.igr_dump_state.argtypes = [vp, C.c_char_p]
+    L.igr_load_state.argtypes = [vp, C.c_char_p]
     L.igr_pattern_route.argtypes = [vp, C.c_int, _i32p, _i32p, _i32p, _i64p, _i32p, _i32p, C.c_int32]
     L.igr_pattern_route_static.argtypes = [vp, C.c_int, vp, C.c_int64, vp, vp, vp, vp, vp, C.c_int64, C.c_int32]
     L.igr_commit_wires.argtypes = [vp, C.c_int32]
@@ -388,6 +390,14 @@ class Ctx:
         p = np.zeros(self.N, dtype=np.float64)
         self._c(lib().igr_get_costs(self.h, v, p))
         return v, p
+
+    def dump_state(self, path: str):
+        """Demand, costs, stamps and difference array to a file (igr_dump_state)."""
+        self._c(lib().igr_dump_state(self.h, str(path).encode()))
+
+    def load_state(self, path: str):
+        """Grid state from a file of igr_dump_state (same grid size)."""
+        self._c(lib().igr_load_state(self.h, str(path).encode()))
 
     def set_costs(self, vcost, presum):
         self._c(lib().igr_set_costs(self.h, np.ascontiguousarray(vcost, dtype=np.float32).reshape(-1),

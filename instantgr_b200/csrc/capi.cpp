@@ -4,6 +4,7 @@
 // message kept for igr_last_error(); nothing here exits the process.
 #include "../../include/instantgr_b200.h"
 
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -421,6 +422,85 @@ int igr_set_costs(igr_ctx *c, const float *vcost, const double *presum) {
         c->d1.upload(presum, c->go.g.N, c->s);
         launch_to_track_layout_d(c->go.g, c->d1.p, c->go.presum.p, c->s);
         cuda_check(cudaMemsetAsync(c->go.dirty_cost.p, 0, c->go.g.ntracks, c->s), "memset");
+        sync_check(c);
+    });
+}
+
+namespace {
+constexpr char kStateMagic[8] = {'I', 'G', 'R', 'S', 'T', 'A', 'T', '1'};
+}
+
+int igr_dump_state(igr_ctx *c, const char *path) {
+    CTX_GUARD(c, {
+        if (!path) throw Error(ERR_INVALID, "null path");
+        const GridDev &g = c->go.g;
+        const size_t N = (size_t)g.N;
+        std::vector<float> dem(N), vc(N);
+        std::vector<double> ps(N);
+        std::vector<int32_t> st(N), pre(N);
+        c->f1.alloc(N);
+        c->d1.alloc(N);
+        c->a.alloc(N);
+        launch_from_track_layout_f(g, c->go.demand.p, c->f1.p, c->s);
+        cuda_check(cudaMemcpyAsync(dem.data(), c->f1.p, N * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
+        launch_from_track_layout_f(g, c->go.vcost.p, c->f1.p, c->s);
+        cuda_check(cudaMemcpyAsync(vc.data(), c->f1.p, N * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
+        launch_from_track_layout_d(g, c->go.presum.p, c->d1.p, c->s);
+        cuda_check(cudaMemcpyAsync(ps.data(), c->d1.p, N * 8, cudaMemcpyDeviceToHost, c->s), "D2H");
+        launch_from_track_layout_i(g, c->go.stamp.p, c->a.p, c->s);
+        cuda_check(cudaMemcpyAsync(st.data(), c->a.p, N * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
+        cuda_check(cudaStreamSynchronize(c->s), "sync");  // c->a is reused below
+        launch_from_track_layout_i(g, c->go.pre.p, c->a.p, c->s);
+        cuda_check(cudaMemcpyAsync(pre.data(), c->a.p, N * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
+        sync_check(c);
+        FILE *f = std::fopen(path, "wb");
+        if (!f) throw Error(ERR_IO, std::string("cannot open ") + path + " for writing");
+        const int32_t dims[3] = {g.L, g.X, g.Y};
+        bool ok = std::fwrite(kStateMagic, 1, 8, f) == 8 && std::fwrite(dims, 4, 3, f) == 3 &&
+                  std::fwrite(dem.data(), 4, N, f) == N && std::fwrite(vc.data(), 4, N, f) == N &&
+                  std::fwrite(ps.data(), 8, N, f) == N && std::fwrite(st.data(), 4, N, f) == N &&
+                  std::fwrite(pre.data(), 4, N, f) == N;
+        ok = std::fclose(f) == 0 && ok;
+        if (!ok) throw Error(ERR_IO, std::string("write failed on ") + path);
+    });
+}
+
+int igr_load_state(igr_ctx *c, const char *path) {
+    CTX_GUARD(c, {
+        if (!path) throw Error(ERR_INVALID, "null path");
+        const GridDev &g = c->go.g;
+        const size_t N = (size_t)g.N;
+        FILE *f = std::fopen(path, "rb");
+        if (!f) throw Error(ERR_IO, std::string("cannot open ") + path);
+        struct Closer {
+            FILE *f;
+            ~Closer() { std::fclose(f); }
+        } closer{f};
+        char magic[8];
+        int32_t dims[3];
+        if (std::fread(magic, 1, 8, f) != 8 || std::memcmp(magic, kStateMagic, 8) != 0 || std::fread(dims, 4, 3, f) != 3)
+            throw Error(ERR_FORMAT, std::string(path) + " is not a grid state file");
+        if (dims[0] != g.L || dims[1] != g.X || dims[2] != g.Y)
+            throw Error(ERR_INVALID, "the state file's grid differs from the context's");
+        std::vector<float> dem(N), vc(N);
+        std::vector<double> ps(N);
+        std::vector<int32_t> st(N), pre(N);
+        if (std::fread(dem.data(), 4, N, f) != N || std::fread(vc.data(), 4, N, f) != N ||
+            std::fread(ps.data(), 8, N, f) != N || std::fread(st.data(), 4, N, f) != N ||
+            std::fread(pre.data(), 4, N, f) != N)
+            throw Error(ERR_FORMAT, std::string(path) + " is shorter than its grid");
+        c->f1.upload(dem.data(), N, c->s);
+        launch_to_track_layout(g, c->f1.p, c->go.demand.p, c->s);
+        c->f2.upload(vc.data(), N, c->s);
+        launch_to_track_layout(g, c->f2.p, c->go.vcost.p, c->s);
+        c->d1.upload(ps.data(), N, c->s);
+        launch_to_track_layout_d(g, c->d1.p, c->go.presum.p, c->s);
+        c->a.upload(st.data(), N, c->s);
+        launch_to_track_layout_i(g, c->a.p, c->go.stamp.p, c->s);
+        c->b.upload(pre.data(), N, c->s);
+        launch_to_track_layout_i(g, c->b.p, c->go.pre.p, c->s);
+        cuda_check(cudaMemsetAsync(c->go.dirty_cost.p, 0, g.ntracks, c->s), "memset");
+        cuda_check(cudaMemsetAsync(c->go.dirty_commit.p, 1, g.ntracks, c->s), "memset");
         sync_check(c);
     });
 }

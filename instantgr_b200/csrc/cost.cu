@@ -476,6 +476,9 @@ void launch_to_track_layout(const GridDev &g, const float *ref, float *trk, cuda
 void launch_to_track_layout_d(const GridDev &g, const double *ref, double *trk, cudaStream_t s) {
     ref_to_track_kernel<double><<<grid_for(g.N), 256, 0, s>>>(g, ref, trk);
 }
+void launch_to_track_layout_i(const GridDev &g, const int *ref, int *trk, cudaStream_t s) {
+    ref_to_track_kernel<int><<<grid_for(g.N), 256, 0, s>>>(g, ref, trk);
+}
 void launch_from_track_layout_i(const GridDev &g, const int *trk, int *ref, cudaStream_t s) {
     track_to_ref_kernel<int><<<grid_for(g.N), 256, 0, s>>>(g, trk, ref);
 }

@@ -173,6 +173,7 @@ void launch_from_track_layout_f(const GridDev &g, const float *trk, float *ref, 
 void launch_from_track_layout_d(const GridDev &g, const double *trk, double *ref, cudaStream_t s);
 void launch_to_track_layout_d(const GridDev &g, const double *ref, double *trk, cudaStream_t s);
 void launch_from_track_layout_i(const GridDev &g, const int *trk, int *ref, cudaStream_t s);
+void launch_to_track_layout_i(const GridDev &g, const int *ref, int *trk, cudaStream_t s);
 
 // ---- conflict shapes and claim lists from the flattened trees (shapes.cu).
 // Shape k is routing net ids[k] (k when ids is null); its points are its tree's

@@ -29,6 +29,7 @@ namespace igr {
 namespace {
 
 constexpr int kBK = 64;                           // K per stage (four MMAs)
+constexpr int kRowPasses = 128 * kBK / 8 / 128;   // 16-byte A chunks per thread and stage
 constexpr unsigned long long kWaitNs = 2000000000ull;
 
 template <int BN>
@@ -76,25 +77,35 @@ struct FwdOp {
         const int lc = ilog2(c.cin);
         const int tap = k >> lc, ci = k & (c.cin - 1), dy = tap / 3, dx = tap - 3 * (tap / 3);
         const int hw = c.hout * c.wout;
-        for (int r = tid >> 3; r < 128; r += 16) {
-            const int m = m0 + r;
-            uint4 v = make_uint4(0, 0, 0, 0);
+        // every load of the stage in flight before the first store
+        uint4 v[kRowPasses];
+#pragma unroll
+        for (int it = 0; it < kRowPasses; it++) {
+            const int m = m0 + (tid >> 3) + 16 * it;
+            v[it] = make_uint4(0, 0, 0, 0);
             if (m < M && k < ke) {
                 const int t = m / hw, rem = m - t * hw, oy = rem / c.wout, ox = rem - oy * c.wout;
                 int iy, ix;
                 if (in_pos(c, oy, ox, dy, dx, iy, ix))
-                    v = *reinterpret_cast<const uint4 *>(X + (((size_t)t * c.hin + iy) * c.win + ix) * c.cin + ci);
+                    v[it] = *reinterpret_cast<const uint4 *>(X + (((size_t)t * c.hin + iy) * c.win + ix) * c.cin + ci);
             }
-            put8(sa, r, kc * 8, v);
         }
+#pragma unroll
+        for (int it = 0; it < kRowPasses; it++) put8(sa, (tid >> 3) + 16 * it, kc * 8, v[it]);
     }
     template <int BN>
     __device__ void load_b(__nv_bfloat16 *sb, int n0, int k0, int ke) const {
-        for (int q = threadIdx.x; q < BN * 8; q += 128) {
-            const int r = q >> 3, kc = q & 7, k = k0 + kc * 8, n = n0 + r;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (n < c.cout && k < ke) v = *reinterpret_cast<const uint4 *>(W + (size_t)n * K + k);
-            put8b(sb, BN, r, kc * 8, v);
+        uint4 v[BN / 16];
+#pragma unroll
+        for (int it = 0; it < BN / 16; it++) {
+            const int q = threadIdx.x + 128 * it, r = q >> 3, kc = q & 7, k = k0 + kc * 8, n = n0 + r;
+            v[it] = make_uint4(0, 0, 0, 0);
+            if (n < c.cout && k < ke) v[it] = *reinterpret_cast<const uint4 *>(W + (size_t)n * K + k);
+        }
+#pragma unroll
+        for (int it = 0; it < BN / 16; it++) {
+            const int q = threadIdx.x + 128 * it;
+            put8b(sb, BN, q >> 3, (q & 7) * 8, v[it]);
         }
     }
     __device__ void store(int row, int n0, const float *v) const {
@@ -122,9 +133,11 @@ struct DgradOp {
         const int sub = k / per, rem = k - sub * per;
         const int tap = rem >> lc, co = rem & (c.cout - 1), dy = tap / 3, dx = tap - 3 * (tap / 3);
         const int hw = c.hin * c.win;
-        for (int r = tid >> 3; r < 128; r += 16) {
-            const int m = m0 + r;
-            uint4 v = make_uint4(0, 0, 0, 0);
+        uint4 v[kRowPasses];
+#pragma unroll
+        for (int it = 0; it < kRowPasses; it++) {
+            const int m = m0 + (tid >> 3) + 16 * it;
+            v[it] = make_uint4(0, 0, 0, 0);
             if (m < M && k < ke) {
                 const int t = m / hw, q = m - t * hw, iy = q / c.win, ix = q - iy * c.win;
                 int oy, ox;
@@ -144,19 +157,27 @@ struct DgradOp {
                     ok = true;
                 }
                 ok = ok && oy >= 0 && ox >= 0 && oy < c.hout && ox < c.wout;
-                if (ok) v = *reinterpret_cast<const uint4 *>(dY + (((size_t)t * c.hout + oy) * c.wout + ox) * c.cout + co);
+                if (ok)
+                    v[it] = *reinterpret_cast<const uint4 *>(dY + (((size_t)t * c.hout + oy) * c.wout + ox) * c.cout + co);
             }
-            put8(sa, r, kc * 8, v);
         }
+#pragma unroll
+        for (int it = 0; it < kRowPasses; it++) put8(sa, (tid >> 3) + 16 * it, kc * 8, v[it]);
     }
     template <int BN>
     __device__ void load_b(__nv_bfloat16 *sb, int n0, int k0, int ke) const {
         const int per = 9 * c.cout;
-        for (int q = threadIdx.x; q < BN * 8; q += 128) {
-            const int r = q >> 3, kc = q & 7, k = k0 + kc * 8, n = n0 + r;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (n < c.cin && k < ke) v = *reinterpret_cast<const uint4 *>(WT + (size_t)n * per + (k % per));
-            put8b(sb, BN, r, kc * 8, v);
+        uint4 v[BN / 16];
+#pragma unroll
+        for (int it = 0; it < BN / 16; it++) {
+            const int q = threadIdx.x + 128 * it, r = q >> 3, kc = q & 7, k = k0 + kc * 8, n = n0 + r;
+            v[it] = make_uint4(0, 0, 0, 0);
+            if (n < c.cin && k < ke) v[it] = *reinterpret_cast<const uint4 *>(WT + (size_t)n * per + (k % per));
+        }
+#pragma unroll
+        for (int it = 0; it < BN / 16; it++) {
+            const int q = threadIdx.x + 128 * it;
+            put8b(sb, BN, q >> 3, (q & 7) * 8, v[it]);
         }
     }
     __device__ void store(int row, int n0, const float *v) const {
@@ -177,29 +198,40 @@ struct WgradOp {
     int M, K;  // M = 9 * cin, K = output pixels
     __device__ void load_a(__nv_bfloat16 *sa, int m0, int k0, int ke) const {
         const int lc = ilog2(c.cin), hw = c.hout * c.wout;
-        for (int q = threadIdx.x; q < 64 * 16; q += 128) {
-            const int kk = q & 63, r = (q >> 6) * 8, k = k0 + kk, m = m0 + r;
-            __align__(16) __nv_bfloat16 e[8];
-            *reinterpret_cast<uint4 *>(e) = make_uint4(0, 0, 0, 0);
+        uint4 v[kRowPasses];
+#pragma unroll
+        for (int it = 0; it < kRowPasses; it++) {
+            const int q = threadIdx.x + 128 * it, kk = q & 63, r = (q >> 6) * 8, k = k0 + kk, m = m0 + r;
+            v[it] = make_uint4(0, 0, 0, 0);
             if (m < M && k < ke) {
                 const int tap = m >> lc, ci = m & (c.cin - 1), dy = tap / 3, dx = tap - 3 * (tap / 3);
                 const int t = k / hw, rem = k - t * hw, oy = rem / c.wout, ox = rem - oy * c.wout;
                 int iy, ix;
                 if (in_pos(c, oy, ox, dy, dx, iy, ix))
-                    *reinterpret_cast<uint4 *>(e) =
-                        *reinterpret_cast<const uint4 *>(X + (((size_t)t * c.hin + iy) * c.win + ix) * c.cin + ci);
+                    v[it] = *reinterpret_cast<const uint4 *>(X + (((size_t)t * c.hin + iy) * c.win + ix) * c.cin + ci);
             }
+        }
+#pragma unroll
+        for (int it = 0; it < kRowPasses; it++) {
+            const int q = threadIdx.x + 128 * it, kk = q & 63, r = (q >> 6) * 8;
+            const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&v[it]);
 #pragma unroll
             for (int j = 0; j < 8; j++) put1(sa, 128, r + j, kk, e[j]);
         }
     }
     template <int BN>
     __device__ void load_b(__nv_bfloat16 *sb, int n0, int k0, int ke) const {
-        for (int q = threadIdx.x; q < 64 * (BN / 8); q += 128) {
-            const int kk = q & 63, r = (q >> 6) * 8, k = k0 + kk, n = n0 + r;
-            __align__(16) __nv_bfloat16 e[8];
-            *reinterpret_cast<uint4 *>(e) = make_uint4(0, 0, 0, 0);
-            if (n < c.cout && k < ke) *reinterpret_cast<uint4 *>(e) = *reinterpret_cast<const uint4 *>(dY + (size_t)k * c.cout + n);
+        uint4 v[BN / 16];
+#pragma unroll
+        for (int it = 0; it < BN / 16; it++) {
+            const int q = threadIdx.x + 128 * it, kk = q & 63, r = (q >> 6) * 8, k = k0 + kk, n = n0 + r;
+            v[it] = make_uint4(0, 0, 0, 0);
+            if (n < c.cout && k < ke) v[it] = *reinterpret_cast<const uint4 *>(dY + (size_t)k * c.cout + n);
+        }
+#pragma unroll
+        for (int it = 0; it < BN / 16; it++) {
+            const int q = threadIdx.x + 128 * it, kk = q & 63, r = (q >> 6) * 8;
+            const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&v[it]);
 #pragma unroll
             for (int j = 0; j < 8; j++) put1(sb, BN, r + j, kk, e[j]);
         }

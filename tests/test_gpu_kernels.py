@@ -260,3 +260,49 @@ def test_dag_route_split_by_size_matches_oracle(split):
         assert _dag_vs_oracle(g, d) == 120
     finally:
         ig.set_test_hook(ig.HOOK_RESET)
+
+
+def test_state_dump_and_load_round_trip(tmp_path):
+    """igr_dump_state / igr_load_state: a second context loaded from the file of
+    the first holds the same demand, costs, stamps and difference array (taken
+    after a tree-DP batch, before its commit), and commits and refreshes to the
+    same grid; a file of another grid size, a short file and a missing file are
+    refused."""
+    g, tb = _pattern_case(31, 64, 50, 1, 120, 8)
+    c = ctx_for(g)
+    c.cost_refresh()
+    total = int(tb["route_off"][-1] + tb["route_cap"][-1])
+    r = np.zeros(total, np.int32)
+    c.pattern_route(tb["node_off"], tb["nodes"], tb["par"], tb["route_off"], tb["route_cap"], r, 5)
+    path = str(tmp_path / "state.bin")
+    c.dump_state(path)
+    d = ig.Ctx(g["L"], g["X"], g["Y"], g["DIR"], g["xlen"], g["ylen"], g["unit_wire"], g["unit_via"], g["short"],
+               g["cap"])
+    d.load_state(path)
+    for get in ("demand", "stamps", "pre"):
+        assert np.array_equal(getattr(c, get)(), getattr(d, get)()), get
+    (v1, p1), (v2, p2) = c.costs(), d.costs()
+    assert np.array_equal(v1, v2) and np.array_equal(p1, p2)
+    for x in (c, d):
+        x.commit_wires(5)
+        x.commit_vias(tb["route_off"], r, 5, 1)
+        x.cost_refresh(only_dirty=True)
+    assert np.array_equal(c.demand(), d.demand())
+    (v1, p1), (v2, p2) = c.costs(), d.costs()
+    assert np.array_equal(v1, v2) and np.array_equal(p1, p2)
+    other = cases.grid_case(32, X=40, Y=30, dir0=1)
+    e = ctx_for(other)
+    with pytest.raises(ig.IgrError) as err:
+        e.load_state(path)
+    assert err.value.code == -1
+    short = str(tmp_path / "short.bin")
+    with open(path, "rb") as f, open(short, "wb") as o:
+        o.write(f.read(1000))
+    with pytest.raises(ig.IgrError) as err:
+        d.load_state(short)
+    assert err.value.code == -3
+    with pytest.raises(ig.IgrError) as err:
+        d.load_state(str(tmp_path / "missing.bin"))
+    assert err.value.code == -2
+    for x in (c, d, e):
+        x.close()
