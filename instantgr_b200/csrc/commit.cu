@@ -32,6 +32,7 @@ __device__ __forceinline__ int warp_incl_scan(int v, int lane) {
 }
 
 __global__ void __launch_bounds__(kThreads) wire_commit_kernel(GridDev g, int stamp, int only_dirty) {
+    chain_begin();
     const int tr = blockIdx.x;
     if (only_dirty && !g.dirty_commit[tr]) return;
     const TrackInfo ti = decode_track(g, tr);
@@ -98,6 +99,7 @@ __device__ __forceinline__ void mark_cost_dirty(const GridDev &g, int l, int x, 
 }
 
 __global__ void via_commit_kernel(GridDev g, ViaBatchDev b, int stamp, int K) {
+    chain_begin();
     const int warps = (gridDim.x * blockDim.x) >> 5;
     const int lane = threadIdx.x & 31;
     const int XY = g.X * g.Y;
@@ -134,6 +136,7 @@ __global__ void via_commit_kernel(GridDev g, ViaBatchDev b, int stamp, int K) {
 }
 
 __global__ void wire_ripup_kernel(GridDev g, ViaBatchDev b, int stamp, int K) {
+    chain_begin();
     const int warps = (gridDim.x * blockDim.x) >> 5;
     const int lane = threadIdx.x & 31;
     const int XY = g.X * g.Y;
@@ -180,17 +183,17 @@ int warps_grid(int n) {
 }  // namespace
 
 void launch_wire_commit(const GridDev &g, int stamp, bool only_dirty, cudaStream_t s) {
-    wire_commit_kernel<<<g.ntracks, kThreads, 0, s>>>(g, stamp, only_dirty ? 1 : 0);
+    launch_chained(wire_commit_kernel, dim3(g.ntracks), dim3(kThreads), 0, s, g, stamp, only_dirty ? 1 : 0);
 }
 
 void launch_via_commit(const GridDev &g, const ViaBatchDev &b, int stamp, int K, cudaStream_t s) {
     if (b.n <= 0) return;
-    via_commit_kernel<<<warps_grid(b.n), 256, 0, s>>>(g, b, stamp, K);
+    launch_chained(via_commit_kernel, dim3(warps_grid(b.n)), dim3(256), 0, s, g, b, stamp, K);
 }
 
 void launch_wire_ripup(const GridDev &g, const ViaBatchDev &b, int stamp, int K, cudaStream_t s) {
     if (b.n <= 0) return;
-    wire_ripup_kernel<<<warps_grid(b.n), 256, 0, s>>>(g, b, stamp, K);
+    launch_chained(wire_ripup_kernel, dim3(warps_grid(b.n)), dim3(256), 0, s, g, b, stamp, K);
 }
 
 }  // namespace igr

@@ -227,6 +227,7 @@ __device__ __forceinline__ void stage_track(const float *a, const float *b, floa
 
 template <int T, int MAXE>
 __global__ void IGR_TRACK_BOUNDS(T) cost_refresh_kernel(GridDev g, int only_dirty) {
+    chain_begin();
     const int tr = blockIdx.x;
     if (only_dirty) {
         if (!g.dirty_cost[tr]) return;
@@ -420,7 +421,7 @@ template <int T, int E>
 static void cost_refresh_e(const GridDev &g, int od, cudaStream_t s) {
     constexpr size_t smem = track_smem<T, E>();
     kernel_setup((const void *)cost_refresh_kernel<T, E>, T, smem);
-    cost_refresh_kernel<T, E><<<g.ntracks, T, smem, s>>>(g, od);
+    launch_chained(cost_refresh_kernel<T, E>, dim3(g.ntracks), dim3(T), smem, s, g, od);
 }
 
 template <int T, int E>

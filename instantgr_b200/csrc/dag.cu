@@ -81,6 +81,7 @@ struct EdgeScratch {
 // lane then scans the positions for one (f, t) pair with the reference's
 // additions in the reference's order.
 __global__ void __launch_bounds__(32 * kEdgeWarps) dag_edge_cost_kernel(GridDev g, DagBatchDev b) {
+    chain_begin();
     __shared__ EdgeScratch scr[kEdgeWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t e = (int64_t)blockIdx.x * kEdgeWarps + warp;
@@ -440,6 +441,7 @@ __device__ void compact_net(const GridDev &g, const DagBatchDev &b, int k, int l
 // fit an SM)
 template <int W, int Sizes>
 __global__ void __launch_bounds__(32 * W) dag_net_kernel(GridDev g, DagBatchDev b, int stamp) {
+    chain_begin();
     constexpr int kThreadsW = 32 * W;
     __shared__ NodeScratch scr[W];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -496,11 +498,12 @@ int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStre
     if (b.n_nodes <= 0 || b.n_nets <= 0) return 0;
     int launches = 0;
     if (b.n_edges > 0) {
-        dag_edge_cost_kernel<<<(int)((b.n_edges + kEdgeWarps - 1) / kEdgeWarps), 32 * kEdgeWarps, 0, s>>>(g, b);
+        launch_chained(dag_edge_cost_kernel, dim3((int)((b.n_edges + kEdgeWarps - 1) / kEdgeWarps)),
+                       dim3(32 * kEdgeWarps), 0, s, g, b);
         launches++;
     }
     if (!aux || b.n_nets < split_nets) {
-        dag_net_kernel<kDagWarps, 0><<<b.n_nets, kDagThreads, 0, s>>>(g, b, stamp);
+        launch_chained(dag_net_kernel<kDagWarps, 0>, dim3(b.n_nets), dim3(kDagThreads), 0, s, g, b, stamp);
         return launches + 1;
     }
     // a batch of many nets: the large nets' CTAs on the side stream, beside

@@ -16,6 +16,36 @@ constexpr int kRouteL = 9;        // routing layers handled by the DP kernels
 
 __device__ __forceinline__ int layer_dir(const GridDev &g, int l) { return (l & 1) ^ g.DIR; }
 
+// Programmatic dependent launch, first statement of the kernels of a reroute
+// batch: the next kernel of the stream may be scheduled from now on, and this
+// one waits until every kernel before it has finished and its writes are
+// visible.  Both are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void chain_begin() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// Launch with programmatic stream serialization: the kernel's CTAs may be
+// scheduled while the previous kernel of the stream finishes (it hides the
+// launch gaps between the short kernels of a reroute batch: 228.3 -> 226.6 ms
+// per route of the 800k-net design, identical results); the kernel must start
+// with chain_begin().
+template <typename... KArgs, typename... Args>
+inline void launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                           Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // offset of cell (l, x, y) in the track-contiguous layout
 __device__ __forceinline__ int64_t cell_at(const GridDev &g, int l, int x, int y) {
     int64_t b = (int64_t)l * g.X * g.Y;

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <exception>
+#include <future>
 #include <memory>
 #include <string>
 #include <thread>
@@ -336,7 +337,21 @@ struct Router {
     // the DAGs, conflict shapes, colouring and batch arrays were done
     bool dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<int>> &batches,
                         std::vector<DagBatchInfo> &bi, const std::vector<int64_t> &old_off, double *tm);
-    void upload_dag_trees();  // trees in adjacency order, once per router
+    void upload_dag_trees();  // trees in adjacency order, once per router (enqueued, no sync)
+    // the trees in adjacency order packed into page-locked buffers; the first
+    // run packs them on a side thread while phase 1 runs on the device
+    struct PackedTrees {
+        int *off = nullptr, *pos = nullptr, *aoff = nullptr, *adj = nullptr;
+        size_t n_off = 0, n_pos = 0, n_aoff = 0, n_adj = 0;
+        PackedTrees() = default;
+        PackedTrees(const PackedTrees &) = delete;
+        PackedTrees &operator=(const PackedTrees &) = delete;
+        ~PackedTrees() { release(); }
+        void release();  // back to the page-locked block cache
+    };
+    PackedTrees dt_pack;
+    std::future<void> dt_packing;  // declared after the trees it reads: joined first on destruction
+    void pack_dag_trees();
 
    private:
     void phase1();
