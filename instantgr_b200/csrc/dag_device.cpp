@@ -45,7 +45,9 @@ void run_class(DeviceDags &d, DagBuildArgs a, int cls, const std::vector<int> &m
         a.work = d.work.p;
     }
     a.n_list = n;
-    if (members.back() == n - 1) {  // ascending and complete: 0 .. n-1
+    bool identity = true;  // 0 .. n-1 in order
+    for (int i = 0; i < n && identity; i++) identity = members[i] == i;
+    if (identity) {
         a.list = nullptr;
     } else {
         d.list.upload(members, s);
@@ -70,7 +72,7 @@ void grow_keep(DevBuf<int> &b, size_t count, size_t keep, cudaStream_t s) {
 
 }  // namespace
 
-void DeviceDags::build(DagBuildArgs a, cudaStream_t s) {
+void DeviceDags::build(DagBuildArgs a, cudaStream_t s, const std::vector<int> *order_key) {
     const int n = a.n_list;
     hs.assign((size_t)n * kDagSizeFields, 0);
     tier.assign(n, 0);
@@ -95,6 +97,12 @@ void DeviceDags::build(DagBuildArgs a, cudaStream_t s) {
     set_pools();
     std::vector<int> members(n), next;  // DAGs to build in this class; for the next class
     for (int k = 0; k < n; k++) members[k] = k;
+    // builders of nets alike in size side by side: a warp's 32 builders then
+    // walk loops of similar lengths and diverge less (c2: 21/18/18 -> 18/13/13
+    // ms per pass); each DAG is built alone, so the DAGs do not change
+    if (order_key)
+        std::stable_sort(members.begin(), members.end(),
+                         [&](int l, int r) { return (*order_key)[l] > (*order_key)[r]; });
     int cls = 0, regrow = 0;
     while (true) {
         run_class(*this, a, cls, members, s);

@@ -1493,8 +1493,14 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
     st.h2d_bytes += (int64_t)of_nets.size() * 4;
     a.ids = d2_ids.p;
     a.n_list = (int)of_nets.size();
+    // build order: tree nodes, then HPWL (nets alike in size side by side)
+    std::vector<int> okey(of_nets.size());
+    for (size_t k = 0; k < of_nets.size(); k++) {
+        const RNet &rn = ns.nets[of_nets[k]];
+        okey[k] = (int)rn.tnode.size() * 65536 + std::min(65535, rn.hpwl);
+    }
     const double tb0 = now_s();
-    ddag.build(a, s);
+    ddag.build(a, s, &okey);
     const double tb1 = now_s();
     st.d2h_bytes += (int64_t)of_nets.size() * kDagSizeFields * 4;
     // the DP keeps at most 10 child slots per node (the reference packs the

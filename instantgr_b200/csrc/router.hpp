@@ -104,7 +104,9 @@ struct DeviceDags {
     std::vector<int> tier;  // work-area size class each DAG fits
     // a.ids, a.n_list and the tree, congestion and grid fields set; the rest
     // is filled in here
-    void build(DagBuildArgs a, cudaStream_t s);
+    // order_key (optional, per DAG): the first class builds its DAGs in
+    // descending key order
+    void build(DagBuildArgs a, cudaStream_t s, const std::vector<int> *order_key = nullptr);
     int sz(int k, int f) const { return hs[(size_t)k * kDagSizeFields + f]; }
 };
 
