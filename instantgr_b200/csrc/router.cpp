@@ -1497,7 +1497,7 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
     std::vector<int> okey(of_nets.size());
     for (size_t k = 0; k < of_nets.size(); k++) {
         const RNet &rn = ns.nets[of_nets[k]];
-        okey[k] = (int)rn.tnode.size() * 65536 + std::min(65535, rn.hpwl);
+        okey[k] = (int)std::min<size_t>(rn.tnode.size(), 32767) * 65536 + std::min(65535, rn.hpwl);
     }
     const double tb0 = now_s();
     ddag.build(a, s, &okey);
