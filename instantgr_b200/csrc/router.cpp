@@ -1563,6 +1563,17 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
     auto e_of = [&](int i) { return ddag.sz(kept[i], 1); };
     auto d_of = [&](int i) { return ddag.sz(kept[i], 3); };
     auto s_of = [&](int i) { return ddag.sz(kept[i], 4); };
+    // within a batch the largest DAGs first: the DP's CTAs start in that order,
+    // so that the longest nets do not begin last (the nets of a batch are
+    // independent; c2: 219 -> 215 ms per route)
+    parallel_for(B, threads, [&](int b0, int e0) {
+        for (int b = b0; b < e0; b++) {
+            std::vector<int> &v = bpos[b];
+            std::stable_sort(v.begin(), v.end(), [&](int l, int r) { return m_of(l) > m_of(r); });
+            batches[b].clear();
+            for (int i : v) batches[b].push_back(of_nets[i]);
+        }
+    });
     bi.assign(B, DagBatchInfo{});
     DagBatchInfo tot{};
     {
