@@ -346,8 +346,13 @@ int igr_seed_set_tile(igr_seed *m, int size, int halo);
 /* All parameters (per layer: weights [cout][3][3][cin], then biases); *n gets the count. */
 int igr_seed_params(igr_seed *m, float *out, int64_t cap, int64_t *n);
 int igr_seed_set_params(igr_seed *m, const float *params, int64_t n);
-/* Features of an opened router's design ([X][Y][16]). */
+/* Features of an opened router's design ([X][Y][16]), on the host threads. */
 int igr_seed_features(igr_router *r, float *out);
+/* The same features computed on the device from the router's resident trees,
+ * as a seeded run computes them (brings up the device state when needed); the
+ * RUDY channels are summed in fixed point there and agree with
+ * igr_seed_features to the BF16 rounding. */
+int igr_seed_features_device(igr_router *r, float *out);
 /* Training maps kept in device memory: explicit maps, or the features and the
  * routed demand of a router's last run. */
 int igr_seed_add_map(igr_seed *m, int X, int Y, const float *features, const float *target, int32_t *map_id);

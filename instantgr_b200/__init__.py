@@ -46,7 +46,7 @@ EXPORTS = [
     "igr_congestion_view", "igr_score", "igr_color_batches", "igr_dag_route", "igr_build_dag", "igr_build_dags",
     "igr_steiner",
     "igr_seed_create", "igr_seed_destroy", "igr_seed_last_error", "igr_seed_set_tile", "igr_seed_params",
-    "igr_seed_set_params", "igr_seed_features", "igr_seed_add_map", "igr_seed_add_routed", "igr_seed_train",
+    "igr_seed_set_params", "igr_seed_features", "igr_seed_features_device", "igr_seed_add_map", "igr_seed_add_routed", "igr_seed_train",
     "igr_seed_eval", "igr_seed_predict", "igr_seed_time_forward", "igr_seed_grad", "igr_router_set_seed", "igr_router_seed_stats",
     "igr_test_hook",
 ]
@@ -142,6 +142,7 @@ def lib() -> C.CDLL:
     L.igr_seed_params.argtypes = [vp, vp, C.c_int64, C.POINTER(C.c_int64)]
     L.igr_seed_set_params.argtypes = [vp, _f32p, C.c_int64]
     L.igr_seed_features.argtypes = [vp, _f32p]
+    L.igr_seed_features_device.argtypes = [vp, _f32p]
     L.igr_seed_add_map.argtypes = [vp, C.c_int, C.c_int, _f32p, _f32p, C.POINTER(C.c_int32)]
     L.igr_seed_add_routed.argtypes = [vp, vp, C.POINTER(C.c_int32)]
     L.igr_seed_train.argtypes = [vp, C.c_int, C.c_int, C.c_float, C.c_uint64, C.c_int, vp]
@@ -602,10 +603,12 @@ class Seed:
         return loss.value, g
 
 
-def seed_features(router: "Router") -> np.ndarray:
-    """Input features of an opened router's design, [X][Y][16]."""
+def seed_features(router: "Router", device: bool = False) -> np.ndarray:
+    """Input features of an opened router's design, [X][Y][16], on the host
+    threads or (device=True) on the GPU as a seeded run computes them."""
     hdr = np.zeros(4, np.int32)
     _check(lib().igr_router_grid(router.h, hdr.ctypes.data_as(C.c_void_p), None, None, None, None))
     out = np.zeros((int(hdr[1]), int(hdr[2]), 16), np.float32)
-    _check(lib().igr_seed_features(router.h, out.reshape(-1)), router.h)
+    fn = lib().igr_seed_features_device if device else lib().igr_seed_features
+    _check(fn(router.h, out.reshape(-1)), router.h)
     return out

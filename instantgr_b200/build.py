@@ -24,7 +24,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CUDA_INC = "/usr/local/cuda/include"
 
 CU_SOURCES = ["cost.cu", "commit.cu", "ripup.cu", "pattern.cu", "pattern_static.cu", "color.cu", "dag.cu", "plan.cu",
-              "seed_nn.cu", "shapes.cu", "eval.cu", "records.cu", "dagbuild.cu", "launch.cu"]
+              "seed_nn.cu", "seed_feat.cu", "shapes.cu", "eval.cu", "records.cu", "dagbuild.cu", "launch.cu"]
 CPP_SOURCES = ["design_io.cpp", "pins.cpp", "netbuild.cpp", "gen.cpp", "dag_build.cpp", "dag_device.cpp", "router.cpp",
                "capi.cpp", "seed_model.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -1038,6 +1038,19 @@ int igr_seed_features(igr_router *h, float *out) {
     });
 }
 
+int igr_seed_features_device(igr_router *h, float *out) {
+    if (!h || !out) return fail(nullptr, IGR_ERR_INVALID, "null argument");
+    return guard(&h->err, [&] {
+        auto &r = h->r;
+        DevBuf<__nv_bfloat16> feat;
+        r.device_seed_features(feat, r.s);
+        std::vector<__nv_bfloat16> f((size_t)r.go.g.X * r.go.g.Y * 16);
+        cuda_check(cudaMemcpyAsync(f.data(), feat.p, f.size() * 2, cudaMemcpyDeviceToHost, r.s), "D2H");
+        cuda_check(cudaStreamSynchronize(r.s), "sync");
+        for (size_t i = 0; i < f.size(); i++) out[i] = __bfloat162float(f[i]);
+    });
+}
+
 int igr_seed_add_map(igr_seed *m, int X, int Y, const float *feat, const float *target, int32_t *map_id) {
     SEED_GUARD(m, {
         if (X < 1 || Y < 1 || !feat || !target) throw Error(ERR_INVALID, "bad map");

@@ -582,18 +582,37 @@ void Router::restore_result(RouteBackup &b) {
 
 // Prediction of the attached congestion seed for this design (once), the
 // seed demand in the track layout and the predicted overflow per GCell.
+void Router::device_seed_features(DevBuf<__nv_bfloat16> &feat, cudaStream_t st) {
+    ensure_device();
+    const int X = go.g.X, Y = go.g.Y;
+    const size_t XY = (size_t)X * Y, D = (size_t)(X + 1) * (Y + 1);
+    DevBuf<float> cap0;
+    DevBuf<int> pins;
+    DevBuf<long long> dh, dv;
+    cap0.upload(d.cap.data(), XY, st);  // file layer 0
+    pins.alloc(XY);
+    dh.alloc(D);
+    dv.alloc(D);
+    feat.alloc(XY * 16);
+    // the trees were uploaded on the router's stream
+    cuda_check(cudaStreamSynchronize(s), "trees");
+    launch_seed_features(go.g, (int)ns.nets.size(), d_tree_off.p, d_tree_nodes.p, cap0.p, d.L, pins.p, dh.p, dv.p,
+                         feat.p, st);
+    cuda_check(cudaGetLastError(), "seed features");
+    cuda_check(cudaStreamSynchronize(st), "seed features");
+}
+
 void Router::prepare_seed() {
     if (seed_ready) return;
     const double t0 = now_s();
     const int L = go.g.L, X = go.g.X, Y = go.g.Y;
-    std::vector<__nv_bfloat16> f;
-    seed_features(d, ns, f);
-    const double t1 = now_s();
+    const size_t nf = (size_t)X * Y * 16;
     DevBuf<__nv_bfloat16> feat;
+    device_seed_features(feat, seed->s);
+    const double t1 = now_s();
     DevBuf<float> pred, ref, cap;
-    feat.upload(f.data(), f.size(), seed->s);
-    pred.alloc(f.size());
-    cuda_check(cudaMemsetAsync(pred.p, 0, f.size() * sizeof(float), seed->s), "memset");
+    pred.alloc(nf);
+    cuda_check(cudaMemsetAsync(pred.p, 0, nf * sizeof(float), seed->s), "memset");
     seed->predict(X, Y, feat.p, pred.p);
     const double t2 = now_s();
     cap.alloc((size_t)L * X * Y);

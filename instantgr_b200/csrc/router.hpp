@@ -1,5 +1,6 @@
 // Host driver of the router and ownership of device memory.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <exception>
@@ -289,6 +290,9 @@ struct Router {
     std::vector<double> seed_sat;     // summed-area table of the predicted overflow
     std::vector<int> hpwl_keys;       // HPWL of every routing net, contiguous (rip-up order keys)
     void prepare_seed();
+    // the seed's input features ([X][Y][16] bf16) on the device from the
+    // resident trees (seed_feat.cu); synchronous on `st`
+    void device_seed_features(DevBuf<__nv_bfloat16> &feat, cudaStream_t st);
     void seed_begin();
     double seed_pressure(int net) const;
     void run_once(bool seeded);

@@ -78,5 +78,13 @@ void launch_adam(int n, float *p, const float *g, float *m, float *v, float lr, 
 // and the gradient layout conversion dW[cout][9][cin] <- dWT[9*cin][cout].
 void launch_seed_weights(int cin, int cout, const float *Wm, __nv_bfloat16 *W, __nv_bfloat16 *WT, cudaStream_t s);
 void launch_seed_grad_layout(int cin, int cout, const float *dWT, float *dW, cudaStream_t s);
+// The 16 input channels of a design ([X][Y][16] bf16, seed_feat.cu) from the
+// resident trees of its n routing nets (positions l*X*Y + x*Y + y, Steiner
+// points at layer g.L), the capacity of file layer 0 (cap0, [x][y]) and the
+// grid's; pins ([X*Y]) and dh, dv ([(X+1)*(Y+1)]) are work arrays.
+struct GridDev;
+void launch_seed_features(const GridDev &g, int n, const int *tree_off, const int *tree_nodes, const float *cap0,
+                          int file_layers, int *pins, long long *dh, long long *dv, __nv_bfloat16 *out,
+                          cudaStream_t s);
 
 }  // namespace igr

@@ -72,3 +72,28 @@ def test_seeded_routing_is_deterministic(heldout, model):
         outs.append(open(out).read())
         r.close()
     assert outs[0] == outs[1]
+
+
+@pytest.mark.parametrize("cfg,seed,scale", [(3, 9001, 1.0), (1, 1, 0.3)])
+def test_device_features_equal_host_features(tmp_path, cfg, seed, scale):
+    """The seed's input features computed on the device from the resident trees
+    (what a seeded run uses) against the host restatement: pins, blocked-layer
+    fraction and capacities identical; the RUDY channels, summed in fixed point
+    on the device (exact) and in double on the host, identical but for the host's
+    cancellation residues (below 1e-9 where the sums are zero) and at most one
+    BF16 step at a few GCells."""
+    cap, net = str(tmp_path / "d.cap"), str(tmp_path / "d.net")
+    ig.generate(cfg, seed, scale, cap, net)
+    r = ig.Router(cap, net)
+    host = ig.seed_features(r)
+    dev = ig.seed_features(r, device=True)
+    r.close()
+    exact = [0] + list(range(3, 16))
+    assert np.array_equal(host[..., exact], dev[..., exact])
+    for ch in (1, 2):
+        h, d = host[..., ch], dev[..., ch]
+        diff = np.abs(h - d)
+        real = diff > 1e-9  # beyond the host's residues of exact cancellations
+        step = np.maximum(np.abs(h), np.abs(d)) * 2.0 ** -7  # one BF16 step at the value
+        assert np.all(diff[real] <= step[real] * 1.0001), f"channel {ch}: {diff[real].max()}"
+        assert np.count_nonzero(real) <= max(2, h.size // 100000), f"channel {ch}: {np.count_nonzero(real)} cells"
