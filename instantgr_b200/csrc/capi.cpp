@@ -949,14 +949,15 @@ int igr_steiner(int n, const int32_t *x, const int32_t *y, int32_t *nx, int32_t 
 int igr_router_set_seed(igr_router *h, igr_seed *m, double alpha, int mode, int kind, int levels) {
     if (!h) return fail(nullptr, IGR_ERR_INVALID, "null router");
     return guard(&h->err, [&] {
-        if (mode < 0 || mode > 2 || !(alpha >= 0) || kind < 0 || kind > 1 || levels < 0)
+        if (mode < 0 || mode > 2 || !(alpha >= 0) || kind < 0 || kind > 3 || levels < 0)
             throw Error(ERR_INVALID, "bad seed mode, kind, levels or weight");
         if (mode && !m) throw Error(ERR_INVALID, "null model");
         auto &r = h->r;
         r.seed = mode ? &m->m : nullptr;
         r.seed_mode = mode;
         r.seed_alpha = alpha;
-        r.seed_kind = kind;
+        r.seed_kind = kind & 1;
+        r.seed_order = (kind & 2) != 0;
         r.seed_levels = levels;
         r.seed_ready = false;
         r.seed_used = false;

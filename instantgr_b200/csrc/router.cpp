@@ -1144,7 +1144,7 @@ bool Router::rrr_pass(int iter) {
         cuda_check(cudaStreamSynchronize(s), "sync");
         st.d2h_bytes += (int64_t)X * Y * 8;
     }
-    if (seed_active) {
+    if (seed_active && seed_order) {
         // predicted congestion first, then HPWL (the reference's order)
         std::vector<double> pr(R, 0.0);
         for (int i : of_nets) pr[i] = seed_pressure(i);

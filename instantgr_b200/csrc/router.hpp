@@ -282,6 +282,7 @@ struct Router {
     double seed_alpha = 0.5;
     int seed_mode = 0;
     int seed_kind = 0;    // 0 predicted demand, 1 predicted overflow only
+    bool seed_order = false;  // rip-up order by predicted overflow instead of HPWL
     int seed_levels = 0;  // 0 constant during phase 1, else shrinks in this many steps
     bool seed_ready = false, seed_active = false, seed_used = false;
     double seed_ms = 0, seed_scores[2] = {0, 0};
