@@ -337,6 +337,14 @@ int igr_test_hook(int key, int64_t value) {
             if (value < 1) return fail(nullptr, IGR_ERR_INVALID, "split threshold must be at least 1");
             h.dag_split_nets = (int)std::min<int64_t>(value, INT32_MAX);
             return IGR_OK;
+        case IGR_HOOK_DAG_BIG_NODES:
+            if (value < 0) return fail(nullptr, IGR_ERR_INVALID, "negative node count");
+            h.dag_big_nodes = (int)std::min<int64_t>(value, INT32_MAX);
+            return IGR_OK;
+        case IGR_HOOK_DAG_STAGE_NODES:
+            if (value < 0 || value > 4096) return fail(nullptr, IGR_ERR_INVALID, "staging limit in 0..4096 nodes");
+            h.dag_stage_nodes = (int)value;
+            return IGR_OK;
         default: return fail(nullptr, IGR_ERR_INVALID, "unknown test hook");
     }
 }
@@ -777,7 +785,7 @@ int igr_dag_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t *nod
         const int64_t ext = records_extent(n, route_off, route_cap, nullptr);
         DevBuf<int> dn, dpo, dp, dcs, dec, dco, dlo, dln, dnl, dno, dids, dcap, dlout, dstage, dscnt, dbc;
         DevBuf<int64_t> droff;
-        DevBuf<double> dcost, dce;
+        DevBuf<double> dcost, dce, doff;
         DevBuf<unsigned long long> dbest, dpk;
         dn.upload(nodes, N, c->s); dpo.upload(par_off, N + 1, c->s); dp.upload(par, E, c->s);
         dcs.upload(child_slot, E, c->s); dec.upload(echild, c->s); dco.upload(child_off, c->s);
@@ -785,6 +793,7 @@ int igr_dag_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t *nod
         dno.upload(node_off, n + 1, c->s);
         dids.upload(ids, c->s); dcap.upload(route_cap, n, c->s); droff.upload(route_off, n, c->s);
         dcost.alloc((size_t)N * 10); dce.alloc((size_t)std::max(E, 1) * 81); dbc.alloc((size_t)std::max(E, 1) * 81);
+        doff.alloc((size_t)std::max(E, 1) * 54);
         dbest.alloc((size_t)std::max(child_off[N], 1) * 10); dpk.alloc((size_t)std::max(child_off[N], 1) * 10);
         dlout.alloc(N); dstage.alloc((size_t)N * 8); dscnt.alloc(N);
         c->routes.upload(routes_out, (size_t)ext, c->s);
@@ -793,14 +802,19 @@ int igr_dag_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t *nod
         db.nodes = dn.p; db.par_off = dpo.p; db.par = dp.p; db.child_slot = dcs.p; db.edge_child = dec.p;
         db.child_off = dco.p; db.level_off = dlo.p; db.level_nodes = dln.p; db.net_level_off = dnl.p;
         db.net_node_off = dno.p; db.net_ids = dids.p; db.costs = dcost.p; db.best_path = dbest.p; db.packed = dpk.p;
-        db.cost_edges = dce.p; db.best_change = dbc.p; db.layer_out = dlout.p; db.stage = dstage.p;
+        db.cost_edges = dce.p; db.best_change = dbc.p; db.layer_out = dlout.p; db.stage = dstage.p; db.offers = doff.p;
         db.stage_cnt = dscnt.p; db.route_off = droff.p; db.route_cap = dcap.p; db.routes = c->routes.p;
         if (!c->aux) {
             cuda_check(cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking), "stream");
             cuda_check(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming), "event");
             cuda_check(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming), "event");
         }
-        launch_dag_route(g, db, stamp, c->s, c->aux, c->fork, c->join, test_hooks().dag_split_nets.load());
+        for (int k = 0; k < n; k++) {
+            db.max_net_nodes = std::max(db.max_net_nodes, node_off[k + 1] - node_off[k]);
+            db.max_net_edges = std::max(db.max_net_edges, par_off[node_off[k + 1]] - par_off[node_off[k]]);
+        }
+        launch_dag_route(g, db, stamp, c->s, c->aux, c->fork, c->join, test_hooks().dag_split_nets.load(),
+                         test_hooks().dag_stage_nodes.load(), test_hooks().dag_big_nodes.load());
         cuda_check(cudaGetLastError(), "DAG launch");
         cuda_check(cudaMemcpyAsync(routes_out, c->routes.p, ext * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
         sync_check(c);

@@ -29,6 +29,8 @@ constexpr int kDagWarps = 8;                 // warps of one net's CTA
 constexpr int kDagThreads = 32 * kDagWarps;
 constexpr int kSmallWarps = 2;               // warps of a small net's CTA
 constexpr int kSmallNodes = 64;              // a small net's DAG has at most this many nodes
+constexpr int kBigWarps = 16;                // warps of a large net's CTA
+constexpr int kMaxStageNodes = 4096;         // staging limit in nodes (4096: 147 KB of shared memory)
 
 __device__ __forceinline__ int32_t f2o(float f) {
     int32_t i = __float_as_int(f);
@@ -152,23 +154,91 @@ struct NodeScratch {
 
 constexpr double kNone = __builtin_huge_val();  // no candidate (every real candidate is below kInf)
 
+// One net's DAG as the DP and the backtrace read it.  S = false: the batch
+// arrays.  S = true: the net's node positions (decoded, packed as
+// layer << 28 | x << 14 | y), child and parent-edge offsets, parents, child
+// slots, level lists and level offsets copied into shared memory at the start
+// of the net, with its chosen layers and segment counts kept there too, so
+// that the dependent lookups of every node stay on chip.  Indices and values
+// are the batch's in both forms; the shared layout (ints) is
+// pos[n] coff[n+1] poff[n+1] lev[n] lo[n] scnt[n] par[m] slot[m] loff[...].
+extern __shared__ int s_dag[];
+constexpr int kStageLevels = 64;  // levels of a staged net, at most
+constexpr int kStageMaxSide = 1 << 14;  // staged positions hold x and y in 14 bits
+
+struct NetLoc {
+    int n0, e0, l0, n, m;  // first node, first parent edge, first level offset; nodes, parent edges
+};
+
+struct NodePos {
+    int l, x, y;  // layer index (9: the Steiner layer) and GCell
+};
+
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(__cvta_generic_to_global(p)));
+}
+
+template <bool S>
+struct Dag {
+    const DagBatchDev &b;
+    NetLoc L;
+    int XY, Y;
+    __device__ __forceinline__ NodePos pos(int node) const {
+        if (S) {
+            const unsigned p = (unsigned)s_dag[node - L.n0];
+            return {(int)(p >> 28), (int)((p >> 14) & 0x3FFF), (int)(p & 0x3FFF)};
+        }
+        const int v = b.nodes[node], l = v / XY, q = v - l * XY, x = q / Y;
+        return {l, x, q - x * Y};
+    }
+    __device__ __forceinline__ int coff(int node) const {
+        return S ? s_dag[L.n + node - L.n0] : b.child_off[node];
+    }
+    __device__ __forceinline__ int poff(int node) const {
+        return S ? s_dag[2 * L.n + 1 + node - L.n0] : b.par_off[node];
+    }
+    __device__ __forceinline__ int lev(int pos) const {
+        return S ? s_dag[3 * L.n + 2 + pos - L.n0] : b.level_nodes[pos];
+    }
+    __device__ __forceinline__ int *lo(int node) const {
+        return S ? s_dag + 4 * L.n + 2 + node - L.n0 : b.layer_out + node;
+    }
+    __device__ __forceinline__ int *scnt(int node) const {
+        return S ? s_dag + 5 * L.n + 2 + node - L.n0 : b.stage_cnt + node;
+    }
+    __device__ __forceinline__ int par(int e) const { return S ? s_dag[6 * L.n + 2 + e - L.e0] : b.par[e]; }
+    __device__ __forceinline__ int slot(int e) const {
+        return S ? s_dag[6 * L.n + 2 + L.m + e - L.e0] : b.child_slot[e];
+    }
+    __device__ __forceinline__ int loff(int d) const {
+        return S ? s_dag[6 * L.n + 2 + 2 * L.m + d] : b.level_off[L.l0 + d];
+    }
+};
+
+// ints of shared memory that a staged net of n nodes and m parent edges takes
+__host__ __device__ constexpr int staged_ints(int n, int m) { return 6 * n + 2 + 2 * m + kStageLevels; }
+
 // what one (parent edge, target layer t) pair needs besides the node's own
 // costs: the parent's packed entry and, per source layer of t's parity
-// (layer = 2 - t % 2 + 2q), the wire cost (layer == t) or the precomputed
-// mid-edge layer change cost, kNone where the reference skips the layer
+// (layer = 2 - t % 2 + 2q), the wire cost (layer == t, bit q of `wire`) or
+// the precomputed mid-edge layer change cost (bit q of `change`; the
+// reference skips it when it is not below INF).  The loads are only issued
+// here: nothing reads their values until the offers are sent.
 struct Offer {
     int64_t dst;
     double v[5];
+    unsigned wire, change;
 };
 
-__device__ __forceinline__ void offer_load(const GridDev &g, const DagBatchDev &b, int node, int x, int y, int e,
-                                           int t, Offer &o) {
-    const int parent = b.par[e];
-    const int pv = b.nodes[parent];
-    const int px = pv / g.Y % g.X, py = pv % g.Y;
+template <bool S>
+__device__ __forceinline__ void offer_load(const GridDev &g, const Dag<S> &D, int x, int y, int e, int t, Offer &o) {
+    const int parent = D.par(e);
+    const NodePos pp = D.pos(parent);
+    const int px = pp.x, py = pp.y;
     const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
     const bool far = abs(x - px) + abs(y - py) > 4;
-    o.dst = ((int64_t)b.child_off[parent] + b.child_slot[e]) * kML + t;
+    o.dst = ((int64_t)D.coff(parent) + D.slot(e)) * kML + t;
+    o.wire = o.change = 0;
 #pragma unroll
     for (int q = 0; q < 5; q++) {
         const int layer = 2 - (t & 1) + 2 * q;
@@ -179,11 +249,45 @@ __device__ __forceinline__ void offer_load(const GridDev &g, const DagBatchDev &
         if (dl == 0 && x != px) continue;
         if (t == layer) {
             o.v[q] = wire_cost(g, layer - 1, minx, maxx, miny, maxy);
+            o.wire |= 1u << q;
         } else if (far) {
-            const double ce = b.cost_edges[(int64_t)e * 81 + (layer - 1) * 9 + (t - 1)];
-            if (ce < kInf) o.v[q] = ce;
+            o.v[q] = D.b.cost_edges[(int64_t)e * 81 + (layer - 1) * 9 + (t - 1)];
+            o.change |= 1u << q;
         }
     }
+}
+
+// The offer records of a staged net are computed once, by all threads of its
+// CTA before the DP starts (they depend on no DP result), at (e * 9 + t - 1)
+// * kOfferRec in b.offers: v[0..4], then wire | change << 8 in the bits of
+// the sixth double.
+constexpr int kOfferRec = 6;
+
+__device__ __forceinline__ void offer_store(const DagBatchDev &b, int e, int t, const Offer &o) {
+    double2 *r = reinterpret_cast<double2 *>(b.offers + ((int64_t)e * 9 + (t - 1)) * kOfferRec);
+    r[0] = make_double2(o.v[0], o.v[1]);
+    r[1] = make_double2(o.v[2], o.v[3]);
+    r[2] = make_double2(o.v[4], __longlong_as_double((long long)(o.wire | o.change << 8)));
+}
+
+template <bool S>
+__device__ __forceinline__ void offer_fetch(const Dag<S> &D, int e, int t, Offer &o) {
+    const double2 *r = reinterpret_cast<const double2 *>(D.b.offers + ((int64_t)e * 9 + (t - 1)) * kOfferRec);
+    const double2 a = r[0], c = r[1], d = r[2];
+    o.v[0] = a.x; o.v[1] = a.y; o.v[2] = c.x; o.v[3] = c.y; o.v[4] = d.x;
+    const unsigned m = (unsigned)__double_as_longlong(d.y);
+    o.wire = m & 0xff;
+    o.change = m >> 8;
+    o.dst = ((int64_t)D.coff(D.par(e)) + D.slot(e)) * kML + t;
+}
+
+// the offer of pair (e, t): computed, or fetched where the net is staged
+template <bool S>
+__device__ __forceinline__ void offer_get(const GridDev &g, const Dag<S> &D, int x, int y, int e, int t, Offer &o) {
+    if (S)
+        offer_fetch(D, e, t, o);
+    else
+        offer_load(g, D, x, y, e, t, o);
 }
 
 // the minimum packed offer of the pair over its source layers, then atomicMin
@@ -194,7 +298,8 @@ __device__ __forceinline__ void offer_send(const DagBatchDev &b, const Offer &o,
 #pragma unroll
     for (int q = 0; q < 5; q++) {
         const int layer = 2 - (t & 1) + 2 * q;
-        if (layer >= kML || !(o.v[q] < kNone)) continue;
+        if (layer >= kML) continue;
+        if (!((o.wire >> q) & 1) && !(((o.change >> q) & 1) && o.v[q] < kInf)) continue;
         const double c2 = cost[layer] + o.v[q];
         const int choice = t == layer ? 82 : (layer - 1) * 9 + (t - 1);
         const unsigned long long nv = pack((float)c2, node * 100 + choice);
@@ -217,57 +322,69 @@ __device__ __forceinline__ void offer_send(const DagBatchDev &b, const Offer &o,
 // child c's first minimum over [low, J] of that winner.  The warp computes the
 // 45 candidates row by row (lane = low, the same additions in the same order),
 // the suffix minima of each row, and per layer the minimum over rows.
-__device__ void dp_node_warp(const GridDev &g, const DagBatchDev &b, int node, int lane, NodeScratch &s) {
-    const int X = g.X, Y = g.Y, XY = X * Y;
-    const int v = b.nodes[node];
-    const int fixed_low = 1 + v / XY;
+template <bool S>
+__device__ void dp_node_warp(const GridDev &g, const Dag<S> &D, int node, int lane, NodeScratch &s) {
+    const DagBatchDev &b = D.b;
+    const NodePos np = D.pos(node);
+    const int fixed_low = 1 + np.l;
     const int fixed_high = fixed_low == 10 ? 0 : fixed_low;
-    const int x = v / Y % X, y = v % Y;
-    const int cb = b.child_off[node], cn = b.child_off[node + 1] - cb;
+    const int x = np.x, y = np.y;
+    const int cb = D.coff(node), cn = D.coff(node + 1) - cb;
     __syncwarp();  // the previous node's scratch is no longer read
-    {
-        // the children's atomics landed in L2: read past L1
-        const unsigned long long *pk = b.packed + (int64_t)cb * kML;
-        for (int i = lane; i < cn * 9; i += 32) {
-            const int c = i / 9, layer = 1 + i % 9;
-            s.pk[c][layer] = __ldcg(pk + c * kML + layer);
-        }
-        if (lane < 8) s.vcol[lane] = g.vcost[cell_at(g, lane, x, y)];
+    // every global load of the node first, so that their latencies overlap:
+    // the children's packed entries (their atomics landed in L2: read past
+    // L1), the via costs of the node's column, and the parent-side inputs
+    // (which do not depend on the DP)
+    const unsigned long long *pk = b.packed + (int64_t)cb * kML;
+    unsigned long long pkv[3];  // entries lane + 32 r of the cn * 9 <= 90
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        const int i = lane + 32 * r;
+        if (i < cn * 9) pkv[r] = __ldcg(pk + (i / 9) * kML + 1 + i % 9);
     }
-    // the parent-side inputs do not depend on the DP: issue their loads now
-    const int pb = b.par_off[node], pn = b.par_off[node + 1] - pb;
+    double vc = 0;
+    if (lane < 8) vc = g.vcost[cell_at(g, lane, x, y)];
+    const int pb = D.poff(node), pn = D.poff(node + 1) - pb;
     Offer o;
-    if (lane < pn * 9) offer_load(g, b, node, x, y, pb + lane / 9, 1 + lane % 9, o);
+    if (lane < pn * 9) offer_get(g, D, x, y, pb + lane / 9, 1 + lane % 9, o);
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        const int i = lane + 32 * r;
+        if (i < cn * 9) s.pk[i / 9][1 + i % 9] = pkv[r];
+    }
+    if (lane < 8) s.vcol[lane] = vc;
     __syncwarp();
     if (lane < 9) {
+        // row `low`: T(low, J) = via(low, J) + the children's first minima
+        // over [low, J], added child by child in child order (the
+        // reference's order); J < low or low > fixed_low take no part
         const int low = lane + 1;
+        const bool on = low <= fixed_low;
         double T[kML];
-        double minc[kML];
-#pragma unroll
-        for (int c = 0; c < kML; c++) minc[c] = kInf;
         double via = 0;
 #pragma unroll
         for (int J = 1; J < kML; J++) {
-            T[J] = kNone;
-            if (J >= low && low <= fixed_low) {
-                if (J > low) via += s.vcol[J - 2];
-                double t = via;
+            if (on && J > low) via += s.vcol[J - 2];
+            T[J] = via;
+        }
+        for (int c = 0; c < cn; c++) {
+            const unsigned long long *row = s.pk[c];
+            double m = kInf;
 #pragma unroll
-                for (int c = 0; c < kML; c++) {
-                    if (c < cn) {
-                        const double cc = packed_cost(s.pk[c][J]);
-                        if (cc < minc[c]) minc[c] = cc;
-                        t += minc[c];
-                    }
+            for (int J = 1; J < kML; J++) {
+                if (on && J >= low) {
+                    const double cc = packed_cost(row[J]);
+                    if (cc < m) m = cc;
+                    T[J] += m;
                 }
-                if (J >= fixed_high && t < kInf) T[J] = t;
             }
         }
         double r = kNone;
         int rj = -1;
 #pragma unroll
         for (int J = kML - 1; J >= 1; J--) {
-            if (T[J] < kNone && T[J] <= r) { r = T[J]; rj = J; }  // equal: the smaller top layer
+            const bool cand = on && J >= low && J >= fixed_high && T[J] < kInf;
+            if (cand && T[J] <= r) { r = T[J]; rj = J; }  // equal: the smaller top layer
             s.row[low][J] = r;
             s.row_at[low][J] = (signed char)rj;
         }
@@ -309,115 +426,122 @@ __device__ void dp_node_warp(const GridDev &g, const DagBatchDev &b, int node, i
     }
     for (int i = lane + 32; i < pn * 9; i += 32) {
         Offer o2;
-        offer_load(g, b, node, x, y, pb + i / 9, 1 + i % 9, o2);
+        offer_get(g, D, x, y, pb + i / 9, 1 + i % 9, o2);
         offer_send(b, o2, s.cost, node);
     }
     if (lane < pn * 9) offer_send(b, o, s.cost, node);
 }
 
-__device__ __forceinline__ void stage2(const DagBatchDev &b, int node, int a, int c, int *err) {
-    int k = b.stage_cnt[node];
+template <bool S>
+__device__ __forceinline__ void stage2(const Dag<S> &D, int node, int a, int c, int *err) {
+    int *cnt = D.scnt(node);
+    const int k = *cnt;
     if (k + 2 > 8) { set_error(err, ERR_CAPACITY); return; }
-    b.stage[(int64_t)node * 8 + k] = a;
-    b.stage[(int64_t)node * 8 + k + 1] = c;
-    b.stage_cnt[node] = k + 2;
+    D.b.stage[(int64_t)node * 8 + k] = a;
+    D.b.stage[(int64_t)node * 8 + k + 1] = c;
+    *cnt = k + 2;
 }
 
 // get_routing_tree_layer_change_cuda for one node
-__device__ void trace_node(const GridDev &g, const DagBatchDev &b, int node, int stamp) {
+template <bool S>
+__device__ void trace_node(const GridDev &g, const Dag<S> &D, int node, int stamp) {
+    const DagBatchDev &b = D.b;
     const int X = g.X, Y = g.Y, XY = X * Y;
-    const int pb = b.par_off[node], pn = b.par_off[node + 1] - pb;
-    const int v = b.nodes[node];
-    const int l = v / XY, cx = v / Y % X, cy = v % Y;
-    const unsigned long long *best = b.best_path + (int64_t)b.child_off[node] * kML;
-    int *lo = b.layer_out;
+    const int pb = D.poff(node), pn = D.poff(node + 1) - pb;
+    const NodePos np = D.pos(node);
+    const int l = np.l, cx = np.x, cy = np.y;
+    const unsigned long long *best = b.best_path + (int64_t)D.coff(node) * kML;
+    int *lo = D.lo(node);
     if (pn == 0) {
         int ml = 0;
         double mc = b.costs[(int64_t)node * kML];
         for (int layer = 1; layer < kML; layer++)
             if (b.costs[(int64_t)node * kML + layer] < mc) { mc = b.costs[(int64_t)node * kML + layer]; ml = layer; }
-        lo[node] = ml;
+        *lo = ml;
     } else {
         int par_layer = -1, par_idx = -1, par_seq = -1;
         for (int pi = 0; pi < pn; pi++) {
             const int e = pb + pi;
-            const int pnode = b.par[e];
-            if (lo[pnode] > 0) {
+            const int pnode = D.par(e);
+            if (*D.lo(pnode) > 0) {
                 par_idx = pnode;
                 par_seq = pi;
-                par_layer = lo[pnode];
-                const int slot = b.child_slot[pb + par_seq];
-                const unsigned long long path = b.best_path[(int64_t)b.child_off[par_idx] * kML + slot * kML + par_layer];
+                par_layer = *D.lo(pnode);
+                const int slot = D.slot(pb + par_seq);
+                const unsigned long long path = b.best_path[(int64_t)D.coff(par_idx) * kML + slot * kML + par_layer];
                 const unsigned long long cid = path / kML / 100;
                 const unsigned long long ch = (path / kML) % 100;
                 if (cid == (unsigned long long)node) {
-                    lo[node] = ch == 82 ? (int)(path % kML) : (int)(ch / 9 + 1);
-                    const int pv = b.nodes[par_idx];
-                    const int px = pv / Y % X, py = pv % Y;
-                    const int L1 = lo[node] - 1;
+                    *lo = ch == 82 ? (int)(path % kML) : (int)(ch / 9 + 1);
+                    const NodePos pp = D.pos(par_idx);
+                    const int px = pp.x, py = pp.y;
+                    const int L1 = *lo - 1;
                     if (px == cx && cy != py) {
                         if (ch == 82) {
                             add_wire(g, L1, px, px, min(py, cy), max(py, cy), stamp);
-                            stage2(b, node, L1 * XY + px * Y + min(py, cy), L1 * XY + px * Y + max(py, cy), g.err);
+                            stage2(D, node, L1 * XY + px * Y + min(py, cy), L1 * XY + px * Y + max(py, cy), g.err);
                         } else {
                             const int fl = (int)(ch / 9), tl = (int)(ch % 9);
                             const int cp = b.best_change[(int64_t)e * 81 + fl * 9 + tl];
                             if (cp <= min(cy, py) || cp >= max(cy, py)) { set_error(g.err, ERR_STATE); return; }
                             add_wire(g, fl, cx, cx, min(cy, cp), max(cy, cp), stamp);
                             add_wire(g, tl, cx, cx, min(py, cp), max(py, cp), stamp);
-                            stage2(b, node, fl * XY + cx * Y + min(cy, cp), fl * XY + cx * Y + max(cy, cp), g.err);
-                            stage2(b, node, min(fl, tl) * XY + cx * Y + cp, max(fl, tl) * XY + cx * Y + cp, g.err);
-                            stage2(b, node, tl * XY + cx * Y + min(py, cp), tl * XY + cx * Y + max(py, cp), g.err);
+                            stage2(D, node, fl * XY + cx * Y + min(cy, cp), fl * XY + cx * Y + max(cy, cp), g.err);
+                            stage2(D, node, min(fl, tl) * XY + cx * Y + cp, max(fl, tl) * XY + cx * Y + cp, g.err);
+                            stage2(D, node, tl * XY + cx * Y + min(py, cp), tl * XY + cx * Y + max(py, cp), g.err);
                         }
                     } else if (py == cy && cx != px) {
                         if (ch == 82) {
                             add_wire(g, L1, min(px, cx), max(px, cx), py, py, stamp);
-                            stage2(b, node, L1 * XY + min(px, cx) * Y + py, L1 * XY + max(px, cx) * Y + py, g.err);
+                            stage2(D, node, L1 * XY + min(px, cx) * Y + py, L1 * XY + max(px, cx) * Y + py, g.err);
                         } else {
                             const int fl = (int)(ch / 9), tl = (int)(ch % 9);
                             const int cp = b.best_change[(int64_t)e * 81 + fl * 9 + tl];
                             if (cp <= min(cx, px) || cp >= max(cx, px)) { set_error(g.err, ERR_STATE); return; }
                             add_wire(g, fl, min(cx, cp), max(cx, cp), cy, cy, stamp);
                             add_wire(g, tl, min(px, cp), max(px, cp), cy, cy, stamp);
-                            stage2(b, node, fl * XY + min(cx, cp) * Y + cy, fl * XY + max(cx, cp) * Y + cy, g.err);
-                            stage2(b, node, min(fl, tl) * XY + cp * Y + cy, max(fl, tl) * XY + cp * Y + cy, g.err);
-                            stage2(b, node, tl * XY + min(px, cp) * Y + cy, tl * XY + max(px, cp) * Y + cy, g.err);
+                            stage2(D, node, fl * XY + min(cx, cp) * Y + cy, fl * XY + max(cx, cp) * Y + cy, g.err);
+                            stage2(D, node, min(fl, tl) * XY + cp * Y + cy, max(fl, tl) * XY + cp * Y + cy, g.err);
+                            stage2(D, node, tl * XY + min(px, cp) * Y + cy, tl * XY + max(px, cp) * Y + cy, g.err);
                         }
                     }
                     break;
                 } else {
-                    lo[node] = -1;
+                    *lo = -1;
                 }
             }
         }
-        if (par_layer == -1) { lo[node] = -1; return; }
-        const int slot = b.child_slot[pb + par_seq];
-        const unsigned long long path = b.best_path[(int64_t)b.child_off[par_idx] * kML + slot * kML + par_layer];
-        if (path / kML / 100 != (unsigned long long)node) { lo[node] = -1; return; }
+        if (par_layer == -1) { *lo = -1; return; }
+        const int slot = D.slot(pb + par_seq);
+        const unsigned long long path = b.best_path[(int64_t)D.coff(par_idx) * kML + slot * kML + par_layer];
+        if (path / kML / 100 != (unsigned long long)node) { *lo = -1; return; }
     }
-    const int cn = b.child_off[node + 1] - b.child_off[node];
+    const int cn = D.coff(node + 1) - D.coff(node);
+    const int lon = *lo;
     int mnl = l + 1;
     int mxl = (l + 1) == kML ? 1 : mnl;
-    mnl = min(mnl, lo[node]);
-    mxl = max(mxl, lo[node]);
+    mnl = min(mnl, lon);
+    mxl = max(mxl, lon);
     for (int c = 0; c < cn; c++) {
-        const int lc = (int)(best[c * kML + lo[node]] % kML);
+        const int lc = (int)(best[c * kML + lon] % kML);
         mnl = min(lc, mnl);
         mxl = max(lc, mxl);
     }
-    if (mnl < mxl) stage2(b, node, (mnl - 1) * XY + cx * Y + cy, (mxl - 1) * XY + cx * Y + cy, g.err);
+    if (mnl < mxl) stage2(D, node, (mnl - 1) * XY + cx * Y + cy, (mxl - 1) * XY + cx * Y + cy, g.err);
 }
 
 // route record of net k in DAG node order, written by one warp
-__device__ void compact_net(const GridDev &g, const DagBatchDev &b, int k, int lane) {
+template <bool S>
+__device__ void compact_net(const GridDev &g, const Dag<S> &D, int k, int lane) {
+    const DagBatchDev &b = D.b;
     const int net = b.net_ids[k];
     int *r = b.routes + b.route_off[net];
     const int cap = b.route_cap[net];
-    const int n0 = b.net_node_off[k], n1 = b.net_node_off[k + 1];
+    const int n0 = D.L.n0, n1 = D.L.n0 + D.L.n;
     int base = 1;
     for (int c0 = n0; c0 < n1; c0 += 32) {
         const int node = c0 + lane;
-        const int cnt = node < n1 ? b.stage_cnt[node] : 0;
+        const int cnt = node < n1 ? *D.scnt(node) : 0;
         int inc = cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -434,39 +558,94 @@ __device__ void compact_net(const GridDev &g, const DagBatchDev &b, int k, int l
     if (lane == 0) r[0] = base <= cap ? base : 1;
 }
 
-// one CTA of W warps per net: initialisation, DP levels deepest first, trace
-// levels root first, compaction.  Sizes: 0 every net, 1 nets of at most
-// kSmallNodes nodes, 2 the larger ones (small DAGs have narrow levels, so a
-// 2-warp CTA leaves fewer warps waiting at the level barriers and more CTAs
-// fit an SM)
-template <int W, int Sizes>
-__global__ void __launch_bounds__(32 * W) dag_net_kernel(GridDev g, DagBatchDev b, int stamp) {
-    chain_begin();
+// one net: initialisation (and the copy into shared memory when staged), DP
+// levels deepest first, trace levels root first, compaction
+template <int W, bool S>
+__device__ void route_net(const GridDev &g, const DagBatchDev &b, int k, const NetLoc &L, int nl, int stamp,
+                          NodeScratch *scr) {
     constexpr int kThreadsW = 32 * W;
-    __shared__ NodeScratch scr[W];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    for (int k = blockIdx.x; k < b.n_nets; k += gridDim.x) {
-        const int n0 = b.net_node_off[k], n1 = b.net_node_off[k + 1];
-        if ((Sizes == 1 && n1 - n0 > kSmallNodes) || (Sizes == 2 && n1 - n0 <= kSmallNodes)) continue;
-        const int64_t s0 = (int64_t)b.child_off[n0] * kML, s1 = (int64_t)b.child_off[n1] * kML;
-        for (int64_t i = s0 + tid; i < s1; i += kThreadsW) b.packed[i] = kInitPacked;
+    const Dag<S> D{b, L, g.X * g.Y, g.Y};
+    const int n0 = L.n0, n1 = L.n0 + L.n;
+    const int64_t s0 = (int64_t)b.child_off[n0] * kML, s1 = (int64_t)b.child_off[n1] * kML;
+    for (int64_t i = s0 + tid; i < s1; i += kThreadsW) b.packed[i] = kInitPacked;
+    if (S) {
+        const int n = L.n, m = L.m, XY = g.X * g.Y;
+        for (int i = tid; i < n; i += kThreadsW) {
+            const int v = b.nodes[n0 + i], l = v / XY, q = v - l * XY, x = q / g.Y;
+            s_dag[i] = (l << 28) | (x << 14) | (q - x * g.Y);
+            s_dag[3 * n + 2 + i] = b.level_nodes[n0 + i];
+            s_dag[4 * n + 2 + i] = -1;
+            s_dag[5 * n + 2 + i] = 0;
+        }
+        for (int i = tid; i <= n; i += kThreadsW) {
+            s_dag[n + i] = b.child_off[n0 + i];
+            s_dag[2 * n + 1 + i] = b.par_off[n0 + i];
+        }
+        for (int j = tid; j < m; j += kThreadsW) {
+            s_dag[6 * n + 2 + j] = b.par[L.e0 + j];
+            s_dag[6 * n + 2 + m + j] = b.child_slot[L.e0 + j];
+        }
+        for (int d = tid; d <= nl; d += kThreadsW) s_dag[6 * n + 2 + 2 * m + d] = b.level_off[L.l0 + d];
+    } else {
         for (int v = n0 + tid; v < n1; v += kThreadsW) {
             b.layer_out[v] = -1;
             b.stage_cnt[v] = 0;
         }
+    }
+    __syncthreads();
+    if (S) {
+        // what no DP result decides, before the DP: each node's via-cost
+        // column into L2, and the offer record of every (parent edge, target
+        // layer) pair
+        for (int i = tid; i < L.n; i += kThreadsW) {
+            const NodePos p = D.pos(n0 + i);
+            for (int l = 0; l < kML - 2; l++) prefetch_l2(g.vcost + cell_at(g, l, p.x, p.y));
+        }
+        for (int i = tid; i < L.m * 9; i += kThreadsW) {
+            const int e = L.e0 + i / 9, t = 1 + i % 9;
+            const NodePos p = D.pos(b.edge_child[e]);
+            Offer o;
+            offer_load(g, D, p.x, p.y, e, t, o);
+            offer_store(b, e, t, o);
+        }
         __syncthreads();
+    }
+    for (int d = nl - 1; d >= 0; d--) {
+        const int a = D.loff(d), e = D.loff(d + 1);
+        for (int s = a + warp; s < e; s += W) dp_node_warp(g, D, D.lev(s), lane, scr[warp]);
+        __syncthreads();
+    }
+    for (int d = 0; d < nl; d++) {
+        const int a = D.loff(d), e = D.loff(d + 1);
+        for (int s = a + tid; s < e; s += kThreadsW) trace_node(g, D, D.lev(s), stamp);
+        __syncthreads();
+    }
+    if (warp == 0) compact_net(g, D, k, lane);
+}
+
+// one CTA of W warps per net.  Sizes: 0 every net, 1 nets of at most
+// split_at nodes, 2 the larger ones (a DAG's level width grows with its size:
+// a CTA of fewer warps leaves fewer of them waiting at the level barriers of a
+// small DAG, one of more warps takes the wide levels of a large DAG in fewer
+// rounds).  A net of at most cap_n nodes, cap_m parent edges and
+// kStageLevels - 1 levels is staged in shared memory (dynamic, staged_ints of
+// the caps).  At most 80 registers a thread: 12 CTAs of 2 warps, 3 of 8 warps
+// or one of 16 warps beside one of 8 per SM.
+template <int W, int Sizes>
+__global__ void __maxnreg__(80) dag_net_kernel(GridDev g, DagBatchDev b, int stamp, int cap_n, int cap_m, int split_at) {
+    chain_begin();
+    __shared__ NodeScratch scr[W];
+    for (int k = blockIdx.x; k < b.n_nets; k += gridDim.x) {
+        const int n0 = b.net_node_off[k], n1 = b.net_node_off[k + 1];
+        if ((Sizes == 1 && n1 - n0 > split_at) || (Sizes == 2 && n1 - n0 <= split_at)) continue;
         const int l0 = b.net_level_off[k], nl = b.net_level_off[k + 1] - l0 - 1;
-        for (int d = nl - 1; d >= 0; d--) {
-            const int a = b.level_off[l0 + d], e = b.level_off[l0 + d + 1];
-            for (int s = a + warp; s < e; s += W) dp_node_warp(g, b, b.level_nodes[s], lane, scr[warp]);
-            __syncthreads();
-        }
-        for (int d = 0; d < nl; d++) {
-            const int a = b.level_off[l0 + d], e = b.level_off[l0 + d + 1];
-            for (int s = a + tid; s < e; s += kThreadsW) trace_node(g, b, b.level_nodes[s], stamp);
-            __syncthreads();
-        }
-        if (warp == 0) compact_net(g, b, k, lane);
+        const int e0 = b.par_off[n0];
+        const NetLoc L{n0, e0, l0, n1 - n0, b.par_off[n1] - e0};
+        if (L.n <= cap_n && L.m <= cap_m && nl < kStageLevels)
+            route_net<W, true>(g, b, k, L, nl, stamp, scr);
+        else
+            route_net<W, false>(g, b, k, L, nl, stamp, scr);
         __syncthreads();
     }
 }
@@ -494,7 +673,7 @@ void dag_levels(int n, const int *node_off, const int *depth, std::vector<int> &
 }
 
 int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStream_t s, cudaStream_t aux,
-                     cudaEvent_t fork, cudaEvent_t join, int split_nets) {
+                     cudaEvent_t fork, cudaEvent_t join, int split_nets, int stage_nodes, int big_nodes) {
     if (b.n_nodes <= 0 || b.n_nets <= 0) return 0;
     int launches = 0;
     if (b.n_edges > 0) {
@@ -502,17 +681,47 @@ int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStre
                        dim3(32 * kEdgeWarps), 0, s, g, b);
         launches++;
     }
-    if (!aux || b.n_nets < split_nets) {
-        launch_chained(dag_net_kernel<kDagWarps, 0>, dim3(b.n_nets), dim3(kDagThreads), 0, s, g, b, stamp);
+    // staging capacity: the batch's largest net (rounded up, so that few
+    // distinct sizes occur), within the limit; none without room for offer
+    // records or where positions do not fit their packed form
+    const int lim = b.offers && g.X <= kStageMaxSide && g.Y <= kStageMaxSide
+                        ? std::max(0, std::min(stage_nodes, kMaxStageNodes))
+                        : 0;
+    const int cap_n = lim ? std::min(lim, b.max_net_nodes > 0 ? (b.max_net_nodes + 63) / 64 * 64 : lim) : 0;
+    const int cap_m = lim ? std::min(2 * lim, b.max_net_edges > 0 ? (b.max_net_edges + 127) / 128 * 128 : 2 * lim) : 0;
+    const size_t smem = cap_n ? (size_t)staged_ints(cap_n, cap_m) * sizeof(int) : 0;
+    const bool many = aux && b.n_nets >= split_nets;
+    const bool big = aux && !many && big_nodes > 0 && b.max_net_nodes > big_nodes;
+    if (!many && !big) {
+        kernel_setup((const void *)dag_net_kernel<kDagWarps, 0>, kDagThreads, smem);
+        launch_chained(dag_net_kernel<kDagWarps, 0>, dim3(b.n_nets), dim3(kDagThreads), smem, s, g, b, stamp, cap_n,
+                       cap_m, 0);
         return launches + 1;
     }
-    // a batch of many nets: the large nets' CTAs on the side stream, beside
-    // the small nets' 2-warp CTAs (the nets of a batch share no state); a
-    // smaller batch is bound by its largest net and gains nothing from it
+    // two launches over the batch, each taking the nets of its size class
+    // (the nets of a batch share no state): the larger nets' CTAs on the side
+    // stream, beside the smaller nets' CTAs
     cudaEventRecord(fork, s);
     cudaStreamWaitEvent(aux, fork, 0);
-    dag_net_kernel<kDagWarps, 2><<<b.n_nets, kDagThreads, 0, aux>>>(g, b, stamp);
-    dag_net_kernel<kSmallWarps, 1><<<b.n_nets, 32 * kSmallWarps, 0, s>>>(g, b, stamp);
+    if (many) {
+        // a batch of many nets: the DAGs of at most kSmallNodes nodes in
+        // 2-warp CTAs, so that more of them are in flight
+        const int small_n = std::min(cap_n, kSmallNodes);
+        const int small_m = std::min(cap_m, 2 * kSmallNodes);
+        const size_t smem_small = small_n ? (size_t)staged_ints(small_n, small_m) * sizeof(int) : 0;
+        kernel_setup((const void *)dag_net_kernel<kDagWarps, 2>, kDagThreads, smem);
+        kernel_setup((const void *)dag_net_kernel<kSmallWarps, 1>, 32 * kSmallWarps, smem_small);
+        dag_net_kernel<kDagWarps, 2><<<b.n_nets, kDagThreads, smem, aux>>>(g, b, stamp, cap_n, cap_m, kSmallNodes);
+        dag_net_kernel<kSmallWarps, 1><<<b.n_nets, 32 * kSmallWarps, smem_small, s>>>(g, b, stamp, small_n, small_m,
+                                                                                      kSmallNodes);
+    } else {
+        // a batch with DAGs of more than big_nodes nodes: those in 16-warp
+        // CTAs, whose wide levels bound the batch
+        kernel_setup((const void *)dag_net_kernel<kBigWarps, 2>, 32 * kBigWarps, smem);
+        kernel_setup((const void *)dag_net_kernel<kDagWarps, 1>, kDagThreads, smem);
+        dag_net_kernel<kBigWarps, 2><<<b.n_nets, 32 * kBigWarps, smem, aux>>>(g, b, stamp, cap_n, cap_m, big_nodes);
+        dag_net_kernel<kDagWarps, 1><<<b.n_nets, kDagThreads, smem, s>>>(g, b, stamp, cap_n, cap_m, big_nodes);
+    }
     cudaEventRecord(join, aux);
     cudaStreamWaitEvent(s, join, 0);
     return launches + 2;

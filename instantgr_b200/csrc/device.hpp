@@ -139,6 +139,12 @@ struct DagBatchDev {
     const int64_t *route_off = nullptr;
     const int *route_cap = nullptr;
     int *routes = nullptr;
+    // the batch's largest net in nodes and in parent edges (0: not known);
+    // they size the shared memory that stages a net's DAG
+    int max_net_nodes = 0, max_net_edges = 0;
+    // 54 doubles per parent edge: the offer records of staged nets (null: no
+    // net is staged)
+    double *offers = nullptr;
 };
 // per-net level lists of n nets whose nodes are node_off[k]..node_off[k+1]:
 // level_nodes holds each net's nodes by depth (stable), level_off the depth_k + 1
@@ -151,9 +157,13 @@ void dag_levels(int n, const int *node_off, const int *depth, std::vector<int> &
 // Batches of `split_nets` nets or more (4096 by default) run the DAGs of at
 // most 64 nodes in 2-warp CTAs on `s` beside the larger ones on `aux`
 // (forked and joined through the two events); smaller batches, or no `aux`,
-// run one launch.
+// run one launch.  Nets of at most `stage_nodes` nodes (up to 4096; 0: none)
+// keep their DAG arrays in shared memory while they are routed.  In smaller
+// batches with `aux`, DAGs of more than `big_nodes` nodes (0: none) run in
+// 16-warp CTAs on `aux` beside the others.
 int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStream_t s, cudaStream_t aux = nullptr,
-                     cudaEvent_t fork = nullptr, cudaEvent_t join = nullptr, int split_nets = 4096);
+                     cudaEvent_t fork = nullptr, cudaEvent_t join = nullptr, int split_nets = 4096,
+                     int stage_nodes = 1024, int big_nodes = 0);
 
 constexpr int kRouteLayers = 9;
 

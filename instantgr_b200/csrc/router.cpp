@@ -1263,13 +1263,15 @@ bool Router::rrr_pass(int iter) {
             for (int b = 0; b < B; b++) {
                 DagBatchInfo &f = bi[b];
                 f = acc;
-                f.n = f.e = f.slots = 0;
+                f.n = f.e = f.slots = f.mx_n = f.mx_e = 0;
                 int lv = 0;
                 for (int id : batches[b]) {
                     const int k = dag_slot[id];
                     const DagNet &dn = dag[k];
                     f.n += (int)dn.nodes.size();
                     f.e += (int)dn.par_nodes.size();
+                    f.mx_n = std::max(f.mx_n, (int)dn.nodes.size());
+                    f.mx_e = std::max(f.mx_e, (int)dn.par_nodes.size());
                     f.slots += net_slots[k];
                     lv += net_levels[k] + 1;
                     // new route record of the net (appended)
@@ -1376,7 +1378,7 @@ bool Router::rrr_pass(int iter) {
     }
     int mn = 1, me = 1, ms = 1;
     for (auto &f : bi) { mn = std::max(mn, f.n); me = std::max(me, f.e); ms = std::max(ms, f.slots); }
-    dg_costs.alloc((size_t)mn * 10); dg_cedges.alloc((size_t)me * 81);
+    dg_costs.alloc((size_t)mn * 10); dg_cedges.alloc((size_t)me * 81); dg_offers.alloc((size_t)me * 54);
     dg_best.alloc((size_t)ms * 10); dg_packed.alloc((size_t)ms * 10);
     dg_bchange.alloc((size_t)me * 81); dg_lout.alloc(mn); dg_stage.alloc((size_t)mn * 8); dg_scnt.alloc(mn);
     for (size_t b = 0; b < bi.size(); b++) {
@@ -1403,8 +1405,10 @@ bool Router::rrr_pass(int iter) {
         db.best_change = dg_bchange.p; db.layer_out = dg_lout.p; db.stage = dg_stage.p; db.stage_cnt = dg_scnt.p;
         db.route_off = d_route_off.p; db.route_cap = d_route_cap.p; db.routes = routes.p;
         kt.begin(KC_DAG);
+        db.max_net_nodes = f.mx_n; db.max_net_edges = f.mx_e; db.offers = dg_offers.p;
         const int nl = launch_dag_route(go.g, db, s2, s, s_cls[0], ev_fork, ev_join[0],
-                                        test_hooks().dag_split_nets.load());
+                                        test_hooks().dag_split_nets.load(), test_hooks().dag_stage_nodes.load(),
+                                        test_hooks().dag_big_nodes.load());
         kt.end(KC_DAG);
         kt.begin(KC_WIRE_COMMIT);
         launch_wire_commit(go.g, s2, true, s);
@@ -1600,12 +1604,14 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
         for (int b = 0; b < B; b++) {
             DagBatchInfo &f = bi[b];
             f = acc;
-            f.n = f.e = f.slots = 0;
+            f.n = f.e = f.slots = f.mx_n = f.mx_e = 0;
             int64_t lv = 0;
             for (int i : bpos[b]) {
                 const int id = of_nets[i];
                 f.n += m_of(i);
                 f.e += e_of(i);
+                f.mx_n = std::max(f.mx_n, m_of(i));
+                f.mx_e = std::max(f.mx_e, e_of(i));
                 f.slots += s_of(i);
                 lv += d_of(i) + 1;
                 // new route record of the net (appended)

@@ -89,6 +89,7 @@ struct DevBuf {
 // its node, edge and child-slot counts.
 struct DagBatchInfo {
     int nb, eb, pb, lb, nnb, nets, n, e, slots;
+    int mx_n, mx_e;  // the largest net's nodes and parent edges
 };
 
 // Detour DAGs built on the device (dagbuild.cu) for a list of routing nets,
@@ -261,7 +262,7 @@ struct Router {
     DevBuf<float> d_xsum, d_ysum;
     DevBuf<int> dg_nodes, dg_paroff, dg_par, dg_cslot, dg_echild, dg_childoff, dg_leveloff, dg_levelnodes, dg_nno,
         dg_netlvl, dg_ids, dg_bchange, dg_lout, dg_stage, dg_scnt;
-    DevBuf<double> dg_costs, dg_cedges;
+    DevBuf<double> dg_costs, dg_cedges, dg_offers;
     DevBuf<unsigned long long> dg_best, dg_packed;
     // arenas of the DAG arrays (declared before the DAGs: freed after them)
     std::vector<std::unique_ptr<std::pmr::monotonic_buffer_resource>> dag_arenas;

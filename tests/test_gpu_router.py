@@ -188,13 +188,15 @@ def test_route_records_after_rerouting(tmp_path):
         assert np.all(via | (xa == xb) | (ya == yb))
 
 
-@pytest.mark.parametrize("hook,values", [("HOOK_SHAPE_DEDUPE", (0, 1)), ("HOOK_COLOR_KEEP_MIN_NETS", (2000000, 1))])
+@pytest.mark.parametrize("hook,values", [("HOOK_SHAPE_DEDUPE", (0, 1)), ("HOOK_COLOR_KEEP_MIN_NETS", (2000000, 1)),
+                                         ("HOOK_DAG_STAGE_NODES", (0, 1024))])
 def test_colouring_variants_give_the_same_routing(tmp_path, hook, values):
     """Conflict points and claims kept once per net or with every repetition,
-    and the round-0 claim map cleared per batch or kept up to date: the same
-    phase-1 batches, and the same demand after three rip-up passes (whose
-    colourings use the same variants).  The order of the nets inside a batch
-    comes from an atomic scatter and does not matter (they share no state)."""
+    the round-0 claim map cleared per batch or kept up to date, and the DAG DP
+    with its DAGs in global or in shared memory: the same phase-1 batches, and
+    the same demand after three rip-up passes (whose colourings use the same
+    variants).  The order of the nets inside a batch comes from an atomic
+    scatter and does not matter (they share no state)."""
     cap, net = str(tmp_path / "d.cap"), str(tmp_path / "d.net")
     ig.generate(1, 5, 0.2, cap, net)
     res = []

@@ -274,3 +274,21 @@ def test_router_refuses_to_write_or_evaluate_before_routing(tmp_path):
         r.write(str(tmp_path / "t.out"))
     assert e.value.code == -7
     r.close()
+
+
+@pytest.mark.parametrize("key,bad,good", [("HOOK_DAG_STAGE_NODES", (-1, 4097), (0, 4096)),
+                                          ("HOOK_DAG_SPLIT_NETS", (0, -5), (1, 4096)),
+                                          ("HOOK_DAG_BIG_NODES", (-1,), (0, 200)),
+                                          ("HOOK_WAIT_NS", (-1,), (0, 2_000_000_000))])
+def test_test_hooks_check_their_ranges(key, bad, good):
+    """Test hooks take values in their documented ranges and refuse others with
+    IGR_ERR_INVALID, leaving the setting unchanged (no GPU is involved)."""
+    try:
+        for v in bad:
+            with pytest.raises(ig.IgrError) as e:
+                ig.set_test_hook(getattr(ig, key), v)
+            assert e.value.code == ig.IGR_ERR_INVALID
+        for v in good:
+            ig.set_test_hook(getattr(ig, key), v)
+    finally:
+        ig.set_test_hook(ig.HOOK_RESET)
