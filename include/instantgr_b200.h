@@ -185,12 +185,8 @@ const char *igr_last_error(const igr_ctx *c);
  *                             every repetition (0); the batches are the same
  *   IGR_HOOK_DAG_STAGE_NODES  the DAG DP keeps the DAG of a net of at most
  *                             this many nodes (0..4096, default 1024; 0: none)
- *                             in shared memory while it routes it; the routes
- *                             are the same
- *   IGR_HOOK_DAG_BIG_NODES    DAG batches below IGR_HOOK_DAG_SPLIT_NETS nets run
- *                             their DAGs of more than this many nodes in
- *                             16-warp CTAs beside the others on a second
- *                             stream (default 0: none); the routes are the same */
+ *                             in shared memory while it routes it, where it
+ *                             fits; the routes are the same */
 enum {
     IGR_HOOK_RESET = 0,
     IGR_HOOK_WAIT_NS = 1,
@@ -201,7 +197,6 @@ enum {
     IGR_HOOK_COLOR_KEEP_MIN_NETS = 6,
     IGR_HOOK_SHAPE_DEDUPE = 7,
     IGR_HOOK_DAG_STAGE_NODES = 8,
-    IGR_HOOK_DAG_BIG_NODES = 9,
 };
 int igr_test_hook(int key, int64_t value);
 

@@ -170,7 +170,7 @@ def _i64(a) -> np.ndarray:
 
 
 (HOOK_RESET, HOOK_WAIT_NS, HOOK_BARRIER_PHANTOM, HOOK_MBAR_PROBE, HOOK_COLOR_KEEP_MAP, HOOK_DAG_SPLIT_NETS,
- HOOK_COLOR_KEEP_MIN_NETS, HOOK_SHAPE_DEDUPE, HOOK_DAG_STAGE_NODES, HOOK_DAG_BIG_NODES) = range(10)
+ HOOK_COLOR_KEEP_MIN_NETS, HOOK_SHAPE_DEDUPE, HOOK_DAG_STAGE_NODES) = range(9)
 
 
 def set_test_hook(key: int, value: int = 0) -> None:

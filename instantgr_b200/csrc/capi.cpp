@@ -337,10 +337,6 @@ int igr_test_hook(int key, int64_t value) {
             if (value < 1) return fail(nullptr, IGR_ERR_INVALID, "split threshold must be at least 1");
             h.dag_split_nets = (int)std::min<int64_t>(value, INT32_MAX);
             return IGR_OK;
-        case IGR_HOOK_DAG_BIG_NODES:
-            if (value < 0) return fail(nullptr, IGR_ERR_INVALID, "negative node count");
-            h.dag_big_nodes = (int)std::min<int64_t>(value, INT32_MAX);
-            return IGR_OK;
         case IGR_HOOK_DAG_STAGE_NODES:
             if (value < 0 || value > 4096) return fail(nullptr, IGR_ERR_INVALID, "staging limit in 0..4096 nodes");
             h.dag_stage_nodes = (int)value;
@@ -814,7 +810,7 @@ int igr_dag_route(igr_ctx *c, int n, const int32_t *node_off, const int32_t *nod
             db.max_net_edges = std::max(db.max_net_edges, par_off[node_off[k + 1]] - par_off[node_off[k]]);
         }
         launch_dag_route(g, db, stamp, c->s, c->aux, c->fork, c->join, test_hooks().dag_split_nets.load(),
-                         test_hooks().dag_stage_nodes.load(), test_hooks().dag_big_nodes.load());
+                         test_hooks().dag_stage_nodes.load());
         cuda_check(cudaGetLastError(), "DAG launch");
         cuda_check(cudaMemcpyAsync(routes_out, c->routes.p, ext * 4, cudaMemcpyDeviceToHost, c->s), "D2H");
         sync_check(c);

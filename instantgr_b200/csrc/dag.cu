@@ -29,8 +29,8 @@ constexpr int kDagWarps = 8;                 // warps of one net's CTA
 constexpr int kDagThreads = 32 * kDagWarps;
 constexpr int kSmallWarps = 2;               // warps of a small net's CTA
 constexpr int kSmallNodes = 64;              // a small net's DAG has at most this many nodes
-constexpr int kBigWarps = 16;                // warps of a large net's CTA
-constexpr int kMaxStageNodes = 4096;         // staging limit in nodes (4096: 147 KB of shared memory)
+constexpr int kSmallStageNodes = 96;         // nets staged with the smaller shared memory when a batch is split
+constexpr int kBigWarps = 16;                // warps of the CTAs of the larger nets of a split batch
 
 __device__ __forceinline__ int32_t f2o(float f) {
     int32_t i = __float_as_int(f);
@@ -155,27 +155,32 @@ struct NodeScratch {
 constexpr double kNone = __builtin_huge_val();  // no candidate (every real candidate is below kInf)
 
 // One net's DAG as the DP and the backtrace read it.  S = false: the batch
-// arrays.  S = true: the net's node positions (decoded, packed as
-// layer << 28 | x << 14 | y), child and parent-edge offsets, parents, child
-// slots, level lists and level offsets copied into shared memory at the start
-// of the net, with its chosen layers and segment counts kept there too, so
-// that the dependent lookups of every node stay on chip.  Indices and values
-// are the batch's in both forms; the shared layout (ints) is
-// pos[n] coff[n+1] poff[n+1] lev[n] lo[n] scnt[n] par[m] slot[m] loff[...].
-extern __shared__ int s_dag[];
+// arrays.  S = true: copied into shared memory at the start of the net (node
+// positions decoded and packed as layer << 28 | x << 14 | y, child and
+// parent-edge offsets, parents, child slots, level lists and level offsets,
+// each node's via-cost column), with the packed child entries, the best
+// paths, the chosen layers and the segment counts kept there too: only the
+// offer records, the node costs and the segments go through L2.  Indices
+// and values are the batch's in both forms.  Shared layout: u64
+// packed[ms * 10], u64 best[ms * 10], double vcol[n * 8], then ints pos[n]
+// coff[n+1] poff[n+1] lev[n] lo[n] scnt[n] par[m] slot[m] loff[levels + 1].
+extern __shared__ __align__(16) unsigned long long s_dag[];
 constexpr int kStageLevels = 64;  // levels of a staged net, at most
 constexpr int kStageMaxSide = 1 << 14;  // staged positions hold x and y in 14 bits
 
 struct NetLoc {
-    int n0, e0, l0, n, m;  // first node, first parent edge, first level offset; nodes, parent edges
+    int n0, e0, l0, c0;  // first node, parent edge, level offset and child slot
+    int n, m, ms;        // nodes, parent edges, child slots
 };
 
 struct NodePos {
     int l, x, y;  // layer index (9: the Steiner layer) and GCell
 };
 
-__device__ __forceinline__ void prefetch_l2(const void *p) {
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(__cvta_generic_to_global(p)));
+// bytes of shared memory that a staged net of n nodes, m parent edges and ms
+// child slots takes
+__host__ __device__ constexpr size_t staged_bytes(int n, int m, int ms) {
+    return 8 * (20 * (size_t)ms + 8 * (size_t)n) + 4 * (size_t)(6 * n + 2 + 2 * m + kStageLevels);
 }
 
 template <bool S>
@@ -183,40 +188,49 @@ struct Dag {
     const DagBatchDev &b;
     NetLoc L;
     int XY, Y;
+    __device__ __forceinline__ int *ints() const { return reinterpret_cast<int *>(s_dag + 20 * L.ms + 8 * L.n); }
     __device__ __forceinline__ NodePos pos(int node) const {
         if (S) {
-            const unsigned p = (unsigned)s_dag[node - L.n0];
+            const unsigned p = (unsigned)ints()[node - L.n0];
             return {(int)(p >> 28), (int)((p >> 14) & 0x3FFF), (int)(p & 0x3FFF)};
         }
         const int v = b.nodes[node], l = v / XY, q = v - l * XY, x = q / Y;
         return {l, x, q - x * Y};
     }
     __device__ __forceinline__ int coff(int node) const {
-        return S ? s_dag[L.n + node - L.n0] : b.child_off[node];
+        return S ? ints()[L.n + node - L.n0] : b.child_off[node];
     }
     __device__ __forceinline__ int poff(int node) const {
-        return S ? s_dag[2 * L.n + 1 + node - L.n0] : b.par_off[node];
+        return S ? ints()[2 * L.n + 1 + node - L.n0] : b.par_off[node];
     }
     __device__ __forceinline__ int lev(int pos) const {
-        return S ? s_dag[3 * L.n + 2 + pos - L.n0] : b.level_nodes[pos];
+        return S ? ints()[3 * L.n + 2 + pos - L.n0] : b.level_nodes[pos];
     }
     __device__ __forceinline__ int *lo(int node) const {
-        return S ? s_dag + 4 * L.n + 2 + node - L.n0 : b.layer_out + node;
+        return S ? ints() + 4 * L.n + 2 + node - L.n0 : b.layer_out + node;
     }
     __device__ __forceinline__ int *scnt(int node) const {
-        return S ? s_dag + 5 * L.n + 2 + node - L.n0 : b.stage_cnt + node;
+        return S ? ints() + 5 * L.n + 2 + node - L.n0 : b.stage_cnt + node;
     }
-    __device__ __forceinline__ int par(int e) const { return S ? s_dag[6 * L.n + 2 + e - L.e0] : b.par[e]; }
+    __device__ __forceinline__ int par(int e) const { return S ? ints()[6 * L.n + 2 + e - L.e0] : b.par[e]; }
     __device__ __forceinline__ int slot(int e) const {
-        return S ? s_dag[6 * L.n + 2 + L.m + e - L.e0] : b.child_slot[e];
+        return S ? ints()[6 * L.n + 2 + L.m + e - L.e0] : b.child_slot[e];
     }
     __device__ __forceinline__ int loff(int d) const {
-        return S ? s_dag[6 * L.n + 2 + 2 * L.m + d] : b.level_off[L.l0 + d];
+        return S ? ints()[6 * L.n + 2 + 2 * L.m + d] : b.level_off[L.l0 + d];
+    }
+    // packed entries and best paths of child slot `sl` (kML per slot)
+    __device__ __forceinline__ unsigned long long *packed(int sl) const {
+        return S ? s_dag + (sl - L.c0) * kML : b.packed + (int64_t)sl * kML;
+    }
+    __device__ __forceinline__ unsigned long long *best(int sl) const {
+        return S ? s_dag + (L.ms + sl - L.c0) * kML : b.best_path + (int64_t)sl * kML;
+    }
+    // via costs of the node's column, layers 0..7 (staged nets)
+    __device__ __forceinline__ const double *vcol(int node) const {
+        return reinterpret_cast<const double *>(s_dag + 20 * L.ms) + (node - L.n0) * 8;
     }
 };
-
-// ints of shared memory that a staged net of n nodes and m parent edges takes
-__host__ __device__ constexpr int staged_ints(int n, int m) { return 6 * n + 2 + 2 * m + kStageLevels; }
 
 // what one (parent edge, target layer t) pair needs besides the node's own
 // costs: the parent's packed entry and, per source layer of t's parity
@@ -227,7 +241,7 @@ __host__ __device__ constexpr int staged_ints(int n, int m) { return 6 * n + 2 +
 struct Offer {
     int64_t dst;
     double v[5];
-    unsigned wire, change;
+    double mask;  // wire | change << 8, in the bits of a double (as stored)
 };
 
 template <bool S>
@@ -238,7 +252,7 @@ __device__ __forceinline__ void offer_load(const GridDev &g, const Dag<S> &D, in
     const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
     const bool far = abs(x - px) + abs(y - py) > 4;
     o.dst = ((int64_t)D.coff(parent) + D.slot(e)) * kML + t;
-    o.wire = o.change = 0;
+    unsigned wire = 0, change = 0;
 #pragma unroll
     for (int q = 0; q < 5; q++) {
         const int layer = 2 - (t & 1) + 2 * q;
@@ -249,25 +263,25 @@ __device__ __forceinline__ void offer_load(const GridDev &g, const Dag<S> &D, in
         if (dl == 0 && x != px) continue;
         if (t == layer) {
             o.v[q] = wire_cost(g, layer - 1, minx, maxx, miny, maxy);
-            o.wire |= 1u << q;
+            wire |= 1u << q;
         } else if (far) {
             o.v[q] = D.b.cost_edges[(int64_t)e * 81 + (layer - 1) * 9 + (t - 1)];
-            o.change |= 1u << q;
+            change |= 1u << q;
         }
     }
+    o.mask = __longlong_as_double((long long)(wire | change << 8));
 }
 
-// The offer records of a staged net are computed once, by all threads of its
-// CTA before the DP starts (they depend on no DP result), at (e * 9 + t - 1)
-// * kOfferRec in b.offers: v[0..4], then wire | change << 8 in the bits of
-// the sixth double.
+// The offer records depend on no DP result: dag_offer_kernel computes them
+// for every (parent edge, target layer) pair of the batch before the DP, at
+// (e * 9 + t - 1) * kOfferRec in b.offers: v[0..4], then the mask.
 constexpr int kOfferRec = 6;
 
 __device__ __forceinline__ void offer_store(const DagBatchDev &b, int e, int t, const Offer &o) {
     double2 *r = reinterpret_cast<double2 *>(b.offers + ((int64_t)e * 9 + (t - 1)) * kOfferRec);
     r[0] = make_double2(o.v[0], o.v[1]);
     r[1] = make_double2(o.v[2], o.v[3]);
-    r[2] = make_double2(o.v[4], __longlong_as_double((long long)(o.wire | o.change << 8)));
+    r[2] = make_double2(o.v[4], o.mask);
 }
 
 template <bool S>
@@ -275,37 +289,54 @@ __device__ __forceinline__ void offer_fetch(const Dag<S> &D, int e, int t, Offer
     const double2 *r = reinterpret_cast<const double2 *>(D.b.offers + ((int64_t)e * 9 + (t - 1)) * kOfferRec);
     const double2 a = r[0], c = r[1], d = r[2];
     o.v[0] = a.x; o.v[1] = a.y; o.v[2] = c.x; o.v[3] = c.y; o.v[4] = d.x;
-    const unsigned m = (unsigned)__double_as_longlong(d.y);
-    o.wire = m & 0xff;
-    o.change = m >> 8;
+    o.mask = d.y;
     o.dst = ((int64_t)D.coff(D.par(e)) + D.slot(e)) * kML + t;
 }
 
-// the offer of pair (e, t): computed, or fetched where the net is staged
+// the offer of pair (e, t): fetched, or computed without offer records
 template <bool S>
 __device__ __forceinline__ void offer_get(const GridDev &g, const Dag<S> &D, int x, int y, int e, int t, Offer &o) {
-    if (S)
+    if (D.b.offers)
         offer_fetch(D, e, t, o);
     else
         offer_load(g, D, x, y, e, t, o);
 }
 
+// one thread per (parent edge, target layer) pair of the batch
+__global__ void __launch_bounds__(256) dag_offer_kernel(GridDev g, DagBatchDev b) {
+    chain_begin();
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)b.n_edges * 9) return;
+    const int e = (int)(i / 9), t = 1 + (int)(i % 9);
+    const Dag<false> D{b, NetLoc{}, g.X * g.Y, g.Y};
+    const NodePos p = D.pos(b.edge_child[e]);
+    Offer o;
+    offer_load(g, D, p.x, p.y, e, t, o);
+    offer_store(b, e, t, o);
+}
+
 // the minimum packed offer of the pair over its source layers, then atomicMin
 // into the parent's entry (the minimum does not depend on the order)
-__device__ __forceinline__ void offer_send(const DagBatchDev &b, const Offer &o, const double *cost, int node) {
+template <bool S>
+__device__ __forceinline__ void offer_send(const Dag<S> &D, const Offer &o, const double *cost, int node) {
     const int t = (int)(o.dst % kML);
+    const unsigned mk = (unsigned)__double_as_longlong(o.mask), wire = mk & 0xff, change = mk >> 8;
     unsigned long long m = ~0ull;
 #pragma unroll
     for (int q = 0; q < 5; q++) {
         const int layer = 2 - (t & 1) + 2 * q;
         if (layer >= kML) continue;
-        if (!((o.wire >> q) & 1) && !(((o.change >> q) & 1) && o.v[q] < kInf)) continue;
+        if (!((wire >> q) & 1) && !(((change >> q) & 1) && o.v[q] < kInf)) continue;
         const double c2 = cost[layer] + o.v[q];
         const int choice = t == layer ? 82 : (layer - 1) * 9 + (t - 1);
         const unsigned long long nv = pack((float)c2, node * 100 + choice);
         if (nv < m) m = nv;
     }
-    if (m != ~0ull) atomicMin(b.packed + o.dst, m);
+    if (m == ~0ull) return;
+    if (S)
+        atomicMin(s_dag + (o.dst - (int64_t)D.L.c0 * kML), m);
+    else
+        atomicMin(D.b.packed + o.dst, m);
 }
 
 // Lshape_route_node_layer_change_cuda for one node, computed by one warp.
@@ -330,30 +361,40 @@ __device__ void dp_node_warp(const GridDev &g, const Dag<S> &D, int node, int la
     const int fixed_high = fixed_low == 10 ? 0 : fixed_low;
     const int x = np.x, y = np.y;
     const int cb = D.coff(node), cn = D.coff(node + 1) - cb;
-    __syncwarp();  // the previous node's scratch is no longer read
-    // every global load of the node first, so that their latencies overlap:
-    // the children's packed entries (their atomics landed in L2: read past
-    // L1), the via costs of the node's column, and the parent-side inputs
-    // (which do not depend on the DP)
-    const unsigned long long *pk = b.packed + (int64_t)cb * kML;
-    unsigned long long pkv[3];  // entries lane + 32 r of the cn * 9 <= 90
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-        const int i = lane + 32 * r;
-        if (i < cn * 9) pkv[r] = __ldcg(pk + (i / 9) * kML + 1 + i % 9);
-    }
-    double vc = 0;
-    if (lane < 8) vc = g.vcost[cell_at(g, lane, x, y)];
     const int pb = D.poff(node), pn = D.poff(node + 1) - pb;
+    __syncwarp();  // the previous node's scratch is no longer read
+    // the children's packed entries (rows of kML) and the via costs of the
+    // node's column: in shared memory where the net is staged, else loaded
+    // here (past L1: the children's atomics landed in L2); every global load
+    // of the node is issued before any is used
+    const unsigned long long *pk;
+    const double *vcol;
     Offer o;
-    if (lane < pn * 9) offer_get(g, D, x, y, pb + lane / 9, 1 + lane % 9, o);
+    if (S) {
+        pk = D.packed(cb);
+        vcol = D.vcol(node);
+        if (lane < pn * 9) offer_get(g, D, x, y, pb + lane / 9, 1 + lane % 9, o);
+    } else {
+        const unsigned long long *gp = b.packed + (int64_t)cb * kML;
+        unsigned long long pkv[3];  // entries lane + 32 r of the cn * 9 <= 90
 #pragma unroll
-    for (int r = 0; r < 3; r++) {
-        const int i = lane + 32 * r;
-        if (i < cn * 9) s.pk[i / 9][1 + i % 9] = pkv[r];
+        for (int r = 0; r < 3; r++) {
+            const int i = lane + 32 * r;
+            if (i < cn * 9) pkv[r] = __ldcg(gp + (i / 9) * kML + 1 + i % 9);
+        }
+        double vc = 0;
+        if (lane < 8) vc = g.vcost[cell_at(g, lane, x, y)];
+        if (lane < pn * 9) offer_get(g, D, x, y, pb + lane / 9, 1 + lane % 9, o);
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            const int i = lane + 32 * r;
+            if (i < cn * 9) s.pk[i / 9][1 + i % 9] = pkv[r];
+        }
+        if (lane < 8) s.vcol[lane] = vc;
+        __syncwarp();
+        pk = &s.pk[0][0];
+        vcol = s.vcol;
     }
-    if (lane < 8) s.vcol[lane] = vc;
-    __syncwarp();
     if (lane < 9) {
         // row `low`: T(low, J) = via(low, J) + the children's first minima
         // over [low, J], added child by child in child order (the
@@ -364,11 +405,11 @@ __device__ void dp_node_warp(const GridDev &g, const Dag<S> &D, int node, int la
         double via = 0;
 #pragma unroll
         for (int J = 1; J < kML; J++) {
-            if (on && J > low) via += s.vcol[J - 2];
+            if (on && J > low) via += vcol[J - 2];
             T[J] = via;
         }
         for (int c = 0; c < cn; c++) {
-            const unsigned long long *row = s.pk[c];
+            const unsigned long long *row = pk + c * kML;
             double m = kInf;
 #pragma unroll
             for (int J = 1; J < kML; J++) {
@@ -409,7 +450,7 @@ __device__ void dp_node_warp(const GridDev &g, const Dag<S> &D, int node, int la
         cost[0] = kInf;
     }
     __syncwarp();
-    unsigned long long *best = b.best_path + (int64_t)cb * kML;
+    unsigned long long *best = D.best(cb);
     for (int i = lane; i < cn * kML; i += 32) {
         const int c = i / kML, j = i % kML;
         const int w = s.win[j];
@@ -417,7 +458,7 @@ __device__ void dp_node_warp(const GridDev &g, const Dag<S> &D, int node, int la
         if (w >= 0) {
             double m = kInf;
             for (int q = w >> 4; q <= (w & 15); q++) {
-                const unsigned long long p = s.pk[c][q];
+                const unsigned long long p = pk[c * kML + q];
                 const double cc = packed_cost(p);
                 if (cc < m) { m = cc; val = (unsigned long long)packed_id(p) * kML + q; }
             }
@@ -427,9 +468,9 @@ __device__ void dp_node_warp(const GridDev &g, const Dag<S> &D, int node, int la
     for (int i = lane + 32; i < pn * 9; i += 32) {
         Offer o2;
         offer_get(g, D, x, y, pb + i / 9, 1 + i % 9, o2);
-        offer_send(b, o2, s.cost, node);
+        offer_send(D, o2, s.cost, node);
     }
-    if (lane < pn * 9) offer_send(b, o, s.cost, node);
+    if (lane < pn * 9) offer_send(D, o, s.cost, node);
 }
 
 template <bool S>
@@ -450,7 +491,7 @@ __device__ void trace_node(const GridDev &g, const Dag<S> &D, int node, int stam
     const int pb = D.poff(node), pn = D.poff(node + 1) - pb;
     const NodePos np = D.pos(node);
     const int l = np.l, cx = np.x, cy = np.y;
-    const unsigned long long *best = b.best_path + (int64_t)D.coff(node) * kML;
+    const unsigned long long *best = D.best(D.coff(node));
     int *lo = D.lo(node);
     if (pn == 0) {
         int ml = 0;
@@ -468,7 +509,7 @@ __device__ void trace_node(const GridDev &g, const Dag<S> &D, int node, int stam
                 par_seq = pi;
                 par_layer = *D.lo(pnode);
                 const int slot = D.slot(pb + par_seq);
-                const unsigned long long path = b.best_path[(int64_t)D.coff(par_idx) * kML + slot * kML + par_layer];
+                const unsigned long long path = D.best(D.coff(par_idx) + slot)[par_layer];
                 const unsigned long long cid = path / kML / 100;
                 const unsigned long long ch = (path / kML) % 100;
                 if (cid == (unsigned long long)node) {
@@ -513,7 +554,7 @@ __device__ void trace_node(const GridDev &g, const Dag<S> &D, int node, int stam
         }
         if (par_layer == -1) { *lo = -1; return; }
         const int slot = D.slot(pb + par_seq);
-        const unsigned long long path = b.best_path[(int64_t)D.coff(par_idx) * kML + slot * kML + par_layer];
+        const unsigned long long path = D.best(D.coff(par_idx) + slot)[par_layer];
         if (path / kML / 100 != (unsigned long long)node) { *lo = -1; return; }
     }
     const int cn = D.coff(node + 1) - D.coff(node);
@@ -567,50 +608,38 @@ __device__ void route_net(const GridDev &g, const DagBatchDev &b, int k, const N
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const Dag<S> D{b, L, g.X * g.Y, g.Y};
     const int n0 = L.n0, n1 = L.n0 + L.n;
-    const int64_t s0 = (int64_t)b.child_off[n0] * kML, s1 = (int64_t)b.child_off[n1] * kML;
-    for (int64_t i = s0 + tid; i < s1; i += kThreadsW) b.packed[i] = kInitPacked;
     if (S) {
         const int n = L.n, m = L.m, XY = g.X * g.Y;
+        for (int i = tid; i < L.ms * kML; i += kThreadsW) s_dag[i] = kInitPacked;
+        double *vcol = reinterpret_cast<double *>(s_dag + 20 * L.ms);
+        int *I = D.ints();
         for (int i = tid; i < n; i += kThreadsW) {
-            const int v = b.nodes[n0 + i], l = v / XY, q = v - l * XY, x = q / g.Y;
-            s_dag[i] = (l << 28) | (x << 14) | (q - x * g.Y);
-            s_dag[3 * n + 2 + i] = b.level_nodes[n0 + i];
-            s_dag[4 * n + 2 + i] = -1;
-            s_dag[5 * n + 2 + i] = 0;
+            const int v = b.nodes[n0 + i], l = v / XY, q = v - l * XY, x = q / g.Y, y = q - x * g.Y;
+            I[i] = (l << 28) | (x << 14) | y;
+            I[3 * n + 2 + i] = b.level_nodes[n0 + i];
+            I[4 * n + 2 + i] = -1;
+            I[5 * n + 2 + i] = 0;
+#pragma unroll
+            for (int c = 0; c < kML - 2; c++) vcol[i * 8 + c] = g.vcost[cell_at(g, c, x, y)];
         }
         for (int i = tid; i <= n; i += kThreadsW) {
-            s_dag[n + i] = b.child_off[n0 + i];
-            s_dag[2 * n + 1 + i] = b.par_off[n0 + i];
+            I[n + i] = b.child_off[n0 + i];
+            I[2 * n + 1 + i] = b.par_off[n0 + i];
         }
         for (int j = tid; j < m; j += kThreadsW) {
-            s_dag[6 * n + 2 + j] = b.par[L.e0 + j];
-            s_dag[6 * n + 2 + m + j] = b.child_slot[L.e0 + j];
+            I[6 * n + 2 + j] = b.par[L.e0 + j];
+            I[6 * n + 2 + m + j] = b.child_slot[L.e0 + j];
         }
-        for (int d = tid; d <= nl; d += kThreadsW) s_dag[6 * n + 2 + 2 * m + d] = b.level_off[L.l0 + d];
+        for (int d = tid; d <= nl; d += kThreadsW) I[6 * n + 2 + 2 * m + d] = b.level_off[L.l0 + d];
     } else {
+        const int64_t s0 = (int64_t)L.c0 * kML, s1 = (int64_t)(L.c0 + L.ms) * kML;
+        for (int64_t i = s0 + tid; i < s1; i += kThreadsW) b.packed[i] = kInitPacked;
         for (int v = n0 + tid; v < n1; v += kThreadsW) {
             b.layer_out[v] = -1;
             b.stage_cnt[v] = 0;
         }
     }
     __syncthreads();
-    if (S) {
-        // what no DP result decides, before the DP: each node's via-cost
-        // column into L2, and the offer record of every (parent edge, target
-        // layer) pair
-        for (int i = tid; i < L.n; i += kThreadsW) {
-            const NodePos p = D.pos(n0 + i);
-            for (int l = 0; l < kML - 2; l++) prefetch_l2(g.vcost + cell_at(g, l, p.x, p.y));
-        }
-        for (int i = tid; i < L.m * 9; i += kThreadsW) {
-            const int e = L.e0 + i / 9, t = 1 + i % 9;
-            const NodePos p = D.pos(b.edge_child[e]);
-            Offer o;
-            offer_load(g, D, p.x, p.y, e, t, o);
-            offer_store(b, e, t, o);
-        }
-        __syncthreads();
-    }
     for (int d = nl - 1; d >= 0; d--) {
         const int a = D.loff(d), e = D.loff(d + 1);
         for (int s = a + warp; s < e; s += W) dp_node_warp(g, D, D.lev(s), lane, scr[warp]);
@@ -625,24 +654,22 @@ __device__ void route_net(const GridDev &g, const DagBatchDev &b, int k, const N
 }
 
 // one CTA of W warps per net.  Sizes: 0 every net, 1 nets of at most
-// split_at nodes, 2 the larger ones (a DAG's level width grows with its size:
-// a CTA of fewer warps leaves fewer of them waiting at the level barriers of a
-// small DAG, one of more warps takes the wide levels of a large DAG in fewer
-// rounds).  A net of at most cap_n nodes, cap_m parent edges and
-// kStageLevels - 1 levels is staged in shared memory (dynamic, staged_ints of
-// the caps).  At most 80 registers a thread: 12 CTAs of 2 warps, 3 of 8 warps
-// or one of 16 warps beside one of 8 per SM.
+// split_at nodes, 2 the larger ones.  A net of at most cap_n nodes and
+// kStageLevels - 1 levels whose staged_bytes fit the launch's dynamic shared
+// memory (smem) is staged there.  At most 80 registers a thread: 12 CTAs of
+// 2 warps, 3 of 8 warps, or one of 16 warps beside one of 8 per SM.
 template <int W, int Sizes>
-__global__ void __maxnreg__(80) dag_net_kernel(GridDev g, DagBatchDev b, int stamp, int cap_n, int cap_m, int split_at) {
+__global__ void __maxnreg__(80) dag_net_kernel(GridDev g, DagBatchDev b, int stamp, int cap_n, int smem,
+                                               int split_at) {
     chain_begin();
     __shared__ NodeScratch scr[W];
     for (int k = blockIdx.x; k < b.n_nets; k += gridDim.x) {
         const int n0 = b.net_node_off[k], n1 = b.net_node_off[k + 1];
         if ((Sizes == 1 && n1 - n0 > split_at) || (Sizes == 2 && n1 - n0 <= split_at)) continue;
         const int l0 = b.net_level_off[k], nl = b.net_level_off[k + 1] - l0 - 1;
-        const int e0 = b.par_off[n0];
-        const NetLoc L{n0, e0, l0, n1 - n0, b.par_off[n1] - e0};
-        if (L.n <= cap_n && L.m <= cap_m && nl < kStageLevels)
+        const int e0 = b.par_off[n0], c0 = b.child_off[n0];
+        const NetLoc L{n0, e0, l0, c0, n1 - n0, b.par_off[n1] - e0, b.child_off[n1] - c0};
+        if (L.n <= cap_n && nl < kStageLevels && staged_bytes(L.n, L.m, L.ms) <= (size_t)smem)
             route_net<W, true>(g, b, k, L, nl, stamp, scr);
         else
             route_net<W, false>(g, b, k, L, nl, stamp, scr);
@@ -673,54 +700,72 @@ void dag_levels(int n, const int *node_off, const int *depth, std::vector<int> &
 }
 
 int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStream_t s, cudaStream_t aux,
-                     cudaEvent_t fork, cudaEvent_t join, int split_nets, int stage_nodes, int big_nodes) {
+                     cudaEvent_t fork, cudaEvent_t join, int split_nets, int stage_nodes) {
     if (b.n_nodes <= 0 || b.n_nets <= 0) return 0;
     int launches = 0;
     if (b.n_edges > 0) {
         launch_chained(dag_edge_cost_kernel, dim3((int)((b.n_edges + kEdgeWarps - 1) / kEdgeWarps)),
                        dim3(32 * kEdgeWarps), 0, s, g, b);
         launches++;
+        if (b.offers) {
+            launch_chained(dag_offer_kernel, dim3((int)(((int64_t)b.n_edges * 9 + 255) / 256)), dim3(256), 0, s, g, b);
+            launches++;
+        }
     }
-    // staging capacity: the batch's largest net (rounded up, so that few
-    // distinct sizes occur), within the limit; none without room for offer
-    // records or where positions do not fit their packed form
-    const int lim = b.offers && g.X <= kStageMaxSide && g.Y <= kStageMaxSide
-                        ? std::max(0, std::min(stage_nodes, kMaxStageNodes))
-                        : 0;
-    const int cap_n = lim ? std::min(lim, b.max_net_nodes > 0 ? (b.max_net_nodes + 63) / 64 * 64 : lim) : 0;
-    const int cap_m = lim ? std::min(2 * lim, b.max_net_edges > 0 ? (b.max_net_edges + 127) / 128 * 128 : 2 * lim) : 0;
-    const size_t smem = cap_n ? (size_t)staged_ints(cap_n, cap_m) * sizeof(int) : 0;
+    // Staging: none without room for offer records or where positions do not
+    // fit their packed form.  The shared memory of a launch fits the largest
+    // net of its size class (rounded up, so that few distinct sizes occur),
+    // within what a CTA can have; nets that do not fit run unstaged.
+    const int cap_n = b.offers && g.X <= kStageMaxSide && g.Y <= kStageMaxSide ? std::max(0, stage_nodes) : 0;
+    auto fit = [&](int n, int m, int warps) -> int {
+        if (!cap_n || n <= 0) return 0;
+        const size_t room = (size_t)dag_solo_smem_limit() - sizeof(NodeScratch) * warps;
+        const int nn = (std::min(n, cap_n) + 31) / 32 * 32, mm = (std::min(m, 2 * nn) + 63) / 64 * 64;
+        return (int)std::min(staged_bytes(nn, mm, mm), room);
+    };
+    const int mx_n = b.max_net_nodes > 0 ? b.max_net_nodes : cap_n;
+    const int mx_m = b.max_net_edges > 0 ? b.max_net_edges : 2 * mx_n;
     const bool many = aux && b.n_nets >= split_nets;
-    const bool big = aux && !many && big_nodes > 0 && b.max_net_nodes > big_nodes;
-    if (!many && !big) {
+    const bool two = aux && !many && mx_n > kSmallStageNodes && cap_n > 0;
+    if (!many && !two) {
+        const int smem = fit(mx_n, mx_m, kDagWarps);
         kernel_setup((const void *)dag_net_kernel<kDagWarps, 0>, kDagThreads, smem);
-        launch_chained(dag_net_kernel<kDagWarps, 0>, dim3(b.n_nets), dim3(kDagThreads), smem, s, g, b, stamp, cap_n,
-                       cap_m, 0);
+        launch_chained(dag_net_kernel<kDagWarps, 0>, dim3(b.n_nets), dim3(kDagThreads), (size_t)smem, s, g, b, stamp,
+                       cap_n, smem, 0);
         return launches + 1;
     }
     // two launches over the batch, each taking the nets of its size class
     // (the nets of a batch share no state): the larger nets' CTAs on the side
-    // stream, beside the smaller nets' CTAs
+    // stream, beside the smaller nets' CTAs, whose shared memory is sized for
+    // their class
+    const int split_at = many ? kSmallNodes : kSmallStageNodes;
+    const int small_w = many ? kSmallWarps : kDagWarps;
+    const int smem_small = fit(std::min(mx_n, split_at), std::min(mx_m, 2 * split_at), small_w);
     cudaEventRecord(fork, s);
     cudaStreamWaitEvent(aux, fork, 0);
     if (many) {
+        const int smem_large = fit(mx_n, mx_m, kDagWarps);
+        kernel_setup((const void *)dag_net_kernel<kDagWarps, 2>, kDagThreads, smem_large);
+        dag_net_kernel<kDagWarps, 2><<<b.n_nets, kDagThreads, smem_large, aux>>>(g, b, stamp, cap_n, smem_large,
+                                                                                split_at);
+    } else {
+        // the larger DAGs bound the batch: their CTAs take 16 warps, so that
+        // their wide levels take fewer rounds
+        const int smem_large = fit(mx_n, mx_m, kBigWarps);
+        kernel_setup((const void *)dag_net_kernel<kBigWarps, 2>, 32 * kBigWarps, smem_large);
+        dag_net_kernel<kBigWarps, 2><<<b.n_nets, 32 * kBigWarps, smem_large, aux>>>(g, b, stamp, cap_n, smem_large,
+                                                                                   split_at);
+    }
+    if (many) {
         // a batch of many nets: the DAGs of at most kSmallNodes nodes in
         // 2-warp CTAs, so that more of them are in flight
-        const int small_n = std::min(cap_n, kSmallNodes);
-        const int small_m = std::min(cap_m, 2 * kSmallNodes);
-        const size_t smem_small = small_n ? (size_t)staged_ints(small_n, small_m) * sizeof(int) : 0;
-        kernel_setup((const void *)dag_net_kernel<kDagWarps, 2>, kDagThreads, smem);
         kernel_setup((const void *)dag_net_kernel<kSmallWarps, 1>, 32 * kSmallWarps, smem_small);
-        dag_net_kernel<kDagWarps, 2><<<b.n_nets, kDagThreads, smem, aux>>>(g, b, stamp, cap_n, cap_m, kSmallNodes);
-        dag_net_kernel<kSmallWarps, 1><<<b.n_nets, 32 * kSmallWarps, smem_small, s>>>(g, b, stamp, small_n, small_m,
-                                                                                      kSmallNodes);
+        dag_net_kernel<kSmallWarps, 1><<<b.n_nets, 32 * kSmallWarps, smem_small, s>>>(g, b, stamp, cap_n, smem_small,
+                                                                                      split_at);
     } else {
-        // a batch with DAGs of more than big_nodes nodes: those in 16-warp
-        // CTAs, whose wide levels bound the batch
-        kernel_setup((const void *)dag_net_kernel<kBigWarps, 2>, 32 * kBigWarps, smem);
-        kernel_setup((const void *)dag_net_kernel<kDagWarps, 1>, kDagThreads, smem);
-        dag_net_kernel<kBigWarps, 2><<<b.n_nets, 32 * kBigWarps, smem, aux>>>(g, b, stamp, cap_n, cap_m, big_nodes);
-        dag_net_kernel<kDagWarps, 1><<<b.n_nets, kDagThreads, smem, s>>>(g, b, stamp, cap_n, cap_m, big_nodes);
+        kernel_setup((const void *)dag_net_kernel<kDagWarps, 1>, kDagThreads, smem_small);
+        dag_net_kernel<kDagWarps, 1><<<b.n_nets, kDagThreads, smem_small, s>>>(g, b, stamp, cap_n, smem_small,
+                                                                              split_at);
     }
     cudaEventRecord(join, aux);
     cudaStreamWaitEvent(s, join, 0);

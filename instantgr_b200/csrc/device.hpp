@@ -157,13 +157,13 @@ void dag_levels(int n, const int *node_off, const int *depth, std::vector<int> &
 // Batches of `split_nets` nets or more (4096 by default) run the DAGs of at
 // most 64 nodes in 2-warp CTAs on `s` beside the larger ones on `aux`
 // (forked and joined through the two events); smaller batches, or no `aux`,
-// run one launch.  Nets of at most `stage_nodes` nodes (up to 4096; 0: none)
-// keep their DAG arrays in shared memory while they are routed.  In smaller
-// batches with `aux`, DAGs of more than `big_nodes` nodes (0: none) run in
-// 16-warp CTAs on `aux` beside the others.
+// run one launch, or (with `aux`, when the batch holds DAGs of more than 96
+// nodes) the DAGs of at most 96 nodes on `s` beside the larger ones on `aux`.
+// Nets of at most `stage_nodes` nodes (0: none) whose DAG fits a CTA's shared
+// memory keep it there while they are routed.
 int launch_dag_route(const GridDev &g, const DagBatchDev &b, int stamp, cudaStream_t s, cudaStream_t aux = nullptr,
                      cudaEvent_t fork = nullptr, cudaEvent_t join = nullptr, int split_nets = 4096,
-                     int stage_nodes = 1024, int big_nodes = 0);
+                     int stage_nodes = 1024);
 
 constexpr int kRouteLayers = 9;
 

@@ -15,7 +15,6 @@ struct TestHooks {
     std::atomic<int> color_keep_min_nets{2000000};  // router: colourings of this many nets or more keep the map
     std::atomic<int> shape_dedupe{1};  // router: each shape's conflict points and claims kept once
     std::atomic<int> dag_stage_nodes{1024};  // DAG DP: nets of at most this many nodes staged in shared memory
-    std::atomic<int> dag_big_nodes{0};  // DAG DP: nets of more nodes in 16-warp CTAs (0: none)
     void reset() {
         wait_ns = 2000000000LL;
         barrier_phantom = 0;
@@ -25,7 +24,6 @@ struct TestHooks {
         color_keep_min_nets = 2000000;
         shape_dedupe = 1;
         dag_stage_nodes = 1024;
-        dag_big_nodes = 0;
     }
 };
 TestHooks &test_hooks();

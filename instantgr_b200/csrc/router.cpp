@@ -1407,8 +1407,7 @@ bool Router::rrr_pass(int iter) {
         kt.begin(KC_DAG);
         db.max_net_nodes = f.mx_n; db.max_net_edges = f.mx_e; db.offers = dg_offers.p;
         const int nl = launch_dag_route(go.g, db, s2, s, s_cls[0], ev_fork, ev_join[0],
-                                        test_hooks().dag_split_nets.load(), test_hooks().dag_stage_nodes.load(),
-                                        test_hooks().dag_big_nodes.load());
+                                        test_hooks().dag_split_nets.load(), test_hooks().dag_stage_nodes.load());
         kt.end(KC_DAG);
         kt.begin(KC_WIRE_COMMIT);
         launch_wire_commit(go.g, s2, true, s);

@@ -245,22 +245,21 @@ def test_dag_route_matches_oracle(seed, X, Y, dir0, n):
     assert np.array_equal(pre_gpu, pre)
 
 
-@pytest.mark.parametrize("split,stage,big", [(2, 1024, 0), (4096, 1024, 0), (4096, 0, 0), (4096, 40, 0), (2, 40, 0),
-                                             (4096, 1024, 50), (4096, 40, 50), (4096, 0, 1)])
-def test_dag_route_split_by_size_matches_oracle(split, stage, big):
+@pytest.mark.parametrize("split,stage", [(2, 1024), (4096, 1024), (4096, 0), (4096, 40), (2, 40), (4096, 100)])
+def test_dag_route_split_by_size_matches_oracle(split, stage):
     """A batch of DAGs of 3 to about 110 nodes through the DAG DP with the
-    size split on (the DAGs of at most 64 nodes in 2-warp CTAs beside the
-    larger ones on a second stream, which the router uses for batches of 4096
-    nets or more) and off, with the DAGs of more than 50 nodes (or all) in
-    16-warp CTAs beside the others, and with every DAG, none, or those of at
-    most 40 nodes staged in shared memory, against the oracle."""
+    split for batches of many nets on (the DAGs of at most 64 nodes in 2-warp
+    CTAs beside the larger ones on a second stream, which the router uses for
+    batches of 4096 nets or more) and off (then the DAGs of more than 96 nodes
+    run beside the others with more shared memory), and with every DAG, none,
+    or those of at most 40 or 100 nodes staged in shared memory, against the
+    oracle."""
     g = cases.grid_case(45, X=90, Y=80, dir0=0)
     d = cases.dag_batch(g, 46, n=120, kmax=40)
     sizes = np.diff(d["node_off"])
     assert (sizes <= 40).sum() > 0 and (sizes > 64).sum() > 0
     ig.set_test_hook(ig.HOOK_DAG_SPLIT_NETS, split)
     ig.set_test_hook(ig.HOOK_DAG_STAGE_NODES, stage)
-    ig.set_test_hook(ig.HOOK_DAG_BIG_NODES, big)
     try:
         assert _dag_vs_oracle(g, d) == 120
     finally:

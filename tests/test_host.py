@@ -278,7 +278,6 @@ def test_router_refuses_to_write_or_evaluate_before_routing(tmp_path):
 
 @pytest.mark.parametrize("key,bad,good", [("HOOK_DAG_STAGE_NODES", (-1, 4097), (0, 4096)),
                                           ("HOOK_DAG_SPLIT_NETS", (0, -5), (1, 4096)),
-                                          ("HOOK_DAG_BIG_NODES", (-1,), (0, 200)),
                                           ("HOOK_WAIT_NS", (-1,), (0, 2_000_000_000))])
 def test_test_hooks_check_their_ranges(key, bad, good):
     """Test hooks take values in their documented ranges and refuse others with
