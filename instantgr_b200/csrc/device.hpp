@@ -171,6 +171,10 @@ constexpr int kRouteLayers = 9;
 // `min_edges` edges with cap + threshold <= demand
 void launch_mark_overflow(const GridDev &g, int threshold, int *of_sum, const ViaBatchDev &nets,
                           int min_edges, uint8_t *is_of, cudaStream_t s);
+// indices i < n with flags[i] set, increasing, into list[0..*count); block_cnt
+// holds flag_list_blocks(n) ints of scratch
+int flag_list_blocks(int n);
+void launch_flag_list(const uint8_t *flags, int n, int *list, int *count, int *block_cnt, cudaStream_t s);
 // 2-D congestion view (graph.hpp:545-584): max over layers of (demand - cap)^+, then
 // exclusive prefix sums along x (xsum) and along y (ysum); layout [x][y]
 void launch_congestion_view(const GridDev &g, float *xsum, float *ysum, cudaStream_t s);
@@ -261,6 +265,11 @@ void launch_record_offsets(const int *routes, const int64_t *route_off, int n, i
                            cudaStream_t s);
 void launch_record_copy(const int *routes, const int64_t *route_off, int n, const int64_t *off, int *dense,
                         cudaStream_t s);
+// record slots of n nets: route_off[id] = offset and route_cap[id] = capacity
+// for slot[3k .. 3k+2] = {id, offset, capacity}
+void launch_record_slots(int n, const int64_t *slot, int64_t *route_off, int *route_cap, cudaStream_t s);
+// dst[k] = src[idx[k]], k < n
+void launch_take_i64(int n, const int *idx, const long long *src, long long *dst, cudaStream_t s);
 
 // ---- evaluation of a routing result with the ISPD2024 evaluator's rules (eval.cu)
 constexpr int kEvalLayers = 10;  // file layers: 0 (pins) and the 9 routing layers

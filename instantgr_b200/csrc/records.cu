@@ -48,6 +48,20 @@ __global__ void __launch_bounds__(kScanThreads) record_scan_kernel(int64_t *a, i
     if (t == 0) a[0] = 0;
 }
 
+__global__ void take_i64_kernel(int n, const int *idx, const long long *src, long long *dst) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) dst[k] = src[idx[k]];
+}
+
+// new record slots of the rerouted nets: slot[k] = {id, offset, capacity}
+__global__ void record_slots_kernel(int n, const int64_t *slot, int64_t *route_off, int *route_cap) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int64_t id = slot[3 * k];
+    route_off[id] = slot[3 * k + 1];
+    route_cap[id] = (int)slot[3 * k + 2];
+}
+
 __global__ void record_copy_kernel(const int *routes, const int64_t *route_off, int n, const int64_t *off,
                                    int *dense) {
     const int lane = threadIdx.x & 31;
@@ -65,6 +79,14 @@ void launch_record_offsets(const int *routes, const int64_t *route_off, int n, i
                            cudaStream_t s) {
     if (n > 0) record_len_kernel<<<(n + 255) / 256, 256, 0, s>>>(routes, route_off, n, end, off);
     record_scan_kernel<<<1, kScanThreads, 0, s>>>(off, n);
+}
+
+void launch_take_i64(int n, const int *idx, const long long *src, long long *dst, cudaStream_t s) {
+    if (n > 0) take_i64_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, idx, src, dst);
+}
+
+void launch_record_slots(int n, const int64_t *slot, int64_t *route_off, int *route_cap, cudaStream_t s) {
+    if (n > 0) record_slots_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, slot, route_off, route_cap);
 }
 
 void launch_record_copy(const int *routes, const int64_t *route_off, int n, const int64_t *off, int *dense,

@@ -17,6 +17,9 @@
 //    any order.
 //  * overflow cost: add_all_overflow_cost (src/graph.hpp:148-157), reduced in a
 //    fixed order (per track, then over tracks) instead of with f64 atomics.
+//  * flag list: the indices of the flagged nets in increasing order, so that
+//    only the list goes to the host: per-block counts, their exclusive scan,
+//    then each block writes its indices from its offset.
 #include "kcommon.cuh"
 
 namespace igr {
@@ -165,6 +168,89 @@ int warps_grid(int n) {
 }
 
 }  // namespace
+
+namespace {
+
+constexpr int kFlagItems = 8;  // flags per thread of the list kernels
+constexpr int kFlagBlock = kThreads * kFlagItems;
+
+// flags [t * 8, t * 8 + 8) of the block's range, counted per thread
+__device__ __forceinline__ int flag_count8(const uint8_t *flags, int n, int base, int t) {
+    int c = 0;
+#pragma unroll
+    for (int j = 0; j < kFlagItems; j++) {
+        const int i = base + t * kFlagItems + j;
+        c += i < n && flags[i];
+    }
+    return c;
+}
+
+// exclusive scan of v over the block's threads; *total gets the block's sum
+__device__ __forceinline__ int block_excl_scan(int v, int *total) {
+    __shared__ int s_w[kThreads / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int inc = warp_incl_scan_i(v, lane);
+    if (lane == 31) s_w[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        const int x = lane < kThreads / 32 ? s_w[lane] : 0;
+        const int xi = warp_incl_scan_i(x, lane);
+        if (lane < kThreads / 32) s_w[lane] = xi - x;
+        if (lane == kThreads / 32 - 1) *total = xi;
+    }
+    __syncthreads();
+    return s_w[w] + inc - v;
+}
+
+__global__ void __launch_bounds__(kThreads) flag_count_kernel(const uint8_t *flags, int n, int *block_cnt) {
+    __shared__ int s_total;
+    const int c = flag_count8(flags, n, blockIdx.x * kFlagBlock, threadIdx.x);
+    block_excl_scan(c, &s_total);
+    if (threadIdx.x == 0) block_cnt[blockIdx.x] = s_total;
+}
+
+// exclusive scan of block_cnt[0..nb) in place (one block); the total to *count
+__global__ void __launch_bounds__(kThreads) flag_offsets_kernel(int *block_cnt, int nb, int *count) {
+    __shared__ int s_total;
+    const int per = (nb + kThreads - 1) / kThreads;
+    const int lo = min(nb, (int)threadIdx.x * per), hi = min(nb, lo + per);
+    int sum = 0;
+    for (int i = lo; i < hi; i++) sum += block_cnt[i];
+    int run = block_excl_scan(sum, &s_total);
+    for (int i = lo; i < hi; i++) {
+        const int c = block_cnt[i];
+        block_cnt[i] = run;
+        run += c;
+    }
+    if (threadIdx.x == 0) *count = s_total;
+}
+
+__global__ void __launch_bounds__(kThreads) flag_write_kernel(const uint8_t *flags, int n, const int *block_off,
+                                                              int *list) {
+    __shared__ int s_total;
+    const int base = blockIdx.x * kFlagBlock, t = threadIdx.x;
+    int at = block_off[blockIdx.x] + block_excl_scan(flag_count8(flags, n, base, t), &s_total);
+#pragma unroll
+    for (int j = 0; j < kFlagItems; j++) {
+        const int i = base + t * kFlagItems + j;
+        if (i < n && flags[i]) list[at++] = i;
+    }
+}
+
+}  // namespace
+
+int flag_list_blocks(int n) { return (n + kFlagBlock - 1) / kFlagBlock; }
+
+void launch_flag_list(const uint8_t *flags, int n, int *list, int *count, int *block_cnt, cudaStream_t s) {
+    const int nb = flag_list_blocks(n);
+    if (nb == 0) {
+        cudaMemsetAsync(count, 0, sizeof(int), s);
+        return;
+    }
+    flag_count_kernel<<<nb, kThreads, 0, s>>>(flags, n, block_cnt);
+    flag_offsets_kernel<<<1, kThreads, 0, s>>>(block_cnt, nb, count);
+    flag_write_kernel<<<nb, kThreads, 0, s>>>(flags, n, block_cnt, list);
+}
 
 void launch_mark_overflow(const GridDev &g, int threshold, int *of_sum, const ViaBatchDev &nets, int min_edges,
                           uint8_t *is_of, cudaStream_t s) {

@@ -1096,6 +1096,34 @@ int Router::run_color(int n, const int *d_perm_ranks, const ShapeDev &shapes, in
 
 // One rip-up-and-reroute pass (main.cpp:37-68, Lshape_route_detour.hpp:726-1112).
 // Returns false when no net overflows.
+// Positions into of_ids (ascending ids) in the order the pass reroutes them:
+// decreasing HPWL, the reference's sort (Lshape_route_detour.hpp:732-734), or
+// predicted congestion first with the seed's rip-up order.  Sorting the
+// positions with the keys of their ids makes the comparisons and moves of
+// sorting the ids themselves, hence the same order.
+std::vector<int> Router::pass_order(const std::vector<int> &of_ids) const {
+    const size_t K = of_ids.size();
+    std::vector<int> ord(K);
+    if (seed_active && seed_order) {
+        std::vector<double> pr(K);
+        for (size_t k = 0; k < K; k++) pr[k] = seed_pressure(of_ids[k]);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::sort(ord.begin(), ord.end(), [&](int l, int r) {
+            if (pr[l] != pr[r]) return pr[l] > pr[r];
+            return ns.nets[of_ids[l]].hpwl > ns.nets[of_ids[r]].hpwl;
+        });
+    } else {
+        // (key, position) pairs compared on the key alone (the HPWL of every
+        // routing net, kept since open)
+        std::vector<std::pair<int, int>> kv(K);
+        for (size_t k = 0; k < K; k++) kv[k] = {hpwl_keys[of_ids[k]], (int)k};
+        std::sort(kv.begin(), kv.end(),
+                  [](const std::pair<int, int> &l, const std::pair<int, int> &r) { return l.first > r.first; });
+        for (size_t k = 0; k < K; k++) ord[k] = kv[k].second;
+    }
+    return ord;
+}
+
 bool Router::rrr_pass(int iter) {
     const int R = (int)ns.nets.size();
     const int X = ns.X, Y = ns.Y;
@@ -1105,31 +1133,36 @@ bool Router::rrr_pass(int iter) {
     d_is_of.alloc(R);
     d_xsum.alloc((size_t)X * Y);
     d_ysum.alloc((size_t)X * Y);
-    if (iter > 0) {  // records moved in the previous pass
-        d_route_off.upload(route_off, s);
-        d_route_cap.upload(route_cap, s);
-        st.h2d_bytes += (int64_t)R * 12;
-    }
+    // (the device's record offsets and capacities were brought up to date at
+    // the end of the previous pass, or by phase 1)
     cuda_check(cudaEventRecord(ev0, s), "event");
     // overflow marking and congestion view (graph.hpp:588-601, main.cpp:42-45)
     ViaBatchDev all{d_all_ids.p, d_route_off.p, routes.p, R};
     kt.begin(KC_RIPUP);
     launch_mark_overflow(go.g, 0, of_sum.p, all, 10, d_is_of.p, s);
     kt.end(KC_RIPUP);
-    st.launches += 2;
-    std::vector<uint8_t> is_of(R);
+    // the flagged nets in id order, listed on the device
+    d_of_list.alloc(R);
+    d_of_blocks.alloc(std::max(1, flag_list_blocks(R)) + 1);
+    launch_flag_list(d_is_of.p, R, d_of_list.p, d_of_blocks.p + flag_list_blocks(R), d_of_blocks.p, s);
+    st.launches += 5;
     CongestionView cv;
     cv.X = X; cv.Y = Y;
     if (host_dags) {
         cv.xsum.resize((size_t)X * Y);
         cv.ysum.resize((size_t)X * Y);
     }
-    cuda_check(cudaMemcpyAsync(is_of.data(), d_is_of.p, R, cudaMemcpyDeviceToHost, s), "D2H");
+    int n_of = 0;
+    cuda_check(cudaMemcpyAsync(&n_of, d_of_blocks.p + flag_list_blocks(R), sizeof(int), cudaMemcpyDeviceToHost, s),
+               "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
-    st.d2h_bytes += R;
-    std::vector<int> of_nets;
-    for (int i = 0; i < R; i++)
-        if (is_of[i]) of_nets.push_back(i);
+    std::vector<int> of_nets(n_of);
+    if (n_of > 0) {
+        cuda_check(cudaMemcpyAsync(of_nets.data(), d_of_list.p, (size_t)n_of * 4, cudaMemcpyDeviceToHost, s), "D2H");
+        cuda_check(cudaStreamSynchronize(s), "sync");
+    }
+    const double tp_mark = now_s();
+    st.d2h_bytes += 4 + (int64_t)n_of * 4;
     st.rerouted = (int)of_nets.size();
     if (verbose) std::fprintf(stderr, "[igr] pass %d: %zu nets to reroute\n", iter, of_nets.size());
     if (of_nets.empty()) return false;
@@ -1144,35 +1177,26 @@ bool Router::rrr_pass(int iter) {
         cuda_check(cudaStreamSynchronize(s), "sync");
         st.d2h_bytes += (int64_t)X * Y * 8;
     }
-    if (seed_active && seed_order) {
-        // predicted congestion first, then HPWL (the reference's order)
-        std::vector<double> pr(R, 0.0);
-        for (int i : of_nets) pr[i] = seed_pressure(i);
-        std::sort(of_nets.begin(), of_nets.end(), [&](int l, int r) {
-            if (pr[l] != pr[r]) return pr[l] > pr[r];
-            return ns.nets[l].hpwl > ns.nets[r].hpwl;
-        });
-    } else {
-        // the comparisons of the reference's sort (Lshape_route_detour.hpp:732-734):
-        // (key, id) pairs compared on the key alone give the same sequence of
-        // comparisons, hence the same order, as the ids compared through a key
-        // table (the HPWL of every routing net, kept since open)
-        std::vector<std::pair<int, int>> kv(of_nets.size());
-        for (size_t k = 0; k < of_nets.size(); k++) kv[k] = {hpwl_keys[of_nets[k]], of_nets[k]};
-        std::sort(kv.begin(), kv.end(),
-                  [](const std::pair<int, int> &l, const std::pair<int, int> &r) { return l.first > r.first; });
-        for (size_t k = 0; k < of_nets.size(); k++) of_nets[k] = kv[k].second;
-    }
     // per colour batch: its first entries in the arrays of the pass and its sizes
     std::vector<std::vector<int>> batches;
     std::vector<DagBatchInfo> bi;
-    std::vector<int64_t> old_off = route_off;
+    std::vector<int64_t> old_off;
     double th0 = now_s(), t_dag = 0, t_shapes = 0, t_color = 0, t_csr = 0;
     if (!host_dags) {
+        // the pass order on a host thread while the device builds the DAGs in id order
+        std::future<std::vector<int>> order =
+            std::async(std::launch::async, [this, &of_nets] { return pass_order(of_nets); });
         double tm[4];
-        if (!dags_on_device(of_nets, batches, bi, old_off, tm)) return false;
+        if (!dags_on_device(of_nets, order, batches, bi, old_off, tm)) return false;
         t_dag = tm[0]; t_shapes = tm[1]; t_color = tm[2]; t_csr = tm[3];
     } else {
+        {
+            const std::vector<int> ord = pass_order(of_nets);
+            std::vector<int> ids(ord.size());
+            for (size_t k = 0; k < ord.size(); k++) ids[k] = of_nets[ord[k]];
+            of_nets.swap(ids);
+        }
+        old_off = route_off;
         // detour DAGs on host threads (Lshape_route_detour.hpp:702-748)
         th0 = now_s();
         // DAGs of the rerouted nets only, by their position in of_nets; their arrays
@@ -1429,10 +1453,11 @@ bool Router::rrr_pass(int iter) {
     if (int e = go.check_error(s)) throw Error(e, "device error in rip-up and reroute");
     if (verbose)
         std::fprintf(stderr,
-                     "[igr] pass %d host: marking and order %.3f s, DAGs %.3f s, conflict shapes %.3f s, colouring %.3f s, "
-                     "batch arrays %.3f s, batches on the device %.3f s (of it enqueueing %zu batches %.3f s)\n",
-                     iter, th0 - tp0, t_dag - th0, t_shapes - t_dag, t_color - t_shapes, t_csr - t_color, now_s() - t_csr,
-                     bi.size(), t_enq - t_csr);
+                     "[igr] pass %d host: marking and order %.3f s (marking on the device %.3f s), DAGs %.3f s, conflict "
+                     "shapes %.3f s, colouring %.3f s, batch arrays %.3f s, batches on the device %.3f s (of it enqueueing "
+                     "%zu batches %.3f s)\n",
+                     iter, th0 - tp0, tp_mark - tp0, t_dag - th0, t_shapes - t_dag, t_color - t_shapes, t_csr - t_color,
+                     now_s() - t_csr, bi.size(), t_enq - t_csr);
     return true;
 }
 
@@ -1503,8 +1528,12 @@ void Router::upload_dag_trees() {
 // Detour DAGs of the rerouted nets built on the device (dagbuild.cu), their
 // conflict shapes and colouring, and the batch-local arrays of every colour
 // batch gathered on the device: the batches and arrays of the host path.
-bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<int>> &batches,
-                            std::vector<DagBatchInfo> &bi, const std::vector<int64_t> &old_off, double *tm) {
+// of_nets: the nets to reroute in id order on entry (DAG k is built for
+// of_nets[k]), the ones rerouted in pass order (`order`, positions into the
+// entry list, computed meanwhile) on return.
+bool Router::dags_on_device(std::vector<int> &of_nets, std::future<std::vector<int>> &order,
+                            std::vector<std::vector<int>> &batches, std::vector<DagBatchInfo> &bi,
+                            const std::vector<int64_t> &, double *tm) {
     const int X = ns.X, Y = ns.Y, R = (int)ns.nets.size();
     const double th0 = now_s();
     upload_dag_trees();
@@ -1525,13 +1554,16 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
     ddag.build(a, s, &okey);
     const double tb1 = now_s();
     st.d2h_bytes += (int64_t)of_nets.size() * kDagSizeFields * 4;
-    // the DP keeps at most 10 child slots per node (the reference packs the
-    // slot as a decimal digit); nets beyond that keep their current route
+    // in pass order, the DAGs of the nets rerouted: the DP keeps at most 10
+    // child slots per node (the reference packs the slot as a decimal digit);
+    // nets beyond that keep their current route
+    const std::vector<int> ord = order.get();
     std::vector<int> kept;
     kept.reserve(of_nets.size());
-    for (int k = 0; k < (int)of_nets.size(); k++)
+    for (int k : ord)
         if (ddag.sz(k, 5) <= 10) kept.push_back(k);
-    const bool all_kept = kept.size() == of_nets.size();
+    bool in_place = kept.size() == of_nets.size();  // kept[i] == i
+    for (size_t i = 0; in_place && i < kept.size(); i++) in_place = kept[i] == (int)i;
     {
         std::vector<int> ids(kept.size());
         for (size_t i = 0; i < kept.size(); i++) ids[i] = of_nets[kept[i]];
@@ -1548,20 +1580,18 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
         ShapeArgs sa;
         sa.tree_off = d_tree_off.p; sa.tree_nodes = d_tree_nodes.p; sa.tree_par = d_tree_par.p;
         sa.ext_pts = ddag.points.p;
-        if (all_kept) {  // shape i is DAG i
+        if (in_place) {  // shape i is DAG i
             sa.ids = d2_ids.p;
             sa.ext_at = ddag.point_at.p; sa.ext_cnt = ddag.sizes.p + 2; sa.ext_stride = kDagSizeFields;
         } else {         // shape i is DAG kept[i]
-            std::vector<long long> at(n);
-            std::vector<long long> all_at(kept.back() + 1);
-            cuda_check(cudaMemcpyAsync(all_at.data(), ddag.point_at.p, all_at.size() * 8, cudaMemcpyDeviceToHost, s),
-                       "D2H");
-            cuda_check(cudaStreamSynchronize(s), "sync");
             std::vector<int> cnt(n);
-            for (int i = 0; i < n; i++) { at[i] = all_at[kept[i]]; cnt[i] = ddag.sz(kept[i], 2); }
+            for (int i = 0; i < n; i++) cnt[i] = ddag.sz(kept[i], 2);
             d_kept.upload(of_nets, s);
-            d2_extat.upload(at, s);
+            d_kept_dag.upload(kept, s);
+            d2_extat.alloc(n);
+            launch_take_i64(n, d_kept_dag.p, ddag.point_at.p, d2_extat.p, s);
             d2_ptoff.upload(cnt, s);
+            st.launches += 1;
             sa.ids = d_kept.p; sa.ext_at = d2_extat.p; sa.ext_cnt = d2_ptoff.p; sa.ext_stride = 1;
         }
         sa.n = n; sa.X = X; sa.Y = Y; sa.sparsity = mode_eff >= 1 ? 2 : 15;
@@ -1677,10 +1707,23 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<i
     }
     tm[3] = now_s();
     grow_routes(route_end);
-    d_old_off.upload(old_off, s);
-    d_route_off.upload(route_off, s);
-    d_route_cap.upload(route_cap, s);
-    st.h2d_bytes += (int64_t)R * 20;
+    // the offsets before this pass's records (the device's are still those),
+    // then the new record slots of the rerouted nets
+    d_old_off.alloc(R);
+    cuda_check(cudaMemcpyAsync(d_old_off.p, d_route_off.p, (size_t)R * 8, cudaMemcpyDeviceToDevice, s), "D2D");
+    {
+        std::vector<int64_t> slot((size_t)3 * n);
+        for (int i = 0; i < n; i++) {
+            const int id = of_nets[i];
+            slot[3 * i] = id;
+            slot[3 * i + 1] = route_off[id];
+            slot[3 * i + 2] = route_cap[id];
+        }
+        d_slots.upload(slot, s);
+        launch_record_slots(n, d_slots.p, d_route_off.p, d_route_cap.p, s);
+        st.h2d_bytes += (int64_t)n * 24;
+        st.launches += 1;
+    }
     return true;
 }
 

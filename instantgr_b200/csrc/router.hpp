@@ -216,7 +216,7 @@ struct Router {
     int64_t route_end1 = 0, route_end = 0;
     bool ran = false;
     DevBuf<int> routes;
-    DevBuf<int64_t> d_route_off, d_old_off;
+    DevBuf<int64_t> d_route_off, d_old_off, d_slots;
     DevBuf<int> d_route_cap;
     // host copy of the live route records, packed on the device and made on
     // demand: page-locked ...
@@ -323,7 +323,8 @@ struct Router {
     DevBuf<int> d2_ptoff, d2_pts, d2_ids;  // DAG points and net ids of the rerouted nets
     // device DAG construction: trees in adjacency order (positions, neighbour
     // lists), the builder, kept nets and the batch layout of the gather
-    DevBuf<int> d_dt_off, d_dt_pos, d_dt_aoff, d_dt_adj, d_kept, d_gdesc, d_gbatch;
+    DevBuf<int> d_dt_off, d_dt_pos, d_dt_aoff, d_dt_adj, d_kept, d_kept_dag, d_gdesc, d_gbatch;
+    DevBuf<int> d_of_list, d_of_blocks;  // nets flagged for rip-up (id order), list scratch and count
     DevBuf<long long> d2_extat;
     bool dt_ready = false;
     DeviceDags ddag;
@@ -343,7 +344,9 @@ struct Router {
     // detour DAGs of the rerouted nets built, coloured and laid out per batch
     // on the device; false when no net is left to reroute.  tm: times at which
     // the DAGs, conflict shapes, colouring and batch arrays were done
-    bool dags_on_device(std::vector<int> &of_nets, std::vector<std::vector<int>> &batches,
+    std::vector<int> pass_order(const std::vector<int> &of_ids) const;
+    bool dags_on_device(std::vector<int> &of_nets, std::future<std::vector<int>> &order,
+                        std::vector<std::vector<int>> &batches,
                         std::vector<DagBatchInfo> &bi, const std::vector<int64_t> &old_off, double *tm);
     void upload_dag_trees();  // trees in adjacency order, once per router (enqueued, no sync)
     // the trees in adjacency order packed into page-locked buffers; the first
