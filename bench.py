@@ -75,6 +75,9 @@ def parse():
                     help="route --warmup + --steps times and print the router statistics (profiling runs)")
     ap.add_argument("--form", default="plain", choices=["plain", "batched", "learned"],
                     help="router form of --route-only")
+    ap.add_argument("--window", action="store_true",
+                    help="--route-only on the centred window of the design that the reference arm routes "
+                         "(--ref-window): a smaller case of the same density, for profiling captures")
     ap.add_argument("--micro", choices=["refresh", "seed"],
                     help="kernel cases for profiling: cost refresh on a seeded 1600x1600x9 grid (every track "
                          "dirty, none, a sixth, every track), or the learned seed's forward convolutions")
@@ -265,7 +268,7 @@ def reference_gpu(cap: str, net: str, workdir: str, rrr_iters: int) -> dict:
 
 def route_only(args):
     import instantgr_b200 as ig
-    cap, net = design_files(args)
+    cap, net = design_files(args, ref_window(args) if args.window else None)
     r = ig.Router(cap, net, rrr_iters=args.rrr_iters, profile=1, verbose=1,
                   batched=0 if args.form == "plain" else 1)
     m = None
