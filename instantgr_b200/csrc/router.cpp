@@ -274,6 +274,7 @@ void ShapeDev::upload(const ShapeSet &sh, int X, int Y, int sp, cudaStream_t st,
 Router::~Router() {
     if (grid_thread.joinable()) grid_thread.join();
     if (dt_packing.valid()) dt_packing.wait();
+    if (order1_pending.valid()) order1_pending.wait();
     if (s) cudaStreamSynchronize(s);  // no copy from a page-locked buffer is in flight below
     kt.collect();
     if (graph1_exec) cudaGraphExecDestroy(graph1_exec);
@@ -322,8 +323,27 @@ void Router::open(const char *cap, const char *net) {
     const double t_read = now_s();
     build_netset(d, ns, threads);
     const double t_nets = now_s();
-    // trees in DFS preorder, net-id order, and the phase-1 route record layout
     const int R = (int)ns.nets.size();
+    // phase-1 routing priority: HPWL, largest first (Lshape_route.hpp:170-172),
+    // with the reference's (unstable) std::sort and comparator: (key, id)
+    // pairs compared on the key alone take the same sequence of comparisons
+    // and moves, hence give the same order, as the ids compared through the
+    // nets.  Sorted on a host thread while the trees are laid out and the
+    // device is set up; the keys stay for the rip-up order of the reroute passes
+    hpwl_keys.resize(R);
+    parallel_for(R, threads, [&](int b, int e) {
+        for (int i = b; i < e; i++) hpwl_keys[i] = ns.nets[i].hpwl;
+    });
+    order1_pending = std::async(std::launch::async, [this, R] {
+        std::vector<std::pair<int, int>> kv(R);
+        for (int i = 0; i < R; i++) kv[i] = {hpwl_keys[i], i};
+        std::sort(kv.begin(), kv.end(),
+                  [](const std::pair<int, int> &l, const std::pair<int, int> &r) { return l.first > r.first; });
+        std::vector<int> order(R);
+        for (int i = 0; i < R; i++) order[i] = kv[i].second;
+        return order;
+    });
+    // trees in DFS preorder, net-id order, and the phase-1 route record layout
     tree_off.assign(R + 1, 0);
     for (int i = 0; i < R; i++) tree_off[i + 1] = tree_off[i] + (int)ns.nets[i].tnode.size();
     tree_nodes.resize(tree_off[R]);
@@ -365,23 +385,6 @@ void Router::open(const char *cap, const char *net) {
     route_off1 = route_off;
     route_cap1 = route_cap;
     dp_bytes = (double)dpb;
-    // phase-1 routing priority: HPWL, largest first (Lshape_route.hpp:170-172),
-    // with the reference's (unstable) std::sort and comparator: (key, id)
-    // pairs compared on the key alone take the same sequence of comparisons
-    // and moves, hence give the same order, as the ids compared through the
-    // nets; the keys stay for the rip-up order of the reroute passes
-    hpwl_keys.resize(R);
-    parallel_for(R, threads, [&](int b, int e) {
-        for (int i = b; i < e; i++) hpwl_keys[i] = ns.nets[i].hpwl;
-    });
-    {
-        std::vector<std::pair<int, int>> kv(R);
-        for (int i = 0; i < R; i++) kv[i] = {hpwl_keys[i], i};
-        std::sort(kv.begin(), kv.end(),
-                  [](const std::pair<int, int> &l, const std::pair<int, int> &r) { return l.first > r.first; });
-        order1.resize(R);
-        for (int i = 0; i < R; i++) order1[i] = kv[i].second;
-    }
     if (verbose)
         std::fprintf(stderr, "[igr] read+trees %.2fs (read %.3f, pins+trees %.3f, layout %.3f): %d nets, %d routing nets\n",
                      now_s() - t0, t_read - t0, t_nets - t_read, now_s() - t_nets, d.num_nets(), R);
@@ -475,6 +478,7 @@ void Router::ensure_device() {
     const double t_shapes = now_s();
     const double t_claims = t_shapes;
     // phase-1 colouring ranks: the reversed routing priority (the last rank wins conflicts)
+    if (order1_pending.valid()) order1 = order1_pending.get();
     std::vector<int> perm1(order1.rbegin(), order1.rend());
     d_perm1.upload(perm1, s);
     std::vector<int> ids(R);
@@ -493,10 +497,13 @@ void Router::ensure_device() {
 }
 
 // Grows the route buffer to `need` ints, keeping the records already written.
+// The first buffer leaves 40% room for the records the rip-up passes append
+// (on the 800k-net design three passes append about 30% of the phase-1
+// records), so that a pass rarely has to grow it.
 void Router::grow_routes(int64_t need) {
     if ((int64_t)routes.n >= need) return;
     DevBuf<int> nb;
-    nb.alloc((size_t)std::max<int64_t>(need, (int64_t)(routes.n * 3 / 2)));
+    nb.alloc((size_t)std::max<int64_t>(need + (routes.n ? 0 : need * 2 / 5), (int64_t)(routes.n * 3 / 2)));
     if (routes.p && routes.n > 0)
         cuda_check(cudaMemcpyAsync(nb.p, routes.p, routes.n * sizeof(int), cudaMemcpyDeviceToDevice, s), "D2D");
     std::swap(routes.p, nb.p);

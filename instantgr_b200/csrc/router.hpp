@@ -362,6 +362,9 @@ struct Router {
     };
     PackedTrees dt_pack;
     std::future<void> dt_packing;  // declared after the trees it reads: joined first on destruction
+    // the phase-1 priority order, sorted on a host thread from open() on (it
+    // reads hpwl_keys); taken into order1 where the device setup needs it
+    std::future<std::vector<int>> order1_pending;
     void pack_dag_trees();
 
    private:
