@@ -34,6 +34,7 @@ void tree_from_positions(const Design &d, int Y, const std::vector<int> &pos2d, 
         igr_steiner::Tree t;
         std::vector<igr_steiner::Branch> br;
         std::vector<std::tuple<int, int, int>> edges;
+        std::vector<uint64_t> ekey, etmp;
         std::vector<std::pair<int, int>> kept;
     };
     thread_local Scratch sc;
@@ -61,7 +62,20 @@ void tree_from_positions(const Design &d, int Y, const std::vector<int> &pos2d, 
             if (u == v) continue;
             edges.emplace_back(std::abs(b1.x - b2.x) + std::abs(b1.y - b2.y), u, v);
         }
-    std::sort(edges.begin(), edges.end());
+    if (edges.size() >= 256 && nodes.size() <= 65536) {
+        // (length, u, v) as one key that sorts as the triple does (lengths
+        // and node indices are non-negative, indices below 2^16)
+        std::vector<uint64_t> &ek = sc.ekey;
+        ek.resize(edges.size());
+        for (size_t i = 0; i < edges.size(); i++)
+            ek[i] = (uint64_t)(uint32_t)std::get<0>(edges[i]) << 32 | (uint64_t)std::get<1>(edges[i]) << 16 |
+                    (uint64_t)std::get<2>(edges[i]);
+        igr_steiner::sort_keys(ek, sc.etmp);
+        for (size_t i = 0; i < edges.size(); i++)
+            edges[i] = {(int)(ek[i] >> 32), (int)(ek[i] >> 16 & 0xffff), (int)(ek[i] & 0xffff)};
+    } else {
+        std::sort(edges.begin(), edges.end());
+    }
     std::vector<int> &parent = sc.parent;
     parent.resize(nodes.size());
     std::iota(parent.begin(), parent.end(), 0);

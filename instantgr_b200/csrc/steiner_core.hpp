@@ -25,7 +25,6 @@
 #include <climits>
 #include <stdexcept>
 #include <numeric>
-#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -39,16 +38,83 @@ struct Tree {
 
 inline int med3(int a, int b, int c) { return std::max(std::min(a, b), std::min(std::max(a, b), c)); }
 
+// Sorts 64-bit keys ascending: a least-significant-digit radix sort over the
+// bytes in which the keys differ (std::sort for few keys).  Any correct sort
+// gives the same sequence of keys, so the trees do not depend on which one
+// runs.
+inline void sort_keys(std::vector<uint64_t> &a, std::vector<uint64_t> &tmp) {
+    const size_t n = a.size();
+    if (n < 256) {
+        std::sort(a.begin(), a.end());
+        return;
+    }
+    uint64_t all_or = 0, all_and = ~0ull;
+    for (uint64_t k : a) { all_or |= k; all_and &= k; }
+    const uint64_t differ = all_or ^ all_and;
+    tmp.resize(n);
+    for (int shift = 0; shift < 64; shift += 8) {
+        if (((differ >> shift) & 0xff) == 0) continue;
+        size_t cnt[257] = {};
+        for (uint64_t k : a) cnt[((k >> shift) & 0xff) + 1]++;
+        for (int b = 0; b < 256; b++) cnt[b + 1] += cnt[b];
+        for (uint64_t k : a) tmp[cnt[(k >> shift) & 0xff]++] = k;
+        a.swap(tmp);
+    }
+}
+
+// The node at each position of a large tree: open addressing with linear
+// probing (a lookup answers the same as any map would).
+struct PosMap {
+    std::vector<int64_t> key;
+    std::vector<int> val;
+    std::vector<uint8_t> used;
+    size_t mask = 0, n = 0;
+    static size_t slot(int64_t k) { return (size_t)(((uint64_t)k * 0x9E3779B97F4A7C15ull) >> 24); }
+    void reset(size_t expect) {
+        size_t cap = 64;
+        while (cap < 4 * expect) cap <<= 1;
+        key.resize(cap);
+        val.resize(cap);
+        used.assign(cap, 0);
+        mask = cap - 1;
+        n = 0;
+    }
+    void put(int64_t k, int v) {
+        if (2 * (n + 1) > mask + 1) grow();
+        size_t i = slot(k) & mask;
+        while (used[i] && key[i] != k) i = (i + 1) & mask;
+        if (!used[i]) { used[i] = 1; key[i] = k; n++; }
+        val[i] = v;
+    }
+    int get(int64_t k) const {
+        for (size_t i = slot(k) & mask; used[i]; i = (i + 1) & mask)
+            if (key[i] == k) return val[i];
+        return -1;
+    }
+    void grow() {
+        std::vector<int64_t> k0;
+        std::vector<int> v0;
+        std::vector<uint8_t> u0;
+        k0.swap(key);
+        v0.swap(val);
+        u0.swap(used);
+        reset(u0.size());
+        for (size_t i = 0; i < u0.size(); i++)
+            if (u0[i]) put(k0[i], v0[i]);
+    }
+};
+
 // Containers of one build, kept per thread so that the small trees of most
 // nets allocate nothing.
 struct BuildScratch {
     std::vector<std::pair<int, int>> pts;
+    std::vector<uint64_t> pkey, ktmp;
     std::vector<std::vector<int>> adj;  // only the first `used` lists are live
     size_t used = 0;
     std::vector<int> sn, nid, nx, ny;
     std::vector<long long> key;
     std::vector<int> from, out, touched, clean;
-    std::unordered_map<int64_t, int> at;
+    PosMap at;
     // n empty adjacency lists
     void lists(size_t n) {
         for (size_t v = 0; v < std::min(n, adj.size()); v++) adj[v].clear();
@@ -75,8 +141,19 @@ inline void build(const std::vector<int> &xin, const std::vector<int> &yin, Tree
     const int n0 = (int)xin.size();
     std::vector<std::pair<int, int>> &pts = bs.pts;
     pts.resize(n0);
-    for (int i = 0; i < n0; i++) pts[i] = {xin[i], yin[i]};
-    std::sort(pts.begin(), pts.end());
+    if (n0 < 256) {
+        for (int i = 0; i < n0; i++) pts[i] = {xin[i], yin[i]};
+        std::sort(pts.begin(), pts.end());
+    } else {
+        // (x, y) as one key that sorts as the pair does (sign bits flipped)
+        std::vector<uint64_t> &pk = bs.pkey;
+        pk.resize(n0);
+        for (int i = 0; i < n0; i++)
+            pk[i] = (uint64_t)((uint32_t)xin[i] ^ 0x80000000u) << 32 | ((uint32_t)yin[i] ^ 0x80000000u);
+        sort_keys(pk, bs.ktmp);
+        for (int i = 0; i < n0; i++)
+            pts[i] = {(int)((uint32_t)(pk[i] >> 32) ^ 0x80000000u), (int)((uint32_t)pk[i] ^ 0x80000000u)};
+    }
     pts.erase(std::unique(pts.begin(), pts.end()), pts.end());
     const int P = (int)pts.size();
     for (auto &p : pts) { t.x.push_back(p.first); t.y.push_back(p.second); }
@@ -151,13 +228,15 @@ inline void build(const std::vector<int> &xin, const std::vector<int> &yin, Tree
         };
         (packed ? (void)ckey.reserve((size_t)8 * P) : cand.reserve((size_t)8 * P));
         std::vector<int> px(t.x), py(t.y), id(P);
-        std::vector<int64_t> order(P);
+        std::vector<uint64_t> order(P), stmp;
         std::vector<std::pair<int, int>> sweep;  // (-y, point), ascending
         sweep.reserve(P);
         for (int k = 0; k < 4; k++) {
             // points by x + y, then by index; sums fit 33 bits, indices 31
-            for (int i = 0; i < P; i++) order[i] = (((int64_t)px[i] + py[i]) << 31) + i;
-            std::sort(order.begin(), order.end());
+            // (the sign bit flipped, so that the keys sort as unsigned)
+            for (int i = 0; i < P; i++)
+                order[i] = (uint64_t)((((int64_t)px[i] + py[i]) << 31) + i) ^ (1ull << 63);
+            sort_keys(order, stmp);
             for (int i = 0; i < P; i++) id[i] = (int)(order[i] & 0x7fffffff);
             sweep.clear();
             for (int i : id) {
@@ -184,7 +263,7 @@ inline void build(const std::vector<int> &xin, const std::vector<int> &yin, Tree
             }
         }
         if (packed) {
-            std::sort(ckey.begin(), ckey.end());
+            sort_keys(ckey, stmp);
             cand.resize(ckey.size());
             for (size_t q = 0; q < ckey.size(); q++)
                 cand[q] = {(int)(ckey[q] >> 32), (int)(ckey[q] >> 16 & 0xffff), (int)(ckey[q] & 0xffff)};
@@ -215,18 +294,14 @@ inline void build(const std::vector<int> &xin, const std::vector<int> &yin, Tree
     // small trees, a hash map above (positions are distinct: the pins are, and
     // a Steiner point is only made where no node is)
     const bool scan = P <= 64;  // (independent of the MST method)
-    std::unordered_map<int64_t, int> &at = bs.at;
+    PosMap &at = bs.at;
     auto key = [](int x, int y) { return ((int64_t)x << 32) ^ (uint32_t)y; };
     if (!scan) {
-        at.clear();
-        at.reserve((size_t)2 * P);
-        for (int i = 0; i < P; i++) at[key(t.x[i], t.y[i])] = i;
+        at.reset((size_t)2 * P);
+        for (int i = 0; i < P; i++) at.put(key(t.x[i], t.y[i]), i);
     }
     auto node_at_pos = [&](int x, int y) {
-        if (!scan) {
-            auto it = at.find(key(x, y));
-            return it == at.end() ? -1 : it->second;
-        }
+        if (!scan) return at.get(key(x, y));
         for (int v = 0; v < (int)t.x.size(); v++)
             if (t.x[v] == x && t.y[v] == y) return v;
         return -1;
@@ -280,7 +355,7 @@ inline void build(const std::vector<int> &xin, const std::vector<int> &yin, Tree
                 s = (int)t.x.size();
                 t.x.push_back(bx); t.y.push_back(by);
                 bs.add_list();
-                if (!scan) at[key(bx, by)] = s;
+                if (!scan) at.put(key(bx, by), s);
                 drop(v, ba); drop(ba, v); drop(v, bb); drop(bb, v);
                 for (int w : {v, ba, bb}) { adj[s].push_back(w); adj[w].push_back(s); }
                 touch(v); touch(ba); touch(bb); touch(s);
@@ -320,7 +395,16 @@ inline void build(const std::vector<int> &xin, const std::vector<int> &yin, Tree
     for (int v = 0; v < V; v++)
         for (int w : adj[v])
             if (v < w) t.edges.push_back({nid[v], nid[w]});
-    std::sort(t.edges.begin(), t.edges.end());
+    if (t.edges.size() < 256) {
+        std::sort(t.edges.begin(), t.edges.end());
+    } else {  // node ids are >= 0: (a, b) as one key
+        std::vector<uint64_t> &ek2 = bs.pkey;
+        ek2.resize(t.edges.size());
+        for (size_t i = 0; i < t.edges.size(); i++)
+            ek2[i] = (uint64_t)(uint32_t)t.edges[i].first << 32 | (uint32_t)t.edges[i].second;
+        sort_keys(ek2, bs.ktmp);
+        for (size_t i = 0; i < t.edges.size(); i++) t.edges[i] = {(int)(ek2[i] >> 32), (int)(uint32_t)ek2[i]};
+    }
     t.x.assign(nx.begin(), nx.end());
     t.y.assign(ny.begin(), ny.end());
 }
@@ -340,7 +424,7 @@ inline void to_branches(const std::vector<int> &xin, const std::vector<int> &yin
     const int V = (int)t.x.size();
     struct Scratch {
         std::vector<std::vector<int>> adj;
-        std::vector<int> par, order, bidx;
+        std::vector<int> par, order, bidx, node_of;
     };
     thread_local Scratch ts;
     std::vector<std::vector<int>> &adj = ts.adj;
@@ -369,15 +453,17 @@ inline void to_branches(const std::vector<int> &xin, const std::vector<int> &yin
         if (lo == t.npins || t.x[lo] != x || t.y[lo] != y) throw std::out_of_range("point not in the tree");
         return lo;
     };
+    std::vector<int> &node_of = ts.node_of;
+    node_of.resize(d);
     for (int i = 0; i < d; i++) {
-        int v = node_at(xin[i], yin[i]);
+        const int v = node_of[i] = node_at(xin[i], yin[i]);
         if (bidx[v] < 0) bidx[v] = i;
     }
     int slot = d;
     for (int v = t.npins; v < V; v++) bidx[v] = slot++;
     for (int v = 0; v < V; v++) br[bidx[v]] = Branch{t.x[v], t.y[v], bidx[par[v]]};
     for (int i = 0; i < d; i++) {
-        int v = node_at(xin[i], yin[i]);
+        const int v = node_of[i];
         if (bidx[v] != i) br[i] = Branch{xin[i], yin[i], bidx[v]};  // duplicate input point
     }
     for (int s = slot; s < 2 * d - 2; s++) br[s] = Branch{t.x[0], t.y[0], bidx[0]};
