@@ -102,6 +102,8 @@ private:
 
     std::vector<int> keys_;
     std::vector<uint8_t> info_;
+    std::vector<int> old_keys_;     // the slots being re-inserted by rehash (storage reused)
+    std::vector<uint8_t> old_info_;
     size_t num_ = 0, mask_ = 0, max_allowed_ = 0;
     uint32_t inc_ = kInitialInc, shift_ = 0;
     uint64_t mult_ = kFirstMultiplier;
@@ -194,14 +196,14 @@ private:
     }
 
     void rehash(size_t buckets) {
-        const std::vector<int> old_keys = keys_;
-        const std::vector<uint8_t> old_info = info_;
         const size_t old_n = with_buffer(mask_ + 1);
         const bool had = mask_ != 0;
+        old_keys_.swap(keys_);
+        old_info_.swap(info_);
         init_data(buckets);
         if (had && old_n > 1)
             for (size_t i = 0; i < old_n; i++)
-                if (old_info[i] != 0) insert_known_new(old_keys[i]);
+                if (old_info_[i] != 0) insert_known_new(old_keys_[i]);
     }
 
     void increase_size() {
