@@ -17,7 +17,6 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
-#include <future>
 #include <thread>
 
 #include <fcntl.h>
@@ -600,34 +599,25 @@ void write_guides(const Design &d, const NetSet &ns, const RouteSource &rs, cons
         }
         out.size = (size_t)(q - out.p.get());
     };
-    // two sets of window buffers: a window is written while the next one is
-    // formatted
     const int W = 8 * std::max(1, threads);
-    std::vector<Buf> bufs[2] = {std::vector<Buf>(W), std::vector<Buf>(W)};
-    std::vector<off_t> at[2] = {std::vector<off_t>(W + 1), std::vector<off_t>(W + 1)};
-    std::atomic<bool> ok{true};
-    std::future<void> writing;
+    std::vector<Buf> bufs(W);
+    std::vector<off_t> at(W + 1);
     off_t pos = 0;
-    for (int c0 = 0, w = 0; c0 < nch; c0 += W, w ^= 1) {
+    for (int c0 = 0; c0 < nch; c0 += W) {
         const int k = std::min(W, nch - c0);
-        std::vector<Buf> &bw = bufs[w];
-        std::vector<off_t> &aw = at[w];
         parallel_for(k, threads, [&](int b, int e) {
-            for (int i = b; i < e; i++) fmt(c0 + i, bw[i]);
+            for (int i = b; i < e; i++) fmt(c0 + i, bufs[i]);
         });
-        aw[0] = pos;
-        for (int i = 0; i < k; i++) aw[i + 1] = aw[i] + (off_t)bw[i].size;
-        pos = aw[k];
-        if (writing.valid()) writing.get();  // the other set is free again
-        writing = std::async(std::launch::async, [&, k, w] {
-            parallel_for(k, threads, [&](int b, int e) {
-                for (int i = b; i < e; i++)
-                    if (!pwrite_all(fd, bufs[w][i].p.get(), bufs[w][i].size, at[w][i])) ok = false;
-            });
+        at[0] = pos;
+        for (int i = 0; i < k; i++) at[i + 1] = at[i] + (off_t)bufs[i].size;
+        std::atomic<bool> ok{true};
+        parallel_for(k, threads, [&](int b, int e) {
+            for (int i = b; i < e; i++)
+                if (!pwrite_all(fd, bufs[i].p.get(), bufs[i].size, at[i])) ok = false;
         });
+        if (!ok) throw Error(ERR_IO, std::string("write failed on ") + path);
+        pos = at[k];
     }
-    if (writing.valid()) writing.get();
-    if (!ok) throw Error(ERR_IO, std::string("write failed on ") + path);
     closer.fd = -1;
     if (::close(fd) != 0) throw Error(ERR_IO, std::string("write failed on ") + path);
 }
