@@ -438,18 +438,30 @@ def main():
 
     # e2e: the whole `-cap/-net/-out` flow through the public API with host files
     # (read, pins, trees, upload, route, download, write guides), plain form
+    # Every step writes a new guide file, as one `-cap/-net/-out` run does (a
+    # step that overwrote the previous step's file would also pay for dropping
+    # its pages while they are written back); the files go after the timing.
     out = os.path.join(args.workdir, f"guides_r{rank}.out")
     e2e_bytes = []
+    e2e_files = []
 
     def e2e_step():
+        path = f"{out}.{len(e2e_files)}"
+        e2e_files.append(path)
         r = ig.Router(cap, net, rrr_iters=args.rrr_iters, batched=0)
         r.run()
-        r.write(out)
+        r.write(path)
         st = r.stats()
         e2e_bytes.append((st["setup_h2d_bytes"] + st["h2d_bytes"], st["d2h_bytes"]))
         r.close()
 
+    for path in [out] + [f"{out}.{k}" for k in range(args.steps)]:
+        if os.path.exists(path):
+            os.remove(path)
     ms_e2e, _ = timed(None, e2e_step)
+    for path in e2e_files:
+        if os.path.exists(path):
+            os.remove(path)
 
     result = None
     if rank == 0:
