@@ -41,6 +41,7 @@ void cuda_check(cudaError_t e, const char *what) {
 namespace {
 std::mutex g_cache_mu;
 std::map<std::pair<int, size_t>, std::vector<void *>> g_cache;  // (device, block bytes) -> free blocks
+std::atomic<long long> g_mallocs{0}, g_malloc_us{0}, g_trims{0};  // cudaMalloc calls and their time, trims
 
 size_t block_bytes(size_t bytes) {
     const size_t g = bytes >= (size_t(1) << 20) ? (size_t(2) << 20) : 512;  // 2 MiB granules for large blocks
@@ -64,12 +65,22 @@ void *dev_alloc(size_t bytes) {
         }
     }
     void *p = nullptr;
+    const auto t0 = std::chrono::steady_clock::now();
     if (cudaMalloc(&p, b) != cudaSuccess) {
         cudaGetLastError();
         dev_trim();
+        g_trims++;
         cuda_check(cudaMalloc(&p, b), "cudaMalloc");
     }
+    g_mallocs++;
+    g_malloc_us += std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t0).count();
     return p;
+}
+
+void dev_alloc_stats(long long *mallocs, long long *us, long long *trims) {
+    *mallocs = g_mallocs.load();
+    *us = g_malloc_us.load();
+    *trims = g_trims.load();
 }
 
 void dev_free(void *p, size_t bytes) {
@@ -425,10 +436,12 @@ void Router::device_shapes(const ShapeArgs &a, ShapeDev &sd) {
     sd.pt_off.alloc((size_t)a.n + 1);
     sd.claim_off.alloc((size_t)a.n + 1);
     d_shape_tot.alloc(2);
+    const double t0 = now_s();
     launch_shape_count(a, sd.pt_off.p, sd.claim_off.p, d_shape_tot.p, s);
     long long h_tot[2] = {0, 0};
     cuda_check(cudaMemcpyAsync(h_tot, d_shape_tot.p, sizeof h_tot, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaStreamSynchronize(s), "shape counts");
+    const double t1 = now_s();
     if (h_tot[0] > INT32_MAX || h_tot[1] > INT32_MAX) throw Error(ERR_CAPACITY, "conflict shapes exceed 32-bit offsets");
     sd.pts.alloc((size_t)h_tot[0]);
     sd.claim.alloc((size_t)h_tot[1]);
@@ -440,6 +453,14 @@ void Router::device_shapes(const ShapeArgs &a, ShapeDev &sd) {
         sd.claim_n.release();
     }
     launch_shape_fill(a, sd.pt_off.p, sd.claim_off.p, sd.pts.p, sd.claim.p, sd.pt_n.p, sd.claim_n.p, s);
+    if (verbose) {
+        long long m = 0, us = 0, tr = 0;
+        dev_alloc_stats(&m, &us, &tr);
+        std::fprintf(stderr,
+                     "[igr] conflict shapes of %d nets: counts %.4f s, allocations and fill launch %.4f s "
+                     "(cudaMalloc so far: %lld calls, %.3f s, %lld trims)\n",
+                     a.n, t1 - t0, now_s() - t1, m, us * 1e-6, tr);
+    }
     sd.npts = (int)h_tot[0];
     sd.nshapes = a.n;
     sd.sparsity = a.sparsity;
@@ -1256,7 +1277,7 @@ bool Router::rrr_pass(int iter) {
         d2_pts.upload(pts, s);
         d2_ids.upload(of_nets, s);
         st.h2d_bytes += (int64_t)(pt_off.size() + pts.size() + of_nets.size()) * 4;
-        ShapeDev shd;
+        ShapeDev &shd = d_shapes2;
         {
             ShapeArgs a;
             a.tree_off = d_tree_off.p; a.tree_nodes = d_tree_nodes.p; a.tree_par = d_tree_par.p;
@@ -1582,7 +1603,7 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::future<std::vector<i
     tm[0] = now_s();
     // conflict shapes of the rerouted nets: their DAG points and their trees'
     // segments (Lshape_route_detour.hpp:751)
-    ShapeDev shd;
+    ShapeDev &shd = d_shapes2;
     {
         ShapeArgs sa;
         sa.tree_off = d_tree_off.p; sa.tree_nodes = d_tree_nodes.p; sa.tree_par = d_tree_par.p;
@@ -1591,6 +1612,7 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::future<std::vector<i
             sa.ids = d2_ids.p;
             sa.ext_at = ddag.point_at.p; sa.ext_cnt = ddag.sizes.p + 2; sa.ext_stride = kDagSizeFields;
         } else {         // shape i is DAG kept[i]
+            const double tk0 = now_s();
             std::vector<int> cnt(n);
             for (int i = 0; i < n; i++) cnt[i] = ddag.sz(kept[i], 2);
             d_kept.upload(of_nets, s);
@@ -1600,6 +1622,7 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::future<std::vector<i
             d2_ptoff.upload(cnt, s);
             st.launches += 1;
             sa.ids = d_kept.p; sa.ext_at = d2_extat.p; sa.ext_cnt = d2_ptoff.p; sa.ext_stride = 1;
+            if (verbose) std::fprintf(stderr, "[igr] shape sources of %d nets: %.4f s\n", n, now_s() - tk0);
         }
         sa.n = n; sa.X = X; sa.Y = Y; sa.sparsity = mode_eff >= 1 ? 2 : 15;
         device_shapes(sa, shd);

@@ -24,6 +24,8 @@ bool cuda_driver_ready();
 // A block is cached only after a device synchronisation, as cudaFree would.
 void *dev_alloc(size_t bytes);
 void dev_free(void *p, size_t bytes);
+// cudaMalloc calls of the device cache so far, their total time (us) and cache trims
+void dev_alloc_stats(long long *mallocs, long long *us, long long *trims);
 // returns every cached block of the current device to the driver
 void dev_trim();
 // The same for page-locked host memory (cudaMallocHost), used for the copies
@@ -210,6 +212,9 @@ struct Router {
     DevBuf<int64_t> d_scratch_off;
     DevBuf<double> d_scratch;
     ShapeDev d_shapes1;
+    // conflict shapes of a rip-up pass's nets: kept by the router, so that its
+    // grow-only buffers serve every pass and run without new allocations
+    ShapeDev d_shapes2;
     // ---- route records: phase-1 records at fixed offsets, reroutes appended per run
     std::vector<int64_t> route_off, route_off1;
     std::vector<int> route_cap, route_cap1;
