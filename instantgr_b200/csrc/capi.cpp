@@ -971,15 +971,17 @@ int igr_router_set_seed(igr_router *h, igr_seed *m, double alpha, int mode, int 
         r.seed_levels = levels;
         r.seed_ready = false;
         r.seed_used = false;
+        r.seed_score_due = false;
     });
 }
 
 int igr_router_seed_stats(igr_router *h, double *out, int n) {
     if (!h || !out) return fail(nullptr, IGR_ERR_INVALID, "null argument");
-    const auto &r = h->r;
-    double v[4] = {r.seed_used ? 1.0 : 0.0, r.seed_scores[1], r.seed_scores[0], r.seed_ms};
-    for (int k = 0; k < n && k < 4; k++) out[k] = v[k];
-    return IGR_OK;
+    return guard(&h->err, [&] {
+        double v[4];
+        h->r.seed_stats(v);
+        for (int k = 0; k < n && k < 4; k++) out[k] = v[k];
+    });
 }
 
 #define SEED_GUARD(m, ...)                                                      \

@@ -543,11 +543,13 @@ void Router::run() {
         return v[3];
     };
     if (seed_mode == 1) {
+        // nothing is decided on the score: it is computed when asked for
         run_once(true);
         seed_used = true;
-        seed_scores[1] = total();
+        seed_score_due = true;
         return;
     }
+    seed_score_due = false;
     // seeded run judged against the plain run: the better total score is kept
     const double t0 = now_s();
     run_once(true);
@@ -564,6 +566,22 @@ void Router::run() {
     if (verbose)
         std::fprintf(stderr, "[igr] seeded %.0f vs plain %.0f: %s result kept\n", seeded_score, plain_score,
                      seed_used ? "seeded" : "plain");
+}
+
+// Seed statistics of the last run (igr_router_seed_stats); a seeded-only
+// run's score is the evaluator's total of its result, computed on the first
+// request.
+void Router::seed_stats(double out[4]) {
+    if (seed_score_due) {
+        double v[4];
+        evaluate(v, nullptr);
+        seed_scores[1] = v[3];
+        seed_score_due = false;
+    }
+    out[0] = seed_used ? 1.0 : 0.0;
+    out[1] = seed_scores[1];
+    out[2] = seed_scores[0];
+    out[3] = seed_ms;
 }
 
 void Router::save_result(RouteBackup &b) {

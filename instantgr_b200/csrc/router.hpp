@@ -290,7 +290,7 @@ struct Router {
     int seed_kind = 0;    // 0 predicted demand, 1 predicted overflow only
     bool seed_order = false;  // rip-up order by predicted overflow instead of HPWL
     int seed_levels = 0;  // 0 constant during phase 1, else shrinks in this many steps
-    bool seed_ready = false, seed_active = false, seed_used = false;
+    bool seed_ready = false, seed_active = false, seed_used = false, seed_score_due = false;
     double seed_ms = 0, seed_scores[2] = {0, 0};
     DevBuf<float> d_seed_dem;         // seed demand at full strength (unrounded), track layout
     DevBuf<float> d_seed_cur;         // seed demand currently added to the demand (half units)
@@ -302,6 +302,7 @@ struct Router {
     void device_seed_features(DevBuf<__nv_bfloat16> &feat, cudaStream_t st);
     void seed_begin();
     double seed_pressure(int net) const;
+    void seed_stats(double out[4]);  // [0] seeded result kept, [1] seeded score, [2] plain score, [3] prediction ms
     void run_once(bool seeded);
     void save_result(RouteBackup &b);
     void restore_result(RouteBackup &b);
