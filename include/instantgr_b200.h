@@ -394,7 +394,8 @@ int igr_seed_time_forward(igr_seed *m, int tiles, int reps, double *layer_ms, do
 int igr_router_set_seed(igr_router *r, igr_seed *m, double alpha, int mode, int kind, int levels);
 /* Seed statistics of the last run: [0] 1 if the seeded result was kept (mode 2),
  * [1] seeded total score, [2] plain total score (mode 2), [3] prediction ms.
- * Scores are the evaluator's totals (igr_router_evaluate). */
+ * Scores are the evaluator's totals (igr_router_evaluate); after a mode-1 run
+ * the seeded score is computed by the first call. */
 int igr_router_seed_stats(igr_router *r, double *out, int n);
 /* One forward and backward pass on T tiles (x, target: [T][size][size][16])
  * without an update: loss and the gradient of every parameter (layout of
