@@ -101,6 +101,8 @@ struct StampedCounts {
 
 struct PinScratch {
     std::vector<int> idx, best;
+    std::vector<int> ax, ay, al, aoff;  // decoded access points of a net of at most 4 pins (pin-major)
+    std::vector<int> kx, ky, kd;        // per 2-D key of a larger net: x, y, distance to the bbox centre (x2)
     std::vector<char> visited;
     std::vector<int> p, p2;
     std::vector<int> order;        // walk order of the pins in the greedy rounds
@@ -141,20 +143,30 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
     if (num <= 4) {
         s.idx.assign(num, 0);
         s.best.assign(num, 0);
+        // every access point decoded once: (x, y, layer) by pin and choice
+        const int64_t a0 = d.ap_off[pb];
+        const int A = (int)(d.ap_off[pb + num] - a0);
+        s.ax.resize(A); s.ay.resize(A); s.al.resize(A); s.aoff.resize(num);
+        for (int i = 0; i < num; i++) s.aoff[i] = (int)(d.ap_off[pb + i] - a0);
+        for (int a = 0; a < A; a++) {
+            const int v = d.ap[a0 + a];
+            s.ax[a] = v / Y % X; s.ay[a] = v % Y; s.al[a] = v / XY;
+        }
+        const int *ax = s.ax.data(), *ay = s.ay.data(), *al = s.al.data(), *ao = s.aoff.data();
         int min_diff = 1000000000, min_m = 1000000000, min_m2 = 1000000000, min_m0 = 1000000000;
         // odometer over access-point choices, pin 0 most significant
         while (true) {
             int xmn = 1000000000, xmx = 0, ymn = 1000000000, ymx = 0, diff = 0, m = 0, m2 = 0;
             for (int i = 0; i < num; i++) {
-                int v = apv(i, s.idx[i]);
-                int xi = v / Y % X, yi = v % Y, li = v / XY;
+                const int a = ao[i] + s.idx[i];
+                const int xi = ax[a], yi = ay[a], li = al[a];
                 xmn = std::min(xmn, xi); xmx = std::max(xmx, xi);
                 ymn = std::min(ymn, yi); ymx = std::max(ymx, yi);
                 m += std::abs(2 * xi - c2x) + std::abs(2 * yi - c2y);
                 m2 += li;
                 for (int j = 0; j < i; j++) {
-                    int w = apv(j, s.idx[j]);
-                    diff += (xi != w / Y % X) + (yi != w % Y);
+                    const int b = ao[j] + s.idx[j];
+                    diff += (xi != ax[b]) + (yi != ay[b]);
                 }
             }
             int m0 = xmx - xmn + ymx - ymn;
@@ -222,6 +234,13 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
         s.cnt.assign(K, 0);
         s.cnt_st.assign(K, 0);
         s.round_st = 0;
+        s.kx.resize(K); s.ky.resize(K); s.kd.resize(K);
+        for (int r = 0; r < K; r++) {
+            const int q = s.first2d[r];
+            s.kx[r] = q / Y;
+            s.ky[r] = q % Y;
+            s.kd[r] = std::abs(s.kx[r] * 2 - c2x) + std::abs(s.ky[r] * 2 - c2y);
+        }
         for (int round = 0; round < num; round++) {
             int max_pos = -1, max_rank = -1, cnt_repeat = 0, max_coord = -1, min_dist = 1000000000;
             ++s.round_st;  // every key's running count starts at zero
@@ -235,8 +254,8 @@ void select_one(const Design &d, int n, PinScratch &s, std::vector<int> &pins, s
                         s.cnt[r] = 0;
                     }
                     const int sz = ++s.cnt[r];
-                    int dist = std::abs(q / Y * 2 - c2x) + std::abs(q % Y * 2 - c2y);
-                    int coord = s.xcnt.get(q / Y) + s.ycnt.get(q % Y);
+                    const int dist = s.kd[r];
+                    const int coord = s.xcnt.get(s.kx[r]) + s.ycnt.get(s.ky[r]);
                     if (sz > cnt_repeat) {
                         max_pos = q; max_rank = r; cnt_repeat = sz; max_coord = coord; min_dist = dist;
                     } else if (sz == cnt_repeat && coord > max_coord) {
