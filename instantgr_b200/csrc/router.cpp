@@ -614,6 +614,8 @@ void Router::restore_result(RouteBackup &b) {
     route_off = b.route_off;
     route_cap = b.route_cap;
     route_end = b.route_end;
+    d_route_off.upload(route_off, s);  // the device's offsets follow the host's
+    d_route_cap.upload(route_cap, s);
     st = b.st;
     score_wl = b.score[0];
     score_via = b.score[1];
@@ -764,20 +766,23 @@ void Router::fetch_routes() {
     }
     // Records sit at offsets with room for their largest size, and each
     // rip-up pass appends new ones: pack the live records on the device
-    // (lengths, scan, copy) and bring only those and their offsets back.
-    d_fetch_off.upload(route_off, s);
+    // (lengths, scan, copy) and bring only those and their offsets back.  The
+    // device holds the record offsets already (every pass brings them up to
+    // date there).
     d_dense_off.alloc((size_t)R + 1);
-    launch_record_offsets(routes.p, d_fetch_off.p, R, route_end, d_dense_off.p, s);
+    launch_record_offsets(routes.p, d_route_off.p, R, route_end, d_dense_off.p, s);
     cuda_check(cudaMemcpyAsync(h_route_at.data(), d_dense_off.p, ((size_t)R + 1) * 8, cudaMemcpyDeviceToHost, s),
                "D2H");
     cuda_check(cudaStreamSynchronize(s), "sync");
     const int64_t live = h_route_at[R];
     d_dense.alloc((size_t)live);
-    launch_record_copy(routes.p, d_fetch_off.p, R, d_dense_off.p, d_dense.p, s);
-    // Page-locked memory copies fastest, but locking a large new block costs
-    // more than the copy it speeds up: a large first copy goes to pageable memory.
+    launch_record_copy(routes.p, d_route_off.p, R, d_dense_off.p, d_dense.p, s);
+    // Page-locked memory copies fastest, but locking a very large new block
+    // costs more than the copy it speeds up: a first copy of more than 512 MB
+    // goes to pageable memory.  Smaller blocks are locked once and, given back
+    // to the process-wide cache when the router closes, serve the next ones.
     const size_t bytes = (size_t)live * sizeof(int);
-    if (bytes <= ((size_t)64 << 20) || (h_routes.p && h_routes.n >= (size_t)live) || pinned_cached(bytes)) {
+    if (bytes <= ((size_t)512 << 20) || (h_routes.p && h_routes.n >= (size_t)live) || pinned_cached(bytes)) {
         h_routes.alloc((size_t)live);
         h_routes_ptr = h_routes.p;
     } else {

@@ -230,7 +230,7 @@ struct Router {
     const int *h_routes_ptr = nullptr;
     std::vector<int64_t> h_route_at;     // [R+1] record of each routing net in the host copy
     bool h_routes_valid = false;
-    DevBuf<int64_t> d_fetch_off, d_dense_off;
+    DevBuf<int64_t> d_dense_off;
     DevBuf<int> d_dense;
     // ---- per-run device buffers (grow-only)
     DevBuf<int4> d_hdr;
