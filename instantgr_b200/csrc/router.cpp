@@ -295,6 +295,8 @@ Router::~Router() {
         if (s_cls[i]) cudaStreamDestroy(s_cls[i]);
     }
     if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_gfork) cudaEventDestroy(ev_gfork);
+    if (ev_gjoin) cudaEventDestroy(ev_gjoin);
     if (ev1) cudaEventDestroy(ev1);
     if (s) cudaStreamDestroy(s);
 }
@@ -410,6 +412,8 @@ void Router::create_grid() {
         cuda_check(cudaEventCreateWithFlags(&ev_join[i], cudaEventDisableTiming), "event");
     }
     cuda_check(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming), "event");
+    cuda_check(cudaEventCreateWithFlags(&ev_gfork, cudaEventDisableTiming), "event");
+    cuda_check(cudaEventCreateWithFlags(&ev_gjoin, cudaEventDisableTiming), "event");
     cuda_check(cudaEventCreate(&ev0), "event");
     cuda_check(cudaEventCreate(&ev1), "event");
     const int L = d.L - 1, X = d.X, Y = d.Y;
@@ -1459,6 +1463,10 @@ bool Router::rrr_pass(int iter) {
     for (size_t b = 0; b < bi.size(); b++) {
         const DagBatchInfo &f = bi[b];
         const int nnet = (int)batches[b].size();
+        if (b == 1 && gather_pending) {  // the later batches' DAGs were gathered on a side stream
+            cuda_check(cudaStreamWaitEvent(s, ev_gjoin, 0), "join");
+            gather_pending = false;
+        }
         ViaBatchDev old{dg_ids.p + f.nets, d_old_off.p, routes.p, nnet};
         const int s1 = ++global_stamp;
         kt.begin(KC_RIPUP);
@@ -1740,9 +1748,27 @@ bool Router::dags_on_device(std::vector<int> &of_nets, std::future<std::vector<i
     g.nodes = dg_nodes.p; g.par_off = dg_paroff.p; g.par = dg_par.p; g.child_slot = dg_cslot.p;
     g.edge_child = dg_echild.p; g.child_off = dg_childoff.p; g.level_off = dg_leveloff.p;
     g.level_nodes = dg_levelnodes.p; g.net_node_off = dg_nno.p; g.net_ids = dg_ids.p; g.net_level_off = dg_netlvl.p;
-    launch_dag_gather(g, s);
-    cuda_check(cudaGetLastError(), "DAG gather launch");
+    // the first batch's DAGs on the router's stream, the later batches' on a
+    // side stream beside the first batch's kernels (batch 1 waits for them)
+    const int n_first = B > 1 ? bi[1].nets : n;
+    if (n_first < n) {
+        cuda_check(cudaEventRecord(ev_gfork, s), "event");
+        cuda_check(cudaStreamWaitEvent(s_cls[1], ev_gfork, 0), "fork");
+    }
+    DagGatherArgs g0 = g;
+    g0.n = n_first;
+    launch_dag_gather(g0, s);
     st.launches += 1;
+    if (n_first < n) {
+        DagGatherArgs g1 = g;
+        g1.desc = g.desc + (size_t)n_first * kDagDescFields;
+        g1.n = n - n_first;
+        launch_dag_gather(g1, s_cls[1]);
+        cuda_check(cudaEventRecord(ev_gjoin, s_cls[1]), "event");
+        gather_pending = true;
+        st.launches += 1;
+    }
+    cuda_check(cudaGetLastError(), "DAG gather launch");
     if (verbose) {
         int64_t mx = 0, dmx = 0, tn = 0, te = 0, tp = 0;
         for (int i = 0; i < n; i++) {

@@ -198,6 +198,10 @@ struct Router {
     // on these streams, forked from and joined back into `s`
     cudaStream_t s_cls[2] = {nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+    // the DAG gather of a pass's later batches runs on s_cls[1] beside the
+    // first batch; batch 1 waits for ev_gjoin
+    cudaEvent_t ev_gfork = nullptr, ev_gjoin = nullptr;
+    bool gather_pending = false;
     RouterStats st;
     KernelTimer kt;
     int global_stamp = 0;
