@@ -299,6 +299,16 @@ Router::~Router() {
     if (ev_gjoin) cudaEventDestroy(ev_gjoin);
     if (ev1) cudaEventDestroy(ev1);
     if (s) cudaStreamDestroy(s);
+    // The host copy of the design and its routing nets (tens of ms of frees on
+    // the 800k-net design) goes on a thread of its own, beside whatever the
+    // caller does next; the nets' arenas return to a block cache that is never
+    // destroyed, so the frees may also outlast the program's static objects.
+    try {
+        auto host = std::make_unique<std::pair<Design, NetSet>>(std::move(d), std::move(ns));
+        std::thread([h = std::move(host)]() mutable { h.reset(); }).detach();
+    } catch (...) {
+        // no thread: the members are freed here, as they would be otherwise
+    }
 }
 
 void Router::open(const char *cap, const char *net) {
