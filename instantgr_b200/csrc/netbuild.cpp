@@ -409,7 +409,9 @@ void flatten_tree(const RNet &n, int *nodes, int *par) {
         st.push_back({e, px, id, 0});
         myidx.push_back(id);
     }
-    (void)cnt;
+    // slots of nodes the DFS did not reach (none for a connected tree) are
+    // zeroed, since the caller's arrays start uninitialised
+    for (int k = cnt; k < (int)n.tnode.size(); k++) nodes[k] = par[k] = 0;
 }
 
 }  // namespace igr

@@ -366,9 +366,19 @@ void Router::open(const char *cap, const char *net) {
         for (int i = 0; i < R; i++) order[i] = kv[i].second;
         return order;
     });
-    // trees in DFS preorder, net-id order, and the phase-1 route record layout
+    // trees in DFS preorder, net-id order, and the phase-1 route record layout:
+    // the nets' sizes and record capacities read in parallel, then the prefix
+    // sums over plain arrays
     tree_off.assign(R + 1, 0);
-    for (int i = 0; i < R; i++) tree_off[i + 1] = tree_off[i] + (int)ns.nets[i].tnode.size();
+    route_cap.assign(R, 0);
+    parallel_for(R, threads, [&](int b, int e) {
+        for (int i = b; i < e; i++) {
+            const auto &n = ns.nets[i];
+            tree_off[i + 1] = (int)n.tnode.size();
+            route_cap[i] = (int)std::max<int64_t>(12 * (int64_t)n.pins.size(), 8 * (int64_t)n.tnode.size() + 1);
+        }
+    });
+    for (int i = 0; i < R; i++) tree_off[i + 1] += tree_off[i];
     tree_nodes.resize(tree_off[R]);
     tree_par.resize(tree_off[R]);
     // algorithmic bytes of one phase-1 tree DP pass: per node the 8 via-column
@@ -391,14 +401,11 @@ void Router::open(const char *cap, const char *net) {
         }
     });
     route_off.assign(R, 0);
-    route_cap.assign(R, 0);
     route_end1 = 0;
     scratch_off.assign(R, -1);
     scratch_nodes = 0;
     int64_t dpb = 0;
     for (int i = 0; i < R; i++) {
-        const auto &n = ns.nets[i];
-        route_cap[i] = (int)std::max<int64_t>(12 * (int64_t)n.pins.size(), 8 * (int64_t)n.tnode.size() + 1);
         route_off[i] = route_end1;
         route_end1 += route_cap[i];
         const int cnt = tree_off[i + 1] - tree_off[i];
@@ -490,8 +497,8 @@ void Router::ensure_device() {
     const double t_grid = now_s();
     // resident inputs
     d_tree_off.upload(tree_off, s);
-    d_tree_nodes.upload(tree_nodes, s);
-    d_tree_par.upload(tree_par, s);
+    d_tree_nodes.upload(tree_nodes.data(), tree_nodes.size(), s);
+    d_tree_par.upload(tree_par.data(), tree_par.size(), s);
     d_scratch_off.upload(scratch_off, s);
     d_scratch.alloc((size_t)pattern_scratch_doubles(scratch_nodes));
     d_vcnt.alloc((size_t)go.g.N);

@@ -89,6 +89,23 @@ struct DevBuf {
 // Colour batch of a rip-up pass: its first entries in the pass-wide DAG
 // arrays (nodes, edges, nodes + 1 per net, depth levels, nets + 1, nets) and
 // its node, edge and child-slot counts.
+// Allocator whose value construction leaves ints uninitialised, for host
+// arrays that are filled in parallel right after they are sized (a serial zero
+// fill of the trees of 1.39M routing nets costs tens of milliseconds).
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind { using other = NoInitAlloc<U>; };
+    NoInitAlloc() = default;
+    template <class U>
+    NoInitAlloc(const NoInitAlloc<U> &) {}
+    template <class U, class... A>
+    void construct(U *p, A &&...a) {
+        if constexpr (sizeof...(A) == 0) ::new ((void *)p) U;
+        else ::new ((void *)p) U(std::forward<A>(a)...);
+    }
+};
+
 struct DagBatchInfo {
     int nb, eb, pb, lb, nnb, nets, n, e, slots;
     int mx_n, mx_e;  // the largest net's nodes and parent edges
@@ -208,7 +225,8 @@ struct Router {
     int mode_eff = 0;
 
     // ---- inputs resident in HBM after open(): trees and conflict shapes in net-id order
-    std::vector<int> tree_off, tree_nodes, tree_par;  // DFS preorder (Lshape_route.hpp:191-208)
+    std::vector<int> tree_off;                                    // DFS preorder (Lshape_route.hpp:191-208)
+    std::vector<int, NoInitAlloc<int>> tree_nodes, tree_par;
     std::vector<int64_t> scratch_off;                  // per net: DP scratch offset, -1 = on chip
     std::vector<int> order1;                           // phase-1 priority order (HPWL descending)
     int64_t scratch_nodes = 0;
