@@ -368,6 +368,9 @@ void build_netset(const Design &d, NetSet &ns, int threads) {
             if (part_of[id] >= 0) {
                 auto &pv = parts[part_of[id]];
                 for (int r = r0; r < r1; r++) ns.nets[r] = std::move(pv[r - r0]);
+                // the split's own copies are freed here, on the worker threads,
+                // not one by one on the calling thread when `parts` goes
+                std::vector<RNet>().swap(pv);
             } else {
                 RNet &r = ns.nets[r0];
                 r.orig = id;
