@@ -366,15 +366,31 @@ void select_pins(Design &d, int threads) {
                 ecount[t].push_back((int64_t)(extra[t].size() - e0));
             }
     });
-    d.sel_off.assign(1, 0); d.extra_off.assign(1, 0);
-    d.sel.clear(); d.extra.clear();
-    d.sel_off.reserve(N + 1); d.extra_off.reserve(N + 1);
+    // the ranges' selections go to their places in the design's arrays in
+    // parallel (and their buffers are freed there), at the prefix sums of
+    // the ranges' sizes
+    std::vector<int64_t> pb(T + 1, 0), eb(T + 1, 0);
     for (int t = 0; t < T; t++) {
-        for (auto c : pcount[t]) d.sel_off.push_back(d.sel_off.back() + c);
-        for (auto c : ecount[t]) d.extra_off.push_back(d.extra_off.back() + c);
-        d.sel.insert(d.sel.end(), pins[t].begin(), pins[t].end());
-        d.extra.insert(d.extra.end(), extra[t].begin(), extra[t].end());
+        pb[t + 1] = pb[t] + (int64_t)pins[t].size();
+        eb[t + 1] = eb[t] + (int64_t)extra[t].size();
     }
+    d.sel_off.assign(N + 1, 0); d.extra_off.assign(N + 1, 0);
+    d.sel.resize(pb[T]); d.extra.resize(eb[T]);
+    parallel_for(T, threads, [&](int b, int e) {
+        for (int t = b; t < e; t++) {
+            std::copy(pins[t].begin(), pins[t].end(), d.sel.begin() + pb[t]);
+            std::copy(extra[t].begin(), extra[t].end(), d.extra.begin() + eb[t]);
+            int64_t ps = pb[t], es = eb[t];
+            for (int n = lo[t]; n < lo[t + 1]; n++) {
+                ps += pcount[t][n - lo[t]];
+                es += ecount[t][n - lo[t]];
+                d.sel_off[n + 1] = ps;
+                d.extra_off[n + 1] = es;
+            }
+            std::vector<int>().swap(pins[t]);
+            std::vector<int>().swap(extra[t]);
+        }
+    });
 }
 
 }  // namespace igr
